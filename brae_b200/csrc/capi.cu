@@ -1,0 +1,643 @@
+// capi.cu -- the extern "C" boundary (include/brae_gamg.h): handles, status codes, the last-error
+// string, host/device argument staging, and the fvSolution entry reader with the reference's
+// refusals (readGamgControls, src/matrices/lduMatrix/solvers/GAMG/gamg_solver_cpp.cu:801-928, and
+// the PCG keys of src/applications/solvers/interFoam/inter_case_cpp.cu:1519-1572).
+#include "solver.cuh"
+
+#include <cctype>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+
+struct b2g_mesh
+{
+    b2g::Mesh m;
+};
+
+struct b2g_matrix
+{
+    b2g_mesh* mesh = nullptr;
+    std::unique_ptr<b2g::Matrix> mat;
+};
+
+namespace {
+
+thread_local std::string g_lastError;
+
+cudaStream_t streamOf(void* s) { return s ? static_cast<cudaStream_t>(s) : cudaStreamPerThread; }
+
+template <class F>
+b2g_status guarded(F&& f)
+{
+    try
+    {
+        f();
+        return B2G_OK;
+    }
+    catch (const b2g::Error& e)
+    {
+        g_lastError = e.what();
+        return e.code;
+    }
+    catch (const std::bad_alloc&)
+    {
+        g_lastError = "b2g: host allocation failed";
+        return B2G_ERR_NO_MEMORY;
+    }
+    catch (const std::exception& e)
+    {
+        g_lastError = e.what();
+        return B2G_ERR_STATE;
+    }
+}
+
+void need(bool ok, const char* msg)
+{
+    if (!ok) b2g::fail(B2G_ERR_ARGUMENT, msg);
+}
+
+template <class T>
+void stage(b2g::DBuf<T>& d, const T* src, size_t n, int memspace, cudaStream_t s)
+{
+    d.alloc(n, s);
+    if (!n) return;
+    B2G_CUDA(cudaMemcpyAsync(d.p, src, n * sizeof(T),
+                             memspace == B2G_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
+}
+
+// ---------------------------------------------------------------------------------------------
+// a minimal OpenFOAM dictionary: `key value;` and `key { ... }`, with // and /* */ comments
+// ---------------------------------------------------------------------------------------------
+
+struct Dict
+{
+    std::map<std::string, std::string> words;
+    std::map<std::string, std::unique_ptr<Dict>> subs;
+    bool found(const std::string& k) const { return words.count(k) || subs.count(k); }
+    const Dict* sub(const std::string& k) const
+    {
+        auto it = subs.find(k);
+        return it == subs.end() ? nullptr : it->second.get();
+    }
+    std::string wordOr(const std::string& k, const std::string& d) const
+    {
+        auto it = words.find(k);
+        return it == words.end() ? d : it->second;
+    }
+};
+
+std::vector<std::string> tokenize(const std::string& t)
+{
+    std::vector<std::string> out;
+    size_t i = 0;
+    while (i < t.size())
+    {
+        const char c = t[i];
+        if (std::isspace(static_cast<unsigned char>(c))) { ++i; continue; }
+        if (c == '/' && i + 1 < t.size() && t[i + 1] == '/')
+        {
+            while (i < t.size() && t[i] != '\n') ++i;
+            continue;
+        }
+        if (c == '/' && i + 1 < t.size() && t[i + 1] == '*')
+        {
+            const size_t e = t.find("*/", i + 2);
+            i = e == std::string::npos ? t.size() : e + 2;
+            continue;
+        }
+        if (c == '{' || c == '}' || c == ';')
+        {
+            out.emplace_back(1, c);
+            ++i;
+            continue;
+        }
+        if (c == '"')
+        {
+            const size_t e = t.find('"', i + 1);
+            out.push_back(t.substr(i + 1, (e == std::string::npos ? t.size() : e) - i - 1));
+            i = e == std::string::npos ? t.size() : e + 1;
+            continue;
+        }
+        size_t j = i;
+        while (j < t.size() && !std::isspace(static_cast<unsigned char>(t[j])) && t[j] != '{' && t[j] != '}' &&
+               t[j] != ';')
+            ++j;
+        out.push_back(t.substr(i, j - i));
+        i = j;
+    }
+    return out;
+}
+
+void parseInto(Dict& d, const std::vector<std::string>& tok, size_t& i, bool nested)
+{
+    while (i < tok.size())
+    {
+        if (tok[i] == "}")
+        {
+            if (!nested) b2g::fail(B2G_ERR_ARGUMENT, "b2g: unbalanced '}' in the solver entry.");
+            ++i;
+            return;
+        }
+        if (tok[i] == ";") { ++i; continue; }
+        const std::string key = tok[i++];
+        if (i < tok.size() && tok[i] == "{")
+        {
+            ++i;
+            auto sub = std::make_unique<Dict>();
+            parseInto(*sub, tok, i, true);
+            d.subs[key] = std::move(sub);
+            continue;
+        }
+        std::string val;
+        while (i < tok.size() && tok[i] != ";" && tok[i] != "}")
+        {
+            if (!val.empty()) val += ' ';
+            val += tok[i++];
+        }
+        if (i < tok.size() && tok[i] == ";") ++i;
+        d.words[key] = val;
+    }
+    if (nested) b2g::fail(B2G_ERR_ARGUMENT, "b2g: unbalanced '{' in the solver entry.");
+}
+
+double scalarOr(const Dict& d, const std::string& k, double def, const std::string& who)
+{
+    if (!d.words.count(k)) return def;
+    const std::string v = d.wordOr(k, "");
+    char* end = nullptr;
+    const double x = std::strtod(v.c_str(), &end);
+    if (end == v.c_str() || *end != '\0') b2g::fail(B2G_ERR_ARGUMENT, who + "has `" + k + " " + v + "`, not a number.");
+    return x;
+}
+
+int intOr(const Dict& d, const std::string& k, int def, const std::string& who)
+{
+    return static_cast<int>(scalarOr(d, k, def, who));
+}
+
+bool switchOr(const Dict& d, const std::string& k, bool def, const std::string& who)
+{
+    if (!d.found(k)) return def;
+    const std::string w = d.wordOr(k, "");
+    if (w == "yes" || w == "true" || w == "on" || w == "y" || w == "t" || w == "1") return true;
+    if (w == "no" || w == "false" || w == "off" || w == "n" || w == "f" || w == "0") return false;
+    b2g::fail(B2G_ERR_REFUSED, who + "has `" + k + " " + w + "`, which is not a Switch.");
+}
+
+// readGamgControls (gamg_solver_cpp.cu:801-928) on a GAMG dictionary
+void readGamg(const Dict& d, b2g_controls& c, const std::string& who)
+{
+    const std::string sm = d.wordOr("smoother", "");
+    if (sm.empty())
+        b2g::fail(B2G_ERR_REFUSED, who + "names no `smoother`. lduMatrix::smoother::New reads it with a mandatory "
+                                         "lookup and OpenFOAM stops without it.");
+    if (sm == "GaussSeidel") c.smoother = B2G_SMOOTHER_GAUSS_SEIDEL;
+    else if (sm == "symGaussSeidel") c.smoother = B2G_SMOOTHER_SYM_GAUSS_SEIDEL;
+    else if (sm == "DIC") c.smoother = B2G_SMOOTHER_DIC;
+    else if (sm == "DICGaussSeidel") c.smoother = B2G_SMOOTHER_DIC_GAUSS_SEIDEL;
+    else if (sm == "DILU" || sm == "DILUGaussSeidel")
+        b2g::fail(B2G_ERR_REFUSED,
+                  who + "asks for `smoother " + sm + "`, which OpenFOAM registers for an ASYMMETRIC matrix only. "
+                  "This matrix is symmetric, so OpenFOAM's own lookup stops: `Unknown symmetric matrix smoother "
+                  "type " + sm + "`. The symmetric smoothers are DIC, DICGaussSeidel, FDIC, GaussSeidel, "
+                  "symGaussSeidel and nonBlockingGaussSeidel.");
+    else
+        b2g::fail(B2G_ERR_REFUSED,
+                  who + "asks for `smoother " + sm + "`, which is not ported: DIC, DICGaussSeidel, GaussSeidel and "
+                  "symGaussSeidel are." +
+                      ((sm == "FDIC" || sm == "nonBlockingGaussSeidel")
+                           ? std::string(" OpenFOAM does accept it on a symmetric matrix.")
+                           : std::string(" OpenFOAM has no smoother of that name either.")));
+    c.nPreSweeps = intOr(d, "nPreSweeps", c.nPreSweeps, who);
+    c.preSweepsLevelMultiplier = intOr(d, "preSweepsLevelMultiplier", c.preSweepsLevelMultiplier, who);
+    c.maxPreSweeps = intOr(d, "maxPreSweeps", c.maxPreSweeps, who);
+    c.nPostSweeps = intOr(d, "nPostSweeps", c.nPostSweeps, who);
+    c.postSweepsLevelMultiplier = intOr(d, "postSweepsLevelMultiplier", c.postSweepsLevelMultiplier, who);
+    c.maxPostSweeps = intOr(d, "maxPostSweeps", c.maxPostSweeps, who);
+    c.nFinestSweeps = intOr(d, "nFinestSweeps", c.nFinestSweeps, who);
+    c.scaleCorrection = switchOr(d, "scaleCorrection", true, who) ? 1 : 0;
+    c.nCellsInCoarsestLevel = intOr(d, "nCellsInCoarsestLevel", 10, who);
+    const std::string agg = d.wordOr("agglomerator", "faceAreaPair");
+    if (agg != "faceAreaPair")
+        b2g::fail(B2G_ERR_REFUSED, who + "asks for `agglomerator " + agg + "`. Only faceAreaPair is built; another "
+                                         "agglomerator is another hierarchy.");
+    if (intOr(d, "mergeLevels", 1, who) != 1)
+        b2g::fail(B2G_ERR_REFUSED, who + "asks for `mergeLevels " + d.wordOr("mergeLevels", "") +
+                                         "`. pairGAMGAgglomeration then folds pairs of levels into one "
+                                         "(combineLevels), which is not built.");
+    if (intOr(d, "updateInterval", 1, who) != 1)
+        b2g::fail(B2G_ERR_REFUSED, who + "sets `updateInterval`. faceAreaPairGAMGAgglomeration then weighs faces by "
+                                         "magSf off the update steps; only the default's branch is built.");
+    if (!switchOr(d, "cacheAgglomeration", true, who))
+        b2g::fail(B2G_ERR_REFUSED, who + "sets `cacheAgglomeration no`. The hierarchy is then rebuilt at every solve "
+                                         "from wherever the static pairing direction was left; it is built once here.");
+    if (switchOr(d, "interpolateCorrection", false, who))
+        b2g::fail(B2G_ERR_REFUSED, who + "sets `interpolateCorrection yes` (GAMGSolverInterpolate.C), which is not built.");
+    if (switchOr(d, "directSolveCoarsest", false, who))
+        b2g::fail(B2G_ERR_REFUSED, who + "sets `directSolveCoarsest yes`. The coarsest level is then LU-factored rather "
+                                         "than solved by PCG to the entry's tolerance (GAMGSolver.C:303), which is "
+                                         "not built.");
+    if (d.sub("coarsestLevelCorr"))
+        b2g::fail(B2G_ERR_REFUSED, who + "carries a `coarsestLevelCorr` sub-dictionary. GAMGSolver then builds the "
+                                         "coarsest level's solver from it instead of PCG with DIC at the entry's own "
+                                         "tolerance.");
+    if (d.found("processorAgglomerator"))
+        b2g::fail(B2G_ERR_REFUSED, who + "names a `processorAgglomerator`. This is a serial solver.");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* b2g_last_error(void) { return g_lastError.c_str(); }
+
+const char* b2g_version(void) { return "brae_b200 0.1 (sm_100a)"; }
+
+b2g_status b2g_set_profiling(int on)
+{
+    b2g::g_profiling = on != 0;
+    return B2G_OK;
+}
+
+b2g_status b2g_controls_default(b2g_controls* out)
+{
+    return guarded([&] {
+        need(out != nullptr, "b2g_controls_default: null output");
+        b2g_controls c;
+        c.solver = B2G_SOLVER_PCG_GAMG;
+        c.tolerance = 1e-6;
+        c.relTol = 0.0;
+        c.maxIter = 1000;
+        c.minIter = 0;
+        c.smoother = B2G_SMOOTHER_GAUSS_SEIDEL;
+        c.precTolerance = 1e-6;
+        c.precRelTol = 0.0;
+        c.nPreSweeps = 0;
+        c.preSweepsLevelMultiplier = 1;
+        c.maxPreSweeps = 4;
+        c.nPostSweeps = 2;
+        c.postSweepsLevelMultiplier = 1;
+        c.maxPostSweeps = 4;
+        c.nFinestSweeps = 2;
+        c.scaleCorrection = 1;
+        c.nCellsInCoarsestLevel = 10;
+        c.nVcycles = 2;
+        c.precision = B2G_PRECISION_FP64;
+        *out = c;
+    });
+}
+
+b2g_status b2g_controls_read(const char* text, b2g_controls* out)
+{
+    return guarded([&] {
+        need(text != nullptr && out != nullptr, "b2g_controls_read: null argument");
+        b2g_controls c;
+        b2g_controls_default(&c);
+        Dict d;
+        const std::vector<std::string> tok = tokenize(text);
+        size_t i = 0;
+        parseInto(d, tok, i, false);
+        const std::string who = "b2g: fvSolution's solver entry ";
+        const std::string solver = d.wordOr("solver", "");
+        // lduMatrix::solver::readControls: tolerance 1e-6, relTol 0, maxIter 1000 when absent
+        c.tolerance = scalarOr(d, "tolerance", 1e-6, who);
+        c.relTol = scalarOr(d, "relTol", 0.0, who);
+        c.maxIter = static_cast<int>(scalarOr(d, "maxIter", 1000, who));
+        c.minIter = intOr(d, "minIter", 0, who);
+        if (solver == "GAMG")
+        {
+            c.solver = B2G_SOLVER_GAMG;
+            readGamg(d, c, who);
+            c.precTolerance = c.tolerance;
+            c.precRelTol = c.relTol;
+        }
+        else if (solver == "PCG")
+        {
+            c.solver = B2G_SOLVER_PCG_GAMG;
+            const Dict* pd = d.sub("preconditioner");
+            if (!pd)
+                b2g::fail(B2G_ERR_REFUSED,
+                          who + "names `preconditioner " + d.wordOr("preconditioner", "") +
+                              "`. This solver is PCG with a `preconditioner { preconditioner GAMG; ... }` "
+                              "sub-dictionary, the form whose controls GAMG reads.");
+            const std::string name = pd->wordOr("preconditioner", "");
+            if (name != "GAMG")
+                b2g::fail(B2G_ERR_REFUSED, who + "has `preconditioner { preconditioner " + name +
+                                                 "; }`. Only the GAMG preconditioner is built here.");
+            const std::string pwho = who + "(its GAMG preconditioner) ";
+            readGamg(*pd, c, pwho);
+            // lduMatrix::solver::readControls on the sub-dictionary: its own defaults
+            c.precTolerance = scalarOr(*pd, "tolerance", 1e-6, pwho);
+            c.precRelTol = scalarOr(*pd, "relTol", 0.0, pwho);
+            c.nVcycles = intOr(*pd, "nVcycles", 2, pwho);
+            if (c.nVcycles < 1) b2g::fail(B2G_ERR_REFUSED, "b2g GAMG preconditioner: nVcycles must be at least 1.");
+        }
+        else
+        {
+            b2g::fail(B2G_ERR_REFUSED, who + "names `solver " + solver + "`. This library solves `solver PCG;` with "
+                                             "the GAMG preconditioner and `solver GAMG;`.");
+        }
+        *out = c;
+    });
+}
+
+b2g_status b2g_mesh_create(int nCells, int nFaces, const int32_t* lower, const int32_t* upper, const double* Sf,
+                           const double* magSf, int nCellsInCoarsestLevel, int* forwardInOut, int memspace,
+                           void* stream, b2g_mesh** out)
+{
+    return guarded([&] {
+        need(out != nullptr, "b2g_mesh_create: null output handle");
+        *out = nullptr;
+        need(nCells > 0 && nFaces >= 0, "b2g_mesh_create: nCells must be positive and nFaces non-negative");
+        need(nFaces == 0 || (lower && upper && Sf && magSf), "b2g_mesh_create: null array");
+        need(forwardInOut != nullptr, "b2g_mesh_create: null direction flag");
+        need(memspace == B2G_MEM_HOST || memspace == B2G_MEM_DEVICE, "b2g_mesh_create: bad memspace");
+        std::unique_ptr<b2g_mesh> h(new b2g_mesh);
+        b2g::Mesh& M = h->m;
+        M.stream = streamOf(stream);
+        cudaGetDevice(&M.device);
+        cudaEvent_t e0, e1;
+        B2G_CUDA(cudaEventCreate(&e0));
+        B2G_CUDA(cudaEventCreate(&e1));
+        B2G_CUDA(cudaEventRecord(e0, M.stream));
+        M.lev.emplace_back();
+        b2g::LevelAddr& L0 = M.lev[0];
+        L0.nCells = nCells;
+        L0.nFaces = nFaces;
+        stage(L0.lower, lower, nFaces, memspace, M.stream);
+        stage(L0.upper, upper, nFaces, memspace, M.stream);
+        b2g::DBuf<double> dSf, dMag;
+        stage(dSf, Sf, 3 * (size_t)nFaces, memspace, M.stream);
+        stage(dMag, magSf, nFaces, memspace, M.stream);
+        b2g::buildHierarchy(M, dSf.p, dMag.p, nCellsInCoarsestLevel, forwardInOut);
+        B2G_CUDA(cudaEventRecord(e1, M.stream));
+        B2G_CUDA(cudaEventSynchronize(e1));
+        B2G_CUDA(cudaEventElapsedTime(&M.buildMs, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        *out = h.release();
+    });
+}
+
+b2g_status b2g_mesh_destroy(b2g_mesh* mesh)
+{
+    return guarded([&] {
+        if (!mesh) return;
+        cudaStream_t s = mesh->m.stream;
+        delete mesh;
+        B2G_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+b2g_status b2g_mesh_levels(const b2g_mesh* mesh, int* nLevels)
+{
+    return guarded([&] {
+        need(mesh && nLevels, "b2g_mesh_levels: null argument");
+        *nLevels = mesh->m.nLevels();
+    });
+}
+
+b2g_status b2g_mesh_level_size(const b2g_mesh* mesh, int level, int* nCells, int* nFaces)
+{
+    return guarded([&] {
+        need(mesh && nCells && nFaces, "b2g_mesh_level_size: null argument");
+        need(level >= 0 && level <= mesh->m.nLevels(), "b2g_mesh_level_size: level out of range");
+        *nCells = mesh->m.lev[level].nCells;
+        *nFaces = mesh->m.lev[level].nFaces;
+    });
+}
+
+b2g_status b2g_mesh_get_step(const b2g_mesh* mesh, int step, int32_t* restrictAddr, int32_t* faceRestrict,
+                             int8_t* flip, int32_t* coarseLower, int32_t* coarseUpper)
+{
+    return guarded([&] {
+        need(mesh != nullptr, "b2g_mesh_get_step: null mesh");
+        const b2g::Mesh& M = mesh->m;
+        need(step >= 0 && step < M.nLevels(), "b2g_mesh_get_step: step out of range");
+        const b2g::Step& S = M.step[step];
+        const b2g::LevelAddr& C = M.lev[step + 1];
+        cudaStream_t s = M.stream;
+        if (restrictAddr)
+            B2G_CUDA(cudaMemcpyAsync(restrictAddr, S.restrictAddr.p, sizeof(int) * S.nFine, cudaMemcpyDeviceToHost, s));
+        if (faceRestrict && S.nFineFaces)
+            B2G_CUDA(cudaMemcpyAsync(faceRestrict, S.faceRestrict.p, sizeof(int) * S.nFineFaces,
+                                     cudaMemcpyDeviceToHost, s));
+        if (flip && S.nFineFaces)
+            B2G_CUDA(cudaMemcpyAsync(flip, S.flip.p, S.nFineFaces, cudaMemcpyDeviceToHost, s));
+        if (coarseLower && C.nFaces)
+            B2G_CUDA(cudaMemcpyAsync(coarseLower, C.lower.p, sizeof(int) * C.nFaces, cudaMemcpyDeviceToHost, s));
+        if (coarseUpper && C.nFaces)
+            B2G_CUDA(cudaMemcpyAsync(coarseUpper, C.upper.p, sizeof(int) * C.nFaces, cudaMemcpyDeviceToHost, s));
+        B2G_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+b2g_status b2g_mesh_build_ms(const b2g_mesh* mesh, float* ms)
+{
+    return guarded([&] {
+        need(mesh && ms, "b2g_mesh_build_ms: null argument");
+        *ms = mesh->m.buildMs;
+    });
+}
+
+b2g_status b2g_matrix_create(b2g_mesh* mesh, const double* diag, const double* upper, int memspace, void* stream,
+                             b2g_matrix** out)
+{
+    return guarded([&] {
+        need(mesh && out && diag, "b2g_matrix_create: null argument");
+        need(memspace == B2G_MEM_HOST || memspace == B2G_MEM_DEVICE, "b2g_matrix_create: bad memspace");
+        need(mesh->m.lev[0].nFaces == 0 || upper, "b2g_matrix_create: null upper");
+        std::unique_ptr<b2g_matrix> h(new b2g_matrix);
+        h->mesh = mesh;
+        (void)stream;
+        h->mat.reset(new b2g::Matrix(&mesh->m, mesh->m.stream));
+        h->mat->setFine(diag, upper, memspace);
+        h->mat->buildCoarse();
+        B2G_CUDA(cudaStreamSynchronize(mesh->m.stream));
+        *out = h.release();
+    });
+}
+
+b2g_status b2g_matrix_destroy(b2g_matrix* m)
+{
+    return guarded([&] {
+        if (!m) return;
+        cudaStream_t s = m->mesh->m.stream;
+        delete m;
+        B2G_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+b2g_status b2g_matrix_get_level(const b2g_matrix* m, int level, double* diag, double* upper)
+{
+    return guarded([&] {
+        need(m != nullptr, "b2g_matrix_get_level: null matrix");
+        const b2g::Matrix& A = *m->mat;
+        need(level >= 0 && level <= A.nLevels(), "b2g_matrix_get_level: level out of range");
+        const b2g::LevelAddr& L = A.mesh->lev[level];
+        cudaStream_t s = A.stream;
+        if (diag)
+            B2G_CUDA(cudaMemcpyAsync(diag, A.v64.coef[level].diag.p, sizeof(double) * L.nCells, cudaMemcpyDeviceToHost, s));
+        if (upper && L.nFaces)
+            B2G_CUDA(cudaMemcpyAsync(upper, A.v64.coef[level].upper.p, sizeof(double) * L.nFaces,
+                                     cudaMemcpyDeviceToHost, s));
+        B2G_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+b2g_status b2g_level_amul(b2g_matrix* m, int level, const double* x, double* y)
+{
+    return guarded([&] {
+        need(m && x && y, "b2g_level_amul: null argument");
+        need(level >= 0 && level <= m->mat->nLevels(), "b2g_level_amul: level out of range");
+        m->mat->amul<double>(level, x, y);
+        B2G_CUDA(cudaStreamSynchronize(m->mat->stream));
+    });
+}
+
+b2g_status b2g_level_smooth(b2g_matrix* m, int level, int smoother, double* psi, const double* source, int nSweeps)
+{
+    return guarded([&] {
+        need(m && psi && source, "b2g_level_smooth: null argument");
+        need(level >= 0 && level <= m->mat->nLevels(), "b2g_level_smooth: level out of range");
+        m->mat->smooth<double>(level, smoother, psi, source, nSweeps);
+        m->mat->checkDeviceError();
+    });
+}
+
+b2g_status b2g_level_scale(b2g_matrix* m, int level, double* field, double* Acf, const double* source)
+{
+    return guarded([&] {
+        need(m && field && Acf && source, "b2g_level_scale: null argument");
+        need(level >= 0 && level <= m->mat->nLevels(), "b2g_level_scale: level out of range");
+        m->mat->scale<double>(level, field, Acf, source);
+        B2G_CUDA(cudaStreamSynchronize(m->mat->stream));
+    });
+}
+
+b2g_status b2g_step_restrict(b2g_matrix* m, int step, const double* fine, double* coarse)
+{
+    return guarded([&] {
+        need(m && fine && coarse, "b2g_step_restrict: null argument");
+        need(step >= 0 && step < m->mat->nLevels(), "b2g_step_restrict: step out of range");
+        m->mat->restrictTo<double>(step, fine, coarse);
+        B2G_CUDA(cudaStreamSynchronize(m->mat->stream));
+    });
+}
+
+b2g_status b2g_step_prolong(b2g_matrix* m, int step, const double* coarse, double* fine)
+{
+    return guarded([&] {
+        need(m && fine && coarse, "b2g_step_prolong: null argument");
+        need(step >= 0 && step < m->mat->nLevels(), "b2g_step_prolong: step out of range");
+        m->mat->prolongFrom<double>(step, coarse, fine);
+        B2G_CUDA(cudaStreamSynchronize(m->mat->stream));
+    });
+}
+
+b2g_status b2g_level_norm_factor(b2g_matrix* m, int level, const double* psi, const double* source,
+                                 const double* Apsi, double* nf)
+{
+    return guarded([&] {
+        need(m && psi && source && Apsi && nf, "b2g_level_norm_factor: null argument");
+        need(level >= 0 && level <= m->mat->nLevels(), "b2g_level_norm_factor: level out of range");
+        *nf = m->mat->normFactor(level, psi, source, Apsi);
+    });
+}
+
+b2g_status b2g_level_pcg_dic(b2g_matrix* m, int level, double* psi, const double* source, double tolerance,
+                             double relTol, b2g_perf* out)
+{
+    return guarded([&] {
+        need(m && psi && source && out, "b2g_level_pcg_dic: null argument");
+        need(level >= 0 && level <= m->mat->nLevels(), "b2g_level_pcg_dic: level out of range");
+        b2g::Matrix& A = *m->mat;
+        const int n = A.mesh->lev[level].nCells;
+        if (static_cast<int>(A.v64.cpA.n) < n)
+            for (b2g::DBuf<double>* b : {&A.v64.cpA, &A.v64.cwA, &A.v64.crA, &A.v64.crD}) b->alloc(n, A.stream);
+        b2g::DBuf<b2g::k::DevPerf> dp;
+        dp.alloc(1, A.stream);
+        A.coarsestSolve<double>(level, psi, source, tolerance, relTol, dp.p, false);
+        std::vector<b2g::k::DevPerf> h = dp.download(A.stream);
+        out->initialResidual = h[0].initialResidual;
+        out->finalResidual = h[0].finalResidual;
+        out->nIterations = h[0].nIterations;
+    });
+}
+
+b2g_status b2g_precondition(b2g_matrix* m, const b2g_controls* controls, double* w, const double* r,
+                            b2g_solve_log* log)
+{
+    return guarded([&] {
+        need(m && controls && w && r, "b2g_precondition: null argument");
+        b2g::Matrix& A = *m->mat;
+        need(A.nLevels() > 0, "b2g_precondition: the mesh has no coarse levels");
+        A.resetLog(log ? std::max(log->coarsestCapacity, 0) : 0);
+        A.precondition(*controls, w, r);
+        A.checkDeviceError();
+        A.readLog(log);
+    });
+}
+
+static void solveOn(b2g::Matrix& A, const double* source, double* psi, const b2g_controls* c, int memspace,
+                    b2g_perf* out, b2g_solve_log* log, bool standalone)
+{
+    need(c && source && psi && out, "b2g solve: null argument");
+    need(memspace == B2G_MEM_HOST || memspace == B2G_MEM_DEVICE, "b2g solve: bad memspace");
+    const int n0 = A.n(0);
+    const cudaMemcpyKind in = memspace == B2G_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    const cudaMemcpyKind outK = memspace == B2G_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    B2G_CUDA(cudaMemcpyAsync(A.source.p, source, sizeof(double) * n0, in, A.stream));
+    B2G_CUDA(cudaMemcpyAsync(A.psi.p, psi, sizeof(double) * n0, in, A.stream));
+    *out = standalone ? A.gamg(*c, log) : A.pcg(*c, log);
+    B2G_CUDA(cudaMemcpyAsync(psi, A.psi.p, sizeof(double) * n0, outK, A.stream));
+    B2G_CUDA(cudaStreamSynchronize(A.stream));
+}
+
+b2g_status b2g_matrix_pcg_solve(b2g_matrix* m, const double* source, double* psi, const b2g_controls* controls,
+                                int memspace, b2g_perf* out, b2g_solve_log* log)
+{
+    return guarded([&] {
+        need(m != nullptr, "b2g_matrix_pcg_solve: null matrix");
+        solveOn(*m->mat, source, psi, controls, memspace, out, log, false);
+    });
+}
+
+b2g_status b2g_pcg_gamg_solve(b2g_mesh* mesh, const double* diag, const double* upper, const double* source,
+                              double* psi, const b2g_controls* controls, int memspace, void* stream, b2g_perf* out,
+                              b2g_solve_log* log)
+{
+    return guarded([&] {
+        need(mesh && diag && controls, "b2g_pcg_gamg_solve: null argument");
+        (void)stream;
+        b2g::Matrix A(&mesh->m, mesh->m.stream);
+        A.setFine(diag, upper, memspace);
+        solveOn(A, source, psi, controls, memspace, out, log, false);
+    });
+}
+
+b2g_status b2g_gamg_solve(b2g_mesh* mesh, const double* diag, const double* upper, const double* source,
+                          double* psi, const b2g_controls* controls, int memspace, void* stream, b2g_perf* out,
+                          b2g_solve_log* log)
+{
+    return guarded([&] {
+        need(mesh && diag && controls, "b2g_gamg_solve: null argument");
+        (void)stream;
+        b2g::Matrix A(&mesh->m, mesh->m.stream);
+        A.setFine(diag, upper, memspace);
+        solveOn(A, source, psi, controls, memspace, out, log, true);
+    });
+}
+
+b2g_status b2g_matrix_timings(const b2g_matrix* m, double* ms4, long long* launches)
+{
+    return guarded([&] {
+        need(m != nullptr, "b2g_matrix_timings: null matrix");
+        if (ms4)
+            for (int i = 0; i < 4; ++i) ms4[i] = m->mat->ms[i];
+        if (launches) *launches = m->mat->launches;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,216 @@
+// coarsest_kernels.cuh -- the coarsest-level solve: PCG with DIC from the psi handed in, to the
+// preconditioner entry's tolerance and relTol, maxIter 1000 (gamg_solver_cpp.cu:321-383), in ONE
+// warp. The coarsest level has nCellsInCoarsestLevel..2x cells (10-20 by default), so the whole
+// solve is a few thousand dependent operations: it stays on the device (the reference's device arm
+// copies it to the host and back every V-cycle, device_gamg_solver.cu:549-569). Sums and the DIC
+// substitution run serially on lane 0 in the reference's order (they decide the iteration count);
+// element-wise work is spread over the lanes. Scratch lives in global memory (L1-resident).
+#pragma once
+
+#include "b2g_common.cuh"
+
+namespace b2g {
+namespace k {
+
+struct DevPerf
+{
+    double initialResidual;
+    double finalResidual;
+    int nIterations;
+    int pad;
+};
+
+template <class T>
+struct CoarsestArgs
+{
+    int n, nF;
+    const int* __restrict__ lower;
+    const int* __restrict__ upper;
+    const int* __restrict__ rowStart;
+    const int* __restrict__ col;
+    const T* __restrict__ val;
+    const T* __restrict__ diag;
+    const T* __restrict__ coef;  // LDU upper
+    const T* source;
+    T* psi;
+    T* pA;
+    T* wA;
+    T* rA;
+    T* rD;
+    T tolerance;
+    T relTol;
+    int maxIter;
+    DevPerf* log;       // may be null
+    int* logCount;      // appended when log != null
+    int logCapacity;
+    DevPerf* out;       // may be null
+};
+
+template <class T> struct PerfConst;
+template <> struct PerfConst<double>
+{
+    static constexpr double small = 1e-20, vsmall = 1e-300, great = 1e+20;
+};
+template <> struct PerfConst<float>
+{
+    static constexpr float small = 1e-20f, vsmall = 1e-37f, great = 1e+20f;
+};
+
+template <class T>
+__device__ __forceinline__ void warpAmul(const CoarsestArgs<T>& a, const T* x, T* y)
+{
+    for (int c = threadIdx.x; c < a.n; c += 32)
+    {
+        T acc = mulRn(a.diag[c], x[c]);
+        for (int e = a.rowStart[c]; e < a.rowStart[c + 1]; ++e) acc = addRn(acc, mulRn(a.val[e], x[a.col[e]]));
+        y[c] = acc;
+    }
+    __syncwarp();
+}
+
+template <class T>
+__device__ __forceinline__ T serialSumProd(int n, const T* x, const T* y)
+{
+    T s = T(0);
+    for (int i = 0; i < n; ++i) s = addRn(s, mulRn(x[i], y[i]));
+    return s;
+}
+
+template <class T>
+__device__ __forceinline__ T serialSumMag(int n, const T* x)
+{
+    T s = T(0);
+    for (int i = 0; i < n; ++i) s = addRn(s, fabs(x[i]));
+    return s;
+}
+
+template <class T>
+__device__ __forceinline__ bool convergedT(T fin, T init, T tol, T relTol)
+{
+    return fin < tol || (relTol > PerfConst<T>::small && fin < mulRn(relTol, init));
+}
+
+// One warp (blockDim.x == 32).
+template <class T>
+__global__ void __launch_bounds__(32) coarsestPcgDic(CoarsestArgs<T> a)
+{
+    __shared__ T shScal[4];  // nf, init, final, flag
+    __shared__ int shIter;
+    __shared__ int shStop;
+    const int lane = threadIdx.x;
+    const int n = a.n;
+    warpAmul(a, a.psi, a.wA);
+    for (int c = lane; c < n; c += 32) a.rA[c] = subRn(a.source[c], a.wA[c]);
+    // normFactor's row sums into pA (scratch, as the reference uses it)
+    for (int c = lane; c < n; c += 32)
+    {
+        T s = a.diag[c];
+        for (int e = a.rowStart[c]; e < a.rowStart[c + 1]; ++e) s = addRn(s, a.val[e]);
+        a.pA[c] = s;
+    }
+    __syncwarp();
+    if (lane == 0)
+    {
+        T avg = T(0);
+        for (int c = 0; c < n; ++c) avg = addRn(avg, a.psi[c]);
+        avg = divRn(avg, static_cast<T>(n));
+        T sum = T(0);
+        for (int c = 0; c < n; ++c)
+        {
+            const T t = mulRn(a.pA[c], avg);
+            sum = addRn(sum, addRn(fabs(subRn(a.wA[c], t)), fabs(subRn(a.source[c], t))));
+        }
+        const T nf = addRn(sum, PerfConst<T>::small);
+        const T init = divRn(serialSumMag(n, a.rA), nf);
+        shScal[0] = nf;
+        shScal[1] = init;
+        shScal[2] = init;
+        shIter = 0;
+        shStop = convergedT(init, init, a.tolerance, a.relTol) ? 1 : 0;
+        if (!shStop)
+        {
+            // DICPreconditioner::calcReciprocalD (GAMG:194-210)
+            for (int c = 0; c < n; ++c) a.rD[c] = a.diag[c];
+            for (int f = 0; f < a.nF; ++f)
+            {
+                const int u = a.upper[f];
+                a.rD[u] = subRn(a.rD[u], divRn(mulRn(a.coef[f], a.coef[f]), a.rD[a.lower[f]]));
+            }
+            for (int c = 0; c < n; ++c) a.rD[c] = divRn(T(1), a.rD[c]);
+        }
+    }
+    __syncwarp();
+    __syncthreads();
+    T wArA = PerfConst<T>::great;
+    const T nf = shScal[0];
+    while (!shStop)
+    {
+        const T wArAold = wArA;
+        for (int c = lane; c < n; c += 32) a.wA[c] = mulRn(a.rD[c], a.rA[c]);
+        __syncwarp();
+        if (lane == 0)
+        {
+            // the two DIC substitution passes (GAMG:212-231)
+            for (int f = 0; f < a.nF; ++f)
+            {
+                const int u = a.upper[f];
+                a.wA[u] = subRn(a.wA[u], mulRn(mulRn(a.rD[u], a.coef[f]), a.wA[a.lower[f]]));
+            }
+            for (int f = a.nF - 1; f >= 0; --f)
+            {
+                const int l = a.lower[f];
+                a.wA[l] = subRn(a.wA[l], mulRn(mulRn(a.rD[l], a.coef[f]), a.wA[a.upper[f]]));
+            }
+            shScal[3] = serialSumProd(n, a.wA, a.rA);
+        }
+        __syncthreads();
+        wArA = shScal[3];
+        if (shIter == 0)
+        {
+            for (int c = lane; c < n; c += 32) a.pA[c] = a.wA[c];
+        }
+        else
+        {
+            const T beta = divRn(wArA, wArAold);
+            for (int c = lane; c < n; c += 32) a.pA[c] = addRn(a.wA[c], mulRn(beta, a.pA[c]));
+        }
+        __syncwarp();
+        warpAmul(a, a.pA, a.wA);
+        if (lane == 0) shScal[3] = serialSumProd(n, a.wA, a.pA);
+        __syncthreads();
+        const T wApA = shScal[3];
+        if (divRn(fabs(wApA), nf) < PerfConst<T>::vsmall) break;  // checkSingularity
+        const T alpha = divRn(wArA, wApA);
+        for (int c = lane; c < n; c += 32)
+        {
+            a.psi[c] = addRn(a.psi[c], mulRn(alpha, a.pA[c]));
+            a.rA[c] = subRn(a.rA[c], mulRn(alpha, a.wA[c]));
+        }
+        __syncwarp();
+        if (lane == 0)
+        {
+            shScal[2] = divRn(serialSumMag(n, a.rA), nf);
+            ++shIter;
+            shStop = (shIter >= a.maxIter || convergedT(shScal[2], shScal[1], a.tolerance, a.relTol)) ? 1 : 0;
+        }
+        __syncthreads();
+    }
+    if (lane == 0)
+    {
+        DevPerf p;
+        p.initialResidual = static_cast<double>(shScal[1]);
+        p.finalResidual = static_cast<double>(shScal[2]);
+        p.nIterations = shIter;
+        p.pad = 0;
+        if (a.out) *a.out = p;
+        if (a.log)
+        {
+            const int i = *a.logCount;
+            if (i < a.logCapacity) a.log[i] = p;
+            *a.logCount = i + 1;
+        }
+    }
+}
+
+}  // namespace k
+}  // namespace b2g

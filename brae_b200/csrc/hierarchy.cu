@@ -1,0 +1,977 @@
+// hierarchy.cu -- the faceAreaPair GAMG hierarchy, built on the device, bit-for-bit the reference's.
+//
+// Reference (paths relative to its project root):
+//   AGG = src/matrices/lduMatrix/solvers/GAMG/GAMGAgglomerations/pair_gamg_agglomeration_cpp.cu
+//
+// THE PAIRING IS A SEQUENTIAL GREEDY (AGG:158-284) and is reproduced exactly by a dependency-
+// counted frontier: when a cell is visited, its decision depends only on which of its neighbours
+// are still unmatched, and a neighbour n is unmatched at c's visit iff n is visited after c and no
+// cell visited before c has paired with n. So c can decide as soon as every cell m visited before
+// it that is either c's neighbour, or the neighbour of one of c's later-visited neighbours, has
+// decided. Each cell counts those (m, path) pairs; a decided cell decrements the counters of the
+// cells that count it, and a counter reaching zero puts the cell on the next frontier. Within one
+// frontier no two cells can touch the same later neighbour (one would count the other), so a
+// frontier decides without races, and every cell decides exactly what the sequential pass decides.
+// The coarse numbering (order of pair creation in visit order, singletons after, the backward
+// renumbering c -> n-1-c) is then a prefix sum over visit order.
+#include "hierarchy.cuh"
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace b2g {
+
+namespace {
+
+constexpr int TPB = 256;
+constexpr double kGreatAgg = 1.0e+15;  // scalar.H GREAT (AGG:15)
+constexpr int kMaxLevels = 50;          // GAMGAgglomeration.C:248 (AGG:13)
+
+inline int grid(long long n) { return std::max(1, ceilDiv(n, TPB)); }
+
+int bitsFor(long long maxValue)
+{
+    int b = 1;
+    while (b < 63 && (1LL << b) <= maxValue) ++b;
+    return b;
+}
+
+// ---------------------------------------------------------------------------------------------
+// layouts
+// ---------------------------------------------------------------------------------------------
+
+__global__ void kCheckOrder(int nF, int nC, const int* __restrict__ lower, const int* __restrict__ upper,
+                            int* err)
+{
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nF) return;
+    const int l = lower[f];
+    const int u = upper[f];
+    if (l < 0 || u < 0 || l >= nC || u >= nC) { atomicOr(err, 1); return; }
+    if (l >= u) atomicOr(err, 2);
+    if (f > 0 && l < lower[f - 1]) atomicOr(err, 4);
+}
+
+__global__ void kCount(const int* __restrict__ keys, int n, int* counts)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) atomicAdd(&counts[keys[i]], 1);
+}
+
+__global__ void kIota(int* v, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = i;
+}
+
+__global__ void kAddInts(const int* a, const int* b, int* out, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = a[i] + b[i];
+}
+
+__global__ void kFillRows(int nC, const int* __restrict__ lower, const int* __restrict__ upper,
+                          const int* __restrict__ ownStart, const int* __restrict__ losortStart,
+                          const int* __restrict__ losort, const int* __restrict__ rowStart,
+                          int* __restrict__ col, int* __restrict__ entFace)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    int k = rowStart[c];
+    for (int q = losortStart[c]; q < losortStart[c + 1]; ++q)
+    {
+        const int f = losort[q];
+        col[k] = lower[f];
+        entFace[k] = f;
+        ++k;
+    }
+    for (int f = ownStart[c]; f < ownStart[c + 1]; ++f)
+    {
+        col[k] = upper[f];
+        entFace[k] = f;
+        ++k;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// pairing (AGG:158-284)
+// ---------------------------------------------------------------------------------------------
+
+enum : int { ST_UNDECIDED = 0, ST_CREATOR = 1, ST_TAKEN = 2, ST_JOINER = 3, ST_LONE = 4 };
+
+__device__ __forceinline__ int rankOf(int c, int n, int fwd) { return fwd ? c : n - 1 - c; }
+
+// mag(cmptMultiply(Sf/sqrt(magSf), (1, 1.01, 1.02))) (AGG:301-311), every operation rounded
+__global__ void kFaceWeights(int nF, const double* __restrict__ Sf, const double* __restrict__ magSf,
+                             double* __restrict__ w)
+{
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nF) return;
+    const double r = __dsqrt_rn(magSf[f]);
+    const double wx = __ddiv_rn(Sf[3 * (size_t)f], r);
+    const double wy = __dmul_rn(__ddiv_rn(Sf[3 * (size_t)f + 1], r), 1.01);
+    const double wz = __dmul_rn(__ddiv_rn(Sf[3 * (size_t)f + 2], r), 1.02);
+    w[f] = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(wx, wx), __dmul_rn(wy, wy)), __dmul_rn(wz, wz)));
+}
+
+// c counts every (m, path) it must wait for: its earlier neighbours, and for each later neighbour
+// n, n's neighbours visited before c.
+__global__ void kPairCounters(int n, int fwd, const int* __restrict__ rowStart, const int* __restrict__ col,
+                              int* __restrict__ ctr)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const int r = rankOf(c, n, fwd);
+    int k = 0;
+    for (int e = rowStart[c]; e < rowStart[c + 1]; ++e)
+    {
+        const int m = col[e];
+        const int rm = rankOf(m, n, fwd);
+        if (rm < r)
+        {
+            ++k;
+        }
+        else if (rm > r)
+        {
+            for (int e2 = rowStart[m]; e2 < rowStart[m + 1]; ++e2)
+            {
+                if (rankOf(col[e2], n, fwd) < r) ++k;
+            }
+        }
+    }
+    ctr[c] = k;
+}
+
+__global__ void kSeedFrontier(int n, const int* __restrict__ ctr, int* __restrict__ frontier, int* size)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < n && ctr[c] == 0) frontier[atomicAdd(size, 1)] = c;
+}
+
+__global__ void kPairRound(int n, int fwd, const int* __restrict__ frontier, int fsize,
+                           const int* __restrict__ rowStart, const int* __restrict__ col,
+                           const int* __restrict__ entFace, const double* __restrict__ w,
+                           int* __restrict__ st, int* __restrict__ partner, int* __restrict__ target,
+                           int* __restrict__ ctr, int* __restrict__ next, int* nextSize)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= fsize) return;
+    const int c = frontier[t];
+    const int r = rankOf(c, n, fwd);
+    const int rb = rowStart[c];
+    const int re = rowStart[c + 1];
+    if (st[c] != ST_TAKEN)
+    {
+        // the first face of maximum weight, in cellFaces order, whose other cell is unmatched
+        int best = -1;
+        double bestW = -kGreatAgg;
+        for (int e = rb; e < re; ++e)
+        {
+            const int nb = col[e];
+            const bool avail = rankOf(nb, n, fwd) > r && st[nb] != ST_TAKEN;
+            const double we = w[entFace[e]];
+            if (avail && we > bestW)
+            {
+                best = e;
+                bestW = we;
+            }
+        }
+        if (best >= 0)
+        {
+            const int nb = col[best];
+            partner[c] = nb;
+            partner[nb] = c;
+            st[nb] = ST_TAKEN;
+            st[c] = ST_CREATOR;
+        }
+        else
+        {
+            // no unmatched neighbour: join the cluster across the heaviest face (AGG:239-257)
+            int cbest = -1;
+            double cw = -kGreatAgg;
+            for (int e = rb; e < re; ++e)
+            {
+                const double we = w[entFace[e]];
+                if (we > cw)
+                {
+                    cbest = e;
+                    cw = we;
+                }
+            }
+            if (cbest >= 0)
+            {
+                target[c] = col[cbest];
+                st[c] = ST_JOINER;
+            }
+            else
+            {
+                st[c] = ST_LONE;
+            }
+        }
+    }
+    // release the cells that counted c
+    for (int e = rb; e < re; ++e)
+    {
+        const int m = col[e];
+        const int rm = rankOf(m, n, fwd);
+        if (rm > r)
+        {
+            if (atomicSub(&ctr[m], 1) == 1) next[atomicAdd(nextSize, 1)] = m;
+        }
+        for (int e2 = rowStart[m]; e2 < rowStart[m + 1]; ++e2)
+        {
+            const int d = col[e2];
+            const int rd = rankOf(d, n, fwd);
+            if (rd > r && rd < rm)
+            {
+                if (atomicSub(&ctr[d], 1) == 1) next[atomicAdd(nextSize, 1)] = d;
+            }
+        }
+    }
+}
+
+// rank-ordered flags: creators (for pair numbering) and lone cells (singletons)
+__global__ void kRankFlags(int n, int fwd, const int* __restrict__ st, int* __restrict__ isCreator,
+                           int* __restrict__ isLone)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const int c = fwd ? r : n - 1 - r;
+    isCreator[r] = st[c] == ST_CREATOR;
+    isLone[r] = st[c] == ST_LONE || st[c] == ST_UNDECIDED;
+}
+
+__global__ void kAssignPairs(int n, int fwd, const int* __restrict__ st, const int* __restrict__ partner,
+                             const int* __restrict__ creatorId, const int* __restrict__ loneId, int nPairs,
+                             int* __restrict__ map)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const int r = rankOf(c, n, fwd);
+    const int s = st[c];
+    if (s == ST_CREATOR) map[c] = creatorId[r];
+    else if (s == ST_TAKEN) map[c] = creatorId[rankOf(partner[c], n, fwd)];
+    else if (s == ST_LONE || s == ST_UNDECIDED) map[c] = nPairs + loneId[r];
+}
+
+__global__ void kAssignJoiners(int n, const int* __restrict__ st, const int* __restrict__ target,
+                               int* __restrict__ map)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n || st[c] != ST_JOINER) return;
+    int t = target[c];
+    for (int guard = 0; st[t] == ST_JOINER && guard < n; ++guard) t = target[t];
+    map[c] = map[t];
+}
+
+__global__ void kReverseMap(int n, int nCoarse, int* map)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < n) map[c] = (nCoarse - 1) - map[c];
+}
+
+// ---------------------------------------------------------------------------------------------
+// coarse addressing (AGG:28-154) and weight restriction (AGG:328-339)
+// ---------------------------------------------------------------------------------------------
+
+__global__ void kFaceKeys(int nF, const int* __restrict__ lower, const int* __restrict__ upper,
+                          const int* __restrict__ map, unsigned long long internalKey,
+                          unsigned long long* __restrict__ keys, int* __restrict__ fr, int* nInternal)
+{
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nF) return;
+    const int ru = map[upper[f]];
+    const int rl = map[lower[f]];
+    if (ru == rl)
+    {
+        fr[f] = -(ru + 1);
+        keys[f] = internalKey;
+        atomicAdd(nInternal, 1);
+        return;
+    }
+    const unsigned long long o = static_cast<unsigned>(min(ru, rl));
+    const unsigned long long nb = static_cast<unsigned>(max(ru, rl));
+    keys[f] = (o << 32) | nb;
+}
+
+__global__ void kSegHeads(int nValid, const unsigned long long* __restrict__ keys, int* __restrict__ head)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nValid) return;
+    head[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1 : 0;
+}
+
+// per unique (owner, neighbour) pair: its fine-face segment and first appearance
+__global__ void kUniqueInfo(int nValid, const unsigned long long* __restrict__ keys,
+                            const int* __restrict__ faces, const int* __restrict__ head,
+                            const int* __restrict__ segScan, unsigned long long* __restrict__ key2,
+                            int* __restrict__ uBeg)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nValid || !head[i]) return;
+    const int u = segScan[i];
+    const unsigned long long own = keys[i] >> 32;
+    key2[u] = (own << 32) | static_cast<unsigned>(faces[i]);  // owner-major, then first appearance
+    uBeg[u] = i;
+}
+
+__global__ void kCoarseFaces(int nUnique, int nValid, const unsigned long long* __restrict__ sortedKeys,
+                             const int* __restrict__ uOrder, const int* __restrict__ uBeg,
+                             const unsigned long long* __restrict__ keys, int* __restrict__ cLower,
+                             int* __restrict__ cUpper, int* __restrict__ faceBeg, int* __restrict__ faceEnd,
+                             int* __restrict__ cfOfU)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nUnique) return;
+    const int u = uOrder[p];
+    const int b = uBeg[u];
+    const unsigned long long k = keys[b];
+    cLower[p] = static_cast<int>(k >> 32);
+    cUpper[p] = static_cast<int>(k & 0xffffffffULL);
+    faceBeg[p] = b;
+    faceEnd[p] = (u + 1 < nUnique) ? uBeg[u + 1] : nValid;
+    cfOfU[u] = p;
+}
+
+// segIncl is the inclusive scan of segment heads: element i belongs to unique pair segIncl[i] - 1
+__global__ void kFaceRestrict(int nValid, const int* __restrict__ faces, const int* __restrict__ segIncl,
+                              const int* __restrict__ cfOfU, int* __restrict__ fr)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nValid) return;
+    fr[faces[i]] = cfOfU[segIncl[i] - 1];
+}
+
+__global__ void kFlip(int nF, const int* __restrict__ lower, const int* __restrict__ upper,
+                      const int* __restrict__ map, const int* __restrict__ fr, int8_t* __restrict__ flip)
+{
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nF) return;
+    // true where the fine face's UPPER cell fell in the coarse OWNER (AGG:127-148)
+    flip[f] = (fr[f] >= 0 && map[upper[f]] < map[lower[f]]) ? 1 : 0;
+}
+
+// next-level weights: each coarse face sums its fine faces' weights in ascending fine face
+__global__ void kRestrictWeights(int nCF, const int* __restrict__ faceBeg, const int* __restrict__ faceEnd,
+                                 const int* __restrict__ faceList, const double* __restrict__ w,
+                                 double* __restrict__ cw)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nCF) return;
+    double s = 0.0;
+    for (int i = faceBeg[p]; i < faceEnd[p]; ++i) s = __dadd_rn(s, w[faceList[i]]);
+    cw[p] = s;
+}
+
+__global__ void kInternalKeys(int nInt, const int* __restrict__ faces, const int* __restrict__ fr,
+                              unsigned* __restrict__ keys)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nInt) keys[i] = static_cast<unsigned>(-1 - fr[faces[i]]);
+}
+
+__global__ void kKeysToInt(int n, const unsigned* __restrict__ k, int* __restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = static_cast<int>(k[i]);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Gauss-Seidel schedule: depths (Kahn's frontier) and parts
+// ---------------------------------------------------------------------------------------------
+
+__global__ void kIndegree(int n, const int* __restrict__ losortStart, int* __restrict__ indeg,
+                          int* __restrict__ frontier, int* size)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const int d = losortStart[c + 1] - losortStart[c];
+    indeg[c] = d;
+    if (d == 0) frontier[atomicAdd(size, 1)] = c;
+}
+
+__global__ void kDepthRound(int round, const int* __restrict__ frontier, int fsize,
+                            const int* __restrict__ ownStart, const int* __restrict__ upper,
+                            int* __restrict__ indeg, int* __restrict__ depth, int* __restrict__ next,
+                            int* nextSize)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= fsize) return;
+    const int c = frontier[t];
+    depth[c] = round;
+    for (int f = ownStart[c]; f < ownStart[c + 1]; ++f)
+    {
+        const int nb = upper[f];
+        if (atomicSub(&indeg[nb], 1) == 1) next[atomicAdd(nextSize, 1)] = nb;
+    }
+}
+
+__global__ void kPartOf(int n, int nParts, const int* __restrict__ partStart, int* __restrict__ partOf)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    int lo = 0, hi = nParts - 1;
+    while (lo < hi)
+    {
+        const int mid = (lo + hi + 1) >> 1;
+        if (partStart[mid] <= c) lo = mid; else hi = mid - 1;
+    }
+    partOf[c] = lo;
+}
+
+__global__ void kSchedKeys(int n, int stride, const int* __restrict__ partOf, const int* __restrict__ depth,
+                           unsigned* __restrict__ keys)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < n) keys[c] = static_cast<unsigned>(partOf[c]) * static_cast<unsigned>(stride) +
+                         static_cast<unsigned>(depth[c]);
+}
+
+__global__ void kKeyHeads(int n, const unsigned* __restrict__ keys, int* __restrict__ head)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) head[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1 : 0;
+}
+
+__global__ void kLevelInfo(int n, int stride, const unsigned* __restrict__ keys, const int* __restrict__ head,
+                           const int* __restrict__ lvlScan, int* __restrict__ lvlStart,
+                           int* __restrict__ lvlDepth, int* __restrict__ lvlPart)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !head[i]) return;
+    const int L = lvlScan[i];
+    lvlStart[L] = i;
+    lvlDepth[L] = static_cast<int>(keys[i] % static_cast<unsigned>(stride));
+    lvlPart[L] = static_cast<int>(keys[i] / static_cast<unsigned>(stride));
+}
+
+// lvlIncl is the inclusive scan of level heads: position i holds local level lvlIncl[i] - 1
+__global__ void kPosLevel(int n, const int* __restrict__ order, const int* __restrict__ lvlIncl,
+                          int* __restrict__ lvlOfCell)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) lvlOfCell[order[i]] = lvlIncl[i] - 1;
+}
+
+// part boundaries: part p starts at the first cell whose cumulative cost (cells + row entries)
+// reaches total*p/P
+__global__ void kPartBounds(int n, int P, const int* __restrict__ rowStart, int* __restrict__ partStart)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p > P) return;
+    if (p == 0) { partStart[0] = 0; return; }
+    if (p == P) { partStart[P] = n; return; }
+    const long long total = static_cast<long long>(n) + rowStart[n];
+    const long long target = total * p / P;
+    int lo = 0, hi = n;
+    while (lo < hi)
+    {
+        const int mid = (lo + hi) >> 1;
+        if (static_cast<long long>(mid) + rowStart[mid] < target) lo = mid + 1; else hi = mid;
+    }
+    partStart[p] = lo;
+}
+
+__global__ void kNeeds(int n, int nParts, const int* __restrict__ partOf, const int* __restrict__ depth,
+                       const int* __restrict__ lvlOfCell, const int* __restrict__ losortStart,
+                       const int* __restrict__ losort, const int* __restrict__ lower,
+                       const int* __restrict__ ownStart, const int* __restrict__ upper,
+                       int* __restrict__ needUp, int* __restrict__ needDown, unsigned* __restrict__ upBits,
+                       unsigned* __restrict__ downBits, int words)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const int p = partOf[c];
+    const int L = lvlOfCell[c];
+    for (int q = losortStart[c]; q < losortStart[c + 1]; ++q)
+    {
+        const int o = lower[losort[q]];
+        const int po = partOf[o];
+        if (po != p)
+        {
+            atomicMax(&needUp[L], depth[o]);
+            atomicOr(&upBits[(size_t)p * words + (po >> 5)], 1u << (po & 31));
+        }
+    }
+    for (int f = ownStart[c]; f < ownStart[c + 1]; ++f)
+    {
+        const int nb = upper[f];
+        const int pn = partOf[nb];
+        if (pn != p)
+        {
+            atomicMax(&needDown[L], depth[nb]);
+            atomicOr(&downBits[(size_t)p * words + (pn >> 5)], 1u << (pn & 31));
+        }
+    }
+}
+
+__global__ void kFillInt(int* v, int n, int value)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = value;
+}
+
+int readInt(const int* d, cudaStream_t s)
+{
+    int h = 0;
+    B2G_CUDA(cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, s));
+    B2G_CUDA(cudaStreamSynchronize(s));
+    return h;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------
+// primitives
+// ---------------------------------------------------------------------------------------------
+
+long long exclusiveScan(const int* in, int* out, int n, cudaStream_t s)
+{
+    B2G_CUDA(cudaMemsetAsync(out, 0, sizeof(int), s));
+    if (n == 0) return 0;
+    size_t tmpBytes = 0;
+    B2G_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmpBytes, in, out + 1, n, s));
+    DBuf<unsigned char> tmp;
+    tmp.alloc(tmpBytes, s);
+    B2G_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, tmpBytes, in, out + 1, n, s));
+    return readInt(out + n, s);
+}
+
+void sortPairs(const unsigned* kin, unsigned* kout, const int* vin, int* vout, int n, int bits,
+               cudaStream_t s)
+{
+    if (n == 0) return;
+    size_t tmpBytes = 0;
+    B2G_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmpBytes, kin, kout, vin, vout, n, 0, bits, s));
+    DBuf<unsigned char> tmp;
+    tmp.alloc(tmpBytes, s);
+    B2G_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tmpBytes, kin, kout, vin, vout, n, 0, bits, s));
+}
+
+void sortPairs64(const unsigned long long* kin, unsigned long long* kout, const int* vin, int* vout,
+                 int n, int bits, cudaStream_t s)
+{
+    if (n == 0) return;
+    size_t tmpBytes = 0;
+    B2G_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmpBytes, kin, kout, vin, vout, n, 0, bits, s));
+    DBuf<unsigned char> tmp;
+    tmp.alloc(tmpBytes, s);
+    B2G_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tmpBytes, kin, kout, vin, vout, n, 0, bits, s));
+}
+
+void countingStarts(const int* keys, int n, int nBins, int* start, cudaStream_t s)
+{
+    DBuf<int> counts;
+    counts.alloc(static_cast<size_t>(nBins), s);
+    counts.zero(s);
+    if (n) kCount<<<grid(n), TPB, 0, s>>>(keys, n, counts.p);
+    B2G_LAUNCH_CHECK();
+    exclusiveScan(counts.p, start, nBins, s);
+}
+
+// ---------------------------------------------------------------------------------------------
+// per-level layouts
+// ---------------------------------------------------------------------------------------------
+
+void buildLevelLayouts(LevelAddr& L, cudaStream_t s)
+{
+    const int nC = L.nCells;
+    const int nF = L.nFaces;
+    {
+        DBuf<int> err;
+        err.alloc(1, s);
+        err.zero(s);
+        if (nF) kCheckOrder<<<grid(nF), TPB, 0, s>>>(nF, nC, L.lower.p, L.upper.p, err.p);
+        B2G_LAUNCH_CHECK();
+        const int e = readInt(err.p, s);
+        if (e & 1) fail(B2G_ERR_ARGUMENT, "b2g: a face's owner or neighbour is outside [0, nCells).");
+        if (e & 6)
+            fail(B2G_ERR_ARGUMENT,
+                 "b2g: the internal faces break OpenFOAM's upper-triangular order (faces sorted by owner, "
+                 "owner < neighbour). The Gauss-Seidel smoother walks the faces each cell owns through "
+                 "ownerStartAddr, which only exists for a mesh ordered that way (smooth_solver_cpp.cu:10-34).");
+    }
+    L.ownStart.alloc(nC + 1, s);
+    countingStarts(L.lower.p, nF, nC, L.ownStart.p, s);
+    L.losortStart.alloc(nC + 1, s);
+    countingStarts(L.upper.p, nF, nC, L.losortStart.p, s);
+    // losort: faces ordered by neighbour, stable so ascending face within a cell
+    L.losort.alloc(nF, s);
+    {
+        DBuf<int> iota;
+        iota.alloc(nF, s);
+        if (nF) kIota<<<grid(nF), TPB, 0, s>>>(iota.p, nF);
+        DBuf<unsigned> kout;
+        kout.alloc(nF, s);
+        sortPairs(reinterpret_cast<const unsigned*>(L.upper.p), kout.p, iota.p, L.losort.p, nF,
+                  bitsFor(nC), s);
+    }
+    L.rowStart.alloc(nC + 1, s);
+    kAddInts<<<grid(nC + 1), TPB, 0, s>>>(L.losortStart.p, L.ownStart.p, L.rowStart.p, nC + 1);
+    L.col.alloc(2 * (size_t)nF, s);
+    L.entFace.alloc(2 * (size_t)nF, s);
+    if (nC)
+        kFillRows<<<grid(nC), TPB, 0, s>>>(nC, L.lower.p, L.upper.p, L.ownStart.p, L.losortStart.p,
+                                           L.losort.p, L.rowStart.p, L.col.p, L.entFace.p);
+    B2G_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------------------------
+// one pairing pass: gamgPairAgglomerate (AGG:158-284)
+// ---------------------------------------------------------------------------------------------
+
+static int pairPass(const LevelAddr& L, const double* w, int fwd, DBuf<int>& map, cudaStream_t s)
+{
+    const int n = L.nCells;
+    DBuf<int> st, partner, target, ctr, fa, fb, sizes;
+    st.alloc(n, s); st.zero(s);
+    partner.alloc(n, s);
+    target.alloc(n, s);
+    ctr.alloc(n, s);
+    fa.alloc(n, s);
+    fb.alloc(n, s);
+    sizes.alloc(2, s);
+    sizes.zero(s);
+    kPairCounters<<<grid(n), TPB, 0, s>>>(n, fwd, L.rowStart.p, L.col.p, ctr.p);
+    kSeedFrontier<<<grid(n), TPB, 0, s>>>(n, ctr.p, fa.p, sizes.p);
+    B2G_LAUNCH_CHECK();
+    int fsize = readInt(sizes.p, s);
+    int* cur = fa.p;
+    int* nxt = fb.p;
+    int resolved = 0;
+    int pinned[2];
+    while (fsize > 0)
+    {
+        resolved += fsize;
+        B2G_CUDA(cudaMemsetAsync(sizes.p + 1, 0, sizeof(int), s));
+        kPairRound<<<grid(fsize), TPB, 0, s>>>(n, fwd, cur, fsize, L.rowStart.p, L.col.p, L.entFace.p, w,
+                                               st.p, partner.p, target.p, ctr.p, nxt, sizes.p + 1);
+        B2G_LAUNCH_CHECK();
+        B2G_CUDA(cudaMemcpyAsync(pinned, sizes.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+        B2G_CUDA(cudaStreamSynchronize(s));
+        fsize = pinned[1];
+        B2G_CUDA(cudaMemcpyAsync(sizes.p, sizes.p + 1, sizeof(int), cudaMemcpyDeviceToDevice, s));
+        std::swap(cur, nxt);
+    }
+    if (resolved != n)
+        fail(B2G_ERR_STATE, "b2g: the agglomeration frontier stopped with " + std::to_string(n - resolved) +
+                                " of " + std::to_string(n) + " cells undecided.");
+    // numbering: pairs in order of creation along the visit order, then singletons
+    DBuf<int> isCre, isLone, creId, loneId;
+    isCre.alloc(n, s);
+    isLone.alloc(n, s);
+    creId.alloc(n + 1, s);
+    loneId.alloc(n + 1, s);
+    kRankFlags<<<grid(n), TPB, 0, s>>>(n, fwd, st.p, isCre.p, isLone.p);
+    const int nPairs = static_cast<int>(exclusiveScan(isCre.p, creId.p, n, s));
+    const int nLone = static_cast<int>(exclusiveScan(isLone.p, loneId.p, n, s));
+    map.alloc(n, s);
+    kAssignPairs<<<grid(n), TPB, 0, s>>>(n, fwd, st.p, partner.p, creId.p, loneId.p, nPairs, map.p);
+    kAssignJoiners<<<grid(n), TPB, 0, s>>>(n, st.p, target.p, map.p);
+    const int nCoarse = nPairs + nLone;
+    if (!fwd) kReverseMap<<<grid(n), TPB, 0, s>>>(n, nCoarse, map.p);
+    B2G_LAUNCH_CHECK();
+    return nCoarse;
+}
+
+// ---------------------------------------------------------------------------------------------
+// agglomerateLduAddressing (AGG:28-154) + restrictFaceField (AGG:328-339)
+// ---------------------------------------------------------------------------------------------
+
+static void coarseAddressing(const LevelAddr& F, Step& S, LevelAddr& Cl, const double* w,
+                             DBuf<double>& cw, cudaStream_t s)
+{
+    const int nF = F.nFaces;
+    const int nC = S.nCoarse;
+    S.faceRestrict.alloc(nF, s);
+    S.flip.alloc(nF, s);
+    DBuf<unsigned long long> keys, skeys;
+    DBuf<int> iota, faces, nInt;
+    nInt.alloc(1, s);
+    nInt.zero(s);
+    keys.alloc(nF, s);
+    skeys.alloc(nF, s);
+    iota.alloc(nF, s);
+    faces.alloc(nF, s);
+    const int cbits = bitsFor(nC);
+    const unsigned long long internalKey = (static_cast<unsigned long long>(nC) << 32);
+    if (nF)
+    {
+        kFaceKeys<<<grid(nF), TPB, 0, s>>>(nF, F.lower.p, F.upper.p, S.restrictAddr.p, internalKey, keys.p,
+                                           S.faceRestrict.p, nInt.p);
+        kIota<<<grid(nF), TPB, 0, s>>>(iota.p, nF);
+        B2G_LAUNCH_CHECK();
+    }
+    sortPairs64(keys.p, skeys.p, iota.p, faces.p, nF, 32 + cbits, s);
+    // faces between two different coarse cells sort before the internal ones
+    const int nValid = nF - readInt(nInt.p, s);
+    DBuf<int> head, segScan, segIncl;
+    head.alloc(nValid, s);
+    segScan.alloc(nValid + 1, s);
+    if (nValid) kSegHeads<<<grid(nValid), TPB, 0, s>>>(nValid, skeys.p, head.p);
+    B2G_LAUNCH_CHECK();
+    const int nUnique = static_cast<int>(exclusiveScan(head.p, segScan.p, nValid, s));
+    DBuf<unsigned long long> key2, skey2;
+    DBuf<int> uBeg, uIota, uOrder, cfOfU;
+    key2.alloc(nUnique, s);
+    skey2.alloc(nUnique, s);
+    uBeg.alloc(nUnique, s);
+    uIota.alloc(nUnique, s);
+    uOrder.alloc(nUnique, s);
+    cfOfU.alloc(nUnique, s);
+    if (nValid) kUniqueInfo<<<grid(nValid), TPB, 0, s>>>(nValid, skeys.p, faces.p, head.p, segScan.p, key2.p, uBeg.p);
+    if (nUnique) kIota<<<grid(nUnique), TPB, 0, s>>>(uIota.p, nUnique);
+    B2G_LAUNCH_CHECK();
+    sortPairs64(key2.p, skey2.p, uIota.p, uOrder.p, nUnique, 32 + cbits, s);
+    Cl.nCells = nC;
+    Cl.nFaces = nUnique;
+    Cl.lower.alloc(nUnique, s);
+    Cl.upper.alloc(nUnique, s);
+    S.faceBeg.alloc(nUnique, s);
+    S.faceEnd.alloc(nUnique, s);
+    if (nUnique)
+        kCoarseFaces<<<grid(nUnique), TPB, 0, s>>>(nUnique, nValid, skey2.p, uOrder.p, uBeg.p, skeys.p,
+                                                   Cl.lower.p, Cl.upper.p, S.faceBeg.p, S.faceEnd.p, cfOfU.p);
+    B2G_LAUNCH_CHECK();
+    if (nValid)
+    {
+        // segScan[i+1] is the inclusive count of heads up to i
+        kFaceRestrict<<<grid(nValid), TPB, 0, s>>>(nValid, faces.p, segScan.p + 1, cfOfU.p, S.faceRestrict.p);
+        B2G_LAUNCH_CHECK();
+    }
+    S.nCoarseFaces = nUnique;
+    if (nF) kFlip<<<grid(nF), TPB, 0, s>>>(nF, F.lower.p, F.upper.p, S.restrictAddr.p, S.faceRestrict.p, S.flip.p);
+    B2G_LAUNCH_CHECK();
+    // fine faces grouped by coarse face (the valid part of the sorted order)
+    S.faceList.alloc(nValid, s);
+    if (nValid)
+        B2G_CUDA(cudaMemcpyAsync(S.faceList.p, faces.p, sizeof(int) * nValid, cudaMemcpyDeviceToDevice, s));
+    cw.alloc(nUnique, s);
+    if (nUnique)
+        kRestrictWeights<<<grid(nUnique), TPB, 0, s>>>(nUnique, S.faceBeg.p, S.faceEnd.p, S.faceList.p, w, cw.p);
+    B2G_LAUNCH_CHECK();
+    // internal faces grouped by coarse cell, ascending
+    const int nInternal = nF - nValid;
+    S.intStart.alloc(nC + 1, s);
+    S.intList.alloc(nInternal, s);
+    {
+        DBuf<unsigned> ik, iks;
+        ik.alloc(nInternal, s);
+        iks.alloc(nInternal, s);
+        if (nInternal)
+            kInternalKeys<<<grid(nInternal), TPB, 0, s>>>(nInternal, faces.p + nValid, S.faceRestrict.p, ik.p);
+        B2G_LAUNCH_CHECK();
+        sortPairs(ik.p, iks.p, faces.p + nValid, S.intList.p, nInternal, cbits, s);
+        DBuf<int> ikInt;
+        ikInt.alloc(nInternal, s);
+        if (nInternal) kKeysToInt<<<grid(nInternal), TPB, 0, s>>>(nInternal, iks.p, ikInt.p);
+        countingStarts(ikInt.p, nInternal, nC, S.intStart.p, s);
+    }
+    // fine cells grouped by coarse cell, ascending
+    S.cellStart.alloc(nC + 1, s);
+    S.cellList.alloc(S.nFine, s);
+    {
+        DBuf<int> ci;
+        DBuf<unsigned> ck;
+        ci.alloc(S.nFine, s);
+        ck.alloc(S.nFine, s);
+        kIota<<<grid(S.nFine), TPB, 0, s>>>(ci.p, S.nFine);
+        B2G_LAUNCH_CHECK();
+        sortPairs(reinterpret_cast<const unsigned*>(S.restrictAddr.p), ck.p, ci.p, S.cellList.p, S.nFine,
+                  cbits, s);
+        countingStarts(S.restrictAddr.p, S.nFine, nC, S.cellStart.p, s);
+    }
+}
+
+void buildHierarchy(Mesh& M, const double* dSf, const double* dMagSf, int nCellsInCoarsestLevel,
+                    int* forward)
+{
+    cudaStream_t s = M.stream;
+    LevelAddr& L0 = M.lev[0];
+    buildLevelLayouts(L0, s);
+    // GAMGAgglomeration.C:285 (AGG:297)
+    int nCoarsest = std::min(L0.nCells / 2, nCellsInCoarsestLevel);
+    nCoarsest = std::max(1, nCoarsest);
+    DBuf<double> w;
+    w.alloc(L0.nFaces, s);
+    if (L0.nFaces) kFaceWeights<<<grid(L0.nFaces), TPB, 0, s>>>(L0.nFaces, dSf, dMagSf, w.p);
+    B2G_LAUNCH_CHECK();
+    int fwd = *forward ? 1 : 0;
+    while (static_cast<int>(M.step.size()) < kMaxLevels - 1)
+    {
+        LevelAddr& F = M.lev.back();
+        DBuf<int> map;
+        const int nCoarse = pairPass(F, w.p, fwd, map, s);
+        fwd = !fwd;  // flips after every pass, the rejected one included (AGG:282)
+        // continueAgglomerating (AGG:17-24)
+        if (nCoarse < nCoarsest || !(nCoarse < F.nCells)) break;
+        M.step.emplace_back();
+        Step& S = M.step.back();
+        S.nFine = F.nCells;
+        S.nCoarse = nCoarse;
+        S.nFineFaces = F.nFaces;
+        S.restrictAddr = std::move(map);
+        M.lev.emplace_back();
+        LevelAddr& Fr = M.lev[M.lev.size() - 2];
+        LevelAddr& Cl = M.lev.back();
+        DBuf<double> cw;
+        coarseAddressing(Fr, S, Cl, w.p, cw, s);
+        buildLevelLayouts(Cl, s);
+        w = std::move(cw);
+    }
+    *forward = fwd;
+    for (auto& L : M.lev) buildGsSchedule(L, s);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Gauss-Seidel schedule
+// ---------------------------------------------------------------------------------------------
+
+void buildGsSchedule(LevelAddr& L, cudaStream_t s)
+{
+    GsSchedule& G = L.gs;
+    const int n = L.nCells;
+    G.depth.alloc(n, s);
+    if (n == 0) return;
+    // depths by Kahn's frontier: a cell's depth is one more than its deepest owner-side neighbour
+    {
+        DBuf<int> indeg, fa, fb, sizes;
+        indeg.alloc(n, s);
+        fa.alloc(n, s);
+        fb.alloc(n, s);
+        sizes.alloc(2, s);
+        sizes.zero(s);
+        kIndegree<<<grid(n), TPB, 0, s>>>(n, L.losortStart.p, indeg.p, fa.p, sizes.p);
+        B2G_LAUNCH_CHECK();
+        int fsize = readInt(sizes.p, s);
+        int round = 0;
+        int done = 0;
+        int* cur = fa.p;
+        int* nxt = fb.p;
+        int hsz[2];
+        while (fsize > 0)
+        {
+            done += fsize;
+            B2G_CUDA(cudaMemsetAsync(sizes.p + 1, 0, sizeof(int), s));
+            kDepthRound<<<grid(fsize), TPB, 0, s>>>(round, cur, fsize, L.ownStart.p, L.upper.p, indeg.p,
+                                                    G.depth.p, nxt, sizes.p + 1);
+            B2G_LAUNCH_CHECK();
+            B2G_CUDA(cudaMemcpyAsync(hsz, sizes.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+            B2G_CUDA(cudaStreamSynchronize(s));
+            fsize = hsz[1];
+            std::swap(cur, nxt);
+            ++round;
+        }
+        if (done != n) fail(B2G_ERR_STATE, "b2g: the Gauss-Seidel dependency graph has a cycle.");
+        G.maxDepth = round - 1;
+    }
+    // parts: contiguous cell ranges balanced by row length; enough of them to fill the GPU when
+    // a depth holds many cells, one when the level is narrow (a single CTA then walks it)
+    const int depthCount = G.maxDepth + 1;
+    const long long avgPerDepth = (static_cast<long long>(n) + depthCount - 1) / depthCount;
+    const int nSM = DeviceInfo::get().numSMs;
+    int P = static_cast<int>(std::min<long long>(nSM, std::max<long long>(1, avgPerDepth / 128)));
+    if (n < 4096) P = 1;
+    G.nParts = P;
+    DBuf<int> dPartStart, partOf;
+    dPartStart.alloc(P + 1, s);
+    kPartBounds<<<grid(P + 1), TPB, 0, s>>>(n, P, L.rowStart.p, dPartStart.p);
+    partOf.alloc(n, s);
+    kPartOf<<<grid(n), TPB, 0, s>>>(n, P, dPartStart.p, partOf.p);
+    const int stride = G.maxDepth + 1;
+    if (static_cast<long long>(P) * stride >= (1LL << 32))
+        fail(B2G_ERR_ARGUMENT, "b2g: the Gauss-Seidel schedule is too deep for its 32-bit keys.");
+    DBuf<unsigned> keys, skeys;
+    DBuf<int> iota;
+    keys.alloc(n, s);
+    skeys.alloc(n, s);
+    iota.alloc(n, s);
+    kSchedKeys<<<grid(n), TPB, 0, s>>>(n, stride, partOf.p, G.depth.p, keys.p);
+    kIota<<<grid(n), TPB, 0, s>>>(iota.p, n);
+    B2G_LAUNCH_CHECK();
+    G.order.alloc(n, s);
+    sortPairs(keys.p, skeys.p, iota.p, G.order.p, n, bitsFor(static_cast<long long>(P) * stride), s);
+    DBuf<int> head, lvlScan;
+    head.alloc(n, s);
+    lvlScan.alloc(n + 1, s);
+    kKeyHeads<<<grid(n), TPB, 0, s>>>(n, skeys.p, head.p);
+    B2G_LAUNCH_CHECK();
+    const int nLvl = static_cast<int>(exclusiveScan(head.p, lvlScan.p, n, s));
+    G.nLocalLevels = nLvl;
+    G.lvlStart.alloc(nLvl + 1, s);
+    G.lvlDepth.alloc(nLvl, s);
+    DBuf<int> lvlPart;
+    lvlPart.alloc(nLvl, s);
+    kLevelInfo<<<grid(n), TPB, 0, s>>>(n, stride, skeys.p, head.p, lvlScan.p, G.lvlStart.p, G.lvlDepth.p,
+                                       lvlPart.p);
+    B2G_CUDA(cudaMemcpyAsync(G.lvlStart.p + nLvl, &n, sizeof(int), cudaMemcpyHostToDevice, s));
+    B2G_CUDA(cudaStreamSynchronize(s));
+    // level of every cell: inclusive scan of heads minus one, at the cell's position
+    DBuf<int> lvlOfCell;
+    lvlOfCell.alloc(n, s);
+    kPosLevel<<<grid(n), TPB, 0, s>>>(n, G.order.p, lvlScan.p + 1, lvlOfCell.p);
+    B2G_LAUNCH_CHECK();
+    G.lvlNeedUp.alloc(nLvl, s);
+    G.lvlNeedDown.alloc(nLvl, s);
+    kFillInt<<<grid(nLvl), TPB, 0, s>>>(G.lvlNeedUp.p, nLvl, -1);
+    kFillInt<<<grid(nLvl), TPB, 0, s>>>(G.lvlNeedDown.p, nLvl, -1);
+    const int words = (P + 31) / 32;
+    DBuf<unsigned> upBits, downBits;
+    upBits.alloc(static_cast<size_t>(P) * words, s);
+    downBits.alloc(static_cast<size_t>(P) * words, s);
+    upBits.zero(s);
+    downBits.zero(s);
+    kNeeds<<<grid(n), TPB, 0, s>>>(n, P, partOf.p, G.depth.p, lvlOfCell.p, L.losortStart.p, L.losort.p,
+                                   L.lower.p, L.ownStart.p, L.upper.p, G.lvlNeedUp.p, G.lvlNeedDown.p,
+                                   upBits.p, downBits.p, words);
+    B2G_LAUNCH_CHECK();
+    // per-part level ranges and dependency lists
+    std::vector<int> hLvlPart = lvlPart.download(s);
+    std::vector<int> partLvlStart(P + 1, 0);
+    for (int Lv = 0; Lv < nLvl; ++Lv) partLvlStart[hLvlPart[Lv] + 1]++;
+    for (int p = 0; p < P; ++p) partLvlStart[p + 1] += partLvlStart[p];
+    G.partLvlStart.upload(partLvlStart.data(), P + 1, s);
+    std::vector<unsigned> hUp = upBits.download(s);
+    std::vector<unsigned> hDown = downBits.download(s);
+    std::vector<int> depStart(2 * P + 1, 0), depList;
+    for (int p = 0; p < P; ++p)
+    {
+        depStart[p] = static_cast<int>(depList.size());
+        for (int q = 0; q < P; ++q)
+            if (hUp[(size_t)p * words + (q >> 5)] & (1u << (q & 31))) depList.push_back(q);
+    }
+    for (int p = 0; p < P; ++p)
+    {
+        depStart[P + p] = static_cast<int>(depList.size());
+        for (int q = 0; q < P; ++q)
+            if (hDown[(size_t)p * words + (q >> 5)] & (1u << (q & 31))) depList.push_back(q);
+    }
+    depStart[2 * P] = static_cast<int>(depList.size());
+    G.depStart.upload(depStart.data(), depStart.size(), s);
+    if (depList.empty()) depList.push_back(0);
+    G.depList.upload(depList.data(), depList.size(), s);
+    G.progress.alloc(P, s);
+    G.progress.zero(s);
+    std::vector<int> hLvlStart = G.lvlStart.download(s);
+    int mx = 0;
+    for (int Lv = 0; Lv < nLvl; ++Lv) mx = std::max(mx, hLvlStart[Lv + 1] - hLvlStart[Lv]);
+    G.maxLevelCells = mx;
+}
+
+const DeviceInfo& DeviceInfo::get()
+{
+    static DeviceInfo info = [] {
+        DeviceInfo d;
+        cudaGetDevice(&d.device);
+        cudaDeviceGetAttribute(&d.numSMs, cudaDevAttrMultiProcessorCount, d.device);
+        cudaDeviceGetAttribute(&d.maxSmemPerBlockOptin, cudaDevAttrMaxSharedMemoryPerBlockOptin, d.device);
+        return d;
+    }();
+    return info;
+}
+
+}  // namespace b2g

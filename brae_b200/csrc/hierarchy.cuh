@@ -1,0 +1,96 @@
+// hierarchy.cuh -- the per-mesh GAMG hierarchy held on the device: each level's LDU addressing
+// with the derived layouts every kernel reads, and each level step's restriction maps.
+#pragma once
+
+#include "b2g_common.cuh"
+
+namespace b2g {
+
+// Forward Gauss-Seidel dependency schedule of one level, partitioned for the part-pipelined sweep
+// kernel (gs.cu). Cells are split into `nParts` contiguous index ranges; each part lists its cells
+// by (depth, cell) where depth is the cell's level in the forward DAG (a cell depends on the
+// owners of the faces it is the neighbour of). Local level = one (part, depth) group.
+struct GsSchedule
+{
+    int nParts = 0;
+    int maxDepth = 0;          // deepest level (0-based)
+    int nLocalLevels = 0;
+    int maxLevelCells = 0;     // largest (part, depth) group
+    DBuf<int> order;           // [nCells] cells in (part, depth, cell) order
+    DBuf<int> partLvlStart;    // [nParts+1] into the local-level arrays
+    DBuf<int> lvlStart;        // [nLocalLevels+1] into order
+    DBuf<int> lvlDepth;        // [nLocalLevels]
+    DBuf<int> lvlNeedUp;       // [nLocalLevels] max depth of lower neighbours in other parts, -1 if none
+    DBuf<int> lvlNeedDown;     // [nLocalLevels] max depth of upper neighbours in other parts, -1 if none
+    DBuf<int> depStart;        // [2*nParts+1]: part p's upstream parts, then its downstream parts
+    DBuf<int> depList;
+    DBuf<unsigned> progress;   // [nParts] per-part progress words (reset before each launch)
+    DBuf<int> depth;           // [nCells]
+};
+
+// One level's addressing and its derived layouts (built once per hierarchy).
+struct LevelAddr
+{
+    int nCells = 0;
+    int nFaces = 0;
+    DBuf<int> lower;        // [nFaces] owner
+    DBuf<int> upper;        // [nFaces] neighbour
+    DBuf<int> ownStart;     // [nCells+1] owned-face ranges (faces are sorted by owner)
+    DBuf<int> losortStart;  // [nCells+1]
+    DBuf<int> losort;       // [nFaces] faces ordered by neighbour cell, ascending face within a cell
+    // Cell-ordered rows in the reference's per-cell accumulation order: the faces the cell is the
+    // neighbour of (ascending face), then the faces it owns (ascending face). Amul, the residual,
+    // normFactor's row sums and the Gauss-Seidel gather all walk a cell's terms in this order.
+    DBuf<int> rowStart;     // [nCells+1] = losortStart + ownStart
+    DBuf<int> col;          // [2*nFaces] the other cell
+    DBuf<int> entFace;      // [2*nFaces] the face
+    GsSchedule gs;
+};
+
+// Level step i -> i+1 (GamgAgglomeration's restrictAddressing / faceRestrictAddressing /
+// faceFlipMap) with the inverse lists the gather kernels need.
+struct Step
+{
+    int nFine = 0, nCoarse = 0, nFineFaces = 0, nCoarseFaces = 0;
+    DBuf<int> restrictAddr;   // [nFine] fine cell -> coarse cell
+    DBuf<int> faceRestrict;   // [nFineFaces] >= 0 coarse face, else -(coarse cell + 1)
+    DBuf<int8_t> flip;        // [nFineFaces]
+    DBuf<int> cellStart;      // [nCoarse+1] coarse cell -> its fine cells, ascending
+    DBuf<int> cellList;       // [nFine]
+    DBuf<int> intStart;       // [nCoarse+1] coarse cell -> fine faces inside it, ascending
+    DBuf<int> intList;
+    DBuf<int> faceBeg;        // [nCoarseFaces] coarse face -> fine faces [faceBeg, faceEnd) of faceList
+    DBuf<int> faceEnd;
+    DBuf<int> faceList;       // fine faces, grouped by coarse face, ascending within a group
+};
+
+struct Mesh
+{
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<LevelAddr> lev;  // [0] the mesh, [i] coarse level i
+    std::vector<Step> step;      // [i] level i -> i+1
+    float buildMs = 0.f;
+    int nLevels() const { return static_cast<int>(step.size()); }
+};
+
+// Builds the derived layouts of `L` from its lower/upper (already on the device). Validates the
+// upper-triangular order (faces sorted by owner, owner < neighbour).
+void buildLevelLayouts(LevelAddr& L, cudaStream_t s);
+// The GS schedule of `L` (depths and parts).
+void buildGsSchedule(LevelAddr& L, cudaStream_t s);
+// The whole agglomeration (faceAreaPairGamgAgglomeration) from device arrays.
+void buildHierarchy(Mesh& M, const double* dSf, const double* dMagSf, int nCellsInCoarsestLevel,
+                    int* forward);
+
+// Exclusive scan helper (n+1 outputs: out[0] = 0 ... out[n] = total); returns the total.
+long long exclusiveScan(const int* in, int* out, int n, cudaStream_t s);
+// Stable radix sort of (key, value) pairs; keys are unsigned, sorted on the low `bits` bits.
+void sortPairs(const unsigned* kin, unsigned* kout, const int* vin, int* vout, int n, int bits,
+               cudaStream_t s);
+void sortPairs64(const unsigned long long* kin, unsigned long long* kout, const int* vin,
+                 int* vout, int n, int bits, cudaStream_t s);
+// Histogram of keys in [0, nBins) and its exclusive scan into start[nBins+1].
+void countingStarts(const int* keys, int n, int nBins, int* start, cudaStream_t s);
+
+}  // namespace b2g

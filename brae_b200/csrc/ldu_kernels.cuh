@@ -1,0 +1,297 @@
+// ldu_kernels.cuh -- the LDU kernels of one level, templated on the value type (double for the
+// parity form, float for the FP32 V-cycle). Every kernel walks a cell's terms in the reference's
+// accumulation order with separately rounded products and sums, so the FP64 instances are
+// bit-for-bit the reference's host loops.
+//
+// Reference: GAMG = src/matrices/lduMatrix/solvers/GAMG/gamg_solver_cpp.cu
+#pragma once
+
+#include "b2g_common.cuh"
+
+namespace b2g {
+namespace k {
+
+template <class T> struct Small;
+template <> struct Small<double>
+{
+    static constexpr double vsmall = 1e-300;  // solverPerformance::vsmall_ (GAMG:17)
+};
+template <> struct Small<float>
+{
+    static constexpr float vsmall = 1e-37f;
+};
+
+// Rows of one level: for cell c the entries [rowStart[c], rowStart[c+1]) hold first the faces c
+// is the neighbour of, then the faces it owns, each ascending -- the order in which lduMatrix::Amul
+// and lduMatrix::residual add a cell's terms (GAMG:62-117). `val` is the coefficient per entry.
+template <class T>
+struct Rows
+{
+    int n;
+    const int* __restrict__ rowStart;
+    const int* __restrict__ col;
+    const T* __restrict__ val;
+    const T* __restrict__ diag;
+};
+
+// lduMatrix::Amul (GAMG:62-88): y = diag*x, then the face terms in face order
+template <class T>
+__global__ void amul(Rows<T> A, const T* __restrict__ x, T* __restrict__ y)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.n; c += gridDim.x * blockDim.x)
+    {
+        T acc = mulRn(A.diag[c], x[c]);
+        const int e1 = A.rowStart[c + 1];
+        for (int e = A.rowStart[c]; e < e1; ++e) acc = addRn(acc, mulRn(A.val[e], x[A.col[e]]));
+        y[c] = acc;
+    }
+}
+
+// A block-wide sum in a fixed shape (deterministic for a fixed blockDim).
+template <class T, int NT>
+__device__ __forceinline__ T blockSum(T v, T* sh)
+{
+    for (int o = 16; o > 0; o >>= 1) v = addRn(v, __shfl_down_sync(0xffffffffu, v, o));
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) sh[w] = v;
+    __syncthreads();
+    T r = T(0);
+    if (threadIdx.x < 32)
+    {
+        r = threadIdx.x < NT / 32 ? sh[threadIdx.x] : T(0);
+        for (int o = 16; o > 0; o >>= 1) r = addRn(r, __shfl_down_sync(0xffffffffu, r, o));
+    }
+    __syncthreads();
+    return r;  // valid in thread 0
+}
+
+// GAMGSolver::scale, first half (GAMG:391-399): Acf = A*field and per-block partial sums of
+// field.source and field.Acf (sums in a fixed tree; the reference sums serially, so these agree to
+// rounding, not bitwise).
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) amulScaleDots(Rows<T> A, const T* __restrict__ field,
+                                                    const T* __restrict__ source, T* __restrict__ Acf,
+                                                    T* __restrict__ partial)
+{
+    __shared__ T sh[NT / 32];
+    T num = T(0), den = T(0);
+    for (int c = blockIdx.x * NT + threadIdx.x; c < A.n; c += gridDim.x * NT)
+    {
+        const T fc = field[c];
+        T acc = mulRn(A.diag[c], fc);
+        const int e1 = A.rowStart[c + 1];
+        for (int e = A.rowStart[c]; e < e1; ++e) acc = addRn(acc, mulRn(A.val[e], field[A.col[e]]));
+        Acf[c] = acc;
+        num = addRn(num, mulRn(fc, source[c]));
+        den = addRn(den, mulRn(fc, acc));
+    }
+    num = blockSum<T, NT>(num, sh);
+    den = blockSum<T, NT>(den, sh);
+    if (threadIdx.x == 0)
+    {
+        partial[2 * blockIdx.x] = num;
+        partial[2 * blockIdx.x + 1] = den;
+    }
+}
+
+// sf = (x.b)/stabilise(x.Ax, vsmall) (GAMG:400-401) from the partials, in one block
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) scaleFactor(const T* __restrict__ partial, int nPartial, T* __restrict__ sf)
+{
+    __shared__ T sh[NT / 32];
+    T num = T(0), den = T(0);
+    for (int i = threadIdx.x; i < nPartial; i += NT)
+    {
+        num = addRn(num, partial[2 * i]);
+        den = addRn(den, partial[2 * i + 1]);
+    }
+    num = blockSum<T, NT>(num, sh);
+    den = blockSum<T, NT>(den, sh);
+    if (threadIdx.x == 0)
+    {
+        const T v = Small<T>::vsmall;
+        *sf = divRn(num, den >= T(0) ? addRn(den, v) : subRn(den, v));
+    }
+}
+
+// field = sf*field + (source - sf*Acf)/diag (GAMG:402-406)
+template <class T>
+__global__ void scaleUpdate(int n, const T* __restrict__ sfp, T* __restrict__ field, const T* __restrict__ source,
+                            const T* __restrict__ Acf, const T* __restrict__ diag)
+{
+    const T sf = *sfp;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+    {
+        field[c] = addRn(mulRn(sf, field[c]), divRn(subRn(source[c], mulRn(sf, Acf[c])), diag[c]));
+    }
+}
+
+// The finest level's scale update fused with psi += finestCorrection (GAMG:716-723): the
+// correction is formed exactly as scale() forms it and added exactly as the reference adds it.
+template <class T>
+__global__ void scaleUpdateAdd(int n, const T* __restrict__ sfp, const T* __restrict__ field,
+                               const T* __restrict__ source, const T* __restrict__ Acf, const T* __restrict__ diag,
+                               T* __restrict__ psi)
+{
+    const T sf = *sfp;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+    {
+        const T corr = addRn(mulRn(sf, field[c]), divRn(subRn(source[c], mulRn(sf, Acf[c])), diag[c]));
+        psi[c] = addRn(psi[c], corr);
+    }
+}
+
+// psi += correction, unscaled (scaleCorrection off)
+template <class T>
+__global__ void addInPlace(int n, T* __restrict__ psi, const T* __restrict__ corr)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+        psi[c] = addRn(psi[c], corr[c]);
+}
+
+// restrictField (GAMG:410-419): cf = 0; cf[map[i]] += ff[i] for ascending i -- gathered per coarse
+// cell over its fine cells in ascending order
+template <class T>
+__global__ void restrictField(int nCoarse, const int* __restrict__ cellStart, const int* __restrict__ cellList,
+                              const T* __restrict__ ff, T* __restrict__ cf)
+{
+    for (int C = blockIdx.x * blockDim.x + threadIdx.x; C < nCoarse; C += gridDim.x * blockDim.x)
+    {
+        T acc = T(0);
+        const int e1 = cellStart[C + 1];
+        for (int e = cellStart[C]; e < e1; ++e) acc = addRn(acc, ff[cellList[e]]);
+        cf[C] = acc;
+    }
+}
+
+// prolongField (GAMG:422-432): injection, overwriting
+template <class T>
+__global__ void prolongField(int nFine, const int* __restrict__ map, const T* __restrict__ cf, T* __restrict__ ff)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nFine; i += gridDim.x * blockDim.x)
+        ff[i] = cf[map[i]];
+}
+
+// agglomerateMatrix (GAMG:474-496), diagonal: restrictField of the fine diagonal, then
+// 2*upper of every fine face inside the coarse cell, ascending
+static __global__ void galerkinDiag(int nCoarse, const int* __restrict__ cellStart, const int* __restrict__ cellList,
+                             const int* __restrict__ intStart, const int* __restrict__ intList,
+                             const double* __restrict__ fdiag, const double* __restrict__ fupper,
+                             double* __restrict__ cdiag)
+{
+    for (int C = blockIdx.x * blockDim.x + threadIdx.x; C < nCoarse; C += gridDim.x * blockDim.x)
+    {
+        double acc = 0.0;
+        for (int e = cellStart[C]; e < cellStart[C + 1]; ++e) acc = __dadd_rn(acc, fdiag[cellList[e]]);
+        for (int e = intStart[C]; e < intStart[C + 1]; ++e) acc = __dadd_rn(acc, __dmul_rn(2.0, fupper[intList[e]]));
+        cdiag[C] = acc;
+    }
+}
+
+// agglomerateMatrix, coarse upper: the sum of its fine faces' coefficients, ascending
+static __global__ void galerkinUpper(int nCF, const int* __restrict__ faceBeg, const int* __restrict__ faceEnd,
+                              const int* __restrict__ faceList, const double* __restrict__ fupper,
+                              double* __restrict__ cupper)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nCF; p += gridDim.x * blockDim.x)
+    {
+        double acc = 0.0;
+        for (int e = faceBeg[p]; e < faceEnd[p]; ++e) acc = __dadd_rn(acc, fupper[faceList[e]]);
+        cupper[p] = acc;
+    }
+}
+
+// the per-entry coefficient of the row layout
+template <class T, class S>
+__global__ void gatherVal(long long nnz, const int* __restrict__ entFace, const S* __restrict__ upper,
+                          T* __restrict__ val)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nnz;
+         e += (long long)gridDim.x * blockDim.x)
+        val[e] = static_cast<T>(upper[entFace[e]]);
+}
+
+template <class T, class S>
+__global__ void castArray(long long n, const S* __restrict__ in, T* __restrict__ out)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = static_cast<T>(in[i]);
+}
+
+// lduMatrix::residual (GAMG:90-117): r = source - diag*psi, then minus the face terms in order
+template <class T>
+__global__ void residual(Rows<T> A, const T* __restrict__ source, const T* __restrict__ psi, T* __restrict__ r)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.n; c += gridDim.x * blockDim.x)
+    {
+        T acc = subRn(source[c], mulRn(A.diag[c], psi[c]));
+        const int e1 = A.rowStart[c + 1];
+        for (int e = A.rowStart[c]; e < e1; ++e) acc = subRn(acc, mulRn(A.val[e], psi[A.col[e]]));
+        r[c] = acc;
+    }
+}
+
+// r = a - b
+template <class T>
+__global__ void subtract(int n, const T* __restrict__ a, const T* __restrict__ b, T* __restrict__ r)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+        r[c] = subRn(a[c], b[c]);
+}
+
+// Two-stage deterministic reductions into a device slot. Stage one: a fixed grid of NT-thread
+// blocks, each thread walking a grid stride; stage two: one block over the partials.
+enum ReduceOp : int { RED_DOT = 0, RED_SUMMAG = 1, RED_SUM = 2 };
+
+template <class T, int NT, int OP>
+__global__ void __launch_bounds__(NT) reducePartial(int n, const T* __restrict__ a, const T* __restrict__ b,
+                                                    T* __restrict__ partial)
+{
+    __shared__ T sh[NT / 32];
+    T s = T(0);
+    for (int i = blockIdx.x * NT + threadIdx.x; i < n; i += gridDim.x * NT)
+    {
+        if (OP == RED_DOT) s = addRn(s, mulRn(a[i], b[i]));
+        else if (OP == RED_SUMMAG) s = addRn(s, fabs(a[i]));
+        else s = addRn(s, a[i]);
+    }
+    s = blockSum<T, NT>(s, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) reduceFinal(const T* __restrict__ partial, int nPartial, T* __restrict__ out)
+{
+    __shared__ T sh[NT / 32];
+    T s = T(0);
+    for (int i = threadIdx.x; i < nPartial; i += NT) s = addRn(s, partial[i]);
+    s = blockSum<T, NT>(s, sh);
+    if (threadIdx.x == 0) *out = s;
+}
+
+// normFactor (GAMG:119-159), the per-cell summand |Apsi - t| + |source - t| with t = sumA*xRef;
+// sumA = diag + the row's coefficients in row order (the reference adds a cell's face terms in
+// face order, which is row order)
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) normFactorPartial(Rows<T> A, const T* __restrict__ psi, const T* __restrict__ source,
+                                                        const T* __restrict__ Apsi, const T* __restrict__ sumPsi,
+                                                        T* __restrict__ partial)
+{
+    __shared__ T sh[NT / 32];
+    const T xRef = divRn(*sumPsi, static_cast<T>(A.n));
+    T s = T(0);
+    for (int c = blockIdx.x * NT + threadIdx.x; c < A.n; c += gridDim.x * NT)
+    {
+        T sumA = A.diag[c];
+        const int e1 = A.rowStart[c + 1];
+        for (int e = A.rowStart[c]; e < e1; ++e) sumA = addRn(sumA, A.val[e]);
+        const T t = mulRn(sumA, xRef);
+        s = addRn(s, addRn(fabs(subRn(Apsi[c], t)), fabs(subRn(source[c], t))));
+    }
+    s = blockSum<T, NT>(s, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+}  // namespace k
+}  // namespace b2g

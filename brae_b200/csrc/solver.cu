@@ -1,0 +1,685 @@
+// solver.cu -- the V-cycle, the PCG with the GAMG preconditioner and the standalone GAMG solver,
+// orchestrated on one stream with every scalar kept on the device.
+//
+// Reference: GAMG = src/matrices/lduMatrix/solvers/GAMG/gamg_solver_cpp.cu
+#include "solver.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace b2g {
+
+bool g_profiling = false;
+
+namespace {
+
+constexpr int NT = 256;          // threads of the row and reduction kernels
+constexpr int kMaxPartials = 1024;
+
+int rowsGrid(int n)
+{
+    const int g = ceilDiv(std::max(n, 1), NT);
+    return std::min(g, 16 * DeviceInfo::get().numSMs);
+}
+int redGrid(int n) { return std::min(ceilDiv(std::max(n, 1), NT), kMaxPartials); }
+
+constexpr double kSmall = 1e-20;   // GAMG:16
+constexpr double kVSmall = 1e-300; // GAMG:17
+constexpr double kGreat = 1e+20;   // GAMG:19
+
+__global__ void kInitResidual(PcgScalars* s)
+{
+    s->initRes = s->sumMag / s->nf;
+    s->finalRes = s->initRes;
+}
+
+__global__ void kNfFinish(PcgScalars* s)
+{
+    s->nf = __dadd_rn(s->nf, kSmall);
+}
+
+__global__ void kPcgStart(PcgScalars* s)
+{
+    s->wArA = kGreat;
+    s->wArAold = kGreat;
+    s->iter = 0;
+    s->singular = 0;
+}
+
+// p = w (first iteration) or p = w + beta*p with beta = wArA/wArAold (PCG.C), or the flexible
+// Polak-Ribiere+ beta of the FP32-preconditioned form, max(0, (z.r_new - z.r_old)/rho_old)
+// (device_amg_pcg.cu:36-48)
+__global__ void kPUpdate(int n, const double* __restrict__ w, double* __restrict__ p, const PcgScalars* s,
+                         int flexible)
+{
+    const int iter = s->iter;
+    double beta = 0.0;
+    if (iter != 0)
+    {
+        if (flexible)
+        {
+            const double d = s->wArAold;
+            beta = (d > 1e-300 || d < -1e-300) ? fmax(0.0, __ddiv_rn(__dsub_rn(s->wArA, s->wrOld), d)) : 0.0;
+        }
+        else
+        {
+            beta = __ddiv_rn(s->wArA, s->wArAold);
+        }
+    }
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+    {
+        p[c] = iter == 0 ? w[c] : __dadd_rn(w[c], __dmul_rn(beta, p[c]));
+    }
+}
+
+// checkSingularity, then psi += alpha*p, r -= alpha*w, with the partial sums of |r| (PCG.C)
+template <int NTT>
+__global__ void __launch_bounds__(NTT) kAlphaUpdate(int n, double* __restrict__ psi, const double* __restrict__ p,
+                                                    double* __restrict__ r, const double* __restrict__ w,
+                                                    double* __restrict__ rOld, PcgScalars* s,
+                                                    double* __restrict__ partial)
+{
+    __shared__ double sh[NTT / 32];
+    const double wApA = s->wApA;
+    const bool singular = __ddiv_rn(fabs(wApA), s->nf) < kVSmall;
+    if (singular)
+    {
+        if (blockIdx.x == 0 && threadIdx.x == 0) s->singular = 1;
+        if (threadIdx.x == 0) partial[blockIdx.x] = 0.0;
+        return;
+    }
+    const double alpha = __ddiv_rn(s->wArA, wApA);
+    double acc = 0.0;
+    for (int c = blockIdx.x * NTT + threadIdx.x; c < n; c += gridDim.x * NTT)
+    {
+        const double rc = r[c];
+        if (rOld) rOld[c] = rc;
+        psi[c] = __dadd_rn(psi[c], __dmul_rn(alpha, p[c]));
+        const double rn = __dsub_rn(rc, __dmul_rn(alpha, w[c]));
+        r[c] = rn;
+        acc = __dadd_rn(acc, fabs(rn));
+    }
+    acc = k::blockSum<double, NTT>(acc, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+}
+
+__global__ void kIterFinish(PcgScalars* s)
+{
+    if (s->singular) return;
+    s->finalRes = __ddiv_rn(s->sumMag, s->nf);
+    s->wArAold = s->wArA;
+    s->iter += 1;
+}
+
+__global__ void kResidualFinish(PcgScalars* s)
+{
+    s->finalRes = __ddiv_rn(s->sumMag, s->nf);
+}
+
+template <class T>
+__global__ void kZero(long long n, T* x)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        x[i] = T(0);
+}
+
+bool convergedH(double fin, double init, double tol, double relTol)
+{
+    return fin < tol || (relTol > kSmall && fin < relTol * init);
+}
+
+template <class T>
+k::Rows<T> rowsOf(const LevelAddr& L, const LevelCoef<T>& C)
+{
+    return k::Rows<T>{L.nCells, L.rowStart.p, L.col.p, C.val.p, C.diag.p};
+}
+
+template <class T, class S>
+void castInto(long long n, const S* in, T* out, cudaStream_t s)
+{
+    if (n) k::castArray<T, S><<<std::min(ceilDiv(n, NT), 4096), NT, 0, s>>>(n, in, out);
+    B2G_LAUNCH_CHECK();
+}
+
+template <class T>
+void zeroArray(long long n, T* x, cudaStream_t s)
+{
+    if (n) kZero<T><<<std::min(ceilDiv(n, NT), 4096), NT, 0, s>>>(n, x);
+    B2G_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+template <> VCycleData<double>& Matrix::data<double>() { return v64; }
+template <> VCycleData<float>& Matrix::data<float>() { return v32; }
+
+Matrix::Matrix(Mesh* m, cudaStream_t s) : mesh(m), stream(s)
+{
+    const int n0 = m->lev[0].nCells;
+    for (DBuf<double>* b : {&psi, &source, &rA, &wA, &pA, &AwA, &fc, &fr}) b->alloc(n0, s);
+    scal.alloc(1, s);
+    scal.zero(s);
+    // reductions run before the coarse levels exist (the initial residual and normFactor)
+    v64.partial.alloc(2 * kMaxPartials, s);
+    v64.sf.alloc(1, s);
+    err.alloc(1, s);
+    err.zero(s);
+    coarseCount.alloc(1, s);
+    coarseCount.zero(s);
+    v64.coef.resize(m->lev.size());
+}
+
+void Matrix::setFine(const double* diag, const double* upper, int memspace)
+{
+    const LevelAddr& L = mesh->lev[0];
+    LevelCoef<double>& C = v64.coef[0];
+    const cudaMemcpyKind kind = memspace == B2G_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    C.diag.alloc(L.nCells, stream);
+    C.upper.alloc(L.nFaces, stream);
+    B2G_CUDA(cudaMemcpyAsync(C.diag.p, diag, sizeof(double) * L.nCells, kind, stream));
+    if (L.nFaces) B2G_CUDA(cudaMemcpyAsync(C.upper.p, upper, sizeof(double) * L.nFaces, kind, stream));
+    C.val.alloc(2 * (size_t)L.nFaces, stream);
+    if (L.nFaces)
+        k::gatherVal<double, double><<<std::min(ceilDiv(2LL * L.nFaces, NT), 8192), NT, 0, stream>>>(
+            2LL * L.nFaces, L.entFace.p, C.upper.p, C.val.p);
+    B2G_LAUNCH_CHECK();
+    coarseBuilt = false;
+    v32.built = false;
+}
+
+// GamgHierarchy::build (GAMG:565-623): Galerkin coarse matrices level by level
+void Matrix::buildCoarse()
+{
+    if (coarseBuilt) return;
+    const int nL = nLevels();
+    for (int i = 0; i < nL; ++i)
+    {
+        const Step& S = mesh->step[i];
+        const LevelAddr& Cl = mesh->lev[i + 1];
+        const LevelCoef<double>& F = v64.coef[i];
+        LevelCoef<double>& C = v64.coef[i + 1];
+        C.diag.alloc(Cl.nCells, stream);
+        C.upper.alloc(Cl.nFaces, stream);
+        C.val.alloc(2 * (size_t)Cl.nFaces, stream);
+        k::galerkinDiag<<<rowsGrid(Cl.nCells), NT, 0, stream>>>(Cl.nCells, S.cellStart.p, S.cellList.p, S.intStart.p,
+                                                                S.intList.p, F.diag.p, F.upper.p, C.diag.p);
+        if (Cl.nFaces)
+        {
+            k::galerkinUpper<<<rowsGrid(Cl.nFaces), NT, 0, stream>>>(Cl.nFaces, S.faceBeg.p, S.faceEnd.p,
+                                                                     S.faceList.p, F.upper.p, C.upper.p);
+            k::gatherVal<double, double><<<std::min(ceilDiv(2LL * Cl.nFaces, NT), 8192), NT, 0, stream>>>(
+                2LL * Cl.nFaces, Cl.entFace.p, C.upper.p, C.val.p);
+        }
+        B2G_LAUNCH_CHECK();
+    }
+    // V-cycle work
+    v64.corr.resize(nL);
+    v64.src.resize(nL);
+    for (int i = 0; i < nL; ++i)
+    {
+        v64.corr[i].alloc(mesh->lev[i + 1].nCells, stream);
+        v64.src[i].alloc(mesh->lev[i + 1].nCells, stream);
+    }
+    const int n0 = mesh->lev[0].nCells;
+    v64.ACf.alloc(n0, stream);
+    v64.preSmoothed.alloc(n0, stream);
+    const int nc = nL > 0 ? mesh->lev[nL].nCells : n0;
+    for (DBuf<double>* b : {&v64.cpA, &v64.cwA, &v64.crA, &v64.crD}) b->alloc(std::max(nc, 1), stream);
+    v64.built = true;
+    coarseBuilt = true;
+}
+
+void Matrix::ensureFp32()
+{
+    if (v32.built) return;
+    buildCoarse();
+    const int nL = nLevels();
+    v32.coef.resize(nL + 1);
+    for (int i = 0; i <= nL; ++i)
+    {
+        const LevelAddr& L = mesh->lev[i];
+        LevelCoef<float>& C = v32.coef[i];
+        C.diag.alloc(L.nCells, stream);
+        C.upper.alloc(L.nFaces, stream);
+        C.val.alloc(2 * (size_t)L.nFaces, stream);
+        castInto<float, double>(L.nCells, v64.coef[i].diag.p, C.diag.p, stream);
+        castInto<float, double>(L.nFaces, v64.coef[i].upper.p, C.upper.p, stream);
+        castInto<float, double>(2LL * L.nFaces, v64.coef[i].val.p, C.val.p, stream);
+    }
+    v32.corr.resize(nL);
+    v32.src.resize(nL);
+    for (int i = 0; i < nL; ++i)
+    {
+        v32.corr[i].alloc(mesh->lev[i + 1].nCells, stream);
+        v32.src[i].alloc(mesh->lev[i + 1].nCells, stream);
+    }
+    const int n0 = mesh->lev[0].nCells;
+    v32.ACf.alloc(n0, stream);
+    v32.preSmoothed.alloc(n0, stream);
+    v32.partial.alloc(2 * kMaxPartials, stream);
+    v32.sf.alloc(1, stream);
+    for (DBuf<float>* b : {&r32, &w32, &AwA32, &fc32, &fr32}) b->alloc(n0, stream);
+    rOld.alloc(n0, stream);
+    v32.built = true;
+}
+
+template <class T>
+void Matrix::amul(int level, const T* x, T* y)
+{
+    const LevelAddr& L = mesh->lev[level];
+    k::amul<T><<<rowsGrid(L.nCells), NT, 0, stream>>>(rowsOf(L, data<T>().coef[level]), x, y);
+    B2G_LAUNCH_CHECK();
+    ++launches;
+}
+
+template <class T>
+void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps)
+{
+    if (nSweeps <= 0) return;
+    if (smoother != B2G_SMOOTHER_GAUSS_SEIDEL)
+        fail(B2G_ERR_REFUSED, "b2g: the device smoother for this entry is GaussSeidel only so far; "
+                              "symGaussSeidel, DIC and DICGaussSeidel are not built on the device yet.");
+    const LevelAddr& L = mesh->lev[level];
+    const GsSchedule& G = L.gs;
+    const LevelCoef<T>& C = data<T>().coef[level];
+    k::GsArgs<T> a;
+    a.nParts = G.nParts;
+    a.maxDepth = G.maxDepth;
+    a.order = G.order.p;
+    a.partLvlStart = G.partLvlStart.p;
+    a.lvlStart = G.lvlStart.p;
+    a.lvlDepth = G.lvlDepth.p;
+    a.lvlNeedUp = G.lvlNeedUp.p;
+    a.lvlNeedDown = G.lvlNeedDown.p;
+    a.depStart = G.depStart.p;
+    a.depList = G.depList.p;
+    a.rowStart = L.rowStart.p;
+    a.losortStart = L.losortStart.p;
+    a.col = L.col.p;
+    a.val = C.val.p;
+    a.diag = C.diag.p;
+    a.b = src;
+    a.psi = psiL;
+    a.progress = G.progress.p;
+    a.err = err.p;
+    int bd = ((G.maxLevelCells + 31) / 32) * 32;
+    bd = std::max(64, std::min(1024, bd));
+    B2G_CUDA(cudaMemsetAsync(G.progress.p, 0, sizeof(unsigned) * G.nParts, stream));
+    k::gsPipelined<T><<<G.nParts, bd, 0, stream>>>(a, nSweeps);
+    B2G_LAUNCH_CHECK();
+    launches += 2;
+}
+
+template <class T>
+void Matrix::scale(int level, T* field, T* Acf, const T* src)
+{
+    const LevelAddr& L = mesh->lev[level];
+    VCycleData<T>& D = data<T>();
+    const int g = redGrid(L.nCells);
+    k::amulScaleDots<T, NT><<<g, NT, 0, stream>>>(rowsOf(L, D.coef[level]), field, src, Acf, D.partial.p);
+    k::scaleFactor<T, NT><<<1, NT, 0, stream>>>(D.partial.p, g, D.sf.p);
+    k::scaleUpdate<T><<<rowsGrid(L.nCells), NT, 0, stream>>>(L.nCells, D.sf.p, field, src, Acf, D.coef[level].diag.p);
+    B2G_LAUNCH_CHECK();
+    launches += 3;
+}
+
+template <class T>
+void Matrix::restrictTo(int step, const T* fine, T* coarse)
+{
+    const Step& S = mesh->step[step];
+    k::restrictField<T><<<rowsGrid(S.nCoarse), NT, 0, stream>>>(S.nCoarse, S.cellStart.p, S.cellList.p, fine, coarse);
+    B2G_LAUNCH_CHECK();
+    ++launches;
+}
+
+template <class T>
+void Matrix::prolongFrom(int step, const T* coarse, T* fine)
+{
+    const Step& S = mesh->step[step];
+    k::prolongField<T><<<rowsGrid(S.nFine), NT, 0, stream>>>(S.nFine, S.restrictAddr.p, coarse, fine);
+    B2G_LAUNCH_CHECK();
+    ++launches;
+}
+
+template <>
+void Matrix::coarsestSolve<double>(int level, double* x, const double* src, double tol, double relTol,
+                                   k::DevPerf* out, bool logIt)
+{
+    const LevelAddr& L = mesh->lev[level];
+    const LevelCoef<double>& C = v64.coef[level];
+    k::CoarsestArgs<double> a;
+    a.n = L.nCells;
+    a.nF = L.nFaces;
+    a.lower = L.lower.p;
+    a.upper = L.upper.p;
+    a.rowStart = L.rowStart.p;
+    a.col = L.col.p;
+    a.val = C.val.p;
+    a.diag = C.diag.p;
+    a.coef = C.upper.p;
+    a.source = src;
+    a.psi = x;
+    a.pA = v64.cpA.p;
+    a.wA = v64.cwA.p;
+    a.rA = v64.crA.p;
+    a.rD = v64.crD.p;
+    a.tolerance = tol;
+    a.relTol = relTol;
+    a.maxIter = 1000;
+    a.log = logIt ? coarseLog.p : nullptr;
+    a.logCount = coarseCount.p;
+    a.logCapacity = coarseLogCapacity;
+    a.out = out;
+    k::coarsestPcgDic<double><<<1, 32, 0, stream>>>(a);
+    B2G_LAUNCH_CHECK();
+    ++launches;
+}
+
+// The FP32 V-cycle solves its coarsest level in FP64 (the level has 10-20 cells; its precision is
+// free): the FP32 source is widened, solved by the same PCG-DIC, and narrowed back.
+template <>
+void Matrix::coarsestSolve<float>(int level, float* x, const float* src, float tol, float relTol,
+                                  k::DevPerf* out, bool logIt)
+{
+    const int n = mesh->lev[level].nCells;
+    double* x64 = v64.corr[level - 1].p;
+    double* s64 = v64.src[level - 1].p;
+    castInto<double, float>(n, src, s64, stream);
+    castInto<double, float>(n, x, x64, stream);
+    coarsestSolve<double>(level, x64, s64, static_cast<double>(tol), static_cast<double>(relTol), out, logIt);
+    castInto<float, double>(n, x64, x, stream);
+}
+
+double Matrix::normFactor(int level, const double* x, const double* src, const double* Apsi)
+{
+    const LevelAddr& L = mesh->lev[level];
+    const int g = redGrid(L.nCells);
+    k::reducePartial<double, NT, k::RED_SUM><<<g, NT, 0, stream>>>(L.nCells, x, nullptr, v64.partial.p);
+    k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->sumPsi);
+    k::normFactorPartial<double, NT><<<g, NT, 0, stream>>>(rowsOf(L, v64.coef[level]), x, src, Apsi,
+                                                           &scal.p->sumPsi, v64.partial.p);
+    k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->nf);
+    kNfFinish<<<1, 1, 0, stream>>>(scal.p);
+    B2G_LAUNCH_CHECK();
+    launches += 5;
+    double nf = 0;
+    B2G_CUDA(cudaMemcpyAsync(&nf, &scal.p->nf, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    B2G_CUDA(cudaStreamSynchronize(stream));
+    return nf;
+}
+
+// GAMGSolver::Vcycle (GAMG:627-735). psi is corrected in place; Apsi is scratch.
+template <class T>
+void Matrix::vcycle(const b2g_controls& c, T* x, const T* src, T* Apsi, T* fcor, const T* fres)
+{
+    VCycleData<T>& D = data<T>();
+    const int coarsest = nLevels() - 1;
+    restrictTo<T>(0, fres, D.src[0].p);
+    for (int li = 0; li < coarsest; ++li)
+    {
+        const int lv = li + 1;
+        if (c.nPreSweeps)
+        {
+            zeroArray<T>(n(lv), D.corr[li].p, stream);
+            smooth<T>(lv, c.smoother, D.corr[li].p, D.src[li].p,
+                      std::min(c.nPreSweeps + c.preSweepsLevelMultiplier * li, c.maxPreSweeps));
+            if (c.scaleCorrection && li < coarsest - 1) scale<T>(lv, D.corr[li].p, D.ACf.p, D.src[li].p);
+            // residual with rA aliasing the source, per cell
+            k::residual<T><<<rowsGrid(n(lv)), NT, 0, stream>>>(rowsOf(mesh->lev[lv], D.coef[lv]), D.src[li].p,
+                                                               D.corr[li].p, D.src[li].p);
+            B2G_LAUNCH_CHECK();
+        }
+        restrictTo<T>(li + 1, D.src[li].p, D.src[li + 1].p);
+    }
+    zeroArray<T>(n(coarsest + 1), D.corr[coarsest].p, stream);
+    coarsestSolve<T>(coarsest + 1, D.corr[coarsest].p, D.src[coarsest].p, static_cast<T>(c.precTolerance),
+                     static_cast<T>(c.precRelTol), nullptr, coarseLogCapacity > 0);
+    for (int li = coarsest - 1; li >= 0; --li)
+    {
+        const int lv = li + 1;
+        if (c.nPreSweeps)
+            B2G_CUDA(cudaMemcpyAsync(D.preSmoothed.p, D.corr[li].p, sizeof(T) * n(lv), cudaMemcpyDeviceToDevice,
+                                     stream));
+        prolongFrom<T>(li + 1, D.corr[li + 1].p, D.corr[li].p);
+        if (c.scaleCorrection && li < coarsest - 1) scale<T>(lv, D.corr[li].p, D.ACf.p, D.src[li].p);
+        if (c.nPreSweeps)
+        {
+            k::addInPlace<T><<<rowsGrid(n(lv)), NT, 0, stream>>>(n(lv), D.corr[li].p, D.preSmoothed.p);
+            B2G_LAUNCH_CHECK();
+        }
+        smooth<T>(lv, c.smoother, D.corr[li].p, D.src[li].p,
+                  std::min(c.nPostSweeps + c.postSweepsLevelMultiplier * li, c.maxPostSweeps));
+    }
+    prolongFrom<T>(0, D.corr[0].p, fcor);
+    const LevelAddr& F = mesh->lev[0];
+    if (c.scaleCorrection)
+    {
+        const int g = redGrid(F.nCells);
+        k::amulScaleDots<T, NT><<<g, NT, 0, stream>>>(rowsOf(F, D.coef[0]), fcor, fres, Apsi, D.partial.p);
+        k::scaleFactor<T, NT><<<1, NT, 0, stream>>>(D.partial.p, g, D.sf.p);
+        k::scaleUpdateAdd<T><<<rowsGrid(F.nCells), NT, 0, stream>>>(F.nCells, D.sf.p, fcor, fres, Apsi,
+                                                                   D.coef[0].diag.p, x);
+        launches += 3;
+    }
+    else
+    {
+        k::addInPlace<T><<<rowsGrid(F.nCells), NT, 0, stream>>>(F.nCells, x, fcor);
+        ++launches;
+    }
+    B2G_LAUNCH_CHECK();
+    smooth<T>(0, c.smoother, x, src, c.nFinestSweeps);
+}
+
+// GAMGPreconditioner::precondition (GAMG:1089-1107)
+void Matrix::precondition(const b2g_controls& c, double* w, const double* r)
+{
+    const int n0 = n(0);
+    if (c.precision == B2G_PRECISION_FP32_PRECOND)
+    {
+        ensureFp32();
+        castInto<float, double>(n0, r, r32.p, stream);
+        zeroArray<float>(n0, w32.p, stream);
+        const float* frp = r32.p;
+        for (int cycle = 0; cycle < c.nVcycles; ++cycle)
+        {
+            vcycle<float>(c, w32.p, r32.p, AwA32.p, fc32.p, frp);
+            if (cycle < c.nVcycles - 1)
+            {
+                amul<float>(0, w32.p, AwA32.p);
+                k::subtract<float><<<rowsGrid(n0), NT, 0, stream>>>(n0, r32.p, AwA32.p, fr32.p);
+                B2G_LAUNCH_CHECK();
+                frp = fr32.p;
+            }
+        }
+        castInto<double, float>(n0, w32.p, w, stream);
+        return;
+    }
+    zeroArray<double>(n0, w, stream);
+    const double* frp = r;
+    for (int cycle = 0; cycle < c.nVcycles; ++cycle)
+    {
+        vcycle<double>(c, w, r, AwA.p, fc.p, frp);
+        if (cycle < c.nVcycles - 1)
+        {
+            amul<double>(0, w, AwA.p);
+            k::subtract<double><<<rowsGrid(n0), NT, 0, stream>>>(n0, r, AwA.p, fr.p);
+            B2G_LAUNCH_CHECK();
+            frp = fr.p;
+        }
+    }
+}
+
+void Matrix::resetLog(int capacity)
+{
+    coarseLogCapacity = capacity;
+    if (capacity > 0 && static_cast<int>(coarseLog.n) < capacity) coarseLog.alloc(capacity, stream);
+    coarseCount.zero(stream);
+}
+
+void Matrix::readLog(b2g_solve_log* log)
+{
+    if (!log) return;
+    int cnt = 0;
+    B2G_CUDA(cudaMemcpyAsync(&cnt, coarseCount.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    B2G_CUDA(cudaStreamSynchronize(stream));
+    log->coarsestCount = cnt;
+    const int m = std::min(cnt, log->coarsestCapacity);
+    if (m > 0 && log->coarsest)
+    {
+        std::vector<k::DevPerf> h(m);
+        B2G_CUDA(cudaMemcpyAsync(h.data(), coarseLog.p, sizeof(k::DevPerf) * m, cudaMemcpyDeviceToHost, stream));
+        B2G_CUDA(cudaStreamSynchronize(stream));
+        for (int i = 0; i < m; ++i)
+        {
+            log->coarsest[i].initialResidual = h[i].initialResidual;
+            log->coarsest[i].finalResidual = h[i].finalResidual;
+            log->coarsest[i].nIterations = h[i].nIterations;
+        }
+    }
+}
+
+void Matrix::checkDeviceError()
+{
+    int e = 0;
+    B2G_CUDA(cudaMemcpyAsync(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    B2G_CUDA(cudaStreamSynchronize(stream));
+    if (e)
+    {
+        err.zero(stream);
+        fail(B2G_ERR_DEVICE_TIMEOUT,
+             "b2g: a bounded device-side wait in the Gauss-Seidel sweep gave up; the result is invalid.");
+    }
+}
+
+// PCG::scalarSolve with the GAMG preconditioner (pcgGamgSolveImpl, GAMG:1031-1143)
+b2g_perf Matrix::pcg(const b2g_controls& c, b2g_solve_log* log)
+{
+    const int n0 = n(0);
+    resetLog(log ? std::max(log->coarsestCapacity, 0) : 0);
+    amul<double>(0, psi.p, wA.p);
+    k::subtract<double><<<rowsGrid(n0), NT, 0, stream>>>(n0, source.p, wA.p, rA.p);
+    B2G_LAUNCH_CHECK();
+    normFactor(0, psi.p, source.p, wA.p);
+    const int g = redGrid(n0);
+    k::reducePartial<double, NT, k::RED_SUMMAG><<<g, NT, 0, stream>>>(n0, rA.p, nullptr, v64.partial.p);
+    k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->sumMag);
+    kInitResidual<<<1, 1, 0, stream>>>(scal.p);
+    B2G_LAUNCH_CHECK();
+    PcgScalars hs;
+    B2G_CUDA(cudaMemcpyAsync(&hs, scal.p, sizeof(hs), cudaMemcpyDeviceToHost, stream));
+    B2G_CUDA(cudaStreamSynchronize(stream));
+    b2g_perf perf;
+    perf.initialResidual = hs.initRes;
+    perf.finalResidual = hs.initRes;
+    perf.nIterations = 0;
+    if (log) log->historyCount = 0;
+    if (c.minIter <= 0 && convergedH(perf.finalResidual, perf.initialResidual, c.tolerance, c.relTol)) return perf;
+    // the preconditioner, built on first use (PCG.C:111-118)
+    if (nLevels() == 0)
+        fail(B2G_ERR_REFUSED, "b2g GAMG: no coarse levels created, either matrix too small for GAMG or "
+                              "nCellsInCoarsestLevel too large (GAMGSolver.C:333).");
+    buildCoarse();
+    const bool flexible = c.precision == B2G_PRECISION_FP32_PRECOND;
+    if (flexible) ensureFp32();
+    kPcgStart<<<1, 1, 0, stream>>>(scal.p);
+    B2G_LAUNCH_CHECK();
+    do
+    {
+        precondition(c, wA.p, rA.p);
+        k::reducePartial<double, NT, k::RED_DOT><<<g, NT, 0, stream>>>(n0, wA.p, rA.p, v64.partial.p);
+        k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->wArA);
+        if (flexible)
+        {
+            k::reducePartial<double, NT, k::RED_DOT><<<g, NT, 0, stream>>>(n0, wA.p, rOld.p, v64.partial.p);
+            k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->wrOld);
+        }
+        kPUpdate<<<rowsGrid(n0), NT, 0, stream>>>(n0, wA.p, pA.p, scal.p, flexible ? 1 : 0);
+        B2G_LAUNCH_CHECK();
+        amul<double>(0, pA.p, wA.p);
+        k::reducePartial<double, NT, k::RED_DOT><<<g, NT, 0, stream>>>(n0, wA.p, pA.p, v64.partial.p);
+        k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->wApA);
+        kAlphaUpdate<NT><<<g, NT, 0, stream>>>(n0, psi.p, pA.p, rA.p, wA.p, flexible ? rOld.p : nullptr, scal.p,
+                                              v64.partial.p);
+        k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->sumMag);
+        kIterFinish<<<1, 1, 0, stream>>>(scal.p);
+        B2G_LAUNCH_CHECK();
+        launches += 9;
+        B2G_CUDA(cudaMemcpyAsync(&hs, scal.p, sizeof(hs), cudaMemcpyDeviceToHost, stream));
+        B2G_CUDA(cudaStreamSynchronize(stream));
+        if (hs.singular) break;
+        perf.finalResidual = hs.finalRes;
+        if (log && log->history && perf.nIterations < log->historyCapacity)
+            log->history[perf.nIterations] = hs.finalRes;
+        ++perf.nIterations;
+        if (log) log->historyCount = perf.nIterations;
+    } while ((perf.nIterations < c.maxIter &&
+              !convergedH(perf.finalResidual, perf.initialResidual, c.tolerance, c.relTol)) ||
+             perf.nIterations < c.minIter);
+    checkDeviceError();
+    readLog(log);
+    return perf;
+}
+
+// gamgSolveFoldedImpl (GAMG:961-1027): the standalone GAMG solver
+b2g_perf Matrix::gamg(const b2g_controls& c, b2g_solve_log* log)
+{
+    const int n0 = n(0);
+    if (nLevels() == 0)
+        fail(B2G_ERR_REFUSED, "b2g GAMG: no coarse levels created, either matrix too small for GAMG or "
+                              "nCellsInCoarsestLevel too large (GAMGSolver.C:333).");
+    resetLog(log ? std::max(log->coarsestCapacity, 0) : 0);
+    buildCoarse();
+    b2g_controls cc = c;
+    // the standalone solver's coarsest level runs to the GAMG entry's own tolerance and relTol
+    cc.precTolerance = c.tolerance;
+    cc.precRelTol = c.relTol;
+    amul<double>(0, psi.p, AwA.p);
+    normFactor(0, psi.p, source.p, AwA.p);
+    k::subtract<double><<<rowsGrid(n0), NT, 0, stream>>>(n0, source.p, AwA.p, fr.p);
+    const int g = redGrid(n0);
+    k::reducePartial<double, NT, k::RED_SUMMAG><<<g, NT, 0, stream>>>(n0, fr.p, nullptr, v64.partial.p);
+    k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->sumMag);
+    kInitResidual<<<1, 1, 0, stream>>>(scal.p);
+    B2G_LAUNCH_CHECK();
+    PcgScalars hs;
+    B2G_CUDA(cudaMemcpyAsync(&hs, scal.p, sizeof(hs), cudaMemcpyDeviceToHost, stream));
+    B2G_CUDA(cudaStreamSynchronize(stream));
+    b2g_perf perf;
+    perf.initialResidual = hs.initRes;
+    perf.finalResidual = hs.initRes;
+    perf.nIterations = 0;
+    if (log) log->historyCount = 0;
+    if (c.minIter <= 0 && convergedH(perf.finalResidual, perf.initialResidual, c.tolerance, c.relTol)) return perf;
+    do
+    {
+        vcycle<double>(cc, psi.p, source.p, AwA.p, fc.p, fr.p);
+        amul<double>(0, psi.p, AwA.p);
+        k::subtract<double><<<rowsGrid(n0), NT, 0, stream>>>(n0, source.p, AwA.p, fr.p);
+        k::reducePartial<double, NT, k::RED_SUMMAG><<<g, NT, 0, stream>>>(n0, fr.p, nullptr, v64.partial.p);
+        k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->sumMag);
+        kResidualFinish<<<1, 1, 0, stream>>>(scal.p);
+        B2G_LAUNCH_CHECK();
+        B2G_CUDA(cudaMemcpyAsync(&hs, scal.p, sizeof(hs), cudaMemcpyDeviceToHost, stream));
+        B2G_CUDA(cudaStreamSynchronize(stream));
+        perf.finalResidual = hs.finalRes;
+        if (log && log->history && perf.nIterations < log->historyCapacity)
+            log->history[perf.nIterations] = hs.finalRes;
+        ++perf.nIterations;
+        if (log) log->historyCount = perf.nIterations;
+    } while ((perf.nIterations < c.maxIter &&
+              !convergedH(perf.finalResidual, perf.initialResidual, c.tolerance, c.relTol)) ||
+             perf.nIterations < c.minIter);
+    checkDeviceError();
+    readLog(log);
+    return perf;
+}
+
+template void Matrix::amul<double>(int, const double*, double*);
+template void Matrix::amul<float>(int, const float*, float*);
+template void Matrix::smooth<double>(int, int, double*, const double*, int);
+template void Matrix::smooth<float>(int, int, float*, const float*, int);
+template void Matrix::scale<double>(int, double*, double*, const double*);
+template void Matrix::restrictTo<double>(int, const double*, double*);
+template void Matrix::prolongFrom<double>(int, const double*, double*);
+
+}  // namespace b2g

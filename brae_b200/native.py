@@ -1,0 +1,361 @@
+"""ctypes bindings of include/brae_gamg.h.
+
+Array arguments may be numpy arrays (host memory, ``B2G_MEM_HOST``) or CUDA tensors (device memory,
+``B2G_MEM_DEVICE``); the two are never mixed in one call. Device work runs on the stream the mesh
+was created on (torch's current stream when created from Python), and every call returns after it
+completes.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import NamedTuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbrae_gamg.so")
+
+B2G_MEM_HOST = 0
+B2G_MEM_DEVICE = 1
+SMOOTHERS = {"GaussSeidel": 0, "symGaussSeidel": 1, "DIC": 2, "DICGaussSeidel": 3}
+STATUS = {0: "OK", 1: "ARGUMENT", 2: "REFUSED", 3: "CUDA", 4: "NO_MEMORY", 5: "DEVICE_TIMEOUT", 6: "STATE"}
+
+
+class GamgError(RuntimeError):
+    """A failed call: ``status`` is the b2g_status name, the message is b2g_last_error()."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{STATUS.get(status, status)}] {message}")
+        self.status = STATUS.get(status, str(status))
+
+
+class Controls(C.Structure):
+    """b2g_controls."""
+    _fields_ = [("solver", C.c_int), ("tolerance", C.c_double), ("relTol", C.c_double),
+                ("maxIter", C.c_int), ("minIter", C.c_int), ("smoother", C.c_int),
+                ("precTolerance", C.c_double), ("precRelTol", C.c_double),
+                ("nPreSweeps", C.c_int), ("preSweepsLevelMultiplier", C.c_int),
+                ("maxPreSweeps", C.c_int), ("nPostSweeps", C.c_int),
+                ("postSweepsLevelMultiplier", C.c_int), ("maxPostSweeps", C.c_int),
+                ("nFinestSweeps", C.c_int), ("scaleCorrection", C.c_int),
+                ("nCellsInCoarsestLevel", C.c_int), ("nVcycles", C.c_int), ("precision", C.c_int)]
+
+
+class _Perf(C.Structure):
+    _fields_ = [("initialResidual", C.c_double), ("finalResidual", C.c_double),
+                ("nIterations", C.c_int)]
+
+
+class _Log(C.Structure):
+    _fields_ = [("history", C.POINTER(C.c_double)), ("historyCapacity", C.c_int),
+                ("historyCount", C.c_int), ("coarsest", C.POINTER(_Perf)),
+                ("coarsestCapacity", C.c_int), ("coarsestCount", C.c_int)]
+
+
+class SolverPerformance(NamedTuple):
+    """SolverPerformance (src/OpenFOAM/matrices/pcg.cuh:16-21)."""
+    initialResidual: float
+    finalResidual: float
+    nIterations: int
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built; run `python -m brae_b200.build` (nvcc, sm_100a)")
+    L = C.CDLL(LIB_PATH)
+    vp, ip, dp = C.c_void_p, C.c_int, C.c_double
+    sig = {
+        "b2g_last_error": (C.c_char_p, []),
+        "b2g_version": (C.c_char_p, []),
+        "b2g_set_profiling": (ip, [ip]),
+        "b2g_controls_default": (ip, [C.POINTER(Controls)]),
+        "b2g_controls_read": (ip, [C.c_char_p, C.POINTER(Controls)]),
+        "b2g_mesh_create": (ip, [ip, ip, vp, vp, vp, vp, ip, C.POINTER(C.c_int), ip, vp,
+                                 C.POINTER(vp)]),
+        "b2g_mesh_destroy": (ip, [vp]),
+        "b2g_mesh_levels": (ip, [vp, C.POINTER(C.c_int)]),
+        "b2g_mesh_level_size": (ip, [vp, ip, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "b2g_mesh_get_step": (ip, [vp, ip, vp, vp, vp, vp, vp]),
+        "b2g_mesh_build_ms": (ip, [vp, C.POINTER(C.c_float)]),
+        "b2g_pcg_gamg_solve": (ip, [vp, vp, vp, vp, vp, C.POINTER(Controls), ip, vp,
+                                    C.POINTER(_Perf), C.POINTER(_Log)]),
+        "b2g_gamg_solve": (ip, [vp, vp, vp, vp, vp, C.POINTER(Controls), ip, vp, C.POINTER(_Perf),
+                                C.POINTER(_Log)]),
+        "b2g_matrix_create": (ip, [vp, vp, vp, ip, vp, C.POINTER(vp)]),
+        "b2g_matrix_destroy": (ip, [vp]),
+        "b2g_matrix_get_level": (ip, [vp, ip, vp, vp]),
+        "b2g_level_amul": (ip, [vp, ip, vp, vp]),
+        "b2g_level_smooth": (ip, [vp, ip, ip, vp, vp, ip]),
+        "b2g_level_scale": (ip, [vp, ip, vp, vp, vp]),
+        "b2g_step_restrict": (ip, [vp, ip, vp, vp]),
+        "b2g_step_prolong": (ip, [vp, ip, vp, vp]),
+        "b2g_level_norm_factor": (ip, [vp, ip, vp, vp, vp, C.POINTER(C.c_double)]),
+        "b2g_level_pcg_dic": (ip, [vp, ip, vp, vp, dp, dp, C.POINTER(_Perf)]),
+        "b2g_precondition": (ip, [vp, C.POINTER(Controls), vp, vp, C.POINTER(_Log)]),
+        "b2g_matrix_pcg_solve": (ip, [vp, vp, vp, C.POINTER(Controls), ip, C.POINTER(_Perf),
+                                      C.POINTER(_Log)]),
+        "b2g_matrix_timings": (ip, [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    return L
+
+
+lib = _load()
+EXPORTED = [
+    "b2g_last_error", "b2g_version", "b2g_set_profiling", "b2g_controls_default",
+    "b2g_controls_read", "b2g_mesh_create", "b2g_mesh_destroy", "b2g_mesh_levels",
+    "b2g_mesh_level_size", "b2g_mesh_get_step", "b2g_mesh_build_ms", "b2g_pcg_gamg_solve",
+    "b2g_gamg_solve", "b2g_matrix_create", "b2g_matrix_destroy", "b2g_matrix_get_level",
+    "b2g_level_amul", "b2g_level_smooth", "b2g_level_scale", "b2g_step_restrict",
+    "b2g_step_prolong", "b2g_level_norm_factor", "b2g_level_pcg_dic", "b2g_precondition",
+    "b2g_matrix_pcg_solve", "b2g_matrix_timings",
+]
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise GamgError(rc, lib.b2g_last_error().decode())
+
+
+def controls_default(**overrides) -> Controls:
+    c = Controls()
+    _check(lib.b2g_controls_default(C.byref(c)))
+    for k, v in overrides.items():
+        if k == "smoother" and isinstance(v, str):
+            v = SMOOTHERS[v]
+        if k == "precision" and isinstance(v, str):
+            v = {"fp64": 0, "fp32_precond": 1}[v]
+        setattr(c, k, v)
+    return c
+
+
+def read_controls(entry_text: str) -> Controls:
+    """Reads an fvSolution solver entry (readGamgControls with the reference's refusals)."""
+    c = Controls()
+    _check(lib.b2g_controls_read(entry_text.encode(), C.byref(c)))
+    return c
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _ptr(x):
+    if x is None:
+        return None
+    if _is_torch(x):
+        return C.c_void_p(x.data_ptr())
+    return C.c_void_p(x.ctypes.data)
+
+
+def _memspace(*arrays) -> int:
+    dev = [_is_torch(a) and a.is_cuda for a in arrays if a is not None]
+    if all(dev):
+        return B2G_MEM_DEVICE
+    if not any(dev):
+        return B2G_MEM_HOST
+    raise ValueError("arrays must be all host (numpy) or all CUDA tensors")
+
+
+def _stream():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    except ImportError:
+        pass
+    return None
+
+
+def _as_host(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+class Mesh:
+    """The mesh's GAMG hierarchy (GamgAgglomerationCache): built once, on the device."""
+
+    def __init__(self, lower, upper, Sf, magSf, n_cells: int, n_coarsest: int = 10,
+                 forward: bool = True):
+        if not _is_torch(lower):
+            lower = _as_host(lower, np.int32)
+            upper = _as_host(upper, np.int32)
+            Sf = _as_host(Sf, np.float64).reshape(-1)
+            magSf = _as_host(magSf, np.float64)
+        ms = _memspace(lower, upper, Sf, magSf)
+        fw = C.c_int(1 if forward else 0)
+        h = C.c_void_p()
+        nF = int(lower.shape[0])
+        _check(lib.b2g_mesh_create(int(n_cells), nF, _ptr(lower), _ptr(upper), _ptr(Sf),
+                                   _ptr(magSf), int(n_coarsest), C.byref(fw), ms, _stream(),
+                                   C.byref(h)))
+        self.handle = h
+        self.forward = bool(fw.value)
+        self.n_cells = int(n_cells)
+        self.n_faces = nF
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            lib.b2g_mesh_destroy(h)
+            self.handle = None
+
+    @property
+    def n_levels(self) -> int:
+        n = C.c_int()
+        _check(lib.b2g_mesh_levels(self.handle, C.byref(n)))
+        return n.value
+
+    def level_size(self, level: int):
+        nc, nf = C.c_int(), C.c_int()
+        _check(lib.b2g_mesh_level_size(self.handle, level, C.byref(nc), C.byref(nf)))
+        return nc.value, nf.value
+
+    @property
+    def build_ms(self) -> float:
+        v = C.c_float()
+        _check(lib.b2g_mesh_build_ms(self.handle, C.byref(v)))
+        return v.value
+
+    def step(self, i: int) -> dict:
+        nc, nf = self.level_size(i)
+        cc, cf = self.level_size(i + 1)
+        r = np.empty(nc, np.int32)
+        fr = np.empty(nf, np.int32)
+        fl = np.empty(nf, np.int8)
+        lo = np.empty(cf, np.int32)
+        up = np.empty(cf, np.int32)
+        _check(lib.b2g_mesh_get_step(self.handle, i, _ptr(r), _ptr(fr), _ptr(fl), _ptr(lo),
+                                     _ptr(up)))
+        return dict(restrict=r, face_restrict=fr, flip=fl, lower=lo, upper=up)
+
+
+class _LogBuf:
+    def __init__(self, history_cap: int, coarsest_cap: int):
+        self.hist = (C.c_double * max(history_cap, 1))()
+        self.coarse = (_Perf * max(coarsest_cap, 1))()
+        self.log = _Log(C.cast(self.hist, C.POINTER(C.c_double)), history_cap, 0,
+                        C.cast(self.coarse, C.POINTER(_Perf)), coarsest_cap, 0)
+
+    def history(self):
+        return [self.hist[i] for i in range(min(self.log.historyCount, self.log.historyCapacity))]
+
+    def coarsest(self):
+        n = min(self.log.coarsestCount, self.log.coarsestCapacity)
+        return [(self.coarse[i].initialResidual, self.coarse[i].finalResidual,
+                 self.coarse[i].nIterations) for i in range(n)]
+
+
+class Matrix:
+    """One folded matrix on a mesh's hierarchy (GamgHierarchy): Galerkin levels on the device."""
+
+    def __init__(self, mesh: Mesh, diag, upper):
+        if not _is_torch(diag):
+            diag = _as_host(diag, np.float64)
+            upper = _as_host(upper, np.float64)
+        ms = _memspace(diag, upper)
+        h = C.c_void_p()
+        _check(lib.b2g_matrix_create(mesh.handle, _ptr(diag), _ptr(upper), ms, _stream(),
+                                     C.byref(h)))
+        self.handle = h
+        self.mesh = mesh
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            lib.b2g_matrix_destroy(h)
+            self.handle = None
+
+    def level(self, level: int):
+        nc, nf = self.mesh.level_size(level)
+        d = np.empty(nc)
+        u = np.empty(nf)
+        _check(lib.b2g_matrix_get_level(self.handle, level, _ptr(d), _ptr(u)))
+        return d, u
+
+    # device pointers only below (CUDA tensors)
+    def amul(self, level, x, y):
+        _check(lib.b2g_level_amul(self.handle, level, _ptr(x), _ptr(y)))
+
+    def smooth(self, level, psi, source, n_sweeps, smoother="GaussSeidel"):
+        _check(lib.b2g_level_smooth(self.handle, level, SMOOTHERS[smoother], _ptr(psi),
+                                    _ptr(source), n_sweeps))
+
+    def scale(self, level, field, Acf, source):
+        _check(lib.b2g_level_scale(self.handle, level, _ptr(field), _ptr(Acf), _ptr(source)))
+
+    def restrict(self, step, fine, coarse):
+        _check(lib.b2g_step_restrict(self.handle, step, _ptr(fine), _ptr(coarse)))
+
+    def prolong(self, step, coarse, fine):
+        _check(lib.b2g_step_prolong(self.handle, step, _ptr(coarse), _ptr(fine)))
+
+    def norm_factor(self, level, psi, source, Apsi) -> float:
+        v = C.c_double()
+        _check(lib.b2g_level_norm_factor(self.handle, level, _ptr(psi), _ptr(source), _ptr(Apsi),
+                                         C.byref(v)))
+        return v.value
+
+    def pcg_dic(self, level, psi, source, tol, rel_tol) -> SolverPerformance:
+        p = _Perf()
+        _check(lib.b2g_level_pcg_dic(self.handle, level, _ptr(psi), _ptr(source), tol, rel_tol,
+                                     C.byref(p)))
+        return SolverPerformance(p.initialResidual, p.finalResidual, p.nIterations)
+
+    def precondition(self, controls: Controls, w, r, coarsest_cap: int = 0):
+        lb = _LogBuf(0, coarsest_cap)
+        _check(lib.b2g_precondition(self.handle, C.byref(controls), _ptr(w), _ptr(r),
+                                    C.byref(lb.log)))
+        return lb.coarsest()
+
+    def solve(self, source, psi, controls: Controls, history_cap=1000, coarsest_cap=0):
+        ms = _memspace(source, psi)
+        p = _Perf()
+        lb = _LogBuf(history_cap, coarsest_cap)
+        _check(lib.b2g_matrix_pcg_solve(self.handle, _ptr(source), _ptr(psi), C.byref(controls),
+                                        ms, C.byref(p), C.byref(lb.log)))
+        return (SolverPerformance(p.initialResidual, p.finalResidual, p.nIterations),
+                lb.history(), lb.coarsest())
+
+    def timings(self):
+        ms = (C.c_double * 4)()
+        n = C.c_longlong()
+        _check(lib.b2g_matrix_timings(self.handle, ms, C.byref(n)))
+        return list(ms), n.value
+
+
+def pcg_gamg_solve(mesh: Mesh, diag, upper, source, psi, controls: Controls | None = None,
+                   history_cap: int = 1000, coarsest_cap: int = 0):
+    """pcgGamgSolve (src/matrices/lduMatrix/solvers/GAMG/gamg_solver_cpp.cuh:217-229) on a folded
+    system. ``psi`` is updated in place (numpy or CUDA tensor). Returns (SolverPerformance,
+    residual history, coarsest-level performances)."""
+    controls = controls or controls_default()
+    if not _is_torch(diag):
+        diag = _as_host(diag, np.float64)
+        upper = _as_host(upper, np.float64)
+        source = _as_host(source, np.float64)
+    ms = _memspace(diag, upper, source, psi)
+    p = _Perf()
+    lb = _LogBuf(history_cap, coarsest_cap)
+    _check(lib.b2g_pcg_gamg_solve(mesh.handle, _ptr(diag), _ptr(upper), _ptr(source), _ptr(psi),
+                                  C.byref(controls), ms, _stream(), C.byref(p), C.byref(lb.log)))
+    return (SolverPerformance(p.initialResidual, p.finalResidual, p.nIterations), lb.history(),
+            lb.coarsest())
+
+
+def gamg_solve(mesh: Mesh, diag, upper, source, psi, controls: Controls,
+               history_cap: int = 100000):
+    """gamgSolveFolded (gamg_solver_cpp.cuh:185-192): the standalone GAMG solver."""
+    if not _is_torch(diag):
+        diag = _as_host(diag, np.float64)
+        upper = _as_host(upper, np.float64)
+        source = _as_host(source, np.float64)
+    ms = _memspace(diag, upper, source, psi)
+    p = _Perf()
+    lb = _LogBuf(history_cap, 0)
+    _check(lib.b2g_gamg_solve(mesh.handle, _ptr(diag), _ptr(upper), _ptr(source), _ptr(psi),
+                              C.byref(controls), ms, _stream(), C.byref(p), C.byref(lb.log)))
+    return SolverPerformance(p.initialResidual, p.finalResidual, p.nIterations), lb.history()

@@ -1,0 +1,260 @@
+/*
+ * brae_gamg.h -- C ABI of the B200-native GAMG-preconditioned PCG pressure solver.
+ *
+ * A drop-in for the reference's (simd-ai/brae) pressure linear solve: OpenFOAM's PCG with the GAMG
+ * preconditioner on a symmetric LDU matrix -- faceAreaPair agglomeration, GaussSeidel smoothing,
+ * restriction/prolongation, the coarsest-level PCG-DIC, lduMatrix::Amul and the normFactor / dot
+ * reductions -- all on one GPU. Plain pointers and sizes only; no C++ or torch types cross it.
+ *
+ * Citations name the reference interface each entry point replaces (paths relative to the
+ * reference project root):
+ *   GAMGH = src/matrices/lduMatrix/solvers/GAMG/gamg_solver_cpp.cuh
+ *   AGGH  = src/matrices/lduMatrix/solvers/GAMG/GAMGAgglomerations/pair_gamg_agglomeration_cpp.cuh
+ *   DGAMG = src/matrices/lduMatrix/solvers/GAMG/device_gamg_solver.cuh
+ *   PCGH  = src/OpenFOAM/matrices/pcg.cuh
+ *
+ * Conventions
+ *   - label = int32, scalar = double. The LDU addressing is OpenFOAM's: `lower` (owner) and
+ *     `upper` (neighbour) per internal face, faces sorted by owner, owner < neighbour.
+ *   - The matrix is the FOLDED symmetric system the solver receives (boundary internalCoeffs in
+ *     `diag`, boundaryCoeffs in `source`), as gamgSolveFolded takes it (GAMGH:185-192).
+ *   - `memspace` says where array arguments live: B2G_MEM_HOST (pageable or pinned host memory;
+ *     copies are made on the stream) or B2G_MEM_DEVICE (device pointers on the current device).
+ *   - `stream` is a cudaStream_t; NULL means cudaStreamPerThread, the reference's stream
+ *     (cmake/BraeCompilerOptions.cmake:9-12). Calls return after the work they describe is
+ *     complete unless stated otherwise.
+ *   - Every call returns a b2g_status; on failure b2g_last_error() gives a message naming the
+ *     refused input, as the reference's std::runtime_error messages do (gamg_solver_cpp.cu:737-766).
+ *   - Handles are not re-entrant: one host thread at a time per handle.
+ */
+#ifndef BRAE_GAMG_H
+#define BRAE_GAMG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B2G_API __attribute__((visibility("default")))
+
+typedef enum
+{
+    B2G_OK = 0,
+    B2G_ERR_ARGUMENT = 1,        /* malformed input: sizes, null pointers, addressing order */
+    B2G_ERR_REFUSED = 2,         /* an input the reference refuses by name (gamg_solver_cpp.cu:801-928) */
+    B2G_ERR_CUDA = 3,            /* a CUDA runtime error */
+    B2G_ERR_NO_MEMORY = 4,       /* device allocation failed, or a request exceeds an admission cap */
+    B2G_ERR_DEVICE_TIMEOUT = 5,  /* a bounded device-side wait gave up; the result is invalid */
+    B2G_ERR_STATE = 6            /* a handle used out of order */
+} b2g_status;
+
+enum
+{
+    B2G_MEM_HOST = 0,
+    B2G_MEM_DEVICE = 1
+};
+
+/* lduMatrix::smoother::New on a symmetric matrix, as GAMGSolver selects it (gamgSmootherPorted,
+ * GAMGH:136) */
+enum
+{
+    B2G_SMOOTHER_GAUSS_SEIDEL = 0,
+    B2G_SMOOTHER_SYM_GAUSS_SEIDEL = 1,
+    B2G_SMOOTHER_DIC = 2,
+    B2G_SMOOTHER_DIC_GAUSS_SEIDEL = 3
+};
+
+enum
+{
+    B2G_PRECISION_FP64 = 0,        /* the parity form: everything in FP64 */
+    B2G_PRECISION_FP32_PRECOND = 1 /* FP64 outer PCG, FP32 V-cycle, flexible (Polak-Ribiere) beta */
+};
+
+/* The solver entry's controls: PCG's tolerance/relTol/maxIter/minIter (lduMatrixSolver.C:195-205
+ * via inter_case_cpp.cu:1519-1572) and the `preconditioner { preconditioner GAMG; ... }`
+ * sub-dictionary's GamgControls + nVcycles (GAMGH:67-85, :128-132). Defaults: b2g_controls_default. */
+enum
+{
+    B2G_SOLVER_PCG_GAMG = 0,       /* solver PCG; preconditioner { preconditioner GAMG; ... } */
+    B2G_SOLVER_GAMG = 1            /* solver GAMG; (the standalone GAMGSolver) */
+};
+
+typedef struct
+{
+    int solver;                  /* B2G_SOLVER_PCG_GAMG */
+    /* PCG (the solver entry); for solver GAMG, the GAMG entry's own */
+    double tolerance;            /* 1e-6 */
+    double relTol;               /* 0 */
+    int maxIter;                 /* 1000 */
+    int minIter;                 /* 0 */
+    /* GAMG preconditioner (its own dictionary) */
+    int smoother;                /* mandatory in the dictionary; GaussSeidel here */
+    double precTolerance;        /* 1e-6: the coarsest-level PCG-DIC stops on these two */
+    double precRelTol;           /* 0 */
+    int nPreSweeps;              /* 0 */
+    int preSweepsLevelMultiplier;/* 1 */
+    int maxPreSweeps;            /* 4 */
+    int nPostSweeps;             /* 2 */
+    int postSweepsLevelMultiplier;/* 1 */
+    int maxPostSweeps;           /* 4 */
+    int nFinestSweeps;           /* 2 */
+    int scaleCorrection;         /* 1 (the matrix is symmetric) */
+    int nCellsInCoarsestLevel;   /* 10 */
+    int nVcycles;                /* 2 (GAMGPreconditioner.C:60) */
+    int precision;               /* B2G_PRECISION_FP64 */
+} b2g_controls;
+
+/* SolverPerformance (PCGH:16-21) */
+typedef struct
+{
+    double initialResidual;
+    double finalResidual;
+    int nIterations;
+} b2g_perf;
+
+/* Optional per-solve record. `history[k]` = the normalised residual after PCG iteration k;
+ * `coarsest` = the coarsest-level PCG-DIC performance of every V-cycle, as GamgSolveLog holds it
+ * (GAMGH:147-150). The caller owns the arrays and states their capacities; counts are written back
+ * (they may exceed the capacities, in which case only the first entries are stored). */
+typedef struct
+{
+    double* history;
+    int historyCapacity;
+    int historyCount;
+    b2g_perf* coarsest;
+    int coarsestCapacity;
+    int coarsestCount;
+} b2g_solve_log;
+
+typedef struct b2g_mesh b2g_mesh;     /* a mesh's GAMG hierarchy (GamgAgglomerationCache) */
+typedef struct b2g_matrix b2g_matrix; /* one matrix on that hierarchy (GamgHierarchy) */
+
+/* ---- errors and controls -------------------------------------------------------------------- */
+
+/* The message of the last failed call on this thread ("" if none). */
+B2G_API const char* b2g_last_error(void);
+
+/* GAMGSolver.C's and lduMatrix::solver's defaults, with smoother GaussSeidel. */
+B2G_API b2g_status b2g_controls_default(b2g_controls* out);
+
+/* Reads one fvSolution solver entry -- the text between (and excluding) its braces, e.g.
+ * "solver PCG; tolerance 1e-6; relTol 0; preconditioner { preconditioner GAMG; smoother
+ * GaussSeidel; nCellsInCoarsestLevel 10; }" -- into controls, refusing by name every key the
+ * reference refuses: a solver other than PCG, a preconditioner other than GAMG, an unported or
+ * asymmetric-only smoother, agglomerator != faceAreaPair, mergeLevels != 1, updateInterval != 1,
+ * cacheAgglomeration no, interpolateCorrection, directSolveCoarsest, a coarsestLevelCorr
+ * sub-dictionary, processorAgglomerator. Replaces readGamgControls (GAMGH:139-144) and the PCG keys
+ * of inter_case_cpp.cu:1519-1572. */
+B2G_API b2g_status b2g_controls_read(const char* entryText, b2g_controls* out);
+
+/* ---- the hierarchy (once per mesh) ---------------------------------------------------------- */
+
+/* Builds the faceAreaPair agglomeration of a mesh on the device: face weights, the alternating
+ * greedy pairing, the coarse addressing numbered owner-major by first appearance, face restrict
+ * and flip maps, restricted weights -- bit-for-bit the reference's hierarchy.
+ * Replaces faceAreaPairGamgAgglomeration (AGGH:99-105) behind GamgAgglomerationCache::get
+ * (GAMGH:110-122) and its device upload DeviceGamgCache::get (DGAMG:109-127).
+ * `Sf` is [nFaces][3], `magSf` [nFaces]. `forwardInOut` is the pairing direction flag OpenFOAM
+ * keeps as a static (pairGAMGAgglomeration::forward_): read on entry, written back as the build
+ * leaves it. Arrays are read from `memspace`; the handle keeps device copies. */
+B2G_API b2g_status b2g_mesh_create(int nCells, int nFaces, const int32_t* lower,
+                                   const int32_t* upper, const double* Sf, const double* magSf,
+                                   int nCellsInCoarsestLevel, int* forwardInOut, int memspace,
+                                   void* stream, b2g_mesh** out);
+B2G_API b2g_status b2g_mesh_destroy(b2g_mesh* mesh);
+
+/* Number of coarse levels (GamgAgglomeration::size(), AGGH:76-79). */
+B2G_API b2g_status b2g_mesh_levels(const b2g_mesh* mesh, int* nLevels);
+/* Cells and faces of level `level` (0 = the mesh, 1..nLevels = coarse levels). */
+B2G_API b2g_status b2g_mesh_level_size(const b2g_mesh* mesh, int level, int* nCells,
+                                       int* nFaces);
+/* Copies step `step` (level step -> step+1) to HOST arrays, any of which may be NULL:
+ * restrictAddressing [nCells(step)], faceRestrictAddressing [nFaces(step)], faceFlipMap
+ * [nFaces(step)], coarse lower/upper [nFaces(step+1)] (AGGH:69-75). */
+B2G_API b2g_status b2g_mesh_get_step(const b2g_mesh* mesh, int step, int32_t* restrictAddr,
+                                     int32_t* faceRestrict, int8_t* flip, int32_t* coarseLower,
+                                     int32_t* coarseUpper);
+/* Milliseconds of device time the hierarchy build took (agglomeration plus the per-level
+ * schedules), measured with events on the build stream. */
+B2G_API b2g_status b2g_mesh_build_ms(const b2g_mesh* mesh, float* ms);
+
+/* ---- the solve ------------------------------------------------------------------------------ */
+
+/* PCG::scalarSolve with the GAMG preconditioner on a folded system: psi (initial guess honoured)
+ * is overwritten with the solution; `out` receives the SolverPerformance. The preconditioner is
+ * built only when the initial residual has not already converged (PCG.C:111-118).
+ * Replaces pcgGamgSolve (GAMGH:217-229) and devicePcgGamgSolve (DGAMG:143-154).
+ * `diag`, `source`, `psi` are [nCells], `upper` is [nFaces] (lower == upper). `log` may be NULL. */
+B2G_API b2g_status b2g_pcg_gamg_solve(b2g_mesh* mesh, const double* diag, const double* upper,
+                                      const double* source, double* psi,
+                                      const b2g_controls* controls, int memspace, void* stream,
+                                      b2g_perf* out, b2g_solve_log* log);
+
+/* GAMGSolver::solve on a folded system: the standalone GAMG solver (V-cycles until converged).
+ * Replaces gamgSolveFolded (GAMGH:185-192) and deviceGamgSolve. The GAMG tolerance, relTol,
+ * maxIter and minIter are controls->tolerance/relTol/maxIter/minIter. */
+B2G_API b2g_status b2g_gamg_solve(b2g_mesh* mesh, const double* diag, const double* upper,
+                                  const double* source, double* psi,
+                                  const b2g_controls* controls, int memspace, void* stream,
+                                  b2g_perf* out, b2g_solve_log* log);
+
+/* ---- one matrix on the hierarchy: the pieces, for callers that drive them (and for tests) ---- */
+
+/* GamgHierarchy::build (gamg_solver_cpp.cu:565-623): uploads the folded fine matrix and builds
+ * every coarse matrix by Galerkin summation in the reference's order (agglomerateMatrix,
+ * gamg_solver_cpp.cu:474-526), plus the per-level coefficient layouts the kernels read. */
+B2G_API b2g_status b2g_matrix_create(b2g_mesh* mesh, const double* diag, const double* upper,
+                                     int memspace, void* stream, b2g_matrix** out);
+B2G_API b2g_status b2g_matrix_destroy(b2g_matrix* m);
+/* Copies level `level`'s diag [nCells] and upper [nFaces] to HOST arrays. */
+B2G_API b2g_status b2g_matrix_get_level(const b2g_matrix* m, int level, double* diag,
+                                        double* upper);
+
+/* The following take DEVICE pointers sized for level `level` and run on the matrix's stream. */
+
+/* lduMatrix::Amul (gamg_solver_cpp.cu:62-88): y = A x, bit-for-bit the reference's order. */
+B2G_API b2g_status b2g_level_amul(b2g_matrix* m, int level, const double* x, double* y);
+/* Smoother::smooth (gamg_solver_cpp.cu:262-316) with `smoother` B2G_SMOOTHER_*: nSweeps sweeps of
+ * psi against source, in the sequential sweep order bit for bit. */
+B2G_API b2g_status b2g_level_smooth(b2g_matrix* m, int level, int smoother, double* psi,
+                                    const double* source, int nSweeps);
+/* GAMGSolver::scale (gamg_solver_cpp.cu:386-407); Acf is scratch [nCells]. */
+B2G_API b2g_status b2g_level_scale(b2g_matrix* m, int level, double* field, double* Acf,
+                                   const double* source);
+/* restrictField / prolongField across step `step` (gamg_solver_cpp.cu:410-432). */
+B2G_API b2g_status b2g_step_restrict(b2g_matrix* m, int step, const double* fine, double* coarse);
+B2G_API b2g_status b2g_step_prolong(b2g_matrix* m, int step, const double* coarse, double* fine);
+/* lduMatrix::solver::normFactor (gamg_solver_cpp.cu:119-159), written to *nf (host). */
+B2G_API b2g_status b2g_level_norm_factor(b2g_matrix* m, int level, const double* psi,
+                                         const double* source, const double* Apsi, double* nf);
+/* The coarsest-level PCG-DIC (gamg_solver_cpp.cu:321-383) on level `level` from psi. */
+B2G_API b2g_status b2g_level_pcg_dic(b2g_matrix* m, int level, double* psi, const double* source,
+                                     double tolerance, double relTol, b2g_perf* out);
+/* GAMGPreconditioner::precondition (gamg_solver_cpp.cu:1089-1107): w = M^-1 r, nVcycles V-cycles
+ * from zero. `log` (may be NULL) receives the coarsest-level performances. */
+B2G_API b2g_status b2g_precondition(b2g_matrix* m, const b2g_controls* controls, double* w,
+                                    const double* r, b2g_solve_log* log);
+/* The PCG solve on an existing matrix (the same as b2g_pcg_gamg_solve after b2g_matrix_create),
+ * with source and psi in `memspace`. */
+B2G_API b2g_status b2g_matrix_pcg_solve(b2g_matrix* m, const double* source, double* psi,
+                                        const b2g_controls* controls, int memspace,
+                                        b2g_perf* out, b2g_solve_log* log);
+
+/* ---- introspection ---------------------------------------------------------------------------- */
+
+/* Device-time of the kernels of the last solve on `m`, by class (milliseconds), and the number of
+ * kernel launches: [0] Amul on the finest level, [1] Gauss-Seidel on the finest level, [2] all
+ * coarse-level work, [3] the whole solve. Timed with events only when b2g_set_profiling(1). */
+B2G_API b2g_status b2g_matrix_timings(const b2g_matrix* m, double* ms4, long long* launches);
+B2G_API b2g_status b2g_set_profiling(int on);
+
+/* Library version string. */
+B2G_API const char* b2g_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BRAE_GAMG_H */
