@@ -1,0 +1,358 @@
+"""Benchmark: the 20M-cell pressure solve (GAMG-preconditioned PCG on OpenFOAM's LDU matrix).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 272]
+
+Workload (one step = one pressure solve, psi from zero): a 272^3 hex box, 2 x 1 x 1 m, graded 20:1
+toward y = 0 and y = 1, fixedValue outlet at x = 2, seeded face-flux source (brae_b200.cases), plain
+FP64 PCG + GAMG(GaussSeidel, 0/2, nCellsInCoarsestLevel 10), tolerance 1e-6, relTol 0.05,
+maxIter 1000. The hierarchy is built once per mesh and timed apart ("mesh_build_s"). The same
+mesh with the 1000:1 two-phase coefficient is then solved in plain FP64 and in the FP32-
+preconditioned form; their times, final residuals and field error are reported beside it.
+
+`value` is seconds per solve with every input resident in HBM (max over ranks); `e2e` is the same
+solve through the C ABI with host (pinned) buffers, copies in the timed region. N > 1 runs N
+independent replicas, one per GPU (the solve does not shard). `--impl reference` times the
+reference's own CPU implementation (oracle/_ref, else the oracle port) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "20M-cell p-solve s, FP32-precond vs FP64 at equal residual; served p50/p99 latency"
+TOL, REL_TOL, MAX_ITER = 1e-6, 0.05, 1000
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_launch(kernel: str, workload: str):
+    """DRAM bytes per launch from a committed ncu summary (profiles/traffic.json), or None."""
+    p = os.path.join(HERE, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    v = d.get(workload, {}).get(kernel)
+    return None if v is None else float(v)
+
+
+def cpu_reference_solve(case, tag):
+    """The reference's own host path (oracle/_ref) if built, else the oracle port: (seconds per
+    solve, kind, perf, psi, build seconds). Single-threaded."""
+    from oracle.bindings import REF_SO, Oracle, Reference
+    if os.path.exists(REF_SO):
+        impl, kind = Reference(), "reference"
+    else:
+        impl, kind = Oracle(), "port"
+    t0 = time.perf_counter()
+    agg = impl.agglomerate(case.lower, case.upper, case.Sf, case.magSf, case.n_cells, 10, True)
+    tb = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    out = impl.pcg_gamg_solve(agg, case.diag, case.coef, case.source, np.zeros(case.n_cells), TOL,
+                              REL_TOL, MAX_ITER)
+    ts = time.perf_counter() - t0
+    return ts, kind, out["perf"], out["psi"], tb
+
+
+def run_reference(args, world, rank):
+    from brae_b200 import cases
+    if rank != 0:
+        return
+    case = cases.graded_channel(args.n)
+    from oracle.bindings import REF_SO, Oracle, Reference
+    impl, kind = (Reference(), "reference") if os.path.exists(REF_SO) else (Oracle(), "port")
+    agg = impl.agglomerate(case.lower, case.upper, case.Sf, case.magSf, case.n_cells, 10, True)
+    steps = max(1, min(args.steps, 3))
+    warm = 0
+    times = []
+    perf = None
+    for k in range(warm + steps):
+        t0 = time.perf_counter()
+        out = impl.pcg_gamg_solve(agg, case.diag, case.coef, case.source, np.zeros(case.n_cells),
+                                  TOL, REL_TOL, MAX_ITER)
+        dt = time.perf_counter() - t0
+        perf = out["perf"]
+        if k >= warm:
+            times.append(dt)
+    v = float(np.mean(times))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": world,
+        "steps": steps, "warmup": warm, "ms_per_step": v * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"graded_channel_{args.n}^3 FP64 PCG+GAMG tol 1e-6 relTol 0.05",
+                   "cells": case.n_cells, "faces": case.n_faces, "solver_perf": list(perf)},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": kind,
+                         "sample": f"full {args.n}^3 solve from psi = 0 (hierarchy built once, untimed)"},
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    import brae_b200.native as b2g
+    from brae_b200 import cases
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    case = cases.graded_channel(args.n)
+    td = lambda a, dt=torch.float64: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)
+    t0 = time.perf_counter()
+    mesh = b2g.Mesh(td(case.lower, torch.int32), td(case.upper, torch.int32), td(case.Sf.reshape(-1)),
+                    td(case.magSf), case.n_cells, 10, True)
+    build_wall = time.perf_counter() - t0
+    A = b2g.Matrix(mesh, td(case.diag), td(case.coef))
+    src = td(case.source)
+    psi = torch.zeros(case.n_cells, dtype=torch.float64, device=dev)
+    ctl = b2g.controls_default(tolerance=TOL, relTol=REL_TOL, maxIter=MAX_ITER)
+    for _ in range(args.warmup):
+        psi.zero_()
+        A.solve(src, psi, ctl, history_cap=0)
+    b2g.set_profiling(True)
+    ms_acc = np.zeros(4)
+    cnt_acc = np.zeros(4)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        e0.record(stream)
+        perf = None
+        for _ in range(args.steps):
+            psi.zero_()
+            perf, _, _ = A.solve(src, psi, ctl, history_cap=0)
+            ms, cnt = A.timings()
+            ms_acc += ms
+            cnt_acc += cnt
+        e1.record(stream)
+        torch.cuda.synchronize()
+    b2g.set_profiling(False)
+    elapsed = barrier_max(e0.elapsed_time(e1) / 1e3, world)
+    per_solve = elapsed / args.steps
+    psi64 = psi.cpu().numpy()
+
+    # end to end: the reference-facing call with pinned host buffers, copies inside the timed region
+    pin = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).pin_memory()
+    h_diag, h_up, h_src = pin(case.diag), pin(case.coef), pin(case.source)
+    h_psi = torch.zeros(case.n_cells, dtype=torch.float64).pin_memory()
+    ctl2 = b2g.controls_default(tolerance=TOL, relTol=REL_TOL, maxIter=MAX_ITER)
+    e2e_steps = max(1, min(args.steps, 3))
+    b2g.pcg_gamg_solve(mesh, h_diag.numpy(), h_up.numpy(), h_src.numpy(), h_psi.numpy(), ctl2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        h_psi.zero_()
+        b2g.pcg_gamg_solve(mesh, h_diag.numpy(), h_up.numpy(), h_src.numpy(), h_psi.numpy(), ctl2)
+    torch.cuda.synchronize()
+    e2e = barrier_max((time.perf_counter() - t0) / e2e_steps, world)
+    h2d = 8 * (3 * case.n_cells + case.n_faces)
+    d2h = 8 * case.n_cells
+    del h_diag, h_up, h_src
+
+    # the precision form on the two-phase (1000:1) coefficient, same mesh and hierarchy
+    tp = cases.graded_channel(args.n, two_phase=True)
+    A2 = b2g.Matrix(mesh, td(tp.diag), td(tp.coef))
+    src2 = td(tp.source)
+    forms = {}
+    for name, prec in (("fp64", 0), ("fp32_precond", 1)):
+        c2 = b2g.controls_default(tolerance=TOL, relTol=REL_TOL, maxIter=MAX_ITER, precision=prec)
+        x = torch.zeros(case.n_cells, dtype=torch.float64, device=dev)
+        A2.solve(src2, x, c2, history_cap=0)
+        ts = []
+        for _ in range(max(1, min(args.steps, 3))):
+            x.zero_()
+            torch.cuda.synchronize()
+            a0 = torch.cuda.Event(enable_timing=True)
+            a1 = torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            p2, _, _ = A2.solve(src2, x, c2, history_cap=0)
+            a1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(a0.elapsed_time(a1) / 1e3)
+        forms[name] = dict(s=barrier_max(float(np.mean(ts)), world), perf=list(p2), psi=x.cpu().numpy())
+    ref_x = forms["fp64"]["psi"]
+    field_err = float(np.abs(forms["fp32_precond"]["psi"] - ref_x).max() / np.abs(ref_x).max())
+
+    # roofline of the dominant kernel: the finest level's Gauss-Seidel sweep (its share is below)
+    peak, peak_kind = measured_peaks()
+    n, nf = case.n_cells, case.n_faces
+    gs_launches = max(cnt_acc[1], 1)
+    gs_ms = ms_acc[1] / gs_launches
+    amul_ms = ms_acc[0] / max(cnt_acc[0], 1)
+    gs_bytes = 32 * n + 16 * nf       # diag, b, psi read + write; upper; two labels
+    amul_bytes = 24 * n + 16 * nf     # diag, x, y; upper; two labels
+    gs_gbs = gs_bytes / (gs_ms * 1e-3) / 1e9
+    amul_gbs = amul_bytes / (amul_ms * 1e-3) / 1e9
+    traffic = traffic_per_launch("gsSweep", f"graded_channel_{args.n}")
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        ts, kind, cperf, cpsi, tb = cpu_reference_solve(case, "fp64")
+        cpu = {"value": ts, "unit": "s", "cores": 1, "kind": kind,
+               "sample": f"one full {args.n}^3 FP64 solve from psi = 0 on one host core "
+                         f"(hierarchy built once, {tb:.1f} s, untimed)",
+               "iterations": cperf[2], "final_residual": cperf[1],
+               "field_rel_diff_vs_gpu": float(np.abs(cpsi - psi64).max() / np.abs(cpsi).max())}
+
+    line = {
+        "metric": METRIC, "value": per_solve, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": per_solve * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {
+            "workload": f"graded_channel_{args.n}^3: FP64 PCG+GAMG(GaussSeidel) tol 1e-6 relTol 0.05",
+            "cells": n, "faces": nf, "levels": mesh.n_levels, "solver_perf": list(perf),
+            "mesh_build_s": mesh.build_ms / 1e3, "mesh_build_wall_s": build_wall,
+            "l2": "inputs larger than L2 (the 20M-cell system is ~2.5 GB)",
+            "parallelism": f"replicas x{world} (one independent solve per GPU)",
+        },
+        "precision_form": {
+            "workload": f"graded_channel_{args.n}^3 two-phase 1000:1, tol 1e-6 relTol 0.05",
+            "fp64_s": forms["fp64"]["s"], "fp32_precond_s": forms["fp32_precond"]["s"],
+            "speedup": forms["fp64"]["s"] / forms["fp32_precond"]["s"],
+            "fp64_perf": forms["fp64"]["perf"], "fp32_precond_perf": forms["fp32_precond"]["perf"],
+            "field_rel_err_vs_fp64": field_err,
+        },
+        "kernels": {
+            "gs_finest_us_per_launch": gs_ms * 1e3, "gs_finest_launches": int(cnt_acc[1]),
+            "gs_finest_share": float(ms_acc[1] / ms_acc[3]),
+            "amul_finest_us_per_launch": amul_ms * 1e3, "amul_finest_gbs": amul_gbs,
+            "amul_finest_share": float(ms_acc[0] / ms_acc[3]),
+        },
+        "roofline": {"kernel": "gsSweep (finest level, one sweep)", "bound": "hbm",
+                     "achieved": gs_gbs, "peak": peak, "unit": "GB/s", "frac": gs_gbs / peak,
+                     "traffic": traffic, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": gs_bytes},
+        "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(cnt_acc[3]),
+        "clocks": clocks.summary(),
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=272)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

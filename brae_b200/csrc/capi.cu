@@ -284,6 +284,7 @@ b2g_status b2g_controls_default(b2g_controls* out)
         c.nCellsInCoarsestLevel = 10;
         c.nVcycles = 2;
         c.precision = B2G_PRECISION_FP64;
+        c.reduction = B2G_REDUCTION_TREE;
         *out = c;
     });
 }
@@ -506,10 +507,32 @@ b2g_status b2g_level_smooth(b2g_matrix* m, int level, int smoother, double* psi,
     });
 }
 
+b2g_status b2g_level_smooth_trace(b2g_matrix* m, int level, double* psi, const double* source,
+                                  unsigned long long* trace, int traceCapacity, int* schedule)
+{
+    return guarded([&] {
+        need(m && psi && source, "b2g_level_smooth_trace: null argument");
+        need(level >= 0 && level <= m->mat->nLevels(), "b2g_level_smooth_trace: level out of range");
+        const b2g::GsSchedule& G = m->mat->mesh->lev[level].gs;
+        if (schedule)
+        {
+            schedule[0] = G.nParts;
+            schedule[1] = G.nChunks;
+            schedule[2] = G.maxCells;
+            schedule[3] = G.maxEnt;
+            schedule[4] = G.maxDepth;
+        }
+        need(trace == nullptr || traceCapacity >= 4 * (G.nChunks + G.nParts), "b2g_level_smooth_trace: trace too small");
+        m->mat->smooth<double>(level, B2G_SMOOTHER_GAUSS_SEIDEL, psi, source, 1, trace);
+        m->mat->checkDeviceError();
+    });
+}
+
 b2g_status b2g_level_scale(b2g_matrix* m, int level, double* field, double* Acf, const double* source)
 {
     return guarded([&] {
         need(m && field && Acf && source, "b2g_level_scale: null argument");
+        m->mat->serial = false;
         need(level >= 0 && level <= m->mat->nLevels(), "b2g_level_scale: level out of range");
         m->mat->scale<double>(level, field, Acf, source);
         B2G_CUDA(cudaStreamSynchronize(m->mat->stream));
@@ -574,6 +597,7 @@ b2g_status b2g_precondition(b2g_matrix* m, const b2g_controls* controls, double*
         b2g::Matrix& A = *m->mat;
         need(A.nLevels() > 0, "b2g_precondition: the mesh has no coarse levels");
         A.resetLog(log ? std::max(log->coarsestCapacity, 0) : 0);
+        A.serial = controls->reduction == B2G_REDUCTION_SERIAL;
         A.precondition(*controls, w, r);
         A.checkDeviceError();
         A.readLog(log);
@@ -630,13 +654,15 @@ b2g_status b2g_gamg_solve(b2g_mesh* mesh, const double* diag, const double* uppe
     });
 }
 
-b2g_status b2g_matrix_timings(const b2g_matrix* m, double* ms4, long long* launches)
+b2g_status b2g_matrix_timings(const b2g_matrix* m, double* ms4, long long* counts4)
 {
     return guarded([&] {
         need(m != nullptr, "b2g_matrix_timings: null matrix");
-        if (ms4)
-            for (int i = 0; i < 4; ++i) ms4[i] = m->mat->ms[i];
-        if (launches) *launches = m->mat->launches;
+        for (int i = 0; i < 4; ++i)
+        {
+            if (ms4) ms4[i] = m->mat->ms[i];
+            if (counts4) counts4[i] = m->mat->counts[i];
+        }
     });
 }
 

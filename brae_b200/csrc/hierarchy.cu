@@ -15,6 +15,7 @@
 // The coarse numbering (order of pair creation in visit order, singletons after, the backward
 // renumbering c -> n-1-c) is then a prefix sum over visit order.
 #include "hierarchy.cuh"
+#include "gs_kernels.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
@@ -449,14 +450,6 @@ __global__ void kLevelInfo(int n, int stride, const unsigned* __restrict__ keys,
     lvlPart[L] = static_cast<int>(keys[i] / static_cast<unsigned>(stride));
 }
 
-// lvlIncl is the inclusive scan of level heads: position i holds local level lvlIncl[i] - 1
-__global__ void kPosLevel(int n, const int* __restrict__ order, const int* __restrict__ lvlIncl,
-                          int* __restrict__ lvlOfCell)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) lvlOfCell[order[i]] = lvlIncl[i] - 1;
-}
-
 // part boundaries: part p starts at the first cell whose cumulative cost (cells + row entries)
 // reaches total*p/P
 __global__ void kPartBounds(int n, int P, const int* __restrict__ rowStart, int* __restrict__ partStart)
@@ -476,36 +469,103 @@ __global__ void kPartBounds(int n, int P, const int* __restrict__ rowStart, int*
     partStart[p] = lo;
 }
 
-__global__ void kNeeds(int n, int nParts, const int* __restrict__ partOf, const int* __restrict__ depth,
-                       const int* __restrict__ lvlOfCell, const int* __restrict__ losortStart,
-                       const int* __restrict__ losort, const int* __restrict__ lower,
-                       const int* __restrict__ ownStart, const int* __restrict__ upper,
-                       int* __restrict__ needUp, int* __restrict__ needDown, unsigned* __restrict__ upBits,
-                       unsigned* __restrict__ downBits, int words)
+__global__ void kChunkRecs(int nCh, const int* __restrict__ chunkStart, const int* __restrict__ posRow,
+                           const int* __restrict__ chunkDepth, const int* __restrict__ chunkNeedUp,
+                           int* __restrict__ rec)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n) return;
-    const int p = partOf[c];
-    const int L = lvlOfCell[c];
-    for (int q = losortStart[c]; q < losortStart[c + 1]; ++q)
+    if (c >= nCh) return;
+    const int p0 = chunkStart[c];
+    const int p1 = chunkStart[c + 1];
+    int* r = rec + 8 * (size_t)c;
+    r[0] = p0;
+    r[1] = p1 - p0;
+    r[2] = posRow[p0];
+    r[3] = posRow[p1] - posRow[p0];
+    r[4] = chunkDepth[c];
+    r[5] = chunkNeedUp[c];
+    r[6] = 0;
+    r[7] = 0;
+}
+
+__global__ void kPosOf(int n, const int* __restrict__ order, int* __restrict__ posOf)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) posOf[order[i]] = i;
+}
+
+__global__ void kPosRowLen(int n, const int* __restrict__ order, const int* __restrict__ rowStart,
+                           int* __restrict__ len)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) len[i] = rowStart[order[i] + 1] - rowStart[order[i]];
+}
+
+__global__ void kChunkOfPos(int n, int nChunks, const int* __restrict__ chunkStart, int* __restrict__ chunkOf)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int lo = 0, hi = nChunks - 1;
+    while (lo < hi)
     {
-        const int o = lower[losort[q]];
-        const int po = partOf[o];
-        if (po != p)
-        {
-            atomicMax(&needUp[L], depth[o]);
-            atomicOr(&upBits[(size_t)p * words + (po >> 5)], 1u << (po & 31));
-        }
+        const int mid = (lo + hi + 1) >> 1;
+        if (chunkStart[mid] <= i) lo = mid; else hi = mid - 1;
     }
-    for (int f = ownStart[c]; f < ownStart[c + 1]; ++f)
+    chunkOf[i] = lo;
+}
+
+// entry codes in position order: RING (an owner this part computed within the ring window),
+// PRE (final before the chunk's stage is issued: every upper neighbour, and owners of this part two
+// or more chunks back), LATE (owners of other parts, and the rare far owner one chunk back)
+__global__ void kEntryCodes(int n, int ring, const int* __restrict__ order, const int* __restrict__ posOf,
+                            const int* __restrict__ partOf, const int* __restrict__ depth,
+                            const int* __restrict__ chunkOf, const int* __restrict__ chunkStart,
+                            const int* __restrict__ posRow, const int* __restrict__ rowStart,
+                            const int* __restrict__ losortStart, const int* __restrict__ col,
+                            const int* __restrict__ entFace, unsigned* __restrict__ entCode,
+                            int* __restrict__ entFacePos, int* __restrict__ chunkNeedUp,
+                            unsigned* __restrict__ upBits, int words)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int c = order[i];
+    const int p = partOf[c];
+    const int d = depth[c];
+    const int ch = chunkOf[i];
+    const int chEnd = chunkStart[ch + 1];
+    const int rb = rowStart[c];
+    const int nLower = losortStart[c + 1] - losortStart[c];
+    const int base = posRow[i];
+    for (int e = rb; e < rowStart[c + 1]; ++e)
     {
-        const int nb = upper[f];
-        const int pn = partOf[nb];
-        if (pn != p)
+        const int k = e - rb;
+        const int o = col[e];
+        unsigned code;
+        if (k < nLower)
         {
-            atomicMax(&needDown[L], depth[nb]);
-            atomicOr(&downBits[(size_t)p * words + (pn >> 5)], 1u << (pn & 31));
+            if (partOf[o] == p)
+            {
+                // the owner's chunk precedes this one; its stage is issued one chunk ahead, so
+                // the owner may be prefetched only when it sits two or more chunks back
+                const int q = posOf[o];
+                if (chEnd - q <= ring) code = (0u << 30) | static_cast<unsigned>(q & (ring - 1));
+                else if (chunkOf[q] <= ch - 2) code = (1u << 30) | static_cast<unsigned>(o);
+                else code = (2u << 30) | static_cast<unsigned>(o);
+            }
+            else
+            {
+                code = (2u << 30) | static_cast<unsigned>(o);
+                atomicMax(&chunkNeedUp[ch], depth[o]);
+                const int po = partOf[o];
+                atomicOr(&upBits[(size_t)p * words + (po >> 5)], 1u << (po & 31));
+            }
         }
+        else
+        {
+            code = (1u << 30) | static_cast<unsigned>(o);
+        }
+        entCode[base + k] = code;
+        entFacePos[base + k] = entFace[e];
     }
 }
 
@@ -869,14 +929,15 @@ void buildGsSchedule(LevelAddr& L, cudaStream_t s)
         if (done != n) fail(B2G_ERR_STATE, "b2g: the Gauss-Seidel dependency graph has a cycle.");
         G.maxDepth = round - 1;
     }
-    // parts: contiguous cell ranges balanced by row length; enough of them to fill the GPU when
-    // a depth holds many cells, one when the level is narrow (a single CTA then walks it)
+    // parts: contiguous cell ranges balanced by row length; enough of them to fill the GPU when a
+    // depth holds many cells, one when the level is narrow (a single CTA then walks it)
     const int depthCount = G.maxDepth + 1;
     const long long avgPerDepth = (static_cast<long long>(n) + depthCount - 1) / depthCount;
     const int nSM = DeviceInfo::get().numSMs;
     int P = static_cast<int>(std::min<long long>(nSM, std::max<long long>(1, avgPerDepth / 128)));
     if (n < 4096) P = 1;
     G.nParts = P;
+    if (n >= (1 << 30)) fail(B2G_ERR_ARGUMENT, "b2g: a level of 2^30 cells or more does not fit the sweep's codes.");
     DBuf<int> dPartStart, partOf;
     dPartStart.alloc(P + 1, s);
     kPartBounds<<<grid(P + 1), TPB, 0, s>>>(n, P, L.rowStart.p, dPartStart.p);
@@ -893,73 +954,111 @@ void buildGsSchedule(LevelAddr& L, cudaStream_t s)
     kSchedKeys<<<grid(n), TPB, 0, s>>>(n, stride, partOf.p, G.depth.p, keys.p);
     kIota<<<grid(n), TPB, 0, s>>>(iota.p, n);
     B2G_LAUNCH_CHECK();
-    G.order.alloc(n, s);
-    sortPairs(keys.p, skeys.p, iota.p, G.order.p, n, bitsFor(static_cast<long long>(P) * stride), s);
+    G.posCell.alloc(n, s);
+    sortPairs(keys.p, skeys.p, iota.p, G.posCell.p, n, bitsFor(static_cast<long long>(P) * stride), s);
+    // (part, depth) groups
     DBuf<int> head, lvlScan;
     head.alloc(n, s);
     lvlScan.alloc(n + 1, s);
     kKeyHeads<<<grid(n), TPB, 0, s>>>(n, skeys.p, head.p);
     B2G_LAUNCH_CHECK();
     const int nLvl = static_cast<int>(exclusiveScan(head.p, lvlScan.p, n, s));
-    G.nLocalLevels = nLvl;
-    G.lvlStart.alloc(nLvl + 1, s);
-    G.lvlDepth.alloc(nLvl, s);
-    DBuf<int> lvlPart;
+    DBuf<int> lvlStart, lvlDepth, lvlPart;
+    lvlStart.alloc(nLvl, s);
+    lvlDepth.alloc(nLvl, s);
     lvlPart.alloc(nLvl, s);
-    kLevelInfo<<<grid(n), TPB, 0, s>>>(n, stride, skeys.p, head.p, lvlScan.p, G.lvlStart.p, G.lvlDepth.p,
-                                       lvlPart.p);
-    B2G_CUDA(cudaMemcpyAsync(G.lvlStart.p + nLvl, &n, sizeof(int), cudaMemcpyHostToDevice, s));
-    B2G_CUDA(cudaStreamSynchronize(s));
-    // level of every cell: inclusive scan of heads minus one, at the cell's position
-    DBuf<int> lvlOfCell;
-    lvlOfCell.alloc(n, s);
-    kPosLevel<<<grid(n), TPB, 0, s>>>(n, G.order.p, lvlScan.p + 1, lvlOfCell.p);
+    kLevelInfo<<<grid(n), TPB, 0, s>>>(n, stride, skeys.p, head.p, lvlScan.p, lvlStart.p, lvlDepth.p, lvlPart.p);
     B2G_LAUNCH_CHECK();
-    G.lvlNeedUp.alloc(nLvl, s);
-    G.lvlNeedDown.alloc(nLvl, s);
-    kFillInt<<<grid(nLvl), TPB, 0, s>>>(G.lvlNeedUp.p, nLvl, -1);
-    kFillInt<<<grid(nLvl), TPB, 0, s>>>(G.lvlNeedDown.p, nLvl, -1);
+    // row layout in position order
+    DBuf<int> posOf, rowLen;
+    posOf.alloc(n, s);
+    rowLen.alloc(n, s);
+    kPosOf<<<grid(n), TPB, 0, s>>>(n, G.posCell.p, posOf.p);
+    kPosRowLen<<<grid(n), TPB, 0, s>>>(n, G.posCell.p, L.rowStart.p, rowLen.p);
+    B2G_LAUNCH_CHECK();
+    G.posRow.alloc(n + 1, s);
+    exclusiveScan(rowLen.p, G.posRow.p, n, s);
+    // chunks: cut each group by cells and entries so a chunk's stage fits in shared memory
+    const std::vector<int> hLvlStart = lvlStart.download(s);
+    const std::vector<int> hLvlDepth = lvlDepth.download(s);
+    const std::vector<int> hLvlPart = lvlPart.download(s);
+    const std::vector<int> hPosRow = G.posRow.download(s);
+    int maxGroup = 0, maxRow = 0;
+    for (int g = 0; g < nLvl; ++g)
+        maxGroup = std::max(maxGroup, (g + 1 < nLvl ? hLvlStart[g + 1] : n) - hLvlStart[g]);
+    for (int i = 0; i < n; ++i) maxRow = std::max(maxRow, hPosRow[i + 1] - hPosRow[i]);
+    // chunk capacity: as many cells as the widest (part, depth) group, within what S pipeline slots
+    // of shared memory hold (M compute threads + one service warp per CTA)
+    const size_t smemCap = 200 * 1024;
+    const int rowCap = std::max(maxRow, 1);
+    int M = std::min(480, std::max(32, ((maxGroup + 31) / 32) * 32));
+    while (M > 32 && k::gsSmemBytes<double>(M, M * rowCap) > smemCap) M -= 32;
+    int E = M * rowCap;
+    while (E > rowCap && k::gsSmemBytes<double>(M, E) > smemCap) E -= rowCap;
+    if (maxRow > E || k::gsSmemBytes<double>(M, E) > smemCap)
+        fail(B2G_ERR_ARGUMENT, "b2g: a cell has more faces than the Gauss-Seidel pipeline holds.");
+    G.maxCells = M;
+    G.maxEnt = E;
+    std::vector<int> hChunkStart, hChunkDepth, hPartChunk(P + 1, 0);
+    for (int g = 0; g < nLvl; ++g)
+    {
+        const int gs = hLvlStart[g];
+        const int ge = g + 1 < nLvl ? hLvlStart[g + 1] : n;
+        int cs = gs;
+        while (cs < ge)
+        {
+            int ce = cs;
+            while (ce < ge && ce - cs < M && hPosRow[ce + 1] - hPosRow[cs] <= E) ++ce;
+            hChunkStart.push_back(cs);
+            hChunkDepth.push_back(hLvlDepth[g]);
+            hPartChunk[hLvlPart[g] + 1]++;
+            cs = ce;
+        }
+    }
+    const int nCh = static_cast<int>(hChunkStart.size());
+    hChunkStart.push_back(n);
+    for (int p = 0; p < P; ++p) hPartChunk[p + 1] += hPartChunk[p];
+    G.nChunks = nCh;
+    G.chunkStart.upload(hChunkStart.data(), hChunkStart.size(), s);
+    G.chunkDepth.upload(hChunkDepth.data(), hChunkDepth.size(), s);
+    G.partChunkStart.upload(hPartChunk.data(), hPartChunk.size(), s);
+    G.chunkNeedUp.alloc(nCh, s);
+    kFillInt<<<grid(nCh), TPB, 0, s>>>(G.chunkNeedUp.p, nCh, -1);
+    DBuf<int> chunkOf;
+    chunkOf.alloc(n, s);
+    kChunkOfPos<<<grid(n), TPB, 0, s>>>(n, nCh, G.chunkStart.p, chunkOf.p);
     const int words = (P + 31) / 32;
-    DBuf<unsigned> upBits, downBits;
+    DBuf<unsigned> upBits;
     upBits.alloc(static_cast<size_t>(P) * words, s);
-    downBits.alloc(static_cast<size_t>(P) * words, s);
     upBits.zero(s);
-    downBits.zero(s);
-    kNeeds<<<grid(n), TPB, 0, s>>>(n, P, partOf.p, G.depth.p, lvlOfCell.p, L.losortStart.p, L.losort.p,
-                                   L.lower.p, L.ownStart.p, L.upper.p, G.lvlNeedUp.p, G.lvlNeedDown.p,
-                                   upBits.p, downBits.p, words);
+    G.entCode.alloc(2 * (size_t)L.nFaces, s);
+    G.entFacePos.alloc(2 * (size_t)L.nFaces, s);
+    kEntryCodes<<<grid(n), TPB, 0, s>>>(n, k::kRing, G.posCell.p, posOf.p, partOf.p, G.depth.p, chunkOf.p,
+                                        G.chunkStart.p, G.posRow.p, L.rowStart.p, L.losortStart.p, L.col.p,
+                                        L.entFace.p, G.entCode.p, G.entFacePos.p, G.chunkNeedUp.p, upBits.p, words);
     B2G_LAUNCH_CHECK();
-    // per-part level ranges and dependency lists
-    std::vector<int> hLvlPart = lvlPart.download(s);
-    std::vector<int> partLvlStart(P + 1, 0);
-    for (int Lv = 0; Lv < nLvl; ++Lv) partLvlStart[hLvlPart[Lv] + 1]++;
-    for (int p = 0; p < P; ++p) partLvlStart[p + 1] += partLvlStart[p];
-    G.partLvlStart.upload(partLvlStart.data(), P + 1, s);
+    G.chunkRec.alloc(8 * (size_t)nCh, s);
+    kChunkRecs<<<grid(nCh), TPB, 0, s>>>(nCh, G.chunkStart.p, G.posRow.p, G.chunkDepth.p, G.chunkNeedUp.p,
+                                         G.chunkRec.p);
+    B2G_LAUNCH_CHECK();
     std::vector<unsigned> hUp = upBits.download(s);
-    std::vector<unsigned> hDown = downBits.download(s);
-    std::vector<int> depStart(2 * P + 1, 0), depList;
+    std::vector<int> upStart(P + 1, 0), upList;
     for (int p = 0; p < P; ++p)
     {
-        depStart[p] = static_cast<int>(depList.size());
+        upStart[p] = static_cast<int>(upList.size());
         for (int q = 0; q < P; ++q)
-            if (hUp[(size_t)p * words + (q >> 5)] & (1u << (q & 31))) depList.push_back(q);
+            if (hUp[(size_t)p * words + (q >> 5)] & (1u << (q & 31))) upList.push_back(q);
     }
-    for (int p = 0; p < P; ++p)
-    {
-        depStart[P + p] = static_cast<int>(depList.size());
-        for (int q = 0; q < P; ++q)
-            if (hDown[(size_t)p * words + (q >> 5)] & (1u << (q & 31))) depList.push_back(q);
-    }
-    depStart[2 * P] = static_cast<int>(depList.size());
-    G.depStart.upload(depStart.data(), depStart.size(), s);
-    if (depList.empty()) depList.push_back(0);
-    G.depList.upload(depList.data(), depList.size(), s);
+    upStart[P] = static_cast<int>(upList.size());
+    std::vector<int> hasDown(P, 0);
+    for (int q : upList) hasDown[q] = 1;
+    G.hasDown.upload(hasDown.data(), hasDown.size(), s);
+    G.upStart.upload(upStart.data(), upStart.size(), s);
+    if (upList.empty()) upList.push_back(0);
+    G.upList.upload(upList.data(), upList.size(), s);
     G.progress.alloc(P, s);
     G.progress.zero(s);
-    std::vector<int> hLvlStart = G.lvlStart.download(s);
-    int mx = 0;
-    for (int Lv = 0; Lv < nLvl; ++Lv) mx = std::max(mx, hLvlStart[Lv + 1] - hLvlStart[Lv]);
-    G.maxLevelCells = mx;
+    B2G_CUDA(cudaStreamSynchronize(s));
 }
 
 const DeviceInfo& DeviceInfo::get()

@@ -6,26 +6,32 @@
 
 namespace b2g {
 
-// Forward Gauss-Seidel dependency schedule of one level, partitioned for the part-pipelined sweep
-// kernel (gs.cu). Cells are split into `nParts` contiguous index ranges; each part lists its cells
-// by (depth, cell) where depth is the cell's level in the forward DAG (a cell depends on the
-// owners of the faces it is the neighbour of). Local level = one (part, depth) group.
+// Forward Gauss-Seidel schedule of one level for the part-pipelined sweep kernel (gs_kernels.cuh).
+// Cells are split into `nParts` contiguous index ranges; each part lists its cells by (depth, cell),
+// depth being the cell's level in the forward DAG (a cell depends on the owners of the faces it is
+// the neighbour of). Positions are indices into that (part, depth, cell) order; a part's positions
+// are cut into chunks of at most maxCells cells and maxEnt row entries of one depth.
 struct GsSchedule
 {
     int nParts = 0;
-    int maxDepth = 0;          // deepest level (0-based)
-    int nLocalLevels = 0;
-    int maxLevelCells = 0;     // largest (part, depth) group
-    DBuf<int> order;           // [nCells] cells in (part, depth, cell) order
-    DBuf<int> partLvlStart;    // [nParts+1] into the local-level arrays
-    DBuf<int> lvlStart;        // [nLocalLevels+1] into order
-    DBuf<int> lvlDepth;        // [nLocalLevels]
-    DBuf<int> lvlNeedUp;       // [nLocalLevels] max depth of lower neighbours in other parts, -1 if none
-    DBuf<int> lvlNeedDown;     // [nLocalLevels] max depth of upper neighbours in other parts, -1 if none
-    DBuf<int> depStart;        // [2*nParts+1]: part p's upstream parts, then its downstream parts
-    DBuf<int> depList;
-    DBuf<unsigned> progress;   // [nParts] per-part progress words (reset before each launch)
+    int maxDepth = 0;
+    int nChunks = 0;
+    int maxCells = 0;          // chunk cell capacity == the kernel's compute threads
+    int maxEnt = 0;            // chunk entry capacity
     DBuf<int> depth;           // [nCells]
+    DBuf<int> partChunkStart;  // [nParts+1]
+    DBuf<int> chunkStart;      // [nChunks+1] positions
+    DBuf<int> chunkDepth;      // [nChunks]
+    DBuf<int> chunkNeedUp;     // [nChunks] deepest owner held by another part, -1 if none
+    DBuf<int> chunkRec;        // [nChunks][8]: pos0, m, e0, ne, depth, needUp, 0, 0 (the kernel's records)
+    DBuf<int> upStart;         // [nParts+1] upstream parts of each part
+    DBuf<int> upList;
+    DBuf<int> hasDown;         // [nParts] 1 if another part reads this part's new values
+    DBuf<int> posCell;         // [nCells] cell at each position
+    DBuf<int> posRow;          // [nCells+1] entry offsets in position order
+    DBuf<unsigned> entCode;    // [2*nFaces] kind << 30 | ring slot or cell
+    DBuf<int> entFacePos;      // [2*nFaces] face of each entry (fills the coefficients per solve)
+    DBuf<unsigned> progress;   // [nParts] per-part progress words (reset before each launch)
 };
 
 // One level's addressing and its derived layouts (built once per hierarchy).

@@ -293,5 +293,105 @@ __global__ void __launch_bounds__(NT) normFactorPartial(Rows<T> A, const T* __re
     if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
+// Serial reductions in the reference's order: one warp streams the terms, lane 0 adds them one
+// after another (s = ((s + t0) + t1) + ...), exactly as the reference's host loops do.
+template <int OP>
+__global__ void __launch_bounds__(32) serialReduce(int n, const double* __restrict__ a, const double* __restrict__ b,
+                                                   double* __restrict__ out)
+{
+    const int lane = threadIdx.x;
+    double s = 0.0;
+    for (int base = 0; base < n; base += 32)
+    {
+        const int i = base + lane;
+        double term = 0.0;
+        if (i < n)
+        {
+            if (OP == RED_DOT) term = __dmul_rn(a[i], b[i]);
+            else if (OP == RED_SUMMAG) term = fabs(a[i]);
+            else term = a[i];
+        }
+        const int cnt = min(32, n - base);
+        for (int j = 0; j < cnt; ++j)
+        {
+            const double v = __shfl_sync(0xffffffffu, term, j);
+            if (lane == 0) s = __dadd_rn(s, v);
+        }
+    }
+    if (lane == 0) *out = s;
+}
+
+// scale's two sums in one serial pass: num += field*source, den += field*Acf
+static __global__ void __launch_bounds__(32) serialScaleDots(int n, const double* __restrict__ field,
+                                                      const double* __restrict__ source, const double* __restrict__ Acf,
+                                                      double* __restrict__ sf)
+{
+    const int lane = threadIdx.x;
+    double num = 0.0, den = 0.0;
+    for (int base = 0; base < n; base += 32)
+    {
+        const int i = base + lane;
+        double tn = 0.0, td = 0.0;
+        if (i < n)
+        {
+            tn = __dmul_rn(field[i], source[i]);
+            td = __dmul_rn(field[i], Acf[i]);
+        }
+        const int cnt = min(32, n - base);
+        for (int j = 0; j < cnt; ++j)
+        {
+            const double vn = __shfl_sync(0xffffffffu, tn, j);
+            const double vd = __shfl_sync(0xffffffffu, td, j);
+            if (lane == 0)
+            {
+                num = __dadd_rn(num, vn);
+                den = __dadd_rn(den, vd);
+            }
+        }
+    }
+    if (lane == 0) *sf = __ddiv_rn(num, den >= 0.0 ? __dadd_rn(den, Small<double>::vsmall) : __dsub_rn(den, Small<double>::vsmall));
+}
+
+// normFactor's sum in the reference's order (GAMG:146-157), with sumA from the rows
+static __global__ void __launch_bounds__(32) serialNormFactor(Rows<double> A, const double* __restrict__ psi,
+                                                       const double* __restrict__ source, const double* __restrict__ Apsi,
+                                                       double* __restrict__ out)
+{
+    const int lane = threadIdx.x;
+    double sumPsi = 0.0;
+    for (int base = 0; base < A.n; base += 32)
+    {
+        const int i = base + lane;
+        const double v = i < A.n ? psi[i] : 0.0;
+        const int cnt = min(32, A.n - base);
+        for (int j = 0; j < cnt; ++j)
+        {
+            const double w = __shfl_sync(0xffffffffu, v, j);
+            if (lane == 0) sumPsi = __dadd_rn(sumPsi, w);
+        }
+    }
+    const double xRef = __ddiv_rn(__shfl_sync(0xffffffffu, sumPsi, 0), static_cast<double>(A.n));
+    double s = 0.0;
+    for (int base = 0; base < A.n; base += 32)
+    {
+        const int c = base + lane;
+        double term = 0.0;
+        if (c < A.n)
+        {
+            double sumA = A.diag[c];
+            for (int e = A.rowStart[c]; e < A.rowStart[c + 1]; ++e) sumA = __dadd_rn(sumA, A.val[e]);
+            const double t = __dmul_rn(sumA, xRef);
+            term = __dadd_rn(fabs(__dsub_rn(Apsi[c], t)), fabs(__dsub_rn(source[c], t)));
+        }
+        const int cnt = min(32, A.n - base);
+        for (int j = 0; j < cnt; ++j)
+        {
+            const double v = __shfl_sync(0xffffffffu, term, j);
+            if (lane == 0) s = __dadd_rn(s, v);
+        }
+    }
+    if (lane == 0) *out = __dadd_rn(s, 1e-20);
+}
+
 }  // namespace k
 }  // namespace b2g

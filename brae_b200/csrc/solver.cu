@@ -134,6 +134,33 @@ k::Rows<T> rowsOf(const LevelAddr& L, const LevelCoef<T>& C)
     return k::Rows<T>{L.nCells, L.rowStart.p, L.col.p, C.val.p, C.diag.p};
 }
 
+// the Gauss-Seidel layout of one level's coefficients (position order)
+template <class T>
+__global__ void kGsLayout(int n, long long nnz, const int* __restrict__ posCell, const int* __restrict__ entFacePos,
+                          const T* __restrict__ diag, const T* __restrict__ upper, T* __restrict__ gsDiag,
+                          T* __restrict__ gsVal)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long m = n > nnz ? n : nnz;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m; i += stride)
+    {
+        if (i < n) gsDiag[i] = diag[posCell[i]];
+        if (i < nnz) gsVal[i] = upper[entFacePos[i]];
+    }
+}
+
+template <class T>
+void fillGsLayout(const LevelAddr& L, LevelCoef<T>& C, cudaStream_t s)
+{
+    C.gsDiag.alloc(L.nCells, s);
+    C.gsVal.alloc(2 * (size_t)L.nFaces, s);
+    const long long nnz = 2LL * L.nFaces;
+    const long long m = std::max<long long>(L.nCells, nnz);
+    if (m) kGsLayout<T><<<std::min(ceilDiv(m, NT), 8192), NT, 0, s>>>(L.nCells, nnz, L.gs.posCell.p, L.gs.entFacePos.p,
+                                                                       C.diag.p, C.upper.p, C.gsDiag.p, C.gsVal.p);
+    B2G_LAUNCH_CHECK();
+}
+
 template <class T, class S>
 void castInto(long long n, const S* in, T* out, cudaStream_t s)
 {
@@ -149,6 +176,90 @@ void zeroArray(long long n, T* x, cudaStream_t s)
 }
 
 }  // namespace
+
+cudaEvent_t Matrix::timedBegin(int cls)
+{
+    if (!g_profiling) return nullptr;
+    std::pair<cudaEvent_t, cudaEvent_t> e;
+    if (!evFree.empty())
+    {
+        e = evFree.back();
+        evFree.pop_back();
+    }
+    else
+    {
+        B2G_CUDA(cudaEventCreate(&e.first));
+        B2G_CUDA(cudaEventCreate(&e.second));
+    }
+    B2G_CUDA(cudaEventRecord(e.first, stream));
+    (cls == 0 ? evAmul : evGs).push_back(e);
+    return e.first;
+}
+
+void Matrix::timedEnd(int cls, cudaEvent_t start)
+{
+    if (!start) return;
+    auto& v = cls == 0 ? evAmul : evGs;
+    B2G_CUDA(cudaEventRecord(v.back().second, stream));
+}
+
+void Matrix::timingsBegin()
+{
+    for (int i = 0; i < 4; ++i)
+    {
+        ms[i] = 0;
+        counts[i] = 0;
+    }
+    launches = 0;
+    if (!g_profiling) return;
+    if (!evSolve[0])
+    {
+        B2G_CUDA(cudaEventCreate(&evSolve[0]));
+        B2G_CUDA(cudaEventCreate(&evSolve[1]));
+    }
+    B2G_CUDA(cudaEventRecord(evSolve[0], stream));
+}
+
+void Matrix::timingsEnd()
+{
+    counts[3] = launches;
+    if (!g_profiling) return;
+    B2G_CUDA(cudaEventRecord(evSolve[1], stream));
+    B2G_CUDA(cudaEventSynchronize(evSolve[1]));
+    float t = 0.f;
+    B2G_CUDA(cudaEventElapsedTime(&t, evSolve[0], evSolve[1]));
+    ms[3] = t;
+    for (int cls = 0; cls < 2; ++cls)
+    {
+        auto& v = cls == 0 ? evAmul : evGs;
+        for (auto& e : v)
+        {
+            float x = 0.f;
+            B2G_CUDA(cudaEventElapsedTime(&x, e.first, e.second));
+            ms[cls] += x;
+            evFree.push_back(e);
+        }
+        counts[cls] = static_cast<long long>(v.size());
+        v.clear();
+    }
+    ms[2] = ms[3] - ms[0] - ms[1];
+    counts[2] = counts[3] - counts[0] - counts[1];
+}
+
+Matrix::~Matrix()
+{
+    for (auto* v : {&evAmul, &evGs, &evFree})
+        for (auto& e : *v)
+        {
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+    if (evSolve[0])
+    {
+        cudaEventDestroy(evSolve[0]);
+        cudaEventDestroy(evSolve[1]);
+    }
+}
 
 template <> VCycleData<double>& Matrix::data<double>() { return v64; }
 template <> VCycleData<float>& Matrix::data<float>() { return v32; }
@@ -183,6 +294,7 @@ void Matrix::setFine(const double* diag, const double* upper, int memspace)
         k::gatherVal<double, double><<<std::min(ceilDiv(2LL * L.nFaces, NT), 8192), NT, 0, stream>>>(
             2LL * L.nFaces, L.entFace.p, C.upper.p, C.val.p);
     B2G_LAUNCH_CHECK();
+    fillGsLayout(L, C, stream);
     coarseBuilt = false;
     v32.built = false;
 }
@@ -211,6 +323,7 @@ void Matrix::buildCoarse()
                 2LL * Cl.nFaces, Cl.entFace.p, C.upper.p, C.val.p);
         }
         B2G_LAUNCH_CHECK();
+        fillGsLayout(Cl, C, stream);
     }
     // V-cycle work
     v64.corr.resize(nL);
@@ -245,6 +358,7 @@ void Matrix::ensureFp32()
         castInto<float, double>(L.nCells, v64.coef[i].diag.p, C.diag.p, stream);
         castInto<float, double>(L.nFaces, v64.coef[i].upper.p, C.upper.p, stream);
         castInto<float, double>(2LL * L.nFaces, v64.coef[i].val.p, C.val.p, stream);
+        fillGsLayout(L, C, stream);
     }
     v32.corr.resize(nL);
     v32.src.resize(nL);
@@ -267,13 +381,15 @@ template <class T>
 void Matrix::amul(int level, const T* x, T* y)
 {
     const LevelAddr& L = mesh->lev[level];
+    cudaEvent_t e = level == 0 ? timedBegin(0) : nullptr;
     k::amul<T><<<rowsGrid(L.nCells), NT, 0, stream>>>(rowsOf(L, data<T>().coef[level]), x, y);
+    timedEnd(0, e);
     B2G_LAUNCH_CHECK();
     ++launches;
 }
 
 template <class T>
-void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps)
+void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps, unsigned long long* trace)
 {
     if (nSweeps <= 0) return;
     if (smoother != B2G_SMOOTHER_GAUSS_SEIDEL)
@@ -284,30 +400,40 @@ void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps)
     const LevelCoef<T>& C = data<T>().coef[level];
     k::GsArgs<T> a;
     a.nParts = G.nParts;
-    a.maxDepth = G.maxDepth;
-    a.order = G.order.p;
-    a.partLvlStart = G.partLvlStart.p;
-    a.lvlStart = G.lvlStart.p;
-    a.lvlDepth = G.lvlDepth.p;
-    a.lvlNeedUp = G.lvlNeedUp.p;
-    a.lvlNeedDown = G.lvlNeedDown.p;
-    a.depStart = G.depStart.p;
-    a.depList = G.depList.p;
-    a.rowStart = L.rowStart.p;
-    a.losortStart = L.losortStart.p;
-    a.col = L.col.p;
-    a.val = C.val.p;
-    a.diag = C.diag.p;
+    a.maxCells = G.maxCells;
+    a.maxEnt = G.maxEnt;
+    a.partChunkStart = G.partChunkStart.p;
+    a.chunkRec = reinterpret_cast<const int4*>(G.chunkRec.p);
+    a.upStart = G.upStart.p;
+    a.upList = G.upList.p;
+    a.hasDown = G.hasDown.p;
+    a.posCell = G.posCell.p;
+    a.posRow = G.posRow.p;
+    a.entCode = G.entCode.p;
+    a.entVal = C.gsVal.p;
+    a.posDiag = C.gsDiag.p;
     a.b = src;
     a.psi = psiL;
     a.progress = G.progress.p;
     a.err = err.p;
-    int bd = ((G.maxLevelCells + 31) / 32) * 32;
-    bd = std::max(64, std::min(1024, bd));
-    B2G_CUDA(cudaMemsetAsync(G.progress.p, 0, sizeof(unsigned) * G.nParts, stream));
-    k::gsPipelined<T><<<G.nParts, bd, 0, stream>>>(a, nSweeps);
-    B2G_LAUNCH_CHECK();
-    launches += 2;
+    a.trace = trace;
+    const size_t smem = k::gsSmemBytes<T>(G.maxCells, G.maxEnt);
+    static bool attrSet[2] = {false, false};
+    bool& set = attrSet[sizeof(T) == 8 ? 0 : 1];
+    if (!set)
+    {
+        B2G_CUDA(cudaFuncSetAttribute(k::gsSweep<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024));
+        set = true;
+    }
+    for (int sw = 0; sw < nSweeps; ++sw)
+    {
+        B2G_CUDA(cudaMemsetAsync(G.progress.p, 0, sizeof(unsigned) * G.nParts, stream));
+        cudaEvent_t e = level == 0 ? timedBegin(1) : nullptr;
+        k::gsSweep<T><<<G.nParts, G.maxCells + 32, smem, stream>>>(a);
+        timedEnd(1, e);
+        B2G_LAUNCH_CHECK();
+        launches += 1;
+    }
 }
 
 template <class T>
@@ -315,12 +441,45 @@ void Matrix::scale(int level, T* field, T* Acf, const T* src)
 {
     const LevelAddr& L = mesh->lev[level];
     VCycleData<T>& D = data<T>();
-    const int g = redGrid(L.nCells);
-    k::amulScaleDots<T, NT><<<g, NT, 0, stream>>>(rowsOf(L, D.coef[level]), field, src, Acf, D.partial.p);
-    k::scaleFactor<T, NT><<<1, NT, 0, stream>>>(D.partial.p, g, D.sf.p);
+    if (serial && sizeof(T) == 8)
+    {
+        k::amul<T><<<rowsGrid(L.nCells), NT, 0, stream>>>(rowsOf(L, D.coef[level]), field, Acf);
+        k::serialScaleDots<<<1, 32, 0, stream>>>(L.nCells, reinterpret_cast<const double*>(field),
+                                                 reinterpret_cast<const double*>(src),
+                                                 reinterpret_cast<const double*>(Acf),
+                                                 reinterpret_cast<double*>(D.sf.p));
+    }
+    else
+    {
+        const int g = redGrid(L.nCells);
+        k::amulScaleDots<T, NT><<<g, NT, 0, stream>>>(rowsOf(L, D.coef[level]), field, src, Acf, D.partial.p);
+        k::scaleFactor<T, NT><<<1, NT, 0, stream>>>(D.partial.p, g, D.sf.p);
+    }
     k::scaleUpdate<T><<<rowsGrid(L.nCells), NT, 0, stream>>>(L.nCells, D.sf.p, field, src, Acf, D.coef[level].diag.p);
     B2G_LAUNCH_CHECK();
     launches += 3;
+}
+
+void Matrix::reduceInto(int op, int n, const double* a, const double* b, double* slot)
+{
+    if (serial)
+    {
+        if (op == k::RED_DOT) k::serialReduce<k::RED_DOT><<<1, 32, 0, stream>>>(n, a, b, slot);
+        else if (op == k::RED_SUMMAG) k::serialReduce<k::RED_SUMMAG><<<1, 32, 0, stream>>>(n, a, b, slot);
+        else k::serialReduce<k::RED_SUM><<<1, 32, 0, stream>>>(n, a, b, slot);
+        ++launches;
+    }
+    else
+    {
+        const int g = redGrid(n);
+        if (op == k::RED_DOT) k::reducePartial<double, NT, k::RED_DOT><<<g, NT, 0, stream>>>(n, a, b, v64.partial.p);
+        else if (op == k::RED_SUMMAG)
+            k::reducePartial<double, NT, k::RED_SUMMAG><<<g, NT, 0, stream>>>(n, a, b, v64.partial.p);
+        else k::reducePartial<double, NT, k::RED_SUM><<<g, NT, 0, stream>>>(n, a, b, v64.partial.p);
+        k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, slot);
+        launches += 2;
+    }
+    B2G_LAUNCH_CHECK();
 }
 
 template <class T>
@@ -393,15 +552,22 @@ void Matrix::coarsestSolve<float>(int level, float* x, const float* src, float t
 double Matrix::normFactor(int level, const double* x, const double* src, const double* Apsi)
 {
     const LevelAddr& L = mesh->lev[level];
-    const int g = redGrid(L.nCells);
-    k::reducePartial<double, NT, k::RED_SUM><<<g, NT, 0, stream>>>(L.nCells, x, nullptr, v64.partial.p);
-    k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->sumPsi);
-    k::normFactorPartial<double, NT><<<g, NT, 0, stream>>>(rowsOf(L, v64.coef[level]), x, src, Apsi,
-                                                           &scal.p->sumPsi, v64.partial.p);
-    k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->nf);
-    kNfFinish<<<1, 1, 0, stream>>>(scal.p);
+    if (serial)
+    {
+        k::serialNormFactor<<<1, 32, 0, stream>>>(rowsOf(L, v64.coef[level]), x, src, Apsi, &scal.p->nf);
+        ++launches;
+    }
+    else
+    {
+        const int g = redGrid(L.nCells);
+        reduceInto(k::RED_SUM, L.nCells, x, nullptr, &scal.p->sumPsi);
+        k::normFactorPartial<double, NT><<<g, NT, 0, stream>>>(rowsOf(L, v64.coef[level]), x, src, Apsi,
+                                                               &scal.p->sumPsi, v64.partial.p);
+        k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->nf);
+        kNfFinish<<<1, 1, 0, stream>>>(scal.p);
+        launches += 3;
+    }
     B2G_LAUNCH_CHECK();
-    launches += 5;
     double nf = 0;
     B2G_CUDA(cudaMemcpyAsync(&nf, &scal.p->nf, sizeof(double), cudaMemcpyDeviceToHost, stream));
     B2G_CUDA(cudaStreamSynchronize(stream));
@@ -454,9 +620,22 @@ void Matrix::vcycle(const b2g_controls& c, T* x, const T* src, T* Apsi, T* fcor,
     const LevelAddr& F = mesh->lev[0];
     if (c.scaleCorrection)
     {
-        const int g = redGrid(F.nCells);
-        k::amulScaleDots<T, NT><<<g, NT, 0, stream>>>(rowsOf(F, D.coef[0]), fcor, fres, Apsi, D.partial.p);
-        k::scaleFactor<T, NT><<<1, NT, 0, stream>>>(D.partial.p, g, D.sf.p);
+        if (serial && sizeof(T) == 8)
+        {
+            k::amul<T><<<rowsGrid(F.nCells), NT, 0, stream>>>(rowsOf(F, D.coef[0]), fcor, Apsi);
+            k::serialScaleDots<<<1, 32, 0, stream>>>(F.nCells, reinterpret_cast<const double*>(fcor),
+                                                     reinterpret_cast<const double*>(fres),
+                                                     reinterpret_cast<const double*>(Apsi),
+                                                     reinterpret_cast<double*>(D.sf.p));
+        }
+        else
+        {
+            const int g = redGrid(F.nCells);
+            cudaEvent_t e = timedBegin(0);
+            k::amulScaleDots<T, NT><<<g, NT, 0, stream>>>(rowsOf(F, D.coef[0]), fcor, fres, Apsi, D.partial.p);
+            timedEnd(0, e);
+            k::scaleFactor<T, NT><<<1, NT, 0, stream>>>(D.partial.p, g, D.sf.p);
+        }
         k::scaleUpdateAdd<T><<<rowsGrid(F.nCells), NT, 0, stream>>>(F.nCells, D.sf.p, fcor, fres, Apsi,
                                                                    D.coef[0].diag.p, x);
         launches += 3;
@@ -555,14 +734,15 @@ void Matrix::checkDeviceError()
 b2g_perf Matrix::pcg(const b2g_controls& c, b2g_solve_log* log)
 {
     const int n0 = n(0);
+    serial = c.reduction == B2G_REDUCTION_SERIAL;
+    timingsBegin();
     resetLog(log ? std::max(log->coarsestCapacity, 0) : 0);
     amul<double>(0, psi.p, wA.p);
     k::subtract<double><<<rowsGrid(n0), NT, 0, stream>>>(n0, source.p, wA.p, rA.p);
     B2G_LAUNCH_CHECK();
     normFactor(0, psi.p, source.p, wA.p);
     const int g = redGrid(n0);
-    k::reducePartial<double, NT, k::RED_SUMMAG><<<g, NT, 0, stream>>>(n0, rA.p, nullptr, v64.partial.p);
-    k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->sumMag);
+    reduceInto(k::RED_SUMMAG, n0, rA.p, nullptr, &scal.p->sumMag);
     kInitResidual<<<1, 1, 0, stream>>>(scal.p);
     B2G_LAUNCH_CHECK();
     PcgScalars hs;
@@ -573,7 +753,11 @@ b2g_perf Matrix::pcg(const b2g_controls& c, b2g_solve_log* log)
     perf.finalResidual = hs.initRes;
     perf.nIterations = 0;
     if (log) log->historyCount = 0;
-    if (c.minIter <= 0 && convergedH(perf.finalResidual, perf.initialResidual, c.tolerance, c.relTol)) return perf;
+    if (c.minIter <= 0 && convergedH(perf.finalResidual, perf.initialResidual, c.tolerance, c.relTol))
+    {
+        timingsEnd();
+        return perf;
+    }
     // the preconditioner, built on first use (PCG.C:111-118)
     if (nLevels() == 0)
         fail(B2G_ERR_REFUSED, "b2g GAMG: no coarse levels created, either matrix too small for GAMG or "
@@ -586,21 +770,16 @@ b2g_perf Matrix::pcg(const b2g_controls& c, b2g_solve_log* log)
     do
     {
         precondition(c, wA.p, rA.p);
-        k::reducePartial<double, NT, k::RED_DOT><<<g, NT, 0, stream>>>(n0, wA.p, rA.p, v64.partial.p);
-        k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->wArA);
-        if (flexible)
-        {
-            k::reducePartial<double, NT, k::RED_DOT><<<g, NT, 0, stream>>>(n0, wA.p, rOld.p, v64.partial.p);
-            k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->wrOld);
-        }
+        reduceInto(k::RED_DOT, n0, wA.p, rA.p, &scal.p->wArA);
+        if (flexible) reduceInto(k::RED_DOT, n0, wA.p, rOld.p, &scal.p->wrOld);
         kPUpdate<<<rowsGrid(n0), NT, 0, stream>>>(n0, wA.p, pA.p, scal.p, flexible ? 1 : 0);
         B2G_LAUNCH_CHECK();
         amul<double>(0, pA.p, wA.p);
-        k::reducePartial<double, NT, k::RED_DOT><<<g, NT, 0, stream>>>(n0, wA.p, pA.p, v64.partial.p);
-        k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->wApA);
+        reduceInto(k::RED_DOT, n0, wA.p, pA.p, &scal.p->wApA);
         kAlphaUpdate<NT><<<g, NT, 0, stream>>>(n0, psi.p, pA.p, rA.p, wA.p, flexible ? rOld.p : nullptr, scal.p,
                                               v64.partial.p);
-        k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->sumMag);
+        if (serial) reduceInto(k::RED_SUMMAG, n0, rA.p, nullptr, &scal.p->sumMag);
+        else k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->sumMag);
         kIterFinish<<<1, 1, 0, stream>>>(scal.p);
         B2G_LAUNCH_CHECK();
         launches += 9;
@@ -615,6 +794,7 @@ b2g_perf Matrix::pcg(const b2g_controls& c, b2g_solve_log* log)
     } while ((perf.nIterations < c.maxIter &&
               !convergedH(perf.finalResidual, perf.initialResidual, c.tolerance, c.relTol)) ||
              perf.nIterations < c.minIter);
+    timingsEnd();
     checkDeviceError();
     readLog(log);
     return perf;
@@ -624,6 +804,8 @@ b2g_perf Matrix::pcg(const b2g_controls& c, b2g_solve_log* log)
 b2g_perf Matrix::gamg(const b2g_controls& c, b2g_solve_log* log)
 {
     const int n0 = n(0);
+    serial = c.reduction == B2G_REDUCTION_SERIAL;
+    timingsBegin();
     if (nLevels() == 0)
         fail(B2G_ERR_REFUSED, "b2g GAMG: no coarse levels created, either matrix too small for GAMG or "
                               "nCellsInCoarsestLevel too large (GAMGSolver.C:333).");
@@ -636,9 +818,7 @@ b2g_perf Matrix::gamg(const b2g_controls& c, b2g_solve_log* log)
     amul<double>(0, psi.p, AwA.p);
     normFactor(0, psi.p, source.p, AwA.p);
     k::subtract<double><<<rowsGrid(n0), NT, 0, stream>>>(n0, source.p, AwA.p, fr.p);
-    const int g = redGrid(n0);
-    k::reducePartial<double, NT, k::RED_SUMMAG><<<g, NT, 0, stream>>>(n0, fr.p, nullptr, v64.partial.p);
-    k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->sumMag);
+    reduceInto(k::RED_SUMMAG, n0, fr.p, nullptr, &scal.p->sumMag);
     kInitResidual<<<1, 1, 0, stream>>>(scal.p);
     B2G_LAUNCH_CHECK();
     PcgScalars hs;
@@ -655,8 +835,7 @@ b2g_perf Matrix::gamg(const b2g_controls& c, b2g_solve_log* log)
         vcycle<double>(cc, psi.p, source.p, AwA.p, fc.p, fr.p);
         amul<double>(0, psi.p, AwA.p);
         k::subtract<double><<<rowsGrid(n0), NT, 0, stream>>>(n0, source.p, AwA.p, fr.p);
-        k::reducePartial<double, NT, k::RED_SUMMAG><<<g, NT, 0, stream>>>(n0, fr.p, nullptr, v64.partial.p);
-        k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->sumMag);
+        reduceInto(k::RED_SUMMAG, n0, fr.p, nullptr, &scal.p->sumMag);
         kResidualFinish<<<1, 1, 0, stream>>>(scal.p);
         B2G_LAUNCH_CHECK();
         B2G_CUDA(cudaMemcpyAsync(&hs, scal.p, sizeof(hs), cudaMemcpyDeviceToHost, stream));
@@ -676,8 +855,8 @@ b2g_perf Matrix::gamg(const b2g_controls& c, b2g_solve_log* log)
 
 template void Matrix::amul<double>(int, const double*, double*);
 template void Matrix::amul<float>(int, const float*, float*);
-template void Matrix::smooth<double>(int, int, double*, const double*, int);
-template void Matrix::smooth<float>(int, int, float*, const float*, int);
+template void Matrix::smooth<double>(int, int, double*, const double*, int, unsigned long long*);
+template void Matrix::smooth<float>(int, int, float*, const float*, int, unsigned long long*);
 template void Matrix::scale<double>(int, double*, double*, const double*);
 template void Matrix::restrictTo<double>(int, const double*, double*);
 template void Matrix::prolongFrom<double>(int, const double*, double*);

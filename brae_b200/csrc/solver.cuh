@@ -22,6 +22,8 @@ struct LevelCoef
     DBuf<T> diag;   // [nCells]
     DBuf<T> upper;  // [nFaces] LDU coefficient (upper == lower)
     DBuf<T> val;    // [2*nFaces] row-layout coefficient
+    DBuf<T> gsDiag; // [nCells] diagonal in Gauss-Seidel position order
+    DBuf<T> gsVal;  // [2*nFaces] coefficients in Gauss-Seidel entry order
 };
 
 // Everything a V-cycle in value type T touches.
@@ -53,9 +55,18 @@ struct Matrix
     DBuf<int> coarseCount;
     DBuf<int> err;
     int coarseLogCapacity = 0;
-    // timing
-    double ms[4] = {0, 0, 0, 0};
+    bool serial = false;                      // B2G_REDUCTION_SERIAL for the current solve
+    // timing (b2g_set_profiling): events around the finest level's Amul and Gauss-Seidel launches
+    double ms[4] = {0, 0, 0, 0};              // finest Amul, finest Gauss-Seidel, other, whole solve
+    long long counts[4] = {0, 0, 0, 0};       // launches of the same classes (whole solve: all)
     long long launches = 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evAmul, evGs, evFree;
+    cudaEvent_t evSolve[2] = {nullptr, nullptr};
+    cudaEvent_t timedBegin(int cls);          // records a start event if profiling (cls 0 Amul, 1 GS)
+    void timedEnd(int cls, cudaEvent_t start);
+    void timingsBegin();
+    void timingsEnd();
+    ~Matrix();
 
     Matrix(Mesh* m, cudaStream_t s);
     void setFine(const double* diag, const double* upper, int memspace);
@@ -66,7 +77,8 @@ struct Matrix
 
     // pieces (device pointers)
     template <class T> void amul(int level, const T* x, T* y);
-    template <class T> void smooth(int level, int smoother, T* psi, const T* source, int nSweeps);
+    template <class T> void smooth(int level, int smoother, T* psi, const T* source, int nSweeps,
+                                   unsigned long long* trace = nullptr);
     template <class T> void scale(int level, T* field, T* Acf, const T* source);
     template <class T> void restrictTo(int step, const T* fine, T* coarse);
     template <class T> void prolongFrom(int step, const T* coarse, T* fine);
@@ -76,6 +88,8 @@ struct Matrix
                                    const T* fr);
     void precondition(const b2g_controls& c, double* w, const double* r);
     double normFactor(int level, const double* psi, const double* source, const double* Apsi);
+    // sum / dot / sum of magnitudes of n values into a device slot, tree or serial per `serial`
+    void reduceInto(int op, int n, const double* a, const double* b, double* slot);
 
     // solves on the fine level (psi/source already in this->psi/source)
     b2g_perf pcg(const b2g_controls& c, b2g_solve_log* log);

@@ -39,7 +39,8 @@ class Controls(C.Structure):
                 ("maxPreSweeps", C.c_int), ("nPostSweeps", C.c_int),
                 ("postSweepsLevelMultiplier", C.c_int), ("maxPostSweeps", C.c_int),
                 ("nFinestSweeps", C.c_int), ("scaleCorrection", C.c_int),
-                ("nCellsInCoarsestLevel", C.c_int), ("nVcycles", C.c_int), ("precision", C.c_int)]
+                ("nCellsInCoarsestLevel", C.c_int), ("nVcycles", C.c_int), ("precision", C.c_int),
+                ("reduction", C.c_int)]
 
 
 class _Perf(C.Structure):
@@ -96,6 +97,7 @@ def _load():
         "b2g_matrix_pcg_solve": (ip, [vp, vp, vp, C.POINTER(Controls), ip, C.POINTER(_Perf),
                                       C.POINTER(_Log)]),
         "b2g_matrix_timings": (ip, [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
+        "b2g_level_smooth_trace": (ip, [vp, ip, vp, vp, vp, ip, C.POINTER(C.c_int)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -112,7 +114,7 @@ EXPORTED = [
     "b2g_gamg_solve", "b2g_matrix_create", "b2g_matrix_destroy", "b2g_matrix_get_level",
     "b2g_level_amul", "b2g_level_smooth", "b2g_level_scale", "b2g_step_restrict",
     "b2g_step_prolong", "b2g_level_norm_factor", "b2g_level_pcg_dic", "b2g_precondition",
-    "b2g_matrix_pcg_solve", "b2g_matrix_timings",
+    "b2g_matrix_pcg_solve", "b2g_matrix_timings", "b2g_level_smooth_trace",
 ]
 
 
@@ -129,6 +131,8 @@ def controls_default(**overrides) -> Controls:
             v = SMOOTHERS[v]
         if k == "precision" and isinstance(v, str):
             v = {"fp64": 0, "fp32_precond": 1}[v]
+        if k == "reduction" and isinstance(v, str):
+            v = {"tree": 0, "serial": 1}[v]
         setattr(c, k, v)
     return c
 
@@ -284,6 +288,16 @@ class Matrix:
         _check(lib.b2g_level_smooth(self.handle, level, SMOOTHERS[smoother], _ptr(psi),
                                     _ptr(source), n_sweeps))
 
+    def smooth_trace(self, level, psi, source, trace=None):
+        """One sweep with per-chunk device-clock stamps; returns (schedule, trace tensor)."""
+        sched = (C.c_int * 5)()
+        _check(lib.b2g_level_smooth_trace(self.handle, level, _ptr(psi), _ptr(source), None, 0, sched))
+        info = dict(parts=sched[0], chunks=sched[1], cells=sched[2], entries=sched[3], depth=sched[4])
+        if trace is not None:
+            _check(lib.b2g_level_smooth_trace(self.handle, level, _ptr(psi), _ptr(source), _ptr(trace),
+                                              int(trace.numel()), sched))
+        return info
+
     def scale(self, level, field, Acf, source):
         _check(lib.b2g_level_scale(self.handle, level, _ptr(field), _ptr(Acf), _ptr(source)))
 
@@ -321,10 +335,15 @@ class Matrix:
                 lb.history(), lb.coarsest())
 
     def timings(self):
+        """(ms, counts) of the last solve: [finest Amul, finest Gauss-Seidel, other, whole solve]."""
         ms = (C.c_double * 4)()
-        n = C.c_longlong()
-        _check(lib.b2g_matrix_timings(self.handle, ms, C.byref(n)))
-        return list(ms), n.value
+        n = (C.c_longlong * 4)()
+        _check(lib.b2g_matrix_timings(self.handle, ms, n))
+        return list(ms), list(n)
+
+
+def set_profiling(on: bool) -> None:
+    _check(lib.b2g_set_profiling(1 if on else 0))
 
 
 def pcg_gamg_solve(mesh: Mesh, diag, upper, source, psi, controls: Controls | None = None,

@@ -72,6 +72,16 @@ enum
     B2G_PRECISION_FP32_PRECOND = 1 /* FP64 outer PCG, FP32 V-cycle, flexible (Polak-Ribiere) beta */
 };
 
+/* How sums and dot products are reduced. TREE is a fixed-shape parallel tree (deterministic, fast);
+ * SERIAL adds in the reference's own order, one term after another (gamg_solver_cpp.cu:119-181), so
+ * the whole FP64 solve is bit-identical to the reference's host path -- a verification mode whose
+ * reductions cost n dependent additions each. */
+enum
+{
+    B2G_REDUCTION_TREE = 0,
+    B2G_REDUCTION_SERIAL = 1
+};
+
 /* The solver entry's controls: PCG's tolerance/relTol/maxIter/minIter (lduMatrixSolver.C:195-205
  * via inter_case_cpp.cu:1519-1572) and the `preconditioner { preconditioner GAMG; ... }`
  * sub-dictionary's GamgControls + nVcycles (GAMGH:67-85, :128-132). Defaults: b2g_controls_default. */
@@ -104,6 +114,7 @@ typedef struct
     int nCellsInCoarsestLevel;   /* 10 */
     int nVcycles;                /* 2 (GAMGPreconditioner.C:60) */
     int precision;               /* B2G_PRECISION_FP64 */
+    int reduction;               /* B2G_REDUCTION_TREE */
 } b2g_controls;
 
 /* SolverPerformance (PCGH:16-21) */
@@ -244,11 +255,20 @@ B2G_API b2g_status b2g_matrix_pcg_solve(b2g_matrix* m, const double* source, dou
 
 /* ---- introspection ---------------------------------------------------------------------------- */
 
-/* Device-time of the kernels of the last solve on `m`, by class (milliseconds), and the number of
- * kernel launches: [0] Amul on the finest level, [1] Gauss-Seidel on the finest level, [2] all
- * coarse-level work, [3] the whole solve. Timed with events only when b2g_set_profiling(1). */
-B2G_API b2g_status b2g_matrix_timings(const b2g_matrix* m, double* ms4, long long* launches);
+/* Device time of the last solve on `m` by kernel class (milliseconds, `ms4`) and launches of each
+ * class (`counts4`): [0] Amul on the finest level, [1] Gauss-Seidel sweeps on the finest level,
+ * [2] everything else, [3] the whole solve. Times are taken with events on the solve's stream only
+ * while b2g_set_profiling(1) is on (counts always). Either pointer may be NULL. */
+B2G_API b2g_status b2g_matrix_timings(const b2g_matrix* m, double* ms4, long long* counts4);
 B2G_API b2g_status b2g_set_profiling(int on);
+
+/* Diagnostic: one Gauss-Seidel sweep of `level` (device pointers) recording into the device array
+ * `trace` [4 * (nChunks + nParts)]: per schedule chunk four SM-cycle stamps (loop top, pipeline
+ * barrier passed, data and upstream parts ready, chunk done), then per part {globaltimer ns, SM
+ * cycles} at its start and end. `schedule` (host, may be NULL) receives {nParts, nChunks, chunk cell
+ * capacity, chunk entry capacity, max depth}. */
+B2G_API b2g_status b2g_level_smooth_trace(b2g_matrix* m, int level, double* psi, const double* source,
+                                          unsigned long long* trace, int traceCapacity, int* schedule);
 
 /* Library version string. */
 B2G_API const char* b2g_version(void);
