@@ -492,8 +492,11 @@ b2g_status b2g_level_amul(b2g_matrix* m, int level, const double* x, double* y)
     return guarded([&] {
         need(m && x && y, "b2g_level_amul: null argument");
         need(level >= 0 && level <= m->mat->nLevels(), "b2g_level_amul: level out of range");
-        m->mat->amul<double>(level, x, y);
-        B2G_CUDA(cudaStreamSynchronize(m->mat->stream));
+        b2g::Matrix& A = *m->mat;
+        A.toPos(level, x, A.ioBuf(0));
+        A.amul<double>(level, A.ioBuf(0), A.ioBuf(1));
+        A.fromPos(level, static_cast<const double*>(A.ioBuf(1)), y);
+        B2G_CUDA(cudaStreamSynchronize(A.stream));
     });
 }
 
@@ -502,8 +505,12 @@ b2g_status b2g_level_smooth(b2g_matrix* m, int level, int smoother, double* psi,
     return guarded([&] {
         need(m && psi && source, "b2g_level_smooth: null argument");
         need(level >= 0 && level <= m->mat->nLevels(), "b2g_level_smooth: level out of range");
-        m->mat->smooth<double>(level, smoother, psi, source, nSweeps);
-        m->mat->checkDeviceError();
+        b2g::Matrix& A = *m->mat;
+        A.toPos(level, static_cast<const double*>(psi), A.ioBuf(0));
+        A.toPos(level, source, A.ioBuf(1));
+        A.smooth<double>(level, smoother, A.ioBuf(0), A.ioBuf(1), nSweeps);
+        A.fromPos(level, static_cast<const double*>(A.ioBuf(0)), psi);
+        A.checkDeviceError();
     });
 }
 
@@ -523,8 +530,12 @@ b2g_status b2g_level_smooth_trace(b2g_matrix* m, int level, double* psi, const d
             schedule[4] = G.maxDepth;
         }
         need(trace == nullptr || traceCapacity >= 4 * (G.nChunks + G.nParts), "b2g_level_smooth_trace: trace too small");
-        m->mat->smooth<double>(level, B2G_SMOOTHER_GAUSS_SEIDEL, psi, source, 1, trace);
-        m->mat->checkDeviceError();
+        b2g::Matrix& A = *m->mat;
+        A.toPos(level, static_cast<const double*>(psi), A.ioBuf(0));
+        A.toPos(level, source, A.ioBuf(1));
+        A.smooth<double>(level, B2G_SMOOTHER_GAUSS_SEIDEL, A.ioBuf(0), A.ioBuf(1), 1, trace);
+        A.fromPos(level, static_cast<const double*>(A.ioBuf(0)), psi);
+        A.checkDeviceError();
     });
 }
 
@@ -534,8 +545,13 @@ b2g_status b2g_level_scale(b2g_matrix* m, int level, double* field, double* Acf,
         need(m && field && Acf && source, "b2g_level_scale: null argument");
         m->mat->serial = false;
         need(level >= 0 && level <= m->mat->nLevels(), "b2g_level_scale: level out of range");
-        m->mat->scale<double>(level, field, Acf, source);
-        B2G_CUDA(cudaStreamSynchronize(m->mat->stream));
+        b2g::Matrix& A = *m->mat;
+        A.toPos(level, static_cast<const double*>(field), A.ioBuf(0));
+        A.toPos(level, source, A.ioBuf(2));
+        A.scale<double>(level, A.ioBuf(0), A.ioBuf(1), A.ioBuf(2));
+        A.fromPos(level, static_cast<const double*>(A.ioBuf(0)), field);
+        A.fromPos(level, static_cast<const double*>(A.ioBuf(1)), Acf);
+        B2G_CUDA(cudaStreamSynchronize(A.stream));
     });
 }
 
@@ -544,8 +560,11 @@ b2g_status b2g_step_restrict(b2g_matrix* m, int step, const double* fine, double
     return guarded([&] {
         need(m && fine && coarse, "b2g_step_restrict: null argument");
         need(step >= 0 && step < m->mat->nLevels(), "b2g_step_restrict: step out of range");
-        m->mat->restrictTo<double>(step, fine, coarse);
-        B2G_CUDA(cudaStreamSynchronize(m->mat->stream));
+        b2g::Matrix& A = *m->mat;
+        A.toPos(step, fine, A.ioBuf(0));
+        A.restrictTo<double>(step, A.ioBuf(0), A.ioBuf(1));
+        A.fromPos(step + 1, static_cast<const double*>(A.ioBuf(1)), coarse);
+        B2G_CUDA(cudaStreamSynchronize(A.stream));
     });
 }
 
@@ -554,8 +573,11 @@ b2g_status b2g_step_prolong(b2g_matrix* m, int step, const double* coarse, doubl
     return guarded([&] {
         need(m && fine && coarse, "b2g_step_prolong: null argument");
         need(step >= 0 && step < m->mat->nLevels(), "b2g_step_prolong: step out of range");
-        m->mat->prolongFrom<double>(step, coarse, fine);
-        B2G_CUDA(cudaStreamSynchronize(m->mat->stream));
+        b2g::Matrix& A = *m->mat;
+        A.toPos(step + 1, coarse, A.ioBuf(0));
+        A.prolongFrom<double>(step, A.ioBuf(0), A.ioBuf(1));
+        A.fromPos(step, static_cast<const double*>(A.ioBuf(1)), fine);
+        B2G_CUDA(cudaStreamSynchronize(A.stream));
     });
 }
 
@@ -565,7 +587,11 @@ b2g_status b2g_level_norm_factor(b2g_matrix* m, int level, const double* psi, co
     return guarded([&] {
         need(m && psi && source && Apsi && nf, "b2g_level_norm_factor: null argument");
         need(level >= 0 && level <= m->mat->nLevels(), "b2g_level_norm_factor: level out of range");
-        *nf = m->mat->normFactor(level, psi, source, Apsi);
+        b2g::Matrix& A = *m->mat;
+        A.toPos(level, psi, A.ioBuf(0));
+        A.toPos(level, source, A.ioBuf(1));
+        A.toPos(level, Apsi, A.ioBuf(2));
+        *nf = A.normFactor(level, A.ioBuf(0), A.ioBuf(1), A.ioBuf(2));
     });
 }
 
@@ -581,7 +607,10 @@ b2g_status b2g_level_pcg_dic(b2g_matrix* m, int level, double* psi, const double
             for (b2g::DBuf<double>* b : {&A.v64.cpA, &A.v64.cwA, &A.v64.crA, &A.v64.crD}) b->alloc(n, A.stream);
         b2g::DBuf<b2g::k::DevPerf> dp;
         dp.alloc(1, A.stream);
-        A.coarsestSolve<double>(level, psi, source, tolerance, relTol, dp.p, false);
+        A.toPos(level, static_cast<const double*>(psi), A.ioBuf(0));
+        A.toPos(level, source, A.ioBuf(1));
+        A.coarsestSolve<double>(level, A.ioBuf(0), A.ioBuf(1), tolerance, relTol, dp.p, false);
+        A.fromPos(level, static_cast<const double*>(A.ioBuf(0)), psi);
         std::vector<b2g::k::DevPerf> h = dp.download(A.stream);
         out->initialResidual = h[0].initialResidual;
         out->finalResidual = h[0].finalResidual;
@@ -598,7 +627,9 @@ b2g_status b2g_precondition(b2g_matrix* m, const b2g_controls* controls, double*
         need(A.nLevels() > 0, "b2g_precondition: the mesh has no coarse levels");
         A.resetLog(log ? std::max(log->coarsestCapacity, 0) : 0);
         A.serial = controls->reduction == B2G_REDUCTION_SERIAL;
-        A.precondition(*controls, w, r);
+        A.toPos(0, r, A.ioBuf(1));
+        A.precondition(*controls, A.ioBuf(0), A.ioBuf(1));
+        A.fromPos(0, static_cast<const double*>(A.ioBuf(0)), w);
         A.checkDeviceError();
         A.readLog(log);
     });
@@ -610,12 +641,30 @@ static void solveOn(b2g::Matrix& A, const double* source, double* psi, const b2g
     need(c && source && psi && out, "b2g solve: null argument");
     need(memspace == B2G_MEM_HOST || memspace == B2G_MEM_DEVICE, "b2g solve: bad memspace");
     const int n0 = A.n(0);
-    const cudaMemcpyKind in = memspace == B2G_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
-    const cudaMemcpyKind outK = memspace == B2G_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
-    B2G_CUDA(cudaMemcpyAsync(A.source.p, source, sizeof(double) * n0, in, A.stream));
-    B2G_CUDA(cudaMemcpyAsync(A.psi.p, psi, sizeof(double) * n0, in, A.stream));
+    // the solve runs in the finest level's position order: host fields are staged in fc/fr (free
+    // outside a solve) and permuted on the device; device fields are permuted in place of a copy
+    if (memspace == B2G_MEM_HOST)
+    {
+        B2G_CUDA(cudaMemcpyAsync(A.fc.p, source, sizeof(double) * n0, cudaMemcpyHostToDevice, A.stream));
+        B2G_CUDA(cudaMemcpyAsync(A.fr.p, psi, sizeof(double) * n0, cudaMemcpyHostToDevice, A.stream));
+        A.toPos(0, static_cast<const double*>(A.fc.p), A.source.p);
+        A.toPos(0, static_cast<const double*>(A.fr.p), A.psi.p);
+    }
+    else
+    {
+        A.toPos(0, source, A.source.p);
+        A.toPos(0, static_cast<const double*>(psi), A.psi.p);
+    }
     *out = standalone ? A.gamg(*c, log) : A.pcg(*c, log);
-    B2G_CUDA(cudaMemcpyAsync(psi, A.psi.p, sizeof(double) * n0, outK, A.stream));
+    if (memspace == B2G_MEM_HOST)
+    {
+        A.fromPos(0, static_cast<const double*>(A.psi.p), A.fc.p);
+        B2G_CUDA(cudaMemcpyAsync(psi, A.fc.p, sizeof(double) * n0, cudaMemcpyDeviceToHost, A.stream));
+    }
+    else
+    {
+        A.fromPos(0, static_cast<const double*>(A.psi.p), psi);
+    }
     B2G_CUDA(cudaStreamSynchronize(A.stream));
 }
 

@@ -5,6 +5,8 @@
 // copies it to the host and back every V-cycle, device_gamg_solver.cu:549-569). Sums and the DIC
 // substitution run serially on lane 0 in the reference's order (they decide the iteration count);
 // element-wise work is spread over the lanes. Scratch lives in global memory (L1-resident).
+// Vectors and rows are in the level's position order; the serial sums and the DIC passes walk cells
+// and faces in the reference's order through posOf (cell -> position).
 #pragma once
 
 #include "b2g_common.cuh"
@@ -24,13 +26,14 @@ template <class T>
 struct CoarsestArgs
 {
     int n, nF;
-    const int* __restrict__ lower;
+    const int* __restrict__ lower;   // by face, cell ids
     const int* __restrict__ upper;
-    const int* __restrict__ rowStart;
+    const int* __restrict__ posOf;   // cell -> position
+    const int* __restrict__ rowStart;  // rows by position (ldu_kernels.cuh Rows)
     const int* __restrict__ col;
     const T* __restrict__ val;
-    const T* __restrict__ diag;
-    const T* __restrict__ coef;  // LDU upper
+    const T* __restrict__ diag;      // by position
+    const T* __restrict__ coef;      // LDU upper, by face
     const T* source;
     T* psi;
     T* pA;
@@ -69,18 +72,18 @@ __device__ __forceinline__ void warpAmul(const CoarsestArgs<T>& a, const T* x, T
 }
 
 template <class T>
-__device__ __forceinline__ T serialSumProd(int n, const T* x, const T* y)
+__device__ __forceinline__ T serialSumProd(int n, const int* posOf, const T* x, const T* y)
 {
     T s = T(0);
-    for (int i = 0; i < n; ++i) s = addRn(s, mulRn(x[i], y[i]));
+    for (int c = 0; c < n; ++c) s = addRn(s, mulRn(x[posOf[c]], y[posOf[c]]));
     return s;
 }
 
 template <class T>
-__device__ __forceinline__ T serialSumMag(int n, const T* x)
+__device__ __forceinline__ T serialSumMag(int n, const int* posOf, const T* x)
 {
     T s = T(0);
-    for (int i = 0; i < n; ++i) s = addRn(s, fabs(x[i]));
+    for (int c = 0; c < n; ++c) s = addRn(s, fabs(x[posOf[c]]));
     return s;
 }
 
@@ -111,17 +114,19 @@ __global__ void __launch_bounds__(32) coarsestPcgDic(CoarsestArgs<T> a)
     __syncwarp();
     if (lane == 0)
     {
+        const int* po = a.posOf;
         T avg = T(0);
-        for (int c = 0; c < n; ++c) avg = addRn(avg, a.psi[c]);
+        for (int c = 0; c < n; ++c) avg = addRn(avg, a.psi[po[c]]);
         avg = divRn(avg, static_cast<T>(n));
         T sum = T(0);
         for (int c = 0; c < n; ++c)
         {
-            const T t = mulRn(a.pA[c], avg);
-            sum = addRn(sum, addRn(fabs(subRn(a.wA[c], t)), fabs(subRn(a.source[c], t))));
+            const int i = po[c];
+            const T t = mulRn(a.pA[i], avg);
+            sum = addRn(sum, addRn(fabs(subRn(a.wA[i], t)), fabs(subRn(a.source[i], t))));
         }
         const T nf = addRn(sum, PerfConst<T>::small);
-        const T init = divRn(serialSumMag(n, a.rA), nf);
+        const T init = divRn(serialSumMag(n, po, a.rA), nf);
         shScal[0] = nf;
         shScal[1] = init;
         shScal[2] = init;
@@ -130,13 +135,13 @@ __global__ void __launch_bounds__(32) coarsestPcgDic(CoarsestArgs<T> a)
         if (!shStop)
         {
             // DICPreconditioner::calcReciprocalD (GAMG:194-210)
-            for (int c = 0; c < n; ++c) a.rD[c] = a.diag[c];
+            for (int i = 0; i < n; ++i) a.rD[i] = a.diag[i];
             for (int f = 0; f < a.nF; ++f)
             {
-                const int u = a.upper[f];
-                a.rD[u] = subRn(a.rD[u], divRn(mulRn(a.coef[f], a.coef[f]), a.rD[a.lower[f]]));
+                const int u = po[a.upper[f]];
+                a.rD[u] = subRn(a.rD[u], divRn(mulRn(a.coef[f], a.coef[f]), a.rD[po[a.lower[f]]]));
             }
-            for (int c = 0; c < n; ++c) a.rD[c] = divRn(T(1), a.rD[c]);
+            for (int i = 0; i < n; ++i) a.rD[i] = divRn(T(1), a.rD[i]);
         }
     }
     __syncwarp();
@@ -151,17 +156,18 @@ __global__ void __launch_bounds__(32) coarsestPcgDic(CoarsestArgs<T> a)
         if (lane == 0)
         {
             // the two DIC substitution passes (GAMG:212-231)
+            const int* po = a.posOf;
             for (int f = 0; f < a.nF; ++f)
             {
-                const int u = a.upper[f];
-                a.wA[u] = subRn(a.wA[u], mulRn(mulRn(a.rD[u], a.coef[f]), a.wA[a.lower[f]]));
+                const int u = po[a.upper[f]];
+                a.wA[u] = subRn(a.wA[u], mulRn(mulRn(a.rD[u], a.coef[f]), a.wA[po[a.lower[f]]]));
             }
             for (int f = a.nF - 1; f >= 0; --f)
             {
-                const int l = a.lower[f];
-                a.wA[l] = subRn(a.wA[l], mulRn(mulRn(a.rD[l], a.coef[f]), a.wA[a.upper[f]]));
+                const int l = po[a.lower[f]];
+                a.wA[l] = subRn(a.wA[l], mulRn(mulRn(a.rD[l], a.coef[f]), a.wA[po[a.upper[f]]]));
             }
-            shScal[3] = serialSumProd(n, a.wA, a.rA);
+            shScal[3] = serialSumProd(n, po, a.wA, a.rA);
         }
         __syncthreads();
         wArA = shScal[3];
@@ -176,7 +182,7 @@ __global__ void __launch_bounds__(32) coarsestPcgDic(CoarsestArgs<T> a)
         }
         __syncwarp();
         warpAmul(a, a.pA, a.wA);
-        if (lane == 0) shScal[3] = serialSumProd(n, a.wA, a.pA);
+        if (lane == 0) shScal[3] = serialSumProd(n, a.posOf, a.wA, a.pA);
         __syncthreads();
         const T wApA = shScal[3];
         if (divRn(fabs(wApA), nf) < PerfConst<T>::vsmall) break;  // checkSingularity
@@ -189,7 +195,7 @@ __global__ void __launch_bounds__(32) coarsestPcgDic(CoarsestArgs<T> a)
         __syncwarp();
         if (lane == 0)
         {
-            shScal[2] = divRn(serialSumMag(n, a.rA), nf);
+            shScal[2] = divRn(serialSumMag(n, a.posOf, a.rA), nf);
             ++shIter;
             shStop = (shIter >= a.maxIter || convergedT(shScal[2], shScal[1], a.tolerance, a.relTol)) ? 1 : 0;
         }

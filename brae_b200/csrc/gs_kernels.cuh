@@ -8,26 +8,30 @@
 // the faces c owns (neighbours n > c, still at their old values). As a gather per cell, a cell
 // needs only its owners' new values: the sweep is a DAG and a cell's "depth" is its level in it.
 //
-// THE SCHEDULE (part-pipelined, one sweep per launch). Cells are split into P contiguous index
-// ranges ("parts"), one persistent CTA per part. A part's cells are laid out by (depth, cell) and cut
-// into "chunks" of at most M cells of one depth, walked in order.
+// SWEEP ORDER. Every vector of a level is stored in "position" order: cells split into P contiguous
+// index ranges ("parts", one persistent CTA each), each part's cells by (depth, cell). A part walks
+// its positions in order, cut into "chunks" of at most M cells of one depth.
 //
-// WARP ROLES. The compute warps run the chunks through an S-slot shared-memory pipeline: a chunk's
-// contiguous data (cell ids, row offsets, diagonal, entry codes and coefficients, all in position
-// order) is copied with cp.async S-1 chunks ahead; G chunks ahead, once its codes have landed, the
-// gathers it needs that are already final are issued too (b, and kind PRE: old values of upper
-// neighbours, and owners two or more chunks back). Owners the part computed within the last R
-// positions come from a shared-memory ring (kind RING). Only owners held by other parts (and rare
-// far owners one chunk back) are read from global memory at compute time (kind LATE). The service
-// warp takes the two global-memory handshakes off the compute path: it publishes the part's
-// progress word ("every cell of depth < d is done", release at GPU scope) whenever the compute warps
-// report a finished depth through shared memory, and it polls the upstream parts' words and posts
-// their minimum in shared memory, which the compute warps check before a chunk with LATE owners.
+// WHAT A CHUNK READS, AND FROM WHERE.
+//   * Its contiguous data -- diagonal, b, row offsets, entry codes, coefficients -- is copied into
+//     one of S shared-memory slots by TMA bulk copies (cp.async.bulk + mbarrier), S-1 chunks ahead.
+//   * psi itself lives, around the sweep front, in a shared-memory window of W positions: behind the
+//     front the part's NEW values (written as they are computed), ahead of it the OLD values,
+//     streamed in by TMA bulk copies as the front advances. Entry kind WIN reads the window.
+//   * What the window does not hold is gathered G chunks ahead (kind GAT): old values of
+//     neighbours outside the window or in other parts, owners computed long enough ago, and owners
+//     held by other parts -- those only once the upstream parts' progress covers them (else at
+//     compute time, after the wait). Kind SLOW (an owner just outside the window, computed too
+//     recently to gather ahead) is read at compute time.
 //
-// WHY PRE IS SAFE. An upper neighbour n of a cell c has depth(n) > depth(c), so n is rewritten only
-// after c's depth completes: in this part after c's chunk, in another part only after that part saw
-// this part's progress pass depth(c), which is published after c's chunk. c's gathers are issued
-// before c's chunk runs.
+// WARP ROLES. Compute warps run the chunks; one service warp publishes the part's progress word
+// ("every cell of depth < d is done", release at GPU scope) when the compute warps report a depth
+// through shared memory, and polls the upstream parts' words, posting their minimum in shared
+// memory for the compute warps.
+//
+// WHY OLD VALUES MAY BE READ EARLY. A neighbour n of a cell c has depth(n) > depth(c), so n is
+// rewritten only after c's depth completes: in this part after c's chunk, in another part only after
+// that part saw this part's progress pass depth(c), which is published after c's chunk.
 //
 // BOUNDED WAITS. Every spin has a budget; when it runs out the error word is set and every later wait
 // returns at once, so a broken schedule ends the kernel with an error instead of hanging the GPU.
@@ -40,15 +44,24 @@
 namespace b2g {
 namespace k {
 
-constexpr int kRingLog = 12;
-constexpr int kRing = 1 << kRingLog;           // shared-memory ring of recent values (positions)
+constexpr int kWin = 4096;                     // W: psi window (positions), a power of two
+constexpr int kFill = 256;                     // B: window fill block (positions)
 constexpr unsigned kKindShift = 30;
 constexpr unsigned kIdxMask = (1u << kKindShift) - 1u;
-enum : unsigned { KIND_RING = 0u, KIND_PRE = 1u, KIND_LATE = 2u };
+enum : unsigned { KIND_WIN = 0u, KIND_GAT = 1u, KIND_SLOW = 2u };
 constexpr int kStages = 6;                     // S: pipeline slots
-constexpr int kGatherAhead = 2;                // G: chunks ahead the gathers are issued (S >= G + 2)
-constexpr int kRowRegs = 8;                    // row entries resolved into registers before the chain
+constexpr int kGatherAhead = 2;                // G: chunks ahead the gathers are issued
 constexpr long long kSpinLimit = 1LL << 24;    // polls before a wait gives up (~1-2 s with backoff)
+
+// Window extents the schedule guarantees for a chunk starting at s and ending at e: positions
+// [s, s + ahead) hold old values, [e - behind, s) new ones. The fills issued S-1 chunks ahead must
+// not overwrite new values a pending chunk still reads, hence ahead + behind + B + (S-2)*M <= W.
+inline void gsWindowExtents(int M, int& ahead, int& behind)
+{
+    const int room = kWin - kFill - (kStages - 2) * M;
+    ahead = room / 2;
+    behind = room - ahead;
+}
 
 template <class T>
 struct GsArgs
@@ -56,18 +69,20 @@ struct GsArgs
     int nParts;
     int maxCells;                  // M: chunk cell capacity (compute threads)
     int maxEnt;                    // E: chunk entry capacity
+    int ahead;                     // window extent ahead of a chunk's start (positions)
+    int nPadded;                   // psi / b / diag arrays are readable up to here (fill blocks)
     const int* __restrict__ partChunkStart;  // [P+1]
+    const int* __restrict__ partPosStart;    // [P+1]
     const int4* __restrict__ chunkRec;       // [nChunks][2]: {pos0, m, e0, ne}, {depth, needUp, -, -}
     const int* __restrict__ upStart;         // [P+1]
     const int* __restrict__ upList;
     const int* __restrict__ hasDown;         // [P] 1 if another part reads this part's values
-    const int* __restrict__ posCell;         // [n]
-    const int* __restrict__ posRow;          // [n+1] entry offsets in position order
-    const unsigned* __restrict__ entCode;    // [nnz] kind << 30 | index (ring slot or cell)
-    const T* __restrict__ entVal;            // [nnz]
-    const T* __restrict__ posDiag;           // [n]
-    const T* __restrict__ b;                 // by cell
-    T* psi;                                  // by cell, updated in place
+    const int* __restrict__ posRow;          // [n+1] entry offsets in position order (padded)
+    const unsigned* __restrict__ entCode;    // [nnz] kind << 30 | window slot or position (padded)
+    const T* __restrict__ entVal;            // [nnz] (padded)
+    const T* __restrict__ posDiag;           // [n] (padded)
+    const T* __restrict__ b;                 // [n] by position (padded)
+    T* psi;                                  // [n] by position, updated in place (padded)
     unsigned* progress;                      // [P]
     int* err;
     unsigned long long* trace;               // diagnostic: [nChunks][4] clock64 stamps + [P][4] part
@@ -81,30 +96,85 @@ __device__ __forceinline__ unsigned long long globalTimer()
     return t;
 }
 
+__device__ __forceinline__ unsigned smemAddr(const void* p)
+{
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbarInit(unsigned long long* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smemAddr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbarExpectTx(unsigned long long* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbarTryWait(unsigned long long* bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(ok)
+        : "r"(smemAddr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// 1-D TMA bulk copy global -> shared, completing on `bar`. dst, src 16-byte aligned; bytes % 16 == 0.
+__device__ __forceinline__ void tmaLoad(void* dst, const void* src, unsigned bytes, unsigned long long* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smemAddr(dst)),
+                 "l"(src), "r"(bytes), "r"(smemAddr(bar))
+                 : "memory");
+}
+
+// A 16-byte-aligned cover of elements [i0, i0 + cnt) of an array whose base is 16-byte aligned.
+struct Cover
+{
+    const char* src;
+    unsigned bytes;
+    int lead;  // elements between the cover's start and element i0
+};
+template <class E>
+__host__ __device__ __forceinline__ Cover coverOf(const E* base, long long i0, int cnt)
+{
+    const long long b0 = i0 * static_cast<long long>(sizeof(E));
+    const long long b1 = (i0 + cnt) * static_cast<long long>(sizeof(E));
+    const long long a0 = b0 & ~15LL;
+    const long long a1 = (b1 + 15) & ~15LL;
+    Cover c;
+    c.src = reinterpret_cast<const char*>(base) + a0;
+    c.bytes = static_cast<unsigned>(a1 - a0);
+    c.lead = static_cast<int>((b0 - a0) / static_cast<long long>(sizeof(E)));
+    return c;
+}
+
 template <class T>
 struct Slot
 {
-    T* diag;
-    T* b;
-    T* val;
-    T* old;
-    int* cell;
-    int* row;        // M + 1 absolute entry offsets
-    unsigned* code;
+    T* diag;        // M + 8
+    T* b;           // M + 8
+    T* val;         // E + 8
+    T* gat;         // E      (gathered values, by entry)
+    int* row;       // M + 9
+    unsigned* code; // E + 8
 };
+
+// Each TMA destination holds its elements plus up to 8 of cover rounding; every array's byte size
+// is rounded up to 16 so the next one stays 16-byte aligned.
+__host__ __device__ inline size_t r16(size_t b) { return (b + 15) & ~size_t(15); }
 
 template <class T>
 __host__ __device__ inline size_t slotBytes(int M, int E)
 {
-    const size_t b = 2 * sizeof(T) * M + 2 * sizeof(T) * E + sizeof(int) * M + sizeof(int) * (M + 1) +
-                     sizeof(unsigned) * E;
-    return (b + 15) & ~size_t(15);
+    return 2 * r16(sizeof(T) * (M + 8)) + r16(sizeof(T) * (E + 8)) + r16(sizeof(int) * (M + 9)) +
+           r16(sizeof(unsigned) * (E + 8)) + r16(sizeof(T) * E);
 }
 
 template <class T>
 __host__ __device__ inline size_t gsSmemBytes(int M, int E)
 {
-    return sizeof(T) * kRing + kStages * slotBytes<T>(M, E);
+    return sizeof(T) * kWin + kStages * slotBytes<T>(M, E);
 }
 
 template <class T>
@@ -112,13 +182,12 @@ __device__ __forceinline__ Slot<T> slotAt(unsigned char* base, int M, int E)
 {
     Slot<T> s;
     unsigned char* p = base;
-    s.diag = reinterpret_cast<T*>(p); p += sizeof(T) * M;
-    s.b = reinterpret_cast<T*>(p); p += sizeof(T) * M;
-    s.val = reinterpret_cast<T*>(p); p += sizeof(T) * E;
-    s.old = reinterpret_cast<T*>(p); p += sizeof(T) * E;
-    s.cell = reinterpret_cast<int*>(p); p += sizeof(int) * M;
-    s.row = reinterpret_cast<int*>(p); p += sizeof(int) * (M + 1);
-    s.code = reinterpret_cast<unsigned*>(p);
+    s.diag = reinterpret_cast<T*>(p); p += r16(sizeof(T) * (M + 8));
+    s.b = reinterpret_cast<T*>(p); p += r16(sizeof(T) * (M + 8));
+    s.val = reinterpret_cast<T*>(p); p += r16(sizeof(T) * (E + 8));
+    s.row = reinterpret_cast<int*>(p); p += r16(sizeof(int) * (M + 9));
+    s.code = reinterpret_cast<unsigned*>(p); p += r16(sizeof(unsigned) * (E + 8));
+    s.gat = reinterpret_cast<T*>(p);
     return s;
 }
 
@@ -147,17 +216,12 @@ __device__ __forceinline__ ChunkRec loadChunkRec(const int4* __restrict__ recs, 
 __device__ __forceinline__ unsigned ldAcquireCta(const unsigned* p)
 {
     unsigned v;
-    asm volatile("ld.acquire.cta.shared.u32 %0, [%1];"
-                 : "=r"(v)
-                 : "r"(static_cast<unsigned>(__cvta_generic_to_shared(p)))
-                 : "memory");
+    asm volatile("ld.acquire.cta.shared.u32 %0, [%1];" : "=r"(v) : "r"(smemAddr(p)) : "memory");
     return v;
 }
 __device__ __forceinline__ void stReleaseCta(unsigned* p, unsigned v)
 {
-    asm volatile("st.release.cta.shared.u32 [%0], %1;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(p))),
-                 "r"(v)
-                 : "memory");
+    asm volatile("st.release.cta.shared.u32 [%0], %1;" ::"r"(smemAddr(p)), "r"(v) : "memory");
 }
 // a barrier among the compute warps only (named barrier 1)
 __device__ __forceinline__ void computeSync(int nThreads)
@@ -165,17 +229,33 @@ __device__ __forceinline__ void computeSync(int nThreads)
     asm volatile("bar.sync 1, %0;" ::"r"(nThreads) : "memory");
 }
 
-// One Gauss-Seidel sweep of one level. Grid = P parts; blockDim = M compute threads + 32.
+__device__ __forceinline__ void waitMbar(unsigned long long* b, unsigned parity, int* err)
+{
+    long long it = 0;
+    while (!mbarTryWait(b, parity))
+    {
+        if (++it > kSpinLimit)
+        {
+            atomicExch(err, 1);
+            break;
+        }
+    }
+}
+
+// One Gauss-Seidel sweep of one level, in position order. Grid = P parts; blockDim = M + 32.
 template <class T>
 __global__ void __launch_bounds__(512) gsSweep(GsArgs<T> a)
 {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     __shared__ ChunkRec rec[kStages];
-    __shared__ unsigned chunksDone;   // chunks of this part the compute warps have finished
-    __shared__ unsigned upMin;        // least progress seen among the upstream parts
+    __shared__ int gatherEarly[kStages];          // the chunk's gathers were issued ahead
+    __shared__ __align__(8) unsigned long long bar[kStages];
+    __shared__ unsigned chunksDone;               // chunks of this part the compute warps finished
+    __shared__ unsigned upMin;                    // least progress seen among the upstream parts
     const int M = a.maxCells;
     const int E = a.maxEnt;
-    T* ring = reinterpret_cast<T*>(smem);
+    T* win = reinterpret_cast<T*>(smem);
+    unsigned char* slots = smem + sizeof(T) * kWin;
     const size_t sb = slotBytes<T>(M, E);
     const int p = blockIdx.x;
     const int t = threadIdx.x;
@@ -185,6 +265,9 @@ __global__ void __launch_bounds__(512) gsSweep(GsArgs<T> a)
     {
         chunksDone = 0u;
         upMin = 0u;
+        for (int s = 0; s < kStages; ++s) mbarInit(&bar[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     __syncthreads();
 
@@ -240,66 +323,90 @@ __global__ void __launch_bounds__(512) gsSweep(GsArgs<T> a)
     }
 
     // ---------------- compute warps ----------------
-    unsigned char* slots = smem + sizeof(T) * kRing;
     auto slotOf = [&](int j) { return slotAt<T>(slots + (j % kStages) * sb, M, E); };
-    // records of the next two chunks to stage, loaded ahead (no dependent loads on the loop)
-    ChunkRec rq0 = loadChunkRec(a.chunkRec, c0, 0 < nCh);
-    ChunkRec rq1 = loadChunkRec(a.chunkRec, c0 + 1, 1 < nCh);
+    const int partEnd = a.partPosStart[p + 1];
+    const int fillEnd = min(a.nPadded, ((partEnd + kFill - 1) / kFill) * kFill);
+    int filled = (a.partPosStart[p] / kFill) * kFill;  // window filled up to here (thread 0's view)
     unsigned long long* ptrace = a.trace ? a.trace + 4 * (size_t)a.partChunkStart[a.nParts] + 4 * (size_t)p : nullptr;
     if (ptrace && t == 0)
     {
         ptrace[0] = globalTimer();
         ptrace[1] = clock64();
     }
+    ChunkRec rq0 = loadChunkRec(a.chunkRec, c0, 0 < nCh);
+    ChunkRec rq1 = loadChunkRec(a.chunkRec, c0 + 1, 1 < nCh);
     for (int r = -(kStages - 1); r < nCh; ++r)
     {
         if (a.trace && t == 0 && r >= 0) a.trace[4 * (size_t)(c0 + r)] = clock64();
-        // (1) chunk r+G's codes have landed (and chunk r-1 is written: this barrier also ends it)
-        __pipeline_wait_prior(kStages - kGatherAhead - 2);
-        computeSync(M);
+        // (1) chunk r+G's data has landed: its gathers can be issued
+        const int jg = r + kGatherAhead;
+        if (jg >= 0 && jg < nCh)
+        {
+            waitMbar(&bar[jg % kStages], static_cast<unsigned>((jg / kStages) & 1), a.err);
+            if (t == 0)
+            {
+                const int nu = rec[jg % kStages].needUp;
+                gatherEarly[jg % kStages] =
+                    (nu < 0 || ldAcquireCta(&upMin) >= static_cast<unsigned>(nu) + 1u) ? 1 : 0;
+            }
+        }
+        computeSync(M);  // also: chunk r-1 is complete and its slot free
         if (a.trace && t == 0 && r >= 0) a.trace[4 * (size_t)(c0 + r) + 1] = clock64();
         if (t == 0 && r >= 1) stReleaseCta(&chunksDone, static_cast<unsigned>(r));
-        // (2) contiguous stage of chunk r+S-1 into the slot chunk r-1 released
+        // (2) chunk r+S-1: its contiguous data and the window's old values it needs, by TMA
         const int jc = r + kStages - 1;
         if (jc < nCh)
         {
-            const Slot<T> s = slotOf(jc);
-            const ChunkRec cr = rq0;
-            if (t == 0) rec[jc % kStages] = cr;
-            for (int i = t; i < cr.m; i += M)
+            if (t == 0)
             {
-                __pipeline_memcpy_async(&s.cell[i], &a.posCell[cr.pos0 + i], sizeof(int));
-                __pipeline_memcpy_async(&s.diag[i], &a.posDiag[cr.pos0 + i], sizeof(T));
-                __pipeline_memcpy_async(&s.row[i], &a.posRow[cr.pos0 + i], sizeof(int));
-            }
-            if (t == 0) __pipeline_memcpy_async(&s.row[cr.m], &a.posRow[cr.pos0 + cr.m], sizeof(int));
-            for (int e = t; e < cr.ne; e += M)
-            {
-                __pipeline_memcpy_async(&s.code[e], &a.entCode[cr.e0 + e], sizeof(unsigned));
-                __pipeline_memcpy_async(&s.val[e], &a.entVal[cr.e0 + e], sizeof(T));
+                const Slot<T> s = slotOf(jc);
+                const ChunkRec cr = rq0;
+                rec[jc % kStages] = cr;
+                const Cover cd = coverOf(a.posDiag, cr.pos0, cr.m);
+                const Cover cbv = coverOf(a.b, cr.pos0, cr.m);
+                const Cover cro = coverOf(a.posRow, cr.pos0, cr.m + 1);
+                const Cover cco = coverOf(a.entCode, cr.e0, cr.ne);
+                const Cover cva = coverOf(a.entVal, cr.e0, cr.ne);
+                const int target = min(fillEnd, ((cr.pos0 + a.ahead + kFill - 1) / kFill) * kFill);
+                const int nFill = target > filled ? (target - filled) / kFill : 0;
+                const unsigned total = cd.bytes + cbv.bytes + cro.bytes + (cr.ne ? cco.bytes + cva.bytes : 0u) +
+                                       static_cast<unsigned>(nFill) * kFill * sizeof(T);
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                unsigned long long* b = &bar[jc % kStages];
+                mbarExpectTx(b, total);
+                tmaLoad(s.diag, cd.src, cd.bytes, b);
+                tmaLoad(s.b, cbv.src, cbv.bytes, b);
+                tmaLoad(s.row, cro.src, cro.bytes, b);
+                if (cr.ne)
+                {
+                    tmaLoad(s.code, cco.src, cco.bytes, b);
+                    tmaLoad(s.val, cva.src, cva.bytes, b);
+                }
+                for (int f = 0; f < nFill; ++f, filled += kFill)
+                    tmaLoad(win + (filled & (kWin - 1)), a.psi + filled, kFill * sizeof(T), b);
             }
             rq0 = rq1;
             rq1 = loadChunkRec(a.chunkRec, c0 + jc + 2, jc + 2 < nCh);
         }
-        // (3) gathers of chunk r+G: b, and every value already final
-        const int jg = r + kGatherAhead;
-        if (jg >= 0 && jg < nCh)
+        // (3) chunk r+G's gathers, when everything they read is final
+        if (jg >= 0 && jg < nCh && gatherEarly[jg % kStages])
         {
             const Slot<T> s = slotOf(jg);
             const ChunkRec& gr = rec[jg % kStages];
-            for (int i = t; i < gr.m; i += M) __pipeline_memcpy_async(&s.b[i], &a.b[s.cell[i]], sizeof(T));
+            const int lc = coverOf(a.entCode, gr.e0, gr.ne).lead;
             for (int e = t; e < gr.ne; e += M)
             {
-                const unsigned c = s.code[e];
-                if ((c >> kKindShift) == KIND_PRE)
-                    __pipeline_memcpy_async(&s.old[e], &a.psi[c & kIdxMask], sizeof(T));
+                const unsigned c = s.code[lc + e];
+                if ((c >> kKindShift) == KIND_GAT) __pipeline_memcpy_async(&s.gat[e], &a.psi[c & kIdxMask], sizeof(T));
             }
         }
         __pipeline_commit();
         if (r < 0) continue;
-        // (4) chunk r's data in place; the parts holding its LATE owners far enough along
+        // (4) chunk r: its data, its gathers, and the parts holding its owners far enough along
         __pipeline_wait_prior(kGatherAhead);
-        const ChunkRec& cr = rec[r % kStages];
+        const ChunkRec cr = rec[r % kStages];
+        waitMbar(&bar[r % kStages], static_cast<unsigned>((r / kStages) & 1), a.err);
+        const bool early = gatherEarly[r % kStages] != 0;
         if (t == 0 && cr.needUp >= 0)
         {
             const unsigned target = static_cast<unsigned>(cr.needUp) + 1u;
@@ -316,37 +423,54 @@ __global__ void __launch_bounds__(512) gsSweep(GsArgs<T> a)
             }
         }
         computeSync(M);
-        if (a.trace && t == 0) a.trace[4 * (size_t)(c0 + r) + 2] = clock64();
-        // (5) the sweep: resolve the row's values first, then the reference's rounding chain
         const Slot<T> s = slotOf(r);
+        const int lc = coverOf(a.entCode, cr.e0, cr.ne).lead;
+        const int lv = coverOf(a.entVal, cr.e0, cr.ne).lead;
+        if (!early)
+        {
+            // the upstream parts were not far enough along when the gathers were due
+            for (int e = t; e < cr.ne; e += M)
+            {
+                const unsigned c = s.code[lc + e];
+                if ((c >> kKindShift) == KIND_GAT) s.gat[e] = ldcg(&a.psi[c & kIdxMask]);
+            }
+            computeSync(M);
+        }
+        if (a.trace && t == 0) a.trace[4 * (size_t)(c0 + r) + 2] = clock64();
+        // (5) the sweep: the row's values first, then the reference's rounding chain
         if (t < cr.m)
         {
-            const int rb = s.row[t] - cr.e0;
-            const int re = s.row[t + 1] - cr.e0;
-            T acc = s.b[t];
-            for (int e0 = rb; e0 < re; e0 += kRowRegs)
+            const int ld = coverOf(a.posDiag, cr.pos0, cr.m).lead;
+            const int lb = coverOf(a.b, cr.pos0, cr.m).lead;
+            const int lr = coverOf(a.posRow, cr.pos0, cr.m + 1).lead;
+            const int rb = s.row[lr + t] - cr.e0;
+            const int re = s.row[lr + t + 1] - cr.e0;
+            T acc = s.b[lb + t];
+            constexpr int kRegs = 8;
+            for (int e0 = rb; e0 < re; e0 += kRegs)
             {
-                T v[kRowRegs], w[kRowRegs];
+                T v[kRegs], w[kRegs];
 #pragma unroll
-                for (int q = 0; q < kRowRegs; ++q)
+                for (int q = 0; q < kRegs; ++q)
                 {
                     const int e = e0 + q;
                     if (e < re)
                     {
-                        const unsigned c = s.code[e];
+                        const unsigned c = s.code[lc + e];
                         const unsigned kind = c >> kKindShift;
                         const unsigned idx = c & kIdxMask;
-                        w[q] = s.val[e];
-                        v[q] = kind == KIND_RING ? ring[idx] : (kind == KIND_PRE ? s.old[e] : ldcg(&a.psi[idx]));
+                        w[q] = s.val[lv + e];
+                        v[q] = kind == KIND_WIN ? win[idx] : (kind == KIND_GAT ? s.gat[e] : ldcg(&a.psi[idx]));
                     }
                 }
 #pragma unroll
-                for (int q = 0; q < kRowRegs; ++q)
+                for (int q = 0; q < kRegs; ++q)
                     if (e0 + q < re) acc = subRn(acc, mulRn(w[q], v[q]));
             }
-            const T res = divRn(acc, s.diag[t]);
-            a.psi[s.cell[t]] = res;
-            ring[(cr.pos0 + t) & (kRing - 1)] = res;
+            const T res = divRn(acc, s.diag[ld + t]);
+            const int pos = cr.pos0 + t;
+            a.psi[pos] = res;
+            win[pos & (kWin - 1)] = res;
         }
         if (a.trace && t == 0) a.trace[4 * (size_t)(c0 + r) + 3] = clock64();
     }

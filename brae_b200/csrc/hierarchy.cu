@@ -488,6 +488,33 @@ __global__ void kChunkRecs(int nCh, const int* __restrict__ chunkStart, const in
     r[7] = 0;
 }
 
+__global__ void kStepCounts(int nCoarse, const int* __restrict__ posCellC, const int* __restrict__ cellStart,
+                            int* __restrict__ cnt)
+{
+    const int P = blockIdx.x * blockDim.x + threadIdx.x;
+    if (P >= nCoarse) return;
+    const int C = posCellC[P];
+    cnt[P] = cellStart[C + 1] - cellStart[C];
+}
+
+__global__ void kStepLists(int nCoarse, const int* __restrict__ posCellC, const int* __restrict__ cellStart,
+                           const int* __restrict__ cellList, const int* __restrict__ posOfF,
+                           const int* __restrict__ rStartP, int* __restrict__ rListP)
+{
+    const int P = blockIdx.x * blockDim.x + threadIdx.x;
+    if (P >= nCoarse) return;
+    const int C = posCellC[P];
+    int k = rStartP[P];
+    for (int e = cellStart[C]; e < cellStart[C + 1]; ++e) rListP[k++] = posOfF[cellList[e]];
+}
+
+__global__ void kProlongMap(int nFine, const int* __restrict__ posCellF, const int* __restrict__ restrictAddr,
+                            const int* __restrict__ posOfC, int* __restrict__ prolongP)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nFine) prolongP[i] = posOfC[restrictAddr[posCellF[i]]];
+}
+
 __global__ void kPosOf(int n, const int* __restrict__ order, int* __restrict__ posOf)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -514,24 +541,27 @@ __global__ void kChunkOfPos(int n, int nChunks, const int* __restrict__ chunkSta
     chunkOf[i] = lo;
 }
 
-// entry codes in position order: RING (an owner this part computed within the ring window),
-// PRE (final before the chunk's stage is issued: every upper neighbour, and owners of this part two
-// or more chunks back), LATE (owners of other parts, and the rare far owner one chunk back)
-__global__ void kEntryCodes(int n, int ring, const int* __restrict__ order, const int* __restrict__ posOf,
+// Entry codes in position order (gs_kernels.cuh): WIN -- a value the part's shared-memory window
+// holds when the chunk runs (an owner of this part within `behind` positions of the chunk's end, or a
+// neighbour of this part within `ahead` positions of its start); GAT -- gathered ahead (neighbours
+// elsewhere, owners of this part at least G+1 chunks back, owners of other parts once their progress
+// covers them); SLOW -- read at compute time (an owner of this part outside the window and too recent).
+__global__ void kEntryCodes(int n, int win, int ahead, int behind, int gatherAhead,
+                            const int* __restrict__ order, const int* __restrict__ posOf,
                             const int* __restrict__ partOf, const int* __restrict__ depth,
                             const int* __restrict__ chunkOf, const int* __restrict__ chunkStart,
                             const int* __restrict__ posRow, const int* __restrict__ rowStart,
                             const int* __restrict__ losortStart, const int* __restrict__ col,
                             const int* __restrict__ entFace, unsigned* __restrict__ entCode,
-                            int* __restrict__ entFacePos, int* __restrict__ chunkNeedUp,
-                            unsigned* __restrict__ upBits, int words)
+                            int* __restrict__ entFacePos, int* __restrict__ entColPos,
+                            int* __restrict__ chunkNeedUp, unsigned* __restrict__ upBits, int words)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int c = order[i];
     const int p = partOf[c];
-    const int d = depth[c];
     const int ch = chunkOf[i];
+    const int chBeg = chunkStart[ch];
     const int chEnd = chunkStart[ch + 1];
     const int rb = rowStart[c];
     const int nLower = losortStart[c + 1] - losortStart[c];
@@ -540,21 +570,17 @@ __global__ void kEntryCodes(int n, int ring, const int* __restrict__ order, cons
     {
         const int k = e - rb;
         const int o = col[e];
+        const int q = posOf[o];
+        const bool same = partOf[o] == p;
         unsigned code;
         if (k < nLower)
         {
-            if (partOf[o] == p)
-            {
-                // the owner's chunk precedes this one; its stage is issued one chunk ahead, so
-                // the owner may be prefetched only when it sits two or more chunks back
-                const int q = posOf[o];
-                if (chEnd - q <= ring) code = (0u << 30) | static_cast<unsigned>(q & (ring - 1));
-                else if (chunkOf[q] <= ch - 2) code = (1u << 30) | static_cast<unsigned>(o);
-                else code = (2u << 30) | static_cast<unsigned>(o);
-            }
+            if (same && q >= chEnd - behind) code = (0u << 30) | static_cast<unsigned>(q & (win - 1));
+            else if (same && chunkOf[q] <= ch - gatherAhead - 1) code = (1u << 30) | static_cast<unsigned>(q);
+            else if (same) code = (2u << 30) | static_cast<unsigned>(q);
             else
             {
-                code = (2u << 30) | static_cast<unsigned>(o);
+                code = (1u << 30) | static_cast<unsigned>(q);
                 atomicMax(&chunkNeedUp[ch], depth[o]);
                 const int po = partOf[o];
                 atomicOr(&upBits[(size_t)p * words + (po >> 5)], 1u << (po & 31));
@@ -562,10 +588,12 @@ __global__ void kEntryCodes(int n, int ring, const int* __restrict__ order, cons
         }
         else
         {
-            code = (1u << 30) | static_cast<unsigned>(o);
+            if (same && q < chBeg + ahead) code = (0u << 30) | static_cast<unsigned>(q & (win - 1));
+            else code = (1u << 30) | static_cast<unsigned>(q);
         }
         entCode[base + k] = code;
         entFacePos[base + k] = entFace[e];
+        entColPos[base + k] = q;
     }
 }
 
@@ -885,6 +913,7 @@ void buildHierarchy(Mesh& M, const double* dSf, const double* dMagSf, int nCells
     }
     *forward = fwd;
     for (auto& L : M.lev) buildGsSchedule(L, s);
+    for (int i = 0; i < M.nLevels(); ++i) buildStepMaps(M, i);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -970,13 +999,14 @@ void buildGsSchedule(LevelAddr& L, cudaStream_t s)
     kLevelInfo<<<grid(n), TPB, 0, s>>>(n, stride, skeys.p, head.p, lvlScan.p, lvlStart.p, lvlDepth.p, lvlPart.p);
     B2G_LAUNCH_CHECK();
     // row layout in position order
-    DBuf<int> posOf, rowLen;
-    posOf.alloc(n, s);
+    DBuf<int> rowLen;
+    G.posOf.alloc(n, s);
     rowLen.alloc(n, s);
-    kPosOf<<<grid(n), TPB, 0, s>>>(n, G.posCell.p, posOf.p);
+    kPosOf<<<grid(n), TPB, 0, s>>>(n, G.posCell.p, G.posOf.p);
     kPosRowLen<<<grid(n), TPB, 0, s>>>(n, G.posCell.p, L.rowStart.p, rowLen.p);
     B2G_LAUNCH_CHECK();
-    G.posRow.alloc(n + 1, s);
+    G.posRow.alloc(n + 1 + 8, s);
+    G.posRow.zero(s);
     exclusiveScan(rowLen.p, G.posRow.p, n, s);
     // chunks: cut each group by cells and entries so a chunk's stage fits in shared memory
     const std::vector<int> hLvlStart = lvlStart.download(s);
@@ -988,17 +1018,29 @@ void buildGsSchedule(LevelAddr& L, cudaStream_t s)
         maxGroup = std::max(maxGroup, (g + 1 < nLvl ? hLvlStart[g + 1] : n) - hLvlStart[g]);
     for (int i = 0; i < n; ++i) maxRow = std::max(maxRow, hPosRow[i + 1] - hPosRow[i]);
     // chunk capacity: as many cells as the widest (part, depth) group, within what S pipeline slots
-    // of shared memory hold (M compute threads + one service warp per CTA)
+    // and the psi window of shared memory hold (M compute threads + one service warp per CTA), and
+    // leaving the window room ahead of and behind a chunk
+    // (entries are budgeted at the average row length plus a margin, at most the longest row: a chunk
+    // with longer rows simply holds fewer cells)
     const size_t smemCap = 200 * 1024;
-    const int rowCap = std::max(maxRow, 1);
+    const int nnz = hPosRow[n];
+    const int avgRow = static_cast<int>((5LL * nnz + 4LL * n - 1) / (4LL * n));  // ceil(1.25 * nnz / n)
+    const int rowCap = std::max(1, std::min(maxRow, avgRow));
     int M = std::min(480, std::max(32, ((maxGroup + 31) / 32) * 32));
-    while (M > 32 && k::gsSmemBytes<double>(M, M * rowCap) > smemCap) M -= 32;
-    int E = M * rowCap;
-    while (E > rowCap && k::gsSmemBytes<double>(M, E) > smemCap) E -= rowCap;
-    if (maxRow > E || k::gsSmemBytes<double>(M, E) > smemCap)
+    auto fits = [&](int m, int e) {
+        int ah, bh;
+        k::gsWindowExtents(m, ah, bh);
+        return k::gsSmemBytes<double>(m, e) <= smemCap && ah >= m && bh >= m;
+    };
+    while (M > 32 && !fits(M, std::max(M * rowCap, maxRow))) M -= 32;
+    int E = std::max(M * rowCap, maxRow);
+    if (!fits(M, E))
         fail(B2G_ERR_ARGUMENT, "b2g: a cell has more faces than the Gauss-Seidel pipeline holds.");
     G.maxCells = M;
     G.maxEnt = E;
+    k::gsWindowExtents(M, G.ahead, G.behind);
+    G.nPadded = ((n + k::kFill - 1) / k::kFill) * k::kFill;
+    G.nAlloc = G.nPadded + k::kFill;
     std::vector<int> hChunkStart, hChunkDepth, hPartChunk(P + 1, 0);
     for (int g = 0; g < nLvl; ++g)
     {
@@ -1019,26 +1061,30 @@ void buildGsSchedule(LevelAddr& L, cudaStream_t s)
     hChunkStart.push_back(n);
     for (int p = 0; p < P; ++p) hPartChunk[p + 1] += hPartChunk[p];
     G.nChunks = nCh;
-    G.chunkStart.upload(hChunkStart.data(), hChunkStart.size(), s);
-    G.chunkDepth.upload(hChunkDepth.data(), hChunkDepth.size(), s);
+    DBuf<int> chunkStart, chunkDepth, chunkNeedUp;
+    chunkStart.upload(hChunkStart.data(), hChunkStart.size(), s);
+    chunkDepth.upload(hChunkDepth.data(), hChunkDepth.size(), s);
     G.partChunkStart.upload(hPartChunk.data(), hPartChunk.size(), s);
-    G.chunkNeedUp.alloc(nCh, s);
-    kFillInt<<<grid(nCh), TPB, 0, s>>>(G.chunkNeedUp.p, nCh, -1);
+    chunkNeedUp.alloc(nCh, s);
+    kFillInt<<<grid(nCh), TPB, 0, s>>>(chunkNeedUp.p, nCh, -1);
     DBuf<int> chunkOf;
     chunkOf.alloc(n, s);
-    kChunkOfPos<<<grid(n), TPB, 0, s>>>(n, nCh, G.chunkStart.p, chunkOf.p);
+    kChunkOfPos<<<grid(n), TPB, 0, s>>>(n, nCh, chunkStart.p, chunkOf.p);
     const int words = (P + 31) / 32;
     DBuf<unsigned> upBits;
     upBits.alloc(static_cast<size_t>(P) * words, s);
     upBits.zero(s);
-    G.entCode.alloc(2 * (size_t)L.nFaces, s);
+    G.entCode.alloc(2 * (size_t)L.nFaces + 8, s);
+    G.entCode.zero(s);
     G.entFacePos.alloc(2 * (size_t)L.nFaces, s);
-    kEntryCodes<<<grid(n), TPB, 0, s>>>(n, k::kRing, G.posCell.p, posOf.p, partOf.p, G.depth.p, chunkOf.p,
-                                        G.chunkStart.p, G.posRow.p, L.rowStart.p, L.losortStart.p, L.col.p,
-                                        L.entFace.p, G.entCode.p, G.entFacePos.p, G.chunkNeedUp.p, upBits.p, words);
+    G.entColPos.alloc(2 * (size_t)L.nFaces, s);
+    kEntryCodes<<<grid(n), TPB, 0, s>>>(n, k::kWin, G.ahead, G.behind, k::kGatherAhead, G.posCell.p, G.posOf.p,
+                                        partOf.p, G.depth.p, chunkOf.p, chunkStart.p, G.posRow.p, L.rowStart.p,
+                                        L.losortStart.p, L.col.p, L.entFace.p, G.entCode.p, G.entFacePos.p,
+                                        G.entColPos.p, chunkNeedUp.p, upBits.p, words);
     B2G_LAUNCH_CHECK();
     G.chunkRec.alloc(8 * (size_t)nCh, s);
-    kChunkRecs<<<grid(nCh), TPB, 0, s>>>(nCh, G.chunkStart.p, G.posRow.p, G.chunkDepth.p, G.chunkNeedUp.p,
+    kChunkRecs<<<grid(nCh), TPB, 0, s>>>(nCh, chunkStart.p, G.posRow.p, chunkDepth.p, chunkNeedUp.p,
                                          G.chunkRec.p);
     B2G_LAUNCH_CHECK();
     std::vector<unsigned> hUp = upBits.download(s);
@@ -1056,9 +1102,29 @@ void buildGsSchedule(LevelAddr& L, cudaStream_t s)
     G.upStart.upload(upStart.data(), upStart.size(), s);
     if (upList.empty()) upList.push_back(0);
     G.upList.upload(upList.data(), upList.size(), s);
+    G.partPosStart = std::move(dPartStart);
     G.progress.alloc(P, s);
     G.progress.zero(s);
     B2G_CUDA(cudaStreamSynchronize(s));
+}
+
+void buildStepMaps(Mesh& M, int i)
+{
+    cudaStream_t s = M.stream;
+    Step& S = M.step[i];
+    const GsSchedule& F = M.lev[i].gs;
+    const GsSchedule& C = M.lev[i + 1].gs;
+    DBuf<int> cnt;
+    cnt.alloc(S.nCoarse, s);
+    kStepCounts<<<grid(S.nCoarse), TPB, 0, s>>>(S.nCoarse, C.posCell.p, S.cellStart.p, cnt.p);
+    S.rStartP.alloc(S.nCoarse + 1, s);
+    exclusiveScan(cnt.p, S.rStartP.p, S.nCoarse, s);
+    S.rListP.alloc(S.nFine, s);
+    kStepLists<<<grid(S.nCoarse), TPB, 0, s>>>(S.nCoarse, C.posCell.p, S.cellStart.p, S.cellList.p, F.posOf.p,
+                                               S.rStartP.p, S.rListP.p);
+    S.prolongP.alloc(S.nFine, s);
+    kProlongMap<<<grid(S.nFine), TPB, 0, s>>>(S.nFine, F.posCell.p, S.restrictAddr.p, C.posOf.p, S.prolongP.p);
+    B2G_LAUNCH_CHECK();
 }
 
 const DeviceInfo& DeviceInfo::get()

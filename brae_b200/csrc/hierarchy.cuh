@@ -6,11 +6,11 @@
 
 namespace b2g {
 
-// Forward Gauss-Seidel schedule of one level for the part-pipelined sweep kernel (gs_kernels.cuh).
-// Cells are split into `nParts` contiguous index ranges; each part lists its cells by (depth, cell),
-// depth being the cell's level in the forward DAG (a cell depends on the owners of the faces it is
-// the neighbour of). Positions are indices into that (part, depth, cell) order; a part's positions
-// are cut into chunks of at most maxCells cells and maxEnt row entries of one depth.
+// The sweep order of one level and its Gauss-Seidel schedule (gs_kernels.cuh). Cells are split into
+// `nParts` contiguous index ranges; each part lists its cells by (depth, cell), depth being the cell's
+// level in the forward DAG (a cell depends on the owners of the faces it is the neighbour of).
+// "Positions" index that (part, depth, cell) order, and EVERY device vector of the level is stored in
+// position order. A part's positions are cut into chunks of at most maxCells cells of one depth.
 struct GsSchedule
 {
     int nParts = 0;
@@ -18,18 +18,22 @@ struct GsSchedule
     int nChunks = 0;
     int maxCells = 0;          // chunk cell capacity == the kernel's compute threads
     int maxEnt = 0;            // chunk entry capacity
-    DBuf<int> depth;           // [nCells]
+    int ahead = 0;             // window extents the entry codes assume (gsWindowExtents)
+    int behind = 0;
+    int nPadded = 0;           // position count rounded up to the window fill block
+    int nAlloc = 0;            // allocation length of every position-ordered vector of the level
+    DBuf<int> depth;           // [nCells] by cell
     DBuf<int> partChunkStart;  // [nParts+1]
-    DBuf<int> chunkStart;      // [nChunks+1] positions
-    DBuf<int> chunkDepth;      // [nChunks]
-    DBuf<int> chunkNeedUp;     // [nChunks] deepest owner held by another part, -1 if none
-    DBuf<int> chunkRec;        // [nChunks][8]: pos0, m, e0, ne, depth, needUp, 0, 0 (the kernel's records)
+    DBuf<int> partPosStart;    // [nParts+1] (a part's positions are its cell range)
+    DBuf<int> chunkRec;        // [nChunks][8]: pos0, m, e0, ne, depth, needUp, 0, 0
     DBuf<int> upStart;         // [nParts+1] upstream parts of each part
     DBuf<int> upList;
     DBuf<int> hasDown;         // [nParts] 1 if another part reads this part's new values
     DBuf<int> posCell;         // [nCells] cell at each position
-    DBuf<int> posRow;          // [nCells+1] entry offsets in position order
-    DBuf<unsigned> entCode;    // [2*nFaces] kind << 30 | ring slot or cell
+    DBuf<int> posOf;           // [nCells] position of each cell
+    DBuf<int> posRow;          // [nCells+1 (+pad)] entry offsets in position order
+    DBuf<int> entColPos;       // [2*nFaces] the other cell's position, per entry in position order
+    DBuf<unsigned> entCode;    // [2*nFaces (+pad)] Gauss-Seidel codes: kind << 30 | window slot or position
     DBuf<int> entFacePos;      // [2*nFaces] face of each entry (fills the coefficients per solve)
     DBuf<unsigned> progress;   // [nParts] per-part progress words (reset before each launch)
 };
@@ -68,6 +72,10 @@ struct Step
     DBuf<int> faceBeg;        // [nCoarseFaces] coarse face -> fine faces [faceBeg, faceEnd) of faceList
     DBuf<int> faceEnd;
     DBuf<int> faceList;       // fine faces, grouped by coarse face, ascending within a group
+    // the same maps on the two levels' position orders
+    DBuf<int> rStartP;        // [nCoarse+1] coarse position -> its fine positions in rListP
+    DBuf<int> rListP;         // [nFine] fine positions, in ascending fine-cell order per coarse cell
+    DBuf<int> prolongP;       // [nFine] fine position -> coarse position
 };
 
 struct Mesh
@@ -83,8 +91,10 @@ struct Mesh
 // Builds the derived layouts of `L` from its lower/upper (already on the device). Validates the
 // upper-triangular order (faces sorted by owner, owner < neighbour).
 void buildLevelLayouts(LevelAddr& L, cudaStream_t s);
-// The GS schedule of `L` (depths and parts).
+// The sweep order and Gauss-Seidel schedule of `L` (depths, parts, positions, chunks, codes).
 void buildGsSchedule(LevelAddr& L, cudaStream_t s);
+// The position-ordered restriction and prolongation maps of step `i` (both levels scheduled).
+void buildStepMaps(Mesh& M, int i);
 // The whole agglomeration (faceAreaPairGamgAgglomeration) from device arrays.
 void buildHierarchy(Mesh& M, const double* dSf, const double* dMagSf, int nCellsInCoarsestLevel,
                     int* forward);

@@ -21,9 +21,12 @@ template <> struct Small<float>
     static constexpr float vsmall = 1e-37f;
 };
 
-// Rows of one level: for cell c the entries [rowStart[c], rowStart[c+1]) hold first the faces c
-// is the neighbour of, then the faces it owns, each ascending -- the order in which lduMatrix::Amul
-// and lduMatrix::residual add a cell's terms (GAMG:62-117). `val` is the coefficient per entry.
+// Rows of one level, in the level's position (sweep) order: for the cell at position i the entries
+// [rowStart[i], rowStart[i+1]) hold first the faces the cell is the neighbour of, then the faces it
+// owns, each ascending -- the order in which lduMatrix::Amul and lduMatrix::residual add a cell's
+// terms (GAMG:62-117). `col` is the other cell's position, `val` the coefficient per entry, `diag`
+// the diagonal by position. Every per-cell result is the reference's bit for bit; only where the
+// cells sit in memory differs.
 template <class T>
 struct Rows
 {
@@ -150,7 +153,7 @@ __global__ void addInPlace(int n, T* __restrict__ psi, const T* __restrict__ cor
 }
 
 // restrictField (GAMG:410-419): cf = 0; cf[map[i]] += ff[i] for ascending i -- gathered per coarse
-// cell over its fine cells in ascending order
+// cell over its fine cells in ascending fine-cell order (lists of positions on both levels)
 template <class T>
 __global__ void restrictField(int nCoarse, const int* __restrict__ cellStart, const int* __restrict__ cellList,
                               const T* __restrict__ ff, T* __restrict__ cf)
@@ -217,6 +220,18 @@ __global__ void castArray(long long n, const S* __restrict__ in, T* __restrict__
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x)
         out[i] = static_cast<T>(in[i]);
+}
+
+// natural cell order <-> position order: pos[i] = nat[posCell[i]] and back
+template <class T>
+__global__ void toPositions(int n, const int* __restrict__ posCell, const T* __restrict__ nat, T* __restrict__ pos)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) pos[i] = nat[posCell[i]];
+}
+template <class T>
+__global__ void fromPositions(int n, const int* __restrict__ posCell, const T* __restrict__ pos, T* __restrict__ nat)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) nat[posCell[i]] = pos[i];
 }
 
 // lduMatrix::residual (GAMG:90-117): r = source - diag*psi, then minus the face terms in order
@@ -293,20 +308,22 @@ __global__ void __launch_bounds__(NT) normFactorPartial(Rows<T> A, const T* __re
     if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
-// Serial reductions in the reference's order: one warp streams the terms, lane 0 adds them one
-// after another (s = ((s + t0) + t1) + ...), exactly as the reference's host loops do.
+// Serial reductions in the reference's order: one warp streams the terms in cell order (the value of
+// cell c sits at position posOf[c]), lane 0 adds them one after another (s = ((s + t0) + t1) + ...),
+// exactly as the reference's host loops do.
 template <int OP>
 __global__ void __launch_bounds__(32) serialReduce(int n, const double* __restrict__ a, const double* __restrict__ b,
-                                                   double* __restrict__ out)
+                                                   const int* __restrict__ posOf, double* __restrict__ out)
 {
     const int lane = threadIdx.x;
     double s = 0.0;
     for (int base = 0; base < n; base += 32)
     {
-        const int i = base + lane;
+        const int c = base + lane;
         double term = 0.0;
-        if (i < n)
+        if (c < n)
         {
+            const int i = posOf[c];
             if (OP == RED_DOT) term = __dmul_rn(a[i], b[i]);
             else if (OP == RED_SUMMAG) term = fabs(a[i]);
             else term = a[i];
@@ -324,16 +341,17 @@ __global__ void __launch_bounds__(32) serialReduce(int n, const double* __restri
 // scale's two sums in one serial pass: num += field*source, den += field*Acf
 static __global__ void __launch_bounds__(32) serialScaleDots(int n, const double* __restrict__ field,
                                                       const double* __restrict__ source, const double* __restrict__ Acf,
-                                                      double* __restrict__ sf)
+                                                      const int* __restrict__ posOf, double* __restrict__ sf)
 {
     const int lane = threadIdx.x;
     double num = 0.0, den = 0.0;
     for (int base = 0; base < n; base += 32)
     {
-        const int i = base + lane;
+        const int c = base + lane;
         double tn = 0.0, td = 0.0;
-        if (i < n)
+        if (c < n)
         {
+            const int i = posOf[c];
             tn = __dmul_rn(field[i], source[i]);
             td = __dmul_rn(field[i], Acf[i]);
         }
@@ -355,14 +373,14 @@ static __global__ void __launch_bounds__(32) serialScaleDots(int n, const double
 // normFactor's sum in the reference's order (GAMG:146-157), with sumA from the rows
 static __global__ void __launch_bounds__(32) serialNormFactor(Rows<double> A, const double* __restrict__ psi,
                                                        const double* __restrict__ source, const double* __restrict__ Apsi,
-                                                       double* __restrict__ out)
+                                                       const int* __restrict__ posOf, double* __restrict__ out)
 {
     const int lane = threadIdx.x;
     double sumPsi = 0.0;
     for (int base = 0; base < A.n; base += 32)
     {
         const int i = base + lane;
-        const double v = i < A.n ? psi[i] : 0.0;
+        const double v = i < A.n ? psi[posOf[i]] : 0.0;
         const int cnt = min(32, A.n - base);
         for (int j = 0; j < cnt; ++j)
         {
@@ -378,10 +396,11 @@ static __global__ void __launch_bounds__(32) serialNormFactor(Rows<double> A, co
         double term = 0.0;
         if (c < A.n)
         {
-            double sumA = A.diag[c];
-            for (int e = A.rowStart[c]; e < A.rowStart[c + 1]; ++e) sumA = __dadd_rn(sumA, A.val[e]);
+            const int i = posOf[c];
+            double sumA = A.diag[i];
+            for (int e = A.rowStart[i]; e < A.rowStart[i + 1]; ++e) sumA = __dadd_rn(sumA, A.val[e]);
             const double t = __dmul_rn(sumA, xRef);
-            term = __dadd_rn(fabs(__dsub_rn(Apsi[c], t)), fabs(__dsub_rn(source[c], t)));
+            term = __dadd_rn(fabs(__dsub_rn(Apsi[i], t)), fabs(__dsub_rn(source[i], t)));
         }
         const int cnt = min(32, A.n - base);
         for (int j = 0; j < cnt; ++j)

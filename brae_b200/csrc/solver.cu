@@ -131,10 +131,10 @@ bool convergedH(double fin, double init, double tol, double relTol)
 template <class T>
 k::Rows<T> rowsOf(const LevelAddr& L, const LevelCoef<T>& C)
 {
-    return k::Rows<T>{L.nCells, L.rowStart.p, L.col.p, C.val.p, C.diag.p};
+    return k::Rows<T>{L.nCells, L.gs.posRow.p, L.gs.entColPos.p, C.gsVal.p, C.gsDiag.p};
 }
 
-// the Gauss-Seidel layout of one level's coefficients (position order)
+// the position-ordered coefficients of one level
 template <class T>
 __global__ void kGsLayout(int n, long long nnz, const int* __restrict__ posCell, const int* __restrict__ entFacePos,
                           const T* __restrict__ diag, const T* __restrict__ upper, T* __restrict__ gsDiag,
@@ -149,15 +149,25 @@ __global__ void kGsLayout(int n, long long nnz, const int* __restrict__ posCell,
     }
 }
 
+// (+8 elements of zeroed padding: the sweep's bulk copies round their extents up to 16 bytes)
 template <class T>
-void fillGsLayout(const LevelAddr& L, LevelCoef<T>& C, cudaStream_t s)
+void allocGsLayout(const LevelAddr& L, LevelCoef<T>& C, cudaStream_t s)
 {
-    C.gsDiag.alloc(L.nCells, s);
-    C.gsVal.alloc(2 * (size_t)L.nFaces, s);
+    C.gsDiag.alloc(L.nCells + 8, s);
+    C.gsVal.alloc(2 * (size_t)L.nFaces + 8, s);
+    C.gsDiag.zero(s);
+    C.gsVal.zero(s);
+}
+
+void fillGsLayout(const LevelAddr& L, LevelCoef<double>& C, cudaStream_t s)
+{
+    allocGsLayout(L, C, s);
     const long long nnz = 2LL * L.nFaces;
     const long long m = std::max<long long>(L.nCells, nnz);
-    if (m) kGsLayout<T><<<std::min(ceilDiv(m, NT), 8192), NT, 0, s>>>(L.nCells, nnz, L.gs.posCell.p, L.gs.entFacePos.p,
-                                                                       C.diag.p, C.upper.p, C.gsDiag.p, C.gsVal.p);
+    if (m)
+        kGsLayout<double><<<std::min(ceilDiv(m, NT), 8192), NT, 0, s>>>(L.nCells, nnz, L.gs.posCell.p,
+                                                                         L.gs.entFacePos.p, C.diag.p, C.upper.p,
+                                                                         C.gsDiag.p, C.gsVal.p);
     B2G_LAUNCH_CHECK();
 }
 
@@ -266,7 +276,7 @@ template <> VCycleData<float>& Matrix::data<float>() { return v32; }
 
 Matrix::Matrix(Mesh* m, cudaStream_t s) : mesh(m), stream(s)
 {
-    const int n0 = m->lev[0].nCells;
+    const size_t n0 = nAlloc(0);
     for (DBuf<double>* b : {&psi, &source, &rA, &wA, &pA, &AwA, &fc, &fr}) b->alloc(n0, s);
     scal.alloc(1, s);
     scal.zero(s);
@@ -289,11 +299,6 @@ void Matrix::setFine(const double* diag, const double* upper, int memspace)
     C.upper.alloc(L.nFaces, stream);
     B2G_CUDA(cudaMemcpyAsync(C.diag.p, diag, sizeof(double) * L.nCells, kind, stream));
     if (L.nFaces) B2G_CUDA(cudaMemcpyAsync(C.upper.p, upper, sizeof(double) * L.nFaces, kind, stream));
-    C.val.alloc(2 * (size_t)L.nFaces, stream);
-    if (L.nFaces)
-        k::gatherVal<double, double><<<std::min(ceilDiv(2LL * L.nFaces, NT), 8192), NT, 0, stream>>>(
-            2LL * L.nFaces, L.entFace.p, C.upper.p, C.val.p);
-    B2G_LAUNCH_CHECK();
     fillGsLayout(L, C, stream);
     coarseBuilt = false;
     v32.built = false;
@@ -312,16 +317,11 @@ void Matrix::buildCoarse()
         LevelCoef<double>& C = v64.coef[i + 1];
         C.diag.alloc(Cl.nCells, stream);
         C.upper.alloc(Cl.nFaces, stream);
-        C.val.alloc(2 * (size_t)Cl.nFaces, stream);
         k::galerkinDiag<<<rowsGrid(Cl.nCells), NT, 0, stream>>>(Cl.nCells, S.cellStart.p, S.cellList.p, S.intStart.p,
                                                                 S.intList.p, F.diag.p, F.upper.p, C.diag.p);
         if (Cl.nFaces)
-        {
             k::galerkinUpper<<<rowsGrid(Cl.nFaces), NT, 0, stream>>>(Cl.nFaces, S.faceBeg.p, S.faceEnd.p,
                                                                      S.faceList.p, F.upper.p, C.upper.p);
-            k::gatherVal<double, double><<<std::min(ceilDiv(2LL * Cl.nFaces, NT), 8192), NT, 0, stream>>>(
-                2LL * Cl.nFaces, Cl.entFace.p, C.upper.p, C.val.p);
-        }
         B2G_LAUNCH_CHECK();
         fillGsLayout(Cl, C, stream);
     }
@@ -330,13 +330,12 @@ void Matrix::buildCoarse()
     v64.src.resize(nL);
     for (int i = 0; i < nL; ++i)
     {
-        v64.corr[i].alloc(mesh->lev[i + 1].nCells, stream);
-        v64.src[i].alloc(mesh->lev[i + 1].nCells, stream);
+        v64.corr[i].alloc(nAlloc(i + 1), stream);
+        v64.src[i].alloc(nAlloc(i + 1), stream);
     }
-    const int n0 = mesh->lev[0].nCells;
-    v64.ACf.alloc(n0, stream);
-    v64.preSmoothed.alloc(n0, stream);
-    const int nc = nL > 0 ? mesh->lev[nL].nCells : n0;
+    v64.ACf.alloc(nAlloc(0), stream);
+    v64.preSmoothed.alloc(nAlloc(0), stream);
+    const int nc = nL > 0 ? mesh->lev[nL].nCells : mesh->lev[0].nCells;
     for (DBuf<double>* b : {&v64.cpA, &v64.cwA, &v64.crA, &v64.crD}) b->alloc(std::max(nc, 1), stream);
     v64.built = true;
     coarseBuilt = true;
@@ -352,22 +351,18 @@ void Matrix::ensureFp32()
     {
         const LevelAddr& L = mesh->lev[i];
         LevelCoef<float>& C = v32.coef[i];
-        C.diag.alloc(L.nCells, stream);
-        C.upper.alloc(L.nFaces, stream);
-        C.val.alloc(2 * (size_t)L.nFaces, stream);
-        castInto<float, double>(L.nCells, v64.coef[i].diag.p, C.diag.p, stream);
-        castInto<float, double>(L.nFaces, v64.coef[i].upper.p, C.upper.p, stream);
-        castInto<float, double>(2LL * L.nFaces, v64.coef[i].val.p, C.val.p, stream);
-        fillGsLayout(L, C, stream);
+        allocGsLayout(L, C, stream);
+        castInto<float, double>(L.nCells, v64.coef[i].gsDiag.p, C.gsDiag.p, stream);
+        castInto<float, double>(2LL * L.nFaces, v64.coef[i].gsVal.p, C.gsVal.p, stream);
     }
     v32.corr.resize(nL);
     v32.src.resize(nL);
     for (int i = 0; i < nL; ++i)
     {
-        v32.corr[i].alloc(mesh->lev[i + 1].nCells, stream);
-        v32.src[i].alloc(mesh->lev[i + 1].nCells, stream);
+        v32.corr[i].alloc(nAlloc(i + 1), stream);
+        v32.src[i].alloc(nAlloc(i + 1), stream);
     }
-    const int n0 = mesh->lev[0].nCells;
+    const size_t n0 = nAlloc(0);
     v32.ACf.alloc(n0, stream);
     v32.preSmoothed.alloc(n0, stream);
     v32.partial.alloc(2 * kMaxPartials, stream);
@@ -375,6 +370,30 @@ void Matrix::ensureFp32()
     for (DBuf<float>* b : {&r32, &w32, &AwA32, &fc32, &fr32}) b->alloc(n0, stream);
     rOld.alloc(n0, stream);
     v32.built = true;
+}
+
+template <class T>
+void Matrix::toPos(int level, const T* nat, T* pos)
+{
+    const LevelAddr& L = mesh->lev[level];
+    if (L.nCells) k::toPositions<T><<<rowsGrid(L.nCells), NT, 0, stream>>>(L.nCells, L.gs.posCell.p, nat, pos);
+    B2G_LAUNCH_CHECK();
+    ++launches;
+}
+
+template <class T>
+void Matrix::fromPos(int level, const T* pos, T* nat)
+{
+    const LevelAddr& L = mesh->lev[level];
+    if (L.nCells) k::fromPositions<T><<<rowsGrid(L.nCells), NT, 0, stream>>>(L.nCells, L.gs.posCell.p, pos, nat);
+    B2G_LAUNCH_CHECK();
+    ++launches;
+}
+
+double* Matrix::ioBuf(int i)
+{
+    if (!io[i].p) io[i].alloc(nAlloc(0), stream);
+    return io[i].p;
 }
 
 template <class T>
@@ -399,15 +418,18 @@ void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps,
     const GsSchedule& G = L.gs;
     const LevelCoef<T>& C = data<T>().coef[level];
     k::GsArgs<T> a;
+    if (L.nCells == 0) return;
     a.nParts = G.nParts;
     a.maxCells = G.maxCells;
     a.maxEnt = G.maxEnt;
+    a.ahead = G.ahead;
+    a.nPadded = G.nPadded;
     a.partChunkStart = G.partChunkStart.p;
+    a.partPosStart = G.partPosStart.p;
     a.chunkRec = reinterpret_cast<const int4*>(G.chunkRec.p);
     a.upStart = G.upStart.p;
     a.upList = G.upList.p;
     a.hasDown = G.hasDown.p;
-    a.posCell = G.posCell.p;
     a.posRow = G.posRow.p;
     a.entCode = G.entCode.p;
     a.entVal = C.gsVal.p;
@@ -446,7 +468,7 @@ void Matrix::scale(int level, T* field, T* Acf, const T* src)
         k::amul<T><<<rowsGrid(L.nCells), NT, 0, stream>>>(rowsOf(L, D.coef[level]), field, Acf);
         k::serialScaleDots<<<1, 32, 0, stream>>>(L.nCells, reinterpret_cast<const double*>(field),
                                                  reinterpret_cast<const double*>(src),
-                                                 reinterpret_cast<const double*>(Acf),
+                                                 reinterpret_cast<const double*>(Acf), L.gs.posOf.p,
                                                  reinterpret_cast<double*>(D.sf.p));
     }
     else
@@ -455,7 +477,8 @@ void Matrix::scale(int level, T* field, T* Acf, const T* src)
         k::amulScaleDots<T, NT><<<g, NT, 0, stream>>>(rowsOf(L, D.coef[level]), field, src, Acf, D.partial.p);
         k::scaleFactor<T, NT><<<1, NT, 0, stream>>>(D.partial.p, g, D.sf.p);
     }
-    k::scaleUpdate<T><<<rowsGrid(L.nCells), NT, 0, stream>>>(L.nCells, D.sf.p, field, src, Acf, D.coef[level].diag.p);
+    k::scaleUpdate<T><<<rowsGrid(L.nCells), NT, 0, stream>>>(L.nCells, D.sf.p, field, src, Acf,
+                                                             D.coef[level].gsDiag.p);
     B2G_LAUNCH_CHECK();
     launches += 3;
 }
@@ -464,9 +487,10 @@ void Matrix::reduceInto(int op, int n, const double* a, const double* b, double*
 {
     if (serial)
     {
-        if (op == k::RED_DOT) k::serialReduce<k::RED_DOT><<<1, 32, 0, stream>>>(n, a, b, slot);
-        else if (op == k::RED_SUMMAG) k::serialReduce<k::RED_SUMMAG><<<1, 32, 0, stream>>>(n, a, b, slot);
-        else k::serialReduce<k::RED_SUM><<<1, 32, 0, stream>>>(n, a, b, slot);
+        const int* po = mesh->lev[0].gs.posOf.p;
+        if (op == k::RED_DOT) k::serialReduce<k::RED_DOT><<<1, 32, 0, stream>>>(n, a, b, po, slot);
+        else if (op == k::RED_SUMMAG) k::serialReduce<k::RED_SUMMAG><<<1, 32, 0, stream>>>(n, a, b, po, slot);
+        else k::serialReduce<k::RED_SUM><<<1, 32, 0, stream>>>(n, a, b, po, slot);
         ++launches;
     }
     else
@@ -486,7 +510,7 @@ template <class T>
 void Matrix::restrictTo(int step, const T* fine, T* coarse)
 {
     const Step& S = mesh->step[step];
-    k::restrictField<T><<<rowsGrid(S.nCoarse), NT, 0, stream>>>(S.nCoarse, S.cellStart.p, S.cellList.p, fine, coarse);
+    k::restrictField<T><<<rowsGrid(S.nCoarse), NT, 0, stream>>>(S.nCoarse, S.rStartP.p, S.rListP.p, fine, coarse);
     B2G_LAUNCH_CHECK();
     ++launches;
 }
@@ -495,7 +519,7 @@ template <class T>
 void Matrix::prolongFrom(int step, const T* coarse, T* fine)
 {
     const Step& S = mesh->step[step];
-    k::prolongField<T><<<rowsGrid(S.nFine), NT, 0, stream>>>(S.nFine, S.restrictAddr.p, coarse, fine);
+    k::prolongField<T><<<rowsGrid(S.nFine), NT, 0, stream>>>(S.nFine, S.prolongP.p, coarse, fine);
     B2G_LAUNCH_CHECK();
     ++launches;
 }
@@ -511,10 +535,11 @@ void Matrix::coarsestSolve<double>(int level, double* x, const double* src, doub
     a.nF = L.nFaces;
     a.lower = L.lower.p;
     a.upper = L.upper.p;
-    a.rowStart = L.rowStart.p;
-    a.col = L.col.p;
-    a.val = C.val.p;
-    a.diag = C.diag.p;
+    a.posOf = L.gs.posOf.p;
+    a.rowStart = L.gs.posRow.p;
+    a.col = L.gs.entColPos.p;
+    a.val = C.gsVal.p;
+    a.diag = C.gsDiag.p;
     a.coef = C.upper.p;
     a.source = src;
     a.psi = x;
@@ -554,7 +579,8 @@ double Matrix::normFactor(int level, const double* x, const double* src, const d
     const LevelAddr& L = mesh->lev[level];
     if (serial)
     {
-        k::serialNormFactor<<<1, 32, 0, stream>>>(rowsOf(L, v64.coef[level]), x, src, Apsi, &scal.p->nf);
+        k::serialNormFactor<<<1, 32, 0, stream>>>(rowsOf(L, v64.coef[level]), x, src, Apsi, L.gs.posOf.p,
+                                                   &scal.p->nf);
         ++launches;
     }
     else
@@ -625,7 +651,7 @@ void Matrix::vcycle(const b2g_controls& c, T* x, const T* src, T* Apsi, T* fcor,
             k::amul<T><<<rowsGrid(F.nCells), NT, 0, stream>>>(rowsOf(F, D.coef[0]), fcor, Apsi);
             k::serialScaleDots<<<1, 32, 0, stream>>>(F.nCells, reinterpret_cast<const double*>(fcor),
                                                      reinterpret_cast<const double*>(fres),
-                                                     reinterpret_cast<const double*>(Apsi),
+                                                     reinterpret_cast<const double*>(Apsi), F.gs.posOf.p,
                                                      reinterpret_cast<double*>(D.sf.p));
         }
         else
@@ -637,7 +663,7 @@ void Matrix::vcycle(const b2g_controls& c, T* x, const T* src, T* Apsi, T* fcor,
             k::scaleFactor<T, NT><<<1, NT, 0, stream>>>(D.partial.p, g, D.sf.p);
         }
         k::scaleUpdateAdd<T><<<rowsGrid(F.nCells), NT, 0, stream>>>(F.nCells, D.sf.p, fcor, fres, Apsi,
-                                                                   D.coef[0].diag.p, x);
+                                                                   D.coef[0].gsDiag.p, x);
         launches += 3;
     }
     else
@@ -853,6 +879,8 @@ b2g_perf Matrix::gamg(const b2g_controls& c, b2g_solve_log* log)
     return perf;
 }
 
+template void Matrix::toPos<double>(int, const double*, double*);
+template void Matrix::fromPos<double>(int, const double*, double*);
 template void Matrix::amul<double>(int, const double*, double*);
 template void Matrix::amul<float>(int, const float*, float*);
 template void Matrix::smooth<double>(int, int, double*, const double*, int, unsigned long long*);

@@ -15,18 +15,19 @@ struct PcgScalars
     int singular, iter, pad0, pad1;
 };
 
-// The coefficient layout of one level in value type T.
+// The coefficients of one level in value type T. The LDU arrays keep the reference's cell and face
+// numbering (the Galerkin sums read them); every kernel of the solve reads the position-ordered pair.
 template <class T>
 struct LevelCoef
 {
-    DBuf<T> diag;   // [nCells]
-    DBuf<T> upper;  // [nFaces] LDU coefficient (upper == lower)
-    DBuf<T> val;    // [2*nFaces] row-layout coefficient
-    DBuf<T> gsDiag; // [nCells] diagonal in Gauss-Seidel position order
-    DBuf<T> gsVal;  // [2*nFaces] coefficients in Gauss-Seidel entry order
+    DBuf<T> diag;   // [nCells] by cell (FP64 only)
+    DBuf<T> upper;  // [nFaces] LDU coefficient, upper == lower (FP64 only)
+    DBuf<T> gsDiag; // [nCells (+pad)] diagonal by position
+    DBuf<T> gsVal;  // [2*nFaces (+pad)] coefficient per entry, rows by position
 };
 
 // Everything a V-cycle in value type T touches.
+// Every level vector is in that level's position order and allocated to its GsSchedule::nAlloc.
 template <class T>
 struct VCycleData
 {
@@ -47,8 +48,9 @@ struct Matrix
     VCycleData<double> v64;
     VCycleData<float> v32;
     bool coarseBuilt = false;
-    // finest-level work (FP64)
+    // finest-level work (FP64), by position
     DBuf<double> psi, source, rA, wA, pA, AwA, fc, fr, rOld;
+    DBuf<double> io[4];                       // level-entry staging (b2g_level_*), finest size
     DBuf<float> r32, w32, AwA32, fc32, fr32;
     DBuf<PcgScalars> scal;
     DBuf<k::DevPerf> coarseLog;
@@ -74,6 +76,11 @@ struct Matrix
     void ensureFp32();                        // float copies of every level
     int nLevels() const { return mesh->nLevels(); }
     int n(int level) const { return mesh->lev[level].nCells; }
+    size_t nAlloc(int level) const { return static_cast<size_t>(std::max(mesh->lev[level].gs.nAlloc, 1)); }
+    // natural cell order <-> the level's position order (device pointers)
+    template <class T> void toPos(int level, const T* nat, T* pos);
+    template <class T> void fromPos(int level, const T* pos, T* nat);
+    double* ioBuf(int i);                     // staging vector i of the level entries
 
     // pieces (device pointers)
     template <class T> void amul(int level, const T* x, T* y);
