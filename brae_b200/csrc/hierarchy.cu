@@ -469,25 +469,6 @@ __global__ void kPartBounds(int n, int P, const int* __restrict__ rowStart, int*
     partStart[p] = lo;
 }
 
-__global__ void kChunkRecs(int nCh, const int* __restrict__ chunkStart, const int* __restrict__ posRow,
-                           const int* __restrict__ chunkDepth, const int* __restrict__ chunkNeedUp,
-                           int* __restrict__ rec)
-{
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nCh) return;
-    const int p0 = chunkStart[c];
-    const int p1 = chunkStart[c + 1];
-    int* r = rec + 8 * (size_t)c;
-    r[0] = p0;
-    r[1] = p1 - p0;
-    r[2] = posRow[p0];
-    r[3] = posRow[p1] - posRow[p0];
-    r[4] = chunkDepth[c];
-    r[5] = chunkNeedUp[c];
-    r[6] = 0;
-    r[7] = 0;
-}
-
 __global__ void kStepCounts(int nCoarse, const int* __restrict__ posCellC, const int* __restrict__ cellStart,
                             int* __restrict__ cnt)
 {
@@ -528,6 +509,24 @@ __global__ void kPosRowLen(int n, const int* __restrict__ order, const int* __re
     if (i < n) len[i] = rowStart[order[i] + 1] - rowStart[order[i]];
 }
 
+// CSR rows in position order (the Amul, residual and reduction kernels): the other cell's position
+// and the face, per entry
+__global__ void kCsrPositions(int n, const int* __restrict__ order, const int* __restrict__ posOf,
+                              const int* __restrict__ rowStart, const int* __restrict__ col,
+                              const int* __restrict__ entFace, const int* __restrict__ posRow,
+                              int* __restrict__ colPos, int* __restrict__ facePos)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int c = order[i];
+    const int base = posRow[i];
+    for (int e = rowStart[c]; e < rowStart[c + 1]; ++e)
+    {
+        colPos[base + e - rowStart[c]] = posOf[col[e]];
+        facePos[base + e - rowStart[c]] = entFace[e];
+    }
+}
+
 __global__ void kChunkOfPos(int n, int nChunks, const int* __restrict__ chunkStart, int* __restrict__ chunkOf)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -541,60 +540,125 @@ __global__ void kChunkOfPos(int n, int nChunks, const int* __restrict__ chunkSta
     chunkOf[i] = lo;
 }
 
-// Entry codes in position order (gs_kernels.cuh): WIN -- a value the part's shared-memory window
-// holds when the chunk runs (an owner of this part within `behind` positions of the chunk's end, or a
-// neighbour of this part within `ahead` positions of its start); GAT -- gathered ahead (neighbours
-// elsewhere, owners of this part at least G+1 chunks back, owners of other parts once their progress
-// covers them); SLOW -- read at compute time (an owner of this part outside the window and too recent).
-__global__ void kEntryCodes(int n, int win, int ahead, int behind, int gatherAhead,
-                            const int* __restrict__ order, const int* __restrict__ posOf,
-                            const int* __restrict__ partOf, const int* __restrict__ depth,
-                            const int* __restrict__ chunkOf, const int* __restrict__ chunkStart,
-                            const int* __restrict__ posRow, const int* __restrict__ rowStart,
-                            const int* __restrict__ losortStart, const int* __restrict__ col,
-                            const int* __restrict__ entFace, unsigned* __restrict__ entCode,
-                            int* __restrict__ entFacePos, int* __restrict__ entColPos,
-                            int* __restrict__ chunkNeedUp, unsigned* __restrict__ upBits, int words)
+// Classification of a sweep entry (gs_kernels.cuh), for the cell at position i of chunk ch and its
+// entry k (CSR row order: the faces the cell is the neighbour of, then the faces it owns). Returns
+// true for a window read (slot in *code), false for a gather.
+struct EntryClass
+{
+    int win, ahead, behind;
+    const int* partOf;
+    const int* chunkOf;
+    const int* chunkStart;
+    __device__ bool window(bool lowerSide, bool samePart, int q, int ch) const
+    {
+        if (!samePart) return false;
+        if (lowerSide) return q >= chunkStart[ch + 1] - behind;  // an owner's new value, just behind
+        return q < chunkStart[ch] + ahead;                       // a neighbour's old value, just ahead
+    }
+};
+
+// pass 1: gathers per position; per chunk the waits they need (other parts' owners: their deepest
+// depth; this part's owners outside the window: their latest chunk), and the upstream part bits
+__global__ void kGatherCounts(int n, EntryClass ec, const int* __restrict__ order, const int* __restrict__ posOf,
+                              const int* __restrict__ depth, const int* __restrict__ rowStart,
+                              const int* __restrict__ losortStart, const int* __restrict__ col,
+                              int* __restrict__ cnt, int* __restrict__ chunkNeedUp, int* __restrict__ chunkSameWait,
+                              unsigned* __restrict__ upBits, int words)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int c = order[i];
-    const int p = partOf[c];
-    const int ch = chunkOf[i];
-    const int chBeg = chunkStart[ch];
-    const int chEnd = chunkStart[ch + 1];
+    const int p = ec.partOf[c];
+    const int ch = ec.chunkOf[i];
     const int rb = rowStart[c];
     const int nLower = losortStart[c + 1] - losortStart[c];
-    const int base = posRow[i];
+    int g = 0;
+    for (int e = rb; e < rowStart[c + 1]; ++e)
+    {
+        const int o = col[e];
+        const int q = posOf[o];
+        const bool lowerSide = e - rb < nLower;
+        const bool same = ec.partOf[o] == p;
+        if (ec.window(lowerSide, same, q, ch)) continue;
+        ++g;
+        if (!lowerSide) continue;  // an old value: final as it is
+        if (same)
+            atomicMax(&chunkSameWait[ch], ec.chunkOf[q]);
+        else
+        {
+            atomicMax(&chunkNeedUp[ch], depth[o]);
+            const int po = ec.partOf[o];
+            atomicOr(&upBits[(size_t)p * words + (po >> 5)], 1u << (po & 31));
+        }
+    }
+    cnt[i] = g;
+}
+
+// pass 2: the sliced-ELL entries (codes and faces) and the gather lists; entries past a row's end
+// keep the padding code and face -1 they were filled with
+__global__ void kSweepEntries(int n, EntryClass ec, const int* __restrict__ order, const int* __restrict__ posOf,
+                              const int* __restrict__ rowStart, const int* __restrict__ losortStart,
+                              const int* __restrict__ col, const int* __restrict__ entFace,
+                              const unsigned* __restrict__ posEnt, const long long* __restrict__ chunkEnt0,
+                              const int* __restrict__ gatOff, unsigned short* __restrict__ code,
+                              int* __restrict__ face, int* __restrict__ gatSrc)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int c = order[i];
+    const int p = ec.partOf[c];
+    const int ch = ec.chunkOf[i];
+    const int rb = rowStart[c];
+    const int nLower = losortStart[c + 1] - losortStart[c];
+    const long long base = chunkEnt0[ch] + static_cast<long long>(posEnt[i] & 0xffffffu);
+    const int g0 = gatOff[ec.chunkStart[ch]];
+    int g = gatOff[i];
     for (int e = rb; e < rowStart[c + 1]; ++e)
     {
         const int k = e - rb;
         const int o = col[e];
         const int q = posOf[o];
-        const bool same = partOf[o] == p;
-        unsigned code;
-        if (k < nLower)
-        {
-            if (same && q >= chEnd - behind) code = (0u << 30) | static_cast<unsigned>(q & (win - 1));
-            else if (same && chunkOf[q] <= ch - gatherAhead - 1) code = (1u << 30) | static_cast<unsigned>(q);
-            else if (same) code = (2u << 30) | static_cast<unsigned>(q);
-            else
-            {
-                code = (1u << 30) | static_cast<unsigned>(q);
-                atomicMax(&chunkNeedUp[ch], depth[o]);
-                const int po = partOf[o];
-                atomicOr(&upBits[(size_t)p * words + (po >> 5)], 1u << (po & 31));
-            }
-        }
+        const bool same = ec.partOf[o] == p;
+        unsigned short cd;
+        if (ec.window(k < nLower, same, q, ch)) cd = static_cast<unsigned short>(q & (ec.win - 1));
         else
         {
-            if (same && q < chBeg + ahead) code = (0u << 30) | static_cast<unsigned>(q & (win - 1));
-            else code = (1u << 30) | static_cast<unsigned>(q);
+            cd = static_cast<unsigned short>(k::kGatBit | static_cast<unsigned>(g - g0));
+            gatSrc[g++] = q;
         }
-        entCode[base + k] = code;
-        entFacePos[base + k] = entFace[e];
-        entColPos[base + k] = q;
+        code[base + 32LL * k] = cd;
+        face[base + 32LL * k] = entFace[e];
     }
+}
+
+__global__ void kChunkRecs(int nCh, const int* __restrict__ chunkStart, const long long* __restrict__ chunkEnt0,
+                           const int* __restrict__ chunkDepth, const int* __restrict__ chunkNewDepth,
+                           const int* __restrict__ gatOff, const int* __restrict__ chunkNeedUp,
+                           const int* __restrict__ chunkSameWait, int* __restrict__ rec)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nCh) return;
+    const int p0 = chunkStart[c];
+    const int p1 = chunkStart[c + 1];
+    int* r = rec + 12 * (size_t)c;
+    r[0] = p0;
+    r[1] = p1 - p0;
+    r[2] = static_cast<int>(chunkEnt0[c]);
+    r[3] = static_cast<int>(chunkEnt0[c + 1] - chunkEnt0[c]);
+    r[4] = gatOff[p0];
+    r[5] = gatOff[p1] - gatOff[p0];
+    r[6] = chunkDepth[c];
+    r[7] = chunkNeedUp[c];
+    r[8] = chunkSameWait[c];
+    r[9] = chunkNewDepth[c];
+    r[10] = 0;
+    r[11] = 0;
+}
+
+__global__ void kFillShort(unsigned short* v, long long n, unsigned short value)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        v[i] = value;
 }
 
 __global__ void kFillInt(int* v, int n, int value)
@@ -1008,7 +1072,12 @@ void buildGsSchedule(LevelAddr& L, cudaStream_t s)
     G.posRow.alloc(n + 1 + 8, s);
     G.posRow.zero(s);
     exclusiveScan(rowLen.p, G.posRow.p, n, s);
-    // chunks: cut each group by cells and entries so a chunk's stage fits in shared memory
+    G.entColPos.alloc(std::max<size_t>(2 * (size_t)L.nFaces, 1), s);
+    G.entFacePos.alloc(std::max<size_t>(2 * (size_t)L.nFaces, 1), s);
+    kCsrPositions<<<grid(n), TPB, 0, s>>>(n, G.posCell.p, G.posOf.p, L.rowStart.p, L.col.p, L.entFace.p, G.posRow.p,
+                                          G.entColPos.p, G.entFacePos.p);
+    B2G_LAUNCH_CHECK();
+    // chunks: each (part, depth) group cut into chunks of at most M cells and E sliced-ELL entries
     const std::vector<int> hLvlStart = lvlStart.download(s);
     const std::vector<int> hLvlDepth = lvlDepth.download(s);
     const std::vector<int> hLvlPart = lvlPart.download(s);
@@ -1017,91 +1086,158 @@ void buildGsSchedule(LevelAddr& L, cudaStream_t s)
     for (int g = 0; g < nLvl; ++g)
         maxGroup = std::max(maxGroup, (g + 1 < nLvl ? hLvlStart[g + 1] : n) - hLvlStart[g]);
     for (int i = 0; i < n; ++i) maxRow = std::max(maxRow, hPosRow[i + 1] - hPosRow[i]);
-    // chunk capacity: as many cells as the widest (part, depth) group, within what S pipeline slots
-    // and the psi window of shared memory hold (M compute threads + one service warp per CTA), and
-    // leaving the window room ahead of and behind a chunk
-    // (entries are budgeted at the average row length plus a margin, at most the longest row: a chunk
-    // with longer rows simply holds fewer cells)
-    const size_t smemCap = 200 * 1024;
+    if (maxRow > 255) fail(B2G_ERR_ARGUMENT, "b2g: a cell with more than 255 faces does not fit the sweep's rows.");
     const int nnz = hPosRow[n];
-    const int avgRow = static_cast<int>((5LL * nnz + 4LL * n - 1) / (4LL * n));  // ceil(1.25 * nnz / n)
-    const int rowCap = std::max(1, std::min(maxRow, avgRow));
-    int M = std::min(480, std::max(32, ((maxGroup + 31) / 32) * 32));
-    auto fits = [&](int m, int e) {
+    const int rowCap = std::max(1, std::min(maxRow, static_cast<int>((5LL * nnz + 4LL * n - 1) / (4LL * n))));
+    const size_t smemCap = 200 * 1024;
+    auto fits = [&](int m, int e, int g) {
         int ah, bh;
         k::gsWindowExtents(m, ah, bh);
-        return k::gsSmemBytes<double>(m, e) <= smemCap && ah >= m && bh >= m;
+        return k::gsSmemBytes<double>(m, e, g) <= smemCap && ah >= m && bh >= m;
     };
-    while (M > 32 && !fits(M, std::max(M * rowCap, maxRow))) M -= 32;
-    int E = std::max(M * rowCap, maxRow);
-    if (!fits(M, E))
-        fail(B2G_ERR_ARGUMENT, "b2g: a cell has more faces than the Gauss-Seidel pipeline holds.");
-    G.maxCells = M;
-    G.maxEnt = E;
-    k::gsWindowExtents(M, G.ahead, G.behind);
-    G.nPadded = ((n + k::kFill - 1) / k::kFill) * k::kFill;
-    G.nAlloc = G.nPadded + k::kFill;
-    std::vector<int> hChunkStart, hChunkDepth, hPartChunk(P + 1, 0);
-    for (int g = 0; g < nLvl; ++g)
-    {
-        const int gs = hLvlStart[g];
-        const int ge = g + 1 < nLvl ? hLvlStart[g + 1] : n;
-        int cs = gs;
-        while (cs < ge)
-        {
-            int ce = cs;
-            while (ce < ge && ce - cs < M && hPosRow[ce + 1] - hPosRow[cs] <= E) ++ce;
-            hChunkStart.push_back(cs);
-            hChunkDepth.push_back(hLvlDepth[g]);
-            hPartChunk[hLvlPart[g] + 1]++;
-            cs = ce;
-        }
-    }
-    const int nCh = static_cast<int>(hChunkStart.size());
-    hChunkStart.push_back(n);
-    for (int p = 0; p < P; ++p) hPartChunk[p + 1] += hPartChunk[p];
-    G.nChunks = nCh;
-    DBuf<int> chunkStart, chunkDepth, chunkNeedUp;
-    chunkStart.upload(hChunkStart.data(), hChunkStart.size(), s);
-    chunkDepth.upload(hChunkDepth.data(), hChunkDepth.size(), s);
-    G.partChunkStart.upload(hPartChunk.data(), hPartChunk.size(), s);
-    chunkNeedUp.alloc(nCh, s);
-    kFillInt<<<grid(nCh), TPB, 0, s>>>(chunkNeedUp.p, nCh, -1);
-    DBuf<int> chunkOf;
-    chunkOf.alloc(n, s);
-    kChunkOfPos<<<grid(n), TPB, 0, s>>>(n, nCh, chunkStart.p, chunkOf.p);
     const int words = (P + 31) / 32;
-    DBuf<unsigned> upBits;
-    upBits.alloc(static_cast<size_t>(P) * words, s);
-    upBits.zero(s);
-    G.entCode.alloc(2 * (size_t)L.nFaces + 8, s);
-    G.entCode.zero(s);
-    G.entFacePos.alloc(2 * (size_t)L.nFaces, s);
-    G.entColPos.alloc(2 * (size_t)L.nFaces, s);
-    kEntryCodes<<<grid(n), TPB, 0, s>>>(n, k::kWin, G.ahead, G.behind, k::kGatherAhead, G.posCell.p, G.posOf.p,
-                                        partOf.p, G.depth.p, chunkOf.p, chunkStart.p, G.posRow.p, L.rowStart.p,
-                                        L.losortStart.p, L.col.p, L.entFace.p, G.entCode.p, G.entFacePos.p,
-                                        G.entColPos.p, chunkNeedUp.p, upBits.p, words);
-    B2G_LAUNCH_CHECK();
-    G.chunkRec.alloc(8 * (size_t)nCh, s);
-    kChunkRecs<<<grid(nCh), TPB, 0, s>>>(nCh, chunkStart.p, G.posRow.p, chunkDepth.p, chunkNeedUp.p,
-                                         G.chunkRec.p);
-    B2G_LAUNCH_CHECK();
-    std::vector<unsigned> hUp = upBits.download(s);
-    std::vector<int> upStart(P + 1, 0), upList;
-    for (int p = 0; p < P; ++p)
+    int M = std::min(k::kMaxCompute, std::max(32, ((maxGroup + 31) / 32) * 32));
+    const EntryClass ecBase{k::kWin, 0, 0, partOf.p, nullptr, nullptr};
+    for (int attempt = 0;; ++attempt)
     {
-        upStart[p] = static_cast<int>(upList.size());
+        // entry budget: the average row (plus a margin) per cell, at least one slice of the longest row
+        int E = std::max(M * rowCap, 32 * maxRow);
+        E = ((E + 31) / 32) * 32;
+        while (M > 32 && !fits(M, E, M)) { M -= 32; E = ((std::max(M * rowCap, 32 * maxRow) + 31) / 32) * 32; }
+        if (!fits(M, E, 32)) fail(B2G_ERR_ARGUMENT, "b2g: a cell has more faces than the Gauss-Seidel pipeline holds.");
+        // host chunking: per chunk its positions and ELL entries; per position its row descriptor
+        std::vector<int> hChunkStart, hChunkDepth, hChunkNewDepth, hPartChunk(P + 1, 0);
+        std::vector<long long> hChunkEnt0;
+        std::vector<unsigned> hPosEnt(static_cast<size_t>(n) + 8, 0u);
+        long long ent = 0;
+        int prevPart = -1;
+        for (int g = 0; g < nLvl; ++g)
+        {
+            const int gs = hLvlStart[g];
+            const int ge = g + 1 < nLvl ? hLvlStart[g + 1] : n;
+            int cs = gs;
+            while (cs < ge)
+            {
+                // grow the chunk slice by slice (32 cells, padded to the slice's longest row)
+                int ce = cs;
+                long long nEnt = 0;
+                while (ce < ge && ce - cs < M)
+                {
+                    const int sEnd = std::min({ce + 32, ge, cs + M});
+                    int w = 0;
+                    for (int i = ce; i < sEnd; ++i) w = std::max(w, hPosRow[i + 1] - hPosRow[i]);
+                    if (nEnt + 32LL * w > E && ce > cs) break;
+                    for (int i = ce; i < sEnd; ++i)
+                        hPosEnt[i] = (static_cast<unsigned>(w) << 24) | static_cast<unsigned>(nEnt + (i - ce));
+                    nEnt += 32LL * w;
+                    ce = sEnd;
+                }
+                hChunkStart.push_back(cs);
+                hChunkEnt0.push_back(ent);
+                hChunkDepth.push_back(hLvlDepth[g]);
+                hChunkNewDepth.push_back(cs == gs && prevPart == hLvlPart[g] ? 1 : 0);
+                hPartChunk[hLvlPart[g] + 1]++;
+                prevPart = hLvlPart[g];
+                ent += nEnt;
+                cs = ce;
+            }
+        }
+        const int nCh = static_cast<int>(hChunkStart.size());
+        hChunkStart.push_back(n);
+        hChunkEnt0.push_back(ent);
+        for (int q = 0; q < P; ++q) hPartChunk[q + 1] += hPartChunk[q];
+        int ahead, behind;
+        k::gsWindowExtents(M, ahead, behind);
+        // device classification
+        DBuf<int> chunkStart, chunkDepth, chunkNewDepth, chunkNeedUp, chunkSameWait, chunkOf, gatCnt, gatOff;
+        DBuf<long long> chunkEnt0;
+        chunkStart.upload(hChunkStart.data(), hChunkStart.size(), s);
+        chunkDepth.upload(hChunkDepth.data(), hChunkDepth.size(), s);
+        chunkNewDepth.upload(hChunkNewDepth.data(), hChunkNewDepth.size(), s);
+        chunkEnt0.upload(hChunkEnt0.data(), hChunkEnt0.size(), s);
+        G.posEnt.upload(hPosEnt.data(), hPosEnt.size(), s);
+        chunkNeedUp.alloc(nCh, s);
+        chunkSameWait.alloc(nCh, s);
+        kFillInt<<<grid(nCh), TPB, 0, s>>>(chunkNeedUp.p, nCh, -1);
+        kFillInt<<<grid(nCh), TPB, 0, s>>>(chunkSameWait.p, nCh, -1);
+        chunkOf.alloc(n, s);
+        kChunkOfPos<<<grid(n), TPB, 0, s>>>(n, nCh, chunkStart.p, chunkOf.p);
+        DBuf<unsigned> upBits;
+        upBits.alloc(static_cast<size_t>(P) * words, s);
+        upBits.zero(s);
+        EntryClass ec = ecBase;
+        ec.ahead = ahead;
+        ec.behind = behind;
+        ec.chunkOf = chunkOf.p;
+        ec.chunkStart = chunkStart.p;
+        gatCnt.alloc(n, s);
+        kGatherCounts<<<grid(n), TPB, 0, s>>>(n, ec, G.posCell.p, G.posOf.p, G.depth.p, L.rowStart.p,
+                                              L.losortStart.p, L.col.p, gatCnt.p, chunkNeedUp.p,
+                                              chunkSameWait.p, upBits.p, words);
+        B2G_LAUNCH_CHECK();
+        gatOff.alloc(n + 1, s);
+        const long long nGather = exclusiveScan(gatCnt.p, gatOff.p, n, s);
+        // the largest gather list of a chunk sizes the slots' gather arrays
+        const std::vector<int> hGatOff = gatOff.download(s);
+        int maxGat = 0;
+        for (int c = 0; c < nCh; ++c)
+            maxGat = std::max(maxGat, hGatOff[hChunkStart[c + 1]] - hGatOff[hChunkStart[c]]);
+        maxGat = ((maxGat + 1 + 7) / 8) * 8;  // + the zero that padding entries read
+        if ((maxGat > k::kMaxGat || !fits(M, E, maxGat)) && M > 32 && attempt < 16)
+        {
+            M -= 32;  // fewer cells per chunk: fewer gathers per chunk, and more room per slot
+            continue;
+        }
+        if (maxGat > k::kMaxGat || !fits(M, E, maxGat))
+            fail(B2G_ERR_ARGUMENT, "b2g: the Gauss-Seidel chunks gather more values than shared memory holds.");
+        G.maxCells = M;
+        G.maxEnt = E;
+        G.maxGat = maxGat;
+        G.ahead = ahead;
+        G.behind = behind;
+        G.nChunks = nCh;
+        G.nEll = ent;
+        G.nGather = nGather;
+        G.nPadded = ((n + k::kFill - 1) / k::kFill) * k::kFill;
+        G.nAlloc = G.nPadded + k::kFill;
+        G.partChunkStart.upload(hPartChunk.data(), hPartChunk.size(), s);
+        G.gsCode.alloc(std::max<long long>(ent, 1), s);
+        G.gsEntFace.alloc(std::max<long long>(ent, 1), s);
+        G.gatSrc.alloc(std::max<long long>(nGather, 1), s);
+        if (ent)
+        {
+            kFillShort<<<std::min<long long>(ceilDiv(ent, TPB), 8192), TPB, 0, s>>>(
+                G.gsCode.p, ent, static_cast<unsigned short>(k::kGatBit | static_cast<unsigned>(maxGat - 1)));
+            kFillInt<<<static_cast<int>(std::min<long long>(ceilDiv(ent, TPB), 1LL << 30)), TPB, 0, s>>>(
+                G.gsEntFace.p, static_cast<int>(ent), -1);
+        }
+        kSweepEntries<<<grid(n), TPB, 0, s>>>(n, ec, G.posCell.p, G.posOf.p, L.rowStart.p, L.losortStart.p, L.col.p,
+                                              L.entFace.p, G.posEnt.p, chunkEnt0.p, gatOff.p, G.gsCode.p,
+                                              G.gsEntFace.p, G.gatSrc.p);
+        B2G_LAUNCH_CHECK();
+        G.chunkRec.alloc(12 * (size_t)nCh, s);
+        kChunkRecs<<<grid(nCh), TPB, 0, s>>>(nCh, chunkStart.p, chunkEnt0.p, chunkDepth.p, chunkNewDepth.p, gatOff.p,
+                                             chunkNeedUp.p, chunkSameWait.p, G.chunkRec.p);
+        B2G_LAUNCH_CHECK();
+        // upstream parts (whose progress a part waits on) and which parts have a downstream
+        std::vector<unsigned> hUp = upBits.download(s);
+        std::vector<int> upStart(P + 1, 0), upList;
         for (int q = 0; q < P; ++q)
-            if (hUp[(size_t)p * words + (q >> 5)] & (1u << (q & 31))) upList.push_back(q);
+        {
+            upStart[q] = static_cast<int>(upList.size());
+            for (int r = 0; r < P; ++r)
+                if (hUp[(size_t)q * words + (r >> 5)] & (1u << (r & 31))) upList.push_back(r);
+        }
+        upStart[P] = static_cast<int>(upList.size());
+        std::vector<int> hasDown(P, 0);
+        for (int r : upList) hasDown[r] = 1;
+        G.hasDown.upload(hasDown.data(), hasDown.size(), s);
+        G.upStart.upload(upStart.data(), upStart.size(), s);
+        if (upList.empty()) upList.push_back(0);
+        G.upList.upload(upList.data(), upList.size(), s);
+        B2G_CUDA(cudaStreamSynchronize(s));
+        break;
     }
-    upStart[P] = static_cast<int>(upList.size());
-    std::vector<int> hasDown(P, 0);
-    for (int q : upList) hasDown[q] = 1;
-    G.hasDown.upload(hasDown.data(), hasDown.size(), s);
-    G.upStart.upload(upStart.data(), upStart.size(), s);
-    if (upList.empty()) upList.push_back(0);
-    G.upList.upload(upList.data(), upList.size(), s);
     G.partPosStart = std::move(dPartStart);
     G.progress.alloc(P, s);
     G.progress.zero(s);

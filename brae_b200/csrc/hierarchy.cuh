@@ -17,24 +17,30 @@ struct GsSchedule
     int maxDepth = 0;
     int nChunks = 0;
     int maxCells = 0;          // chunk cell capacity == the kernel's compute threads
-    int maxEnt = 0;            // chunk entry capacity
+    int maxEnt = 0;            // chunk ELL entry capacity
+    int maxGat = 0;            // chunk gather capacity, + 1 for the zero padding entries read
     int ahead = 0;             // window extents the entry codes assume (gsWindowExtents)
     int behind = 0;
     int nPadded = 0;           // position count rounded up to the window fill block
     int nAlloc = 0;            // allocation length of every position-ordered vector of the level
+    long long nEll = 0;        // ELL entries (whole 32-cell slices, padding included)
+    long long nGather = 0;     // gathered values over all chunks
     DBuf<int> depth;           // [nCells] by cell
     DBuf<int> partChunkStart;  // [nParts+1]
     DBuf<int> partPosStart;    // [nParts+1] (a part's positions are its cell range)
-    DBuf<int> chunkRec;        // [nChunks][8]: pos0, m, e0, ne, depth, needUp, 0, 0
+    DBuf<int> chunkRec;        // [nChunks][12] (gs_kernels.cuh ChunkRec)
     DBuf<int> upStart;         // [nParts+1] upstream parts of each part
     DBuf<int> upList;
     DBuf<int> hasDown;         // [nParts] 1 if another part reads this part's new values
     DBuf<int> posCell;         // [nCells] cell at each position
     DBuf<int> posOf;           // [nCells] position of each cell
-    DBuf<int> posRow;          // [nCells+1 (+pad)] entry offsets in position order
-    DBuf<int> entColPos;       // [2*nFaces] the other cell's position, per entry in position order
-    DBuf<unsigned> entCode;    // [2*nFaces (+pad)] Gauss-Seidel codes: kind << 30 | window slot or position
-    DBuf<int> entFacePos;      // [2*nFaces] face of each entry (fills the coefficients per solve)
+    DBuf<int> posRow;          // [nCells+1 (+pad)] CSR entry offsets in position order
+    DBuf<int> entColPos;       // [2*nFaces] CSR: the other cell's position per entry
+    DBuf<int> entFacePos;      // [2*nFaces] CSR: face of each entry
+    DBuf<unsigned> posEnt;     // [nCells (+pad)] sweep row descriptor: slice width << 24 | chunk-relative base
+    DBuf<unsigned short> gsCode;  // [nEll] sweep entry codes (gs_kernels.cuh)
+    DBuf<int> gsEntFace;       // [nEll] face of each sweep entry, -1 for padding
+    DBuf<int> gatSrc;          // [nGather] position of each gathered value
     DBuf<unsigned> progress;   // [nParts] per-part progress words (reset before each launch)
 };
 

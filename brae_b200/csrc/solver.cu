@@ -131,43 +131,49 @@ bool convergedH(double fin, double init, double tol, double relTol)
 template <class T>
 k::Rows<T> rowsOf(const LevelAddr& L, const LevelCoef<T>& C)
 {
-    return k::Rows<T>{L.nCells, L.gs.posRow.p, L.gs.entColPos.p, C.gsVal.p, C.gsDiag.p};
+    return k::Rows<T>{L.nCells, L.gs.posRow.p, L.gs.entColPos.p, C.rowVal.p, C.gsDiag.p};
 }
 
-// the position-ordered coefficients of one level
-template <class T>
-__global__ void kGsLayout(int n, long long nnz, const int* __restrict__ posCell, const int* __restrict__ entFacePos,
-                          const T* __restrict__ diag, const T* __restrict__ upper, T* __restrict__ gsDiag,
-                          T* __restrict__ gsVal)
+// the position-ordered coefficients of one level: diagonal, CSR rows, sweep (sliced ELL) entries
+__global__ void kGsLayout(int n, long long nnz, long long nEll, const int* __restrict__ posCell,
+                          const int* __restrict__ entFacePos, const int* __restrict__ gsEntFace,
+                          const double* __restrict__ diag, const double* __restrict__ upper, double* __restrict__ gsDiag,
+                          double* __restrict__ rowVal, double* __restrict__ gsVal)
 {
     const long long stride = (long long)gridDim.x * blockDim.x;
-    const long long m = n > nnz ? n : nnz;
+    const long long m = max(static_cast<long long>(n), max(nnz, nEll));
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m; i += stride)
     {
         if (i < n) gsDiag[i] = diag[posCell[i]];
-        if (i < nnz) gsVal[i] = upper[entFacePos[i]];
+        if (i < nnz) rowVal[i] = upper[entFacePos[i]];
+        if (i < nEll)
+        {
+            const int f = gsEntFace[i];
+            gsVal[i] = f >= 0 ? upper[f] : 0.0;
+        }
     }
 }
 
-// (+8 elements of zeroed padding: the sweep's bulk copies round their extents up to 16 bytes)
+// (+8 elements of zeroed padding past the diagonal: the sweep's bulk copies round position ranges
+// out to 16 bytes)
 template <class T>
 void allocGsLayout(const LevelAddr& L, LevelCoef<T>& C, cudaStream_t s)
 {
     C.gsDiag.alloc(L.nCells + 8, s);
-    C.gsVal.alloc(2 * (size_t)L.nFaces + 8, s);
     C.gsDiag.zero(s);
-    C.gsVal.zero(s);
+    C.rowVal.alloc(std::max<size_t>(2 * (size_t)L.nFaces, 1), s);
+    C.gsVal.alloc(static_cast<size_t>(std::max<long long>(L.gs.nEll, 1)), s);
 }
 
 void fillGsLayout(const LevelAddr& L, LevelCoef<double>& C, cudaStream_t s)
 {
     allocGsLayout(L, C, s);
     const long long nnz = 2LL * L.nFaces;
-    const long long m = std::max<long long>(L.nCells, nnz);
+    const long long m = std::max<long long>(L.nCells, std::max(nnz, L.gs.nEll));
     if (m)
-        kGsLayout<double><<<std::min(ceilDiv(m, NT), 8192), NT, 0, s>>>(L.nCells, nnz, L.gs.posCell.p,
-                                                                         L.gs.entFacePos.p, C.diag.p, C.upper.p,
-                                                                         C.gsDiag.p, C.gsVal.p);
+        kGsLayout<<<std::min(ceilDiv(m, NT), 8192), NT, 0, s>>>(L.nCells, nnz, L.gs.nEll, L.gs.posCell.p,
+                                                                L.gs.entFacePos.p, L.gs.gsEntFace.p, C.diag.p,
+                                                                C.upper.p, C.gsDiag.p, C.rowVal.p, C.gsVal.p);
     B2G_LAUNCH_CHECK();
 }
 
@@ -353,7 +359,8 @@ void Matrix::ensureFp32()
         LevelCoef<float>& C = v32.coef[i];
         allocGsLayout(L, C, stream);
         castInto<float, double>(L.nCells, v64.coef[i].gsDiag.p, C.gsDiag.p, stream);
-        castInto<float, double>(2LL * L.nFaces, v64.coef[i].gsVal.p, C.gsVal.p, stream);
+        castInto<float, double>(2LL * L.nFaces, v64.coef[i].rowVal.p, C.rowVal.p, stream);
+        castInto<float, double>(L.gs.nEll, v64.coef[i].gsVal.p, C.gsVal.p, stream);
     }
     v32.corr.resize(nL);
     v32.src.resize(nL);
@@ -422,6 +429,7 @@ void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps,
     a.nParts = G.nParts;
     a.maxCells = G.maxCells;
     a.maxEnt = G.maxEnt;
+    a.maxGat = G.maxGat;
     a.ahead = G.ahead;
     a.nPadded = G.nPadded;
     a.partChunkStart = G.partChunkStart.p;
@@ -430,16 +438,17 @@ void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps,
     a.upStart = G.upStart.p;
     a.upList = G.upList.p;
     a.hasDown = G.hasDown.p;
-    a.posRow = G.posRow.p;
-    a.entCode = G.entCode.p;
+    a.posEnt = G.posEnt.p;
+    a.entCode = G.gsCode.p;
     a.entVal = C.gsVal.p;
+    a.gatSrc = G.gatSrc.p;
     a.posDiag = C.gsDiag.p;
     a.b = src;
     a.psi = psiL;
     a.progress = G.progress.p;
     a.err = err.p;
     a.trace = trace;
-    const size_t smem = k::gsSmemBytes<T>(G.maxCells, G.maxEnt);
+    const size_t smem = k::gsSmemBytes<T>(G.maxCells, G.maxEnt, G.maxGat);
     static bool attrSet[2] = {false, false};
     bool& set = attrSet[sizeof(T) == 8 ? 0 : 1];
     if (!set)
@@ -451,7 +460,7 @@ void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps,
     {
         B2G_CUDA(cudaMemsetAsync(G.progress.p, 0, sizeof(unsigned) * G.nParts, stream));
         cudaEvent_t e = level == 0 ? timedBegin(1) : nullptr;
-        k::gsSweep<T><<<G.nParts, G.maxCells + 32, smem, stream>>>(a);
+        k::gsSweep<T><<<G.nParts, G.maxCells + 64, smem, stream>>>(a);
         timedEnd(1, e);
         B2G_LAUNCH_CHECK();
         launches += 1;
@@ -538,7 +547,7 @@ void Matrix::coarsestSolve<double>(int level, double* x, const double* src, doub
     a.posOf = L.gs.posOf.p;
     a.rowStart = L.gs.posRow.p;
     a.col = L.gs.entColPos.p;
-    a.val = C.gsVal.p;
+    a.val = C.rowVal.p;
     a.diag = C.gsDiag.p;
     a.coef = C.upper.p;
     a.source = src;

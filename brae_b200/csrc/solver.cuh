@@ -23,7 +23,8 @@ struct LevelCoef
     DBuf<T> diag;   // [nCells] by cell (FP64 only)
     DBuf<T> upper;  // [nFaces] LDU coefficient, upper == lower (FP64 only)
     DBuf<T> gsDiag; // [nCells (+pad)] diagonal by position
-    DBuf<T> gsVal;  // [2*nFaces (+pad)] coefficient per entry, rows by position
+    DBuf<T> rowVal; // [2*nFaces] coefficient per CSR entry, rows by position
+    DBuf<T> gsVal;  // [ELL entries] coefficient per sweep entry (sliced ELL), 0 for padding
 };
 
 // Everything a V-cycle in value type T touches.

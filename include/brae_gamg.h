@@ -263,9 +263,10 @@ B2G_API b2g_status b2g_matrix_timings(const b2g_matrix* m, double* ms4, long lon
 B2G_API b2g_status b2g_set_profiling(int on);
 
 /* Diagnostic: one Gauss-Seidel sweep of `level` (device pointers) recording into the device array
- * `trace` [4 * (nChunks + nParts)]: per schedule chunk four SM-cycle stamps (loop top, pipeline
- * barrier passed, data and upstream parts ready, chunk done), then per part {globaltimer ns, SM
- * cycles} at its start and end. `schedule` (host, may be NULL) receives {nParts, nChunks, chunk cell
+ * `trace` [6 * nChunks + 4 * nParts]: per schedule chunk four SM-cycle stamps of the first compute
+ * thread (chunk start, staged data ready, row computed, slot released), then per part
+ * {globaltimer ns, SM cycles} at its start and end, then per chunk two stamps of the staging warp
+ * (start, copies issued). `schedule` (host, may be NULL) receives {nParts, nChunks, chunk cell
  * capacity, chunk entry capacity, max depth}. */
 B2G_API b2g_status b2g_level_smooth_trace(b2g_matrix* m, int level, double* psi, const double* source,
                                           unsigned long long* trace, int traceCapacity, int* schedule);
