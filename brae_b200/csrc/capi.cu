@@ -8,6 +8,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 
 struct b2g_mesh
@@ -716,3 +717,116 @@ b2g_status b2g_matrix_timings(const b2g_matrix* m, double* ms4, long long* count
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// The coarsest-level PCG-DIC with no device allocation (b2g_level_pcg_dic_static)
+// ---------------------------------------------------------------------------------------------
+//
+// Some callers may not allocate device memory during a solve: a host code whose device memory is
+// owned by another allocator (a framework's caching pool that has reserved the GPU), or a loop that
+// cannot afford the implicit device synchronisation cudaMalloc/cudaFree may bring. For them this
+// entry keeps every scratch vector of the coarsest-level solve in one file-scope device array that
+// the library image carries, so the call itself allocates nothing.
+namespace {
+
+constexpr int kStaticCells = 4096;  // the largest level the static scratch holds
+// six vectors of kStaticCells doubles (psi and source in position order, pA, wA, rA, rD) and the
+// solver-performance record: about 192 KiB, held on every GPU that loads the library until exit
+constexpr size_t kStaticDoubles = 6 * static_cast<size_t>(kStaticCells) + 4;
+static __device__ __align__(256) double g_staticScratch[kStaticDoubles];
+
+// Nothing in the array needs to start at zero: each call writes every scratch value before it
+// reads it (the copies of psi and source, the residual, the DIC reciprocals, the PCG vectors and
+// the performance record), whatever an earlier call left there.
+//
+// The device address of g_staticScratch on the current device. In host code the symbol is only a
+// host-side stand-in, so the address is looked up once per device (with that device current) and
+// cached; the first call on a device does this.
+double* staticScratchAddress()
+{
+    static std::mutex mu;
+    static double* addr[64] = {};
+    int dev = 0;
+    B2G_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) b2g::fail(B2G_ERR_STATE, "b2g_level_pcg_dic_static: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev])
+    {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_staticScratch);
+        if (e != cudaSuccess)
+            b2g::fail(B2G_ERR_CUDA, std::string("b2g_level_pcg_dic_static: cudaGetSymbolAddress failed: ") +
+                                        cudaGetErrorString(e));
+        addr[dev] = static_cast<double*>(p);
+    }
+    return addr[dev];
+}
+
+}  // namespace
+
+extern "C" B2G_API b2g_status b2g_level_pcg_dic_static(b2g_matrix* m, int level, double* psi, const double* source,
+                                                       double tolerance, double relTol, b2g_perf* out)
+{
+    return guarded([&] {
+        need(m && psi && source && out, "b2g_level_pcg_dic_static: null argument");
+        b2g::Matrix& A = *m->mat;
+        need(level >= 0 && level <= A.nLevels(), "b2g_level_pcg_dic_static: level out of range");
+        const b2g::LevelAddr& L = A.mesh->lev[level];
+        const int n = L.nCells;
+        if (n > kStaticCells)
+            b2g::fail(B2G_ERR_ARGUMENT, "b2g_level_pcg_dic_static: the level has " + std::to_string(n) +
+                                            " cells; the static scratch holds at most " +
+                                            std::to_string(kStaticCells));
+        int dev = 0;
+        B2G_CUDA(cudaGetDevice(&dev));
+        need(dev == A.mesh->device, "b2g_level_pcg_dic_static: make the matrix's device current first");
+        double* base = staticScratchAddress();
+        double* psiPos = base;
+        double* srcPos = base + kStaticCells;
+        b2g::k::DevPerf* perf = reinterpret_cast<b2g::k::DevPerf*>(base + 6 * static_cast<size_t>(kStaticCells));
+        cudaStream_t s = A.stream;
+        const int grid = std::max(1, (n + 255) / 256);
+        if (n)
+        {
+            b2g::k::toPositions<double><<<grid, 256, 0, s>>>(n, L.gs.posCell.p, psi, psiPos);
+            b2g::k::toPositions<double><<<grid, 256, 0, s>>>(n, L.gs.posCell.p, source, srcPos);
+        }
+        B2G_LAUNCH_CHECK();
+        // the same kernel and arguments as b2g_level_pcg_dic, with the scratch vectors in the array
+        const b2g::LevelCoef<double>& C = A.v64.coef[level];
+        b2g::k::CoarsestArgs<double> a;
+        a.n = n;
+        a.nF = L.nFaces;
+        a.lower = L.lower.p;
+        a.upper = L.upper.p;
+        a.posOf = L.gs.posOf.p;
+        a.rowStart = L.gs.posRow.p;
+        a.col = L.gs.entColPos.p;
+        a.val = C.rowVal.p;
+        a.diag = C.gsDiag.p;
+        a.coef = C.upper.p;
+        a.source = srcPos;
+        a.psi = psiPos;
+        a.pA = base + 2 * static_cast<size_t>(kStaticCells);
+        a.wA = base + 3 * static_cast<size_t>(kStaticCells);
+        a.rA = base + 4 * static_cast<size_t>(kStaticCells);
+        a.rD = base + 5 * static_cast<size_t>(kStaticCells);
+        a.tolerance = tolerance;
+        a.relTol = relTol;
+        a.maxIter = 1000;
+        a.log = nullptr;
+        a.logCount = nullptr;
+        a.logCapacity = 0;
+        a.out = perf;
+        b2g::k::coarsestPcgDic<double><<<1, 32, 0, s>>>(a);
+        B2G_LAUNCH_CHECK();
+        if (n) b2g::k::fromPositions<double><<<grid, 256, 0, s>>>(n, L.gs.posCell.p, psiPos, psi);
+        B2G_LAUNCH_CHECK();
+        b2g::k::DevPerf h;
+        B2G_CUDA(cudaMemcpyAsync(&h, perf, sizeof(h), cudaMemcpyDeviceToHost, s));
+        B2G_CUDA(cudaStreamSynchronize(s));
+        out->initialResidual = h.initialResidual;
+        out->finalResidual = h.finalResidual;
+        out->nIterations = h.nIterations;
+    });
+}

@@ -93,6 +93,7 @@ def _load():
         "b2g_step_prolong": (ip, [vp, ip, vp, vp]),
         "b2g_level_norm_factor": (ip, [vp, ip, vp, vp, vp, C.POINTER(C.c_double)]),
         "b2g_level_pcg_dic": (ip, [vp, ip, vp, vp, dp, dp, C.POINTER(_Perf)]),
+        "b2g_level_pcg_dic_static": (ip, [vp, ip, vp, vp, dp, dp, C.POINTER(_Perf)]),
         "b2g_precondition": (ip, [vp, C.POINTER(Controls), vp, vp, C.POINTER(_Log)]),
         "b2g_matrix_pcg_solve": (ip, [vp, vp, vp, C.POINTER(Controls), ip, C.POINTER(_Perf),
                                       C.POINTER(_Log)]),
@@ -114,7 +115,7 @@ EXPORTED = [
     "b2g_gamg_solve", "b2g_matrix_create", "b2g_matrix_destroy", "b2g_matrix_get_level",
     "b2g_level_amul", "b2g_level_smooth", "b2g_level_scale", "b2g_step_restrict",
     "b2g_step_prolong", "b2g_level_norm_factor", "b2g_level_pcg_dic", "b2g_precondition",
-    "b2g_matrix_pcg_solve", "b2g_matrix_timings", "b2g_level_smooth_trace",
+    "b2g_matrix_pcg_solve", "b2g_matrix_timings", "b2g_level_smooth_trace", "b2g_level_pcg_dic_static",
 ]
 
 

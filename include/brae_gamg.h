@@ -243,6 +243,17 @@ B2G_API b2g_status b2g_level_norm_factor(b2g_matrix* m, int level, const double*
 /* The coarsest-level PCG-DIC (gamg_solver_cpp.cu:321-383) on level `level` from psi. */
 B2G_API b2g_status b2g_level_pcg_dic(b2g_matrix* m, int level, double* psi, const double* source,
                                      double tolerance, double relTol, b2g_perf* out);
+/* b2g_level_pcg_dic without any device allocation: no counterpart in the reference. For callers that
+ * may not allocate device memory during a solve (device memory owned by another allocator, or no
+ * room for the synchronisation cudaMalloc/cudaFree can bring). Its scratch vectors live in one
+ * static device array of the library (about 192 KiB, held on every GPU that loads the library until
+ * the process exits), so levels of at most 4096 cells are accepted; larger ones return
+ * B2G_ERR_ARGUMENT. The matrix's device must be current. The first call on a device looks the
+ * array's device address up (make it before any stream capture). Every call shares the array:
+ * calls that overlap on the GPU (other streams, other threads) race. Results are bit for bit those
+ * of b2g_level_pcg_dic. */
+B2G_API b2g_status b2g_level_pcg_dic_static(b2g_matrix* m, int level, double* psi, const double* source,
+                                            double tolerance, double relTol, b2g_perf* out);
 /* GAMGPreconditioner::precondition (gamg_solver_cpp.cu:1089-1107): w = M^-1 r, nVcycles V-cycles
  * from zero. `log` (may be NULL) receives the coarsest-level performances. */
 B2G_API b2g_status b2g_precondition(b2g_matrix* m, const b2g_controls* controls, double* w,
