@@ -530,13 +530,30 @@ b2g_status b2g_level_smooth_trace(b2g_matrix* m, int level, double* psi, const d
             schedule[3] = G.maxEnt;
             schedule[4] = G.maxDepth;
         }
-        need(trace == nullptr || traceCapacity >= 6 * G.nChunks + 4 * G.nParts, "b2g_level_smooth_trace: trace too small");
+        need(trace == nullptr || traceCapacity >= 8 * G.nChunks + 4 * G.nParts, "b2g_level_smooth_trace: trace too small");
         b2g::Matrix& A = *m->mat;
         A.toPos(level, static_cast<const double*>(psi), A.ioBuf(0));
         A.toPos(level, source, A.ioBuf(1));
         A.smooth<double>(level, B2G_SMOOTHER_GAUSS_SEIDEL, A.ioBuf(0), A.ioBuf(1), 1, trace);
         A.fromPos(level, static_cast<const double*>(A.ioBuf(0)), psi);
         A.checkDeviceError();
+    });
+}
+
+b2g_status b2g_level_schedule(const b2g_mesh* mesh, int level, int* partChunkStart, int* chunkRecords)
+{
+    return guarded([&] {
+        need(mesh != nullptr, "b2g_level_schedule: null mesh");
+        need(level >= 0 && level <= mesh->m.nLevels(), "b2g_level_schedule: level out of range");
+        const b2g::GsSchedule& G = mesh->m.lev[level].gs;
+        cudaStream_t s = mesh->m.stream;
+        if (partChunkStart && G.nParts)
+            B2G_CUDA(cudaMemcpyAsync(partChunkStart, G.partChunkStart.p, sizeof(int) * (G.nParts + 1),
+                                     cudaMemcpyDeviceToHost, s));
+        if (chunkRecords && G.nChunks)
+            B2G_CUDA(cudaMemcpyAsync(chunkRecords, G.chunkRec.p, sizeof(int) * 12 * (size_t)G.nChunks,
+                                     cudaMemcpyDeviceToHost, s));
+        B2G_CUDA(cudaStreamSynchronize(s));
     });
 }
 

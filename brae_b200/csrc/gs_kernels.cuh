@@ -13,24 +13,30 @@
 // its positions in order, cut into "chunks" of at most M cells of one depth. Cells of one depth do
 // not depend on each other, so a CTA barrier is needed only where the depth changes.
 //
-// THE CRITICAL PATH. A sweep takes about (DAG depth) x (time per chunk), so everything but the
-// row arithmetic is taken off the compute warps:
+// THE CRITICAL PATH. A sweep takes about (DAG depth) x (time per chunk), and a chunk's time is the
+// instruction stream of its rows (a lone warp issues about one instruction per 5 cycles of this
+// code), so everything but the row arithmetic is taken off the compute warps, and a row entry is
+// reduced to three loads (code, coefficient, value), a multiply and a subtraction:
 //   * a PRODUCER warp stages chunk j, S-1 chunks ahead, into one of S shared-memory slots: the
-//     chunk's contiguous data (diagonal, b, row descriptors, entry codes, coefficients) by TMA bulk
-//     copies, the psi window's old values ahead of the front (TMA), and the values the window does
-//     not hold by cp.async gathers; all of it completes on the slot's `full` mbarrier;
+//     chunk's blob (diagonal, row descriptors, coefficients, codes -- one contiguous TMA bulk copy)
+//     and b (a second one), the psi window's old values ahead of the front (TMA), and by cp.async
+//     the values the window does not hold; all of it completes on the slot's `full` mbarrier;
 //   * a SERVICE warp publishes the part's progress word and polls the upstream parts' words;
 //   * the COMPUTE warps (one thread per cell) wait on `full`, compute their rows from shared
 //     memory only, and release the slot warp by warp on its `empty` mbarrier.
+//
+// THE VALUE TABLE. One shared-memory array holds every value a row reads: [0, W) the psi window,
+// [W + s*G, W + (s+1)*G) the values gathered for the chunk in stage s, and W + S*G a zero. An entry
+// code is the 16-bit index of its value in the table: the schedule knows each chunk's stage (the
+// chunk's index in its part, mod S), so no code needs decoding.
 //
 // ENTRY LAYOUT (sliced ELL, per chunk). A chunk's entries are stored in slices of 32 cells (one
 // warp): entry q of the cell in lane l of a slice sits at sliceBase + 32*q + l, so a warp reads 32
 // consecutive codes and coefficients per entry -- free of shared-memory bank conflicts. A cell's
 // row descriptor is width << 24 | (its slice base + lane, relative to the chunk), the width being
 // the slice's longest row: every lane of a warp walks the same number of entries, the shorter rows
-// padded with entries that read a zero with coefficient zero (acc - 0*0 == acc, so the padding
-// leaves the result bit for bit as it is). Codes are 16 bits: bit 15 clear -> window slot
-// (position mod W); set -> index into the chunk's gathered values (the last index: the zero).
+// padded with entries that read the zero with coefficient zero (acc - 0*0 == acc, so the padding
+// leaves the result bit for bit as it is).
 //
 // WHAT THE WINDOW HOLDS. W positions of psi around the front: behind it the part's NEW values
 // (written as they are computed), ahead of it the OLD values (filled by TMA as the front advances).
@@ -47,8 +53,6 @@
 // up at once, so a broken schedule ends the kernel with an error instead of hanging the GPU.
 #pragma once
 
-#include <cuda_pipeline.h>
-
 #include "b2g_common.cuh"
 
 namespace b2g {
@@ -57,9 +61,8 @@ namespace k {
 constexpr int kWin = 4096;                     // W: psi window (positions), a power of two
 constexpr int kFill = 256;                     // B: window fill block (positions)
 constexpr int kStages = 6;                     // S: pipeline slots
-constexpr unsigned kGatBit = 0x8000u;          // code bit: gathered value
-constexpr int kMaxGat = 0x8000;                // gathered values per chunk, at most
-constexpr int kMaxCompute = 448;               // compute threads per CTA, at most (+ 2 warps)
+constexpr int kMaxTable = 65535;               // value-table entries a 16-bit code can name
+constexpr int kMaxCompute = 416;               // compute threads per CTA, at most (+ 3 warps)
 constexpr long long kSpinLimit = 1LL << 24;    // polls before a wait gives up
 
 // Window extents the schedule relies on for a chunk starting at s and ending at e: positions
@@ -74,14 +77,63 @@ inline void gsWindowExtents(int M, int& ahead, int& behind)
     behind = room - ahead;
 }
 
+__host__ __device__ inline unsigned r16(unsigned b) { return (b + 15u) & ~15u; }
+
+// A chunk's blob: [diagonal: m T][row descriptors: m u32][coefficients: nEnt T][codes: nEnt u16],
+// each part starting 16-byte aligned (nEnt is a multiple of 32).
+struct BlobLayout
+{
+    unsigned desc, val, code, bytes;
+};
+template <class T>
+__host__ __device__ inline BlobLayout blobLayout(int m, int nEnt)
+{
+    BlobLayout L;
+    L.desc = r16(static_cast<unsigned>(sizeof(T)) * m);
+    L.val = L.desc + r16(4u * m);
+    L.code = L.val + static_cast<unsigned>(sizeof(T)) * nEnt;
+    L.bytes = L.code + r16(2u * nEnt);
+    return L;
+}
+
 // Chunk record, 12 ints (three int4).
 struct ChunkRec
 {
     int pos0, m, ent0, nEnt;        // positions [pos0, pos0+m); ELL entries [ent0, ent0+nEnt)
     int gat0, nGat, depth, needUp;  // gather list [gat0, gat0+nGat); other-part owners' max depth or -1
-    int sameWait, newDepth, pad0, pad1;  // last same-part chunk a gather reads (global index) or -1;
-                                         // 1 where the depth changes within the part
+    int sameWait;                   // last same-part chunk a gather reads (global index) or -1
+    int newDepth, nOld;             // stored as newDepth | nOld << 1: 1 where the depth changes within
+                                    // the part; the gather list's leading old values (final already)
+    int blob64, blob32;             // the chunk's blob offset in 16-byte units (FP64 / FP32 blobs)
 };
+
+// The shared-memory footprint of the sweep: the value table, then S slots of
+// [blob | b | gather sources]. The sources (int positions) keep a 16-byte cover's lead.
+template <class T>
+__host__ __device__ inline unsigned tableBytes(int G)
+{
+    return r16(static_cast<unsigned>(sizeof(T)) * (kWin + kStages * G + 1));
+}
+template <class T>
+__host__ __device__ inline unsigned slotBOffset(int M, int E)
+{
+    return blobLayout<T>(M, E).bytes;
+}
+template <class T>
+__host__ __device__ inline unsigned slotListOffset(int M, int E)
+{
+    return slotBOffset<T>(M, E) + r16(static_cast<unsigned>(sizeof(T)) * (M + 8));
+}
+template <class T>
+__host__ __device__ inline unsigned slotBytes(int M, int E, int G)
+{
+    return slotListOffset<T>(M, E) + r16(4u * (G + 8));
+}
+template <class T>
+__host__ __device__ inline size_t gsSmemBytes(int M, int E, int G)
+{
+    return static_cast<size_t>(tableBytes<T>(G)) + kStages * static_cast<size_t>(slotBytes<T>(M, E, G));
+}
 
 template <class T>
 struct GsArgs
@@ -89,7 +141,7 @@ struct GsArgs
     int nParts;
     int maxCells;                  // M: chunk cell capacity (compute threads, a multiple of 32)
     int maxEnt;                    // E: chunk ELL entry capacity (a multiple of 32)
-    int maxGat;                    // chunk gather capacity; index maxGat-1 holds the zero
+    int maxGat;                    // G: gathered values per chunk (per stage in the table)
     int ahead;                     // window extent ahead of a chunk's start (positions)
     int nPadded;                   // psi is readable up to here (whole fill blocks)
     const int* __restrict__ partChunkStart;  // [P+1]
@@ -98,20 +150,18 @@ struct GsArgs
     const int* __restrict__ upStart;         // [P+1]
     const int* __restrict__ upList;
     const int* __restrict__ hasDown;         // [P] 1 if another part reads this part's values
-    const unsigned* __restrict__ posEnt;     // [n (+pad)] row descriptor by position
-    const unsigned short* __restrict__ entCode;  // [ELL entries]
-    const T* __restrict__ entVal;            // [ELL entries]
+    const unsigned char* __restrict__ blob;  // the chunks' blobs for this T
     const int* __restrict__ gatSrc;          // [gathers] position of each gathered value
-    const T* __restrict__ posDiag;           // [n (+pad)]
     const T* __restrict__ b;                 // [n (+pad)] by position
     T* psi;                                  // [n] by position, updated in place (padded)
     unsigned* progress;                      // [P]
     int* err;
     unsigned long long* trace;               // diagnostic, or null: [nChunks][4] clock64 stamps of
-                                             // compute thread 0 (start, data ready, computed,
-                                             // released), [P][4] {globaltimer, clock64} at the
-                                             // part's start and end, [nChunks][2] producer stamps
-                                             // (start, copies issued)
+                                             // compute thread 0 (start, staged data ready,
+                                             // computed, released), [P][4] {globaltimer, clock64}
+                                             // at the part's start and end, [nChunks][4] producer
+                                             // stamps (start, slot free, copies issued, gathers
+                                             // issued)
 };
 
 __device__ __forceinline__ unsigned long long globalTimer()
@@ -160,14 +210,29 @@ __device__ __forceinline__ bool mbarTryWait(unsigned long long* bar, unsigned pa
         : "memory");
     return ok != 0;
 }
-// 1-D TMA bulk copy global -> shared, completing on `bar`. dst, src 16-byte aligned; bytes % 16 == 0.
-__device__ __forceinline__ void tmaLoad(void* dst, const void* src, unsigned bytes, unsigned long long* bar)
+// 1-D TMA bulk copy global -> shared (32-bit shared address), completing on `bar`. dst, src
+// 16-byte aligned; bytes % 16 == 0.
+__device__ __forceinline__ void tmaLoad(unsigned dst, const void* src, unsigned bytes, unsigned long long* bar)
 {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smemAddr(dst)),
+                     dst),
                  "l"(src), "r"(bytes), "r"(smemAddr(bar))
                  : "memory");
 }
+// one 8- or 4-byte cp.async global -> shared (32-bit shared address)
+__device__ __forceinline__ void cpAsync(unsigned dst, const double* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpAsync(unsigned dst, const float* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void fenceProxyAsyncShared()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 // Shared-memory accesses by 32-bit address (volatile: they stay ordered against the barrier waits)
 __device__ __forceinline__ unsigned ldsU32(unsigned a)
 {
@@ -196,11 +261,6 @@ __device__ __forceinline__ float ldsT(unsigned a, float)
 __device__ __forceinline__ void stsT(unsigned a, double v) { asm volatile("st.shared.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory"); }
 __device__ __forceinline__ void stsT(unsigned a, float v) { asm volatile("st.shared.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory"); }
 
-__device__ __forceinline__ void fenceProxyAsyncShared()
-{
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
 // A 16-byte-aligned cover of elements [i0, i0 + cnt) of an array whose base is 16-byte aligned.
 struct Cover
 {
@@ -222,47 +282,6 @@ __host__ __device__ __forceinline__ Cover coverOf(const E* base, long long i0, i
     return c;
 }
 
-template <class T>
-struct Slot
-{
-    T* diag;               // M + 8 (16-byte covers of position-indexed data: a lead and a tail)
-    T* b;                  // M + 8
-    unsigned* ent;         // M + 8
-    T* val;                // E (chunk entry ranges are whole slices: no cover slack)
-    unsigned short* code;  // E
-    T* gat;                // Gcap (the last one holds zero: what padding entries read)
-};
-
-// Every array's byte size is rounded up to 16 so the next one stays 16-byte aligned.
-__host__ __device__ inline size_t r16(size_t b) { return (b + 15) & ~size_t(15); }
-
-template <class T>
-__host__ __device__ inline size_t slotBytes(int M, int E, int G)
-{
-    return 2 * r16(sizeof(T) * (M + 8)) + r16(sizeof(unsigned) * (M + 8)) + r16(sizeof(T) * E) +
-           r16(sizeof(unsigned short) * E) + r16(sizeof(T) * G);
-}
-
-template <class T>
-__host__ __device__ inline size_t gsSmemBytes(int M, int E, int G)
-{
-    return sizeof(T) * kWin + kStages * slotBytes<T>(M, E, G);
-}
-
-template <class T>
-__device__ __forceinline__ Slot<T> slotAt(unsigned char* base, int M, int E)
-{
-    Slot<T> s;
-    unsigned char* p = base;
-    s.diag = reinterpret_cast<T*>(p); p += r16(sizeof(T) * (M + 8));
-    s.b = reinterpret_cast<T*>(p); p += r16(sizeof(T) * (M + 8));
-    s.ent = reinterpret_cast<unsigned*>(p); p += r16(sizeof(unsigned) * (M + 8));
-    s.val = reinterpret_cast<T*>(p); p += r16(sizeof(T) * E);
-    s.code = reinterpret_cast<unsigned short*>(p); p += r16(sizeof(unsigned short) * E);
-    s.gat = reinterpret_cast<T*>(p);
-    return s;
-}
-
 __device__ __forceinline__ ChunkRec loadChunkRec(const int4* __restrict__ recs, int c)
 {
     const int4 a = recs[3 * (size_t)c];
@@ -271,8 +290,13 @@ __device__ __forceinline__ ChunkRec loadChunkRec(const int4* __restrict__ recs, 
     ChunkRec r;
     r.pos0 = a.x; r.m = a.y; r.ent0 = a.z; r.nEnt = a.w;
     r.gat0 = b.x; r.nGat = b.y; r.depth = b.z; r.needUp = b.w;
-    r.sameWait = d.x; r.newDepth = d.y; r.pad0 = d.z; r.pad1 = d.w;
+    r.sameWait = d.x; r.newDepth = d.y & 1; r.nOld = d.y >> 1; r.blob64 = d.z; r.blob32 = d.w;
     return r;
+}
+template <class T>
+__host__ __device__ __forceinline__ int blobOf(const ChunkRec& r)
+{
+    return sizeof(T) == 8 ? r.blob64 : r.blob32;
 }
 
 __device__ __forceinline__ unsigned ldAcquireCta(const unsigned* p)
@@ -324,91 +348,107 @@ __device__ __forceinline__ void waitShared(const unsigned* w, unsigned target, i
     }
 }
 
-// One Gauss-Seidel sweep of one level, in position order. Grid = P parts; blockDim = M + 64:
-// M compute threads, then the producer warp, then the service warp.
+// K entries of a row, straight-line: the codes and coefficients (independent loads at fixed
+// offsets), then the values, then the reference's rounding chain in entry order.
+template <class T, int K>
+__device__ __forceinline__ T rowTerms(T acc, unsigned cA, unsigned vA, unsigned tableA)
+{
+    unsigned c[K];
+    T w[K], v[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q)
+    {
+        c[q] = ldsU16(cA + 64u * q);
+        w[q] = ldsT(vA + 32u * static_cast<unsigned>(sizeof(T)) * q, T());
+    }
+#pragma unroll
+    for (int q = 0; q < K; ++q) v[q] = ldsT(tableA + static_cast<unsigned>(sizeof(T)) * c[q], T());
+#pragma unroll
+    for (int q = 0; q < K; ++q) acc = subRn(acc, mulRn(w[q], v[q]));
+    return acc;
+}
+
+// One Gauss-Seidel sweep of one level, in position order. Grid = P parts; blockDim = M + 96:
+// M compute threads, then the TMA warp, the gather warp and the service warp.
 template <class T>
-__global__ void __launch_bounds__(kMaxCompute + 64, 1) gsSweep(GsArgs<T> a)
+__global__ void __launch_bounds__(kMaxCompute + 96, 1) gsSweep(GsArgs<T> a)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) unsigned long long full[kStages];
     __shared__ __align__(8) unsigned long long empty[kStages];
-    __shared__ unsigned chunksDone;   // chunks of this part all compute warps finished (for progress)
+    __shared__ __align__(8) unsigned long long lists[kStages];  // a stage's record and gather sources
+    __shared__ __align__(16) int4 srec[kStages][3];              // the staged chunk's record
+    __shared__ unsigned pubDepth;     // every cell of this part below this depth is done (compute ->
+                                      // service warp; 0x7fffffff at the end)
     __shared__ unsigned upMin;        // least progress seen among the upstream parts
+    constexpr unsigned kT = sizeof(T);
     const int M = a.maxCells;
-    const int E = a.maxEnt;
-    T* win = reinterpret_cast<T*>(smem);
-    unsigned char* slots = smem + sizeof(T) * kWin;
-    const size_t sb = slotBytes<T>(M, E, a.maxGat);
+    const int G = a.maxGat;
+    const unsigned tableA = smemAddr(smem);
+    const unsigned slotsA = tableA + tableBytes<T>(G);
+    const unsigned sb = slotBytes<T>(M, a.maxEnt, G);
+    const unsigned bOff = slotBOffset<T>(M, a.maxEnt);     // b follows the blob in a slot
+    const unsigned lOff = slotListOffset<T>(M, a.maxEnt);  // then the gather sources
     const int p = blockIdx.x;
     const int t = threadIdx.x;
     const int c0 = a.partChunkStart[p];
     const int nCh = a.partChunkStart[p + 1] - c0;
     const int nComputeWarps = M >> 5;
-    if (t < kStages)
-    {
-        T* g = slotAt<T>(slots + t * sb, M, E).gat;
-        g[a.maxGat - 1] = T(0);
-    }
     if (t == 0)
     {
-        chunksDone = 0u;
+        stsT(tableA + kT * static_cast<unsigned>(kWin + kStages * G), T(0));  // what padding entries read
+        pubDepth = nCh > 0 ? static_cast<unsigned>(a.chunkRec[3 * (size_t)c0 + 1].z) : 0x7fffffffu;
         upMin = 0u;
         for (int s = 0; s < kStages; ++s)
         {
-            mbarInit(&full[s], 1 + 32);        // the producer's expect_tx + its 32 lanes' gathers
+            mbarInit(&full[s], 1 + 32);        // the TMA warp's expect_tx + the gather warp's 32 lanes
             mbarInit(&empty[s], nComputeWarps);
+            mbarInit(&lists[s], 1);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         fenceProxyAsyncShared();
     }
     __syncthreads();
-    auto slotOf = [&](int j) { return slotAt<T>(slots + (j % kStages) * sb, M, E); };
 
-    if (t >= M + 32)
+    if (t >= M + 64)
     {
         // ---------------- service warp: progress out, upstream progress in ----------------
-        const int lane = t - M - 32;
+        // Everything it polls is in shared memory or in registers, but the upstream parts' progress
+        // words: one L2 round trip per poll.
+        const int lane = t - M - 64;
         const int upBeg = a.upStart[p];
-        const int upEnd = a.upStart[p + 1];
+        const int nUp = a.upStart[p + 1] - upBeg;
+        const int myUp = lane < nUp ? a.upList[upBeg + lane] : -1;  // parts beyond 32: read per poll
         const bool publish = a.hasDown[p] != 0;
-        unsigned published = 0u;
-        if (publish && lane == 0 && nCh > 0)
-        {
-            published = static_cast<unsigned>(a.chunkRec[3 * (size_t)c0 + 1].z);
-            stRelease(&a.progress[p], published);  // nothing of this part lies below its first depth
-        }
+        unsigned published = 0xffffffffu;
         long long it = 0;
-        unsigned lastDone = 0u;
         while (true)
         {
             // one value for the whole warp: lanes must agree before the shuffles below
-            const unsigned done = __shfl_sync(0xffffffffu, ldAcquireCta(&chunksDone), 0);
-            if (publish && done != lastDone)
+            const unsigned v = __shfl_sync(0xffffffffu, ldAcquireCta(&pubDepth), 0);
+            if (publish && v != published)
             {
-                lastDone = done;
-                const unsigned v = done < static_cast<unsigned>(nCh)
-                                       ? static_cast<unsigned>(a.chunkRec[3 * (size_t)(c0 + done) + 1].z)
-                                       : 0x7fffffffu;
-                if (lane == 0 && v > published)
-                {
-                    __threadfence();
-                    stRelease(&a.progress[p], v);
-                    published = v;
-                }
+                // release at GPU scope: cumulative over the psi stores the compute warps made before
+                // their barrier and their release of pubDepth, which this warp acquired
+                if (lane == 0) stRelease(&a.progress[p], v);
+                published = v;
             }
-            if (done >= static_cast<unsigned>(nCh)) break;
-            if (upEnd > upBeg)
+            if (v == 0x7fffffffu) break;
+            if (nUp > 0)
             {
-                unsigned m = 0xffffffffu;
-                for (int i = upBeg + lane; i < upEnd; i += 32) m = min(m, ldAcquire(&a.progress[a.upList[i]]));
+                unsigned m = myUp >= 0 ? ldAcquire(&a.progress[myUp]) : 0xffffffffu;
+                for (int i = upBeg + 32 + lane; i < upBeg + nUp; i += 32) m = min(m, ldAcquire(&a.progress[a.upList[i]]));
                 for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
                 if (lane == 0 && m > ldAcquireCta(&upMin)) stReleaseCta(&upMin, m);
             }
-            if (__shfl_sync(0xffffffffu, errSet(a.err) ? 1 : 0, 0)) break;
-            if (++it > 16 * kSpinLimit)
+            if ((++it & 63) == 0)
             {
-                if (lane == 0) atomicExch(a.err, 1);
-                break;
+                if (__shfl_sync(0xffffffffu, errSet(a.err) ? 1 : 0, 0)) break;
+                if (it > 16 * kSpinLimit)
+                {
+                    if (lane == 0) atomicExch(a.err, 1);
+                    break;
+                }
             }
             __nanosleep(20);
         }
@@ -417,76 +457,91 @@ __global__ void __launch_bounds__(kMaxCompute + 64, 1) gsSweep(GsArgs<T> a)
 
     if (t >= M)
     {
-        // ---------------- producer warp: stages chunk j into slot j % S ----------------
-        const int lane = t - M;
-        const int partEnd = a.partPosStart[p + 1];
-        const int fillEnd = min(a.nPadded, ((partEnd + kFill - 1) / kFill) * kFill);
-        int filled = (a.partPosStart[p] / kFill) * kFill;  // window filled up to here
-        // the next chunk's record and first gather sources are loaded a chunk ahead, off the path
-        // from a free slot to its copies
-        constexpr int kPre = 4;
-        ChunkRec nx = nCh > 0 ? loadChunkRec(a.chunkRec, c0) : ChunkRec{};
-        int pre[kPre];
-#pragma unroll
-        for (int k = 0; k < kPre; ++k) pre[k] = (nCh > 0 && lane + 32 * k < nx.nGat) ? a.gatSrc[nx.gat0 + lane + 32 * k] : 0;
+        // ---------------- staging: chunk j into slot j % S, by two warps ----------------
+        // The TMA warp (one lane) issues the bulk copies; the gather warp issues the gathers and
+        // waits for what they need, so a wait for an upstream part never delays the bulk copies of
+        // the chunks behind it. Chunk records and gather sources are loaded two chunks ahead: no
+        // iteration waits for a load it issued itself.
         unsigned long long* ptr = a.trace ? a.trace + 4 * (size_t)a.partChunkStart[a.nParts] + 4 * (size_t)a.nParts : nullptr;
-        for (int j = 0; j < nCh; ++j)
+        if (t < M + 32)
         {
-            const int s = j % kStages;
-            const ChunkRec cr = nx;
-            int src[kPre];
-#pragma unroll
-            for (int k = 0; k < kPre; ++k) src[k] = pre[k];
-            if (j + 1 < nCh)
+            if (t != M) return;
+            const int partEnd = a.partPosStart[p + 1];
+            const int fillEnd = min(a.nPadded, ((partEnd + kFill - 1) / kFill) * kFill);
+            int filled = (a.partPosStart[p] / kFill) * kFill;  // window filled up to here
+            ChunkRec r1 = nCh > 0 ? loadChunkRec(a.chunkRec, c0) : ChunkRec{};
+            ChunkRec r2 = nCh > 1 ? loadChunkRec(a.chunkRec, c0 + 1) : ChunkRec{};
+            int s = 0;
+            for (int j = 0; j < nCh; ++j)
             {
-                nx = loadChunkRec(a.chunkRec, c0 + j + 1);
-#pragma unroll
-                for (int k = 0; k < kPre; ++k)
-                    pre[k] = lane + 32 * k < nx.nGat ? a.gatSrc[nx.gat0 + lane + 32 * k] : 0;
-            }
-            if (ptr && lane == 0) ptr[2 * (size_t)(c0 + j)] = clockStamp();
-            if (j >= kStages) waitMbar(&empty[s], static_cast<unsigned>((j / kStages - 1) & 1), a.err);
-            const Slot<T> sl = slotOf(j);
-            if (lane == 0)
-            {
-                const Cover cd = coverOf(a.posDiag, cr.pos0, cr.m);
+                const ChunkRec cr = r1;
+                r1 = r2;
+                if (j + 2 < nCh) r2 = loadChunkRec(a.chunkRec, c0 + j + 2);
+                if (ptr) ptr[4 * (size_t)(c0 + j)] = clockStamp();
+                if (j >= kStages) waitMbar(&empty[s], static_cast<unsigned>((j / kStages - 1) & 1), a.err);
+                if (ptr) ptr[4 * (size_t)(c0 + j) + 1] = clockStamp();
+                const unsigned slotA = slotsA + static_cast<unsigned>(s) * sb;
+                // the record and the gather sources first: the gather warp starts from them
+                const int4* rg = a.chunkRec + 3 * (size_t)(c0 + j);
+                srec[s][0] = rg[0];
+                srec[s][1] = rg[1];
+                srec[s][2] = rg[2];
+                const Cover cl = coverOf(a.gatSrc, cr.gat0, cr.nGat);
+                mbarExpectTx(&lists[s], cr.nGat ? cl.bytes : 0u);
+                if (cr.nGat) tmaLoad(slotA + lOff, cl.src, cl.bytes, &lists[s]);
+                const BlobLayout bl = blobLayout<T>(cr.m, cr.nEnt);
                 const Cover cbv = coverOf(a.b, cr.pos0, cr.m);
-                const Cover cen = coverOf(a.posEnt, cr.pos0, cr.m);
-                const unsigned vBytes = static_cast<unsigned>(sizeof(T) * cr.nEnt);
-                const unsigned cBytes = static_cast<unsigned>(sizeof(unsigned short) * cr.nEnt);
                 const int target = min(fillEnd, ((cr.pos0 + a.ahead + kFill - 1) / kFill) * kFill);
                 const int nFill = target > filled ? (target - filled) / kFill : 0;
-                const unsigned total = cd.bytes + cbv.bytes + cen.bytes + vBytes + cBytes +
-                                       static_cast<unsigned>(nFill) * kFill * sizeof(T);
-                mbarExpectTx(&full[s], total);
-                tmaLoad(sl.diag, cd.src, cd.bytes, &full[s]);
-                tmaLoad(sl.b, cbv.src, cbv.bytes, &full[s]);
-                tmaLoad(sl.ent, cen.src, cen.bytes, &full[s]);
-                if (cr.nEnt)
-                {
-                    tmaLoad(sl.val, a.entVal + cr.ent0, vBytes, &full[s]);
-                    tmaLoad(sl.code, a.entCode + cr.ent0, cBytes, &full[s]);
-                }
+                mbarExpectTx(&full[s], bl.bytes + cbv.bytes + static_cast<unsigned>(nFill) * kFill * kT);
+                tmaLoad(slotA, a.blob + 16 * static_cast<size_t>(blobOf<T>(cr)), bl.bytes, &full[s]);
+                tmaLoad(slotA + bOff, cbv.src, cbv.bytes, &full[s]);
                 for (int f = 0; f < nFill; ++f, filled += kFill)
-                    tmaLoad(win + (filled & (kWin - 1)), a.psi + filled, kFill * sizeof(T), &full[s]);
-                // gathered values must be final: owners of other parts once those parts are far
+                    tmaLoad(tableA + kT * static_cast<unsigned>(filled & (kWin - 1)), a.psi + filled, kFill * kT,
+                            &full[s]);
+                if (ptr) ptr[4 * (size_t)(c0 + j) + 2] = clockStamp();
+                if (++s == kStages) s = 0;
+            }
+            return;
+        }
+        const int lane = t - M - 32;
+        int s = 0;
+        unsigned phase = 0u;
+        for (int j = 0; j < nCh; ++j)
+        {
+            // the TMA warp published this stage's record and sources once the slot was free
+            waitMbar(&lists[s], phase, a.err);
+            const int4 rb1 = srec[s][1];
+            const int4 rb2 = srec[s][2];
+            const int gat0 = rb1.x, nGat = rb1.y, needUp = rb1.w, sameWait = rb2.x, nOld = rb2.y >> 1;
+            const unsigned listA = slotsA + static_cast<unsigned>(s) * sb + lOff +
+                                   4u * static_cast<unsigned>(coverOf(a.gatSrc, gat0, 0).lead);
+            const unsigned gA = tableA + kT * static_cast<unsigned>(kWin + s * G);
+            // the old values first: they are final as they are
+            for (int g = lane; g < nOld; g += 32)
+                cpAsync(gA + kT * static_cast<unsigned>(g), &a.psi[static_cast<int>(ldsU32(listA + 4u * g))]);
+            if (lane == 0)
+            {
+                // gathered new values must be final: owners of other parts once those parts are far
                 // enough along, owners of this part once their chunk is consumed (chunk sw is done
-                // when empty[sw % S] completes phase sw / S; the wait for slot j - S above already
+                // when empty[sw % S] completes phase sw / S; the slot wait for chunk j already
                 // covers every chunk up to j - S, and phase sw / S + 1 needs chunk sw + S > j, so
                 // the parity is unambiguous)
-                if (cr.needUp >= 0) waitShared(&upMin, static_cast<unsigned>(cr.needUp) + 1u, a.err);
-                const int sw = cr.sameWait - c0;
-                if (cr.sameWait >= 0 && sw > j - kStages)
+                if (needUp >= 0) waitShared(&upMin, static_cast<unsigned>(needUp) + 1u, a.err);
+                const int sw = sameWait - c0;
+                if (sameWait >= 0 && sw > j - kStages)
                     waitMbar(&empty[sw % kStages], static_cast<unsigned>((sw / kStages) & 1), a.err);
             }
             __syncwarp();
-#pragma unroll
-            for (int k = 0; k < kPre; ++k)
-                if (lane + 32 * k < cr.nGat) __pipeline_memcpy_async(&sl.gat[lane + 32 * k], &a.psi[src[k]], sizeof(T));
-            for (int g = lane + 32 * kPre; g < cr.nGat; g += 32)
-                __pipeline_memcpy_async(&sl.gat[g], &a.psi[a.gatSrc[cr.gat0 + g]], sizeof(T));
+            for (int g = nOld + lane; g < nGat; g += 32)
+                cpAsync(gA + kT * static_cast<unsigned>(g), &a.psi[static_cast<int>(ldsU32(listA + 4u * g))]);
             mbarArriveCpAsync(&full[s]);
-            if (ptr && lane == 0) ptr[2 * (size_t)(c0 + j) + 1] = clockStamp();
+            if (ptr && lane == 0) ptr[4 * (size_t)(c0 + j) + 3] = clockStamp();
+            if (++s == kStages)
+            {
+                s = 0;
+                phase ^= 1u;
+            }
         }
         return;
     }
@@ -499,67 +554,53 @@ __global__ void __launch_bounds__(kMaxCompute + 64, 1) gsSweep(GsArgs<T> a)
         ptrace[0] = globalTimer();
         ptrace[1] = clockStamp();
     }
-    // 32-bit shared addresses: the window, and slot 0's arrays (slot s is sb bytes further on)
-    const unsigned winA = smemAddr(win);
-    const Slot<T> s0 = slotAt<T>(slots, M, E);
-    const unsigned diagA = smemAddr(s0.diag), bA = smemAddr(s0.b), entA = smemAddr(s0.ent);
-    const unsigned valA = smemAddr(s0.val), codeA = smemAddr(s0.code), gatA = smemAddr(s0.gat);
-    const unsigned sb32 = static_cast<unsigned>(sb);
-    constexpr unsigned kT = sizeof(T);
-    ChunkRec nx = nCh > 0 ? loadChunkRec(a.chunkRec, c0) : ChunkRec{};
     int s = 0;
     unsigned phase = 0u;
     for (int j = 0; j < nCh; ++j)
     {
-        const ChunkRec cr = nx;
-        if (j + 1 < nCh) nx = loadChunkRec(a.chunkRec, c0 + j + 1);
         if (a.trace && t == 0) a.trace[4 * (size_t)(c0 + j)] = clockStamp();
+        // the record is published with the stage's gather sources, well before the data: the
+        // progress this part publishes at a depth change must not wait for this chunk's data
+        waitMbar(&lists[s], phase, a.err);
+        const ChunkRec cr = loadChunkRec(srec[s], 0);
         if (cr.newDepth && j > 0)
         {
-            // the owners this chunk reads were computed by any compute warp: wait for all of them
+            // the owners this chunk reads were computed by any compute warp: wait for all of them;
+            // then every cell of this part below this chunk's depth is done
             computeSync(M);
-            if (t == 0) stReleaseCta(&chunksDone, static_cast<unsigned>(j));
+            if (t == 0) stReleaseCta(&pubDepth, static_cast<unsigned>(cr.depth));
         }
         waitMbar(&full[s], phase, a.err);
         if (a.trace && t == 0) a.trace[4 * (size_t)(c0 + j) + 1] = clockStamp();
         if (t < cr.m)
         {
-            const unsigned so = static_cast<unsigned>(s) * sb32;
-            // leads of the 16-byte covers the producer copied (diagonal and b: T; descriptors: u32)
-            const unsigned lT = (static_cast<unsigned>(cr.pos0) * kT & 15u) / kT;
-            const unsigned lE = static_cast<unsigned>(cr.pos0) & 3u;
-            const unsigned pe = ldsU32(entA + so + 4u * (lE + t));
-            T acc = ldsT(bA + so + kT * (lT + t), T());
-            const T dg = ldsT(diagA + so + kT * (lT + t), T());
+            const unsigned slotA = slotsA + static_cast<unsigned>(s) * sb;
+            const BlobLayout bl = blobLayout<T>(cr.m, cr.nEnt);
+            const unsigned lb = (static_cast<unsigned>(cr.pos0) * kT & 15u) / kT;  // lead of b's cover
+            const unsigned pe = ldsU32(slotA + bl.desc + 4u * t);
+            T acc = ldsT(slotA + bOff + kT * (lb + t), T());
+            const T dg = ldsT(slotA + kT * t, T());
             const int width = static_cast<int>(pe >> 24);
             const unsigned rb = pe & 0xffffffu;
-            const unsigned cA = codeA + so + 2u * rb;
-            const unsigned vA = valA + so + kT * rb;
-            const unsigned gA = gatA + so;
-            constexpr int kRegs = 8;
-            for (int q0 = 0; q0 < width; q0 += kRegs)
+            unsigned cA = slotA + bl.code + 2u * rb;
+            unsigned vA = slotA + bl.val + kT * rb;
+            int left = width;
+            for (; left >= 8; left -= 8, cA += 64u * 8, vA += 32u * kT * 8) acc = rowTerms<T, 8>(acc, cA, vA, tableA);
+            // the width is the same for the whole warp: this switch does not diverge
+            switch (left)
             {
-                // width is the same for the whole warp: these branches do not diverge
-                unsigned c[kRegs];
-                T w[kRegs], v[kRegs];
-#pragma unroll
-                for (int q = 0; q < kRegs; ++q)
-                    if (q0 + q < width)
-                    {
-                        c[q] = ldsU16(cA + 64u * (q0 + q));
-                        w[q] = ldsT(vA + 32u * kT * (q0 + q), T());
-                    }
-#pragma unroll
-                for (int q = 0; q < kRegs; ++q)
-                    if (q0 + q < width)
-                        v[q] = ldsT((c[q] & kGatBit) ? gA + kT * (c[q] & (kGatBit - 1u)) : winA + kT * c[q], T());
-#pragma unroll
-                for (int q = 0; q < kRegs; ++q)
-                    if (q0 + q < width) acc = subRn(acc, mulRn(w[q], v[q]));
+            case 7: acc = rowTerms<T, 7>(acc, cA, vA, tableA); break;
+            case 6: acc = rowTerms<T, 6>(acc, cA, vA, tableA); break;
+            case 5: acc = rowTerms<T, 5>(acc, cA, vA, tableA); break;
+            case 4: acc = rowTerms<T, 4>(acc, cA, vA, tableA); break;
+            case 3: acc = rowTerms<T, 3>(acc, cA, vA, tableA); break;
+            case 2: acc = rowTerms<T, 2>(acc, cA, vA, tableA); break;
+            case 1: acc = rowTerms<T, 1>(acc, cA, vA, tableA); break;
+            default: break;
             }
             const T res = divRn(acc, dg);
             const int pos = cr.pos0 + t;
-            stsT(winA + kT * static_cast<unsigned>(pos & (kWin - 1)), res);
+            stsT(tableA + kT * static_cast<unsigned>(pos & (kWin - 1)), res);
             // this window slot is refilled by TMA (the async proxy) one window later; the fence comes
             // before the global store so that it does not wait for that store
             fenceProxyAsyncShared();
@@ -576,11 +617,42 @@ __global__ void __launch_bounds__(kMaxCompute + 64, 1) gsSweep(GsArgs<T> a)
         }
     }
     computeSync(M);
-    if (t == 0) stReleaseCta(&chunksDone, static_cast<unsigned>(nCh));
+    if (t == 0) stReleaseCta(&pubDepth, 0x7fffffffu);
     if (ptrace && t == 0)
     {
         ptrace[2] = globalTimer();
         ptrace[3] = clockStamp();
+    }
+}
+
+// The chunk blobs of one level in value type T (one block per chunk): the diagonal and row
+// descriptors by position, the coefficients and codes by ELL entry.
+template <class T>
+__global__ void buildChunkBlobs(int nCh, const int4* __restrict__ recs, const T* __restrict__ posDiag,
+                                const unsigned* __restrict__ posEnt, const unsigned short* __restrict__ code,
+                                const int* __restrict__ entFace, const double* __restrict__ upper,
+                                unsigned char* __restrict__ blob)
+{
+    for (int c = blockIdx.x; c < nCh; c += gridDim.x)
+    {
+        const ChunkRec r = loadChunkRec(recs, c);
+        const BlobLayout L = blobLayout<T>(r.m, r.nEnt);
+        unsigned char* b = blob + 16 * static_cast<size_t>(blobOf<T>(r));
+        T* dg = reinterpret_cast<T*>(b);
+        unsigned* ds = reinterpret_cast<unsigned*>(b + L.desc);
+        T* vl = reinterpret_cast<T*>(b + L.val);
+        unsigned short* cd = reinterpret_cast<unsigned short*>(b + L.code);
+        for (int i = threadIdx.x; i < r.m; i += blockDim.x)
+        {
+            dg[i] = posDiag[r.pos0 + i];
+            ds[i] = posEnt[r.pos0 + i];
+        }
+        for (int e = threadIdx.x; e < r.nEnt; e += blockDim.x)
+        {
+            const int f = entFace[r.ent0 + e];
+            vl[e] = f >= 0 ? static_cast<T>(upper[f]) : T(0);
+            cd[e] = code[r.ent0 + e];
+        }
     }
 }
 

@@ -557,13 +557,14 @@ struct EntryClass
     }
 };
 
-// pass 1: gathers per position; per chunk the waits they need (other parts' owners: their deepest
-// depth; this part's owners outside the window: their latest chunk), and the upstream part bits
+// pass 1: gathers per position, of old values (neighbours: final as they are) and of new values
+// (owners); per chunk the waits the new ones need (other parts' owners: their deepest depth; this
+// part's owners outside the window: their latest chunk), and the upstream part bits
 __global__ void kGatherCounts(int n, EntryClass ec, const int* __restrict__ order, const int* __restrict__ posOf,
                               const int* __restrict__ depth, const int* __restrict__ rowStart,
                               const int* __restrict__ losortStart, const int* __restrict__ col,
-                              int* __restrict__ cnt, int* __restrict__ chunkNeedUp, int* __restrict__ chunkSameWait,
-                              unsigned* __restrict__ upBits, int words)
+                              int* __restrict__ cntOld, int* __restrict__ cntNew, int* __restrict__ chunkNeedUp,
+                              int* __restrict__ chunkSameWait, unsigned* __restrict__ upBits, int words)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -572,7 +573,7 @@ __global__ void kGatherCounts(int n, EntryClass ec, const int* __restrict__ orde
     const int ch = ec.chunkOf[i];
     const int rb = rowStart[c];
     const int nLower = losortStart[c + 1] - losortStart[c];
-    int g = 0;
+    int gOld = 0, gNew = 0;
     for (int e = rb; e < rowStart[c + 1]; ++e)
     {
         const int o = col[e];
@@ -580,8 +581,12 @@ __global__ void kGatherCounts(int n, EntryClass ec, const int* __restrict__ orde
         const bool lowerSide = e - rb < nLower;
         const bool same = ec.partOf[o] == p;
         if (ec.window(lowerSide, same, q, ch)) continue;
-        ++g;
-        if (!lowerSide) continue;  // an old value: final as it is
+        if (!lowerSide)
+        {
+            ++gOld;  // an old value: final as it is
+            continue;
+        }
+        ++gNew;
         if (same)
             atomicMax(&chunkSameWait[ch], ec.chunkOf[q]);
         else
@@ -591,17 +596,20 @@ __global__ void kGatherCounts(int n, EntryClass ec, const int* __restrict__ orde
             atomicOr(&upBits[(size_t)p * words + (po >> 5)], 1u << (po & 31));
         }
     }
-    cnt[i] = g;
+    cntOld[i] = gOld;
+    cntNew[i] = gNew;
 }
 
-// pass 2: the sliced-ELL entries (codes and faces) and the gather lists; entries past a row's end
-// keep the padding code and face -1 they were filled with
-__global__ void kSweepEntries(int n, EntryClass ec, const int* __restrict__ order, const int* __restrict__ posOf,
+// pass 2: the sliced-ELL entries (codes and faces) and the gather lists, each chunk's list holding
+// its old values first, then its new ones; entries past a row's end keep the padding code and
+// face -1 they were filled with
+__global__ void kSweepEntries(int n, EntryClass ec, int maxGat, const int* __restrict__ partChunkStart,
+                              const int* __restrict__ order, const int* __restrict__ posOf,
                               const int* __restrict__ rowStart, const int* __restrict__ losortStart,
                               const int* __restrict__ col, const int* __restrict__ entFace,
                               const unsigned* __restrict__ posEnt, const long long* __restrict__ chunkEnt0,
-                              const int* __restrict__ gatOff, unsigned short* __restrict__ code,
-                              int* __restrict__ face, int* __restrict__ gatSrc)
+                              const int* __restrict__ oldOff, const int* __restrict__ newOff,
+                              unsigned short* __restrict__ code, int* __restrict__ face, int* __restrict__ gatSrc)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -610,9 +618,15 @@ __global__ void kSweepEntries(int n, EntryClass ec, const int* __restrict__ orde
     const int ch = ec.chunkOf[i];
     const int rb = rowStart[c];
     const int nLower = losortStart[c + 1] - losortStart[c];
-    const long long base = chunkEnt0[ch] + static_cast<long long>(posEnt[i] & 0xffffffu);
-    const int g0 = gatOff[ec.chunkStart[ch]];
-    int g = gatOff[i];
+    const long long ell = chunkEnt0[ch] + static_cast<long long>(posEnt[i] & 0xffffffu);
+    // the chunk's gathered values sit in its stage's part of the value table
+    const int stage = (ch - partChunkStart[p]) % k::kStages;
+    const int cs = ec.chunkStart[ch];
+    const int ce = ec.chunkStart[ch + 1];
+    const int base = oldOff[cs] + newOff[cs];
+    const int g0 = base - (k::kWin + stage * maxGat);
+    int gOld = base + (oldOff[i] - oldOff[cs]);
+    int gNew = base + (oldOff[ce] - oldOff[cs]) + (newOff[i] - newOff[cs]);
     for (int e = rb; e < rowStart[c + 1]; ++e)
     {
         const int k = e - rb;
@@ -623,18 +637,21 @@ __global__ void kSweepEntries(int n, EntryClass ec, const int* __restrict__ orde
         if (ec.window(k < nLower, same, q, ch)) cd = static_cast<unsigned short>(q & (ec.win - 1));
         else
         {
-            cd = static_cast<unsigned short>(k::kGatBit | static_cast<unsigned>(g - g0));
+            int& g = k < nLower ? gNew : gOld;
+            cd = static_cast<unsigned short>(g - g0);
             gatSrc[g++] = q;
         }
-        code[base + 32LL * k] = cd;
-        face[base + 32LL * k] = entFace[e];
+        code[ell + 32LL * k] = cd;
+        face[ell + 32LL * k] = entFace[e];
     }
 }
 
 __global__ void kChunkRecs(int nCh, const int* __restrict__ chunkStart, const long long* __restrict__ chunkEnt0,
                            const int* __restrict__ chunkDepth, const int* __restrict__ chunkNewDepth,
-                           const int* __restrict__ gatOff, const int* __restrict__ chunkNeedUp,
-                           const int* __restrict__ chunkSameWait, int* __restrict__ rec)
+                           const int* __restrict__ oldOff, const int* __restrict__ newOff,
+                           const int* __restrict__ chunkNeedUp,
+                           const int* __restrict__ chunkSameWait, const int2* __restrict__ chunkBlob,
+                           int* __restrict__ rec)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nCh) return;
@@ -645,14 +662,15 @@ __global__ void kChunkRecs(int nCh, const int* __restrict__ chunkStart, const lo
     r[1] = p1 - p0;
     r[2] = static_cast<int>(chunkEnt0[c]);
     r[3] = static_cast<int>(chunkEnt0[c + 1] - chunkEnt0[c]);
-    r[4] = gatOff[p0];
-    r[5] = gatOff[p1] - gatOff[p0];
+    const int nOld = oldOff[p1] - oldOff[p0];
+    r[4] = oldOff[p0] + newOff[p0];
+    r[5] = nOld + newOff[p1] - newOff[p0];
     r[6] = chunkDepth[c];
     r[7] = chunkNeedUp[c];
     r[8] = chunkSameWait[c];
-    r[9] = chunkNewDepth[c];
-    r[10] = 0;
-    r[11] = 0;
+    r[9] = chunkNewDepth[c] | (nOld << 1);
+    r[10] = chunkBlob[c].x;
+    r[11] = chunkBlob[c].y;
 }
 
 __global__ void kFillShort(unsigned short* v, long long n, unsigned short value)
@@ -1093,7 +1111,8 @@ void buildGsSchedule(LevelAddr& L, cudaStream_t s)
     auto fits = [&](int m, int e, int g) {
         int ah, bh;
         k::gsWindowExtents(m, ah, bh);
-        return k::gsSmemBytes<double>(m, e, g) <= smemCap && ah >= m && bh >= m;
+        return k::gsSmemBytes<double>(m, e, g) <= smemCap && ah >= m && bh >= m &&
+               k::kWin + k::kStages * g + 1 <= k::kMaxTable;
     };
     const int words = (P + 31) / 32;
     int M = std::min(k::kMaxCompute, std::max(32, ((maxGroup + 31) / 32) * 32));
@@ -1149,7 +1168,8 @@ void buildGsSchedule(LevelAddr& L, cudaStream_t s)
         int ahead, behind;
         k::gsWindowExtents(M, ahead, behind);
         // device classification
-        DBuf<int> chunkStart, chunkDepth, chunkNewDepth, chunkNeedUp, chunkSameWait, chunkOf, gatCnt, gatOff;
+        DBuf<int> chunkStart, chunkDepth, chunkNewDepth, chunkNeedUp, chunkSameWait, chunkOf;
+        DBuf<int> cntOld, cntNew, oldOff, newOff;
         DBuf<long long> chunkEnt0;
         chunkStart.upload(hChunkStart.data(), hChunkStart.size(), s);
         chunkDepth.upload(hChunkDepth.data(), hChunkDepth.size(), s);
@@ -1170,25 +1190,29 @@ void buildGsSchedule(LevelAddr& L, cudaStream_t s)
         ec.behind = behind;
         ec.chunkOf = chunkOf.p;
         ec.chunkStart = chunkStart.p;
-        gatCnt.alloc(n, s);
+        cntOld.alloc(n, s);
+        cntNew.alloc(n, s);
         kGatherCounts<<<grid(n), TPB, 0, s>>>(n, ec, G.posCell.p, G.posOf.p, G.depth.p, L.rowStart.p,
-                                              L.losortStart.p, L.col.p, gatCnt.p, chunkNeedUp.p,
+                                              L.losortStart.p, L.col.p, cntOld.p, cntNew.p, chunkNeedUp.p,
                                               chunkSameWait.p, upBits.p, words);
         B2G_LAUNCH_CHECK();
-        gatOff.alloc(n + 1, s);
-        const long long nGather = exclusiveScan(gatCnt.p, gatOff.p, n, s);
+        oldOff.alloc(n + 1, s);
+        newOff.alloc(n + 1, s);
+        const long long nGather = exclusiveScan(cntOld.p, oldOff.p, n, s) + exclusiveScan(cntNew.p, newOff.p, n, s);
         // the largest gather list of a chunk sizes the slots' gather arrays
-        const std::vector<int> hGatOff = gatOff.download(s);
+        const std::vector<int> hOldOff = oldOff.download(s);
+        const std::vector<int> hNewOff = newOff.download(s);
         int maxGat = 0;
         for (int c = 0; c < nCh; ++c)
-            maxGat = std::max(maxGat, hGatOff[hChunkStart[c + 1]] - hGatOff[hChunkStart[c]]);
-        maxGat = ((maxGat + 1 + 7) / 8) * 8;  // + the zero that padding entries read
-        if ((maxGat > k::kMaxGat || !fits(M, E, maxGat)) && M > 32 && attempt < 16)
+            maxGat = std::max(maxGat, hOldOff[hChunkStart[c + 1]] - hOldOff[hChunkStart[c]] +
+                                          hNewOff[hChunkStart[c + 1]] - hNewOff[hChunkStart[c]]);
+        maxGat = ((maxGat + 1) / 2) * 2;
+        if (!fits(M, E, maxGat) && M > 32 && attempt < 16)
         {
             M -= 32;  // fewer cells per chunk: fewer gathers per chunk, and more room per slot
             continue;
         }
-        if (maxGat > k::kMaxGat || !fits(M, E, maxGat))
+        if (!fits(M, E, maxGat))
             fail(B2G_ERR_ARGUMENT, "b2g: the Gauss-Seidel chunks gather more values than shared memory holds.");
         G.maxCells = M;
         G.maxEnt = E;
@@ -1203,21 +1227,38 @@ void buildGsSchedule(LevelAddr& L, cudaStream_t s)
         G.partChunkStart.upload(hPartChunk.data(), hPartChunk.size(), s);
         G.gsCode.alloc(std::max<long long>(ent, 1), s);
         G.gsEntFace.alloc(std::max<long long>(ent, 1), s);
-        G.gatSrc.alloc(std::max<long long>(nGather, 1), s);
+        G.gatSrc.alloc(std::max<long long>(nGather, 1) + 8, s);  // + the 16-byte cover of a bulk copy
         if (ent)
         {
+            // padding entries read the table's zero
             kFillShort<<<std::min<long long>(ceilDiv(ent, TPB), 8192), TPB, 0, s>>>(
-                G.gsCode.p, ent, static_cast<unsigned short>(k::kGatBit | static_cast<unsigned>(maxGat - 1)));
+                G.gsCode.p, ent, static_cast<unsigned short>(k::kWin + k::kStages * maxGat));
             kFillInt<<<static_cast<int>(std::min<long long>(ceilDiv(ent, TPB), 1LL << 30)), TPB, 0, s>>>(
                 G.gsEntFace.p, static_cast<int>(ent), -1);
         }
-        kSweepEntries<<<grid(n), TPB, 0, s>>>(n, ec, G.posCell.p, G.posOf.p, L.rowStart.p, L.losortStart.p, L.col.p,
-                                              L.entFace.p, G.posEnt.p, chunkEnt0.p, gatOff.p, G.gsCode.p,
-                                              G.gsEntFace.p, G.gatSrc.p);
+        kSweepEntries<<<grid(n), TPB, 0, s>>>(n, ec, maxGat, G.partChunkStart.p, G.posCell.p, G.posOf.p, L.rowStart.p,
+                                              L.losortStart.p, L.col.p, L.entFace.p, G.posEnt.p, chunkEnt0.p, oldOff.p,
+                                              newOff.p, G.gsCode.p, G.gsEntFace.p, G.gatSrc.p);
         B2G_LAUNCH_CHECK();
+        // each chunk's blob offset (16-byte units) in the FP64 and the FP32 blobs
+        std::vector<int2> hBlob(nCh);
+        long long b64 = 0, b32 = 0;
+        for (int c = 0; c < nCh; ++c)
+        {
+            const int m = hChunkStart[c + 1] - hChunkStart[c];
+            const int ne = static_cast<int>(hChunkEnt0[c + 1] - hChunkEnt0[c]);
+            hBlob[c] = make_int2(static_cast<int>(b64 / 16), static_cast<int>(b32 / 16));
+            b64 += k::blobLayout<double>(m, ne).bytes;
+            b32 += k::blobLayout<float>(m, ne).bytes;
+        }
+        if (b64 / 16 >= (1LL << 31)) fail(B2G_ERR_ARGUMENT, "b2g: the level's sweep data exceeds 32 GiB.");
+        G.blobBytes64 = b64;
+        G.blobBytes32 = b32;
+        DBuf<int2> chunkBlob;
+        chunkBlob.upload(hBlob.data(), hBlob.size(), s);
         G.chunkRec.alloc(12 * (size_t)nCh, s);
-        kChunkRecs<<<grid(nCh), TPB, 0, s>>>(nCh, chunkStart.p, chunkEnt0.p, chunkDepth.p, chunkNewDepth.p, gatOff.p,
-                                             chunkNeedUp.p, chunkSameWait.p, G.chunkRec.p);
+        kChunkRecs<<<grid(nCh), TPB, 0, s>>>(nCh, chunkStart.p, chunkEnt0.p, chunkDepth.p, chunkNewDepth.p, oldOff.p,
+                                             newOff.p, chunkNeedUp.p, chunkSameWait.p, chunkBlob.p, G.chunkRec.p);
         B2G_LAUNCH_CHECK();
         // upstream parts (whose progress a part waits on) and which parts have a downstream
         std::vector<unsigned> hUp = upBits.download(s);

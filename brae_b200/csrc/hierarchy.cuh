@@ -18,13 +18,15 @@ struct GsSchedule
     int nChunks = 0;
     int maxCells = 0;          // chunk cell capacity == the kernel's compute threads
     int maxEnt = 0;            // chunk ELL entry capacity
-    int maxGat = 0;            // chunk gather capacity, + 1 for the zero padding entries read
+    int maxGat = 0;            // chunk gather capacity (per stage in the sweep's value table)
     int ahead = 0;             // window extents the entry codes assume (gsWindowExtents)
     int behind = 0;
     int nPadded = 0;           // position count rounded up to the window fill block
     int nAlloc = 0;            // allocation length of every position-ordered vector of the level
     long long nEll = 0;        // ELL entries (whole 32-cell slices, padding included)
     long long nGather = 0;     // gathered values over all chunks
+    long long blobBytes64 = 0; // the chunks' blobs (gs_kernels.cuh) in FP64 and in FP32
+    long long blobBytes32 = 0;
     DBuf<int> depth;           // [nCells] by cell
     DBuf<int> partChunkStart;  // [nParts+1]
     DBuf<int> partPosStart;    // [nParts+1] (a part's positions are its cell range)
@@ -38,7 +40,7 @@ struct GsSchedule
     DBuf<int> entColPos;       // [2*nFaces] CSR: the other cell's position per entry
     DBuf<int> entFacePos;      // [2*nFaces] CSR: face of each entry
     DBuf<unsigned> posEnt;     // [nCells (+pad)] sweep row descriptor: slice width << 24 | chunk-relative base
-    DBuf<unsigned short> gsCode;  // [nEll] sweep entry codes (gs_kernels.cuh)
+    DBuf<unsigned short> gsCode;  // [nEll] sweep entry codes: value-table indices (gs_kernels.cuh)
     DBuf<int> gsEntFace;       // [nEll] face of each sweep entry, -1 for padding
     DBuf<int> gatSrc;          // [nGather] position of each gathered value
     DBuf<unsigned> progress;   // [nParts] per-part progress words (reset before each launch)

@@ -134,47 +134,54 @@ k::Rows<T> rowsOf(const LevelAddr& L, const LevelCoef<T>& C)
     return k::Rows<T>{L.nCells, L.gs.posRow.p, L.gs.entColPos.p, C.rowVal.p, C.gsDiag.p};
 }
 
-// the position-ordered coefficients of one level: diagonal, CSR rows, sweep (sliced ELL) entries
-__global__ void kGsLayout(int n, long long nnz, long long nEll, const int* __restrict__ posCell,
-                          const int* __restrict__ entFacePos, const int* __restrict__ gsEntFace,
+// the position-ordered coefficients of one level: diagonal and CSR rows
+__global__ void kGsLayout(int n, long long nnz, const int* __restrict__ posCell, const int* __restrict__ entFacePos,
                           const double* __restrict__ diag, const double* __restrict__ upper, double* __restrict__ gsDiag,
-                          double* __restrict__ rowVal, double* __restrict__ gsVal)
+                          double* __restrict__ rowVal)
 {
     const long long stride = (long long)gridDim.x * blockDim.x;
-    const long long m = max(static_cast<long long>(n), max(nnz, nEll));
+    const long long m = max(static_cast<long long>(n), nnz);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m; i += stride)
     {
         if (i < n) gsDiag[i] = diag[posCell[i]];
         if (i < nnz) rowVal[i] = upper[entFacePos[i]];
-        if (i < nEll)
-        {
-            const int f = gsEntFace[i];
-            gsVal[i] = f >= 0 ? upper[f] : 0.0;
-        }
     }
 }
 
-// (+8 elements of zeroed padding past the diagonal: the sweep's bulk copies round position ranges
-// out to 16 bytes)
+// (+8 elements of zeroed padding past the diagonal: bulk copies round position ranges out to 16 bytes)
 template <class T>
 void allocGsLayout(const LevelAddr& L, LevelCoef<T>& C, cudaStream_t s)
 {
     C.gsDiag.alloc(L.nCells + 8, s);
     C.gsDiag.zero(s);
     C.rowVal.alloc(std::max<size_t>(2 * (size_t)L.nFaces, 1), s);
-    C.gsVal.alloc(static_cast<size_t>(std::max<long long>(L.gs.nEll, 1)), s);
+    const long long bytes = sizeof(T) == 8 ? L.gs.blobBytes64 : L.gs.blobBytes32;
+    C.blob.alloc(static_cast<size_t>(std::max<long long>(bytes, 16)), s);
+    C.blob.zero(s);
+}
+
+// the sweep's chunk blobs in T, from the FP64 LDU coefficients
+template <class T>
+void fillBlobs(const LevelAddr& L, LevelCoef<T>& C, const double* upper, cudaStream_t s)
+{
+    const GsSchedule& G = L.gs;
+    if (G.nChunks)
+        k::buildChunkBlobs<T><<<std::min(G.nChunks, 65535), 128, 0, s>>>(
+            G.nChunks, reinterpret_cast<const int4*>(G.chunkRec.p), C.gsDiag.p, G.posEnt.p, G.gsCode.p,
+            G.gsEntFace.p, upper, C.blob.p);
+    B2G_LAUNCH_CHECK();
 }
 
 void fillGsLayout(const LevelAddr& L, LevelCoef<double>& C, cudaStream_t s)
 {
     allocGsLayout(L, C, s);
     const long long nnz = 2LL * L.nFaces;
-    const long long m = std::max<long long>(L.nCells, std::max(nnz, L.gs.nEll));
+    const long long m = std::max<long long>(L.nCells, nnz);
     if (m)
-        kGsLayout<<<std::min(ceilDiv(m, NT), 8192), NT, 0, s>>>(L.nCells, nnz, L.gs.nEll, L.gs.posCell.p,
-                                                                L.gs.entFacePos.p, L.gs.gsEntFace.p, C.diag.p,
-                                                                C.upper.p, C.gsDiag.p, C.rowVal.p, C.gsVal.p);
+        kGsLayout<<<std::min(ceilDiv(m, NT), 8192), NT, 0, s>>>(L.nCells, nnz, L.gs.posCell.p, L.gs.entFacePos.p,
+                                                                C.diag.p, C.upper.p, C.gsDiag.p, C.rowVal.p);
     B2G_LAUNCH_CHECK();
+    fillBlobs<double>(L, C, C.upper.p, s);
 }
 
 template <class T, class S>
@@ -360,7 +367,7 @@ void Matrix::ensureFp32()
         allocGsLayout(L, C, stream);
         castInto<float, double>(L.nCells, v64.coef[i].gsDiag.p, C.gsDiag.p, stream);
         castInto<float, double>(2LL * L.nFaces, v64.coef[i].rowVal.p, C.rowVal.p, stream);
-        castInto<float, double>(L.gs.nEll, v64.coef[i].gsVal.p, C.gsVal.p, stream);
+        fillBlobs<float>(L, C, v64.coef[i].upper.p, stream);
     }
     v32.corr.resize(nL);
     v32.src.resize(nL);
@@ -438,11 +445,8 @@ void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps,
     a.upStart = G.upStart.p;
     a.upList = G.upList.p;
     a.hasDown = G.hasDown.p;
-    a.posEnt = G.posEnt.p;
-    a.entCode = G.gsCode.p;
-    a.entVal = C.gsVal.p;
+    a.blob = C.blob.p;
     a.gatSrc = G.gatSrc.p;
-    a.posDiag = C.gsDiag.p;
     a.b = src;
     a.psi = psiL;
     a.progress = G.progress.p;
@@ -460,7 +464,7 @@ void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps,
     {
         B2G_CUDA(cudaMemsetAsync(G.progress.p, 0, sizeof(unsigned) * G.nParts, stream));
         cudaEvent_t e = level == 0 ? timedBegin(1) : nullptr;
-        k::gsSweep<T><<<G.nParts, G.maxCells + 64, smem, stream>>>(a);
+        k::gsSweep<T><<<G.nParts, G.maxCells + 96, smem, stream>>>(a);
         timedEnd(1, e);
         B2G_LAUNCH_CHECK();
         launches += 1;

@@ -24,7 +24,7 @@ struct LevelCoef
     DBuf<T> upper;  // [nFaces] LDU coefficient, upper == lower (FP64 only)
     DBuf<T> gsDiag; // [nCells (+pad)] diagonal by position
     DBuf<T> rowVal; // [2*nFaces] coefficient per CSR entry, rows by position
-    DBuf<T> gsVal;  // [ELL entries] coefficient per sweep entry (sliced ELL), 0 for padding
+    DBuf<unsigned char> blob;  // the sweep's chunk blobs (gs_kernels.cuh) in T
 };
 
 // Everything a V-cycle in value type T touches.

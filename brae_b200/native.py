@@ -94,6 +94,7 @@ def _load():
         "b2g_level_norm_factor": (ip, [vp, ip, vp, vp, vp, C.POINTER(C.c_double)]),
         "b2g_level_pcg_dic": (ip, [vp, ip, vp, vp, dp, dp, C.POINTER(_Perf)]),
         "b2g_level_pcg_dic_static": (ip, [vp, ip, vp, vp, dp, dp, C.POINTER(_Perf)]),
+        "b2g_level_schedule": (ip, [vp, ip, vp, vp]),
         "b2g_precondition": (ip, [vp, C.POINTER(Controls), vp, vp, C.POINTER(_Log)]),
         "b2g_matrix_pcg_solve": (ip, [vp, vp, vp, C.POINTER(Controls), ip, C.POINTER(_Perf),
                                       C.POINTER(_Log)]),
@@ -116,6 +117,7 @@ EXPORTED = [
     "b2g_level_amul", "b2g_level_smooth", "b2g_level_scale", "b2g_step_restrict",
     "b2g_step_prolong", "b2g_level_norm_factor", "b2g_level_pcg_dic", "b2g_precondition",
     "b2g_matrix_pcg_solve", "b2g_matrix_timings", "b2g_level_smooth_trace", "b2g_level_pcg_dic_static",
+    "b2g_level_schedule",
 ]
 
 
@@ -224,6 +226,13 @@ class Mesh:
         v = C.c_float()
         _check(lib.b2g_mesh_build_ms(self.handle, C.byref(v)))
         return v.value
+
+    def schedule(self, level: int, n_parts: int, n_chunks: int):
+        """The Gauss-Seidel schedule of a level (diagnostic): (partChunkStart, chunk records [n, 12])."""
+        pcs = np.empty(n_parts + 1, np.int32)
+        rec = np.empty((n_chunks, 12), np.int32)
+        _check(lib.b2g_level_schedule(self.handle, level, pcs.ctypes.data_as(C.c_void_p), rec.ctypes.data_as(C.c_void_p)))
+        return pcs, rec
 
     def step(self, i: int) -> dict:
         nc, nf = self.level_size(i)

@@ -274,13 +274,17 @@ B2G_API b2g_status b2g_matrix_timings(const b2g_matrix* m, double* ms4, long lon
 B2G_API b2g_status b2g_set_profiling(int on);
 
 /* Diagnostic: one Gauss-Seidel sweep of `level` (device pointers) recording into the device array
- * `trace` [6 * nChunks + 4 * nParts]: per schedule chunk four SM-cycle stamps of the first compute
+ * `trace` [8 * nChunks + 4 * nParts]: per schedule chunk four SM-cycle stamps of the first compute
  * thread (chunk start, staged data ready, row computed, slot released), then per part
- * {globaltimer ns, SM cycles} at its start and end, then per chunk two stamps of the staging warp
- * (start, copies issued). `schedule` (host, may be NULL) receives {nParts, nChunks, chunk cell
+ * {globaltimer ns, SM cycles} at its start and end, then per chunk four stamps of the staging warp
+ * (start, slot free, bulk copies issued, gathers issued). `schedule` (host, may be NULL) receives {nParts, nChunks, chunk cell
  * capacity, chunk entry capacity, max depth}. */
 B2G_API b2g_status b2g_level_smooth_trace(b2g_matrix* m, int level, double* psi, const double* source,
                                           unsigned long long* trace, int traceCapacity, int* schedule);
+/* Diagnostic: the Gauss-Seidel schedule of `level` to HOST arrays (either may be NULL):
+ * partChunkStart [nParts + 1] and the chunk records [12 * nChunks] (positions, sweep entries,
+ * gathers, depth, upstream depth, same-part wait, depth change, blob offsets). */
+B2G_API b2g_status b2g_level_schedule(const b2g_mesh* mesh, int level, int* partChunkStart, int* chunkRecords);
 
 /* Library version string. */
 B2G_API const char* b2g_version(void);
