@@ -333,6 +333,33 @@ def run_ours(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_sweep(args):
+    """The finest-level Gauss-Seidel sweep alone (a small, fixed case for ncu): `--sweep --n N` builds
+    the N^3 graded box and times three sweeps with CUDA events on the solve's stream."""
+    import torch
+
+    import brae_b200.native as b2g
+    from brae_b200 import cases
+    case = cases.graded_channel(args.n)
+    td = lambda a, dt=torch.float64: torch.as_tensor(np.ascontiguousarray(a)).to("cuda", dt)
+    mesh = b2g.Mesh(td(case.lower, torch.int32), td(case.upper, torch.int32), td(case.Sf.reshape(-1)),
+                    td(case.magSf), case.n_cells, 10, True)
+    A = b2g.Matrix(mesh, td(case.diag), td(case.coef))
+    x = torch.zeros(case.n_cells, dtype=torch.float64, device="cuda")
+    src = td(case.source)
+    A.smooth(0, x, src, 1)
+    b2g.set_profiling(True)
+    ctl = b2g.controls_default(tolerance=TOL, relTol=REL_TOL, maxIter=1)
+    A.solve(src, x, ctl, history_cap=0)
+    ms, cnt = A.timings()
+    b2g.set_profiling(False)
+    n, nf = case.n_cells, case.n_faces
+    gs_us = ms[1] / max(cnt[1], 1) * 1e3
+    print(json.dumps({"sweep": f"graded_channel_{args.n}^3 finest level", "cells": n, "faces": nf,
+                      "gs_us_per_launch": gs_us, "gs_launches": int(cnt[1]),
+                      "gs_algorithmic_gbs": (32 * n + 16 * nf) / (gs_us * 1e-6) / 1e9}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -341,7 +368,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=272)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--sweep", action="store_true",
+                    help="time the finest-level Gauss-Seidel sweep of the --n box alone (for profiling)")
     args = ap.parse_args()
+    if args.sweep:
+        run_sweep(args)
+        return
     world, rank, local = dist_setup()
     try:
         if args.impl == "reference":

@@ -35,7 +35,13 @@ inline void cudaCheck(cudaError_t e, const char* what, const char* file, int lin
 #define B2G_CUDA(x) ::b2g::cudaCheck((x), #x, __FILE__, __LINE__)
 #define B2G_LAUNCH_CHECK() ::b2g::cudaCheck(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
 
-// A device array. Allocation is stream-ordered (cudaMallocAsync from the device's default pool).
+// The library's own stream-ordered memory pool on the current device. It keeps the memory freed
+// into it (release threshold: never), so the work arrays of one solve are reused by the next
+// instead of being unmapped at every synchronisation and mapped again; the process's default pool
+// is left as it is.
+cudaMemPool_t libraryPool();
+
+// A device array. Allocation is stream-ordered (cudaMallocFromPoolAsync from libraryPool()).
 template <class T>
 struct DBuf
 {
@@ -66,7 +72,7 @@ struct DBuf
         n = count;
         if (count)
         {
-            B2G_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p), count * sizeof(T), stream));
+            B2G_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), count * sizeof(T), libraryPool(), stream));
         }
     }
     void zero(cudaStream_t stream)

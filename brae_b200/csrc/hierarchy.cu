@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 namespace b2g {
 
@@ -1302,6 +1303,27 @@ void buildStepMaps(Mesh& M, int i)
     S.prolongP.alloc(S.nFine, s);
     kProlongMap<<<grid(S.nFine), TPB, 0, s>>>(S.nFine, F.posCell.p, S.restrictAddr.p, C.posOf.p, S.prolongP.p);
     B2G_LAUNCH_CHECK();
+}
+
+cudaMemPool_t libraryPool()
+{
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    B2G_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) fail(B2G_ERR_STATE, "b2g: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!pools[dev])
+    {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        B2G_CUDA(cudaMemPoolCreate(&pools[dev], &props));
+        unsigned long long keep = ~0ULL;  // the attribute is a 64-bit unsigned integer
+        B2G_CUDA(cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep));
+    }
+    return pools[dev];
 }
 
 const DeviceInfo& DeviceInfo::get()
