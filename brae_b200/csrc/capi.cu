@@ -530,7 +530,8 @@ b2g_status b2g_level_smooth_trace(b2g_matrix* m, int level, double* psi, const d
             schedule[3] = G.maxEnt;
             schedule[4] = G.maxDepth;
         }
-        need(trace == nullptr || traceCapacity >= 8 * G.nChunks + 4 * G.nParts, "b2g_level_smooth_trace: trace too small");
+        need(trace == nullptr || traceCapacity >= 8LL * G.nChunks + 4LL * G.nParts + 2LL * G.nParts * (G.maxDepth + 2),
+             "b2g_level_smooth_trace: trace too small");
         b2g::Matrix& A = *m->mat;
         A.toPos(level, static_cast<const double*>(psi), A.ioBuf(0));
         A.toPos(level, source, A.ioBuf(1));

@@ -21,7 +21,8 @@
 //     chunk's blob (diagonal, row descriptors, coefficients, codes -- one contiguous TMA bulk copy)
 //     and b (a second one), the psi window's old values ahead of the front (TMA), and by cp.async
 //     the values the window does not hold; all of it completes on the slot's `full` mbarrier;
-//   * a SERVICE warp publishes the part's progress word and polls the upstream parts' words;
+//   * a PUBLISHER warp releases the part's progress word as the compute warps pass each depth, and
+//     a WATCHER warp polls the upstream parts' words;
 //   * the COMPUTE warps (one thread per cell) wait on `full`, compute their rows from shared
 //     memory only, and release the slot warp by warp on its `empty` mbarrier.
 //
@@ -60,10 +61,12 @@ namespace k {
 
 constexpr int kWin = 4096;                     // W: psi window (positions), a power of two
 constexpr int kFill = 256;                     // B: window fill block (positions)
-constexpr int kStages = 6;                     // S: pipeline slots
+constexpr int kStages = 4;                     // S: pipeline slots
 constexpr int kMaxTable = 65535;               // value-table entries a 16-bit code can name
-constexpr int kMaxCompute = 416;               // compute threads per CTA, at most (+ 3 warps)
+constexpr int kMaxCompute = 384;               // compute threads per CTA, at most (+ 4 warps)
 constexpr long long kSpinLimit = 1LL << 24;    // polls before a wait gives up
+constexpr int kProgressStride = 32;            // progress words 128 bytes apart: one L2 line per part,
+                                               // so that a part's publishes meet only its own pollers
 
 // Window extents the schedule relies on for a chunk starting at s and ending at e: positions
 // [s, s + ahead) hold old values, [e - behind, s) new ones. Fills for chunk j are issued once chunk
@@ -154,14 +157,17 @@ struct GsArgs
     const int* __restrict__ gatSrc;          // [gathers] position of each gathered value
     const T* __restrict__ b;                 // [n (+pad)] by position
     T* psi;                                  // [n] by position, updated in place (padded)
-    unsigned* progress;                      // [P]
+    unsigned* progress;                      // [P][kProgressStride] (word 0 of each line used)
     int* err;
-    unsigned long long* trace;               // diagnostic, or null: [nChunks][4] clock64 stamps of
-                                             // compute thread 0 (start, staged data ready,
-                                             // computed, released), [P][4] {globaltimer, clock64}
-                                             // at the part's start and end, [nChunks][4] producer
-                                             // stamps (start, slot free, copies issued, gathers
-                                             // issued)
+    unsigned long long* trace;               // diagnostic, or null (SM clock64 stamps): [nChunks][4]
+                                             // compute thread 0 (chunk start, past the depth
+                                             // barrier, data ready, computed); [P][4] {globaltimer,
+                                             // clock64} at the part's start and end; [nChunks][4]
+                                             // staging (TMA warp start, bulk copies issued, gather
+                                             // warp past its waits, gathers issued); [P][traceDepths]
+                                             // [2] per depth d: when the publisher released d and
+                                             // when the watcher first saw the upstream parts at d
+    int traceDepths;
 };
 
 __device__ __forceinline__ unsigned long long globalTimer()
@@ -315,7 +321,11 @@ __device__ __forceinline__ void computeSync(int nThreads)
     asm volatile("bar.sync 1, %0;" ::"r"(nThreads) : "memory");
 }
 
-// Bounded waits: on running out, set the error word; once it is set, give up at once.
+// Bounded waits: on running out, set the error word; once it is set, give up soon. The error word
+// is one L2 line that every waiting warp of every part would read, so it is read only every few
+// thousand polls: giving up a little later after another wait ran out costs nothing, a hot line
+// shared by all SMs slows every hand-off.
+constexpr long long kErrPollMask = 4095;
 __device__ __forceinline__ bool errSet(const int* err) { return *reinterpret_cast<const volatile int*>(err) != 0; }
 
 __device__ __forceinline__ void waitMbar(unsigned long long* b, unsigned parity, int* err)
@@ -323,7 +333,7 @@ __device__ __forceinline__ void waitMbar(unsigned long long* b, unsigned parity,
     long long it = 0;
     while (!mbarTryWait(b, parity))
     {
-        if ((++it & 255) == 0 && errSet(err)) return;
+        if ((++it & kErrPollMask) == 0 && errSet(err)) return;
         if (it > kSpinLimit)
         {
             atomicExch(err, 1);
@@ -338,7 +348,7 @@ __device__ __forceinline__ void waitShared(const unsigned* w, unsigned target, i
     long long it = 0;
     while (ldAcquireCta(w) < target)
     {
-        if ((++it & 63) == 0 && errSet(err)) return;
+        if ((++it & kErrPollMask) == 0 && errSet(err)) return;
         if (it > kSpinLimit)
         {
             atomicExch(err, 1);
@@ -368,10 +378,10 @@ __device__ __forceinline__ T rowTerms(T acc, unsigned cA, unsigned vA, unsigned 
     return acc;
 }
 
-// One Gauss-Seidel sweep of one level, in position order. Grid = P parts; blockDim = M + 96:
-// M compute threads, then the TMA warp, the gather warp and the service warp.
+// One Gauss-Seidel sweep of one level, in position order. Grid = P parts; blockDim = M + 128:
+// M compute threads, then the TMA warp, the gather warp, the publisher warp and the watcher warp.
 template <class T>
-__global__ void __launch_bounds__(kMaxCompute + 96, 1) gsSweep(GsArgs<T> a)
+__global__ void __launch_bounds__(kMaxCompute + 128, 1) gsSweep(GsArgs<T> a)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) unsigned long long full[kStages];
@@ -379,7 +389,7 @@ __global__ void __launch_bounds__(kMaxCompute + 96, 1) gsSweep(GsArgs<T> a)
     __shared__ __align__(8) unsigned long long lists[kStages];  // a stage's record and gather sources
     __shared__ __align__(16) int4 srec[kStages][3];              // the staged chunk's record
     __shared__ unsigned pubDepth;     // every cell of this part below this depth is done (compute ->
-                                      // service warp; 0x7fffffff at the end)
+                                      // publisher warp; 0x7fffffff at the end)
     __shared__ unsigned upMin;        // least progress seen among the upstream parts
     constexpr unsigned kT = sizeof(T);
     const int M = a.maxCells;
@@ -394,6 +404,11 @@ __global__ void __launch_bounds__(kMaxCompute + 96, 1) gsSweep(GsArgs<T> a)
     const int c0 = a.partChunkStart[p];
     const int nCh = a.partChunkStart[p + 1] - c0;
     const int nComputeWarps = M >> 5;
+    // per-depth hand-off stamps of this part (diagnostic)
+    unsigned long long* depthTrace =
+        a.trace ? a.trace + 8 * (size_t)a.partChunkStart[a.nParts] + 4 * (size_t)a.nParts +
+                      2 * (size_t)a.traceDepths * p
+                : nullptr;
     if (t == 0)
     {
         stsT(tableA + kT * static_cast<unsigned>(kWin + kStages * G), T(0));  // what padding entries read
@@ -410,38 +425,39 @@ __global__ void __launch_bounds__(kMaxCompute + 96, 1) gsSweep(GsArgs<T> a)
     }
     __syncthreads();
 
-    if (t >= M + 64)
+    if (t >= M + 96)
     {
-        // ---------------- service warp: progress out, upstream progress in ----------------
-        // Everything it polls is in shared memory or in registers, but the upstream parts' progress
-        // words: one L2 round trip per poll.
-        const int lane = t - M - 64;
+        // ---------------- watcher warp: upstream progress in ----------------
+        // Polls the upstream parts' progress words back to back (relaxed loads: one L2 round trip
+        // each) and publishes their least value in shared memory, with an acquire fence first, so
+        // that the gathers issued on it read what the upstream parts released.
+        const int lane = t - M - 96;
         const int upBeg = a.upStart[p];
         const int nUp = a.upStart[p + 1] - upBeg;
+        if (nUp == 0) return;
         const int myUp = lane < nUp ? a.upList[upBeg + lane] : -1;  // parts beyond 32: read per poll
-        const bool publish = a.hasDown[p] != 0;
-        unsigned published = 0xffffffffu;
+        unsigned seen = 0u;
         long long it = 0;
         while (true)
         {
-            // one value for the whole warp: lanes must agree before the shuffles below
-            const unsigned v = __shfl_sync(0xffffffffu, ldAcquireCta(&pubDepth), 0);
-            if (publish && v != published)
+            unsigned m = myUp >= 0 ? ldRelaxedGpu(&a.progress[kProgressStride * myUp]) : 0xffffffffu;
+            for (int i = upBeg + 32 + lane; i < upBeg + nUp; i += 32) m = min(m, ldRelaxedGpu(&a.progress[kProgressStride * a.upList[i]]));
+            for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
+            if (m > seen)
             {
-                // release at GPU scope: cumulative over the psi stores the compute warps made before
-                // their barrier and their release of pubDepth, which this warp acquired
-                if (lane == 0) stRelease(&a.progress[p], v);
-                published = v;
+                fenceAcqRelGpu();
+                if (lane == 0) stReleaseCta(&upMin, m);
+                if (depthTrace && lane == 0)
+                {
+                    const unsigned long long now = clockStamp();
+                    for (unsigned d = seen + 1; d <= m && d < static_cast<unsigned>(a.traceDepths); ++d)
+                        depthTrace[2 * d + 1] = now;
+                }
+                seen = m;
             }
-            if (v == 0x7fffffffu) break;
-            if (nUp > 0)
-            {
-                unsigned m = myUp >= 0 ? ldAcquire(&a.progress[myUp]) : 0xffffffffu;
-                for (int i = upBeg + 32 + lane; i < upBeg + nUp; i += 32) m = min(m, ldAcquire(&a.progress[a.upList[i]]));
-                for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
-                if (lane == 0 && m > ldAcquireCta(&upMin)) stReleaseCta(&upMin, m);
-            }
-            if ((++it & 63) == 0)
+            // done when every upstream part is, or when this part is (it needs no more values)
+            if (seen == 0x7fffffffu || __shfl_sync(0xffffffffu, ldAcquireCta(&pubDepth), 0) == 0x7fffffffu) break;
+            if ((++it & kErrPollMask) == 0)
             {
                 if (__shfl_sync(0xffffffffu, errSet(a.err) ? 1 : 0, 0)) break;
                 if (it > 16 * kSpinLimit)
@@ -450,7 +466,38 @@ __global__ void __launch_bounds__(kMaxCompute + 96, 1) gsSweep(GsArgs<T> a)
                     break;
                 }
             }
-            __nanosleep(20);
+        }
+        return;
+    }
+
+    if (t >= M + 64)
+    {
+        // ---------------- publisher warp: this part's progress out ----------------
+        // One lane spins on the shared pubDepth and releases each new value at GPU scope at once:
+        // the release is cumulative over the psi stores the compute warps made before their barrier
+        // and their release of pubDepth, which this lane acquired.
+        if (t != M + 64 || a.hasDown[p] == 0) return;
+        unsigned published = 0xffffffffu;
+        long long it = 0;
+        while (true)
+        {
+            const unsigned v = ldAcquireCta(&pubDepth);
+            if (v != published)
+            {
+                stRelease(&a.progress[kProgressStride * p], v);
+                if (depthTrace && v < static_cast<unsigned>(a.traceDepths)) depthTrace[2 * v] = clockStamp();
+                published = v;
+            }
+            if (v == 0x7fffffffu) break;
+            if ((++it & kErrPollMask) == 0)
+            {
+                if (errSet(a.err)) break;
+                if (it > 256 * kSpinLimit)
+                {
+                    atomicExch(a.err, 1);
+                    break;
+                }
+            }
         }
         return;
     }
@@ -479,7 +526,6 @@ __global__ void __launch_bounds__(kMaxCompute + 96, 1) gsSweep(GsArgs<T> a)
                 if (j + 2 < nCh) r2 = loadChunkRec(a.chunkRec, c0 + j + 2);
                 if (ptr) ptr[4 * (size_t)(c0 + j)] = clockStamp();
                 if (j >= kStages) waitMbar(&empty[s], static_cast<unsigned>((j / kStages - 1) & 1), a.err);
-                if (ptr) ptr[4 * (size_t)(c0 + j) + 1] = clockStamp();
                 const unsigned slotA = slotsA + static_cast<unsigned>(s) * sb;
                 // the record and the gather sources first: the gather warp starts from them
                 const int4* rg = a.chunkRec + 3 * (size_t)(c0 + j);
@@ -499,7 +545,7 @@ __global__ void __launch_bounds__(kMaxCompute + 96, 1) gsSweep(GsArgs<T> a)
                 for (int f = 0; f < nFill; ++f, filled += kFill)
                     tmaLoad(tableA + kT * static_cast<unsigned>(filled & (kWin - 1)), a.psi + filled, kFill * kT,
                             &full[s]);
-                if (ptr) ptr[4 * (size_t)(c0 + j) + 2] = clockStamp();
+                if (ptr) ptr[4 * (size_t)(c0 + j) + 1] = clockStamp();
                 if (++s == kStages) s = 0;
             }
             return;
@@ -531,6 +577,7 @@ __global__ void __launch_bounds__(kMaxCompute + 96, 1) gsSweep(GsArgs<T> a)
                 const int sw = sameWait - c0;
                 if (sameWait >= 0 && sw > j - kStages)
                     waitMbar(&empty[sw % kStages], static_cast<unsigned>((sw / kStages) & 1), a.err);
+                if (ptr) ptr[4 * (size_t)(c0 + j) + 2] = clockStamp();
             }
             __syncwarp();
             for (int g = nOld + lane; g < nGat; g += 32)
@@ -570,8 +617,9 @@ __global__ void __launch_bounds__(kMaxCompute + 96, 1) gsSweep(GsArgs<T> a)
             computeSync(M);
             if (t == 0) stReleaseCta(&pubDepth, static_cast<unsigned>(cr.depth));
         }
-        waitMbar(&full[s], phase, a.err);
         if (a.trace && t == 0) a.trace[4 * (size_t)(c0 + j) + 1] = clockStamp();
+        waitMbar(&full[s], phase, a.err);
+        if (a.trace && t == 0) a.trace[4 * (size_t)(c0 + j) + 2] = clockStamp();
         if (t < cr.m)
         {
             const unsigned slotA = slotsA + static_cast<unsigned>(s) * sb;
@@ -606,10 +654,9 @@ __global__ void __launch_bounds__(kMaxCompute + 96, 1) gsSweep(GsArgs<T> a)
             fenceProxyAsyncShared();
             a.psi[pos] = res;
         }
-        if (a.trace && t == 0) a.trace[4 * (size_t)(c0 + j) + 2] = clockStamp();
+        if (a.trace && t == 0) a.trace[4 * (size_t)(c0 + j) + 3] = clockStamp();
         __syncwarp();
         if (lane == 0) mbarArrive(&empty[s]);
-        if (a.trace && t == 0) a.trace[4 * (size_t)(c0 + j) + 3] = clockStamp();
         if (++s == kStages)
         {
             s = 0;

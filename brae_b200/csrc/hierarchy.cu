@@ -1281,7 +1281,7 @@ void buildGsSchedule(LevelAddr& L, cudaStream_t s)
         break;
     }
     G.partPosStart = std::move(dPartStart);
-    G.progress.alloc(P, s);
+    G.progress.alloc(static_cast<size_t>(P) * k::kProgressStride, s);
     G.progress.zero(s);
     B2G_CUDA(cudaStreamSynchronize(s));
 }

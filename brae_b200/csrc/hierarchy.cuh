@@ -43,7 +43,8 @@ struct GsSchedule
     DBuf<unsigned short> gsCode;  // [nEll] sweep entry codes: value-table indices (gs_kernels.cuh)
     DBuf<int> gsEntFace;       // [nEll] face of each sweep entry, -1 for padding
     DBuf<int> gatSrc;          // [nGather] position of each gathered value
-    DBuf<unsigned> progress;   // [nParts] per-part progress words (reset before each launch)
+    DBuf<unsigned> progress;   // [nParts][kProgressStride] per-part progress words, one L2 line each
+                               // (reset before each launch)
 };
 
 // One level's addressing and its derived layouts (built once per hierarchy).

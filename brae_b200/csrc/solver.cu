@@ -452,6 +452,7 @@ void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps,
     a.progress = G.progress.p;
     a.err = err.p;
     a.trace = trace;
+    a.traceDepths = G.maxDepth + 2;
     const size_t smem = k::gsSmemBytes<T>(G.maxCells, G.maxEnt, G.maxGat);
     static bool attrSet[2] = {false, false};
     bool& set = attrSet[sizeof(T) == 8 ? 0 : 1];
@@ -462,9 +463,9 @@ void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps,
     }
     for (int sw = 0; sw < nSweeps; ++sw)
     {
-        B2G_CUDA(cudaMemsetAsync(G.progress.p, 0, sizeof(unsigned) * G.nParts, stream));
+        B2G_CUDA(cudaMemsetAsync(G.progress.p, 0, G.progress.bytes(), stream));
         cudaEvent_t e = level == 0 ? timedBegin(1) : nullptr;
-        k::gsSweep<T><<<G.nParts, G.maxCells + 96, smem, stream>>>(a);
+        k::gsSweep<T><<<G.nParts, G.maxCells + 128, smem, stream>>>(a);
         timedEnd(1, e);
         B2G_LAUNCH_CHECK();
         launches += 1;

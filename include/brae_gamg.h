@@ -274,11 +274,13 @@ B2G_API b2g_status b2g_matrix_timings(const b2g_matrix* m, double* ms4, long lon
 B2G_API b2g_status b2g_set_profiling(int on);
 
 /* Diagnostic: one Gauss-Seidel sweep of `level` (device pointers) recording into the device array
- * `trace` [8 * nChunks + 4 * nParts]: per schedule chunk four SM-cycle stamps of the first compute
- * thread (chunk start, staged data ready, row computed, slot released), then per part
- * {globaltimer ns, SM cycles} at its start and end, then per chunk four stamps of the staging warp
- * (start, slot free, bulk copies issued, gathers issued). `schedule` (host, may be NULL) receives {nParts, nChunks, chunk cell
- * capacity, chunk entry capacity, max depth}. */
+ * `trace` [8 * nChunks + 4 * nParts + 2 * nParts * (maxDepth + 2)] (SM-cycle stamps): per schedule
+ * chunk four of the first compute thread (chunk start, past the depth barrier, data ready, row
+ * computed); per part {globaltimer ns, SM cycles} at its start and end; per chunk four of the
+ * staging warps (bulk copies started, issued, gathers past their waits, gathers issued); per part
+ * and depth d two (d published to the downstream parts, upstream parts first seen at d).
+ * `schedule` (host, may be NULL) receives {nParts, nChunks, chunk cell capacity, chunk entry
+ * capacity, max depth}. */
 B2G_API b2g_status b2g_level_smooth_trace(b2g_matrix* m, int level, double* psi, const double* source,
                                           unsigned long long* trace, int traceCapacity, int* schedule);
 /* Diagnostic: the Gauss-Seidel schedule of `level` to HOST arrays (either may be NULL):
