@@ -13,6 +13,10 @@ preconditioned form; their times, final residuals and field error are reported b
 solve through the C ABI with host (pinned) buffers, copies in the timed region. N > 1 runs N
 independent replicas, one per GPU (the solve does not shard). `--impl reference` times the
 reference's own CPU implementation (oracle/_ref, else the oracle port) on the same workload.
+
+The "served" object is the serving form (b2g_server): Poisson arrivals at --serve-rate per second
+(500) for --serve-seconds (4; the full stream is 60 s) over a resident population of graded boxes
+(70 % 16k-128k cells, 25 % 0.5M-2M, 5 % 8M), both forms, with p50/p99 latency and solves/s.
 """
 from __future__ import annotations
 
@@ -210,7 +214,12 @@ def run_ours(args, world, rank, local):
     for _ in range(args.warmup):
         psi.zero_()
         A.solve(src, psi, ctl, history_cap=0)
+    # finest-level Amul and Gauss-Seidel launches are bracketed by CUDA events (event-record nodes
+    # inside each iteration's graph), read after every iteration: live per-kernel times of the
+    # timed solves themselves
     b2g.set_profiling(True)
+    psi.zero_()
+    A.solve(src, psi, ctl, history_cap=0)  # captures the profiled graphs (untimed)
     ms_acc = np.zeros(4)
     cnt_acc = np.zeros(4)
     stream = torch.cuda.current_stream()
@@ -296,6 +305,10 @@ def run_ours(args, world, rank, local):
                "iterations": cperf[2], "final_residual": cperf[1],
                "field_rel_diff_vs_gpu": float(np.abs(cpsi - psi64).max() / np.abs(cpsi).max())}
 
+    served = None
+    if not args.no_serve and world == 1:
+        served = serve_stream(args, b2g, local)
+
     line = {
         "metric": METRIC, "value": per_solve, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": per_solve * 1e3, "higher_is_better": False,
@@ -328,9 +341,98 @@ def run_ours(args, world, rank, local):
         "gpu_launches": int(cnt_acc[3]),
         "clocks": clocks.summary(),
         "cpu_baseline": cpu,
+        "served": served,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def serve_stream(args, b2g, local):
+    """The served stream: Poisson arrivals of pressure solves (seed 2) over a resident population of
+    graded boxes in three size classes (70 % 16k-128k cells, 25 % 0.5M-2M, 5 % 8M), HBM cap 150 GB,
+    run once in plain FP64 and once in the FP32-preconditioned form. Latency is arrival to result
+    (the server's clock); solves/s counts the whole stream, arrival of the first to the last result."""
+    import queue as _queue
+
+    from brae_b200 import cases
+    t0 = time.perf_counter()
+    srv = b2g.Server(150 << 30, slots=args.serve_slots)
+    pop = cases.served_population()
+    resident = []  # per class: [(case id, n cells, source)]
+    for k, sizes in enumerate(pop):
+        row = []
+        for j, n in enumerate(sizes):
+            c = cases.served_box(n, seed=100 * k + j)
+            row.append((srv.add_case(c.lower, c.upper, c.Sf, c.magSf, c.n_cells, c.diag, c.coef), c.n_cells,
+                        np.ascontiguousarray(c.source)))
+            del c
+        resident.append(row)
+    # two solution buffers per case, touched now, recycled by the stream (zeroed after each result)
+    free = {cid: [np.full(n, 0.0) for _ in range(2)] for row in resident for cid, n, _ in row}
+    setup_s = time.perf_counter() - t0
+    probs = np.cumsum([p for p, _, _ in cases.SERVED_CLASSES])
+    out = {"population": {"cases_per_class": [len(r) for r in resident],
+                          "cells": [[n for _, n, _ in r] for r in resident], "setup_s": setup_s,
+                          "slots": args.serve_slots, "hbm_cap_gb": 150},
+           "offered_rate_per_s": args.serve_rate, "stream_s": args.serve_seconds}
+    for form, prec in (("fp64", 0), ("fp32_precond", 1)):
+        ctl = b2g.controls_default(tolerance=TOL, relTol=REL_TOL, maxIter=MAX_ITER, precision=prec)
+        # warm every case once in this form (captures its iteration graph)
+        for row in resident:
+            for cid, n, src in row:
+                buf = free[cid][0]
+                srv.wait(srv.submit(cid, src, ctl, out=buf))
+                buf[:] = 0.0
+        rng = np.random.default_rng(2)
+        gaps = rng.exponential(1.0 / args.serve_rate, size=int(args.serve_rate * args.serve_seconds * 1.5) + 16)
+        arrivals = np.cumsum(gaps)
+        arrivals = arrivals[arrivals < args.serve_seconds]
+        cls = np.searchsorted(probs, rng.random(arrivals.size), side="right").clip(0, 2)
+        pick = rng.random(arrivals.size)
+        lock = threading.Lock()
+        done = _queue.Queue()
+        lat, iters = [], []
+        outstanding = [0, 0]      # now, max
+        def collect():
+            while True:
+                item = done.get()
+                if item is None:
+                    return
+                t, cid = item
+                psi, perf, ms = srv.wait(t)
+                psi[:] = 0.0
+                with lock:
+                    lat.append(ms)
+                    iters.append(perf.nIterations)
+                    free.setdefault(cid, []).append(psi)
+                    outstanding[0] -= 1
+        th = threading.Thread(target=collect)
+        th.start()
+        start = time.perf_counter()
+        for a, k, u in zip(arrivals, cls, pick):
+            row = resident[k]
+            cid, n, src = row[min(int(u * len(row)), len(row) - 1)]
+            delay = start + a - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            with lock:
+                bufs = free.get(cid)
+                buf = bufs.pop() if bufs else None
+                outstanding[0] += 1
+                outstanding[1] = max(outstanding[1], outstanding[0])
+            if buf is None:
+                buf = np.zeros(n)
+            done.put((srv.submit(cid, src, ctl, out=buf), cid))
+        done.put(None)
+        th.join()
+        wall = time.perf_counter() - start
+        lat_a = np.asarray(lat)
+        out[form] = {"requests": int(arrivals.size), "p50_ms": float(np.percentile(lat_a, 50)),
+                     "p99_ms": float(np.percentile(lat_a, 99)), "mean_ms": float(lat_a.mean()),
+                     "solves_per_s": arrivals.size / wall, "drain_s": wall - args.serve_seconds,
+                     "max_outstanding": outstanding[1], "mean_iterations": float(np.mean(iters))}
+    srv.close()
+    return out
 
 
 def run_sweep(args):
@@ -368,11 +470,24 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=272)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-stream leg")
+    ap.add_argument("--serve-seconds", type=float, default=4.0,
+                    help="length of the served stream's arrival window (the full stream is 60 s)")
+    ap.add_argument("--serve-rate", type=float, default=500.0, help="offered requests per second")
+    ap.add_argument("--serve-slots", type=int, default=16, help="server worker slots")
+    ap.add_argument("--serve", action="store_true", help="run the served stream alone")
     ap.add_argument("--sweep", action="store_true",
                     help="time the finest-level Gauss-Seidel sweep of the --n box alone (for profiling)")
     args = ap.parse_args()
     if args.sweep:
         run_sweep(args)
+        return
+    if args.serve:
+        import torch
+
+        import brae_b200.native as b2g
+        torch.cuda.set_device(0)
+        print(json.dumps({"served": serve_stream(args, b2g, 0)}), flush=True)
         return
     world, rank, local = dist_setup()
     try:

@@ -194,3 +194,27 @@ def mixed_batch_sizes(n_cases: int = 256, lo: int = 4096, hi: int = 1048576, see
         nz = max(2, int(round(base * ay)))
         out.append(dict(n=(nx, ny, nz), lengths=(ax, 1.0, ay), grading=grading))
     return out
+
+
+def served_box(target_cells: float, seed: int = 0) -> BoxCase:
+    """A served-stream case: the graded channel's construction (2 x 1 x 1 m, 20:1 toward the y
+    walls, outlet at x = 2) on a 2m x m x m grid with 2 m^3 nearest ``target_cells``."""
+    m = max(4, int(round((target_cells / 2.0) ** (1.0 / 3.0))))
+    return box_case(2 * m, m, m, (2.0, 1.0, 1.0), 20.0, False, seed, name=f"served_{2 * m}x{m}x{m}")
+
+
+# size classes of the served stream: (probability, low cells, high cells), log-uniform within a class
+SERVED_CLASSES = ((0.70, 16e3, 128e3), (0.25, 0.5e6, 2e6), (0.05, 8e6, 8e6))
+
+
+def served_population(per_class=(32, 4, 1), seed: int = 2):
+    """Target cell counts of the resident cases the served stream draws from, per size class."""
+    u = splitmix64_uniform(seed, sum(per_class))
+    out, k = [], 0
+    for (p, lo, hi), cnt in zip(SERVED_CLASSES, per_class):
+        sizes = []
+        for _ in range(cnt):
+            sizes.append(math.exp(math.log(lo) + u[k] * (math.log(hi) - math.log(lo))))
+            k += 1
+        out.append(sizes)
+    return out

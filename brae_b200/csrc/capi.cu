@@ -2,7 +2,7 @@
 // string, host/device argument staging, and the fvSolution entry reader with the reference's
 // refusals (readGamgControls, src/matrices/lduMatrix/solvers/GAMG/gamg_solver_cpp.cu:801-928, and
 // the PCG keys of src/applications/solvers/interFoam/inter_case_cpp.cu:1519-1572).
-#include "solver.cuh"
+#include "capi_internal.cuh"
 
 #include <cctype>
 #include <cstring>
@@ -11,52 +11,25 @@
 #include <mutex>
 #include <string>
 
-struct b2g_mesh
-{
-    b2g::Mesh m;
-};
+namespace b2g {
+namespace capi {
 
-struct b2g_matrix
-{
-    b2g_mesh* mesh = nullptr;
-    std::unique_ptr<b2g::Matrix> mat;
-};
-
-namespace {
-
-thread_local std::string g_lastError;
-
-cudaStream_t streamOf(void* s) { return s ? static_cast<cudaStream_t>(s) : cudaStreamPerThread; }
-
-template <class F>
-b2g_status guarded(F&& f)
-{
-    try
-    {
-        f();
-        return B2G_OK;
-    }
-    catch (const b2g::Error& e)
-    {
-        g_lastError = e.what();
-        return e.code;
-    }
-    catch (const std::bad_alloc&)
-    {
-        g_lastError = "b2g: host allocation failed";
-        return B2G_ERR_NO_MEMORY;
-    }
-    catch (const std::exception& e)
-    {
-        g_lastError = e.what();
-        return B2G_ERR_STATE;
-    }
-}
+thread_local std::string lastError;
 
 void need(bool ok, const char* msg)
 {
     if (!ok) b2g::fail(B2G_ERR_ARGUMENT, msg);
 }
+
+}  // namespace capi
+}  // namespace b2g
+
+namespace {
+
+using b2g::capi::guarded;
+using b2g::capi::need;
+
+cudaStream_t streamOf(void* s) { return s ? static_cast<cudaStream_t>(s) : cudaStreamPerThread; }
 
 template <class T>
 void stage(b2g::DBuf<T>& d, const T* src, size_t n, int memspace, cudaStream_t s)
@@ -249,9 +222,82 @@ void readGamg(const Dict& d, b2g_controls& c, const std::string& who)
 
 }  // namespace
 
+namespace b2g {
+namespace capi {
+
+std::unique_ptr<b2g_mesh> createMesh(int nCells, int nFaces, const int32_t* lower, const int32_t* upper,
+                                     const double* Sf, const double* magSf, int nCellsInCoarsestLevel,
+                                     int* forwardInOut, int memspace, cudaStream_t stream)
+{
+    need(nCells > 0 && nFaces >= 0, "b2g_mesh_create: nCells must be positive and nFaces non-negative");
+    need(nFaces == 0 || (lower && upper && Sf && magSf), "b2g_mesh_create: null array");
+    need(forwardInOut != nullptr, "b2g_mesh_create: null direction flag");
+    need(memspace == B2G_MEM_HOST || memspace == B2G_MEM_DEVICE, "b2g_mesh_create: bad memspace");
+    std::unique_ptr<b2g_mesh> h(new b2g_mesh);
+    b2g::Mesh& M = h->m;
+    M.stream = stream;
+    cudaGetDevice(&M.device);
+    cudaEvent_t e0, e1;
+    B2G_CUDA(cudaEventCreate(&e0));
+    B2G_CUDA(cudaEventCreate(&e1));
+    B2G_CUDA(cudaEventRecord(e0, M.stream));
+    M.lev.emplace_back();
+    b2g::LevelAddr& L0 = M.lev[0];
+    L0.nCells = nCells;
+    L0.nFaces = nFaces;
+    stage(L0.lower, lower, nFaces, memspace, M.stream);
+    stage(L0.upper, upper, nFaces, memspace, M.stream);
+    b2g::DBuf<double> dSf, dMag;
+    stage(dSf, Sf, 3 * (size_t)nFaces, memspace, M.stream);
+    stage(dMag, magSf, nFaces, memspace, M.stream);
+    b2g::buildHierarchy(M, dSf.p, dMag.p, nCellsInCoarsestLevel, forwardInOut);
+    B2G_CUDA(cudaEventRecord(e1, M.stream));
+    B2G_CUDA(cudaEventSynchronize(e1));
+    B2G_CUDA(cudaEventElapsedTime(&M.buildMs, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return h;
+}
+
+void solveOn(b2g::Matrix& A, const double* source, double* psi, const b2g_controls* c, int memspace,
+             b2g_perf* out, b2g_solve_log* log, bool standalone)
+{
+    need(c && source && psi && out, "b2g solve: null argument");
+    need(memspace == B2G_MEM_HOST || memspace == B2G_MEM_DEVICE, "b2g solve: bad memspace");
+    const int n0 = A.n(0);
+    // the solve runs in the finest level's position order: host fields are staged in fc/fr (free
+    // outside a solve) and permuted on the device; device fields are permuted in place of a copy
+    if (memspace == B2G_MEM_HOST)
+    {
+        B2G_CUDA(cudaMemcpyAsync(A.fc.p, source, sizeof(double) * n0, cudaMemcpyHostToDevice, A.stream));
+        B2G_CUDA(cudaMemcpyAsync(A.fr.p, psi, sizeof(double) * n0, cudaMemcpyHostToDevice, A.stream));
+        A.toPos(0, static_cast<const double*>(A.fc.p), A.source.p);
+        A.toPos(0, static_cast<const double*>(A.fr.p), A.psi.p);
+    }
+    else
+    {
+        A.toPos(0, source, A.source.p);
+        A.toPos(0, static_cast<const double*>(psi), A.psi.p);
+    }
+    *out = standalone ? A.gamg(*c, log) : A.pcg(*c, log);
+    if (memspace == B2G_MEM_HOST)
+    {
+        A.fromPos(0, static_cast<const double*>(A.psi.p), A.fc.p);
+        B2G_CUDA(cudaMemcpyAsync(psi, A.fc.p, sizeof(double) * n0, cudaMemcpyDeviceToHost, A.stream));
+    }
+    else
+    {
+        A.fromPos(0, static_cast<const double*>(A.psi.p), psi);
+    }
+    B2G_CUDA(cudaStreamSynchronize(A.stream));
+}
+
+}  // namespace capi
+}  // namespace b2g
+
 extern "C" {
 
-const char* b2g_last_error(void) { return g_lastError.c_str(); }
+const char* b2g_last_error(void) { return b2g::capi::lastError.c_str(); }
 
 const char* b2g_version(void) { return "brae_b200 0.1 (sm_100a)"; }
 
@@ -351,34 +397,9 @@ b2g_status b2g_mesh_create(int nCells, int nFaces, const int32_t* lower, const i
     return guarded([&] {
         need(out != nullptr, "b2g_mesh_create: null output handle");
         *out = nullptr;
-        need(nCells > 0 && nFaces >= 0, "b2g_mesh_create: nCells must be positive and nFaces non-negative");
-        need(nFaces == 0 || (lower && upper && Sf && magSf), "b2g_mesh_create: null array");
-        need(forwardInOut != nullptr, "b2g_mesh_create: null direction flag");
-        need(memspace == B2G_MEM_HOST || memspace == B2G_MEM_DEVICE, "b2g_mesh_create: bad memspace");
-        std::unique_ptr<b2g_mesh> h(new b2g_mesh);
-        b2g::Mesh& M = h->m;
-        M.stream = streamOf(stream);
-        cudaGetDevice(&M.device);
-        cudaEvent_t e0, e1;
-        B2G_CUDA(cudaEventCreate(&e0));
-        B2G_CUDA(cudaEventCreate(&e1));
-        B2G_CUDA(cudaEventRecord(e0, M.stream));
-        M.lev.emplace_back();
-        b2g::LevelAddr& L0 = M.lev[0];
-        L0.nCells = nCells;
-        L0.nFaces = nFaces;
-        stage(L0.lower, lower, nFaces, memspace, M.stream);
-        stage(L0.upper, upper, nFaces, memspace, M.stream);
-        b2g::DBuf<double> dSf, dMag;
-        stage(dSf, Sf, 3 * (size_t)nFaces, memspace, M.stream);
-        stage(dMag, magSf, nFaces, memspace, M.stream);
-        b2g::buildHierarchy(M, dSf.p, dMag.p, nCellsInCoarsestLevel, forwardInOut);
-        B2G_CUDA(cudaEventRecord(e1, M.stream));
-        B2G_CUDA(cudaEventSynchronize(e1));
-        B2G_CUDA(cudaEventElapsedTime(&M.buildMs, e0, e1));
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        *out = h.release();
+        *out = b2g::capi::createMesh(nCells, nFaces, lower, upper, Sf, magSf, nCellsInCoarsestLevel, forwardInOut,
+                                     memspace, streamOf(stream))
+                   .release();
     });
 }
 
@@ -654,45 +675,12 @@ b2g_status b2g_precondition(b2g_matrix* m, const b2g_controls* controls, double*
     });
 }
 
-static void solveOn(b2g::Matrix& A, const double* source, double* psi, const b2g_controls* c, int memspace,
-                    b2g_perf* out, b2g_solve_log* log, bool standalone)
-{
-    need(c && source && psi && out, "b2g solve: null argument");
-    need(memspace == B2G_MEM_HOST || memspace == B2G_MEM_DEVICE, "b2g solve: bad memspace");
-    const int n0 = A.n(0);
-    // the solve runs in the finest level's position order: host fields are staged in fc/fr (free
-    // outside a solve) and permuted on the device; device fields are permuted in place of a copy
-    if (memspace == B2G_MEM_HOST)
-    {
-        B2G_CUDA(cudaMemcpyAsync(A.fc.p, source, sizeof(double) * n0, cudaMemcpyHostToDevice, A.stream));
-        B2G_CUDA(cudaMemcpyAsync(A.fr.p, psi, sizeof(double) * n0, cudaMemcpyHostToDevice, A.stream));
-        A.toPos(0, static_cast<const double*>(A.fc.p), A.source.p);
-        A.toPos(0, static_cast<const double*>(A.fr.p), A.psi.p);
-    }
-    else
-    {
-        A.toPos(0, source, A.source.p);
-        A.toPos(0, static_cast<const double*>(psi), A.psi.p);
-    }
-    *out = standalone ? A.gamg(*c, log) : A.pcg(*c, log);
-    if (memspace == B2G_MEM_HOST)
-    {
-        A.fromPos(0, static_cast<const double*>(A.psi.p), A.fc.p);
-        B2G_CUDA(cudaMemcpyAsync(psi, A.fc.p, sizeof(double) * n0, cudaMemcpyDeviceToHost, A.stream));
-    }
-    else
-    {
-        A.fromPos(0, static_cast<const double*>(A.psi.p), psi);
-    }
-    B2G_CUDA(cudaStreamSynchronize(A.stream));
-}
-
 b2g_status b2g_matrix_pcg_solve(b2g_matrix* m, const double* source, double* psi, const b2g_controls* controls,
                                 int memspace, b2g_perf* out, b2g_solve_log* log)
 {
     return guarded([&] {
         need(m != nullptr, "b2g_matrix_pcg_solve: null matrix");
-        solveOn(*m->mat, source, psi, controls, memspace, out, log, false);
+        b2g::capi::solveOn(*m->mat, source, psi, controls, memspace, out, log, false);
     });
 }
 
@@ -705,7 +693,7 @@ b2g_status b2g_pcg_gamg_solve(b2g_mesh* mesh, const double* diag, const double* 
         (void)stream;
         b2g::Matrix A(&mesh->m, mesh->m.stream);
         A.setFine(diag, upper, memspace);
-        solveOn(A, source, psi, controls, memspace, out, log, false);
+        b2g::capi::solveOn(A, source, psi, controls, memspace, out, log, false);
     });
 }
 
@@ -718,7 +706,7 @@ b2g_status b2g_gamg_solve(b2g_mesh* mesh, const double* diag, const double* uppe
         (void)stream;
         b2g::Matrix A(&mesh->m, mesh->m.stream);
         A.setFine(diag, upper, memspace);
-        solveOn(A, source, psi, controls, memspace, out, log, true);
+        b2g::capi::solveOn(A, source, psi, controls, memspace, out, log, true);
     });
 }
 

@@ -5,7 +5,9 @@
 #include "solver.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <cstring>
 
 namespace b2g {
 
@@ -200,6 +202,19 @@ void zeroArray(long long n, T* x, cudaStream_t s)
 
 }  // namespace
 
+// The sweep's shared-memory ceiling, raised once per device and value type before the first launch
+// (outside any stream capture: the matrix constructor calls it).
+template <class T>
+void allowSweepSmem(int device)
+{
+    static std::atomic<unsigned long long> done[2]{};
+    const unsigned long long bit = 1ull << (device & 63);
+    std::atomic<unsigned long long>& d = done[sizeof(T) == 8 ? 0 : 1];
+    if (d.load() & bit) return;
+    B2G_CUDA(cudaFuncSetAttribute(k::gsSweep<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024));
+    d.fetch_or(bit);
+}
+
 cudaEvent_t Matrix::timedBegin(int cls)
 {
     if (!g_profiling) return nullptr;
@@ -214,16 +229,51 @@ cudaEvent_t Matrix::timedBegin(int cls)
         B2G_CUDA(cudaEventCreate(&e.first));
         B2G_CUDA(cudaEventCreate(&e.second));
     }
-    B2G_CUDA(cudaEventRecord(e.first, stream));
-    (cls == 0 ? evAmul : evGs).push_back(e);
+    if (capturing)
+    {
+        // an event-record node in the graph, re-recorded by every replay
+        B2G_CUDA(cudaEventRecordWithFlags(e.first, stream, cudaEventRecordExternal));
+        capturing->ev[cls].push_back(e);
+    }
+    else
+    {
+        B2G_CUDA(cudaEventRecord(e.first, stream));
+        (cls == 0 ? evAmul : evGs).push_back(e);
+    }
     return e.first;
 }
 
 void Matrix::timedEnd(int cls, cudaEvent_t start)
 {
     if (!start) return;
-    auto& v = cls == 0 ? evAmul : evGs;
-    B2G_CUDA(cudaEventRecord(v.back().second, stream));
+    if (capturing)
+        B2G_CUDA(cudaEventRecordWithFlags(capturing->ev[cls].back().second, stream, cudaEventRecordExternal));
+    else
+        B2G_CUDA(cudaEventRecord((cls == 0 ? evAmul : evGs).back().second, stream));
+}
+
+void Matrix::collectGraphTimings(IterationGraph& G)
+{
+    if (!g_profiling) return;
+    for (int cls = 0; cls < 2; ++cls)
+        for (auto& e : G.ev[cls])
+        {
+            float x = 0.f;
+            B2G_CUDA(cudaEventElapsedTime(&x, e.first, e.second));
+            graphMs[cls] += x;
+            graphCounts[cls] += 1;
+        }
+}
+
+void Matrix::releaseGraph(IterationGraph& G)
+{
+    if (G.exec) cudaGraphExecDestroy(G.exec);
+    G.exec = nullptr;
+    for (auto& v : G.ev)
+    {
+        for (auto& e : v) evFree.push_back(e);
+        v.clear();
+    }
 }
 
 void Matrix::timingsBegin()
@@ -234,6 +284,8 @@ void Matrix::timingsBegin()
         counts[i] = 0;
     }
     launches = 0;
+    graphMs[0] = graphMs[1] = 0.0;
+    graphCounts[0] = graphCounts[1] = 0;
     if (!g_profiling) return;
     if (!evSolve[0])
     {
@@ -262,7 +314,8 @@ void Matrix::timingsEnd()
             ms[cls] += x;
             evFree.push_back(e);
         }
-        counts[cls] = static_cast<long long>(v.size());
+        counts[cls] = static_cast<long long>(v.size()) + graphCounts[cls];
+        ms[cls] += graphMs[cls];
         v.clear();
     }
     ms[2] = ms[3] - ms[0] - ms[1];
@@ -271,6 +324,7 @@ void Matrix::timingsEnd()
 
 Matrix::~Matrix()
 {
+    for (IterationGraph* g : {&pcgGraph, &gamgGraph}) releaseGraph(*g);
     for (auto* v : {&evAmul, &evGs, &evFree})
         for (auto& e : *v)
         {
@@ -301,6 +355,10 @@ Matrix::Matrix(Mesh* m, cudaStream_t s) : mesh(m), stream(s)
     coarseCount.alloc(1, s);
     coarseCount.zero(s);
     v64.coef.resize(m->lev.size());
+    int dev = 0;
+    B2G_CUDA(cudaGetDevice(&dev));
+    allowSweepSmem<double>(dev);
+    allowSweepSmem<float>(dev);
 }
 
 void Matrix::setFine(const double* diag, const double* upper, int memspace)
@@ -454,13 +512,6 @@ void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps,
     a.trace = trace;
     a.traceDepths = G.maxDepth + 2;
     const size_t smem = k::gsSmemBytes<T>(G.maxCells, G.maxEnt, G.maxGat);
-    static bool attrSet[2] = {false, false};
-    bool& set = attrSet[sizeof(T) == 8 ? 0 : 1];
-    if (!set)
-    {
-        B2G_CUDA(cudaFuncSetAttribute(k::gsSweep<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024));
-        set = true;
-    }
     for (int sw = 0; sw < nSweeps; ++sw)
     {
         B2G_CUDA(cudaMemsetAsync(G.progress.p, 0, G.progress.bytes(), stream));
@@ -588,7 +639,7 @@ void Matrix::coarsestSolve<float>(int level, float* x, const float* src, float t
     castInto<float, double>(n, x64, x, stream);
 }
 
-double Matrix::normFactor(int level, const double* x, const double* src, const double* Apsi)
+double Matrix::normFactor(int level, const double* x, const double* src, const double* Apsi, bool readBack)
 {
     const LevelAddr& L = mesh->lev[level];
     if (serial)
@@ -609,6 +660,7 @@ double Matrix::normFactor(int level, const double* x, const double* src, const d
     }
     B2G_LAUNCH_CHECK();
     double nf = 0;
+    if (!readBack) return nf;
     B2G_CUDA(cudaMemcpyAsync(&nf, &scal.p->nf, sizeof(double), cudaMemcpyDeviceToHost, stream));
     B2G_CUDA(cudaStreamSynchronize(stream));
     return nf;
@@ -770,6 +822,52 @@ void Matrix::checkDeviceError()
     }
 }
 
+template <class F>
+void Matrix::runIteration(IterationGraph& G, const b2g_controls& c, F&& body)
+{
+    std::vector<unsigned char> key(sizeof(b2g_controls) + sizeof(void*) + 3 * sizeof(int));
+    unsigned char* k = key.data();
+    std::memcpy(k, &c, sizeof(b2g_controls));
+    k += sizeof(b2g_controls);
+    const void* logp = coarseLog.p;
+    std::memcpy(k, &logp, sizeof(void*));
+    k += sizeof(void*);
+    const int flags[3] = {coarseLogCapacity, serial ? 1 : 0, g_profiling ? 1 : 0};
+    std::memcpy(k, flags, sizeof(flags));
+    if (!G.exec || G.key != key)
+    {
+        releaseGraph(G);
+        const long long l0 = launches;
+        B2G_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        capturing = &G;
+        try
+        {
+            body();
+        }
+        catch (...)
+        {
+            capturing = nullptr;
+            cudaGraph_t dropped = nullptr;
+            cudaStreamEndCapture(stream, &dropped);
+            if (dropped) cudaGraphDestroy(dropped);
+            throw;
+        }
+        capturing = nullptr;
+        cudaGraph_t graph = nullptr;
+        B2G_CUDA(cudaStreamEndCapture(stream, &graph));
+        const cudaError_t e = cudaGraphInstantiate(&G.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        B2G_CUDA(e);
+        G.launchesPerReplay = launches - l0;
+        G.key = std::move(key);
+    }
+    else
+    {
+        launches += G.launchesPerReplay;
+    }
+    B2G_CUDA(cudaGraphLaunch(G.exec, stream));
+}
+
 // PCG::scalarSolve with the GAMG preconditioner (pcgGamgSolveImpl, GAMG:1031-1143)
 b2g_perf Matrix::pcg(const b2g_controls& c, b2g_solve_log* log)
 {
@@ -780,7 +878,7 @@ b2g_perf Matrix::pcg(const b2g_controls& c, b2g_solve_log* log)
     amul<double>(0, psi.p, wA.p);
     k::subtract<double><<<rowsGrid(n0), NT, 0, stream>>>(n0, source.p, wA.p, rA.p);
     B2G_LAUNCH_CHECK();
-    normFactor(0, psi.p, source.p, wA.p);
+    normFactor(0, psi.p, source.p, wA.p, false);
     const int g = redGrid(n0);
     reduceInto(k::RED_SUMMAG, n0, rA.p, nullptr, &scal.p->sumMag);
     kInitResidual<<<1, 1, 0, stream>>>(scal.p);
@@ -809,22 +907,25 @@ b2g_perf Matrix::pcg(const b2g_controls& c, b2g_solve_log* log)
     B2G_LAUNCH_CHECK();
     do
     {
-        precondition(c, wA.p, rA.p);
-        reduceInto(k::RED_DOT, n0, wA.p, rA.p, &scal.p->wArA);
-        if (flexible) reduceInto(k::RED_DOT, n0, wA.p, rOld.p, &scal.p->wrOld);
-        kPUpdate<<<rowsGrid(n0), NT, 0, stream>>>(n0, wA.p, pA.p, scal.p, flexible ? 1 : 0);
-        B2G_LAUNCH_CHECK();
-        amul<double>(0, pA.p, wA.p);
-        reduceInto(k::RED_DOT, n0, wA.p, pA.p, &scal.p->wApA);
-        kAlphaUpdate<NT><<<g, NT, 0, stream>>>(n0, psi.p, pA.p, rA.p, wA.p, flexible ? rOld.p : nullptr, scal.p,
-                                              v64.partial.p);
-        if (serial) reduceInto(k::RED_SUMMAG, n0, rA.p, nullptr, &scal.p->sumMag);
-        else k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->sumMag);
-        kIterFinish<<<1, 1, 0, stream>>>(scal.p);
-        B2G_LAUNCH_CHECK();
-        launches += 9;
+        runIteration(pcgGraph, c, [&] {
+            precondition(c, wA.p, rA.p);
+            reduceInto(k::RED_DOT, n0, wA.p, rA.p, &scal.p->wArA);
+            if (flexible) reduceInto(k::RED_DOT, n0, wA.p, rOld.p, &scal.p->wrOld);
+            kPUpdate<<<rowsGrid(n0), NT, 0, stream>>>(n0, wA.p, pA.p, scal.p, flexible ? 1 : 0);
+            B2G_LAUNCH_CHECK();
+            amul<double>(0, pA.p, wA.p);
+            reduceInto(k::RED_DOT, n0, wA.p, pA.p, &scal.p->wApA);
+            kAlphaUpdate<NT><<<g, NT, 0, stream>>>(n0, psi.p, pA.p, rA.p, wA.p, flexible ? rOld.p : nullptr,
+                                                  scal.p, v64.partial.p);
+            if (serial) reduceInto(k::RED_SUMMAG, n0, rA.p, nullptr, &scal.p->sumMag);
+            else k::reduceFinal<double, NT><<<1, NT, 0, stream>>>(v64.partial.p, g, &scal.p->sumMag);
+            kIterFinish<<<1, 1, 0, stream>>>(scal.p);
+            B2G_LAUNCH_CHECK();
+            launches += 9;
+        });
         B2G_CUDA(cudaMemcpyAsync(&hs, scal.p, sizeof(hs), cudaMemcpyDeviceToHost, stream));
         B2G_CUDA(cudaStreamSynchronize(stream));
+        collectGraphTimings(pcgGraph);
         if (hs.singular) break;
         perf.finalResidual = hs.finalRes;
         if (log && log->history && perf.nIterations < log->historyCapacity)
@@ -856,7 +957,7 @@ b2g_perf Matrix::gamg(const b2g_controls& c, b2g_solve_log* log)
     cc.precTolerance = c.tolerance;
     cc.precRelTol = c.relTol;
     amul<double>(0, psi.p, AwA.p);
-    normFactor(0, psi.p, source.p, AwA.p);
+    normFactor(0, psi.p, source.p, AwA.p, false);
     k::subtract<double><<<rowsGrid(n0), NT, 0, stream>>>(n0, source.p, AwA.p, fr.p);
     reduceInto(k::RED_SUMMAG, n0, fr.p, nullptr, &scal.p->sumMag);
     kInitResidual<<<1, 1, 0, stream>>>(scal.p);
@@ -869,17 +970,25 @@ b2g_perf Matrix::gamg(const b2g_controls& c, b2g_solve_log* log)
     perf.finalResidual = hs.initRes;
     perf.nIterations = 0;
     if (log) log->historyCount = 0;
-    if (c.minIter <= 0 && convergedH(perf.finalResidual, perf.initialResidual, c.tolerance, c.relTol)) return perf;
+    if (c.minIter <= 0 && convergedH(perf.finalResidual, perf.initialResidual, c.tolerance, c.relTol))
+    {
+        timingsEnd();
+        return perf;
+    }
     do
     {
-        vcycle<double>(cc, psi.p, source.p, AwA.p, fc.p, fr.p);
-        amul<double>(0, psi.p, AwA.p);
-        k::subtract<double><<<rowsGrid(n0), NT, 0, stream>>>(n0, source.p, AwA.p, fr.p);
-        reduceInto(k::RED_SUMMAG, n0, fr.p, nullptr, &scal.p->sumMag);
-        kResidualFinish<<<1, 1, 0, stream>>>(scal.p);
-        B2G_LAUNCH_CHECK();
+        runIteration(gamgGraph, cc, [&] {
+            vcycle<double>(cc, psi.p, source.p, AwA.p, fc.p, fr.p);
+            amul<double>(0, psi.p, AwA.p);
+            k::subtract<double><<<rowsGrid(n0), NT, 0, stream>>>(n0, source.p, AwA.p, fr.p);
+            reduceInto(k::RED_SUMMAG, n0, fr.p, nullptr, &scal.p->sumMag);
+            kResidualFinish<<<1, 1, 0, stream>>>(scal.p);
+            B2G_LAUNCH_CHECK();
+            launches += 2;
+        });
         B2G_CUDA(cudaMemcpyAsync(&hs, scal.p, sizeof(hs), cudaMemcpyDeviceToHost, stream));
         B2G_CUDA(cudaStreamSynchronize(stream));
+        collectGraphTimings(gamgGraph);
         perf.finalResidual = hs.finalRes;
         if (log && log->history && perf.nIterations < log->historyCapacity)
             log->history[perf.nIterations] = hs.finalRes;
@@ -888,6 +997,7 @@ b2g_perf Matrix::gamg(const b2g_controls& c, b2g_solve_log* log)
     } while ((perf.nIterations < c.maxIter &&
               !convergedH(perf.finalResidual, perf.initialResidual, c.tolerance, c.relTol)) ||
              perf.nIterations < c.minIter);
+    timingsEnd();
     checkDeviceError();
     readLog(log);
     return perf;

@@ -42,6 +42,19 @@ struct VCycleData
     bool built = false;
 };
 
+// One PCG (or GAMG) iteration captured as a CUDA graph, replayed while the launches it captured stay
+// valid: the key holds what they depend on beyond the matrix's fixed buffers (the controls, the
+// coarsest-level log, the reduction order).
+struct IterationGraph
+{
+    cudaGraphExec_t exec = nullptr;
+    std::vector<unsigned char> key;
+    long long launchesPerReplay = 0;
+    // profiling: event pairs captured as event-record nodes around the finest level's Amul (0) and
+    // Gauss-Seidel (1) launches; re-recorded by every replay, read after it
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[2];
+};
+
 struct Matrix
 {
     Mesh* mesh = nullptr;
@@ -58,13 +71,17 @@ struct Matrix
     DBuf<int> coarseCount;
     DBuf<int> err;
     int coarseLogCapacity = 0;
+    IterationGraph pcgGraph, gamgGraph;
     bool serial = false;                      // B2G_REDUCTION_SERIAL for the current solve
     // timing (b2g_set_profiling): events around the finest level's Amul and Gauss-Seidel launches
     double ms[4] = {0, 0, 0, 0};              // finest Amul, finest Gauss-Seidel, other, whole solve
     long long counts[4] = {0, 0, 0, 0};       // launches of the same classes (whole solve: all)
     long long launches = 0;
+    double graphMs[2] = {0, 0};               // finest Amul / Gauss-Seidel time inside graph replays
+    long long graphCounts[2] = {0, 0};
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evAmul, evGs, evFree;
     cudaEvent_t evSolve[2] = {nullptr, nullptr};
+    IterationGraph* capturing = nullptr;      // the graph being captured, if any
     cudaEvent_t timedBegin(int cls);          // records a start event if profiling (cls 0 Amul, 1 GS)
     void timedEnd(int cls, cudaEvent_t start);
     void timingsBegin();
@@ -95,7 +112,9 @@ struct Matrix
     template <class T> void vcycle(const b2g_controls& c, T* psi, const T* source, T* Apsi, T* fc,
                                    const T* fr);
     void precondition(const b2g_controls& c, double* w, const double* r);
-    double normFactor(int level, const double* psi, const double* source, const double* Apsi);
+    // the normalisation factor into scal->nf; read back and returned when `readBack` (else 0)
+    double normFactor(int level, const double* psi, const double* source, const double* Apsi,
+                      bool readBack = true);
     // sum / dot / sum of magnitudes of n values into a device slot, tree or serial per `serial`
     void reduceInto(int op, int n, const double* a, const double* b, double* slot);
 
@@ -106,6 +125,10 @@ struct Matrix
     void resetLog(int capacity);
     void readLog(b2g_solve_log* log);
     void checkDeviceError();
+    // runs `body` (the launches of one iteration) through G: captured on first use, replayed after
+    template <class F> void runIteration(IterationGraph& G, const b2g_controls& c, F&& body);
+    void collectGraphTimings(IterationGraph& G);  // after a replay has finished
+    void releaseGraph(IterationGraph& G);
     template <class T> VCycleData<T>& data();
 };
 

@@ -100,6 +100,12 @@ def _load():
                                       C.POINTER(_Log)]),
         "b2g_matrix_timings": (ip, [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
         "b2g_level_smooth_trace": (ip, [vp, ip, vp, vp, vp, ip, C.POINTER(C.c_int)]),
+        "b2g_server_create": (ip, [C.c_ulonglong, ip, C.POINTER(vp)]),
+        "b2g_server_destroy": (ip, [vp]),
+        "b2g_server_add_case": (ip, [vp, ip, ip, vp, vp, vp, vp, vp, vp, ip, ip, C.POINTER(C.c_int)]),
+        "b2g_server_submit": (ip, [vp, ip, vp, vp, C.POINTER(Controls), C.POINTER(C.c_longlong)]),
+        "b2g_server_wait": (ip, [vp, C.c_longlong, C.POINTER(_Perf), C.POINTER(C.c_double), ip]),
+        "b2g_server_case_bytes": (ip, [vp, ip, C.POINTER(C.c_ulonglong)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -117,7 +123,8 @@ EXPORTED = [
     "b2g_level_amul", "b2g_level_smooth", "b2g_level_scale", "b2g_step_restrict",
     "b2g_step_prolong", "b2g_level_norm_factor", "b2g_level_pcg_dic", "b2g_precondition",
     "b2g_matrix_pcg_solve", "b2g_matrix_timings", "b2g_level_smooth_trace", "b2g_level_pcg_dic_static",
-    "b2g_level_schedule",
+    "b2g_level_schedule", "b2g_server_create", "b2g_server_destroy", "b2g_server_add_case",
+    "b2g_server_submit", "b2g_server_wait", "b2g_server_case_bytes",
 ]
 
 
@@ -136,6 +143,8 @@ def controls_default(**overrides) -> Controls:
             v = {"fp64": 0, "fp32_precond": 1}[v]
         if k == "reduction" and isinstance(v, str):
             v = {"tree": 0, "serial": 1}[v]
+        if k == "solver" and isinstance(v, str):
+            v = {"PCG": 0, "GAMG": 1}[v]
         setattr(c, k, v)
     return c
 
@@ -206,7 +215,7 @@ class Mesh:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h is not None and h.value:
+        if h is not None and h.value and lib is not None:
             lib.b2g_mesh_destroy(h)
             self.handle = None
 
@@ -279,7 +288,7 @@ class Matrix:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h is not None and h.value:
+        if h is not None and h.value and lib is not None:
             lib.b2g_matrix_destroy(h)
             self.handle = None
 
@@ -388,3 +397,74 @@ def gamg_solve(mesh: Mesh, diag, upper, source, psi, controls: Controls,
     _check(lib.b2g_gamg_solve(mesh.handle, _ptr(diag), _ptr(upper), _ptr(source), _ptr(psi),
                               C.byref(controls), ms, _stream(), C.byref(p), C.byref(lb.log)))
     return SolverPerformance(p.initialResidual, p.finalResidual, p.nIterations), lb.history()
+
+
+class Server:
+    """The serving form (b2g_server_*): cases registered once and kept resident, solves queued as
+    they arrive and run on `slots` worker streams side by side. Host arrays in and out."""
+
+    def __init__(self, hbm_cap_bytes: int, slots: int = 4):
+        h = C.c_void_p()
+        _check(lib.b2g_server_create(int(hbm_cap_bytes), int(slots), C.byref(h)))
+        self.handle = h
+        self.n_cells = {}
+        self._pending = {}
+
+    def add_case(self, lower, upper, Sf, magSf, n_cells, diag, coef, n_coarsest=10) -> int:
+        lower = np.ascontiguousarray(lower, np.int32)
+        upper = np.ascontiguousarray(upper, np.int32)
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (np.asarray(Sf).reshape(-1), magSf, diag, coef)]
+        cid = C.c_int()
+        _check(lib.b2g_server_add_case(self.handle, int(n_cells), int(lower.shape[0]), _ptr(lower), _ptr(upper),
+                                       _ptr(arrs[0]), _ptr(arrs[1]), _ptr(arrs[2]), _ptr(arrs[3]),
+                                       int(n_coarsest), B2G_MEM_HOST, C.byref(cid)))
+        self.n_cells[cid.value] = int(n_cells)
+        return cid.value
+
+    def submit(self, case_id: int, source, controls: Controls, psi0=None, out=None) -> int:
+        """Queues a solve. The server reads `source` and solves into `out` (a float64 array of the
+        case's size; a new one if None) in place, starting from psi0 (zero if None). Both arrays
+        are held here until wait() hands the solution back."""
+        n = self.n_cells[case_id]
+        src = np.ascontiguousarray(source, np.float64)
+        if out is None:
+            out = np.zeros(n, np.float64)
+        if psi0 is not None:
+            out[:] = psi0
+        if out.dtype != np.float64 or not out.flags.c_contiguous or out.shape != (n,) or src.shape != (n,):
+            raise ValueError("submit: source and out must be float64 arrays of the case's size")
+        t = C.c_longlong()
+        _check(lib.b2g_server_submit(self.handle, int(case_id), _ptr(src), _ptr(out), C.byref(controls),
+                                     C.byref(t)))
+        self._pending[t.value] = (src, out)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        """(psi, SolverPerformance, latency ms) of a submitted solve."""
+        perf = _Perf()
+        lat = C.c_double()
+        rc = lib.b2g_server_wait(self.handle, int(ticket), C.byref(perf), C.byref(lat), int(timeout_ms))
+        if rc != 0:
+            msg = lib.b2g_last_error().decode()
+            if "still pending" not in msg:  # a pending request keeps its buffers held
+                self._pending.pop(ticket, None)
+            raise GamgError(rc, msg)
+        _, psi = self._pending.pop(ticket)
+        return psi, SolverPerformance(perf.initialResidual, perf.finalResidual, perf.nIterations), lat.value
+
+    def case_bytes(self, case_id: int) -> int:
+        v = C.c_ulonglong()
+        _check(lib.b2g_server_case_bytes(self.handle, int(case_id), C.byref(v)))
+        return v.value
+
+    def close(self):
+        if self.handle is not None and lib is not None:
+            _check(lib.b2g_server_destroy(self.handle))
+        self.handle = None
+        self._pending.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -288,6 +288,39 @@ B2G_API b2g_status b2g_level_smooth_trace(b2g_matrix* m, int level, double* psi,
  * gathers, depth, upstream depth, same-part wait, depth change, blob offsets). */
 B2G_API b2g_status b2g_level_schedule(const b2g_mesh* mesh, int level, int* partChunkStart, int* chunkRecords);
 
+/* ---- the serving form: many independent cases, solves queued as they arrive ------------------ */
+
+/* A request loop on the current device (no counterpart in the reference's solver interface; it
+ * serves the same solve, b2g_matrix_pcg_solve, to many cases at once). nSlots worker threads, each
+ * with its own stream, take queued requests oldest first, so a request that arrives while others
+ * are on the GPU starts as soon as a slot frees up, and their work overlaps on the device. A case
+ * is solved by one slot at a time. Each PCG iteration of a case runs as one CUDA graph launch. */
+typedef struct b2g_server b2g_server;
+B2G_API b2g_status b2g_server_create(unsigned long long hbmCapBytes, int nSlots, b2g_server** out);
+/* Stops the workers (queued requests are dropped) and frees every case. */
+B2G_API b2g_status b2g_server_destroy(b2g_server* server);
+/* Registers a case: builds its hierarchy and its matrix (FP64 and FP32 levels) and keeps both
+ * resident, admitted by their HBM footprint: idle cases without queued requests are evicted, least
+ * recently used first, until the case fits under the cap; else B2G_ERR_NO_MEMORY. Arguments as
+ * b2g_mesh_create and b2g_matrix_create (folded diagonal, upper == lower coefficients). */
+B2G_API b2g_status b2g_server_add_case(b2g_server* server, int nCells, int nFaces, const int32_t* lower,
+                                       const int32_t* upper, const double* Sf, const double* magSf,
+                                       const double* diag, const double* upperCoef, int nCellsInCoarsestLevel,
+                                       int memspace, int* caseId);
+/* Queues one solve of case `caseId`. `source` (HOST, [nCells]) is read and `psi` (HOST, [nCells])
+ * holds the initial guess on entry and the solution once b2g_server_wait has returned for the ticket.
+ * Both are the caller's buffers, used in place: they must stay valid, and psi untouched, until then.
+ * controls->solver picks PCG + GAMG or GAMG. */
+B2G_API b2g_status b2g_server_submit(b2g_server* server, int caseId, const double* source, double* psi,
+                                     const b2g_controls* controls, long long* ticket);
+/* Waits for a request (timeoutMs < 0: as long as it takes): `out` receives the SolverPerformance,
+ * latencyMs the time from submit to result. Returns the solve's own status; B2G_ERR_STATE with
+ * "still pending" if the request has not finished at the timeout (its buffers stay in use). */
+B2G_API b2g_status b2g_server_wait(b2g_server* server, long long ticket, b2g_perf* out, double* latencyMs,
+                                   int timeoutMs);
+/* The HBM footprint a case was admitted with (bytes). */
+B2G_API b2g_status b2g_server_case_bytes(b2g_server* server, int caseId, unsigned long long* bytes);
+
 /* Library version string. */
 B2G_API const char* b2g_version(void);
 
