@@ -95,7 +95,7 @@ __device__ __forceinline__ bool convergedT(T fin, T init, T tol, T relTol)
 
 // One warp (blockDim.x == 32).
 template <class T>
-__global__ void __launch_bounds__(32) coarsestPcgDic(CoarsestArgs<T> a)
+__device__ __forceinline__ void coarsestPcgDicWarp(const CoarsestArgs<T>& a)
 {
     __shared__ T shScal[4];  // nf, init, final, flag
     __shared__ int shIter;
@@ -216,6 +216,25 @@ __global__ void __launch_bounds__(32) coarsestPcgDic(CoarsestArgs<T> a)
             *a.logCount = i + 1;
         }
     }
+}
+
+template <class T>
+__global__ void __launch_bounds__(32) coarsestPcgDic(CoarsestArgs<T> a)
+{
+    coarsestPcgDicWarp<T>(a);
+}
+
+// The coarsest solves of many independent cases, one warp each (block i solves cases[i]) to the
+// given tolerance and relTol; a case whose `active` flag (may be null) is 0 is skipped.
+static __global__ void __launch_bounds__(32) coarsestPcgDicBatch(const CoarsestArgs<double>* __restrict__ cases,
+                                                          double tolerance, double relTol,
+                                                          const int* __restrict__ active)
+{
+    if (active && active[blockIdx.x] == 0) return;
+    CoarsestArgs<double> a = cases[blockIdx.x];
+    a.tolerance = tolerance;
+    a.relTol = relTol;
+    coarsestPcgDicWarp<double>(a);
 }
 
 }  // namespace k

@@ -378,10 +378,11 @@ __device__ __forceinline__ T rowTerms(T acc, unsigned cA, unsigned vA, unsigned 
     return acc;
 }
 
-// One Gauss-Seidel sweep of one level, in position order. Grid = P parts; blockDim = M + 128:
-// M compute threads, then the TMA warp, the gather warp, the publisher warp and the watcher warp.
+// Part p of one Gauss-Seidel sweep of one level, in position order. blockDim >= M + 128: M compute
+// threads, then the TMA warp, the gather warp, the publisher warp and the watcher warp; warps
+// beyond those (a batched launch sized for a larger M) leave after the set-up barrier.
 template <class T>
-__global__ void __launch_bounds__(kMaxCompute + 128, 1) gsSweep(GsArgs<T> a)
+__device__ __forceinline__ void gsSweepPart(const GsArgs<T>& a, const int p)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) unsigned long long full[kStages];
@@ -399,7 +400,6 @@ __global__ void __launch_bounds__(kMaxCompute + 128, 1) gsSweep(GsArgs<T> a)
     const unsigned sb = slotBytes<T>(M, a.maxEnt, G);
     const unsigned bOff = slotBOffset<T>(M, a.maxEnt);     // b follows the blob in a slot
     const unsigned lOff = slotListOffset<T>(M, a.maxEnt);  // then the gather sources
-    const int p = blockIdx.x;
     const int t = threadIdx.x;
     const int c0 = a.partChunkStart[p];
     const int nCh = a.partChunkStart[p + 1] - c0;
@@ -424,6 +424,7 @@ __global__ void __launch_bounds__(kMaxCompute + 128, 1) gsSweep(GsArgs<T> a)
         fenceProxyAsyncShared();
     }
     __syncthreads();
+    if (t >= M + 128) return;
 
     if (t >= M + 96)
     {
@@ -670,6 +671,33 @@ __global__ void __launch_bounds__(kMaxCompute + 128, 1) gsSweep(GsArgs<T> a)
         ptrace[2] = globalTimer();
         ptrace[3] = clockStamp();
     }
+}
+
+// One sweep of one level: grid = the level's P parts.
+template <class T>
+__global__ void __launch_bounds__(kMaxCompute + 128, 1) gsSweep(GsArgs<T> a)
+{
+    gsSweepPart<T>(a, blockIdx.x);
+}
+
+// One sweep of one level of many independent cases in ONE launch: block i runs part parts[i].y of
+// the case whose arguments are cases[parts[i].x]; parts[i].z indexes `active` (may be null), and a
+// case whose flag is 0 is skipped. A case's parts follow each other in block order, and a part waits
+// only for lower-numbered parts of its own case, which are dispatched first.
+template <class T>
+__global__ void __launch_bounds__(kMaxCompute + 128, 1) gsSweepBatch(const GsArgs<T>* __restrict__ cases,
+                                                                     const int4* __restrict__ parts,
+                                                                     const int* __restrict__ active)
+{
+    __shared__ __align__(16) GsArgs<T> sa;
+    const int4 cp = parts[blockIdx.x];
+    if (active && active[cp.z] == 0) return;
+    static_assert(sizeof(GsArgs<T>) % 4 == 0, "GsArgs copied word by word");
+    constexpr int kWords = static_cast<int>(sizeof(GsArgs<T>) / 4);
+    const int* src = reinterpret_cast<const int*>(cases + cp.x);
+    for (int i = threadIdx.x; i < kWords; i += blockDim.x) reinterpret_cast<int*>(&sa)[i] = src[i];
+    __syncthreads();
+    gsSweepPart<T>(sa, cp.y);
 }
 
 // The chunk blobs of one level in value type T (one block per chunk): the diagonal and row

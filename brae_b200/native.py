@@ -100,6 +100,10 @@ def _load():
                                       C.POINTER(_Log)]),
         "b2g_matrix_timings": (ip, [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
         "b2g_level_smooth_trace": (ip, [vp, ip, vp, vp, vp, ip, C.POINTER(C.c_int)]),
+        "b2g_batch_create": (ip, [C.POINTER(vp), ip, C.POINTER(vp)]),
+        "b2g_batch_solve": (ip, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(Controls), ip, C.POINTER(_Perf)]),
+        "b2g_batch_launches": (ip, [vp, C.POINTER(C.c_longlong)]),
+        "b2g_batch_destroy": (ip, [vp]),
         "b2g_server_create": (ip, [C.c_ulonglong, ip, C.POINTER(vp)]),
         "b2g_server_destroy": (ip, [vp]),
         "b2g_server_add_case": (ip, [vp, ip, ip, vp, vp, vp, vp, vp, vp, ip, ip, C.POINTER(C.c_int)]),
@@ -124,7 +128,8 @@ EXPORTED = [
     "b2g_step_prolong", "b2g_level_norm_factor", "b2g_level_pcg_dic", "b2g_precondition",
     "b2g_matrix_pcg_solve", "b2g_matrix_timings", "b2g_level_smooth_trace", "b2g_level_pcg_dic_static",
     "b2g_level_schedule", "b2g_server_create", "b2g_server_destroy", "b2g_server_add_case",
-    "b2g_server_submit", "b2g_server_wait", "b2g_server_case_bytes",
+    "b2g_server_submit", "b2g_server_wait", "b2g_server_case_bytes", "b2g_batch_create", "b2g_batch_solve",
+    "b2g_batch_launches", "b2g_batch_destroy",
 ]
 
 
@@ -468,3 +473,47 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+class Batch:
+    """The batched form (b2g_batch_*): many matrices, each on its own mesh, solved together with every
+    level step one launch over all cases. The matrices are kept alive as long as the batch."""
+
+    def __init__(self, matrices):
+        self.matrices = list(matrices)
+        arr = (C.c_void_p * len(self.matrices))(*[m.handle.value for m in self.matrices])
+        h = C.c_void_p()
+        _check(lib.b2g_batch_create(arr, len(self.matrices), C.byref(h)))
+        self.handle = h
+
+    def solve(self, sources, psis, controls: Controls):
+        """Solves every case: sources[k], psis[k] (numpy arrays or CUDA tensors, all of one kind, natural
+        cell order); psis are overwritten. Returns the list of SolverPerformance."""
+        K = len(self.matrices)
+        if len(sources) != K or len(psis) != K:
+            raise ValueError("one source and one psi per case")
+        hold = []
+        src_p = (C.c_void_p * K)()
+        psi_p = (C.c_void_p * K)()
+        for k in range(K):
+            s, x = sources[k], psis[k]
+            if not _is_torch(s):
+                s = _as_host(s, np.float64)
+                hold.append(s)
+            src_p[k] = _ptr(s)
+            psi_p[k] = _ptr(x)
+        ms = _memspace(*sources, *psis)
+        perfs = (_Perf * K)()
+        _check(lib.b2g_batch_solve(self.handle, src_p, psi_p, C.byref(controls), ms, perfs))
+        return [SolverPerformance(p.initialResidual, p.finalResidual, p.nIterations) for p in perfs]
+
+    def launches(self) -> int:
+        v = C.c_longlong()
+        _check(lib.b2g_batch_launches(self.handle, C.byref(v)))
+        return v.value
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value and lib is not None:
+            lib.b2g_batch_destroy(h)
+            self.handle = None

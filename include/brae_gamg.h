@@ -288,6 +288,26 @@ B2G_API b2g_status b2g_level_smooth_trace(b2g_matrix* m, int level, double* psi,
  * gathers, depth, upstream depth, same-part wait, depth change, blob offsets). */
 B2G_API b2g_status b2g_level_schedule(const b2g_mesh* mesh, int level, int* partChunkStart, int* chunkRecords);
 
+/* ---- the batched form: many independent cases in one solve ------------------------------------ */
+
+/* A batch of matrices (each on its own mesh), solved together: every step of every level is one
+ * launch over all the cases that have that level (levels aligned from the finest), the coarsest
+ * solves run one warp per case in one launch, and each PCG iteration is one CUDA graph. Each case's
+ * result is the one b2g_matrix_pcg_solve gives: bit for bit with serial-order reductions; with tree
+ * reductions the sums are shaped per 2048-cell tile (the same alone or in any batch). No counterpart
+ * in the reference's solver interface. The matrices must outlive the batch; the batch runs on a
+ * stream of its own. */
+typedef struct b2g_batch b2g_batch;
+B2G_API b2g_status b2g_batch_create(b2g_matrix* const* matrices, int count, b2g_batch** out);
+/* Solves every case (controls->solver must be PCG + GAMG; both precision forms): sources[k] and
+ * psis[k] are case k's fields in natural cell order in `memspace`, psis[k] overwritten with the
+ * solution; perfs[count] receives each case's SolverPerformance. */
+B2G_API b2g_status b2g_batch_solve(b2g_batch* batch, const double* const* sources, double* const* psis,
+                                   const b2g_controls* controls, int memspace, b2g_perf* perfs);
+/* Kernel launches of the last b2g_batch_solve (a graph replay counts its launches). */
+B2G_API b2g_status b2g_batch_launches(const b2g_batch* batch, long long* launches);
+B2G_API b2g_status b2g_batch_destroy(b2g_batch* batch);
+
 /* ---- the serving form: many independent cases, solves queued as they arrive ------------------ */
 
 /* A request loop on the current device (no counterpart in the reference's solver interface; it
