@@ -305,6 +305,9 @@ def run_ours(args, world, rank, local):
                "iterations": cperf[2], "final_residual": cperf[1],
                "field_rel_diff_vs_gpu": float(np.abs(cpsi - psi64).max() / np.abs(cpsi).max())}
 
+    batched = None
+    if not args.no_batched and world == 1:
+        batched = batched_leg(args, b2g, local)
     served = None
     if not args.no_serve and world == 1:
         served = serve_stream(args, b2g, local)
@@ -341,10 +344,87 @@ def run_ours(args, world, rank, local):
         "gpu_launches": int(cnt_acc[3]),
         "clocks": clocks.summary(),
         "cpu_baseline": cpu,
+        "batched": batched,
         "served": served,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def batched_leg(args, b2g, local):
+    """The batched form: 256 cases (cell counts log-uniform in 4,096..1,048,576, aspect ratios
+    uniform[1,8], grading uniform[1,20], seed 1), FP32-preconditioned PCG to tolerance 1e-6 (relTol 0)
+    from psi = 0, all solved by one b2g_batch; beside it the same cases solved one after another
+    through the single-case path. Fields are resident on the device in both."""
+    import torch
+
+    from brae_b200 import cases
+    dev = torch.device("cuda", local)
+    t0 = time.perf_counter()
+    dims = cases.mixed_batch_sizes(args.batch_cases)
+    built, meshes, mats = [], [], []
+    td = lambda a, dt=torch.float64: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)
+    for d in dims:
+        c = cases.box_case(*d["n"], d["lengths"], d["grading"], False, 0)
+        m = b2g.Mesh(td(c.lower, torch.int32), td(c.upper, torch.int32), td(c.Sf.reshape(-1)), td(c.magSf),
+                     c.n_cells, 10, True)
+        meshes.append(m)
+        mats.append(b2g.Matrix(m, td(c.diag), td(c.coef)))
+        built.append((c.n_cells, c.n_faces, c.source))
+        del c
+    sizes = [n for n, _, _ in built]
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    src_all = torch.cat([td(s) for _, _, s in built])
+    psi_all = torch.zeros(int(off[-1]), dtype=torch.float64, device=dev)
+    srcs = [src_all[off[k]:off[k + 1]] for k in range(len(sizes))]
+    psis = [psi_all[off[k]:off[k + 1]] for k in range(len(sizes))]
+    batch = b2g.Batch(mats)
+    setup_s = time.perf_counter() - t0
+    ctl = b2g.controls_default(tolerance=1e-6, relTol=0.0, maxIter=MAX_ITER, precision="fp32_precond")
+    stream = torch.cuda.current_stream()
+    for _ in range(max(1, args.warmup)):
+        psi_all.zero_()
+        batch.solve(srcs, psis, ctl)
+    ts = []
+    for _ in range(max(1, args.steps)):
+        psi_all.zero_()
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        perfs = batch.solve(srcs, psis, ctl)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        ts.append(a0.elapsed_time(a1) / 1e3)
+    batch_s = float(np.median(ts))
+    launches = batch.launches()
+    x_batch = psi_all.cpu().numpy()
+    # the same cases one after another through the single-case path (graphs captured by a warm-up)
+    for k in range(len(mats)):
+        psis[k].zero_()
+        mats[k].solve(srcs[k], psis[k], ctl, history_cap=0)
+    psi_all.zero_()
+    torch.cuda.synchronize()
+    b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b0.record(stream)
+    single_its = []
+    for k in range(len(mats)):
+        single_its.append(mats[k].solve(srcs[k], psis[k], ctl, history_cap=0)[0].nIterations)
+    b1.record(stream)
+    torch.cuda.synchronize()
+    seq_s = b0.elapsed_time(b1) / 1e3
+    x_seq = psi_all.cpu().numpy()
+    its = [p.nIterations for p in perfs]
+    diff = max(float(np.abs(x_batch[off[k]:off[k + 1]] - x_seq[off[k]:off[k + 1]]).max() /
+                     max(np.abs(x_seq[off[k]:off[k + 1]]).max(), 1e-300)) for k in range(len(sizes)))
+    return {"workload": f"{len(sizes)} cases, cells log-uniform 4096..1048576 (seed 1), FP32-precond PCG+GAMG "
+                        f"tol 1e-6 relTol 0", "cases": len(sizes), "cells": int(off[-1]),
+            "setup_s": setup_s, "batch_s": batch_s, "cases_per_s": len(sizes) / batch_s,
+            "cells_per_s": float(off[-1]) / batch_s, "gpu_launches": int(launches),
+            "iterations": {"min": int(min(its)), "max": int(max(its)), "mean": float(np.mean(its))},
+            "sequential_s": seq_s, "speedup_vs_sequential": seq_s / batch_s,
+            "iterations_match_sequential": int(sum(a == b for a, b in zip(its, single_its))),
+            "max_field_rel_diff_vs_sequential": diff,
+            "max_final_residual": float(max(p.finalResidual for p in perfs))}
 
 
 def serve_stream(args, b2g, local):
@@ -471,6 +551,9 @@ def main():
     ap.add_argument("--n", type=int, default=272)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream leg")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched leg")
+    ap.add_argument("--batch-cases", type=int, default=256, help="cases in the batched leg")
+    ap.add_argument("--batched", action="store_true", help="run the batched leg alone")
     ap.add_argument("--serve-seconds", type=float, default=4.0,
                     help="length of the served stream's arrival window (the full stream is 60 s)")
     ap.add_argument("--serve-rate", type=float, default=500.0, help="offered requests per second")
@@ -481,6 +564,13 @@ def main():
     args = ap.parse_args()
     if args.sweep:
         run_sweep(args)
+        return
+    if args.batched:
+        import torch
+
+        import brae_b200.native as b2g
+        torch.cuda.set_device(0)
+        print(json.dumps({"batched": batched_leg(args, b2g, 0)}), flush=True)
         return
     if args.serve:
         import torch
