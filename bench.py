@@ -437,7 +437,7 @@ def serve_stream(args, b2g, local):
     from brae_b200 import cases
     t0 = time.perf_counter()
     srv = b2g.Server(150 << 30, slots=args.serve_slots)
-    pop = cases.served_population()
+    pop = cases.served_population(per_class=(48, 16, 4))
     resident = []  # per class: [(case id, n cells, source)]
     for k, sizes in enumerate(pop):
         row = []
@@ -455,7 +455,10 @@ def serve_stream(args, b2g, local):
                           "cells": [[n for _, n, _ in r] for r in resident], "setup_s": setup_s,
                           "slots": args.serve_slots, "hbm_cap_gb": 150},
            "offered_rate_per_s": args.serve_rate, "stream_s": args.serve_seconds}
-    for form, prec in (("fp64", 0), ("fp32_precond", 1)):
+    runs = [(form, prec, args.serve_rate) for form, prec in (("fp64", 0), ("fp32_precond", 1))]
+    if args.serve_rate_low > 0:
+        runs += [(form + "_at_low_rate", prec, args.serve_rate_low) for form, prec in (("fp64", 0), ("fp32_precond", 1))]
+    for form, prec, rate in runs:
         ctl = b2g.controls_default(tolerance=TOL, relTol=REL_TOL, maxIter=MAX_ITER, precision=prec)
         # warm every case once in this form (captures its iteration graph)
         for row in resident:
@@ -464,7 +467,7 @@ def serve_stream(args, b2g, local):
                 srv.wait(srv.submit(cid, src, ctl, out=buf))
                 buf[:] = 0.0
         rng = np.random.default_rng(2)
-        gaps = rng.exponential(1.0 / args.serve_rate, size=int(args.serve_rate * args.serve_seconds * 1.5) + 16)
+        gaps = rng.exponential(1.0 / rate, size=int(rate * args.serve_seconds * 1.5) + 16)
         arrivals = np.cumsum(gaps)
         arrivals = arrivals[arrivals < args.serve_seconds]
         cls = np.searchsorted(probs, rng.random(arrivals.size), side="right").clip(0, 2)
@@ -472,17 +475,19 @@ def serve_stream(args, b2g, local):
         lock = threading.Lock()
         done = _queue.Queue()
         lat, iters = [], []
+        lat_cls = [[], [], []]
         outstanding = [0, 0]      # now, max
         def collect():
             while True:
                 item = done.get()
                 if item is None:
                     return
-                t, cid = item
+                t, cid, k = item
                 psi, perf, ms = srv.wait(t)
                 psi[:] = 0.0
                 with lock:
                     lat.append(ms)
+                    lat_cls[k].append(ms)
                     iters.append(perf.nIterations)
                     free.setdefault(cid, []).append(psi)
                     outstanding[0] -= 1
@@ -502,15 +507,17 @@ def serve_stream(args, b2g, local):
                 outstanding[1] = max(outstanding[1], outstanding[0])
             if buf is None:
                 buf = np.zeros(n)
-            done.put((srv.submit(cid, src, ctl, out=buf), cid))
+            done.put((srv.submit(cid, src, ctl, out=buf), cid, int(k)))
         done.put(None)
         th.join()
         wall = time.perf_counter() - start
         lat_a = np.asarray(lat)
-        out[form] = {"requests": int(arrivals.size), "p50_ms": float(np.percentile(lat_a, 50)),
+        out[form] = {"offered_rate_per_s": rate, "requests": int(arrivals.size), "p50_ms": float(np.percentile(lat_a, 50)),
                      "p99_ms": float(np.percentile(lat_a, 99)), "mean_ms": float(lat_a.mean()),
                      "solves_per_s": arrivals.size / wall, "drain_s": wall - args.serve_seconds,
-                     "max_outstanding": outstanding[1], "mean_iterations": float(np.mean(iters))}
+                     "max_outstanding": outstanding[1], "mean_iterations": float(np.mean(iters)),
+                     "by_class": [{"requests": len(l), "p50_ms": float(np.percentile(l, 50)) if l else None,
+                                   "p99_ms": float(np.percentile(l, 99)) if l else None} for l in lat_cls]}
     srv.close()
     return out
 
@@ -557,7 +564,9 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=4.0,
                     help="length of the served stream's arrival window (the full stream is 60 s)")
     ap.add_argument("--serve-rate", type=float, default=500.0, help="offered requests per second")
-    ap.add_argument("--serve-slots", type=int, default=16, help="server worker slots")
+    ap.add_argument("--serve-slots", type=int, default=6, help="server worker slots")
+    ap.add_argument("--serve-rate-low", type=float, default=150.0,
+                    help="a second stream below the server's capacity (0: none)")
     ap.add_argument("--serve", action="store_true", help="run the served stream alone")
     ap.add_argument("--sweep", action="store_true",
                     help="time the finest-level Gauss-Seidel sweep of the --n box alone (for profiling)")

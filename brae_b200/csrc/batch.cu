@@ -702,6 +702,12 @@ Batch::Batch(std::vector<Matrix*> cs, cudaStream_t s) : stream(s), cases(std::mo
     if (K < 1) fail(B2G_ERR_ARGUMENT, "b2g batch: no cases");
     int dev = 0;
     B2G_CUDA(cudaGetDevice(&dev));
+    {
+        std::vector<Matrix*> sorted(cases);
+        std::sort(sorted.begin(), sorted.end());
+        if (std::adjacent_find(sorted.begin(), sorted.end()) != sorted.end())
+            fail(B2G_ERR_ARGUMENT, "b2g batch: a matrix appears twice (each case is one matrix)");
+    }
     for (Matrix* A : cases)
     {
         if (!A) fail(B2G_ERR_ARGUMENT, "b2g batch: null case");
@@ -1200,7 +1206,14 @@ void Batch::solve(const b2g_controls& c, const double* const* source, double* co
         std::vector<unsigned char> key(sizeof(b2g_controls) + 1);
         std::memcpy(key.data(), &c, sizeof(b2g_controls));
         key[sizeof(b2g_controls)] = serial ? 1 : 0;
-        if (!graph.exec || graph.key != key)
+        if (eagerIterations == 0 && (!graph.exec || graph.key != key))
+        {
+            // a batch's first iteration runs as plain launches: capturing pays off only from the
+            // first replay, and many batches (a serving group) iterate once
+            ++eagerIterations;
+            iteration(c);
+        }
+        else if (!graph.exec || graph.key != key)
         {
             if (graph.exec) B2G_CUDA(cudaGraphExecDestroy(graph.exec));
             graph.exec = nullptr;
@@ -1229,7 +1242,7 @@ void Batch::solve(const b2g_controls& c, const double* const* source, double* co
         {
             launches += graph.launchesPerReplay;
         }
-        B2G_CUDA(cudaGraphLaunch(graph.exec, stream));
+        if (graph.exec && graph.key == key) B2G_CUDA(cudaGraphLaunch(graph.exec, stream));
         B2G_CUDA(cudaMemcpyAsync(&going, nActive.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
         B2G_CUDA(cudaStreamSynchronize(stream));
     }

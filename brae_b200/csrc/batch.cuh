@@ -111,6 +111,7 @@ struct Batch
     DBuf<float> partial32, sf32;
     DBuf<BatchPerf> perf;                   // [K]
     IterationGraph graph;
+    int eagerIterations = 0;                // iterations run without a graph (the first one)
     bool serial = false;
     long long launches = 0;
 

@@ -311,10 +311,14 @@ B2G_API b2g_status b2g_batch_destroy(b2g_batch* batch);
 /* ---- the serving form: many independent cases, solves queued as they arrive ------------------ */
 
 /* A request loop on the current device (no counterpart in the reference's solver interface; it
- * serves the same solve, b2g_matrix_pcg_solve, to many cases at once). nSlots worker threads, each
- * with its own stream, take queued requests oldest first, so a request that arrives while others
- * are on the GPU starts as soon as a slot frees up, and their work overlaps on the device. A case
- * is solved by one slot at a time. Each PCG iteration of a case runs as one CUDA graph launch. */
+ * serves the PCG + GAMG solve to many cases at once). nSlots worker threads, each with its own
+ * stream and a size class it serves first (slot i: class i mod 3; classes below 2^18 cells, below
+ * 2^22, larger), take the oldest queued request of that class (else of any class) together with the
+ * queued requests of other idle cases of its class (at most 64, 16 and 4 cases) and controls,
+ * and solve the group as one batch (b2g_batch_*: each level step one launch over all of them, each
+ * PCG iteration one CUDA graph). Requests that arrive while others are on the GPU join the next
+ * group, and the slots' groups overlap on the device. A case is solved by one slot at a time; its
+ * result is the same in any group (b2g_batch_solve's). Standalone GAMG requests are solved alone. */
 typedef struct b2g_server b2g_server;
 B2G_API b2g_status b2g_server_create(unsigned long long hbmCapBytes, int nSlots, b2g_server** out);
 /* Stops the workers (queued requests are dropped) and frees every case. */

@@ -136,3 +136,5 @@ def test_batch_device_fields_and_refusals(b2g, oracle):
     with pytest.raises(b2g.GamgError, match="batched solve is PCG"):
         batch.solve([c.source for c in built], [np.zeros(c.n_cells) for c in built],
                     b2g.controls_default(solver="GAMG"))
+    with pytest.raises(b2g.GamgError, match="appears twice"):
+        b2g.Batch([mats[0], mats[1], mats[0]])

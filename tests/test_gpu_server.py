@@ -1,10 +1,10 @@
 """The serving form (b2g_server_*): each result is the same alone and in the mix, and admission by
 HBM footprint evicts idle cases least recently used first, or refuses.
 
-A solve in the mix runs the same kernels on the same resident case as a solve alone, with
-deterministic reductions, so the bar is bit-for-bit identity between the two, for both forms
-(plain FP64 and the FP32 V-cycle) and both reduction orders; the serial-order FP64 results are
-also checked bit for bit against the oracle's pcgGamgSolve.
+A solve in the mix is the same batched solve as a solve alone (a case's reductions are its own, in
+a fixed order, whatever group it is solved in), so the bar is bit-for-bit identity between the two,
+for both forms (plain FP64 and the FP32 V-cycle) and both reduction orders; the serial-order FP64
+results are also checked bit for bit against the oracle's pcgGamgSolve.
 """
 import numpy as np
 import pytest
@@ -78,8 +78,11 @@ def test_initial_guess_and_standalone_gamg(b2g):
             got, perf, _ = srv.wait(srv.submit(cid, c.source, ctl, psi0=psi0))
             mesh = b2g.Mesh(c.lower, c.upper, c.Sf, c.magSf, c.n_cells)
             want = psi0.copy()
-            solve = b2g.pcg_gamg_solve if solver == "PCG" else b2g.gamg_solve
-            wperf = solve(mesh, c.diag, c.coef, c.source, want, ctl)[0]
+            if solver == "PCG":  # served as a batch: the batched solve's result
+                A = b2g.Matrix(mesh, c.diag, c.coef)
+                wperf = b2g.Batch([A]).solve([c.source], [want], ctl)[0]
+            else:                # served alone: the standalone solver's
+                wperf = b2g.gamg_solve(mesh, c.diag, c.coef, c.source, want, ctl)[0]
             assert tuple(perf) == tuple(wperf)
             assert np.array_equal(got, want)
     finally:
