@@ -265,7 +265,7 @@ def run_ours(args, world, rank, local):
     A2 = b2g.Matrix(mesh, td(tp.diag), td(tp.coef))
     src2 = td(tp.source)
     forms = {}
-    for name, prec in (("fp64", 0), ("fp32_precond", 1)):
+    for name, prec in (("fp64", 0), ("fp32_precond", 1), ("fp32_precond_multicolour", 2)):
         c2 = b2g.controls_default(tolerance=TOL, relTol=REL_TOL, maxIter=MAX_ITER, precision=prec)
         x = torch.zeros(case.n_cells, dtype=torch.float64, device=dev)
         A2.solve(src2, x, c2, history_cap=0)
@@ -283,6 +283,7 @@ def run_ours(args, world, rank, local):
         forms[name] = dict(s=barrier_max(float(np.mean(ts)), world), perf=list(p2), psi=x.cpu().numpy())
     ref_x = forms["fp64"]["psi"]
     field_err = float(np.abs(forms["fp32_precond"]["psi"] - ref_x).max() / np.abs(ref_x).max())
+    field_err_mc = float(np.abs(forms["fp32_precond_multicolour"]["psi"] - ref_x).max() / np.abs(ref_x).max())
 
     # roofline of the dominant kernel: the finest level's Gauss-Seidel sweep (its share is below)
     peak, peak_kind = measured_peaks()
@@ -329,6 +330,13 @@ def run_ours(args, world, rank, local):
             "speedup": forms["fp64"]["s"] / forms["fp32_precond"]["s"],
             "fp64_perf": forms["fp64"]["perf"], "fp32_precond_perf": forms["fp32_precond"]["perf"],
             "field_rel_err_vs_fp64": field_err,
+            "multicolour": {
+                "s": forms["fp32_precond_multicolour"]["s"],
+                "speedup": forms["fp64"]["s"] / forms["fp32_precond_multicolour"]["s"],
+                "perf": forms["fp32_precond_multicolour"]["perf"],
+                "field_rel_err_vs_fp64": field_err_mc,
+                "note": "FP32 V-cycle with Gauss-Seidel sweeps colour by colour (B2G_PRECISION_FP32_PRECOND_MULTICOLOUR)",
+            },
         },
         "kernels": {
             "gs_finest_us_per_launch": gs_ms * 1e3, "gs_finest_launches": int(cnt_acc[1]),
@@ -398,6 +406,24 @@ def batched_leg(args, b2g, local):
     batch_s = float(np.median(ts))
     launches = batch.launches()
     x_batch = psi_all.cpu().numpy()
+    # the multicolour FP32 form of the same batch
+    ctl_mc = b2g.controls_default(tolerance=1e-6, relTol=0.0, maxIter=MAX_ITER, precision="fp32_precond_multicolour")
+    psi_all.zero_()
+    t_prep = time.perf_counter()
+    batch.solve(srcs, psis, ctl_mc)  # prepares the colourings (untimed)
+    prep_s = time.perf_counter() - t_prep
+    ts_mc = []
+    for _ in range(max(1, args.steps)):
+        psi_all.zero_()
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        perfs_mc = batch.solve(srcs, psis, ctl_mc)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        ts_mc.append(a0.elapsed_time(a1) / 1e3)
+    batch_mc_s = float(np.median(ts_mc))
+    its_mc = [p.nIterations for p in perfs_mc]
     # the same cases one after another through the single-case path (graphs captured by a warm-up)
     for k in range(len(mats)):
         psis[k].zero_()
@@ -424,7 +450,14 @@ def batched_leg(args, b2g, local):
             "sequential_s": seq_s, "speedup_vs_sequential": seq_s / batch_s,
             "iterations_match_sequential": int(sum(a == b for a, b in zip(its, single_its))),
             "max_field_rel_diff_vs_sequential": diff,
-            "max_final_residual": float(max(p.finalResidual for p in perfs))}
+            "max_final_residual": float(max(p.finalResidual for p in perfs)),
+            "multicolour": {"batch_s": batch_mc_s, "cases_per_s": len(sizes) / batch_mc_s,
+                            "cells_per_s": float(off[-1]) / batch_mc_s,
+                            "speedup_vs_sequential": seq_s / batch_mc_s,
+                            "iterations": {"min": int(min(its_mc)), "max": int(max(its_mc)),
+                                           "mean": float(np.mean(its_mc))},
+                            "max_final_residual": float(max(p.finalResidual for p in perfs_mc)),
+                            "colouring_build_s": prep_s}}
 
 
 def serve_stream(args, b2g, local):
@@ -455,9 +488,11 @@ def serve_stream(args, b2g, local):
                           "cells": [[n for _, n, _ in r] for r in resident], "setup_s": setup_s,
                           "slots": args.serve_slots, "hbm_cap_gb": 150},
            "offered_rate_per_s": args.serve_rate, "stream_s": args.serve_seconds}
-    runs = [(form, prec, args.serve_rate) for form, prec in (("fp64", 0), ("fp32_precond", 1))]
+    runs = [(form, prec, args.serve_rate) for form, prec in (("fp64", 0), ("fp32_precond", 1),
+                                                               ("fp32_precond_multicolour", 2))]
     if args.serve_rate_low > 0:
-        runs += [(form + "_at_low_rate", prec, args.serve_rate_low) for form, prec in (("fp64", 0), ("fp32_precond", 1))]
+        runs += [(form + "_at_low_rate", prec, args.serve_rate_low)
+                 for form, prec in (("fp64", 0), ("fp32_precond", 1), ("fp32_precond_multicolour", 2))]
     for form, prec, rate in runs:
         ctl = b2g.controls_default(tolerance=TOL, relTol=REL_TOL, maxIter=MAX_ITER, precision=prec)
         # warm every case once in this form (captures its iteration graph)

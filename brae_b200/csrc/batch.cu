@@ -189,6 +189,33 @@ __global__ void __launch_bounds__(BT) bProlong(const int4* __restrict__ tiles, c
     for (int i = t.y + threadIdx.x; i < t.z; i += BT) ff[i] = cf[map[i]];
 }
 
+// one colour of a multicolour Gauss-Seidel sweep of the FP32 V-cycle: tiles of one colour's rows
+__global__ void __launch_bounds__(BT) bMcSweep(const int4* __restrict__ tiles, const SegLevel<float>* __restrict__ segs,
+                                               int rpsi, int rsrc, const int* __restrict__ active)
+{
+    const int4 t = tiles[blockIdx.x];
+    const SegLevel<float>& s = segs[t.x];
+    if (inactive(s, active)) return;
+    const int* __restrict__ pos = s.mcPos;
+    const int* __restrict__ slice = s.mcSlice;
+    const int* __restrict__ col = s.mcCol;
+    const float* __restrict__ val = s.mcVal;
+    const float* __restrict__ diag = s.mcDiag;
+    const float* __restrict__ b = s.v[rsrc];
+    float* __restrict__ psi = s.v[rpsi];
+    for (int r = t.y + threadIdx.x; r < t.z; r += BT)
+    {
+        const int p = pos[r];
+        if (p < 0) continue;
+        const int sl = r >> 5;
+        const int base = slice[sl];
+        const int w = (slice[sl + 1] - base) >> 5;
+        float acc = b[p];
+        for (int q = 0, e = base + (r & 31); q < w; ++q, e += 32) acc = fmaf(-val[e], psi[col[e]], acc);
+        psi[p] = acc / diag[r];
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // scale (GAMG:386-407), per case
 // ---------------------------------------------------------------------------------------------
@@ -791,6 +818,7 @@ Batch::Batch(std::vector<Matrix*> cs, cudaStream_t s) : stream(s), cases(std::mo
             hD[segOfCase[c][lv]].coarseSeg = hF[segOfCase[c][lv]].coarseSeg = segOfCase[c][lv + 1];
     segD.upload(hD.data(), hD.size(), stream);
     segF.upload(hF.data(), hF.size(), stream);
+    hostF = hF;
     err.alloc(1, stream);
     err.zero(stream);
     // tile lists and the Gauss-Seidel launch of each level
@@ -916,6 +944,57 @@ Batch::Batch(std::vector<Matrix*> cs, cudaStream_t s) : stream(s), cases(std::mo
     B2G_CUDA(cudaStreamSynchronize(stream));
 }
 
+// The multicolour layout of every case's levels (built on each mesh once) in the FP32 descriptors,
+// and per level and colour the tiles of the swept cases' rows of that colour.
+void Batch::prepareMulticolour()
+{
+    if (mcReady) return;
+    const int K = static_cast<int>(cases.size());
+    for (Matrix* A : cases)
+    {
+        A->ensureMulticolour();
+        B2G_CUDA(cudaStreamSynchronize(A->stream));
+    }
+    for (int c = 0; c < K; ++c)
+        for (int lv = 0; lv <= nLevelsOf[c]; ++lv)
+        {
+            const Colouring& C = cases[c]->mesh->lev[lv].mc;
+            SegLevel<float>& f = hostF[segOfCase[c][lv]];
+            f.mcPos = C.pos.p;
+            f.mcSlice = C.sliceBase.p;
+            f.mcCol = C.col.p;
+            f.mcVal = cases[c]->v32.coef[lv].mcVal.p;
+            f.mcDiag = cases[c]->v32.coef[lv].mcDiag.p;
+        }
+    segF.upload(hostF.data(), hostF.size(), stream);
+    for (int lv = 0; lv <= maxLevels; ++lv)
+    {
+        int nCol = 0;
+        for (int c = 0; c < K; ++c)
+            if (nLevelsOf[c] >= lv + 1) nCol = std::max(nCol, cases[c]->mesh->lev[lv].mc.nColours);
+        lev[lv].mc.clear();
+        lev[lv].mc.resize(nCol);
+        for (int k = 0; k < nCol; ++k)
+        {
+            std::vector<int4> tiles;
+            for (int c = 0; c < K; ++c)
+            {
+                if (nLevelsOf[c] < lv + 1) continue;
+                const Colouring& C = cases[c]->mesh->lev[lv].mc;
+                if (k >= C.nColours) continue;
+                const int sg = segOfCase[c][lv];
+                for (int b = C.colourStart[k]; b < C.colourStart[k + 1]; b += kTile)
+                    tiles.push_back(make_int4(sg, b, std::min(C.colourStart[k + 1], b + kTile), 0));
+            }
+            TileList& L = lev[lv].mc[k];
+            L.nTiles = static_cast<int>(tiles.size());
+            if (!tiles.empty()) L.tiles.upload(tiles.data(), tiles.size(), stream);
+        }
+    }
+    B2G_CUDA(cudaStreamSynchronize(stream));
+    mcReady = true;
+}
+
 Batch::~Batch()
 {
     if (graph.exec) cudaGraphExecDestroy(graph.exec);
@@ -930,6 +1009,20 @@ void Batch::smooth(int lv, int nSweeps)
 {
     BatchLevel& B = lev[lv];
     if (nSweeps <= 0 || B.nParts == 0) return;
+    if (sizeof(T) == 4 && multicolour)
+    {
+        const int rpsi = lv == 0 ? V_W : V_CORR;
+        const int rsrc = lv == 0 ? V_R : V_SRC;
+        for (int sw = 0; sw < nSweeps; ++sw)
+            for (const TileList& L : B.mc)
+            {
+                if (L.nTiles == 0) continue;
+                bMcSweep<<<L.nTiles, BT, 0, stream>>>(L.tiles.p, segF.p, rpsi, rsrc, active.p);
+                ++launches;
+            }
+        B2G_LAUNCH_CHECK();
+        return;
+    }
     const k::GsArgs<T>* args = sizeof(T) == 8 ? reinterpret_cast<const k::GsArgs<T>*>(B.gs64.p)
                                               : reinterpret_cast<const k::GsArgs<T>*>(B.gs32.p);
     const size_t smem = sizeof(T) == 8 ? B.smem64 : B.smem32;
@@ -1051,7 +1144,7 @@ void Batch::precondition(const b2g_controls& c)
 {
     const TileList& L = lev[0].all;
     const int* act = active.p;
-    if (c.precision == B2G_PRECISION_FP32_PRECOND)
+    if (c.precision != B2G_PRECISION_FP64)
     {
         bCast<float, double><<<B2G_TILES(L)>>>(L.tiles.p, segF.p, segD.p, V_R, V_R, act);
         bZero<float><<<B2G_TILES(L)>>>(L.tiles.p, segF.p, V_W, act);
@@ -1120,7 +1213,7 @@ void Batch::iteration(const b2g_controls& c)
 {
     const TileList& L = lev[0].all;
     const int* act = active.p;
-    const bool flexible = c.precision == B2G_PRECISION_FP32_PRECOND;
+    const bool flexible = c.precision != B2G_PRECISION_FP64;
     const int K = static_cast<int>(cases.size());
     precondition(c);
     reduce(k::RED_DOT, V_W, V_R, offsetof(PcgScalars, wArA));
@@ -1154,6 +1247,10 @@ void Batch::solve(const b2g_controls& c, const double* const* source, double* co
         fail(B2G_ERR_REFUSED, "b2g: the device smoother for this entry is GaussSeidel only so far; "
                               "symGaussSeidel, DIC and DICGaussSeidel are not built on the device yet.");
     if (memspace != B2G_MEM_HOST && memspace != B2G_MEM_DEVICE) fail(B2G_ERR_ARGUMENT, "b2g batch: bad memspace");
+    if (c.precision < B2G_PRECISION_FP64 || c.precision > B2G_PRECISION_FP32_PRECOND_MULTICOLOUR)
+        fail(B2G_ERR_ARGUMENT, "b2g batch: unknown precision form");
+    multicolour = c.precision == B2G_PRECISION_FP32_PRECOND_MULTICOLOUR;
+    if (multicolour) prepareMulticolour();
     const int K = static_cast<int>(cases.size());
     serial = c.reduction == B2G_REDUCTION_SERIAL;
     launches = 0;

@@ -54,6 +54,12 @@ struct SegLevel
     PcgScalars* scal;         // the case's PCG scalars
     int caseIdx;
     int pad;
+    // the multicolour layout (hierarchy.cuh Colouring) and its FP32 values, once prepared
+    const int* mcPos;
+    const int* mcSlice;
+    const int* mcCol;
+    const float* mcVal;
+    const float* mcDiag;
 };
 
 // Tiles of cells of some cases on one level: {descriptor, begin, end, the case's index in the list};
@@ -88,6 +94,7 @@ struct BatchLevel
     int block = 0;
     size_t smem64 = 0, smem32 = 0;
     DBuf<unsigned> progress;
+    std::vector<TileList> mc;  // per colour: the swept cases' rows of that colour (multicolour form)
 };
 
 struct Batch
@@ -111,6 +118,9 @@ struct Batch
     DBuf<float> partial32, sf32;
     DBuf<BatchPerf> perf;                   // [K]
     IterationGraph graph;
+    std::vector<SegLevel<float>> hostF;    // host copy of segF
+    bool mcReady = false;                   // the multicolour layouts are prepared
+    bool multicolour = false;               // the current solve sweeps the FP32 V-cycle colour by colour
     int eagerIterations = 0;                // iterations run without a graph (the first one)
     bool serial = false;
     long long launches = 0;
@@ -128,6 +138,7 @@ struct Batch
     void precondition(const b2g_controls& c);
     void reduce(int op, int a, int b, size_t member);
     void iteration(const b2g_controls& c);
+    void prepareMulticolour();
 };
 
 }  // namespace b2g

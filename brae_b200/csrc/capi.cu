@@ -264,6 +264,8 @@ void solveOn(b2g::Matrix& A, const double* source, double* psi, const b2g_contro
 {
     need(c && source && psi && out, "b2g solve: null argument");
     need(memspace == B2G_MEM_HOST || memspace == B2G_MEM_DEVICE, "b2g solve: bad memspace");
+    need(c->precision >= B2G_PRECISION_FP64 && c->precision <= B2G_PRECISION_FP32_PRECOND_MULTICOLOUR,
+         "b2g solve: unknown precision form");
     const int n0 = A.n(0);
     // the solve runs in the finest level's position order: host fields are staged in fc/fr (free
     // outside a solve) and permuted on the device; device fields are permuted in place of a copy

@@ -1286,6 +1286,92 @@ void buildGsSchedule(LevelAddr& L, cudaStream_t s)
     B2G_CUDA(cudaStreamSynchronize(s));
 }
 
+void buildColouring(LevelAddr& L, cudaStream_t s)
+{
+    Colouring& C = L.mc;
+    if (C.nColours > 0) return;
+    const int n = L.nCells;
+    const std::vector<int> rowStart = L.rowStart.download(s);
+    const std::vector<int> col = L.col.download(s);
+    const std::vector<int> entFace = L.entFace.download(s);
+    const std::vector<int> posOf = L.gs.posOf.download(s);
+    // greedy colouring in cell order: the smallest colour no earlier neighbour has
+    std::vector<int> colour(n, -1);
+    std::vector<int> mark;
+    int nColours = 0;
+    for (int c = 0; c < n; ++c)
+    {
+        for (int e = rowStart[c]; e < rowStart[c + 1]; ++e)
+        {
+            const int k = colour[col[e]];
+            if (k >= 0)
+            {
+                if (k >= static_cast<int>(mark.size())) mark.resize(k + 1, -1);
+                mark[k] = c;
+            }
+        }
+        int k = 0;
+        while (k < static_cast<int>(mark.size()) && mark[k] == c) ++k;
+        colour[c] = k;
+        nColours = std::max(nColours, k + 1);
+    }
+    std::vector<std::vector<int>> cellsOf(nColours);
+    for (int c = 0; c < n; ++c) cellsOf[colour[c]].push_back(c);
+    C.colourStart.assign(1, 0);
+    std::vector<int> pos, sliceBase(1, 0), colP, faceP;
+    for (int k = 0; k < nColours; ++k)
+    {
+        const std::vector<int>& cells = cellsOf[k];
+        const int padded = ((static_cast<int>(cells.size()) + 31) / 32) * 32;
+        for (int b = 0; b < padded; b += 32)
+        {
+            int w = 0;
+            for (int l = 0; l < 32 && b + l < static_cast<int>(cells.size()); ++l)
+                w = std::max(w, rowStart[cells[b + l] + 1] - rowStart[cells[b + l]]);
+            const size_t base = colP.size();
+            colP.resize(base + 32 * static_cast<size_t>(w));
+            faceP.resize(base + 32 * static_cast<size_t>(w));
+            for (int l = 0; l < 32; ++l)
+            {
+                const bool real = b + l < static_cast<int>(cells.size());
+                const int cell = real ? cells[b + l] : -1;
+                pos.push_back(real ? posOf[cell] : -1);
+                const int len = real ? rowStart[cell + 1] - rowStart[cell] : 0;
+                for (int q = 0; q < w; ++q)
+                {
+                    const size_t e = base + 32 * static_cast<size_t>(q) + l;
+                    if (q < len)
+                    {
+                        colP[e] = posOf[col[rowStart[cell] + q]];
+                        faceP[e] = entFace[rowStart[cell] + q];
+                    }
+                    else
+                    {
+                        colP[e] = real ? posOf[cell] : 0;  // reads a value with coefficient zero
+                        faceP[e] = -1;
+                    }
+                }
+            }
+            if (colP.size() >= (1ull << 31)) fail(B2G_ERR_ARGUMENT, "b2g: the multicolour layout exceeds 2^31 entries.");
+            sliceBase.push_back(static_cast<int>(colP.size()));
+        }
+        C.colourStart.push_back(static_cast<int>(pos.size()));
+    }
+    C.nRows = static_cast<int>(pos.size());
+    C.nEnt = static_cast<long long>(colP.size());
+    C.pos.upload(pos.data(), pos.size(), s);
+    C.sliceBase.upload(sliceBase.data(), sliceBase.size(), s);
+    if (colP.empty())
+    {
+        colP.push_back(0);
+        faceP.push_back(-1);
+    }
+    C.col.upload(colP.data(), colP.size(), s);
+    C.face.upload(faceP.data(), faceP.size(), s);
+    B2G_CUDA(cudaStreamSynchronize(s));
+    C.nColours = nColours;
+}
+
 void buildStepMaps(Mesh& M, int i)
 {
     cudaStream_t s = M.stream;

@@ -47,6 +47,23 @@ struct GsSchedule
                                // (reset before each launch)
 };
 
+// A colouring of one level for the multicolour sweep of the FP32 V-cycle: no two cells of one colour
+// share a face, so a colour's cells are updated in parallel. Rows are the level's cells colour by
+// colour (ascending cell within a colour), each colour padded to whole 32-row slices, entries in
+// sliced ELL (entry q of the row in lane l of slice s at sliceBase[s] + 32*q + l); padding rows have
+// pos -1, padding entries face -1.
+struct Colouring
+{
+    int nColours = 0;
+    std::vector<int> colourStart;  // [nColours+1] rows (host)
+    int nRows = 0;
+    long long nEnt = 0;
+    DBuf<int> pos;                 // [nRows] position of each row's cell
+    DBuf<int> sliceBase;           // [nRows/32 + 1]
+    DBuf<int> col;                 // [nEnt] the other cell's position
+    DBuf<int> face;                // [nEnt] the face, -1 for padding
+};
+
 // One level's addressing and its derived layouts (built once per hierarchy).
 struct LevelAddr
 {
@@ -64,6 +81,7 @@ struct LevelAddr
     DBuf<int> col;          // [2*nFaces] the other cell
     DBuf<int> entFace;      // [2*nFaces] the face
     GsSchedule gs;
+    Colouring mc;           // built on first use (buildColouring)
 };
 
 // Level step i -> i+1 (GamgAgglomeration's restrictAddressing / faceRestrictAddressing /
@@ -102,6 +120,9 @@ struct Mesh
 void buildLevelLayouts(LevelAddr& L, cudaStream_t s);
 // The sweep order and Gauss-Seidel schedule of `L` (depths, parts, positions, chunks, codes).
 void buildGsSchedule(LevelAddr& L, cudaStream_t s);
+// The multicolour layout of `L` (greedy colouring in cell order; a structured hex level gets the two
+// colours of a checkerboard). Needs the level's schedule (positions).
+void buildColouring(LevelAddr& L, cudaStream_t s);
 // The position-ordered restriction and prolongation maps of step `i` (both levels scheduled).
 void buildStepMaps(Mesh& M, int i);
 // The whole agglomeration (faceAreaPairGamgAgglomeration) from device arrays.

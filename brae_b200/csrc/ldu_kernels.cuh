@@ -412,5 +412,18 @@ static __global__ void __launch_bounds__(32) serialNormFactor(Rows<double> A, co
     if (lane == 0) *out = __dadd_rn(s, 1e-20);
 }
 
+// One colour of a multicolour Gauss-Seidel sweep (FP32 V-cycle): rows [rowBegin, rowEnd) of the
+// level's colour-major sliced-ELL layout (hierarchy.cuh Colouring), one thread per row. No two rows
+// of a colour share a face, so every value a row reads is final for this colour.
+__global__ void mcSweep(int rowBegin, int rowEnd, const int* __restrict__ pos, const int* __restrict__ sliceBase,
+                        const int* __restrict__ col, const float* __restrict__ val, const float* __restrict__ diag,
+                        const float* __restrict__ b, float* __restrict__ psi);
+
+// The FP32 coefficients of the multicolour layout: per entry upper[face] (0 for padding), per row
+// the diagonal at its position.
+__global__ void mcValues(long long nEnt, int nRows, const int* __restrict__ face, const int* __restrict__ pos,
+                         const double* __restrict__ upper, const float* __restrict__ posDiag, float* __restrict__ val,
+                         float* __restrict__ diag);
+
 }  // namespace k
 }  // namespace b2g

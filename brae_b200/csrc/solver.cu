@@ -202,6 +202,44 @@ void zeroArray(long long n, T* x, cudaStream_t s)
 
 }  // namespace
 
+namespace k {
+
+__global__ void mcSweep(int rowBegin, int rowEnd, const int* __restrict__ pos, const int* __restrict__ sliceBase,
+                        const int* __restrict__ col, const float* __restrict__ val, const float* __restrict__ diag,
+                        const float* __restrict__ b, float* __restrict__ psi)
+{
+    for (int r = rowBegin + blockIdx.x * blockDim.x + threadIdx.x; r < rowEnd; r += gridDim.x * blockDim.x)
+    {
+        const int p = pos[r];
+        if (p < 0) continue;
+        const int sl = r >> 5;
+        const int base = sliceBase[sl];
+        const int w = (sliceBase[sl + 1] - base) >> 5;
+        float acc = b[p];
+        for (int q = 0, e = base + (r & 31); q < w; ++q, e += 32) acc = fmaf(-val[e], psi[col[e]], acc);
+        psi[p] = acc / diag[r];
+    }
+}
+
+__global__ void mcValues(long long nEnt, int nRows, const int* __restrict__ face, const int* __restrict__ pos,
+                         const double* __restrict__ upper, const float* __restrict__ posDiag, float* __restrict__ val,
+                         float* __restrict__ diag)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nEnt; i += stride)
+    {
+        const int f = face[i];
+        val[i] = f >= 0 ? static_cast<float>(upper[f]) : 0.0f;
+        if (i < nRows)
+        {
+            const int p = pos[i];
+            diag[i] = p >= 0 ? posDiag[p] : 1.0f;
+        }
+    }
+}
+
+}  // namespace k
+
 // The sweep's shared-memory ceiling, raised once per device and value type before the first launch
 // (outside any stream capture: the matrix constructor calls it).
 template <class T>
@@ -486,6 +524,11 @@ void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps,
     if (smoother != B2G_SMOOTHER_GAUSS_SEIDEL)
         fail(B2G_ERR_REFUSED, "b2g: the device smoother for this entry is GaussSeidel only so far; "
                               "symGaussSeidel, DIC and DICGaussSeidel are not built on the device yet.");
+    if (sizeof(T) == 4 && multicolour)
+    {
+        mcSmooth(level, reinterpret_cast<float*>(psiL), reinterpret_cast<const float*>(src), nSweeps);
+        return;
+    }
     const LevelAddr& L = mesh->lev[level];
     const GsSchedule& G = L.gs;
     const LevelCoef<T>& C = data<T>().coef[level];
@@ -521,6 +564,48 @@ void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps,
         B2G_LAUNCH_CHECK();
         launches += 1;
     }
+}
+
+// Gauss-Seidel sweeps of the FP32 V-cycle, colour by colour (B2G_PRECISION_FP32_PRECOND_MULTICOLOUR)
+void Matrix::mcSmooth(int level, float* psiL, const float* src, int nSweeps)
+{
+    const Colouring& C = mesh->lev[level].mc;
+    const LevelCoef<float>& F = v32.coef[level];
+    for (int sw = 0; sw < nSweeps; ++sw)
+        for (int k = 0; k < C.nColours; ++k)
+        {
+            const int b = C.colourStart[k], e = C.colourStart[k + 1];
+            if (e <= b) continue;
+            cudaEvent_t ev = level == 0 ? timedBegin(1) : nullptr;
+            k::mcSweep<<<std::min(ceilDiv(e - b, NT), 16 * DeviceInfo::get().numSMs), NT, 0, stream>>>(
+                b, e, C.pos.p, C.sliceBase.p, C.col.p, F.mcVal.p, F.mcDiag.p, src, psiL);
+            timedEnd(1, ev);
+            B2G_LAUNCH_CHECK();
+            ++launches;
+        }
+}
+
+// The multicolour layout of every level (on the mesh, once) and this matrix's FP32 values in it.
+void Matrix::ensureMulticolour()
+{
+    ensureFp32();
+    if (mcBuilt) return;
+    for (int i = 0; i <= nLevels(); ++i)
+    {
+        LevelAddr& L = mesh->lev[i];
+        buildColouring(L, stream);
+        LevelCoef<float>& F = v32.coef[i];
+        const Colouring& C = L.mc;
+        F.mcVal.alloc(std::max<long long>(C.nEnt, 1), stream);
+        F.mcDiag.alloc(std::max(C.nRows, 1), stream);
+        const long long m = std::max<long long>(C.nEnt, C.nRows);
+        if (m)
+            k::mcValues<<<std::min(ceilDiv(m, NT), 8192), NT, 0, stream>>>(C.nEnt, C.nRows, C.face.p, C.pos.p,
+                                                                           v64.coef[i].upper.p, F.gsDiag.p,
+                                                                           F.mcVal.p, F.mcDiag.p);
+        B2G_LAUNCH_CHECK();
+    }
+    mcBuilt = true;
 }
 
 template <class T>
@@ -745,8 +830,10 @@ void Matrix::vcycle(const b2g_controls& c, T* x, const T* src, T* Apsi, T* fcor,
 void Matrix::precondition(const b2g_controls& c, double* w, const double* r)
 {
     const int n0 = n(0);
-    if (c.precision == B2G_PRECISION_FP32_PRECOND)
+    multicolour = c.precision == B2G_PRECISION_FP32_PRECOND_MULTICOLOUR;
+    if (c.precision == B2G_PRECISION_FP32_PRECOND || multicolour)
     {
+        if (multicolour) ensureMulticolour();
         ensureFp32();
         castInto<float, double>(n0, r, r32.p, stream);
         zeroArray<float>(n0, w32.p, stream);
@@ -901,8 +988,9 @@ b2g_perf Matrix::pcg(const b2g_controls& c, b2g_solve_log* log)
         fail(B2G_ERR_REFUSED, "b2g GAMG: no coarse levels created, either matrix too small for GAMG or "
                               "nCellsInCoarsestLevel too large (GAMGSolver.C:333).");
     buildCoarse();
-    const bool flexible = c.precision == B2G_PRECISION_FP32_PRECOND;
+    const bool flexible = c.precision != B2G_PRECISION_FP64;
     if (flexible) ensureFp32();
+    if (c.precision == B2G_PRECISION_FP32_PRECOND_MULTICOLOUR) ensureMulticolour();
     kPcgStart<<<1, 1, 0, stream>>>(scal.p);
     B2G_LAUNCH_CHECK();
     do

@@ -25,6 +25,7 @@ struct LevelCoef
     DBuf<T> gsDiag; // [nCells (+pad)] diagonal by position
     DBuf<T> rowVal; // [2*nFaces] coefficient per CSR entry, rows by position
     DBuf<unsigned char> blob;  // the sweep's chunk blobs (gs_kernels.cuh) in T
+    DBuf<float> mcVal, mcDiag;  // FP32 only: the multicolour layout's coefficients (hierarchy.cuh Colouring)
 };
 
 // Everything a V-cycle in value type T touches.
@@ -73,6 +74,8 @@ struct Matrix
     int coarseLogCapacity = 0;
     IterationGraph pcgGraph, gamgGraph;
     bool serial = false;                      // B2G_REDUCTION_SERIAL for the current solve
+    bool multicolour = false;                 // the FP32 V-cycle sweeps colour by colour
+    bool mcBuilt = false;
     // timing (b2g_set_profiling): events around the finest level's Amul and Gauss-Seidel launches
     double ms[4] = {0, 0, 0, 0};              // finest Amul, finest Gauss-Seidel, other, whole solve
     long long counts[4] = {0, 0, 0, 0};       // launches of the same classes (whole solve: all)
@@ -92,6 +95,8 @@ struct Matrix
     void setFine(const double* diag, const double* upper, int memspace);
     void buildCoarse();                       // Galerkin matrices of every coarse level
     void ensureFp32();                        // float copies of every level
+    void ensureMulticolour();                 // the multicolour layout and its FP32 values
+    void mcSmooth(int level, float* psi, const float* source, int nSweeps);
     int nLevels() const { return mesh->nLevels(); }
     int n(int level) const { return mesh->lev[level].nCells; }
     size_t nAlloc(int level) const { return static_cast<size_t>(std::max(mesh->lev[level].gs.nAlloc, 1)); }

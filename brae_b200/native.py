@@ -145,7 +145,7 @@ def controls_default(**overrides) -> Controls:
         if k == "smoother" and isinstance(v, str):
             v = SMOOTHERS[v]
         if k == "precision" and isinstance(v, str):
-            v = {"fp64": 0, "fp32_precond": 1}[v]
+            v = {"fp64": 0, "fp32_precond": 1, "fp32_precond_multicolour": 2}[v]
         if k == "reduction" and isinstance(v, str):
             v = {"tree": 0, "serial": 1}[v]
         if k == "solver" and isinstance(v, str):

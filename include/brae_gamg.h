@@ -69,7 +69,13 @@ enum
 enum
 {
     B2G_PRECISION_FP64 = 0,        /* the parity form: everything in FP64 */
-    B2G_PRECISION_FP32_PRECOND = 1 /* FP64 outer PCG, FP32 V-cycle, flexible (Polak-Ribiere) beta */
+    B2G_PRECISION_FP32_PRECOND = 1, /* FP64 outer PCG, FP32 V-cycle, flexible (Polak-Ribiere) beta */
+    /* The same, with the FP32 V-cycle's Gauss-Seidel sweeps taken colour by colour: a greedy
+     * colouring of each level (two colours on a structured hex level) whose cells of one colour
+     * share no face, each colour one parallel update of its cells. The same GaussSeidel update in
+     * another cell order; bandwidth-bound where the sequential order is bound by the sweep's
+     * dependency chain. Built on first use (a host pass over every level's faces). */
+    B2G_PRECISION_FP32_PRECOND_MULTICOLOUR = 2
 };
 
 /* How sums and dot products are reduced. TREE is a fixed-shape parallel tree (deterministic, fast);

@@ -119,6 +119,26 @@ def test_batch_fp32_form(b2g, oracle):
         assert abs(single.nIterations - perf.nIterations) <= 1
 
 
+def test_batch_fp32_multicolour_form(b2g, oracle):
+    built, meshes, mats = _build(b2g, BOXES)
+    tol = 1e-9
+    ctl = b2g.controls_default(tolerance=tol, relTol=0.0, precision="fp32_precond_multicolour")
+    batch = b2g.Batch(mats)
+    for _ in range(2):  # the second solve runs on the prepared layouts and the captured graph
+        psis = [np.zeros(c.n_cells) for c in built]
+        perfs = batch.solve([c.source for c in built], psis, ctl)
+        for c, m, psi, perf in zip(built, meshes, psis, perfs):
+            assert perf.finalResidual < tol
+            want = _oracle(oracle, c, tol, 0.0, {})
+            assert 1 <= perf.nIterations <= want["perf"][2] + 2
+            assert np.abs(psi - want["psi"]).max() / np.abs(want["psi"]).max() < 1e-6
+    # the same sweeps as the single solve's multicolour form: the same iteration counts (+-1)
+    for c, m, perf in zip(built, meshes, perfs):
+        x = np.zeros(c.n_cells)
+        single = b2g.pcg_gamg_solve(m, c.diag, c.coef, c.source, x, ctl)[0]
+        assert abs(single.nIterations - perf.nIterations) <= 1
+
+
 def test_batch_device_fields_and_refusals(b2g, oracle):
     built, meshes, mats = _build(b2g, BOXES[:3])
     batch = b2g.Batch(mats)

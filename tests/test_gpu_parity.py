@@ -257,6 +257,27 @@ def test_fp32_preconditioned_form(b2g, oracle):
     assert err < 1e-6
 
 
+@pytest.mark.parametrize("kw", [dict(nx=32, ny=30, nz=28, lengths=(2.0, 1.0, 1.0), grading_y=20.0),
+                                dict(nx=24, ny=20, nz=22, lengths=(2.0, 1.0, 1.0), grading_y=20.0, two_phase=True),
+                                dict(nx=40, ny=40, nz=40)], ids=["graded", "two_phase", "cube40"])
+def test_fp32_multicolour_form(b2g, oracle, kw):
+    # the FP32 V-cycle sweeping colour by colour: the same GaussSeidel update in another cell order,
+    # so not bit-comparable; it must reach the tolerance in at most the FP64 iteration count + 2, with
+    # the FP64 oracle's field
+    c = cases.box_case(**kw)
+    mesh = b2g.Mesh(c.lower, c.upper, c.Sf, c.magSf, c.n_cells, 10, True)
+    agg = oracle.agglomerate(c.lower, c.upper, c.Sf, c.magSf, c.n_cells, 10, True)
+    want = oracle.pcg_gamg_solve(agg, c.diag, c.coef, c.source, np.zeros(c.n_cells), 1e-9, 0.0)
+    for _ in range(2):  # the second solve runs on the layout built by the first
+        psi = np.zeros(c.n_cells)
+        ctl = b2g.controls_default(tolerance=1e-9, relTol=0.0, precision="fp32_precond_multicolour")
+        perf, hist, _ = b2g.pcg_gamg_solve(mesh, c.diag, c.coef, c.source, psi, ctl)
+        assert perf.finalResidual < 1e-9
+        assert 1 <= perf.nIterations <= want["perf"][2] + 2
+        err = np.abs(psi - want["psi"]).max() / np.abs(want["psi"]).max()
+        assert err < 1e-6
+
+
 def test_refusals(b2g):
     # three cells and no faces: no pass reduces the count, so no coarse level exists and the solve
     # refuses by name, as GAMGSolver.C:333 does
