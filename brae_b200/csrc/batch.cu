@@ -216,6 +216,41 @@ __global__ void __launch_bounds__(BT) bMcSweep(const int4* __restrict__ tiles, c
     }
 }
 
+// every sweep of one small case's multicolour smoothing in one block (block i: descriptor cases[i])
+__global__ void __launch_bounds__(1024) bMcSmoothSmall(const int* __restrict__ cases,
+                                                       const SegLevel<float>* __restrict__ segs, int rpsi, int rsrc,
+                                                       int nSweeps, const int* __restrict__ active)
+{
+    const SegLevel<float>& s = segs[cases[blockIdx.x]];
+    if (inactive(s, active)) return;
+    const int* __restrict__ pos = s.mcPos;
+    const int* __restrict__ slice = s.mcSlice;
+    const int* __restrict__ col = s.mcCol;
+    const float* __restrict__ val = s.mcVal;
+    const float* __restrict__ diag = s.mcDiag;
+    const int* __restrict__ cs = s.mcColourStart;
+    const int nColours = s.mcColours;
+    const float* __restrict__ b = s.v[rsrc];
+    float* __restrict__ psi = s.v[rpsi];
+    for (int sw = 0; sw < nSweeps; ++sw)
+        for (int k = 0; k < nColours; ++k)
+        {
+            const int end = cs[k + 1];
+            for (int r = cs[k] + threadIdx.x; r < end; r += blockDim.x)
+            {
+                const int p = pos[r];
+                if (p < 0) continue;
+                const int sl = r >> 5;
+                const int base = slice[sl];
+                const int w = (slice[sl + 1] - base) >> 5;
+                float acc = b[p];
+                for (int q = 0, e = base + (r & 31); q < w; ++q, e += 32) acc = fmaf(-val[e], psi[col[e]], acc);
+                psi[p] = acc / diag[r];
+            }
+            __syncthreads();
+        }
+}
+
 // ---------------------------------------------------------------------------------------------
 // scale (GAMG:386-407), per case
 // ---------------------------------------------------------------------------------------------
@@ -965,13 +1000,25 @@ void Batch::prepareMulticolour()
             f.mcCol = C.col.p;
             f.mcVal = cases[c]->v32.coef[lv].mcVal.p;
             f.mcDiag = cases[c]->v32.coef[lv].mcDiag.p;
+            f.mcColourStart = C.colourStartD.p;
+            f.mcColours = C.nColours;
+            f.mcRows = C.nRows;
         }
     segF.upload(hostF.data(), hostF.size(), stream);
     for (int lv = 0; lv <= maxLevels; ++lv)
     {
+        // small cases: one block each sweeps the whole level; large ones: a launch per colour
+        std::vector<int> small;
+        auto isSmall = [&](int c) { return cases[c]->mesh->lev[lv].mc.nRows <= k::kMcSmallRows; };
         int nCol = 0;
         for (int c = 0; c < K; ++c)
-            if (nLevelsOf[c] >= lv + 1) nCol = std::max(nCol, cases[c]->mesh->lev[lv].mc.nColours);
+        {
+            if (nLevelsOf[c] < lv + 1) continue;
+            if (isSmall(c)) small.push_back(segOfCase[c][lv]);
+            else nCol = std::max(nCol, cases[c]->mesh->lev[lv].mc.nColours);
+        }
+        lev[lv].nMcSmall = static_cast<int>(small.size());
+        if (!small.empty()) lev[lv].mcSmall.upload(small.data(), small.size(), stream);
         lev[lv].mc.clear();
         lev[lv].mc.resize(nCol);
         for (int k = 0; k < nCol; ++k)
@@ -979,7 +1026,7 @@ void Batch::prepareMulticolour()
             std::vector<int4> tiles;
             for (int c = 0; c < K; ++c)
             {
-                if (nLevelsOf[c] < lv + 1) continue;
+                if (nLevelsOf[c] < lv + 1 || isSmall(c)) continue;
                 const Colouring& C = cases[c]->mesh->lev[lv].mc;
                 if (k >= C.nColours) continue;
                 const int sg = segOfCase[c][lv];
@@ -1013,6 +1060,11 @@ void Batch::smooth(int lv, int nSweeps)
     {
         const int rpsi = lv == 0 ? V_W : V_CORR;
         const int rsrc = lv == 0 ? V_R : V_SRC;
+        if (B.nMcSmall)
+        {
+            bMcSmoothSmall<<<B.nMcSmall, 1024, 0, stream>>>(B.mcSmall.p, segF.p, rpsi, rsrc, nSweeps, active.p);
+            ++launches;
+        }
         for (int sw = 0; sw < nSweeps; ++sw)
             for (const TileList& L : B.mc)
             {

@@ -60,6 +60,9 @@ struct SegLevel
     const int* mcCol;
     const float* mcVal;
     const float* mcDiag;
+    const int* mcColourStart;  // [mcColours+1] rows of each colour
+    int mcColours;
+    int mcRows;
 };
 
 // Tiles of cells of some cases on one level: {descriptor, begin, end, the case's index in the list};
@@ -94,7 +97,9 @@ struct BatchLevel
     int block = 0;
     size_t smem64 = 0, smem32 = 0;
     DBuf<unsigned> progress;
-    std::vector<TileList> mc;  // per colour: the swept cases' rows of that colour (multicolour form)
+    std::vector<TileList> mc;  // per colour: the swept large cases' rows of that colour (multicolour form)
+    DBuf<int> mcSmall;         // the swept small cases (descriptors): one block each sweeps them whole
+    int nMcSmall = 0;
 };
 
 struct Batch

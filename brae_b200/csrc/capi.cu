@@ -581,6 +581,18 @@ b2g_status b2g_level_schedule(const b2g_mesh* mesh, int level, int* partChunkSta
     });
 }
 
+b2g_status b2g_level_colouring(const b2g_mesh* mesh, int level, int* nColours, int* colourStart)
+{
+    return guarded([&] {
+        need(mesh && nColours, "b2g_level_colouring: null argument");
+        need(level >= 0 && level <= mesh->m.nLevels(), "b2g_level_colouring: no such level");
+        const b2g::Colouring& C = mesh->m.lev[level].mc;
+        *nColours = C.nColours;
+        if (colourStart)
+            for (int k = 0; k <= C.nColours; ++k) colourStart[k] = C.colourStart[k];
+    });
+}
+
 b2g_status b2g_level_scale(b2g_matrix* m, int level, double* field, double* Acf, const double* source)
 {
     return guarded([&] {

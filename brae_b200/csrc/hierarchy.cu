@@ -1315,8 +1315,14 @@ void buildColouring(LevelAddr& L, cudaStream_t s)
         colour[c] = k;
         nColours = std::max(nColours, k + 1);
     }
+    // a colour's rows in position order: a sweep then reads b and writes psi nearly in sequence, and
+    // the neighbours it reads sit in the adjacent depth groups
     std::vector<std::vector<int>> cellsOf(nColours);
-    for (int c = 0; c < n; ++c) cellsOf[colour[c]].push_back(c);
+    {
+        std::vector<int> byPos(n);
+        for (int c = 0; c < n; ++c) byPos[posOf[c]] = c;
+        for (int i = 0; i < n; ++i) cellsOf[colour[byPos[i]]].push_back(byPos[i]);
+    }
     C.colourStart.assign(1, 0);
     std::vector<int> pos, sliceBase(1, 0), colP, faceP;
     for (int k = 0; k < nColours; ++k)
@@ -1360,6 +1366,7 @@ void buildColouring(LevelAddr& L, cudaStream_t s)
     C.nRows = static_cast<int>(pos.size());
     C.nEnt = static_cast<long long>(colP.size());
     C.pos.upload(pos.data(), pos.size(), s);
+    C.colourStartD.upload(C.colourStart.data(), C.colourStart.size(), s);
     C.sliceBase.upload(sliceBase.data(), sliceBase.size(), s);
     if (colP.empty())
     {

@@ -51,11 +51,12 @@ struct GsSchedule
 // share a face, so a colour's cells are updated in parallel. Rows are the level's cells colour by
 // colour (ascending cell within a colour), each colour padded to whole 32-row slices, entries in
 // sliced ELL (entry q of the row in lane l of slice s at sliceBase[s] + 32*q + l); padding rows have
-// pos -1, padding entries face -1.
+// pos -1, padding entries face -1. Within a colour, rows follow the level's position order.
 struct Colouring
 {
     int nColours = 0;
     std::vector<int> colourStart;  // [nColours+1] rows (host)
+    DBuf<int> colourStartD;        // the same on the device
     int nRows = 0;
     long long nEnt = 0;
     DBuf<int> pos;                 // [nRows] position of each row's cell

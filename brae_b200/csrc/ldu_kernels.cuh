@@ -419,6 +419,14 @@ __global__ void mcSweep(int rowBegin, int rowEnd, const int* __restrict__ pos, c
                         const int* __restrict__ col, const float* __restrict__ val, const float* __restrict__ diag,
                         const float* __restrict__ b, float* __restrict__ psi);
 
+// Every sweep of a small level's multicolour smoothing in ONE block: the colours one after another,
+// a block barrier between them (levels of at most kMcSmallRows rows).
+constexpr int kMcSmallRows = 16384;
+__global__ void mcSmoothSmall(int nColours, const int* __restrict__ colourStart, int nSweeps,
+                              const int* __restrict__ pos, const int* __restrict__ sliceBase,
+                              const int* __restrict__ col, const float* __restrict__ val,
+                              const float* __restrict__ diag, const float* __restrict__ b, float* __restrict__ psi);
+
 // The FP32 coefficients of the multicolour layout: per entry upper[face] (0 for padding), per row
 // the diagonal at its position.
 __global__ void mcValues(long long nEnt, int nRows, const int* __restrict__ face, const int* __restrict__ pos,

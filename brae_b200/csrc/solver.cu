@@ -204,21 +204,42 @@ void zeroArray(long long n, T* x, cudaStream_t s)
 
 namespace k {
 
+__device__ __forceinline__ void mcRow(int r, const int* __restrict__ pos, const int* __restrict__ sliceBase,
+                                      const int* __restrict__ col, const float* __restrict__ val,
+                                      const float* __restrict__ diag, const float* __restrict__ b,
+                                      float* __restrict__ psi)
+{
+    const int p = pos[r];
+    if (p < 0) return;
+    const int sl = r >> 5;
+    const int base = sliceBase[sl];
+    const int w = (sliceBase[sl + 1] - base) >> 5;
+    float acc = b[p];
+    for (int q = 0, e = base + (r & 31); q < w; ++q, e += 32) acc = fmaf(-val[e], psi[col[e]], acc);
+    psi[p] = acc / diag[r];
+}
+
 __global__ void mcSweep(int rowBegin, int rowEnd, const int* __restrict__ pos, const int* __restrict__ sliceBase,
                         const int* __restrict__ col, const float* __restrict__ val, const float* __restrict__ diag,
                         const float* __restrict__ b, float* __restrict__ psi)
 {
     for (int r = rowBegin + blockIdx.x * blockDim.x + threadIdx.x; r < rowEnd; r += gridDim.x * blockDim.x)
-    {
-        const int p = pos[r];
-        if (p < 0) continue;
-        const int sl = r >> 5;
-        const int base = sliceBase[sl];
-        const int w = (sliceBase[sl + 1] - base) >> 5;
-        float acc = b[p];
-        for (int q = 0, e = base + (r & 31); q < w; ++q, e += 32) acc = fmaf(-val[e], psi[col[e]], acc);
-        psi[p] = acc / diag[r];
-    }
+        mcRow(r, pos, sliceBase, col, val, diag, b, psi);
+}
+
+__global__ void __launch_bounds__(1024) mcSmoothSmall(int nColours, const int* __restrict__ colourStart, int nSweeps,
+                                                      const int* __restrict__ pos, const int* __restrict__ sliceBase,
+                                                      const int* __restrict__ col, const float* __restrict__ val,
+                                                      const float* __restrict__ diag, const float* __restrict__ b,
+                                                      float* __restrict__ psi)
+{
+    for (int sw = 0; sw < nSweeps; ++sw)
+        for (int k = 0; k < nColours; ++k)
+        {
+            const int e = colourStart[k + 1];
+            for (int r = colourStart[k] + threadIdx.x; r < e; r += blockDim.x) mcRow(r, pos, sliceBase, col, val, diag, b, psi);
+            __syncthreads();
+        }
 }
 
 __global__ void mcValues(long long nEnt, int nRows, const int* __restrict__ face, const int* __restrict__ pos,
@@ -571,6 +592,16 @@ void Matrix::mcSmooth(int level, float* psiL, const float* src, int nSweeps)
 {
     const Colouring& C = mesh->lev[level].mc;
     const LevelCoef<float>& F = v32.coef[level];
+    if (C.nRows <= k::kMcSmallRows)
+    {
+        cudaEvent_t ev = level == 0 ? timedBegin(1) : nullptr;
+        k::mcSmoothSmall<<<1, 1024, 0, stream>>>(C.nColours, C.colourStartD.p, nSweeps, C.pos.p, C.sliceBase.p,
+                                                  C.col.p, F.mcVal.p, F.mcDiag.p, src, psiL);
+        timedEnd(1, ev);
+        B2G_LAUNCH_CHECK();
+        ++launches;
+        return;
+    }
     for (int sw = 0; sw < nSweeps; ++sw)
         for (int k = 0; k < C.nColours; ++k)
         {

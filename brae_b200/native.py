@@ -95,6 +95,7 @@ def _load():
         "b2g_level_pcg_dic": (ip, [vp, ip, vp, vp, dp, dp, C.POINTER(_Perf)]),
         "b2g_level_pcg_dic_static": (ip, [vp, ip, vp, vp, dp, dp, C.POINTER(_Perf)]),
         "b2g_level_schedule": (ip, [vp, ip, vp, vp]),
+        "b2g_level_colouring": (ip, [vp, ip, C.POINTER(C.c_int), vp]),
         "b2g_precondition": (ip, [vp, C.POINTER(Controls), vp, vp, C.POINTER(_Log)]),
         "b2g_matrix_pcg_solve": (ip, [vp, vp, vp, C.POINTER(Controls), ip, C.POINTER(_Perf),
                                       C.POINTER(_Log)]),
@@ -127,7 +128,7 @@ EXPORTED = [
     "b2g_level_amul", "b2g_level_smooth", "b2g_level_scale", "b2g_step_restrict",
     "b2g_step_prolong", "b2g_level_norm_factor", "b2g_level_pcg_dic", "b2g_precondition",
     "b2g_matrix_pcg_solve", "b2g_matrix_timings", "b2g_level_smooth_trace", "b2g_level_pcg_dic_static",
-    "b2g_level_schedule", "b2g_server_create", "b2g_server_destroy", "b2g_server_add_case",
+    "b2g_level_schedule", "b2g_level_colouring", "b2g_server_create", "b2g_server_destroy", "b2g_server_add_case",
     "b2g_server_submit", "b2g_server_wait", "b2g_server_case_bytes", "b2g_batch_create", "b2g_batch_solve",
     "b2g_batch_launches", "b2g_batch_destroy",
 ]
@@ -247,6 +248,14 @@ class Mesh:
         rec = np.empty((n_chunks, 12), np.int32)
         _check(lib.b2g_level_schedule(self.handle, level, pcs.ctypes.data_as(C.c_void_p), rec.ctypes.data_as(C.c_void_p)))
         return pcs, rec
+
+    def colouring(self, level: int):
+        """The level's multicolour row ranges (empty before the multicolour form's first solve)."""
+        n = C.c_int()
+        _check(lib.b2g_level_colouring(self.handle, level, C.byref(n), None))
+        starts = np.zeros(n.value + 1, np.int32)
+        _check(lib.b2g_level_colouring(self.handle, level, C.byref(n), _ptr(starts)))
+        return starts
 
     def step(self, i: int) -> dict:
         nc, nf = self.level_size(i)

@@ -351,6 +351,11 @@ B2G_API b2g_status b2g_server_wait(b2g_server* server, long long ticket, b2g_per
 /* The HBM footprint a case was admitted with (bytes). */
 B2G_API b2g_status b2g_server_case_bytes(b2g_server* server, int caseId, unsigned long long* bytes);
 
+/* Diagnostic: the multicolour layout of `level` (B2G_PRECISION_FP32_PRECOND_MULTICOLOUR; built on
+ * that form's first solve on the mesh): *nColours (0 if not built yet) and, if colourStart is not
+ * NULL, the colours' row ranges colourStart[nColours + 1] (HOST; rows padded to 32 per colour). */
+B2G_API b2g_status b2g_level_colouring(const b2g_mesh* mesh, int level, int* nColours, int* colourStart);
+
 /* Library version string. */
 B2G_API const char* b2g_version(void);
 
