@@ -291,6 +291,8 @@ def run_ours(args, world, rank, local):
     mc_ms, mc_cnt = A2.timings()
     b2g.set_profiling(False)
     n_colours = len(mesh.colouring(0)) - 1
+    tuned = [dict(level=l, cells=mesh.level_size(l)[0], colours=len(mesh.colouring(l)) - 1, **mesh.sweep_shape(l))
+             for l in range(mesh.n_levels + 1)]
     mc_sweeps = mc_cnt[1] / max(n_colours, 1)
     mc_sweep_ms = mc_ms[1] / max(mc_sweeps, 1)
     mc_bytes = 20 * case.n_cells + 16 * case.n_faces  # FP32: diag, b, psi read + write, row position; two (column, coefficient) entries per face
@@ -350,6 +352,7 @@ def run_ours(args, world, rank, local):
                 "perf": forms["fp32_precond_multicolour"]["perf"],
                 "field_rel_err_vs_fp64": field_err_mc,
                 "note": "FP32 V-cycle with Gauss-Seidel sweeps colour by colour (B2G_PRECISION_FP32_PRECOND_MULTICOLOUR)",
+                "autotuned_sweep_shapes": tuned,
                 "finest_sweep": {"colours": n_colours, "ms": mc_sweep_ms, "algorithmic_bytes": mc_bytes,
                                  "achieved_gbs": mc_gbs, "frac_of_measured_hbm": mc_gbs / measured_peaks()[0]},
             },

@@ -1009,7 +1009,7 @@ void Batch::prepareMulticolour()
     {
         // small cases: one block each sweeps the whole level; large ones: a launch per colour
         std::vector<int> small;
-        auto isSmall = [&](int c) { return cases[c]->mesh->lev[lv].mc.nRows <= k::kMcSmallRows; };
+        auto isSmall = [&](int c) { return cases[c]->mesh->lev[lv].mc.fused; };
         int nCol = 0;
         for (int c = 0; c < K; ++c)
         {

@@ -63,6 +63,12 @@ struct Colouring
     DBuf<int> sliceBase;           // [nRows/32 + 1]
     DBuf<int> col;                 // [nEnt] the other cell's position
     DBuf<int> face;                // [nEnt] the face, -1 for padding
+    // the sweep's launch shape, chosen by measurement (Matrix::tuneMulticolour): one block sweeping
+    // the whole level, or one launch per colour of `block` threads per block
+    bool tuned = false;
+    bool fused = false;
+    int block = 256;
+    float msPerSweep = 0.f;
 };
 
 // One level's addressing and its derived layouts (built once per hierarchy).

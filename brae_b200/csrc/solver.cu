@@ -591,10 +591,18 @@ void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps,
 void Matrix::mcSmooth(int level, float* psiL, const float* src, int nSweeps)
 {
     const Colouring& C = mesh->lev[level].mc;
+    mcLaunch(level, C.fused, C.block, psiL, src, nSweeps, true);
+}
+
+// nSweeps multicolour sweeps of one level in a given shape: one block for the whole level, or one
+// launch per colour of `block` threads per block
+void Matrix::mcLaunch(int level, bool fused, int block, float* psiL, const float* src, int nSweeps, bool timed)
+{
+    const Colouring& C = mesh->lev[level].mc;
     const LevelCoef<float>& F = v32.coef[level];
-    if (C.nRows <= k::kMcSmallRows)
+    if (fused)
     {
-        cudaEvent_t ev = level == 0 ? timedBegin(1) : nullptr;
+        cudaEvent_t ev = timed && level == 0 ? timedBegin(1) : nullptr;
         k::mcSmoothSmall<<<1, 1024, 0, stream>>>(C.nColours, C.colourStartD.p, nSweeps, C.pos.p, C.sliceBase.p,
                                                   C.col.p, F.mcVal.p, F.mcDiag.p, src, psiL);
         timedEnd(1, ev);
@@ -607,13 +615,62 @@ void Matrix::mcSmooth(int level, float* psiL, const float* src, int nSweeps)
         {
             const int b = C.colourStart[k], e = C.colourStart[k + 1];
             if (e <= b) continue;
-            cudaEvent_t ev = level == 0 ? timedBegin(1) : nullptr;
-            k::mcSweep<<<std::min(ceilDiv(e - b, NT), 16 * DeviceInfo::get().numSMs), NT, 0, stream>>>(
+            cudaEvent_t ev = timed && level == 0 ? timedBegin(1) : nullptr;
+            k::mcSweep<<<std::min(ceilDiv(e - b, block), 16 * DeviceInfo::get().numSMs), block, 0, stream>>>(
                 b, e, C.pos.p, C.sliceBase.p, C.col.p, F.mcVal.p, F.mcDiag.p, src, psiL);
             timedEnd(1, ev);
             B2G_LAUNCH_CHECK();
             ++launches;
         }
+}
+
+// The autotuner of the multicolour sweep: times every candidate launch shape on the level's own
+// layout (one block sweeping the whole level when it has at most kMcSmallRows rows; one launch per
+// colour at 128, 256 or 512 threads per block) and keeps the fastest. Runs once per mesh level, on
+// this matrix's FP32 values and scratch vectors, outside any capture.
+void Matrix::tuneMulticolour(int level)
+{
+    Colouring& C = mesh->lev[level].mc;
+    if (C.tuned) return;
+    float* x = level == 0 ? w32.p : v32.corr[level - 1].p;
+    float* b = level == 0 ? r32.p : v32.src[level - 1].p;
+    zeroArray<float>(static_cast<long long>(nAlloc(level)), x, stream);
+    castInto<float, double>(n(level), v64.coef[level].gsDiag.p, b, stream);
+    struct Shape
+    {
+        bool fused;
+        int block;
+    };
+    std::vector<Shape> shapes;
+    if (C.nRows <= k::kMcSmallRows) shapes.push_back({true, 1024});
+    for (int bl : {128, 256, 512}) shapes.push_back({false, bl});
+    cudaEvent_t e0, e1;
+    B2G_CUDA(cudaEventCreate(&e0));
+    B2G_CUDA(cudaEventCreate(&e1));
+    float best = 0.f;
+    const long long l0 = launches;
+    for (const Shape& sh : shapes)
+    {
+        mcLaunch(level, sh.fused, sh.block, x, b, 1, false);  // warm
+        B2G_CUDA(cudaEventRecord(e0, stream));
+        mcLaunch(level, sh.fused, sh.block, x, b, 3, false);
+        B2G_CUDA(cudaEventRecord(e1, stream));
+        B2G_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        B2G_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        ms /= 3.f;
+        if (!C.tuned || ms < best)
+        {
+            best = ms;
+            C.fused = sh.fused;
+            C.block = sh.block;
+            C.tuned = true;
+        }
+    }
+    launches = l0;
+    C.msPerSweep = best;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
 }
 
 // The multicolour layout of every level (on the mesh, once) and this matrix's FP32 values in it.
@@ -635,6 +692,7 @@ void Matrix::ensureMulticolour()
                                                                            v64.coef[i].upper.p, F.gsDiag.p,
                                                                            F.mcVal.p, F.mcDiag.p);
         B2G_LAUNCH_CHECK();
+        tuneMulticolour(i);
     }
     mcBuilt = true;
 }

@@ -97,6 +97,8 @@ struct Matrix
     void ensureFp32();                        // float copies of every level
     void ensureMulticolour();                 // the multicolour layout and its FP32 values
     void mcSmooth(int level, float* psi, const float* source, int nSweeps);
+    void mcLaunch(int level, bool fused, int block, float* psi, const float* source, int nSweeps, bool timed);
+    void tuneMulticolour(int level);
     int nLevels() const { return mesh->nLevels(); }
     int n(int level) const { return mesh->lev[level].nCells; }
     size_t nAlloc(int level) const { return static_cast<size_t>(std::max(mesh->lev[level].gs.nAlloc, 1)); }

@@ -96,6 +96,7 @@ def _load():
         "b2g_level_pcg_dic_static": (ip, [vp, ip, vp, vp, dp, dp, C.POINTER(_Perf)]),
         "b2g_level_schedule": (ip, [vp, ip, vp, vp]),
         "b2g_level_colouring": (ip, [vp, ip, C.POINTER(C.c_int), vp]),
+        "b2g_level_sweep_shape": (ip, [vp, ip, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float)]),
         "b2g_precondition": (ip, [vp, C.POINTER(Controls), vp, vp, C.POINTER(_Log)]),
         "b2g_matrix_pcg_solve": (ip, [vp, vp, vp, C.POINTER(Controls), ip, C.POINTER(_Perf),
                                       C.POINTER(_Log)]),
@@ -128,7 +129,7 @@ EXPORTED = [
     "b2g_level_amul", "b2g_level_smooth", "b2g_level_scale", "b2g_step_restrict",
     "b2g_step_prolong", "b2g_level_norm_factor", "b2g_level_pcg_dic", "b2g_precondition",
     "b2g_matrix_pcg_solve", "b2g_matrix_timings", "b2g_level_smooth_trace", "b2g_level_pcg_dic_static",
-    "b2g_level_schedule", "b2g_level_colouring", "b2g_server_create", "b2g_server_destroy", "b2g_server_add_case",
+    "b2g_level_schedule", "b2g_level_colouring", "b2g_level_sweep_shape", "b2g_server_create", "b2g_server_destroy", "b2g_server_add_case",
     "b2g_server_submit", "b2g_server_wait", "b2g_server_case_bytes", "b2g_batch_create", "b2g_batch_solve",
     "b2g_batch_launches", "b2g_batch_destroy",
 ]
@@ -256,6 +257,12 @@ class Mesh:
         starts = np.zeros(n.value + 1, np.int32)
         _check(lib.b2g_level_colouring(self.handle, level, C.byref(n), _ptr(starts)))
         return starts
+
+    def sweep_shape(self, level: int) -> dict:
+        """The autotuner's multicolour sweep shape for `level` (zeros before the form's first solve)."""
+        one, thr, ms = C.c_int(), C.c_int(), C.c_float()
+        _check(lib.b2g_level_sweep_shape(self.handle, level, C.byref(one), C.byref(thr), C.byref(ms)))
+        return {"one_block": bool(one.value), "threads": thr.value, "ms_per_sweep": ms.value}
 
     def step(self, i: int) -> dict:
         nc, nf = self.level_size(i)

@@ -276,6 +276,11 @@ def test_fp32_multicolour_form(b2g, oracle, kw):
         assert 1 <= perf.nIterations <= want["perf"][2] + 2
         err = np.abs(psi - want["psi"]).max() / np.abs(want["psi"]).max()
         assert err < 1e-6
+    # every level's sweep shape was chosen by the autotuner's measurements
+    for level in range(mesh.n_levels + 1):
+        shape = mesh.sweep_shape(level)
+        assert shape["threads"] in (128, 256, 512, 1024) and shape["ms_per_sweep"] > 0.0
+        assert len(mesh.colouring(level)) >= 2
 
 
 def test_refusals(b2g):
