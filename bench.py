@@ -37,7 +37,14 @@ METRIC = "20M-cell p-solve s, FP32-precond vs FP64 at equal residual; served p50
 TOL, REL_TOL, MAX_ITER = 1e-6, 0.05, 1000
 
 
-def dist_setup():
+BACKEND = "nccl"
+
+
+def dist_setup(backend: str = "nccl"):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE); `gloo` runs the same plumbing
+    on CPU processes."""
+    global BACKEND
+    BACKEND = backend
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -46,19 +53,44 @@ def dist_setup():
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     return world, rank, local
 
 
-def barrier_max(x: float, world: int) -> float:
+def _reduce(x: float, world: int, op) -> float:
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if BACKEND == "nccl" else "cpu")
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def barrier_max(x: float, world: int) -> float:
+    """The max over ranks (every multi-GPU time is the slowest rank's)."""
+    import torch.distributed as dist
+    return _reduce(x, world, dist.ReduceOp.MAX if world > 1 else None)
+
+
+def sum_over_ranks(x: float, world: int) -> float:
+    import torch.distributed as dist
+    return _reduce(x, world, dist.ReduceOp.SUM if world > 1 else None)
+
+
+def cases_for_rank(cells, rank: int, world: int):
+    """The batched workload sharded by case (no collective on the data path): the largest case first to
+    the rank with the fewest cells so far. Returns this rank's case indices, ascending."""
+    load = [0] * world
+    mine = []
+    for i in sorted(range(len(cells)), key=lambda i: (-cells[i], i)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        load[r] += cells[i]
+        if r == rank:
+            mine.append(i)
+    return sorted(mine)
 
 
 def barrier(world: int):
@@ -323,8 +355,8 @@ def run_ours(args, world, rank, local):
                "field_rel_diff_vs_gpu": float(np.abs(cpsi - psi64).max() / np.abs(cpsi).max())}
 
     batched = None
-    if not args.no_batched and world == 1:
-        batched = batched_leg(args, b2g, local)
+    if not args.no_batched:
+        batched = batched_leg(args, b2g, local, world, rank)
     served = None
     if not args.no_serve and world == 1:
         served = serve_stream(args, b2g, local)
@@ -378,17 +410,21 @@ def run_ours(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
-def batched_leg(args, b2g, local):
+def batched_leg(args, b2g, local, world=1, rank=0):
     """The batched form: 256 cases (cell counts log-uniform in 4,096..1,048,576, aspect ratios
     uniform[1,8], grading uniform[1,20], seed 1), FP32-preconditioned PCG to tolerance 1e-6 (relTol 0)
     from psi = 0, all solved by one b2g_batch; beside it the same cases solved one after another
-    through the single-case path. Fields are resident on the device in both."""
+    through the single-case path. Fields are resident on the device in both. With N ranks the cases are
+    sharded by case (cases_for_rank), each rank solving its share as one batch; times are the slowest
+    rank's."""
     import torch
 
     from brae_b200 import cases
     dev = torch.device("cuda", local)
     t0 = time.perf_counter()
-    dims = cases.mixed_batch_sizes(args.batch_cases)
+    all_dims = cases.mixed_batch_sizes(args.batch_cases)
+    mine = cases_for_rank([d["n"][0] * d["n"][1] * d["n"][2] for d in all_dims], rank, world)
+    dims = [all_dims[i] for i in mine]
     built, meshes, mats = [], [], []
     td = lambda a, dt=torch.float64: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)
     for d in dims:
@@ -415,6 +451,7 @@ def batched_leg(args, b2g, local):
     ts = []
     for _ in range(max(1, args.steps)):
         psi_all.zero_()
+        barrier(world)
         torch.cuda.synchronize()
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a0.record(stream)
@@ -422,7 +459,7 @@ def batched_leg(args, b2g, local):
         a1.record(stream)
         torch.cuda.synchronize()
         ts.append(a0.elapsed_time(a1) / 1e3)
-    batch_s = float(np.median(ts))
+    batch_s = barrier_max(float(np.median(ts)), world)
     launches = batch.launches()
     x_batch = psi_all.cpu().numpy()
     # the multicolour FP32 form of the same batch
@@ -434,6 +471,7 @@ def batched_leg(args, b2g, local):
     ts_mc = []
     for _ in range(max(1, args.steps)):
         psi_all.zero_()
+        barrier(world)
         torch.cuda.synchronize()
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a0.record(stream)
@@ -441,7 +479,7 @@ def batched_leg(args, b2g, local):
         a1.record(stream)
         torch.cuda.synchronize()
         ts_mc.append(a0.elapsed_time(a1) / 1e3)
-    batch_mc_s = float(np.median(ts_mc))
+    batch_mc_s = barrier_max(float(np.median(ts_mc)), world)
     its_mc = [p.nIterations for p in perfs_mc]
     # the same cases one after another through the single-case path (graphs captured by a warm-up)
     for k in range(len(mats)):
@@ -456,22 +494,25 @@ def batched_leg(args, b2g, local):
         single_its.append(mats[k].solve(srcs[k], psis[k], ctl, history_cap=0)[0].nIterations)
     b1.record(stream)
     torch.cuda.synchronize()
-    seq_s = b0.elapsed_time(b1) / 1e3
+    seq_s = barrier_max(b0.elapsed_time(b1) / 1e3, world)
     x_seq = psi_all.cpu().numpy()
     its = [p.nIterations for p in perfs]
     diff = max(float(np.abs(x_batch[off[k]:off[k + 1]] - x_seq[off[k]:off[k + 1]]).max() /
                      max(np.abs(x_seq[off[k]:off[k + 1]]).max(), 1e-300)) for k in range(len(sizes)))
-    return {"workload": f"{len(sizes)} cases, cells log-uniform 4096..1048576 (seed 1), FP32-precond PCG+GAMG "
-                        f"tol 1e-6 relTol 0", "cases": len(sizes), "cells": int(off[-1]),
-            "setup_s": setup_s, "batch_s": batch_s, "cases_per_s": len(sizes) / batch_s,
-            "cells_per_s": float(off[-1]) / batch_s, "gpu_launches": int(launches),
+    n_cases = len(all_dims)
+    n_cells = sum_over_ranks(float(off[-1]), world)
+    return {"workload": f"{n_cases} cases, cells log-uniform 4096..1048576 (seed 1), FP32-precond PCG+GAMG "
+                        f"tol 1e-6 relTol 0", "cases": n_cases, "cells": int(n_cells),
+            "sharding": f"by case over {world} rank(s), no collective on the data path",
+            "setup_s": setup_s, "batch_s": batch_s, "cases_per_s": n_cases / batch_s,
+            "cells_per_s": n_cells / batch_s, "gpu_launches": int(launches),
             "iterations": {"min": int(min(its)), "max": int(max(its)), "mean": float(np.mean(its))},
             "sequential_s": seq_s, "speedup_vs_sequential": seq_s / batch_s,
             "iterations_match_sequential": int(sum(a == b for a, b in zip(its, single_its))),
             "max_field_rel_diff_vs_sequential": diff,
             "max_final_residual": float(max(p.finalResidual for p in perfs)),
-            "multicolour": {"batch_s": batch_mc_s, "cases_per_s": len(sizes) / batch_mc_s,
-                            "cells_per_s": float(off[-1]) / batch_mc_s,
+            "multicolour": {"batch_s": batch_mc_s, "cases_per_s": n_cases / batch_mc_s,
+                            "cells_per_s": n_cells / batch_mc_s,
                             "speedup_vs_sequential": seq_s / batch_mc_s,
                             "iterations": {"min": int(min(its_mc)), "max": int(max(its_mc)),
                                            "mean": float(np.mean(its_mc))},
