@@ -1379,6 +1379,70 @@ void buildColouring(LevelAddr& L, cudaStream_t s)
     C.nColours = nColours;
 }
 
+namespace {
+
+// the reversed faces: face f' is losort[nF-1-f'] (neighbours descending, faces descending within
+// one), owner' = n-1-neighbour, neighbour' = n-1-owner: again sorted by owner'
+__global__ void kRevFaces(int nF, int nC, const int* __restrict__ losort, const int* __restrict__ lower,
+                          const int* __restrict__ upper, int* __restrict__ rl, int* __restrict__ ru)
+{
+    const int f2 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f2 >= nF) return;
+    const int f = losort[nF - 1 - f2];
+    rl[f2] = nC - 1 - upper[f];
+    ru[f2] = nC - 1 - lower[f];
+}
+
+// the reversed rows: for cell c' = n-1-c, the faces c owns in ascending face order (the order in
+// which the backward walk subtracts them), the other cell in reversed numbering
+__global__ void kRevRows(int nC, const int* __restrict__ ownStart, const int* __restrict__ upper,
+                         const int* __restrict__ rowStartR, int* __restrict__ colR, int* __restrict__ faceR)
+{
+    const int c2 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c2 >= nC) return;
+    const int c = nC - 1 - c2;
+    int k = rowStartR[c2];
+    for (int f = ownStart[c]; f < ownStart[c + 1]; ++f)
+    {
+        colR[k] = nC - 1 - upper[f];
+        faceR[k] = f;
+        ++k;
+    }
+}
+
+__global__ void kRevPos(int n, const int* __restrict__ posCellF, const int* __restrict__ posOfR,
+                        int* __restrict__ revPos)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n) revPos[p] = posOfR[n - 1 - posCellF[p]];
+}
+
+}  // namespace
+
+void buildReversedLevel(LevelAddr& L, cudaStream_t s)
+{
+    if (L.rev) return;
+    const int n = L.nCells, nF = L.nFaces;
+    std::unique_ptr<LevelAddr> R(new LevelAddr);
+    R->nCells = n;
+    R->nFaces = nF;
+    R->lower.alloc(std::max(nF, 1), s);
+    R->upper.alloc(std::max(nF, 1), s);
+    if (nF) kRevFaces<<<grid(nF), TPB, 0, s>>>(nF, n, L.losort.p, L.lower.p, L.upper.p, R->lower.p, R->upper.p);
+    B2G_LAUNCH_CHECK();
+    buildLevelLayouts(*R, s);
+    // rows of the own faces only: the counts are the reversed level's neighbour counts
+    B2G_CUDA(cudaMemcpyAsync(R->rowStart.p, R->losortStart.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToDevice, s));
+    if (n) kRevRows<<<grid(n), TPB, 0, s>>>(n, L.ownStart.p, L.upper.p, R->rowStart.p, R->col.p, R->entFace.p);
+    B2G_LAUNCH_CHECK();
+    buildGsSchedule(*R, s);
+    L.revPos.alloc(std::max(n, 1), s);
+    if (n) kRevPos<<<grid(n), TPB, 0, s>>>(n, L.gs.posCell.p, R->gs.posOf.p, L.revPos.p);
+    B2G_LAUNCH_CHECK();
+    B2G_CUDA(cudaStreamSynchronize(s));
+    L.rev = std::move(R);
+}
+
 void buildStepMaps(Mesh& M, int i)
 {
     cudaStream_t s = M.stream;

@@ -4,6 +4,8 @@
 
 #include "b2g_common.cuh"
 
+#include <memory>
+
 namespace b2g {
 
 // The sweep order of one level and its Gauss-Seidel schedule (gs_kernels.cuh). Cells are split into
@@ -89,6 +91,11 @@ struct LevelAddr
     DBuf<int> entFace;      // [2*nFaces] the face
     GsSchedule gs;
     Colouring mc;           // built on first use (buildColouring)
+    // The backward walk of symGaussSeidel as a forward sweep (built on first use, buildReversedLevel):
+    // cells renumbered n-1-c, each row holding only the cell's own faces (it owns them in this level)
+    // in ascending face order, tagged with this level's face ids; its own schedule and positions.
+    std::unique_ptr<LevelAddr> rev;
+    DBuf<int> revPos;       // [nCells] this level's position -> the reversed level's position
 };
 
 // Level step i -> i+1 (GamgAgglomeration's restrictAddressing / faceRestrictAddressing /
@@ -130,6 +137,8 @@ void buildGsSchedule(LevelAddr& L, cudaStream_t s);
 // The multicolour layout of `L` (greedy colouring in cell order; a structured hex level gets the two
 // colours of a checkerboard). Needs the level's schedule (positions).
 void buildColouring(LevelAddr& L, cudaStream_t s);
+// The reversed level of `L` for symGaussSeidel's backward walk (needs L's schedule).
+void buildReversedLevel(LevelAddr& L, cudaStream_t s);
 // The position-ordered restriction and prolongation maps of step `i` (both levels scheduled).
 void buildStepMaps(Mesh& M, int i);
 // The whole agglomeration (faceAreaPairGamgAgglomeration) from device arrays.

@@ -422,7 +422,7 @@ __global__ void mcSweep(int rowBegin, int rowEnd, const int* __restrict__ pos, c
 // Every sweep of a small level's multicolour smoothing in ONE block: the colours one after another,
 // a block barrier between them (levels of at most kMcSmallRows rows).
 constexpr int kMcSmallRows = 65536;  // the largest level the tuner tries to sweep in one block
-__global__ void mcSmoothSmall(int nColours, const int* __restrict__ colourStart, int nSweeps,
+__global__ void mcSmoothSmall(int nColours, const int* __restrict__ colourStart, int nSweeps, int symmetric,
                               const int* __restrict__ pos, const int* __restrict__ sliceBase,
                               const int* __restrict__ col, const float* __restrict__ val,
                               const float* __restrict__ diag, const float* __restrict__ b, float* __restrict__ psi);

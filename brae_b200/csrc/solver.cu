@@ -228,18 +228,54 @@ __global__ void mcSweep(int rowBegin, int rowEnd, const int* __restrict__ pos, c
 }
 
 __global__ void __launch_bounds__(1024) mcSmoothSmall(int nColours, const int* __restrict__ colourStart, int nSweeps,
-                                                      const int* __restrict__ pos, const int* __restrict__ sliceBase,
-                                                      const int* __restrict__ col, const float* __restrict__ val,
-                                                      const float* __restrict__ diag, const float* __restrict__ b,
-                                                      float* __restrict__ psi)
+                                                      int symmetric, const int* __restrict__ pos,
+                                                      const int* __restrict__ sliceBase, const int* __restrict__ col,
+                                                      const float* __restrict__ val, const float* __restrict__ diag,
+                                                      const float* __restrict__ b, float* __restrict__ psi)
 {
+    const int steps = symmetric ? 2 * nColours : nColours;
     for (int sw = 0; sw < nSweeps; ++sw)
-        for (int k = 0; k < nColours; ++k)
+        for (int i = 0; i < steps; ++i)
         {
+            const int k = i < nColours ? i : 2 * nColours - 1 - i;  // symmetric: the colours back again
             const int e = colourStart[k + 1];
             for (int r = colourStart[k] + threadIdx.x; r < e; r += blockDim.x) mcRow(r, pos, sliceBase, col, val, diag, b, psi);
             __syncthreads();
         }
+}
+
+// symGaussSeidel: bPrime = source minus the row's first (neighbour-of) terms, in the reversed
+// positions with psi beside it
+template <class T>
+__global__ void symPrepare(Rows<T> A, const int* __restrict__ posCell, const int* __restrict__ losortStart,
+                           const int* __restrict__ revPos, const T* __restrict__ src, const T* __restrict__ psi,
+                           T* __restrict__ bRev, T* __restrict__ xRev)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < A.n; p += gridDim.x * blockDim.x)
+    {
+        const int c = posCell[p];
+        const int e0 = A.rowStart[p];
+        const int e1 = e0 + (losortStart[c + 1] - losortStart[c]);
+        T acc = src[p];
+        for (int e = e0; e < e1; ++e) acc = subRn(acc, mulRn(A.val[e], psi[A.col[e]]));
+        const int q = revPos[p];
+        bRev[q] = acc;
+        xRev[q] = psi[p];
+    }
+}
+
+template <class T>
+__global__ void symFinish(int n, const int* __restrict__ revPos, const T* __restrict__ xRev, T* __restrict__ psi)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) psi[p] = xRev[revPos[p]];
+}
+
+// the diagonal by reversed position (cell n-1-c of the reversed level is cell c)
+template <class T>
+__global__ void revDiag(int n, const int* __restrict__ posCellR, const double* __restrict__ diag, T* __restrict__ out)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+        out[q] = static_cast<T>(diag[n - 1 - posCellR[q]]);
 }
 
 __global__ void mcValues(long long nEnt, int nRows, const int* __restrict__ face, const int* __restrict__ pos,
@@ -542,19 +578,31 @@ template <class T>
 void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps, unsigned long long* trace)
 {
     if (nSweeps <= 0) return;
-    if (smoother != B2G_SMOOTHER_GAUSS_SEIDEL)
-        fail(B2G_ERR_REFUSED, "b2g: the device smoother for this entry is GaussSeidel only so far; "
-                              "symGaussSeidel, DIC and DICGaussSeidel are not built on the device yet.");
+    if (smoother != B2G_SMOOTHER_GAUSS_SEIDEL && smoother != B2G_SMOOTHER_SYM_GAUSS_SEIDEL)
+        fail(B2G_ERR_REFUSED, "b2g: the device smoothers for this entry are GaussSeidel and symGaussSeidel so "
+                              "far; DIC and DICGaussSeidel are not built on the device yet.");
+    const bool symmetric = smoother == B2G_SMOOTHER_SYM_GAUSS_SEIDEL;
     if (sizeof(T) == 4 && multicolour)
     {
-        mcSmooth(level, reinterpret_cast<float*>(psiL), reinterpret_cast<const float*>(src), nSweeps);
+        mcSmooth(level, reinterpret_cast<float*>(psiL), reinterpret_cast<const float*>(src), nSweeps, symmetric);
         return;
     }
-    const LevelAddr& L = mesh->lev[level];
+    if (mesh->lev[level].nCells == 0) return;
+    if (symmetric)
+    {
+        symSmooth<T>(level, psiL, src, nSweeps);
+        return;
+    }
+    for (int sw = 0; sw < nSweeps; ++sw) gsLaunch<T>(mesh->lev[level], data<T>().coef[level], psiL, src, trace, level == 0);
+}
+
+// One exact Gauss-Seidel sweep of level L (its schedule) with coefficients C.
+template <class T>
+void Matrix::gsLaunch(const LevelAddr& L, const LevelCoef<T>& C, T* psiL, const T* src, unsigned long long* trace,
+                      bool timed)
+{
     const GsSchedule& G = L.gs;
-    const LevelCoef<T>& C = data<T>().coef[level];
     k::GsArgs<T> a;
-    if (L.nCells == 0) return;
     a.nParts = G.nParts;
     a.maxCells = G.maxCells;
     a.maxEnt = G.maxEnt;
@@ -576,43 +624,108 @@ void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps,
     a.trace = trace;
     a.traceDepths = G.maxDepth + 2;
     const size_t smem = k::gsSmemBytes<T>(G.maxCells, G.maxEnt, G.maxGat);
+    B2G_CUDA(cudaMemsetAsync(G.progress.p, 0, G.progress.bytes(), stream));
+    cudaEvent_t e = timed ? timedBegin(1) : nullptr;
+    k::gsSweep<T><<<G.nParts, G.maxCells + 128, smem, stream>>>(a);
+    timedEnd(1, e);
+    B2G_LAUNCH_CHECK();
+    launches += 1;
+}
+
+// The reversed layout of one level in T (once per matrix): the mesh's reversed level, the diagonal
+// by reversed position and the chunk blobs with this matrix's coefficients; the scratch vectors.
+template <class T>
+void Matrix::ensureSym(int level)
+{
+    VCycleData<T>& D = data<T>();
+    if (static_cast<int>(D.rev.size()) <= level) D.rev.resize(mesh->lev.size());
+    if (static_cast<int>(D.revB.size()) <= level)
+    {
+        D.revB.resize(mesh->lev.size());
+        D.revX.resize(mesh->lev.size());
+    }
+    if (D.rev[level].blob.p) return;
+    LevelAddr& L = mesh->lev[level];
+    buildReversedLevel(L, stream);
+    const LevelAddr& R = *L.rev;
+    LevelCoef<T>& C = D.rev[level];
+    allocGsLayout(R, C, stream);
+    k::revDiag<T><<<rowsGrid(R.nCells), NT, 0, stream>>>(R.nCells, R.gs.posCell.p, v64.coef[level].diag.p, C.gsDiag.p);
+    B2G_LAUNCH_CHECK();
+    fillBlobs<T>(R, C, v64.coef[level].upper.p, stream);
+    D.revB[level].alloc(std::max(R.gs.nAlloc, 1), stream);
+    D.revX[level].alloc(std::max(R.gs.nAlloc, 1), stream);
+    D.revB[level].zero(stream);
+    D.revX[level].zero(stream);
+}
+
+// What the smoother needs built before an iteration is captured (builds synchronise the stream).
+void Matrix::prepareSmoother(const b2g_controls& c)
+{
+    if (c.smoother != B2G_SMOOTHER_SYM_GAUSS_SEIDEL) return;
+    for (int i = 0; i < nLevels(); ++i)
+    {
+        if (c.precision == B2G_PRECISION_FP64 || c.solver == B2G_SOLVER_GAMG) ensureSym<double>(i);
+        else if (c.precision == B2G_PRECISION_FP32_PRECOND) ensureSym<float>(i);
+    }
+    B2G_CUDA(cudaStreamSynchronize(stream));
+}
+
+// symGaussSeidel sweeps (gaussSeidelSweeps' symmetric variant, smooth_solver_cpp.cu:87-166): the
+// forward walk; then bPrime = source minus the faces the cell is the neighbour of times the new psi
+// (subtracted in ascending face order, as the forward walk distributes them), moved with psi to the
+// reversed positions; the backward walk as a forward sweep of the reversed level; psi moved back.
+template <class T>
+void Matrix::symSmooth(int level, T* psiL, const T* src, int nSweeps)
+{
+    ensureSym<T>(level);
+    const LevelAddr& L = mesh->lev[level];
+    VCycleData<T>& D = data<T>();
+    const LevelCoef<T>& C = D.coef[level];
     for (int sw = 0; sw < nSweeps; ++sw)
     {
-        B2G_CUDA(cudaMemsetAsync(G.progress.p, 0, G.progress.bytes(), stream));
-        cudaEvent_t e = level == 0 ? timedBegin(1) : nullptr;
-        k::gsSweep<T><<<G.nParts, G.maxCells + 128, smem, stream>>>(a);
-        timedEnd(1, e);
+        gsLaunch<T>(L, C, psiL, src, nullptr, level == 0);
+        k::symPrepare<T><<<rowsGrid(L.nCells), NT, 0, stream>>>(rowsOf(L, C), L.gs.posCell.p, L.losortStart.p,
+                                                               L.revPos.p, src, psiL, D.revB[level].p,
+                                                               D.revX[level].p);
         B2G_LAUNCH_CHECK();
-        launches += 1;
+        gsLaunch<T>(*L.rev, D.rev[level], D.revX[level].p, D.revB[level].p, nullptr, level == 0);
+        k::symFinish<T><<<rowsGrid(L.nCells), NT, 0, stream>>>(L.nCells, L.revPos.p, D.revX[level].p, psiL);
+        B2G_LAUNCH_CHECK();
+        launches += 2;
     }
 }
 
-// Gauss-Seidel sweeps of the FP32 V-cycle, colour by colour (B2G_PRECISION_FP32_PRECOND_MULTICOLOUR)
-void Matrix::mcSmooth(int level, float* psiL, const float* src, int nSweeps)
+// Gauss-Seidel sweeps of the FP32 V-cycle, colour by colour (B2G_PRECISION_FP32_PRECOND_MULTICOLOUR);
+// symmetric: each sweep takes the colours forward, then back
+void Matrix::mcSmooth(int level, float* psiL, const float* src, int nSweeps, bool symmetric)
 {
     const Colouring& C = mesh->lev[level].mc;
-    mcLaunch(level, C.fused, C.block, psiL, src, nSweeps, true);
+    mcLaunch(level, C.fused, C.block, psiL, src, nSweeps, true, symmetric);
 }
 
 // nSweeps multicolour sweeps of one level in a given shape: one block for the whole level, or one
 // launch per colour of `block` threads per block
-void Matrix::mcLaunch(int level, bool fused, int block, float* psiL, const float* src, int nSweeps, bool timed)
+void Matrix::mcLaunch(int level, bool fused, int block, float* psiL, const float* src, int nSweeps, bool timed,
+                      bool symmetric)
 {
     const Colouring& C = mesh->lev[level].mc;
     const LevelCoef<float>& F = v32.coef[level];
     if (fused)
     {
         cudaEvent_t ev = timed && level == 0 ? timedBegin(1) : nullptr;
-        k::mcSmoothSmall<<<1, 1024, 0, stream>>>(C.nColours, C.colourStartD.p, nSweeps, C.pos.p, C.sliceBase.p,
-                                                  C.col.p, F.mcVal.p, F.mcDiag.p, src, psiL);
+        k::mcSmoothSmall<<<1, 1024, 0, stream>>>(C.nColours, C.colourStartD.p, nSweeps, symmetric ? 1 : 0, C.pos.p,
+                                                  C.sliceBase.p, C.col.p, F.mcVal.p, F.mcDiag.p, src, psiL);
         timedEnd(1, ev);
         B2G_LAUNCH_CHECK();
         ++launches;
         return;
     }
+    const int steps = symmetric ? 2 * C.nColours : C.nColours;
     for (int sw = 0; sw < nSweeps; ++sw)
-        for (int k = 0; k < C.nColours; ++k)
+        for (int i = 0; i < steps; ++i)
         {
+            const int k = i < C.nColours ? i : 2 * C.nColours - 1 - i;
             const int b = C.colourStart[k], e = C.colourStart[k + 1];
             if (e <= b) continue;
             cudaEvent_t ev = timed && level == 0 ? timedBegin(1) : nullptr;
@@ -1080,6 +1193,7 @@ b2g_perf Matrix::pcg(const b2g_controls& c, b2g_solve_log* log)
     const bool flexible = c.precision != B2G_PRECISION_FP64;
     if (flexible) ensureFp32();
     if (c.precision == B2G_PRECISION_FP32_PRECOND_MULTICOLOUR) ensureMulticolour();
+    prepareSmoother(c);
     kPcgStart<<<1, 1, 0, stream>>>(scal.p);
     B2G_LAUNCH_CHECK();
     do
@@ -1129,6 +1243,7 @@ b2g_perf Matrix::gamg(const b2g_controls& c, b2g_solve_log* log)
                               "nCellsInCoarsestLevel too large (GAMGSolver.C:333).");
     resetLog(log ? std::max(log->coarsestCapacity, 0) : 0);
     buildCoarse();
+    prepareSmoother(c);
     b2g_controls cc = c;
     // the standalone solver's coarsest level runs to the GAMG entry's own tolerance and relTol
     cc.precTolerance = c.tolerance;

@@ -39,6 +39,10 @@ struct VCycleData
     DBuf<T> partial;                  // reduction partials
     DBuf<T> sf;                       // scale factor slot
     DBuf<T> cpA, cwA, crA, crD;       // coarsest scratch
+    // symGaussSeidel: each level's reversed layout (diagonal and chunk blobs by reversed position)
+    // and the backward walk's source and psi in reversed positions
+    std::vector<LevelCoef<T>> rev;
+    std::vector<DBuf<T>> revB, revX;
     // FP32 form only: dense Cholesky of the coarsest level
     bool built = false;
 };
@@ -96,8 +100,14 @@ struct Matrix
     void buildCoarse();                       // Galerkin matrices of every coarse level
     void ensureFp32();                        // float copies of every level
     void ensureMulticolour();                 // the multicolour layout and its FP32 values
-    void mcSmooth(int level, float* psi, const float* source, int nSweeps);
-    void mcLaunch(int level, bool fused, int block, float* psi, const float* source, int nSweeps, bool timed);
+    void mcSmooth(int level, float* psi, const float* source, int nSweeps, bool symmetric);
+    template <class T> void gsLaunch(const LevelAddr& L, const LevelCoef<T>& C, T* psi, const T* source,
+                                     unsigned long long* trace, bool timed);
+    template <class T> void ensureSym(int level);   // the reversed layout of `level` in T
+    void prepareSmoother(const b2g_controls& c);
+    template <class T> void symSmooth(int level, T* psi, const T* source, int nSweeps);
+    void mcLaunch(int level, bool fused, int block, float* psi, const float* source, int nSweeps, bool timed,
+                  bool symmetric = false);
     void tuneMulticolour(int level);
     int nLevels() const { return mesh->nLevels(); }
     int n(int level) const { return mesh->lev[level].nCells; }

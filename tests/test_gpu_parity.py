@@ -104,6 +104,11 @@ def test_level_kernels_bitexact(b2g, oracle, name, kw):
             A.smooth(lv, psi, dev(b), sweeps)
             want = oracle.smooth(lo, up, d, u, x, b, sweeps, "GaussSeidel")
             assert np.array_equal(host(psi), want), f"GaussSeidel level {lv} sweeps {sweeps}"
+        for sweeps in (1, 2):
+            psi = dev(x)
+            A.smooth(lv, psi, dev(b), sweeps, smoother="symGaussSeidel")
+            want = oracle.smooth(lo, up, d, u, x, b, sweeps, "symGaussSeidel")
+            assert np.array_equal(host(psi), want), f"symGaussSeidel level {lv} sweeps {sweeps}"
         # scale: dots differ in summation order only
         f = dev(x)
         acf = torch.empty_like(f)
@@ -184,6 +189,30 @@ def test_pcg_gamg_solve_parity_options(b2g, oracle, reduction):
                   reduction=reduction)
     _solve_parity(b2g, oracle, c, 1e-6, 0.05, dict(scaleCorrection=False),
                   psi0=np.linspace(-1.0, 1.0, c.n_cells), reduction=reduction)
+
+
+@pytest.mark.parametrize("reduction", ["serial", "tree"])
+@pytest.mark.parametrize("name,kw", BOXES[1:4], ids=[b[0] for b in BOXES[1:4]])
+def test_pcg_gamg_sym_gauss_seidel_parity(b2g, oracle, name, kw, reduction):
+    # the symmetric smoother: its backward walk runs as a forward sweep of the reversed level
+    c = cases.box_case(**kw)
+    _solve_parity(b2g, oracle, c, 1e-8, 0.0, dict(smoother="symGaussSeidel"), reduction=reduction)
+    _solve_parity(b2g, oracle, c, 1e-8, 0.0, dict(smoother="symGaussSeidel", nPreSweeps=1), reduction=reduction)
+
+
+@pytest.mark.parametrize("precision", ["fp32_precond", "fp32_precond_multicolour"])
+def test_sym_gauss_seidel_fp32_forms(b2g, oracle, precision):
+    c = cases.box_case(24, 20, 22, (2.0, 1.0, 1.0), 20.0, True)
+    mesh = b2g.Mesh(c.lower, c.upper, c.Sf, c.magSf, c.n_cells, 10, True)
+    agg = oracle.agglomerate(c.lower, c.upper, c.Sf, c.magSf, c.n_cells, 10, True)
+    want = oracle.pcg_gamg_solve(agg, c.diag, c.coef, c.source, np.zeros(c.n_cells), 1e-9, 0.0,
+                                 ctl=oc_controls(smoother="symGaussSeidel"))
+    psi = np.zeros(c.n_cells)
+    ctl = b2g.controls_default(tolerance=1e-9, relTol=0.0, precision=precision, smoother="symGaussSeidel")
+    perf = b2g.pcg_gamg_solve(mesh, c.diag, c.coef, c.source, psi, ctl)[0]
+    assert perf.finalResidual < 1e-9
+    assert 1 <= perf.nIterations <= want["perf"][2] + 2
+    assert np.abs(psi - want["psi"]).max() / np.abs(want["psi"]).max() < 1e-6
 
 
 @pytest.mark.parametrize("reduction", ["serial", "tree"])
