@@ -20,7 +20,7 @@ LIB = os.path.join(HERE, "libbrae_gamg.so")
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 SOURCES = ["hierarchy.cu", "solver.cu", "capi.cu", "server.cu", "batch.cu"]
 FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
-         "--fmad=false", "-Xcompiler", "-fPIC,-fvisibility=hidden", "-Xptxas", "-O3"]
+         "--fmad=false", "-Xcompiler", "-fPIC,-fvisibility=hidden,-ffp-contract=off", "-Xptxas", "-O3"]
 
 
 def _deps(src: str) -> list[str]:

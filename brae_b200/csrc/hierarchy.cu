@@ -1396,18 +1396,41 @@ __global__ void kRevFaces(int nF, int nC, const int* __restrict__ losort, const 
 // the reversed rows: for cell c' = n-1-c, the faces c owns in ascending face order (the order in
 // which the backward walk subtracts them), the other cell in reversed numbering
 __global__ void kRevRows(int nC, const int* __restrict__ ownStart, const int* __restrict__ upper,
-                         const int* __restrict__ rowStartR, int* __restrict__ colR, int* __restrict__ faceR)
+                         const int* __restrict__ rowStartR, int* __restrict__ colR, int* __restrict__ faceR,
+                         int descending)
 {
     const int c2 = blockIdx.x * blockDim.x + threadIdx.x;
     if (c2 >= nC) return;
     const int c = nC - 1 - c2;
     int k = rowStartR[c2];
-    for (int f = ownStart[c]; f < ownStart[c + 1]; ++f)
+    const int f0 = ownStart[c], f1 = ownStart[c + 1];
+    for (int i = 0; i < f1 - f0; ++i)
     {
+        const int f = descending ? f1 - 1 - i : f0 + i;
         colR[k] = nC - 1 - upper[f];
         faceR[k] = f;
         ++k;
     }
+}
+
+// the lower-only rows: the faces the cell is the neighbour of, ascending (losort order)
+__global__ void kLowerRows(int nC, const int* __restrict__ losortStart, const int* __restrict__ losort,
+                           const int* __restrict__ lower, int* __restrict__ col, int* __restrict__ face)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nC) return;
+    for (int q = losortStart[c]; q < losortStart[c + 1]; ++q)
+    {
+        col[q] = lower[losort[q]];
+        face[q] = losort[q];
+    }
+}
+
+__global__ void kSamePos(int n, const int* __restrict__ posCellF, const int* __restrict__ posOfR,
+                         int* __restrict__ outPos)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n) outPos[p] = posOfR[posCellF[p]];
 }
 
 __global__ void kRevPos(int n, const int* __restrict__ posCellF, const int* __restrict__ posOfR,
@@ -1419,9 +1442,9 @@ __global__ void kRevPos(int n, const int* __restrict__ posCellF, const int* __re
 
 }  // namespace
 
-void buildReversedLevel(LevelAddr& L, cudaStream_t s)
+void buildReversedLevel(LevelAddr& L, cudaStream_t s, bool descending)
 {
-    if (L.rev) return;
+    if (descending ? static_cast<bool>(L.revDesc) : static_cast<bool>(L.rev)) return;
     const int n = L.nCells, nF = L.nFaces;
     std::unique_ptr<LevelAddr> R(new LevelAddr);
     R->nCells = n;
@@ -1433,14 +1456,43 @@ void buildReversedLevel(LevelAddr& L, cudaStream_t s)
     buildLevelLayouts(*R, s);
     // rows of the own faces only: the counts are the reversed level's neighbour counts
     B2G_CUDA(cudaMemcpyAsync(R->rowStart.p, R->losortStart.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToDevice, s));
-    if (n) kRevRows<<<grid(n), TPB, 0, s>>>(n, L.ownStart.p, L.upper.p, R->rowStart.p, R->col.p, R->entFace.p);
+    if (n)
+        kRevRows<<<grid(n), TPB, 0, s>>>(n, L.ownStart.p, L.upper.p, R->rowStart.p, R->col.p, R->entFace.p,
+                                         descending ? 1 : 0);
     B2G_LAUNCH_CHECK();
     buildGsSchedule(*R, s);
-    L.revPos.alloc(std::max(n, 1), s);
-    if (n) kRevPos<<<grid(n), TPB, 0, s>>>(n, L.gs.posCell.p, R->gs.posOf.p, L.revPos.p);
+    DBuf<int>& pos = descending ? L.revDescPos : L.revPos;
+    pos.alloc(std::max(n, 1), s);
+    if (n) kRevPos<<<grid(n), TPB, 0, s>>>(n, L.gs.posCell.p, R->gs.posOf.p, pos.p);
     B2G_LAUNCH_CHECK();
     B2G_CUDA(cudaStreamSynchronize(s));
-    L.rev = std::move(R);
+    (descending ? L.revDesc : L.rev) = std::move(R);
+}
+
+void buildLowerLevel(LevelAddr& L, cudaStream_t s)
+{
+    if (L.lowerOnly) return;
+    const int n = L.nCells, nF = L.nFaces;
+    std::unique_ptr<LevelAddr> R(new LevelAddr);
+    R->nCells = n;
+    R->nFaces = nF;
+    R->lower.alloc(std::max(nF, 1), s);
+    R->upper.alloc(std::max(nF, 1), s);
+    if (nF)
+    {
+        B2G_CUDA(cudaMemcpyAsync(R->lower.p, L.lower.p, sizeof(int) * nF, cudaMemcpyDeviceToDevice, s));
+        B2G_CUDA(cudaMemcpyAsync(R->upper.p, L.upper.p, sizeof(int) * nF, cudaMemcpyDeviceToDevice, s));
+    }
+    buildLevelLayouts(*R, s);
+    B2G_CUDA(cudaMemcpyAsync(R->rowStart.p, R->losortStart.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToDevice, s));
+    if (n) kLowerRows<<<grid(n), TPB, 0, s>>>(n, R->losortStart.p, R->losort.p, R->lower.p, R->col.p, R->entFace.p);
+    B2G_LAUNCH_CHECK();
+    buildGsSchedule(*R, s);
+    L.lowerPos.alloc(std::max(n, 1), s);
+    if (n) kSamePos<<<grid(n), TPB, 0, s>>>(n, L.gs.posCell.p, R->gs.posOf.p, L.lowerPos.p);
+    B2G_LAUNCH_CHECK();
+    B2G_CUDA(cudaStreamSynchronize(s));
+    L.lowerOnly = std::move(R);
 }
 
 void buildStepMaps(Mesh& M, int i)

@@ -96,6 +96,13 @@ struct LevelAddr
     // in ascending face order, tagged with this level's face ids; its own schedule and positions.
     std::unique_ptr<LevelAddr> rev;
     DBuf<int> revPos;       // [nCells] this level's position -> the reversed level's position
+    // DIC's substitutions as forward sweeps (built on first use): the forward one on a level whose
+    // rows hold only the faces the cell is the neighbour of (ascending), the backward one on a
+    // reversed level whose rows hold the cell's own faces in DESCENDING face order
+    std::unique_ptr<LevelAddr> lowerOnly;
+    DBuf<int> lowerPos;
+    std::unique_ptr<LevelAddr> revDesc;
+    DBuf<int> revDescPos;
 };
 
 // Level step i -> i+1 (GamgAgglomeration's restrictAddressing / faceRestrictAddressing /
@@ -137,8 +144,11 @@ void buildGsSchedule(LevelAddr& L, cudaStream_t s);
 // The multicolour layout of `L` (greedy colouring in cell order; a structured hex level gets the two
 // colours of a checkerboard). Needs the level's schedule (positions).
 void buildColouring(LevelAddr& L, cudaStream_t s);
-// The reversed level of `L` for symGaussSeidel's backward walk (needs L's schedule).
-void buildReversedLevel(LevelAddr& L, cudaStream_t s);
+// The reversed level of `L` for symGaussSeidel's backward walk (needs L's schedule); with
+// `descending`, the one for DIC's backward substitution (L.revDesc).
+void buildReversedLevel(LevelAddr& L, cudaStream_t s, bool descending = false);
+// The lower-only level of `L` for DIC's forward substitution (L.lowerOnly).
+void buildLowerLevel(LevelAddr& L, cudaStream_t s);
 // The position-ordered restriction and prolongation maps of step `i` (both levels scheduled).
 void buildStepMaps(Mesh& M, int i);
 // The whole agglomeration (faceAreaPairGamgAgglomeration) from device arrays.

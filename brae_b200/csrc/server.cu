@@ -22,8 +22,8 @@
 // boundary through pinned staging buffers, one pair per slot (copies from pageable memory are
 // synchronous and serialise across threads), and the solution goes back into the caller's psi.
 //
-// The standalone GAMG solver (controls->solver == B2G_SOLVER_GAMG) is solved alone, as
-// b2g_matrix_pcg_solve's sibling b2g_gamg_solve does.
+// The standalone GAMG solver (controls->solver == B2G_SOLVER_GAMG) and the smoothers other than
+// GaussSeidel are solved alone, by the single-case path (the batch sweeps GaussSeidel).
 #include "batch.cuh"
 #include "capi_internal.cuh"
 
@@ -233,7 +233,7 @@ void workerLoop(b2g_server* S, int slot)
             if (S->stopping) return;
             auto it0 = runnable();
             const b2g_controls c0 = it0->controls;
-            alone = c0.solver != B2G_SOLVER_PCG_GAMG;
+            alone = c0.solver != B2G_SOLVER_PCG_GAMG || c0.smoother != B2G_SMOOTHER_GAUSS_SEIDEL;
             const int cls = sizeClass(S->cases[it0->caseId]->nCells);
             // the oldest runnable request, then the queued requests of other idle cases that can
             // share its batch, oldest first
@@ -242,6 +242,7 @@ void workerLoop(b2g_server* S, int slot)
             {
                 b2g_server::Case* c = S->cases[it->caseId].get();
                 const bool fits = first || (!alone && !c->busy && it->controls.solver == B2G_SOLVER_PCG_GAMG &&
+                                            it->controls.smoother == B2G_SMOOTHER_GAUSS_SEIDEL &&
                                             sizeClass(c->nCells) == cls &&
                                             std::memcmp(&it->controls, &c0, sizeof(b2g_controls)) == 0);
                 first = false;

@@ -270,6 +270,70 @@ __global__ void symFinish(int n, const int* __restrict__ revPos, const T* __rest
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) psi[p] = xRev[revPos[p]];
 }
 
+// DIC: w0 = r * rD at the lower-only level's positions (source and starting psi of the forward
+// substitution)
+template <class T>
+__global__ void dicStart(int n, const T* __restrict__ r, const T* __restrict__ rdPos, const int* __restrict__ toLo,
+                         T* __restrict__ bLo, T* __restrict__ xLo)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+    {
+        const T w = mulRn(r[p], rdPos[p]);
+        const int q = toLo[p];
+        bLo[q] = w;
+        xLo[q] = w;
+    }
+}
+
+// DIC: the forward substitution's result moved to the descending reversed level's positions
+template <class T>
+__global__ void dicMid(int n, const int* __restrict__ toLo, const int* __restrict__ toUp, const T* __restrict__ xLo,
+                       T* __restrict__ bUp, T* __restrict__ xUp)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+    {
+        const T w = xLo[toLo[p]];
+        const int q = toUp[p];
+        bUp[q] = w;
+        xUp[q] = w;
+    }
+}
+
+// DIC: psi += w
+template <class T>
+__global__ void dicAdd(int n, const int* __restrict__ toUp, const T* __restrict__ xUp, T* __restrict__ psi)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+        psi[p] = addRn(psi[p], xUp[toUp[p]]);
+}
+
+// per face rD[cell]*coef (the substitution's coefficient for the row of `cell`: the neighbour in the
+// forward substitution, the owner in the backward one)
+__global__ void dicFaceVals(int nF, const int* __restrict__ lower, const int* __restrict__ upper,
+                            const double* __restrict__ coef, const double* __restrict__ rD, double* __restrict__ lo,
+                            double* __restrict__ up)
+{
+    for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nF; f += gridDim.x * blockDim.x)
+    {
+        lo[f] = __dmul_rn(rD[upper[f]], coef[f]);
+        up[f] = __dmul_rn(rD[lower[f]], coef[f]);
+    }
+}
+
+template <class T>
+__global__ void byPosition(int n, const int* __restrict__ posCell, const double* __restrict__ byCell, T* __restrict__ out)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+        out[p] = static_cast<T>(byCell[posCell[p]]);
+}
+
+template <class T>
+__global__ void fillValue(long long n, T* __restrict__ x, T v)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        x[i] = v;
+}
+
 // the diagonal by reversed position (cell n-1-c of the reversed level is cell c)
 template <class T>
 __global__ void revDiag(int n, const int* __restrict__ posCellR, const double* __restrict__ diag, T* __restrict__ out)
@@ -578,9 +642,16 @@ template <class T>
 void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps, unsigned long long* trace)
 {
     if (nSweeps <= 0) return;
-    if (smoother != B2G_SMOOTHER_GAUSS_SEIDEL && smoother != B2G_SMOOTHER_SYM_GAUSS_SEIDEL)
-        fail(B2G_ERR_REFUSED, "b2g: the device smoothers for this entry are GaussSeidel and symGaussSeidel so "
-                              "far; DIC and DICGaussSeidel are not built on the device yet.");
+    if (smoother < B2G_SMOOTHER_GAUSS_SEIDEL || smoother > B2G_SMOOTHER_DIC_GAUSS_SEIDEL)
+        fail(B2G_ERR_ARGUMENT, "b2g: unknown smoother");
+    if (smoother == B2G_SMOOTHER_DIC || smoother == B2G_SMOOTHER_DIC_GAUSS_SEIDEL)
+    {
+        // DICSmoother's sweeps; DICGaussSeidel then sweeps Gauss-Seidel as often (GAMG:234-317)
+        if (mesh->lev[level].nCells == 0) return;
+        dicSmooth<T>(level, psiL, src, nSweeps);
+        if (smoother == B2G_SMOOTHER_DIC) return;
+        smoother = B2G_SMOOTHER_GAUSS_SEIDEL;
+    }
     const bool symmetric = smoother == B2G_SMOOTHER_SYM_GAUSS_SEIDEL;
     if (sizeof(T) == 4 && multicolour)
     {
@@ -662,13 +733,111 @@ void Matrix::ensureSym(int level)
 // What the smoother needs built before an iteration is captured (builds synchronise the stream).
 void Matrix::prepareSmoother(const b2g_controls& c)
 {
-    if (c.smoother != B2G_SMOOTHER_SYM_GAUSS_SEIDEL) return;
+    const bool sym = c.smoother == B2G_SMOOTHER_SYM_GAUSS_SEIDEL;
+    const bool dic = c.smoother == B2G_SMOOTHER_DIC || c.smoother == B2G_SMOOTHER_DIC_GAUSS_SEIDEL;
+    if (!sym && !dic) return;
+    const bool fp64 = c.precision == B2G_PRECISION_FP64 || c.solver == B2G_SOLVER_GAMG;
     for (int i = 0; i < nLevels(); ++i)
     {
-        if (c.precision == B2G_PRECISION_FP64 || c.solver == B2G_SOLVER_GAMG) ensureSym<double>(i);
-        else if (c.precision == B2G_PRECISION_FP32_PRECOND) ensureSym<float>(i);
+        // the multicolour form sweeps symGaussSeidel by colour; DIC there runs in exact order
+        if (sym && fp64) ensureSym<double>(i);
+        else if (sym && c.precision == B2G_PRECISION_FP32_PRECOND) ensureSym<float>(i);
+        if (dic && fp64) ensureDic<double>(i);
+        else if (dic) ensureDic<float>(i);
     }
     B2G_CUDA(cudaStreamSynchronize(stream));
+}
+
+// DIC's layouts for one level in T (once per matrix): rD by the reference's recurrence
+// (DICPreconditioner::calcReciprocalD, gamg_solver_cpp.cu:194-210) on the host, in face order;
+// the substitutions' per-face coefficients; the lower-only and descending reversed levels (on the
+// mesh, once) with blobs of diagonal 1; rD by position; scratch vectors.
+template <class T>
+void Matrix::ensureDic(int level)
+{
+    VCycleData<T>& D = data<T>();
+    const size_t nl = mesh->lev.size();
+    for (auto* v : {&D.dicLo, &D.dicUp})
+        if (v->size() < nl) v->resize(nl);
+    for (auto* v : {&D.rdPos, &D.dicR, &D.dicLoB, &D.dicLoX, &D.dicUpB, &D.dicUpX})
+        if (v->size() < nl) v->resize(nl);
+    if (D.dicLo[level].blob.p) return;
+    LevelAddr& L = mesh->lev[level];
+    const int n = L.nCells, nF = L.nFaces;
+    if (rdCell.size() < nl) rdCell.resize(nl);
+    if (!rdCell[level].p)
+    {
+        const std::vector<double> diag = v64.coef[level].diag.download(stream);
+        const std::vector<double> coef = v64.coef[level].upper.download(stream);
+        const std::vector<int> lo = L.lower.download(stream);
+        const std::vector<int> up = L.upper.download(stream);
+        std::vector<double> rD(diag);
+        for (int f = 0; f < nF; ++f) rD[up[f]] -= coef[f] * coef[f] / rD[lo[f]];
+        for (int c = 0; c < n; ++c) rD[c] = 1.0 / rD[c];
+        rdCell[level].upload(rD.data(), rD.size(), stream);
+    }
+    buildLowerLevel(L, stream);
+    buildReversedLevel(L, stream, true);
+    DBuf<double> loVal, upVal;
+    loVal.alloc(std::max(nF, 1), stream);
+    upVal.alloc(std::max(nF, 1), stream);
+    if (nF)
+        k::dicFaceVals<<<std::min(ceilDiv(nF, NT), 8192), NT, 0, stream>>>(nF, L.lower.p, L.upper.p,
+                                                                          v64.coef[level].upper.p, rdCell[level].p,
+                                                                          loVal.p, upVal.p);
+    B2G_LAUNCH_CHECK();
+    for (int which = 0; which < 2; ++which)
+    {
+        const LevelAddr& R = which == 0 ? *L.lowerOnly : *L.revDesc;
+        LevelCoef<T>& C = which == 0 ? D.dicLo[level] : D.dicUp[level];
+        allocGsLayout(R, C, stream);
+        k::fillValue<T><<<rowsGrid(n), NT, 0, stream>>>(n, C.gsDiag.p, T(1));
+        B2G_LAUNCH_CHECK();
+        fillBlobs<T>(R, C, which == 0 ? loVal.p : upVal.p, stream);
+    }
+    D.rdPos[level].alloc(nAlloc(level), stream);
+    D.rdPos[level].zero(stream);
+    k::byPosition<T><<<rowsGrid(n), NT, 0, stream>>>(n, L.gs.posCell.p, rdCell[level].p, D.rdPos[level].p);
+    B2G_LAUNCH_CHECK();
+    D.dicR[level].alloc(nAlloc(level), stream);
+    for (auto* v : {&D.dicLoB, &D.dicLoX})
+    {
+        (*v)[level].alloc(std::max(L.lowerOnly->gs.nAlloc, 1), stream);
+        (*v)[level].zero(stream);
+    }
+    for (auto* v : {&D.dicUpB, &D.dicUpX})
+    {
+        (*v)[level].alloc(std::max(L.revDesc->gs.nAlloc, 1), stream);
+        (*v)[level].zero(stream);
+    }
+    B2G_CUDA(cudaStreamSynchronize(stream));  // loVal / upVal are read by the blob builds
+}
+
+// DICSmoother::smooth (gamg_solver_cpp.cu:234-317): per sweep r = source - A psi, w = rD r, the two
+// DIC substitutions (DICPreconditioner, :212-231) as forward sweeps of the lower-only and the
+// descending reversed levels, psi += w
+template <class T>
+void Matrix::dicSmooth(int level, T* psiL, const T* src, int nSweeps)
+{
+    ensureDic<T>(level);
+    const LevelAddr& L = mesh->lev[level];
+    VCycleData<T>& D = data<T>();
+    const int n = L.nCells;
+    for (int sw = 0; sw < nSweeps; ++sw)
+    {
+        k::residual<T><<<rowsGrid(n), NT, 0, stream>>>(rowsOf(L, D.coef[level]), src, psiL, D.dicR[level].p);
+        k::dicStart<T><<<rowsGrid(n), NT, 0, stream>>>(n, D.dicR[level].p, D.rdPos[level].p, L.lowerPos.p,
+                                                       D.dicLoB[level].p, D.dicLoX[level].p);
+        B2G_LAUNCH_CHECK();
+        gsLaunch<T>(*L.lowerOnly, D.dicLo[level], D.dicLoX[level].p, D.dicLoB[level].p, nullptr, false);
+        k::dicMid<T><<<rowsGrid(n), NT, 0, stream>>>(n, L.lowerPos.p, L.revDescPos.p, D.dicLoX[level].p,
+                                                     D.dicUpB[level].p, D.dicUpX[level].p);
+        B2G_LAUNCH_CHECK();
+        gsLaunch<T>(*L.revDesc, D.dicUp[level], D.dicUpX[level].p, D.dicUpB[level].p, nullptr, false);
+        k::dicAdd<T><<<rowsGrid(n), NT, 0, stream>>>(n, L.revDescPos.p, D.dicUpX[level].p, psiL);
+        B2G_LAUNCH_CHECK();
+        launches += 4;
+    }
 }
 
 // symGaussSeidel sweeps (gaussSeidelSweeps' symmetric variant, smooth_solver_cpp.cu:87-166): the

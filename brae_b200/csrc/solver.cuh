@@ -43,6 +43,10 @@ struct VCycleData
     // and the backward walk's source and psi in reversed positions
     std::vector<LevelCoef<T>> rev;
     std::vector<DBuf<T>> revB, revX;
+    // DIC / DICGaussSeidel: per level the substitutions' layouts (the lower-only level's and the
+    // descending reversed level's chunk blobs, diagonal 1), rD by position, and scratch vectors
+    std::vector<LevelCoef<T>> dicLo, dicUp;
+    std::vector<DBuf<T>> rdPos, dicR, dicLoB, dicLoX, dicUpB, dicUpX;
     // FP32 form only: dense Cholesky of the coarsest level
     bool built = false;
 };
@@ -105,6 +109,9 @@ struct Matrix
                                      unsigned long long* trace, bool timed);
     template <class T> void ensureSym(int level);   // the reversed layout of `level` in T
     void prepareSmoother(const b2g_controls& c);
+    std::vector<DBuf<double>> rdCell;              // DIC's reciprocal diagonal by cell, per level (FP64)
+    template <class T> void ensureDic(int level);
+    template <class T> void dicSmooth(int level, T* psi, const T* source, int nSweeps);
     template <class T> void symSmooth(int level, T* psi, const T* source, int nSweeps);
     void mcLaunch(int level, bool fused, int block, float* psi, const float* source, int nSweeps, bool timed,
                   bool symmetric = false);

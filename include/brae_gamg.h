@@ -324,7 +324,8 @@ B2G_API b2g_status b2g_batch_destroy(b2g_batch* batch);
  * and solve the group as one batch (b2g_batch_*: each level step one launch over all of them, each
  * PCG iteration one CUDA graph). Requests that arrive while others are on the GPU join the next
  * group, and the slots' groups overlap on the device. A case is solved by one slot at a time; its
- * result is the same in any group (b2g_batch_solve's). Standalone GAMG requests are solved alone. */
+ * result is the same in any group (b2g_batch_solve's). Standalone GAMG requests and requests with a
+ * smoother other than GaussSeidel are solved alone (the single-case solve). */
 typedef struct b2g_server b2g_server;
 B2G_API b2g_status b2g_server_create(unsigned long long hbmCapBytes, int nSlots, b2g_server** out);
 /* Stops the workers (queued requests are dropped) and frees every case. */

@@ -104,11 +104,12 @@ def test_level_kernels_bitexact(b2g, oracle, name, kw):
             A.smooth(lv, psi, dev(b), sweeps)
             want = oracle.smooth(lo, up, d, u, x, b, sweeps, "GaussSeidel")
             assert np.array_equal(host(psi), want), f"GaussSeidel level {lv} sweeps {sweeps}"
-        for sweeps in (1, 2):
-            psi = dev(x)
-            A.smooth(lv, psi, dev(b), sweeps, smoother="symGaussSeidel")
-            want = oracle.smooth(lo, up, d, u, x, b, sweeps, "symGaussSeidel")
-            assert np.array_equal(host(psi), want), f"symGaussSeidel level {lv} sweeps {sweeps}"
+        for sm in ("symGaussSeidel", "DIC", "DICGaussSeidel"):
+            for sweeps in (1, 2):
+                psi = dev(x)
+                A.smooth(lv, psi, dev(b), sweeps, smoother=sm)
+                want = oracle.smooth(lo, up, d, u, x, b, sweeps, sm)
+                assert np.array_equal(host(psi), want), f"{sm} level {lv} sweeps {sweeps}"
         # scale: dots differ in summation order only
         f = dev(x)
         acf = torch.empty_like(f)
@@ -193,11 +194,28 @@ def test_pcg_gamg_solve_parity_options(b2g, oracle, reduction):
 
 @pytest.mark.parametrize("reduction", ["serial", "tree"])
 @pytest.mark.parametrize("name,kw", BOXES[1:4], ids=[b[0] for b in BOXES[1:4]])
-def test_pcg_gamg_sym_gauss_seidel_parity(b2g, oracle, name, kw, reduction):
-    # the symmetric smoother: its backward walk runs as a forward sweep of the reversed level
+@pytest.mark.parametrize("smoother", ["symGaussSeidel", "DIC", "DICGaussSeidel"])
+def test_pcg_gamg_other_smoothers_parity(b2g, oracle, name, kw, reduction, smoother):
+    # symGaussSeidel's backward walk and DIC's backward substitution run as forward sweeps of
+    # reversed levels, DIC's forward substitution as one of a lower-only level
     c = cases.box_case(**kw)
-    _solve_parity(b2g, oracle, c, 1e-8, 0.0, dict(smoother="symGaussSeidel"), reduction=reduction)
-    _solve_parity(b2g, oracle, c, 1e-8, 0.0, dict(smoother="symGaussSeidel", nPreSweeps=1), reduction=reduction)
+    _solve_parity(b2g, oracle, c, 1e-8, 0.0, dict(smoother=smoother), reduction=reduction)
+    _solve_parity(b2g, oracle, c, 1e-8, 0.0, dict(smoother=smoother, nPreSweeps=1), reduction=reduction)
+
+
+@pytest.mark.parametrize("smoother", ["DIC", "DICGaussSeidel"])
+def test_standalone_gamg_dic_parity(b2g, oracle, smoother):
+    # interFoam's p_rghFinal default: solver GAMG; smoother DIC
+    c = cases.box_case(16, 14, 12, (2.0, 1.0, 1.0), 8.0)
+    mesh, agg = _pair(b2g, oracle, c)
+    want = oracle.gamg_solve(agg, c.diag, c.coef, c.source, np.zeros(c.n_cells),
+                             oc_controls(tolerance=1e-8, relTol=0.0, smoother=smoother))
+    psi = np.zeros(c.n_cells)
+    ctl = b2g.controls_default(solver=1, tolerance=1e-8, relTol=0.0, reduction="serial", smoother=smoother)
+    perf, hist = b2g.gamg_solve(mesh, c.diag, c.coef, c.source, psi, ctl)
+    assert tuple(perf) == want["perf"]
+    assert hist == list(want["history"])
+    assert np.array_equal(psi, want["psi"])
 
 
 @pytest.mark.parametrize("precision", ["fp32_precond", "fp32_precond_multicolour"])
