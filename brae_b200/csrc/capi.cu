@@ -31,6 +31,41 @@ using b2g::capi::need;
 
 cudaStream_t streamOf(void* s) { return s ? static_cast<cudaStream_t>(s) : cudaStreamPerThread; }
 
+__global__ void kCheckCells(int n, int nCells, const int* __restrict__ cells, int* __restrict__ err)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && (cells[i] < 0 || cells[i] >= nCells)) atomicOr(err, 1);
+}
+
+__global__ void kIotaInt(int n, int* __restrict__ v)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = i;
+}
+
+// foldBoundary (gamg_solver_cpp.cu:769-797) per cell: its boundary faces in (patch, face) order,
+// every patch's internal coefficient onto the diagonal, the uncoupled patches' boundary coefficient
+// onto the source, one after another as the reference's loop adds them
+__global__ void kFold(int nCells, const int* __restrict__ start, const int* __restrict__ order,
+                      const double* __restrict__ ic, const double* __restrict__ bc,
+                      const unsigned char* __restrict__ coupled, double* __restrict__ diag,
+                      double* __restrict__ source)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nCells) return;
+    const int e0 = start[c], e1 = start[c + 1];
+    if (e0 == e1) return;
+    double d = diag[c], s = source[c];
+    for (int e = e0; e < e1; ++e)
+    {
+        const int i = order[e];
+        d = __dadd_rn(d, ic[i]);
+        if (!coupled[i]) s = __dadd_rn(s, bc[i]);
+    }
+    diag[c] = d;
+    source[c] = s;
+}
+
 template <class T>
 void stage(b2g::DBuf<T>& d, const T* src, size_t n, int memspace, cudaStream_t s)
 {
@@ -603,6 +638,56 @@ b2g_status b2g_level_sweep_shape(const b2g_mesh* mesh, int level, int* oneBlock,
         *oneBlock = C.tuned && C.fused ? 1 : 0;
         *threadsPerBlock = C.tuned ? (C.fused ? 1024 : C.block) : 0;
         *msPerSweep = C.tuned ? C.msPerSweep : 0.f;
+    });
+}
+
+b2g_status b2g_fold_boundary(int nCells, int nBFaces, const int32_t* faceCells, const double* internalCoeffs,
+                             const double* boundaryCoeffs, const unsigned char* coupled, double* diag, double* source,
+                             int memspace, void* stream)
+{
+    return guarded([&] {
+        need(nCells > 0 && nBFaces >= 0, "b2g_fold_boundary: nCells must be positive and nBFaces non-negative");
+        need(diag && source, "b2g_fold_boundary: null diag or source");
+        need(nBFaces == 0 || (faceCells && internalCoeffs && boundaryCoeffs && coupled),
+             "b2g_fold_boundary: null boundary array");
+        need(memspace == B2G_MEM_HOST || memspace == B2G_MEM_DEVICE, "b2g_fold_boundary: bad memspace");
+        cudaStream_t s = streamOf(stream);
+        b2g::DBuf<int> cells, order;
+        b2g::DBuf<double> ic, bc, d, src;
+        b2g::DBuf<unsigned char> cp;
+        stage(cells, faceCells, nBFaces, memspace, s);
+        stage(ic, internalCoeffs, nBFaces, memspace, s);
+        stage(bc, boundaryCoeffs, nBFaces, memspace, s);
+        stage(cp, coupled, nBFaces, memspace, s);
+        stage(d, static_cast<const double*>(diag), nCells, memspace, s);
+        stage(src, static_cast<const double*>(source), nCells, memspace, s);
+        b2g::DBuf<int> err;
+        err.alloc(1, s);
+        err.zero(s);
+        if (nBFaces) kCheckCells<<<b2g::ceilDiv(nBFaces, 256), 256, 0, s>>>(nBFaces, nCells, cells.p, err.p);
+        B2G_LAUNCH_CHECK();
+        int e = 0;
+        B2G_CUDA(cudaMemcpyAsync(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        B2G_CUDA(cudaStreamSynchronize(s));
+        need(e == 0, "b2g_fold_boundary: a face cell is outside [0, nCells)");
+        // each cell's boundary faces in (patch, face) order: a stable sort of the face indices by cell
+        b2g::DBuf<int> start, iota;
+        b2g::DBuf<unsigned> keys;
+        start.alloc(nCells + 1, s);
+        b2g::countingStarts(cells.p, nBFaces, nCells, start.p, s);
+        order.alloc(std::max(nBFaces, 1), s);
+        iota.alloc(std::max(nBFaces, 1), s);
+        keys.alloc(std::max(nBFaces, 1), s);
+        if (nBFaces) kIotaInt<<<b2g::ceilDiv(nBFaces, 256), 256, 0, s>>>(nBFaces, iota.p);
+        int bits = 1;
+        while ((1LL << bits) < nCells) ++bits;
+        b2g::sortPairs(reinterpret_cast<const unsigned*>(cells.p), keys.p, iota.p, order.p, nBFaces, bits, s);
+        kFold<<<b2g::ceilDiv(nCells, 256), 256, 0, s>>>(nCells, start.p, order.p, ic.p, bc.p, cp.p, d.p, src.p);
+        B2G_LAUNCH_CHECK();
+        const cudaMemcpyKind back = memspace == B2G_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+        B2G_CUDA(cudaMemcpyAsync(diag, d.p, sizeof(double) * nCells, back, s));
+        B2G_CUDA(cudaMemcpyAsync(source, src.p, sizeof(double) * nCells, back, s));
+        B2G_CUDA(cudaStreamSynchronize(s));
     });
 }
 

@@ -96,6 +96,7 @@ def _load():
         "b2g_level_pcg_dic_static": (ip, [vp, ip, vp, vp, dp, dp, C.POINTER(_Perf)]),
         "b2g_level_schedule": (ip, [vp, ip, vp, vp]),
         "b2g_level_colouring": (ip, [vp, ip, C.POINTER(C.c_int), vp]),
+        "b2g_fold_boundary": (ip, [ip, ip, vp, vp, vp, vp, vp, vp, ip, vp]),
         "b2g_level_sweep_shape": (ip, [vp, ip, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float)]),
         "b2g_precondition": (ip, [vp, C.POINTER(Controls), vp, vp, C.POINTER(_Log)]),
         "b2g_matrix_pcg_solve": (ip, [vp, vp, vp, C.POINTER(Controls), ip, C.POINTER(_Perf),
@@ -129,7 +130,7 @@ EXPORTED = [
     "b2g_level_amul", "b2g_level_smooth", "b2g_level_scale", "b2g_step_restrict",
     "b2g_step_prolong", "b2g_level_norm_factor", "b2g_level_pcg_dic", "b2g_precondition",
     "b2g_matrix_pcg_solve", "b2g_matrix_timings", "b2g_level_smooth_trace", "b2g_level_pcg_dic_static",
-    "b2g_level_schedule", "b2g_level_colouring", "b2g_level_sweep_shape", "b2g_server_create", "b2g_server_destroy", "b2g_server_add_case",
+    "b2g_level_schedule", "b2g_level_colouring", "b2g_fold_boundary", "b2g_level_sweep_shape", "b2g_server_create", "b2g_server_destroy", "b2g_server_add_case",
     "b2g_server_submit", "b2g_server_wait", "b2g_server_case_bytes", "b2g_batch_create", "b2g_batch_solve",
     "b2g_batch_launches", "b2g_batch_destroy",
 ]
@@ -418,6 +419,20 @@ def gamg_solve(mesh: Mesh, diag, upper, source, psi, controls: Controls,
     _check(lib.b2g_gamg_solve(mesh.handle, _ptr(diag), _ptr(upper), _ptr(source), _ptr(psi),
                               C.byref(controls), ms, _stream(), C.byref(p), C.byref(lb.log)))
     return SolverPerformance(p.initialResidual, p.finalResidual, p.nIterations), lb.history()
+
+
+def fold_boundary(diag, source, face_cells, internal_coeffs, boundary_coeffs, coupled):
+    """foldBoundary (gamg_solver_cpp.cu:769-797) on the device: returns the folded (diag, source).
+    The boundary arrays are all patches' faces concatenated in patch order; `coupled` per face."""
+    d = np.array(diag, dtype=np.float64, copy=True)
+    s = np.array(source, dtype=np.float64, copy=True)
+    fc = np.ascontiguousarray(face_cells, np.int32)
+    ic = np.ascontiguousarray(internal_coeffs, np.float64)
+    bc = np.ascontiguousarray(boundary_coeffs, np.float64)
+    cp = np.ascontiguousarray(coupled, np.uint8)
+    _check(lib.b2g_fold_boundary(d.shape[0], fc.shape[0], _ptr(fc), _ptr(ic), _ptr(bc), _ptr(cp), _ptr(d), _ptr(s),
+                                 B2G_MEM_HOST, None))
+    return d, s
 
 
 class Server:

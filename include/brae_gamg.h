@@ -294,6 +294,19 @@ B2G_API b2g_status b2g_level_smooth_trace(b2g_matrix* m, int level, double* psi,
  * gathers, depth, upstream depth, same-part wait, depth change, blob offsets). */
 B2G_API b2g_status b2g_level_schedule(const b2g_mesh* mesh, int level, int* partChunkStart, int* chunkRecords);
 
+/* ---- the step before the solve ------------------------------------------------------------------ */
+
+/* foldBoundary (gamg_solver_cpp.cu:769-797, fvMatrix::solveSegregated's addBoundaryDiag and
+ * addBoundarySource) on the device: the nBFaces boundary faces of all patches concatenated in patch
+ * order, each with its cell (faceCells), internal and boundary coefficient and a flag that is
+ * nonzero where its patch is coupled. diag [nCells] (the matrix's) becomes the folded diagonal:
+ * plus every face's internal coefficient; source [nCells] plus the uncoupled faces' boundary
+ * coefficients, added per cell in (patch, face) order as the reference's loop does. All arrays in
+ * `memspace`; diag and source in/out. */
+B2G_API b2g_status b2g_fold_boundary(int nCells, int nBFaces, const int32_t* faceCells, const double* internalCoeffs,
+                                     const double* boundaryCoeffs, const unsigned char* coupled, double* diag,
+                                     double* source, int memspace, void* stream);
+
 /* ---- the batched form: many independent cases in one solve ------------------------------------ */
 
 /* A batch of matrices (each on its own mesh), solved together: every step of every level is one
