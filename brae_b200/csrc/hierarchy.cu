@@ -1286,95 +1286,196 @@ void buildGsSchedule(LevelAddr& L, cudaStream_t s)
     B2G_CUDA(cudaStreamSynchronize(s));
 }
 
+namespace {
+
+// greedy colouring, one depth group at a time: a cell's neighbours of smaller depth are coloured,
+// those of larger depth not yet, and cells of one depth share no face; the cell takes the smallest
+// colour its coloured neighbours do not have
+__global__ void kColourDepth(int b, int e, const int* __restrict__ byDepth, const int* __restrict__ rowStart,
+                             const int* __restrict__ col, int* __restrict__ colour, int* __restrict__ err)
+{
+    const int i = b + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= e) return;
+    const int c = byDepth[i];
+    unsigned long long used = 0ull;
+    for (int q = rowStart[c]; q < rowStart[c + 1]; ++q)
+    {
+        const int k = colour[col[q]];
+        if (k >= 0) used |= 1ull << k;
+    }
+    if (used == ~0ull)
+    {
+        atomicOr(err, 1);
+        colour[c] = 63;
+        return;
+    }
+    colour[c] = __ffsll(static_cast<long long>(~used)) - 1;
+}
+
+__global__ void kCheckColours(int nF, const int* __restrict__ lower, const int* __restrict__ upper,
+                              const int* __restrict__ colour, int* __restrict__ err, int* __restrict__ maxColour)
+{
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nF) return;
+    const int a = colour[lower[f]], b = colour[upper[f]];
+    if (a == b || a < 0 || b < 0) atomicOr(err, 2);
+    atomicMax(maxColour, max(a, b));
+}
+
+__global__ void kColourOfPos(int n, const int* __restrict__ posCell, const int* __restrict__ colour,
+                             unsigned* __restrict__ key, int* __restrict__ iota, int* __restrict__ maxColour)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const int k = colour[posCell[p]];
+    key[p] = static_cast<unsigned>(k);
+    iota[p] = p;
+    atomicMax(maxColour, k);
+}
+
+// the colour-major rows: sorted position i of colour k goes to padded row padStart[k] + i - start[k]
+__global__ void kScatterRows(int n, const unsigned* __restrict__ sortedKey, const int* __restrict__ sortedPos,
+                             const int* __restrict__ start, const int* __restrict__ padStart, int* __restrict__ rowPos)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int k = static_cast<int>(sortedKey[i]);
+    rowPos[padStart[k] + i - start[k]] = sortedPos[i];
+}
+
+// a slice's width: the longest row of its 32
+__global__ void kSliceWidth(int nSlices, const int* __restrict__ rowPos, const int* __restrict__ posCell,
+                            const int* __restrict__ rowStart, int* __restrict__ width32)
+{
+    const int sl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sl >= nSlices) return;
+    int w = 0;
+    for (int l = 0; l < 32; ++l)
+    {
+        const int p = rowPos[32 * sl + l];
+        if (p >= 0)
+        {
+            const int c = posCell[p];
+            w = max(w, rowStart[c + 1] - rowStart[c]);
+        }
+    }
+    width32[sl] = 32 * w;
+}
+
+__global__ void kFillSlices(int nRows, const int* __restrict__ rowPos, const int* __restrict__ sliceBase,
+                            const int* __restrict__ posCell, const int* __restrict__ posOf,
+                            const int* __restrict__ rowStart, const int* __restrict__ col,
+                            const int* __restrict__ entFace, int* __restrict__ colP, int* __restrict__ faceP)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nRows) return;
+    const int sl = r >> 5, lane = r & 31;
+    const int base = sliceBase[sl];
+    const int w = (sliceBase[sl + 1] - base) >> 5;
+    const int p = rowPos[r];
+    const int c = p >= 0 ? posCell[p] : -1;
+    const int len = c >= 0 ? rowStart[c + 1] - rowStart[c] : 0;
+    for (int q = 0; q < w; ++q)
+    {
+        const int e = base + 32 * q + lane;
+        if (q < len)
+        {
+            colP[e] = posOf[col[rowStart[c] + q]];
+            faceP[e] = entFace[rowStart[c] + q];
+        }
+        else
+        {
+            colP[e] = p >= 0 ? p : 0;  // reads a value with coefficient zero
+            faceP[e] = -1;
+        }
+    }
+}
+
+}  // namespace
+
+// On the device: greedy colouring in depth order (a structured hex level gets a checkerboard's two
+// colours), checked face by face; then the colour-major sliced-ELL rows in position order.
 void buildColouring(LevelAddr& L, cudaStream_t s)
 {
     Colouring& C = L.mc;
     if (C.nColours > 0) return;
-    const int n = L.nCells;
-    const std::vector<int> rowStart = L.rowStart.download(s);
-    const std::vector<int> col = L.col.download(s);
-    const std::vector<int> entFace = L.entFace.download(s);
-    const std::vector<int> posOf = L.gs.posOf.download(s);
-    // greedy colouring in cell order: the smallest colour no earlier neighbour has
-    std::vector<int> colour(n, -1);
-    std::vector<int> mark;
-    int nColours = 0;
-    for (int c = 0; c < n; ++c)
+    const int n = L.nCells, nF = L.nFaces;
+    const GsSchedule& G = L.gs;
+    DBuf<int> colour, byDepth, depthStart, err, maxC;
+    colour.alloc(std::max(n, 1), s);
+    kFillInt<<<grid(n), TPB, 0, s>>>(colour.p, n, -1);
+    err.alloc(1, s);
+    err.zero(s);
+    maxC.alloc(1, s);
+    maxC.zero(s);
     {
-        for (int e = rowStart[c]; e < rowStart[c + 1]; ++e)
-        {
-            const int k = colour[col[e]];
-            if (k >= 0)
-            {
-                if (k >= static_cast<int>(mark.size())) mark.resize(k + 1, -1);
-                mark[k] = c;
-            }
-        }
-        int k = 0;
-        while (k < static_cast<int>(mark.size()) && mark[k] == c) ++k;
-        colour[c] = k;
-        nColours = std::max(nColours, k + 1);
+        DBuf<int> iota;
+        DBuf<unsigned> kout;
+        iota.alloc(std::max(n, 1), s);
+        kout.alloc(std::max(n, 1), s);
+        byDepth.alloc(std::max(n, 1), s);
+        kIota<<<grid(n), TPB, 0, s>>>(iota.p, n);
+        B2G_LAUNCH_CHECK();
+        sortPairs(reinterpret_cast<const unsigned*>(G.depth.p), kout.p, iota.p, byDepth.p, n, bitsFor(G.maxDepth + 1), s);
+        depthStart.alloc(G.maxDepth + 2, s);
+        countingStarts(G.depth.p, n, G.maxDepth + 1, depthStart.p, s);
     }
-    // a colour's rows in position order: a sweep then reads b and writes psi nearly in sequence, and
-    // the neighbours it reads sit in the adjacent depth groups
-    std::vector<std::vector<int>> cellsOf(nColours);
+    const std::vector<int> hDepth = depthStart.download(s);
+    for (int d = 0; d <= G.maxDepth; ++d)
     {
-        std::vector<int> byPos(n);
-        for (int c = 0; c < n; ++c) byPos[posOf[c]] = c;
-        for (int i = 0; i < n; ++i) cellsOf[colour[byPos[i]]].push_back(byPos[i]);
+        const int b = hDepth[d], e = hDepth[d + 1];
+        if (e > b) kColourDepth<<<grid(e - b), TPB, 0, s>>>(b, e, byDepth.p, L.rowStart.p, L.col.p, colour.p, err.p);
     }
+    B2G_LAUNCH_CHECK();
+    if (nF) kCheckColours<<<grid(nF), TPB, 0, s>>>(nF, L.lower.p, L.upper.p, colour.p, err.p, maxC.p);
+    B2G_LAUNCH_CHECK();
+    const int e = readInt(err.p, s);
+    if (e & 1) fail(B2G_ERR_ARGUMENT, "b2g: a level needs more than 63 colours for the multicolour sweep.");
+    if (e & 2) fail(B2G_ERR_STATE, "b2g: the multicolour layout has two neighbours of one colour.");
+    // positions by colour, ascending within a colour (stable sort)
+    DBuf<unsigned> key, skey;
+    DBuf<int> iota, spos;
+    key.alloc(std::max(n, 1), s);
+    skey.alloc(std::max(n, 1), s);
+    iota.alloc(std::max(n, 1), s);
+    spos.alloc(std::max(n, 1), s);
+    if (n) kColourOfPos<<<grid(n), TPB, 0, s>>>(n, G.posCell.p, colour.p, key.p, iota.p, maxC.p);
+    B2G_LAUNCH_CHECK();
+    const int nColours = readInt(maxC.p, s) + 1;
+    sortPairs(key.p, skey.p, iota.p, spos.p, n, bitsFor(nColours), s);
+    DBuf<int> start;
+    start.alloc(nColours + 1, s);
+    countingStarts(reinterpret_cast<const int*>(key.p), n, nColours, start.p, s);
+    const std::vector<int> hStart = start.download(s);
     C.colourStart.assign(1, 0);
-    std::vector<int> pos, sliceBase(1, 0), colP, faceP;
     for (int k = 0; k < nColours; ++k)
-    {
-        const std::vector<int>& cells = cellsOf[k];
-        const int padded = ((static_cast<int>(cells.size()) + 31) / 32) * 32;
-        for (int b = 0; b < padded; b += 32)
-        {
-            int w = 0;
-            for (int l = 0; l < 32 && b + l < static_cast<int>(cells.size()); ++l)
-                w = std::max(w, rowStart[cells[b + l] + 1] - rowStart[cells[b + l]]);
-            const size_t base = colP.size();
-            colP.resize(base + 32 * static_cast<size_t>(w));
-            faceP.resize(base + 32 * static_cast<size_t>(w));
-            for (int l = 0; l < 32; ++l)
-            {
-                const bool real = b + l < static_cast<int>(cells.size());
-                const int cell = real ? cells[b + l] : -1;
-                pos.push_back(real ? posOf[cell] : -1);
-                const int len = real ? rowStart[cell + 1] - rowStart[cell] : 0;
-                for (int q = 0; q < w; ++q)
-                {
-                    const size_t e = base + 32 * static_cast<size_t>(q) + l;
-                    if (q < len)
-                    {
-                        colP[e] = posOf[col[rowStart[cell] + q]];
-                        faceP[e] = entFace[rowStart[cell] + q];
-                    }
-                    else
-                    {
-                        colP[e] = real ? posOf[cell] : 0;  // reads a value with coefficient zero
-                        faceP[e] = -1;
-                    }
-                }
-            }
-            if (colP.size() >= (1ull << 31)) fail(B2G_ERR_ARGUMENT, "b2g: the multicolour layout exceeds 2^31 entries.");
-            sliceBase.push_back(static_cast<int>(colP.size()));
-        }
-        C.colourStart.push_back(static_cast<int>(pos.size()));
-    }
-    C.nRows = static_cast<int>(pos.size());
-    C.nEnt = static_cast<long long>(colP.size());
-    C.pos.upload(pos.data(), pos.size(), s);
+        C.colourStart.push_back(C.colourStart.back() + ((hStart[k + 1] - hStart[k] + 31) / 32) * 32);
+    C.nRows = C.colourStart.back();
     C.colourStartD.upload(C.colourStart.data(), C.colourStart.size(), s);
-    C.sliceBase.upload(sliceBase.data(), sliceBase.size(), s);
-    if (colP.empty())
+    C.pos.alloc(std::max(C.nRows, 1), s);
+    kFillInt<<<grid(std::max(C.nRows, 1)), TPB, 0, s>>>(C.pos.p, std::max(C.nRows, 1), -1);
+    if (n) kScatterRows<<<grid(n), TPB, 0, s>>>(n, skey.p, spos.p, start.p, C.colourStartD.p, C.pos.p);
+    B2G_LAUNCH_CHECK();
+    const int nSlices = C.nRows / 32;
+    DBuf<int> width32;
+    width32.alloc(std::max(nSlices, 1), s);
+    if (nSlices) kSliceWidth<<<grid(nSlices), TPB, 0, s>>>(nSlices, C.pos.p, G.posCell.p, L.rowStart.p, width32.p);
+    B2G_LAUNCH_CHECK();
+    C.sliceBase.alloc(nSlices + 1, s);
+    const long long nEnt = exclusiveScan(width32.p, C.sliceBase.p, nSlices, s);
+    if (nEnt >= (1LL << 31)) fail(B2G_ERR_ARGUMENT, "b2g: the multicolour layout exceeds 2^31 entries.");
+    C.nEnt = nEnt;
+    C.col.alloc(std::max<long long>(nEnt, 1), s);
+    C.face.alloc(std::max<long long>(nEnt, 1), s);
+    if (nEnt == 0)
     {
-        colP.push_back(0);
-        faceP.push_back(-1);
+        kFillInt<<<1, 1, 0, s>>>(C.col.p, 1, 0);
+        kFillInt<<<1, 1, 0, s>>>(C.face.p, 1, -1);
     }
-    C.col.upload(colP.data(), colP.size(), s);
-    C.face.upload(faceP.data(), faceP.size(), s);
+    if (C.nRows)
+        kFillSlices<<<grid(C.nRows), TPB, 0, s>>>(C.nRows, C.pos.p, C.sliceBase.p, G.posCell.p, G.posOf.p,
+                                                  L.rowStart.p, L.col.p, L.entFace.p, C.col.p, C.face.p);
+    B2G_LAUNCH_CHECK();
     B2G_CUDA(cudaStreamSynchronize(s));
     C.nColours = nColours;
 }

@@ -74,7 +74,7 @@ enum
      * colouring of each level (two colours on a structured hex level) whose cells of one colour
      * share no face, each colour one parallel update of its cells. The same GaussSeidel update in
      * another cell order; bandwidth-bound where the sequential order is bound by the sweep's
-     * dependency chain. Built on first use (a host pass over every level's faces). */
+     * dependency chain. Built on first use (a greedy colouring by sweep depth, on the device). */
     B2G_PRECISION_FP32_PRECOND_MULTICOLOUR = 2
 };
 
