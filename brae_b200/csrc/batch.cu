@@ -1005,41 +1005,83 @@ void Batch::prepareMulticolour()
             f.mcRows = C.nRows;
         }
     segF.upload(hostF.data(), hostF.size(), stream);
+    // the batch's own autotuner: per level, the largest case that one block sweeps whole (one launch
+    // for all of them) while the larger ones go by tiles, one launch per colour; every candidate is
+    // timed on the level's own data and the fastest kept
+    multicolour = true;
+    B2G_CUDA(cudaMemsetAsync(active.p, 0xff, sizeof(int) * K, stream));  // every case swept while timing
+    cudaEvent_t e0, e1;
+    B2G_CUDA(cudaEventCreate(&e0));
+    B2G_CUDA(cudaEventCreate(&e1));
+    const long long l0 = launches;
+    mcThreshold.assign(maxLevels + 1, 0);
+    mcSweepMs.assign(maxLevels + 1, 0.f);
     for (int lv = 0; lv <= maxLevels; ++lv)
     {
-        // small cases: one block each sweeps the whole level; large ones: a launch per colour
-        std::vector<int> small;
-        auto isSmall = [&](int c) { return cases[c]->mesh->lev[lv].mc.fused; };
-        int nCol = 0;
-        for (int c = 0; c < K; ++c)
+        if (lev[lv].nParts == 0) continue;
+        float best = 0.f;
+        int bestThr = -1;
+        for (int thr : {0, 4096, 16384, k::kMcSmallRows})
         {
-            if (nLevelsOf[c] < lv + 1) continue;
-            if (isSmall(c)) small.push_back(segOfCase[c][lv]);
-            else nCol = std::max(nCol, cases[c]->mesh->lev[lv].mc.nColours);
-        }
-        lev[lv].nMcSmall = static_cast<int>(small.size());
-        if (!small.empty()) lev[lv].mcSmall.upload(small.data(), small.size(), stream);
-        lev[lv].mc.clear();
-        lev[lv].mc.resize(nCol);
-        for (int k = 0; k < nCol; ++k)
-        {
-            std::vector<int4> tiles;
-            for (int c = 0; c < K; ++c)
+            buildMcLists(lv, thr);
+            smooth<float>(lv, 1);  // warm
+            B2G_CUDA(cudaEventRecord(e0, stream));
+            smooth<float>(lv, 2);
+            B2G_CUDA(cudaEventRecord(e1, stream));
+            B2G_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            B2G_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (bestThr < 0 || ms < best)
             {
-                if (nLevelsOf[c] < lv + 1 || isSmall(c)) continue;
-                const Colouring& C = cases[c]->mesh->lev[lv].mc;
-                if (k >= C.nColours) continue;
-                const int sg = segOfCase[c][lv];
-                for (int b = C.colourStart[k]; b < C.colourStart[k + 1]; b += kTile)
-                    tiles.push_back(make_int4(sg, b, std::min(C.colourStart[k + 1], b + kTile), 0));
+                best = ms;
+                bestThr = thr;
             }
-            TileList& L = lev[lv].mc[k];
-            L.nTiles = static_cast<int>(tiles.size());
-            if (!tiles.empty()) L.tiles.upload(tiles.data(), tiles.size(), stream);
         }
+        buildMcLists(lv, bestThr);
+        mcThreshold[lv] = bestThr;
+        mcSweepMs[lv] = best / 2.f;
     }
+    launches = l0;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     B2G_CUDA(cudaStreamSynchronize(stream));
     mcReady = true;
+}
+
+// The multicolour launch lists of level lv: cases with at most `threshold` rows are swept whole by
+// one block each (one launch for all), the others by tiles of their rows, one launch per colour.
+void Batch::buildMcLists(int lv, int threshold)
+{
+    const int K = static_cast<int>(cases.size());
+    std::vector<int> small;
+    auto isSmall = [&](int c) { return cases[c]->mesh->lev[lv].mc.nRows <= threshold; };
+    int nCol = 0;
+    for (int c = 0; c < K; ++c)
+    {
+        if (nLevelsOf[c] < lv + 1) continue;
+        if (isSmall(c)) small.push_back(segOfCase[c][lv]);
+        else nCol = std::max(nCol, cases[c]->mesh->lev[lv].mc.nColours);
+    }
+    lev[lv].nMcSmall = static_cast<int>(small.size());
+    if (!small.empty()) lev[lv].mcSmall.upload(small.data(), small.size(), stream);
+    lev[lv].mc.clear();
+    lev[lv].mc.resize(nCol);
+    for (int k = 0; k < nCol; ++k)
+    {
+        std::vector<int4> tiles;
+        for (int c = 0; c < K; ++c)
+        {
+            if (nLevelsOf[c] < lv + 1 || isSmall(c)) continue;
+            const Colouring& C = cases[c]->mesh->lev[lv].mc;
+            if (k >= C.nColours) continue;
+            const int sg = segOfCase[c][lv];
+            for (int b = C.colourStart[k]; b < C.colourStart[k + 1]; b += kTile)
+                tiles.push_back(make_int4(sg, b, std::min(C.colourStart[k + 1], b + kTile), 0));
+        }
+        TileList& L = lev[lv].mc[k];
+        L.nTiles = static_cast<int>(tiles.size());
+        if (!tiles.empty()) L.tiles.upload(tiles.data(), tiles.size(), stream);
+    }
 }
 
 Batch::~Batch()

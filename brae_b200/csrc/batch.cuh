@@ -144,6 +144,9 @@ struct Batch
     void reduce(int op, int a, int b, size_t member);
     void iteration(const b2g_controls& c);
     void prepareMulticolour();
+    void buildMcLists(int lv, int threshold);
+    std::vector<int> mcThreshold;           // per level: the tuned largest case swept by one block
+    std::vector<float> mcSweepMs;           // per level: the tuned sweep's measured time
 };
 
 }  // namespace b2g

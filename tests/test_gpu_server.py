@@ -37,7 +37,7 @@ def _add(srv, c):
     return srv.add_case(c.lower, c.upper, c.Sf, c.magSf, c.n_cells, c.diag, c.coef)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32_precond"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32_precond", "fp32_precond_multicolour"])
 @pytest.mark.parametrize("reduction", ["serial", "tree"])
 def test_same_alone_and_in_the_mix(b2g, oracle, precision, reduction):
     built = [cases.box_case(**kw) for kw in MIX]
