@@ -5,6 +5,7 @@
 #include "capi_internal.cuh"
 
 #include <cctype>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -30,6 +31,118 @@ using b2g::capi::guarded;
 using b2g::capi::need;
 
 cudaStream_t streamOf(void* s) { return s ? static_cast<cudaStream_t>(s) : cudaStreamPerThread; }
+
+// ---------------------------------------------------------------------------------------------
+// the hierarchy cache: a content signature of the agglomeration's inputs and the file that keeps
+// each step's restriction map
+// ---------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z)
+{
+    // the SplitMix64 finaliser
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+// XOR of a hash of every (array, index, word): independent of the order the threads run in
+__global__ void kSignature(long long nWords, const unsigned* __restrict__ words, unsigned long long salt,
+                           unsigned long long* __restrict__ out)
+{
+    unsigned long long acc = 0ull;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nWords; i += (long long)gridDim.x * blockDim.x)
+        acc ^= mix64(salt ^ mix64(static_cast<unsigned long long>(i) * 0x9e3779b97f4a7c15ull + words[i]));
+    for (int o = 16; o > 0; o >>= 1) acc ^= __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0 && acc) atomicXor(out, acc);
+}
+
+unsigned long long meshSignature(int nCells, int nFaces, const int* lower, const int* upper, const double* Sf,
+                                 const double* magSf, int nCoarsest, int forward, cudaStream_t s)
+{
+    b2g::DBuf<unsigned long long> acc;
+    acc.alloc(1, s);
+    acc.zero(s);
+    const struct
+    {
+        const void* p;
+        long long words;
+        unsigned long long salt;
+    } arrays[] = {{lower, nFaces, 0x6c6f776572ull}, {upper, nFaces, 0x7570706572ull},
+                  {Sf, 6LL * nFaces, 0x5366ull}, {magSf, 2LL * nFaces, 0x6d61675366ull}};
+    for (const auto& a : arrays)
+        if (a.words)
+            kSignature<<<std::min<long long>(b2g::ceilDiv(a.words, 256), 4096), 256, 0, s>>>(
+                a.words, static_cast<const unsigned*>(a.p), a.salt, acc.p);
+    B2G_LAUNCH_CHECK();
+    unsigned long long h = 0;
+    B2G_CUDA(cudaMemcpyAsync(&h, acc.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    B2G_CUDA(cudaStreamSynchronize(s));
+    // the sizes and controls that also decide the agglomeration
+    const unsigned long long scal[4] = {static_cast<unsigned long long>(nCells), static_cast<unsigned long long>(nFaces),
+                                        static_cast<unsigned long long>(nCoarsest),
+                                        static_cast<unsigned long long>(forward ? 1 : 0)};
+    for (unsigned long long v : scal) h = (h ^ v) * 0x100000001b3ull + 0x9e3779b97f4a7c15ull;
+    return h;
+}
+
+struct CachedAgglomeration
+{
+    int forwardOut = 1;
+    std::vector<std::vector<int>> maps;
+    std::vector<int> nCoarse;
+};
+
+constexpr char kCacheMagic[8] = {'B', '2', 'G', 'A', 'G', 'G', '0', '1'};
+
+// The file: magic, signature, the direction flag after agglomerating, the step count, then per step
+// nFine, nCoarse and the restriction map. False when it is missing, unreadable or for other inputs.
+bool readCache(const char* path, unsigned long long sig, CachedAgglomeration& ca)
+{
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return false;
+    bool ok = false;
+    char magic[8];
+    unsigned long long fsig = 0;
+    int hdr[2] = {0, 0};
+    if (std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kCacheMagic, 8) == 0 &&
+        std::fread(&fsig, sizeof(fsig), 1, f) == 1 && fsig == sig && std::fread(hdr, sizeof(int), 2, f) == 2 &&
+        hdr[1] >= 0 && hdr[1] < 64)
+    {
+        ca.forwardOut = hdr[0];
+        ok = true;
+        for (int i = 0; i < hdr[1] && ok; ++i)
+        {
+            int sz[2];
+            if (std::fread(sz, sizeof(int), 2, f) != 2 || sz[0] < 0 || sz[1] < 1) { ok = false; break; }
+            std::vector<int> m(static_cast<size_t>(sz[0]));
+            if (sz[0] && std::fread(m.data(), sizeof(int), m.size(), f) != m.size()) { ok = false; break; }
+            for (int v : m)
+                if (v < 0 || v >= sz[1]) { ok = false; break; }
+            ca.maps.push_back(std::move(m));
+            ca.nCoarse.push_back(sz[1]);
+        }
+    }
+    std::fclose(f);
+    if (!ok) ca = CachedAgglomeration{};
+    return ok;
+}
+
+void writeCache(const char* path, unsigned long long sig, const CachedAgglomeration& ca)
+{
+    FILE* f = std::fopen(path, "wb");
+    if (!f) b2g::fail(B2G_ERR_STATE, std::string("b2g_mesh_create_cached: cannot write ") + path);
+    bool ok = std::fwrite(kCacheMagic, 1, 8, f) == 8 && std::fwrite(&sig, sizeof(sig), 1, f) == 1;
+    const int hdr[2] = {ca.forwardOut, static_cast<int>(ca.maps.size())};
+    ok = ok && std::fwrite(hdr, sizeof(int), 2, f) == 2;
+    for (size_t i = 0; i < ca.maps.size() && ok; ++i)
+    {
+        const int sz[2] = {static_cast<int>(ca.maps[i].size()), ca.nCoarse[i]};
+        ok = std::fwrite(sz, sizeof(int), 2, f) == 2 &&
+             std::fwrite(ca.maps[i].data(), sizeof(int), ca.maps[i].size(), f) == ca.maps[i].size();
+    }
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) b2g::fail(B2G_ERR_STATE, std::string("b2g_mesh_create_cached: cannot write ") + path);
+}
 
 __global__ void kCheckCells(int n, int nCells, const int* __restrict__ cells, int* __restrict__ err)
 {
@@ -262,7 +375,8 @@ namespace capi {
 
 std::unique_ptr<b2g_mesh> createMesh(int nCells, int nFaces, const int32_t* lower, const int32_t* upper,
                                      const double* Sf, const double* magSf, int nCellsInCoarsestLevel,
-                                     int* forwardInOut, int memspace, cudaStream_t stream)
+                                     int* forwardInOut, int memspace, cudaStream_t stream, const char* cachePath,
+                                     int* fromCache)
 {
     need(nCells > 0 && nFaces >= 0, "b2g_mesh_create: nCells must be positive and nFaces non-negative");
     need(nFaces == 0 || (lower && upper && Sf && magSf), "b2g_mesh_create: null array");
@@ -285,7 +399,36 @@ std::unique_ptr<b2g_mesh> createMesh(int nCells, int nFaces, const int32_t* lowe
     b2g::DBuf<double> dSf, dMag;
     stage(dSf, Sf, 3 * (size_t)nFaces, memspace, M.stream);
     stage(dMag, magSf, nFaces, memspace, M.stream);
-    b2g::buildHierarchy(M, dSf.p, dMag.p, nCellsInCoarsestLevel, forwardInOut);
+    if (fromCache) *fromCache = 0;
+    if (!cachePath)
+    {
+        b2g::buildHierarchy(M, dSf.p, dMag.p, nCellsInCoarsestLevel, forwardInOut);
+    }
+    else
+    {
+        const unsigned long long sig = meshSignature(nCells, nFaces, L0.lower.p, L0.upper.p, dSf.p, dMag.p,
+                                                     nCellsInCoarsestLevel, *forwardInOut, M.stream);
+        CachedAgglomeration ca;
+        if (readCache(cachePath, sig, ca))
+        {
+            b2g::buildHierarchyFromMaps(M, dSf.p, dMag.p, ca.maps, ca.nCoarse);
+            *forwardInOut = ca.forwardOut;
+            if (fromCache) *fromCache = 1;
+        }
+        else
+        {
+            const int fwdIn = *forwardInOut;
+            b2g::buildHierarchy(M, dSf.p, dMag.p, nCellsInCoarsestLevel, forwardInOut);
+            ca.forwardOut = *forwardInOut;
+            for (const b2g::Step& st : M.step)
+            {
+                ca.maps.push_back(st.restrictAddr.download(M.stream));
+                ca.nCoarse.push_back(st.nCoarse);
+            }
+            (void)fwdIn;
+            writeCache(cachePath, sig, ca);
+        }
+    }
     B2G_CUDA(cudaEventRecord(e1, M.stream));
     B2G_CUDA(cudaEventSynchronize(e1));
     B2G_CUDA(cudaEventElapsedTime(&M.buildMs, e0, e1));
@@ -436,6 +579,19 @@ b2g_status b2g_mesh_create(int nCells, int nFaces, const int32_t* lower, const i
         *out = nullptr;
         *out = b2g::capi::createMesh(nCells, nFaces, lower, upper, Sf, magSf, nCellsInCoarsestLevel, forwardInOut,
                                      memspace, streamOf(stream))
+                   .release();
+    });
+}
+
+b2g_status b2g_mesh_create_cached(int nCells, int nFaces, const int32_t* lower, const int32_t* upper,
+                                  const double* Sf, const double* magSf, int nCellsInCoarsestLevel, int* forwardInOut,
+                                  int memspace, void* stream, const char* cachePath, b2g_mesh** out, int* fromCache)
+{
+    return guarded([&] {
+        need(out != nullptr && cachePath != nullptr, "b2g_mesh_create_cached: null output handle or path");
+        *out = nullptr;
+        *out = b2g::capi::createMesh(nCells, nFaces, lower, upper, Sf, magSf, nCellsInCoarsestLevel, forwardInOut,
+                                     memspace, streamOf(stream), cachePath, fromCache)
                    .release();
     });
 }

@@ -52,10 +52,13 @@ b2g_status guarded(F&& f)
 // Refuses with B2G_ERR_ARGUMENT and `msg` unless `ok`.
 void need(bool ok, const char* msg);
 
-// Builds a mesh handle (the device hierarchy) on `stream` from host or device arrays.
+// Builds a mesh handle (the device hierarchy) on `stream` from host or device arrays. With
+// `cachePath`, a cached agglomeration whose content signature matches is loaded from that file
+// (*fromCache = 1), else the hierarchy is built and the file written (*fromCache = 0).
 std::unique_ptr<b2g_mesh> createMesh(int nCells, int nFaces, const int32_t* lower, const int32_t* upper,
                                      const double* Sf, const double* magSf, int nCellsInCoarsestLevel,
-                                     int* forwardInOut, int memspace, cudaStream_t stream);
+                                     int* forwardInOut, int memspace, cudaStream_t stream,
+                                     const char* cachePath = nullptr, int* fromCache = nullptr);
 
 // A whole solve on the finest level of A (on A.stream): source and psi from `memspace`, psi
 // overwritten with the solution; the PCG + GAMG solver, or GAMG alone when `standalone`.

@@ -999,6 +999,40 @@ void buildHierarchy(Mesh& M, const double* dSf, const double* dMagSf, int nCells
     for (int i = 0; i < M.nLevels(); ++i) buildStepMaps(M, i);
 }
 
+void buildHierarchyFromMaps(Mesh& M, const double* dSf, const double* dMagSf,
+                            const std::vector<std::vector<int>>& maps, const std::vector<int>& nCoarse)
+{
+    cudaStream_t s = M.stream;
+    LevelAddr& L0 = M.lev[0];
+    buildLevelLayouts(L0, s);
+    DBuf<double> w;
+    w.alloc(std::max(L0.nFaces, 1), s);
+    if (L0.nFaces) kFaceWeights<<<grid(L0.nFaces), TPB, 0, s>>>(L0.nFaces, dSf, dMagSf, w.p);
+    B2G_LAUNCH_CHECK();
+    for (size_t i = 0; i < maps.size(); ++i)
+    {
+        LevelAddr& F = M.lev.back();
+        if (static_cast<int>(maps[i].size()) != F.nCells)
+            fail(B2G_ERR_STATE, "b2g: the cached hierarchy does not fit this mesh (restriction map size).");
+        M.step.emplace_back();
+        Step& S = M.step.back();
+        S.nFine = F.nCells;
+        S.nCoarse = nCoarse[i];
+        S.nFineFaces = F.nFaces;
+        S.restrictAddr.upload(maps[i].data(), maps[i].size(), s);
+        M.lev.emplace_back();
+        LevelAddr& Fr = M.lev[M.lev.size() - 2];
+        LevelAddr& Cl = M.lev.back();
+        DBuf<double> cw;
+        coarseAddressing(Fr, S, Cl, w.p, cw, s);
+        buildLevelLayouts(Cl, s);
+        w = std::move(cw);
+    }
+    for (auto& L : M.lev) buildGsSchedule(L, s);
+    for (int i = 0; i < M.nLevels(); ++i) buildStepMaps(M, i);
+}
+
+
 // ---------------------------------------------------------------------------------------------
 // Gauss-Seidel schedule
 // ---------------------------------------------------------------------------------------------

@@ -155,6 +155,11 @@ void buildStepMaps(Mesh& M, int i);
 void buildHierarchy(Mesh& M, const double* dSf, const double* dMagSf, int nCellsInCoarsestLevel,
                     int* forward);
 
+// The same hierarchy from known restriction maps (a cached agglomeration): the pairing passes are
+// skipped; maps[i] is step i's restrictAddr (host), nCoarse[i] its coarse cell count.
+void buildHierarchyFromMaps(Mesh& M, const double* dSf, const double* dMagSf,
+                            const std::vector<std::vector<int>>& maps, const std::vector<int>& nCoarse);
+
 // Exclusive scan helper (n+1 outputs: out[0] = 0 ... out[n] = total); returns the total.
 long long exclusiveScan(const int* in, int* out, int n, cudaStream_t s);
 // Stable radix sort of (key, value) pairs; keys are unsigned, sorted on the low `bits` bits.

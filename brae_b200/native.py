@@ -74,6 +74,8 @@ def _load():
         "b2g_controls_read": (ip, [C.c_char_p, C.POINTER(Controls)]),
         "b2g_mesh_create": (ip, [ip, ip, vp, vp, vp, vp, ip, C.POINTER(C.c_int), ip, vp,
                                  C.POINTER(vp)]),
+        "b2g_mesh_create_cached": (ip, [ip, ip, vp, vp, vp, vp, ip, C.POINTER(C.c_int), ip, vp, C.c_char_p,
+                                        C.POINTER(vp), C.POINTER(C.c_int)]),
         "b2g_mesh_destroy": (ip, [vp]),
         "b2g_mesh_levels": (ip, [vp, C.POINTER(C.c_int)]),
         "b2g_mesh_level_size": (ip, [vp, ip, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
@@ -124,7 +126,7 @@ def _load():
 lib = _load()
 EXPORTED = [
     "b2g_last_error", "b2g_version", "b2g_set_profiling", "b2g_controls_default",
-    "b2g_controls_read", "b2g_mesh_create", "b2g_mesh_destroy", "b2g_mesh_levels",
+    "b2g_controls_read", "b2g_mesh_create", "b2g_mesh_create_cached", "b2g_mesh_destroy", "b2g_mesh_levels",
     "b2g_mesh_level_size", "b2g_mesh_get_step", "b2g_mesh_build_ms", "b2g_pcg_gamg_solve",
     "b2g_gamg_solve", "b2g_matrix_create", "b2g_matrix_destroy", "b2g_matrix_get_level",
     "b2g_level_amul", "b2g_level_smooth", "b2g_level_scale", "b2g_step_restrict",
@@ -203,7 +205,7 @@ class Mesh:
     """The mesh's GAMG hierarchy (GamgAgglomerationCache): built once, on the device."""
 
     def __init__(self, lower, upper, Sf, magSf, n_cells: int, n_coarsest: int = 10,
-                 forward: bool = True):
+                 forward: bool = True, cache_path: str | None = None):
         if not _is_torch(lower):
             lower = _as_host(lower, np.int32)
             upper = _as_host(upper, np.int32)
@@ -213,9 +215,17 @@ class Mesh:
         fw = C.c_int(1 if forward else 0)
         h = C.c_void_p()
         nF = int(lower.shape[0])
-        _check(lib.b2g_mesh_create(int(n_cells), nF, _ptr(lower), _ptr(upper), _ptr(Sf),
-                                   _ptr(magSf), int(n_coarsest), C.byref(fw), ms, _stream(),
-                                   C.byref(h)))
+        self.from_cache = False
+        if cache_path is None:
+            _check(lib.b2g_mesh_create(int(n_cells), nF, _ptr(lower), _ptr(upper), _ptr(Sf),
+                                       _ptr(magSf), int(n_coarsest), C.byref(fw), ms, _stream(),
+                                       C.byref(h)))
+        else:
+            hit = C.c_int(0)
+            _check(lib.b2g_mesh_create_cached(int(n_cells), nF, _ptr(lower), _ptr(upper), _ptr(Sf),
+                                              _ptr(magSf), int(n_coarsest), C.byref(fw), ms, _stream(),
+                                              str(cache_path).encode(), C.byref(h), C.byref(hit)))
+            self.from_cache = bool(hit.value)
         self.handle = h
         self.forward = bool(fw.value)
         self.n_cells = int(n_cells)

@@ -180,6 +180,16 @@ B2G_API b2g_status b2g_mesh_create(int nCells, int nFaces, const int32_t* lower,
                                    const int32_t* upper, const double* Sf, const double* magSf,
                                    int nCellsInCoarsestLevel, int* forwardInOut, int memspace,
                                    void* stream, b2g_mesh** out);
+/* b2g_mesh_create with a hierarchy cache on disk (the warm start brae's own AMG cache gives,
+ * device_amg_cache.cu): the agglomeration's inputs (sizes, lower, upper, Sf, magSf,
+ * nCellsInCoarsestLevel, the direction flag) are hashed on the device; if `cachePath` holds an
+ * agglomeration with the same signature its restriction maps are used and the pairing passes skipped
+ * (*fromCache = 1, *forwardInOut set as the original build left it), else the hierarchy is built and
+ * written there (*fromCache = 0). The hierarchy is the same either way. fromCache may be NULL. */
+B2G_API b2g_status b2g_mesh_create_cached(int nCells, int nFaces, const int32_t* lower, const int32_t* upper,
+                                          const double* Sf, const double* magSf, int nCellsInCoarsestLevel,
+                                          int* forwardInOut, int memspace, void* stream, const char* cachePath,
+                                          b2g_mesh** out, int* fromCache);
 B2G_API b2g_status b2g_mesh_destroy(b2g_mesh* mesh);
 
 /* Number of coarse levels (GamgAgglomeration::size(), AGGH:76-79). */
