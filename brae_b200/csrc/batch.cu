@@ -203,17 +203,7 @@ __global__ void __launch_bounds__(BT) bMcSweep(const int4* __restrict__ tiles, c
     const float* __restrict__ diag = s.mcDiag;
     const float* __restrict__ b = s.v[rsrc];
     float* __restrict__ psi = s.v[rpsi];
-    for (int r = t.y + threadIdx.x; r < t.z; r += BT)
-    {
-        const int p = pos[r];
-        if (p < 0) continue;
-        const int sl = r >> 5;
-        const int base = slice[sl];
-        const int w = (slice[sl + 1] - base) >> 5;
-        float acc = b[p];
-        for (int q = 0, e = base + (r & 31); q < w; ++q, e += 32) acc = fmaf(-val[e], psi[col[e]], acc);
-        psi[p] = acc / diag[r];
-    }
+    for (int r = t.y + threadIdx.x; r < t.z; r += BT) k::mcRowUpdate(r, pos, slice, col, val, diag, b, psi);
 }
 
 // every sweep of one small case's multicolour smoothing in one block (block i: descriptor cases[i])
@@ -233,20 +223,11 @@ __global__ void __launch_bounds__(1024) bMcSmoothSmall(const int* __restrict__ c
     const float* __restrict__ b = s.v[rsrc];
     float* __restrict__ psi = s.v[rpsi];
     for (int sw = 0; sw < nSweeps; ++sw)
-        for (int k = 0; k < nColours; ++k)
+        for (int c = 0; c < nColours; ++c)
         {
-            const int end = cs[k + 1];
-            for (int r = cs[k] + threadIdx.x; r < end; r += blockDim.x)
-            {
-                const int p = pos[r];
-                if (p < 0) continue;
-                const int sl = r >> 5;
-                const int base = slice[sl];
-                const int w = (slice[sl + 1] - base) >> 5;
-                float acc = b[p];
-                for (int q = 0, e = base + (r & 31); q < w; ++q, e += 32) acc = fmaf(-val[e], psi[col[e]], acc);
-                psi[p] = acc / diag[r];
-            }
+            const int end = cs[c + 1];
+            for (int r = cs[c] + threadIdx.x; r < end; r += blockDim.x)
+                k::mcRowUpdate(r, pos, slice, col, val, diag, b, psi);
             __syncthreads();
         }
 }

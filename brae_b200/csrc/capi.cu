@@ -784,15 +784,15 @@ b2g_status b2g_level_colouring(const b2g_mesh* mesh, int level, int* nColours, i
     });
 }
 
-b2g_status b2g_level_sweep_shape(const b2g_mesh* mesh, int level, int* oneBlock, int* threadsPerBlock,
+b2g_status b2g_level_sweep_shape(const b2g_mesh* mesh, int level, int* wholeLevelCtas, int* threadsPerBlock,
                                  float* msPerSweep)
 {
     return guarded([&] {
-        need(mesh && oneBlock && threadsPerBlock && msPerSweep, "b2g_level_sweep_shape: null argument");
+        need(mesh && wholeLevelCtas && threadsPerBlock && msPerSweep, "b2g_level_sweep_shape: null argument");
         need(level >= 0 && level <= mesh->m.nLevels(), "b2g_level_sweep_shape: no such level");
         const b2g::Colouring& C = mesh->m.lev[level].mc;
-        *oneBlock = C.tuned && C.fused ? 1 : 0;
-        *threadsPerBlock = C.tuned ? (C.fused ? 1024 : C.block) : 0;
+        *wholeLevelCtas = !C.tuned ? 0 : C.cluster > 0 ? C.cluster : C.fused ? 1 : 0;
+        *threadsPerBlock = C.tuned ? (C.fused || C.cluster > 0 ? 1024 : C.block) : 0;
         *msPerSweep = C.tuned ? C.msPerSweep : 0.f;
     });
 }

@@ -66,9 +66,11 @@ struct Colouring
     DBuf<int> col;                 // [nEnt] the other cell's position
     DBuf<int> face;                // [nEnt] the face, -1 for padding
     // the sweep's launch shape, chosen by measurement (Matrix::tuneMulticolour): one block sweeping
-    // the whole level, or one launch per colour of `block` threads per block
+    // the whole level, one thread-block cluster of `cluster` CTAs sweeping it (cluster > 0), or one
+    // launch per colour of `block` threads per block
     bool tuned = false;
     bool fused = false;
+    int cluster = 0;
     int block = 256;
     float msPerSweep = 0.f;
 };

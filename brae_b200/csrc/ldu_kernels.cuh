@@ -412,6 +412,43 @@ static __global__ void __launch_bounds__(32) serialNormFactor(Rows<double> A, co
     if (lane == 0) *out = __dadd_rn(s, 1e-20);
 }
 
+// One row of a multicolour Gauss-Seidel sweep in the colour-major sliced-ELL layout (hierarchy.cuh
+// Colouring): psi[p] = (b[p] - sum val*psi[col]) / diag, the entries in layout order. Every load that
+// does not depend on the row's position (its slice bounds, its diagonal) and four entries' columns and
+// coefficients at a time are issued before they are used, so a thread waits about four memory
+// latencies per row rather than one per entry; on the small levels, where a few threads sweep a colour
+// each, that latency chain is the sweep's time. The arithmetic order is the plain loop's.
+// Row r < nRows: the layout pads each colour to whole slices of 32, so r's slice and its successor
+// bound exist whatever pos[r] holds.
+__device__ __forceinline__ void mcRowUpdate(int r, const int* __restrict__ pos, const int* __restrict__ sliceBase,
+                                            const int* __restrict__ col, const float* __restrict__ val,
+                                            const float* __restrict__ diag, const float* __restrict__ b,
+                                            float* __restrict__ psi)
+{
+    const int sl = r >> 5;
+    const int p = pos[r];
+    const int base = sliceBase[sl];
+    const int end = sliceBase[sl + 1];
+    const float d = diag[r];
+    if (p < 0) return;
+    const int w = (end - base) >> 5;
+    float acc = b[p];
+    int e = base + (r & 31);
+    int q = 0;
+    for (; q + 4 <= w; q += 4, e += 128)
+    {
+        const int c0 = col[e], c1 = col[e + 32], c2 = col[e + 64], c3 = col[e + 96];
+        const float v0 = val[e], v1 = val[e + 32], v2 = val[e + 64], v3 = val[e + 96];
+        const float x0 = psi[c0], x1 = psi[c1], x2 = psi[c2], x3 = psi[c3];
+        acc = fmaf(-v0, x0, acc);
+        acc = fmaf(-v1, x1, acc);
+        acc = fmaf(-v2, x2, acc);
+        acc = fmaf(-v3, x3, acc);
+    }
+    for (; q < w; ++q, e += 32) acc = fmaf(-val[e], psi[col[e]], acc);
+    psi[p] = acc / d;
+}
+
 // One colour of a multicolour Gauss-Seidel sweep (FP32 V-cycle): rows [rowBegin, rowEnd) of the
 // level's colour-major sliced-ELL layout (hierarchy.cuh Colouring), one thread per row. No two rows
 // of a colour share a face, so every value a row reads is final for this colour.
@@ -426,6 +463,16 @@ __global__ void mcSmoothSmall(int nColours, const int* __restrict__ colourStart,
                               const int* __restrict__ pos, const int* __restrict__ sliceBase,
                               const int* __restrict__ col, const float* __restrict__ val,
                               const float* __restrict__ diag, const float* __restrict__ b, float* __restrict__ psi);
+
+// The same in one thread-block cluster (mid-size levels): the cluster's CTAs share each colour's rows
+// and meet at the cluster barrier (release/acquire at cluster scope) between colours. The CTAs of a
+// cluster are resident together by construction, so the barrier always completes. Launched with a
+// cluster dimension equal to the grid (kMcClusterMaxRows rows at most).
+constexpr int kMcClusterMaxRows = 262144;
+__global__ void mcSmoothCluster(int nColours, const int* __restrict__ colourStart, int nSweeps, int symmetric,
+                                const int* __restrict__ pos, const int* __restrict__ sliceBase,
+                                const int* __restrict__ col, const float* __restrict__ val,
+                                const float* __restrict__ diag, const float* __restrict__ b, float* __restrict__ psi);
 
 // The FP32 coefficients of the multicolour layout: per entry upper[face] (0 for padding), per row
 // the diagonal at its position.

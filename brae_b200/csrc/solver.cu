@@ -4,6 +4,8 @@
 // Reference: GAMG = src/matrices/lduMatrix/solvers/GAMG/gamg_solver_cpp.cu
 #include "solver.cuh"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -204,27 +206,12 @@ void zeroArray(long long n, T* x, cudaStream_t s)
 
 namespace k {
 
-__device__ __forceinline__ void mcRow(int r, const int* __restrict__ pos, const int* __restrict__ sliceBase,
-                                      const int* __restrict__ col, const float* __restrict__ val,
-                                      const float* __restrict__ diag, const float* __restrict__ b,
-                                      float* __restrict__ psi)
-{
-    const int p = pos[r];
-    if (p < 0) return;
-    const int sl = r >> 5;
-    const int base = sliceBase[sl];
-    const int w = (sliceBase[sl + 1] - base) >> 5;
-    float acc = b[p];
-    for (int q = 0, e = base + (r & 31); q < w; ++q, e += 32) acc = fmaf(-val[e], psi[col[e]], acc);
-    psi[p] = acc / diag[r];
-}
-
 __global__ void mcSweep(int rowBegin, int rowEnd, const int* __restrict__ pos, const int* __restrict__ sliceBase,
                         const int* __restrict__ col, const float* __restrict__ val, const float* __restrict__ diag,
                         const float* __restrict__ b, float* __restrict__ psi)
 {
     for (int r = rowBegin + blockIdx.x * blockDim.x + threadIdx.x; r < rowEnd; r += gridDim.x * blockDim.x)
-        mcRow(r, pos, sliceBase, col, val, diag, b, psi);
+        mcRowUpdate(r, pos, sliceBase, col, val, diag, b, psi);
 }
 
 __global__ void __launch_bounds__(1024) mcSmoothSmall(int nColours, const int* __restrict__ colourStart, int nSweeps,
@@ -239,8 +226,29 @@ __global__ void __launch_bounds__(1024) mcSmoothSmall(int nColours, const int* _
         {
             const int k = i < nColours ? i : 2 * nColours - 1 - i;  // symmetric: the colours back again
             const int e = colourStart[k + 1];
-            for (int r = colourStart[k] + threadIdx.x; r < e; r += blockDim.x) mcRow(r, pos, sliceBase, col, val, diag, b, psi);
+            for (int r = colourStart[k] + threadIdx.x; r < e; r += blockDim.x)
+                mcRowUpdate(r, pos, sliceBase, col, val, diag, b, psi);
             __syncthreads();
+        }
+}
+
+__global__ void __launch_bounds__(1024) mcSmoothCluster(int nColours, const int* __restrict__ colourStart,
+                                                        int nSweeps, int symmetric, const int* __restrict__ pos,
+                                                        const int* __restrict__ sliceBase, const int* __restrict__ col,
+                                                        const float* __restrict__ val, const float* __restrict__ diag,
+                                                        const float* __restrict__ b, float* __restrict__ psi)
+{
+    cooperative_groups::cluster_group cluster = cooperative_groups::this_cluster();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int stride = gridDim.x * blockDim.x;
+    const int steps = symmetric ? 2 * nColours : nColours;
+    for (int sw = 0; sw < nSweeps; ++sw)
+        for (int i = 0; i < steps; ++i)
+        {
+            const int k = i < nColours ? i : 2 * nColours - 1 - i;
+            const int e = colourStart[k + 1];
+            for (int r = colourStart[k] + t; r < e; r += stride) mcRowUpdate(r, pos, sliceBase, col, val, diag, b, psi);
+            cluster.sync();  // every thread of every CTA, once per colour
         }
 }
 
@@ -870,16 +878,74 @@ void Matrix::symSmooth(int level, T* psiL, const T* src, int nSweeps)
 void Matrix::mcSmooth(int level, float* psiL, const float* src, int nSweeps, bool symmetric)
 {
     const Colouring& C = mesh->lev[level].mc;
-    mcLaunch(level, C.fused, C.block, psiL, src, nSweeps, true, symmetric);
+    mcLaunch(level, C.fused, C.cluster, C.block, psiL, src, nSweeps, true, symmetric);
 }
 
-// nSweeps multicolour sweeps of one level in a given shape: one block for the whole level, or one
-// launch per colour of `block` threads per block
-void Matrix::mcLaunch(int level, bool fused, int block, float* psiL, const float* src, int nSweeps, bool timed,
-                      bool symmetric)
+namespace {
+
+// The launch configuration of mcSmoothCluster: one cluster of `ctas` CTAs of 1024 threads (the grid).
+struct ClusterLaunch
+{
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg;
+    ClusterLaunch(int ctas, cudaStream_t s)
+    {
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = static_cast<unsigned>(ctas);
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg = cudaLaunchConfig_t{};
+        cfg.gridDim = dim3(static_cast<unsigned>(ctas));
+        cfg.blockDim = dim3(1024);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = s;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+    }
+};
+
+// Whether one cluster of `ctas` 1024-thread CTAs of mcSmoothCluster can be resident on this device
+// (sizes above 8 are non-portable and need the kernel's opt-in on the current device, set here).
+bool clusterFits(int ctas, cudaStream_t s)
+{
+    if (ctas > 8 &&
+        cudaFuncSetAttribute(k::mcSmoothCluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return false;
+    }
+    ClusterLaunch L(ctas, s);
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k::mcSmoothCluster, &L.cfg) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return false;
+    }
+    return n >= 1;
+}
+
+}  // namespace
+
+// nSweeps multicolour sweeps of one level in a given shape: one block for the whole level, one
+// cluster of `cluster` CTAs for the whole level, or one launch per colour of `block` threads per block
+void Matrix::mcLaunch(int level, bool fused, int cluster, int block, float* psiL, const float* src, int nSweeps,
+                      bool timed, bool symmetric)
 {
     const Colouring& C = mesh->lev[level].mc;
     const LevelCoef<float>& F = v32.coef[level];
+    if (cluster > 0)
+    {
+        cudaEvent_t ev = timed && level == 0 ? timedBegin(1) : nullptr;
+        ClusterLaunch L(cluster, stream);
+        B2G_CUDA(cudaLaunchKernelEx(&L.cfg, k::mcSmoothCluster, C.nColours, static_cast<const int*>(C.colourStartD.p),
+                                    nSweeps, symmetric ? 1 : 0, static_cast<const int*>(C.pos.p),
+                                    static_cast<const int*>(C.sliceBase.p), static_cast<const int*>(C.col.p),
+                                    static_cast<const float*>(F.mcVal.p), static_cast<const float*>(F.mcDiag.p), src,
+                                    psiL));
+        timedEnd(1, ev);
+        ++launches;
+        return;
+    }
     if (fused)
     {
         cudaEvent_t ev = timed && level == 0 ? timedBegin(1) : nullptr;
@@ -907,8 +973,11 @@ void Matrix::mcLaunch(int level, bool fused, int block, float* psiL, const float
 }
 
 // The autotuner of the multicolour sweep: times every candidate launch shape on the level's own
-// layout (one block sweeping the whole level when it has at most kMcSmallRows rows; one launch per
-// colour at 128, 256 or 512 threads per block) and keeps the fastest. Runs once per mesh level, on
+// layout (one block sweeping the whole level when it has at most kMcSmallRows rows; one cluster of 4,
+// 8 or 16 CTAs sweeping it when it has at most kMcClusterMaxRows rows and the cluster fits the device;
+// one launch per colour at 128, 256 or 512 threads per block) and keeps the fastest. Every shape
+// computes each row with the same arithmetic on the same final values, so the choice changes the time
+// only. Runs once per mesh level, on
 // this matrix's FP32 values and scratch vectors, outside any capture.
 void Matrix::tuneMulticolour(int level)
 {
@@ -921,11 +990,15 @@ void Matrix::tuneMulticolour(int level)
     struct Shape
     {
         bool fused;
+        int cluster;
         int block;
     };
     std::vector<Shape> shapes;
-    if (C.nRows <= k::kMcSmallRows) shapes.push_back({true, 1024});
-    for (int bl : {128, 256, 512}) shapes.push_back({false, bl});
+    if (C.nRows <= k::kMcSmallRows) shapes.push_back({true, 0, 1024});
+    if (C.nRows <= k::kMcClusterMaxRows)
+        for (int ctas : {4, 8, 16})
+            if (clusterFits(ctas, stream)) shapes.push_back({false, ctas, 1024});
+    for (int bl : {128, 256, 512}) shapes.push_back({false, 0, bl});
     cudaEvent_t e0, e1;
     B2G_CUDA(cudaEventCreate(&e0));
     B2G_CUDA(cudaEventCreate(&e1));
@@ -933,9 +1006,9 @@ void Matrix::tuneMulticolour(int level)
     const long long l0 = launches;
     for (const Shape& sh : shapes)
     {
-        mcLaunch(level, sh.fused, sh.block, x, b, 1, false);  // warm
+        mcLaunch(level, sh.fused, sh.cluster, sh.block, x, b, 1, false);  // warm
         B2G_CUDA(cudaEventRecord(e0, stream));
-        mcLaunch(level, sh.fused, sh.block, x, b, 3, false);
+        mcLaunch(level, sh.fused, sh.cluster, sh.block, x, b, 3, false);
         B2G_CUDA(cudaEventRecord(e1, stream));
         B2G_CUDA(cudaEventSynchronize(e1));
         float ms = 0.f;
@@ -945,6 +1018,7 @@ void Matrix::tuneMulticolour(int level)
         {
             best = ms;
             C.fused = sh.fused;
+            C.cluster = sh.cluster;
             C.block = sh.block;
             C.tuned = true;
         }

@@ -270,10 +270,12 @@ class Mesh:
         return starts
 
     def sweep_shape(self, level: int) -> dict:
-        """The autotuner's multicolour sweep shape for `level` (zeros before the form's first solve)."""
-        one, thr, ms = C.c_int(), C.c_int(), C.c_float()
-        _check(lib.b2g_level_sweep_shape(self.handle, level, C.byref(one), C.byref(thr), C.byref(ms)))
-        return {"one_block": bool(one.value), "threads": thr.value, "ms_per_sweep": ms.value}
+        """The autotuner's multicolour sweep shape for `level` (zeros before the form's first solve):
+        one block for the whole level, one cluster of `cluster_ctas` CTAs, or one launch per colour."""
+        whole, thr, ms = C.c_int(), C.c_int(), C.c_float()
+        _check(lib.b2g_level_sweep_shape(self.handle, level, C.byref(whole), C.byref(thr), C.byref(ms)))
+        return {"one_block": whole.value == 1, "cluster_ctas": whole.value if whole.value > 1 else 0,
+                "threads": thr.value, "ms_per_sweep": ms.value}
 
     def step(self, i: int) -> dict:
         nc, nf = self.level_size(i)

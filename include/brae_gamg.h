@@ -381,10 +381,11 @@ B2G_API b2g_status b2g_server_case_bytes(b2g_server* server, int caseId, unsigne
 B2G_API b2g_status b2g_level_colouring(const b2g_mesh* mesh, int level, int* nColours, int* colourStart);
 
 /* Diagnostic: the launch shape the autotuner chose for `level`'s multicolour sweep (measured on the
- * form's first solve on the mesh): *oneBlock 1 if one block sweeps the whole level, else one launch
- * per colour of *threadsPerBlock threads; *msPerSweep the measured time of one sweep. All 0 before. */
-B2G_API b2g_status b2g_level_sweep_shape(const b2g_mesh* mesh, int level, int* oneBlock, int* threadsPerBlock,
-                                         float* msPerSweep);
+ * form's first solve on the mesh): *wholeLevelCtas 1 if one block sweeps the whole level, c > 1 if
+ * one thread-block cluster of c CTAs does, 0 for one launch per colour; *threadsPerBlock the CTAs'
+ * size; *msPerSweep the measured time of one sweep. All 0 before. */
+B2G_API b2g_status b2g_level_sweep_shape(const b2g_mesh* mesh, int level, int* wholeLevelCtas,
+                                         int* threadsPerBlock, float* msPerSweep);
 
 /* Library version string. */
 B2G_API const char* b2g_version(void);
