@@ -165,6 +165,37 @@ def box_case(nx: int, ny: int, nz: int, lengths=(1.0, 1.0, 1.0), grading_y: floa
                    max_aspect=float(aspect))
 
 
+def periodic_box(nx: int, ny: int, nz: int, lengths=(2.0, 1.0, 1.0), grading_y: float = 1.0,
+                 two_phase: bool = False, seed: int = 0):
+    """box_case with a cyclic pair joining the z = 0 and z = Lz faces: two coupled patches, the
+    bottom one first, each listing its cells in face order (x fastest) and its neighbours across the
+    pair face for face. Returns (case, own, nbr, coeff): the pair in the form a coupled patch's
+    faceCells / neighbour faceCells / boundaryCoeffs give it, with the matrix's sign convention that
+    Amul subtracts coeff * psi[nbr]. The pair's diagonal share is folded into case.diag (the coupled
+    patch's internalCoeffs), so the pair coefficient is the off-diagonal's negative."""
+    c = box_case(nx, ny, nz, lengths, grading_y, two_phase, seed, name=f"periodic_{nx}x{ny}x{nz}")
+    lx, ly, lz = lengths
+    dx = np.full(nx, lx / nx)
+    dy = graded_spacing(ny, ly, grading_y)
+    dz = lz / nz
+    j, i = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    i = i.ravel(); j = j.ravel()
+    bottom = (j * nx + i).astype(np.int64)
+    top = bottom + (nz - 1) * nx * ny
+    area = dx[i] * dy[j]
+    coeff = area / dz  # the two half-cells across the pair face
+    if two_phase:
+        zc0 = 0.5 * dz
+        coeff = coeff / _rho(np.full(coeff.shape, zc0), dz)
+    own = np.concatenate([bottom, top]).astype(np.int32)
+    nbr = np.concatenate([top, bottom]).astype(np.int32)
+    pc = np.concatenate([coeff, coeff])
+    diag = c.diag.copy()
+    np.add.at(diag, own, pc)
+    c.diag = diag
+    return c, own, nbr, pc
+
+
 def unit_cube(n: int = 64, seed: int = 0) -> BoxCase:
     """The CPU-sized case: an n^3 uniform unit cube (n = 64: 262,144 cells)."""
     return box_case(n, n, n, (1.0, 1.0, 1.0), 1.0, False, seed, name=f"unit_cube_{n}")

@@ -170,6 +170,16 @@ class Oracle:
         L.oc_gamg_solve.restype = Perf
         L.oc_gamg_solve.argtypes = [C.c_void_p, _f64p, _f64p, _f64p, _f64p, C.POINTER(Controls),
                                     C.c_void_p, C.c_int]
+        pair = [C.c_int, _i32p, _i32p, _f64p]
+        L.oc_hier_build_pair.restype = C.c_void_p
+        L.oc_hier_build_pair.argtypes = [C.c_void_p, _f64p, _f64p] + pair
+        L.oc_hier_level_pair.restype = C.c_int
+        L.oc_hier_level_pair.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oc_gamg_solve_pair.restype = Perf
+        L.oc_gamg_solve_pair.argtypes = [C.c_void_p, _f64p, _f64p] + pair + [
+            _f64p, _f64p, C.POINTER(Controls), C.c_void_p, C.c_int]
+        L.oc_amul_pair.argtypes = lvl + pair + [_f64p, _f64p]
+        L.oc_smooth_pair.argtypes = lvl + pair + [_f64p, _f64p, C.c_int, C.c_int]
 
     # -- agglomeration --------------------------------------------------------------------------
     def agglomerate(self, lower, upper, Sf, magSf, n_cells, n_coarsest=10, forward=True):
@@ -272,6 +282,49 @@ class Oracle:
                                    hist.ctypes.data, cap)
         return dict(psi=x, perf=p.as_tuple(), history=hist[:min(p.nIterations, cap)])
 
+    # -- the coupled pair -----------------------------------------------------------------------
+    @staticmethod
+    def _pair(own, nbr, coeff):
+        return (int(len(own)), np.ascontiguousarray(own, np.int32), np.ascontiguousarray(nbr, np.int32),
+                np.ascontiguousarray(coeff, np.float64))
+
+    def gamg_solve_pair(self, agg: _Agglom, diag, coef, own, nbr, pcoef, source, psi, ctl: Controls,
+                        cap=100000):
+        x = np.array(psi, dtype=np.float64, copy=True)
+        hist = np.zeros(cap)
+        p = self.lib.oc_gamg_solve_pair(agg.handle, np.ascontiguousarray(diag, np.float64),
+                                        np.ascontiguousarray(coef, np.float64), *self._pair(own, nbr, pcoef),
+                                        np.ascontiguousarray(source, np.float64), x, C.byref(ctl),
+                                        hist.ctypes.data, cap)
+        return dict(psi=x, perf=p.as_tuple(), history=hist[:min(p.nIterations, cap)])
+
+    def hierarchy_pairs(self, agg: _Agglom, diag, coef, own, nbr, pcoef):
+        """Every level's pair (own, nbr, coeff) after agglomeration, level 0 first."""
+        h = self.lib.oc_hier_build_pair(agg.handle, np.ascontiguousarray(diag, np.float64),
+                                        np.ascontiguousarray(coef, np.float64), *self._pair(own, nbr, pcoef))
+        out = []
+        for lv in range(agg.hierarchy.n_levels + 1 if hasattr(agg.hierarchy, "n_levels")
+                        else len(agg.hierarchy.n_cells)):
+            m = self.lib.oc_hier_level_pair(h, lv, None, None, None)
+            o = np.empty(m, np.int32); nb = np.empty(m, np.int32); c = np.empty(m, np.float64)
+            self.lib.oc_hier_level_pair(h, lv, o.ctypes.data, nb.ctypes.data, c.ctypes.data)
+            out.append((o, nb, c))
+        self.lib.oc_hier_free(h)
+        return out
+
+    def amul_pair(self, lower, upper, diag, coef, own, nbr, pcoef, x):
+        y = np.empty_like(diag, dtype=np.float64)
+        self.lib.oc_amul_pair(*self._lvl(lower, upper, diag, coef), *self._pair(own, nbr, pcoef),
+                              np.ascontiguousarray(x), y)
+        return y
+
+    def smooth_pair(self, lower, upper, diag, coef, own, nbr, pcoef, psi, source, n_sweeps,
+                    smoother="GaussSeidel"):
+        x = np.array(psi, dtype=np.float64, copy=True)
+        self.lib.oc_smooth_pair(*self._lvl(lower, upper, diag, coef), *self._pair(own, nbr, pcoef), x,
+                                np.ascontiguousarray(source), n_sweeps, SMOOTHERS[smoother])
+        return x
+
 
 class Reference:
     """The reference's own host path (oracle/_ref/libref.so)."""
@@ -298,6 +351,8 @@ class Reference:
                                      C.POINTER(Perf)]
         L.ref_gs_smooth.argtypes = [C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, _f64p,
                                     C.c_int, C.c_int]
+        L.ref_gamg_solve_pair.argtypes = [C.c_void_p, _f64p, _f64p, _f64p, _f64p, C.c_int, _i32p, _i32p,
+                                          _f64p, C.POINTER(Controls), C.POINTER(Perf)]
         L.ref_coarsest_pcg_dic.argtypes = [C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p,
                                            _f64p, C.c_double, C.c_double, C.POINTER(Perf)]
 
@@ -340,6 +395,17 @@ class Reference:
                                             np.ascontiguousarray(coef, np.float64),
                                             np.ascontiguousarray(source, np.float64), x,
                                             C.byref(ctl), C.byref(perf)))
+        return dict(psi=x, perf=perf.as_tuple())
+
+    def gamg_solve_pair(self, agg: _Agglom, diag, coef, own, nbr, pcoef, source, psi, ctl: Controls):
+        """gamgSolve with one coupled patch carrying the pair (its internalCoeffs zero)."""
+        x = np.array(psi, dtype=np.float64, copy=True)
+        perf = Perf()
+        self._check(self.lib.ref_gamg_solve_pair(
+            agg.handle, np.ascontiguousarray(diag, np.float64), np.ascontiguousarray(coef, np.float64),
+            np.ascontiguousarray(source, np.float64), x, int(len(own)), np.ascontiguousarray(own, np.int32),
+            np.ascontiguousarray(nbr, np.int32), np.ascontiguousarray(pcoef, np.float64), C.byref(ctl),
+            C.byref(perf)))
         return dict(psi=x, perf=perf.as_tuple())
 
     def gs_smooth(self, lower, upper, diag, coef, psi, b, n_sweeps, symmetric=False):

@@ -372,6 +372,12 @@ typedef struct
     const int* upper;
     double* diag;
     double* coef; /* upper == lower (symmetric) */
+    /* the coupled (cyclic) pair, each face once from its own side (LduLevel::ifOwn/ifNbr/ifCoeff,
+     * GAMG:25-36), in the sign convention Amul subtracts; nIf 0 = none */
+    int nIf;
+    const int* ifOwn;
+    const int* ifNbr;
+    const double* ifCoeff;
 } oc_level;
 
 /* lduMatrix::Amul (GAMG:62-88) */
@@ -385,6 +391,8 @@ static void amul_l(const oc_level* A, const double* psi, double* Apsi)
         Apsi[u] += A->coef[f] * psi[l];
         Apsi[l] += A->coef[f] * psi[u];
     }
+    /* the pair, as updateMatrixInterfaces applies it (GAMG:82-87) */
+    for (int f = 0; f < A->nIf; ++f) Apsi[A->ifOwn[f]] -= A->ifCoeff[f] * psi[A->ifNbr[f]];
 }
 
 /* lduMatrix::residual (GAMG:90-117); rA may alias source */
@@ -398,6 +406,8 @@ static void residual_l(const oc_level* A, double* rA, const double* psi, const d
         rA[u] -= A->coef[f] * psi[l];
         rA[l] -= A->coef[f] * psi[u];
     }
+    /* the pair, with the sign Amul's term does not have (GAMG:110-115) */
+    for (int f = 0; f < A->nIf; ++f) rA[A->ifOwn[f]] += A->ifCoeff[f] * psi[A->ifNbr[f]];
 }
 
 /* lduMatrix::solver::normFactor (GAMG:119-159) */
@@ -410,6 +420,8 @@ static double norm_factor_l(const oc_level* A, const double* psi, const double* 
         tmp[A->upper[f]] += A->coef[f];
         tmp[A->lower[f]] += A->coef[f];
     }
+    /* sumA takes the pair with Amul's sign (GAMG:137-145) */
+    for (int f = 0; f < A->nIf; ++f) tmp[A->ifOwn[f]] -= A->ifCoeff[f];
     double average = 0;
     for (int c = 0; c < A->nCells; ++c) average += psi[c];
     average /= (double)A->nCells;
@@ -560,7 +572,17 @@ static void smoother_smooth(const oc_smoother* s, double* psi, const double* sou
     }
     if (s->kind != SM_DIC)
     {
-        gs_sweeps(A, s->os, source, psi, nSweeps, s->kind == SM_SYMGS, tmp);
+        /* the pair enters through bPrime, once per smooth() with psi as it stands at entry
+         * (GAMG:287-305) */
+        double* b = NULL;
+        if (A->nIf > 0)
+        {
+            b = (double*)xmalloc(sizeof(double) * (size_t)(n ? n : 1));
+            memcpy(b, source, sizeof(double) * (size_t)n);
+            for (int f = 0; f < A->nIf; ++f) b[A->ifOwn[f]] += A->ifCoeff[f] * psi[A->ifNbr[f]];
+        }
+        gs_sweeps(A, s->os, b ? b : source, psi, nSweeps, s->kind == SM_SYMGS, tmp);
+        free(b);
     }
     free(tmp);
 }
@@ -660,7 +682,57 @@ struct oc_hier
     oc_level lev[MAX_LEVELS];  /* lev[0] = the folded fine matrix, lev[i] = coarse level i */
 };
 
+/* GAMGSolver::agglomerateMatrix's coarse interface (GAMG:497-524): each fine pair face keyed on
+ * the coarse cell pair (own, nbr) it joins, in fine face order; a new pair appends a coarse face, a
+ * seen one reuses it; the coefficients summed onto it from zero in fine face order. The lookup is an
+ * open-addressing table on the pair. */
+static void agglomerate_pair(const oc_level* fm, oc_level* cm, const int* restrictAddr)
+{
+    cm->nIf = 0;
+    cm->ifOwn = NULL;
+    cm->ifNbr = NULL;
+    cm->ifCoeff = NULL;
+    if (fm->nIf == 0) return;
+    const int nF = fm->nIf;
+    int* own = (int*)xmalloc(sizeof(int) * (size_t)nF);
+    int* nbr = (int*)xmalloc(sizeof(int) * (size_t)nF);
+    double* coeff = (double*)xmalloc(sizeof(double) * (size_t)nF);
+    size_t cap = 16;
+    while (cap < 2 * (size_t)nF) cap <<= 1;
+    int* slot = (int*)xmalloc(sizeof(int) * cap);
+    for (size_t i = 0; i < cap; ++i) slot[i] = -1;
+    int nC = 0;
+    for (int f = 0; f < nF; ++f)
+    {
+        const int co = restrictAddr[fm->ifOwn[f]];
+        const int cn = restrictAddr[fm->ifNbr[f]];
+        uint64_t hsh = ((uint64_t)(uint32_t)co * 0x9E3779B97F4A7C15ull) ^ ((uint64_t)(uint32_t)cn * 0xC2B2AE3D27D4EB4Full);
+        size_t i = (size_t)(hsh ^ (hsh >> 29)) & (cap - 1);
+        while (slot[i] >= 0 && !(own[slot[i]] == co && nbr[slot[i]] == cn)) i = (i + 1) & (cap - 1);
+        if (slot[i] < 0)
+        {
+            slot[i] = nC;
+            own[nC] = co;
+            nbr[nC] = cn;
+            coeff[nC] = 0.0;
+            ++nC;
+        }
+        coeff[slot[i]] += fm->ifCoeff[f];
+    }
+    free(slot);
+    cm->nIf = nC;
+    cm->ifOwn = own;
+    cm->ifNbr = nbr;
+    cm->ifCoeff = coeff;
+}
+
 oc_hier* oc_hier_build(const oc_agglom* a, const double* diag, const double* upper)
+{
+    return oc_hier_build_pair(a, diag, upper, 0, NULL, NULL, NULL);
+}
+
+oc_hier* oc_hier_build_pair(const oc_agglom* a, const double* diag, const double* upper, int nIf,
+                            const int* ifOwn, const int* ifNbr, const double* ifCoeff)
 {
     oc_hier* h = (oc_hier*)xcalloc(1, sizeof(oc_hier));
     h->a = a;
@@ -674,6 +746,19 @@ oc_hier* oc_hier_build(const oc_agglom* a, const double* diag, const double* upp
     f0->coef = (double*)xmalloc(sizeof(double) * (size_t)(f0->nFaces ? f0->nFaces : 1));
     memcpy(f0->diag, diag, sizeof(double) * (size_t)f0->nCells);
     memcpy(f0->coef, upper, sizeof(double) * (size_t)f0->nFaces);
+    f0->nIf = nIf;
+    if (nIf > 0)
+    {
+        int* o = (int*)xmalloc(sizeof(int) * (size_t)nIf);
+        int* nb = (int*)xmalloc(sizeof(int) * (size_t)nIf);
+        double* cf = (double*)xmalloc(sizeof(double) * (size_t)nIf);
+        memcpy(o, ifOwn, sizeof(int) * (size_t)nIf);
+        memcpy(nb, ifNbr, sizeof(int) * (size_t)nIf);
+        memcpy(cf, ifCoeff, sizeof(double) * (size_t)nIf);
+        f0->ifOwn = o;
+        f0->ifNbr = nb;
+        f0->ifCoeff = cf;
+    }
     for (int i = 0; i < a->nLevels; ++i)
     {
         const oc_level* fm = &h->lev[i];
@@ -692,6 +777,7 @@ oc_hier* oc_hier_build(const oc_agglom* a, const double* diag, const double* upp
             if (c >= 0) cm->coef[c] += fm->coef[f];
             else cm->diag[-1 - c] += 2 * fm->coef[f];
         }
+        agglomerate_pair(fm, cm, a->restrictAddr[i]);
     }
     return h;
 }
@@ -703,8 +789,20 @@ void oc_hier_free(oc_hier* h)
     {
         free(h->lev[i].diag);
         free(h->lev[i].coef);
+        free((void*)h->lev[i].ifOwn);
+        free((void*)h->lev[i].ifNbr);
+        free((void*)h->lev[i].ifCoeff);
     }
     free(h);
+}
+
+int oc_hier_level_pair(const oc_hier* h, int level, int* ifOwn, int* ifNbr, double* ifCoeff)
+{
+    const oc_level* L = &h->lev[level];
+    if (ifOwn) memcpy(ifOwn, L->ifOwn, sizeof(int) * (size_t)L->nIf);
+    if (ifNbr) memcpy(ifNbr, L->ifNbr, sizeof(int) * (size_t)L->nIf);
+    if (ifCoeff) memcpy(ifCoeff, L->ifCoeff, sizeof(double) * (size_t)L->nIf);
+    return L->nIf;
 }
 
 void oc_hier_level(const oc_hier* h, int level, double* diag, double* upper)
@@ -860,6 +958,10 @@ oc_perf oc_pcg_gamg_solve(const oc_agglom* a, const double* diag, const double* 
     A.upper = a->fine.upper;
     A.diag = (double*)diag;
     A.coef = (double*)upper;
+    A.nIf = 0;
+    A.ifOwn = NULL;
+    A.ifNbr = NULL;
+    A.ifCoeff = NULL;
     double* pA = (double*)xcalloc((size_t)n, sizeof(double));
     double* wA = (double*)xcalloc((size_t)n, sizeof(double));
     double* rA = (double*)xcalloc((size_t)n, sizeof(double));
@@ -930,7 +1032,17 @@ oc_perf oc_gamg_solve(const oc_agglom* a, const double* diag, const double* uppe
                       const double* source, double* psi, const oc_controls* c, double* history,
                       int historyCap)
 {
-    oc_hier* h = oc_hier_build(a, diag, upper);
+    return oc_gamg_solve_pair(a, diag, upper, 0, NULL, NULL, NULL, source, psi, c, history, historyCap);
+}
+
+/* gamgSolve (GAMG:943-959) with a coupled pair: gamgLevel0Interface's pair (GAMG:440-470) on the
+ * finest level, agglomerated onto every coarse level, on a folded system */
+oc_perf oc_gamg_solve_pair(const oc_agglom* a, const double* diag, const double* upper, int nIf,
+                           const int* ifOwn, const int* ifNbr, const double* ifCoeff,
+                           const double* source, double* psi, const oc_controls* c, double* history,
+                           int historyCap)
+{
+    oc_hier* h = oc_hier_build_pair(a, diag, upper, nIf, ifOwn, ifNbr, ifCoeff);
     const oc_level* F = &h->lev[0];
     const int n = F->nCells;
     double* Apsi = (double*)xcalloc((size_t)n, sizeof(double));
@@ -983,6 +1095,10 @@ static oc_level flat_level(int nC, int nF, const int* lower, const int* upper, c
     L.upper = upper;
     L.diag = (double*)diag;
     L.coef = (double*)coef;
+    L.nIf = 0;
+    L.ifOwn = NULL;
+    L.ifNbr = NULL;
+    L.ifCoeff = NULL;
     return L;
 }
 
@@ -1027,4 +1143,31 @@ void oc_scale(int nCells, int nFaces, const int* lower, const int* upper, const 
 {
     oc_level L = flat_level(nCells, nFaces, lower, upper, diag, coef);
     scale_l(&L, field, Acf, source);
+}
+
+void oc_amul_pair(int nCells, int nFaces, const int* lower, const int* upper, const double* diag,
+                  const double* coef, int nIf, const int* ifOwn, const int* ifNbr, const double* ifCoeff,
+                  const double* psi, double* Apsi)
+{
+    oc_level L = flat_level(nCells, nFaces, lower, upper, diag, coef);
+    L.nIf = nIf;
+    L.ifOwn = ifOwn;
+    L.ifNbr = ifNbr;
+    L.ifCoeff = ifCoeff;
+    amul_l(&L, psi, Apsi);
+}
+
+void oc_smooth_pair(int nCells, int nFaces, const int* lower, const int* upper, const double* diag,
+                    const double* coef, int nIf, const int* ifOwn, const int* ifNbr, const double* ifCoeff,
+                    double* psi, const double* source, int nSweeps, int smoother)
+{
+    oc_level L = flat_level(nCells, nFaces, lower, upper, diag, coef);
+    L.nIf = nIf;
+    L.ifOwn = ifOwn;
+    L.ifNbr = ifNbr;
+    L.ifCoeff = ifCoeff;
+    oc_smoother sm;
+    smoother_init(&sm, &L, smoother);
+    smoother_smooth(&sm, psi, source, nSweeps);
+    smoother_free(&sm);
 }

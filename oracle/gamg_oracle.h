@@ -72,8 +72,15 @@ void oc_agglom_weights(const oc_agglom* a, int step, double* w);
 /* Galerkin coarse matrices (GAMG:474-526); level i = 1..nLevels */
 typedef struct oc_hier oc_hier;
 oc_hier* oc_hier_build(const oc_agglom* a, const double* diag, const double* upper);
+/* ... with the finest level's coupled pair (nIf faces, each once from its own side; ifCoeff in the
+ * sign convention Amul subtracts, GAMG:25-36) and every coarse level's agglomerated from it
+ * (GAMG:497-524) */
+oc_hier* oc_hier_build_pair(const oc_agglom* a, const double* diag, const double* upper, int nIf,
+                            const int* ifOwn, const int* ifNbr, const double* ifCoeff);
 void oc_hier_free(oc_hier* h);
 void oc_hier_level(const oc_hier* h, int level, double* diag, double* upper);
+/* level `level`'s pair (any array may be NULL); returns its face count */
+int oc_hier_level_pair(const oc_hier* h, int level, int* ifOwn, int* ifNbr, double* ifCoeff);
 
 /* lduMatrix pieces on one level (GAMG:62-191) */
 void oc_amul(int nCells, int nFaces, const int* lower, const int* upper, const double* diag,
@@ -113,6 +120,19 @@ oc_perf oc_pcg_gamg_solve(const oc_agglom* a, const double* diag, const double* 
 oc_perf oc_gamg_solve(const oc_agglom* a, const double* diag, const double* upper,
                       const double* source, double* psi, const oc_controls* c, double* history,
                       int historyCap);
+/* gamgSolve with a coupled patch (GAMG:943-959): the same on a folded system with the finest
+ * level's pair (as oc_hier_build_pair takes it) */
+oc_perf oc_gamg_solve_pair(const oc_agglom* a, const double* diag, const double* upper, int nIf,
+                           const int* ifOwn, const int* ifNbr, const double* ifCoeff,
+                           const double* source, double* psi, const oc_controls* c, double* history,
+                           int historyCap);
+/* Amul and Smoother::smooth on one level with a pair (GAMG:82-87, :287-305) */
+void oc_amul_pair(int nCells, int nFaces, const int* lower, const int* upper, const double* diag,
+                  const double* coef, int nIf, const int* ifOwn, const int* ifNbr, const double* ifCoeff,
+                  const double* psi, double* Apsi);
+void oc_smooth_pair(int nCells, int nFaces, const int* lower, const int* upper, const double* diag,
+                    const double* coef, int nIf, const int* ifOwn, const int* ifNbr, const double* ifCoeff,
+                    double* psi, const double* source, int nSweeps, int smoother);
 
 #ifdef __cplusplus
 }

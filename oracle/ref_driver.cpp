@@ -8,12 +8,14 @@
 //                                  pair_gamg_agglomeration_cpp.cuh:99-105
 //   pcgGamgSolve (hierarchy form)  src/matrices/lduMatrix/solvers/GAMG/gamg_solver_cpp.cuh:202-213
 //   gamgSolveFolded                gamg_solver_cpp.cuh:185-192
+//   gamgSolve (with patches)       gamg_solver_cpp.cuh:170-177 (one coupled patch: the pair)
 //   gamgCoarsestPcgDic             gamg_solver_cpp.cuh:152-162
 //   gaussSeidelSmoothFolded        src/OpenFOAM/matrices/smooth_solver_cpp.cuh
 //   lduOwnerStart                  src/OpenFOAM/matrices/smooth_solver_cpp.cu:10-34
 #include "gamg_solver_cpp.cuh"
 #include "smooth_solver_cpp.cuh"
 #include "fv_geometry.cuh"
+#include "fv_patch.cuh"
 #include "primitive_mesh.cuh"
 
 #include <cstring>
@@ -223,6 +225,47 @@ int ref_gamg_solve(void* h, const double* diag, const double* upper, const doubl
         const SolverPerformance p = gamgSolveFolded(a, d, u, s, x, toGamg(*c), nullptr);
         std::memcpy(psi, x.data(), sizeof(double) * static_cast<std::size_t>(nC));
         *out = toPerf(p);
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+// gamgSolve on a folded system plus one coupled patch carrying the pair: faceCells `own`, the
+// neighbour cells `nbr` face for face, boundaryCoeffs `coeff` (the interface coefficients) and
+// internalCoeffs zero, so foldBoundary leaves diag and source as they are handed in.
+int ref_gamg_solve_pair(void* h, const double* diag, const double* upper, const double* source,
+                        double* psi, int nIf, const int* own, const int* nbr, const double* coeff,
+                        const Controls* c, Perf* out)
+{
+    try
+    {
+        const GamgAgglomeration& a = static_cast<RefAgglom*>(h)->a;
+        const int nC = a.fineMesh.nCells;
+        const int nF = static_cast<int>(a.fineMesh.upperAddr.size());
+        PrimitiveMesh m = addressingMesh(nC, nF, a.fineMesh.lowerAddr.data(), a.fineMesh.upperAddr.data());
+        FvScalarMatrix M;
+        M.diag.assign(diag, diag + nC);
+        M.upper.assign(upper, upper + nF);
+        M.lower = M.upper;
+        M.source.assign(source, source + nC);
+        std::vector<FvPatch> patches(1);
+        FvPatch& p = patches[0];
+        p.name = "pair";
+        p.type = "cyclic";
+        p.size = nIf;
+        p.faceCells.assign(own, own + nIf);
+        p.nbrFaceCells.assign(nbr, nbr + nIf);
+        p.coupled = true;
+        M.internalCoeffs.assign(1, std::vector<scalar>(static_cast<std::size_t>(nIf), scalar(0)));
+        M.boundaryCoeffs.assign(1, std::vector<scalar>(coeff, coeff + nIf));
+        std::vector<scalar> x(psi, psi + nC);
+        const SolverPerformance perf = gamgSolve(M, x, m, patches, a, toGamg(*c), nullptr);
+        std::memcpy(psi, x.data(), sizeof(double) * static_cast<std::size_t>(nC));
+        *out = toPerf(perf);
         return 0;
     }
     catch (const std::exception& e)
