@@ -755,6 +755,8 @@ Batch::Batch(std::vector<Matrix*> cs, cudaStream_t s) : stream(s), cases(std::mo
     {
         if (!A) fail(B2G_ERR_ARGUMENT, "b2g batch: null case");
         if (A->mesh->device != dev) fail(B2G_ERR_ARGUMENT, "b2g batch: every case must live on the current device");
+        if (A->coupled)
+            fail(B2G_ERR_REFUSED, "b2g batch: a matrix with a coupled pair is solved alone (b2g_gamg_solve_coupled)");
         if (A->nLevels() == 0)
             fail(B2G_ERR_REFUSED, "b2g GAMG: no coarse levels created, either matrix too small for GAMG or "
                                   "nCellsInCoarsestLevel too large (GAMGSolver.C:333).");

@@ -444,6 +444,12 @@ void solveOn(b2g::Matrix& A, const double* source, double* psi, const b2g_contro
     need(memspace == B2G_MEM_HOST || memspace == B2G_MEM_DEVICE, "b2g solve: bad memspace");
     need(c->precision >= B2G_PRECISION_FP64 && c->precision <= B2G_PRECISION_FP32_PRECOND_MULTICOLOUR,
          "b2g solve: unknown precision form");
+    if (A.coupled && !standalone)
+        b2g::fail(B2G_ERR_REFUSED, "b2g: PCG with the GAMG preconditioner refuses coupled patches, as the reference's "
+                                   "pcgGamgSolve does (gamg_solver_cpp.cu:1045); the standalone GAMG solve carries the "
+                                   "pair (b2g_gamg_solve_coupled)");
+    if (A.coupled && c->precision != B2G_PRECISION_FP64)
+        b2g::fail(B2G_ERR_REFUSED, "b2g: a matrix with a coupled pair is solved in the FP64 form only");
     const int n0 = A.n(0);
     // the solve runs in the finest level's position order: host fields are staged in fc/fr (free
     // outside a solve) and permuted on the device; device fields are permuted in place of a copy
@@ -978,6 +984,92 @@ b2g_status b2g_gamg_solve(b2g_mesh* mesh, const double* diag, const double* uppe
     });
 }
 
+b2g_status b2g_mesh_set_pair(b2g_mesh* mesh, int nPairFaces, const int32_t* faceCells, const int32_t* nbrFaceCells,
+                             int memspace, void* stream)
+{
+    return guarded([&] {
+        need(mesh && faceCells && nbrFaceCells, "b2g_mesh_set_pair: null argument");
+        need(memspace == B2G_MEM_HOST || memspace == B2G_MEM_DEVICE, "b2g_mesh_set_pair: bad memspace");
+        need(nPairFaces > 0, "b2g_mesh_set_pair: nPairFaces must be positive");
+        (void)stream;
+        std::vector<int> own(static_cast<size_t>(nPairFaces)), nbr(static_cast<size_t>(nPairFaces));
+        const cudaMemcpyKind kind = memspace == B2G_MEM_HOST ? cudaMemcpyHostToHost : cudaMemcpyDeviceToHost;
+        B2G_CUDA(cudaMemcpy(own.data(), faceCells, sizeof(int) * own.size(), kind));
+        B2G_CUDA(cudaMemcpy(nbr.data(), nbrFaceCells, sizeof(int) * nbr.size(), kind));
+        b2g::buildPair(mesh->m, nPairFaces, own.data(), nbr.data());
+    });
+}
+
+b2g_status b2g_mesh_level_pair(const b2g_mesh* mesh, int level, int* nPairFaces, int32_t* own, int32_t* nbr)
+{
+    return guarded([&] {
+        need(mesh && nPairFaces, "b2g_mesh_level_pair: null argument");
+        need(level >= 0 && level <= mesh->m.nLevels(), "b2g_mesh_level_pair: level out of range");
+        const b2g::PairLevel& P = mesh->m.lev[level].pair;
+        *nPairFaces = P.nFaces;
+        if (own) std::copy(P.own.begin(), P.own.end(), own);
+        if (nbr) std::copy(P.nbr.begin(), P.nbr.end(), nbr);
+    });
+}
+
+b2g_status b2g_matrix_create_coupled(b2g_mesh* mesh, const double* diag, const double* upper, const double* pairCoeffs,
+                                     int memspace, void* stream, b2g_matrix** out)
+{
+    return guarded([&] {
+        need(mesh && out && diag && pairCoeffs, "b2g_matrix_create_coupled: null argument");
+        need(memspace == B2G_MEM_HOST || memspace == B2G_MEM_DEVICE, "b2g_matrix_create_coupled: bad memspace");
+        need(mesh->m.lev[0].nFaces == 0 || upper, "b2g_matrix_create_coupled: null upper");
+        need(mesh->m.hasPair, "b2g_matrix_create_coupled: the mesh carries no coupled pair (b2g_mesh_set_pair)");
+        std::unique_ptr<b2g_matrix> h(new b2g_matrix);
+        h->mesh = mesh;
+        (void)stream;
+        h->mat.reset(new b2g::Matrix(&mesh->m, mesh->m.stream));
+        h->mat->setFine(diag, upper, memspace);
+        h->mat->setPairCoeffs(pairCoeffs, memspace);
+        h->mat->buildCoarse();
+        B2G_CUDA(cudaStreamSynchronize(mesh->m.stream));
+        *out = h.release();
+    });
+}
+
+b2g_status b2g_matrix_level_pair_coeffs(const b2g_matrix* m, int level, double* coeffs)
+{
+    return guarded([&] {
+        need(m && coeffs, "b2g_matrix_level_pair_coeffs: null argument");
+        const b2g::Matrix& A = *m->mat;
+        need(level >= 0 && level <= A.nLevels(), "b2g_matrix_level_pair_coeffs: level out of range");
+        need(A.coupled, "b2g_matrix_level_pair_coeffs: the matrix carries no coupled pair");
+        const int nF = A.mesh->lev[level].pair.nFaces;
+        B2G_CUDA(cudaMemcpyAsync(coeffs, A.v64.coef[level].pairCoef.p, sizeof(double) * nF, cudaMemcpyDeviceToHost,
+                                 A.stream));
+        B2G_CUDA(cudaStreamSynchronize(A.stream));
+    });
+}
+
+b2g_status b2g_gamg_solve_coupled(b2g_mesh* mesh, const double* diag, const double* upper, const double* pairCoeffs,
+                                  const double* source, double* psi, const b2g_controls* controls, int memspace,
+                                  void* stream, b2g_perf* out, b2g_solve_log* log)
+{
+    return guarded([&] {
+        need(mesh && diag && pairCoeffs && controls, "b2g_gamg_solve_coupled: null argument");
+        need(mesh->m.hasPair, "b2g_gamg_solve_coupled: the mesh carries no coupled pair (b2g_mesh_set_pair)");
+        (void)stream;
+        b2g::Matrix A(&mesh->m, mesh->m.stream);
+        A.setFine(diag, upper, memspace);
+        A.setPairCoeffs(pairCoeffs, memspace);
+        b2g::capi::solveOn(A, source, psi, controls, memspace, out, log, true);
+    });
+}
+
+b2g_status b2g_matrix_gamg_solve(b2g_matrix* m, const double* source, double* psi, const b2g_controls* controls,
+                                 int memspace, b2g_perf* out, b2g_solve_log* log)
+{
+    return guarded([&] {
+        need(m != nullptr, "b2g_matrix_gamg_solve: null matrix");
+        b2g::capi::solveOn(*m->mat, source, psi, controls, memspace, out, log, true);
+    });
+}
+
 b2g_status b2g_matrix_timings(const b2g_matrix* m, double* ms4, long long* counts4)
 {
     return guarded([&] {
@@ -1092,6 +1184,12 @@ extern "C" B2G_API b2g_status b2g_level_pcg_dic_static(b2g_matrix* m, int level,
         a.logCount = nullptr;
         a.logCapacity = 0;
         a.out = perf;
+        if (C.pairVal.p && L.pair.nFaces > 0)
+        {
+            a.pairStart = L.pair.start.p;
+            a.pairCol = L.pair.col.p;
+            a.pairVal = C.pairVal.p;
+        }
         b2g::k::coarsestPcgDic<double><<<1, 32, 0, s>>>(a);
         B2G_LAUNCH_CHECK();
         if (n) b2g::k::fromPositions<double><<<grid, 256, 0, s>>>(n, L.gs.posCell.p, psiPos, psi);

@@ -47,6 +47,12 @@ struct CoarsestArgs
     int* logCount;      // appended when log != null
     int logCapacity;
     DevPerf* out;       // may be null
+    // the level's coupled pair by position (ldu_kernels.cuh Rows), or null: Amul subtracts
+    // pairVal * x[pairCol] after the face terms, sumA subtracts pairVal (GAMG:82-87, :137-145); DIC's
+    // factorisation does not see it (GAMG:194-231)
+    const int* __restrict__ pairStart = nullptr;
+    const int* __restrict__ pairCol = nullptr;
+    const T* __restrict__ pairVal = nullptr;
 };
 
 template <class T> struct PerfConst;
@@ -66,6 +72,9 @@ __device__ __forceinline__ void warpAmul(const CoarsestArgs<T>& a, const T* x, T
     {
         T acc = mulRn(a.diag[c], x[c]);
         for (int e = a.rowStart[c]; e < a.rowStart[c + 1]; ++e) acc = addRn(acc, mulRn(a.val[e], x[a.col[e]]));
+        if (a.pairStart)
+            for (int k = a.pairStart[c]; k < a.pairStart[c + 1]; ++k)
+                acc = subRn(acc, mulRn(a.pairVal[k], x[a.pairCol[k]]));
         y[c] = acc;
     }
     __syncwarp();
@@ -109,6 +118,8 @@ __device__ __forceinline__ void coarsestPcgDicWarp(const CoarsestArgs<T>& a)
     {
         T s = a.diag[c];
         for (int e = a.rowStart[c]; e < a.rowStart[c + 1]; ++e) s = addRn(s, a.val[e]);
+        if (a.pairStart)
+            for (int k = a.pairStart[c]; k < a.pairStart[c + 1]; ++k) s = subRn(s, a.pairVal[k]);
         a.pA[c] = s;
     }
     __syncwarp();

@@ -75,6 +75,21 @@ struct Colouring
     float msPerSweep = 0.f;
 };
 
+// The coupled (cyclic) pair of one level (pair.cu, b2g_mesh_set_pair): its faces, each once from
+// its own side, as (own, nbr) cells of this level in face order -- the finest level's as the coupled
+// patches list them (gamgLevel0Interface, GAMG:440-470), a coarse level's agglomerated from the finer
+// one on the coarse cell pair (GAMG:497-524). By position, the pair entries of each row in face order.
+struct PairLevel
+{
+    int nFaces = 0;
+    std::vector<int> own, nbr;  // host, cells of this level
+    DBuf<int> start;            // [nCells+1] position -> its entries (the faces the cell owns)
+    DBuf<int> col;              // [nFaces] per entry: the neighbour's position
+    DBuf<int> face;             // [nFaces] per entry: the pair face
+    DBuf<int> fStart;           // coarse levels: [nFaces+1] this level's face -> the finer level's
+    DBuf<int> fList;            //   faces that merged into it, ascending (the coefficient sum's order)
+};
+
 // One level's addressing and its derived layouts (built once per hierarchy).
 struct LevelAddr
 {
@@ -105,6 +120,7 @@ struct LevelAddr
     DBuf<int> lowerPos;
     std::unique_ptr<LevelAddr> revDesc;
     DBuf<int> revDescPos;
+    PairLevel pair;         // the coupled pair, if the mesh carries one (nFaces 0 otherwise)
 };
 
 // Level step i -> i+1 (GamgAgglomeration's restrictAddressing / faceRestrictAddressing /
@@ -135,6 +151,7 @@ struct Mesh
     std::vector<LevelAddr> lev;  // [0] the mesh, [i] coarse level i
     std::vector<Step> step;      // [i] level i -> i+1
     float buildMs = 0.f;
+    bool hasPair = false;        // b2g_mesh_set_pair was called (every level's PairLevel is built)
     int nLevels() const { return static_cast<int>(step.size()); }
 };
 
@@ -161,6 +178,10 @@ void buildHierarchy(Mesh& M, const double* dSf, const double* dMagSf, int nCells
 // skipped; maps[i] is step i's restrictAddr (host), nCoarse[i] its coarse cell count.
 void buildHierarchyFromMaps(Mesh& M, const double* dSf, const double* dMagSf,
                             const std::vector<std::vector<int>>& maps, const std::vector<int>& nCoarse);
+
+// The coupled pair on every level (pair.cu): the finest level's nFaces faces (host cells own/nbr),
+// each coarse level's agglomerated from the finer one.
+void buildPair(Mesh& M, int nFaces, const int* own, const int* nbr);
 
 // Exclusive scan helper (n+1 outputs: out[0] = 0 ... out[n] = total); returns the total.
 long long exclusiveScan(const int* in, int* out, int n, cudaStream_t s);

@@ -27,6 +27,11 @@ template <> struct Small<float>
 // terms (GAMG:62-117). `col` is the other cell's position, `val` the coefficient per entry, `diag`
 // the diagonal by position. Every per-cell result is the reference's bit for bit; only where the
 // cells sit in memory differs.
+//
+// A coupled (cyclic) pair, when the level carries one (pair.cu): per position the pair faces the cell
+// owns, in face order -- [pairStart[i], pairStart[i+1]) -- with the neighbour's position and the
+// coefficient, in the reference's sign convention (Amul subtracts coefficient * x[neighbour],
+// GAMG:82-87). pairStart null: no pair, and every kernel below computes exactly what it did without.
 template <class T>
 struct Rows
 {
@@ -35,7 +40,22 @@ struct Rows
     const int* __restrict__ col;
     const T* __restrict__ val;
     const T* __restrict__ diag;
+    const int* __restrict__ pairStart = nullptr;
+    const int* __restrict__ pairCol = nullptr;
+    const T* __restrict__ pairVal = nullptr;
 };
+
+// The pair's terms of row c after the face terms, in face order: acc - coef*x[nbr] each (Amul's sign)
+template <class T>
+__device__ __forceinline__ T pairSub(const Rows<T>& A, int c, T acc, const T* __restrict__ x)
+{
+    if (A.pairStart)
+    {
+        const int k1 = A.pairStart[c + 1];
+        for (int k = A.pairStart[c]; k < k1; ++k) acc = subRn(acc, mulRn(A.pairVal[k], x[A.pairCol[k]]));
+    }
+    return acc;
+}
 
 // lduMatrix::Amul (GAMG:62-88): y = diag*x, then the face terms in face order
 template <class T>
@@ -46,7 +66,7 @@ __global__ void amul(Rows<T> A, const T* __restrict__ x, T* __restrict__ y)
         T acc = mulRn(A.diag[c], x[c]);
         const int e1 = A.rowStart[c + 1];
         for (int e = A.rowStart[c]; e < e1; ++e) acc = addRn(acc, mulRn(A.val[e], x[A.col[e]]));
-        y[c] = acc;
+        y[c] = pairSub(A, c, acc, x);
     }
 }
 
@@ -84,6 +104,7 @@ __global__ void __launch_bounds__(NT) amulScaleDots(Rows<T> A, const T* __restri
         T acc = mulRn(A.diag[c], fc);
         const int e1 = A.rowStart[c + 1];
         for (int e = A.rowStart[c]; e < e1; ++e) acc = addRn(acc, mulRn(A.val[e], field[A.col[e]]));
+        acc = pairSub(A, c, acc, field);
         Acf[c] = acc;
         num = addRn(num, mulRn(fc, source[c]));
         den = addRn(den, mulRn(fc, acc));
@@ -243,6 +264,10 @@ __global__ void residual(Rows<T> A, const T* __restrict__ source, const T* __res
         T acc = subRn(source[c], mulRn(A.diag[c], psi[c]));
         const int e1 = A.rowStart[c + 1];
         for (int e = A.rowStart[c]; e < e1; ++e) acc = subRn(acc, mulRn(A.val[e], psi[A.col[e]]));
+        // the pair with the sign Amul's term does not have (GAMG:110-115)
+        if (A.pairStart)
+            for (int k = A.pairStart[c]; k < A.pairStart[c + 1]; ++k)
+                acc = addRn(acc, mulRn(A.pairVal[k], psi[A.pairCol[k]]));
         r[c] = acc;
     }
 }
@@ -285,6 +310,28 @@ __global__ void __launch_bounds__(NT) reduceFinal(const T* __restrict__ partial,
     if (threadIdx.x == 0) *out = s;
 }
 
+// sumA's pair terms (GAMG:137-145): minus each coefficient, in face order
+template <class T>
+__device__ __forceinline__ T pairRowSum(const Rows<T>& A, int c, T sumA)
+{
+    if (A.pairStart)
+        for (int k = A.pairStart[c]; k < A.pairStart[c + 1]; ++k) sumA = subRn(sumA, A.pairVal[k]);
+    return sumA;
+}
+
+// GaussSeidelSmoother's bPrime with the pair moved to the right-hand side (GAMG:287-305): source plus
+// coefficient * psi[neighbour] per pair face, in face order, from psi as it stands
+template <class T>
+__global__ void pairFold(Rows<T> A, const T* __restrict__ source, const T* __restrict__ psi, T* __restrict__ bPrime)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.n; c += gridDim.x * blockDim.x)
+    {
+        T b = source[c];
+        for (int k = A.pairStart[c]; k < A.pairStart[c + 1]; ++k) b = addRn(b, mulRn(A.pairVal[k], psi[A.pairCol[k]]));
+        bPrime[c] = b;
+    }
+}
+
 // normFactor (GAMG:119-159), the per-cell summand |Apsi - t| + |source - t| with t = sumA*xRef;
 // sumA = diag + the row's coefficients in row order (the reference adds a cell's face terms in
 // face order, which is row order)
@@ -301,6 +348,7 @@ __global__ void __launch_bounds__(NT) normFactorPartial(Rows<T> A, const T* __re
         T sumA = A.diag[c];
         const int e1 = A.rowStart[c + 1];
         for (int e = A.rowStart[c]; e < e1; ++e) sumA = addRn(sumA, A.val[e]);
+        sumA = pairRowSum(A, c, sumA);
         const T t = mulRn(sumA, xRef);
         s = addRn(s, addRn(fabs(subRn(Apsi[c], t)), fabs(subRn(source[c], t))));
     }
@@ -399,6 +447,7 @@ static __global__ void __launch_bounds__(32) serialNormFactor(Rows<double> A, co
             const int i = posOf[c];
             double sumA = A.diag[i];
             for (int e = A.rowStart[i]; e < A.rowStart[i + 1]; ++e) sumA = __dadd_rn(sumA, A.val[e]);
+            sumA = pairRowSum(A, i, sumA);
             const double t = __dmul_rn(sumA, xRef);
             term = __dadd_rn(fabs(__dsub_rn(Apsi[i], t)), fabs(__dsub_rn(source[i], t)));
         }

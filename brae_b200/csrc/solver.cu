@@ -132,10 +132,18 @@ bool convergedH(double fin, double init, double tol, double relTol)
     return fin < tol || (relTol > kSmall && fin < relTol * init);
 }
 
+// the level's rows, with the coupled pair's entries when the matrix carries one
 template <class T>
 k::Rows<T> rowsOf(const LevelAddr& L, const LevelCoef<T>& C)
 {
-    return k::Rows<T>{L.nCells, L.gs.posRow.p, L.gs.entColPos.p, C.rowVal.p, C.gsDiag.p};
+    k::Rows<T> r{L.nCells, L.gs.posRow.p, L.gs.entColPos.p, C.rowVal.p, C.gsDiag.p};
+    if (C.pairVal.p && L.pair.nFaces > 0)
+    {
+        r.pairStart = L.pair.start.p;
+        r.pairCol = L.pair.col.p;
+        r.pairVal = C.pairVal.p;
+    }
+    return r;
 }
 
 // the position-ordered coefficients of one level: diagonal and CSR rows
@@ -667,6 +675,20 @@ void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps,
         return;
     }
     if (mesh->lev[level].nCells == 0) return;
+    const LevelAddr& L = mesh->lev[level];
+    VCycleData<T>& D = data<T>();
+    if (D.coef[level].pairVal.p && L.pair.nFaces > 0)
+    {
+        // the pair enters the Gauss-Seidel smoothers through bPrime, once per smooth() call, from psi
+        // as it stands (GAMG:287-305); the sweeps then run on bPrime
+        if (D.pairB.size() <= static_cast<size_t>(level)) D.pairB.resize(level + 1);
+        if (!D.pairB[level].p) D.pairB[level].alloc(nAlloc(level), stream);
+        k::pairFold<T><<<rowsGrid(L.nCells), NT, 0, stream>>>(rowsOf(L, D.coef[level]), src, psiL,
+                                                               D.pairB[level].p);
+        B2G_LAUNCH_CHECK();
+        ++launches;
+        src = D.pairB[level].p;
+    }
     if (symmetric)
     {
         symSmooth<T>(level, psiL, src, nSweeps);
@@ -743,6 +765,13 @@ void Matrix::prepareSmoother(const b2g_controls& c)
 {
     const bool sym = c.smoother == B2G_SMOOTHER_SYM_GAUSS_SEIDEL;
     const bool dic = c.smoother == B2G_SMOOTHER_DIC || c.smoother == B2G_SMOOTHER_DIC_GAUSS_SEIDEL;
+    if (coupled && c.smoother != B2G_SMOOTHER_DIC)
+    {
+        // the Gauss-Seidel smoothers' bPrime per level, allocated before any iteration is captured
+        if (v64.pairB.size() < static_cast<size_t>(nLevels())) v64.pairB.resize(nLevels());
+        for (int i = 0; i < nLevels(); ++i)
+            if (!v64.pairB[i].p) v64.pairB[i].alloc(nAlloc(i), stream);
+    }
     if (!sym && !dic) return;
     const bool fp64 = c.precision == B2G_PRECISION_FP64 || c.solver == B2G_SOLVER_GAMG;
     for (int i = 0; i < nLevels(); ++i)
@@ -1149,6 +1178,12 @@ void Matrix::coarsestSolve<double>(int level, double* x, const double* src, doub
     a.logCount = coarseCount.p;
     a.logCapacity = coarseLogCapacity;
     a.out = out;
+    if (C.pairVal.p && L.pair.nFaces > 0)
+    {
+        a.pairStart = L.pair.start.p;
+        a.pairCol = L.pair.col.p;
+        a.pairVal = C.pairVal.p;
+    }
     k::coarsestPcgDic<double><<<1, 32, 0, stream>>>(a);
     B2G_LAUNCH_CHECK();
     ++launches;
@@ -1276,6 +1311,8 @@ void Matrix::precondition(const b2g_controls& c, double* w, const double* r)
 {
     const int n0 = n(0);
     multicolour = c.precision == B2G_PRECISION_FP32_PRECOND_MULTICOLOUR;
+    if (coupled && c.precision != B2G_PRECISION_FP64)
+        fail(B2G_ERR_REFUSED, "b2g: a matrix with a coupled pair is solved in the FP64 form only.");
     if (c.precision == B2G_PRECISION_FP32_PRECOND || multicolour)
     {
         if (multicolour) ensureMulticolour();

@@ -26,6 +26,8 @@ struct LevelCoef
     DBuf<T> rowVal; // [2*nFaces] coefficient per CSR entry, rows by position
     DBuf<unsigned char> blob;  // the sweep's chunk blobs (gs_kernels.cuh) in T
     DBuf<float> mcVal, mcDiag;  // FP32 only: the multicolour layout's coefficients (hierarchy.cuh Colouring)
+    // FP64 only, a coupled matrix: the pair's coefficient per pair face and per row entry (pair.cu)
+    DBuf<T> pairCoef, pairVal;
 };
 
 // Everything a V-cycle in value type T touches.
@@ -47,6 +49,8 @@ struct VCycleData
     // descending reversed level's chunk blobs, diagonal 1), rD by position, and scratch vectors
     std::vector<LevelCoef<T>> dicLo, dicUp;
     std::vector<DBuf<T>> rdPos, dicR, dicLoB, dicLoX, dicUpB, dicUpX;
+    // a coupled matrix: per level the Gauss-Seidel smoothers' bPrime with the pair folded in
+    std::vector<DBuf<T>> pairB;
     // FP32 form only: dense Cholesky of the coarsest level
     bool built = false;
 };
@@ -82,6 +86,7 @@ struct Matrix
     int coarseLogCapacity = 0;
     IterationGraph pcgGraph, gamgGraph;
     bool serial = false;                      // B2G_REDUCTION_SERIAL for the current solve
+    bool coupled = false;                     // the matrix carries the mesh's coupled pair (FP64 only)
     bool multicolour = false;                 // the FP32 V-cycle sweeps colour by colour
     bool mcBuilt = false;
     // timing (b2g_set_profiling): events around the finest level's Amul and Gauss-Seidel launches
@@ -101,6 +106,7 @@ struct Matrix
 
     Matrix(Mesh* m, cudaStream_t s);
     void setFine(const double* diag, const double* upper, int memspace);
+    void setPairCoeffs(const double* coeff, int memspace);  // the coupled pair's coefficients (pair.cu)
     void buildCoarse();                       // Galerkin matrices of every coarse level
     void ensureFp32();                        // float copies of every level
     void ensureMulticolour();                 // the multicolour layout and its FP32 values

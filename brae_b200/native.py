@@ -115,6 +115,13 @@ def _load():
         "b2g_server_submit": (ip, [vp, ip, vp, vp, C.POINTER(Controls), C.POINTER(C.c_longlong)]),
         "b2g_server_wait": (ip, [vp, C.c_longlong, C.POINTER(_Perf), C.POINTER(C.c_double), ip]),
         "b2g_server_case_bytes": (ip, [vp, ip, C.POINTER(C.c_ulonglong)]),
+        "b2g_mesh_set_pair": (ip, [vp, ip, vp, vp, ip, vp]),
+        "b2g_mesh_level_pair": (ip, [vp, ip, C.POINTER(C.c_int), vp, vp]),
+        "b2g_gamg_solve_coupled": (ip, [vp, vp, vp, vp, vp, vp, C.POINTER(Controls), ip, vp, C.POINTER(_Perf),
+                                        C.POINTER(_Log)]),
+        "b2g_matrix_create_coupled": (ip, [vp, vp, vp, vp, ip, vp, C.POINTER(vp)]),
+        "b2g_matrix_level_pair_coeffs": (ip, [vp, ip, vp]),
+        "b2g_matrix_gamg_solve": (ip, [vp, vp, vp, C.POINTER(Controls), ip, C.POINTER(_Perf), C.POINTER(_Log)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -134,7 +141,8 @@ EXPORTED = [
     "b2g_matrix_pcg_solve", "b2g_matrix_timings", "b2g_level_smooth_trace", "b2g_level_pcg_dic_static",
     "b2g_level_schedule", "b2g_level_colouring", "b2g_fold_boundary", "b2g_level_sweep_shape", "b2g_server_create", "b2g_server_destroy", "b2g_server_add_case",
     "b2g_server_submit", "b2g_server_wait", "b2g_server_case_bytes", "b2g_batch_create", "b2g_batch_solve",
-    "b2g_batch_launches", "b2g_batch_destroy",
+    "b2g_batch_launches", "b2g_batch_destroy", "b2g_mesh_set_pair", "b2g_mesh_level_pair",
+    "b2g_gamg_solve_coupled", "b2g_matrix_create_coupled", "b2g_matrix_level_pair_coeffs", "b2g_matrix_gamg_solve",
 ]
 
 
@@ -277,6 +285,22 @@ class Mesh:
         return {"one_block": whole.value == 1, "cluster_ctas": whole.value if whole.value > 1 else 0,
                 "threads": thr.value, "ms_per_sweep": ms.value}
 
+    def set_pair(self, own, nbr) -> None:
+        """The coupled (cyclic) pair: faceCells and neighbour cells of the coupled patches' faces, each
+        face once from its own side (b2g_mesh_set_pair); every coarse level's is built from it."""
+        o = np.ascontiguousarray(own, np.int32)
+        n = np.ascontiguousarray(nbr, np.int32)
+        _check(lib.b2g_mesh_set_pair(self.handle, int(o.shape[0]), _ptr(o), _ptr(n), B2G_MEM_HOST, None))
+
+    def level_pair(self, level: int):
+        """Level `level`'s pair as (own, nbr) cell arrays of that level."""
+        m = C.c_int()
+        _check(lib.b2g_mesh_level_pair(self.handle, level, C.byref(m), None, None))
+        o = np.empty(m.value, np.int32)
+        n = np.empty(m.value, np.int32)
+        _check(lib.b2g_mesh_level_pair(self.handle, level, C.byref(m), _ptr(o), _ptr(n)))
+        return o, n
+
     def step(self, i: int) -> dict:
         nc, nf = self.level_size(i)
         cc, cf = self.level_size(i + 1)
@@ -309,16 +333,36 @@ class _LogBuf:
 class Matrix:
     """One folded matrix on a mesh's hierarchy (GamgHierarchy): Galerkin levels on the device."""
 
-    def __init__(self, mesh: Mesh, diag, upper):
+    def __init__(self, mesh: Mesh, diag, upper, pair_coeffs=None):
         if not _is_torch(diag):
             diag = _as_host(diag, np.float64)
             upper = _as_host(upper, np.float64)
+            if pair_coeffs is not None:
+                pair_coeffs = _as_host(pair_coeffs, np.float64)
         ms = _memspace(diag, upper)
         h = C.c_void_p()
-        _check(lib.b2g_matrix_create(mesh.handle, _ptr(diag), _ptr(upper), ms, _stream(),
-                                     C.byref(h)))
+        if pair_coeffs is None:
+            _check(lib.b2g_matrix_create(mesh.handle, _ptr(diag), _ptr(upper), ms, _stream(), C.byref(h)))
+        else:
+            _check(lib.b2g_matrix_create_coupled(mesh.handle, _ptr(diag), _ptr(upper), _ptr(pair_coeffs), ms,
+                                                 _stream(), C.byref(h)))
         self.handle = h
         self.mesh = mesh
+
+    def pair_coeffs(self, level: int):
+        m = len(self.mesh.level_pair(level)[0])
+        c = np.empty(m)
+        _check(lib.b2g_matrix_level_pair_coeffs(self.handle, level, _ptr(c)))
+        return c
+
+    def gamg_solve(self, source, psi, controls: Controls, history_cap=100000):
+        """The standalone GAMG solve on this matrix (b2g_matrix_gamg_solve)."""
+        ms = _memspace(source, psi)
+        p = _Perf()
+        lb = _LogBuf(history_cap, 0)
+        _check(lib.b2g_matrix_gamg_solve(self.handle, _ptr(source), _ptr(psi), C.byref(controls), ms, C.byref(p),
+                                         C.byref(lb.log)))
+        return SolverPerformance(p.initialResidual, p.finalResidual, p.nIterations), lb.history()
 
     def __del__(self):
         h = getattr(self, "handle", None)
@@ -430,6 +474,23 @@ def gamg_solve(mesh: Mesh, diag, upper, source, psi, controls: Controls,
     lb = _LogBuf(history_cap, 0)
     _check(lib.b2g_gamg_solve(mesh.handle, _ptr(diag), _ptr(upper), _ptr(source), _ptr(psi),
                               C.byref(controls), ms, _stream(), C.byref(p), C.byref(lb.log)))
+    return SolverPerformance(p.initialResidual, p.finalResidual, p.nIterations), lb.history()
+
+
+def gamg_solve_coupled(mesh: Mesh, diag, upper, pair_coeffs, source, psi, controls: Controls,
+                       history_cap: int = 100000):
+    """gamgSolve with coupled patches (gamg_solver_cpp.cuh:174-181) on a folded system: the mesh's
+    pair (Mesh.set_pair) with these coefficients, in the sign convention Amul subtracts."""
+    if not _is_torch(diag):
+        diag = _as_host(diag, np.float64)
+        upper = _as_host(upper, np.float64)
+        pair_coeffs = _as_host(pair_coeffs, np.float64)
+        source = _as_host(source, np.float64)
+    ms = _memspace(diag, upper, pair_coeffs, source, psi)
+    p = _Perf()
+    lb = _LogBuf(history_cap, 0)
+    _check(lib.b2g_gamg_solve_coupled(mesh.handle, _ptr(diag), _ptr(upper), _ptr(pair_coeffs), _ptr(source),
+                                      _ptr(psi), C.byref(controls), ms, _stream(), C.byref(p), C.byref(lb.log)))
     return SolverPerformance(p.initialResidual, p.finalResidual, p.nIterations), lb.history()
 
 

@@ -11,6 +11,8 @@
  *   GAMGH = src/matrices/lduMatrix/solvers/GAMG/gamg_solver_cpp.cuh
  *   AGGH  = src/matrices/lduMatrix/solvers/GAMG/GAMGAgglomerations/pair_gamg_agglomeration_cpp.cuh
  *   DGAMG = src/matrices/lduMatrix/solvers/GAMG/device_gamg_solver.cuh
+ *   GAMG  = src/matrices/lduMatrix/solvers/GAMG/gamg_solver_cpp.cu
+ *   DGAMGC = src/matrices/lduMatrix/solvers/GAMG/device_gamg_solver.cu
  *   PCGH  = src/OpenFOAM/matrices/pcg.cuh
  *
  * Conventions
@@ -226,6 +228,46 @@ B2G_API b2g_status b2g_gamg_solve(b2g_mesh* mesh, const double* diag, const doub
                                   const double* source, double* psi,
                                   const b2g_controls* controls, int memspace, void* stream,
                                   b2g_perf* out, b2g_solve_log* log);
+
+/* ---- the coupled (cyclic) pair ------------------------------------------------------------------ */
+
+/* The mesh's coupled pair, once per mesh: the faces of its coupled (cyclic) patches, each once from
+ * its own side -- faceCells[i] the cell the face belongs to, nbrFaceCells[i] the cell across the pair
+ * -- in patch order, then face order, as gamgLevel0Interface lists them (GAMG:440-470). Every coarse
+ * level's pair is agglomerated from it on the coarse cell pair, the first face of a pair making the
+ * coarse face and later ones merging into it (agglomerateMatrix, GAMG:497-524; the reference's device
+ * arm builds the same in buildGamgInterfaces, DGAMGC:335-391). A second call is refused. */
+B2G_API b2g_status b2g_mesh_set_pair(b2g_mesh* mesh, int nPairFaces, const int32_t* faceCells,
+                                     const int32_t* nbrFaceCells, int memspace, void* stream);
+/* Level `level`'s pair: *nPairFaces and, if not NULL, its faces' cells (HOST arrays of that size). */
+B2G_API b2g_status b2g_mesh_level_pair(const b2g_mesh* mesh, int level, int* nPairFaces, int32_t* own,
+                                       int32_t* nbr);
+
+/* gamgSolve with coupled patches (GAMGH:174-181; its device arm deviceGamgSolve, DGAMGC:713-764): the standalone GAMG solve of a folded system whose coupled patches carry the pair.
+ * `pairCoeffs` [nPairFaces] are the coupled patches' boundaryCoeffs in b2g_mesh_set_pair's face
+ * order, in the reference's sign convention: Amul subtracts pairCoeffs[i]*psi[nbrFaceCells[i]] from
+ * row faceCells[i]. Their diagonal share (the patches' internalCoeffs) is folded into `diag`; their
+ * source is not folded (b2g_fold_boundary with the coupled flag set). The pair enters the residual,
+ * normFactor's row sums, every level's Amul, the Gauss-Seidel smoothers' bPrime once per smoothing
+ * call, DIC through the residual, and the coarsest PCG-DIC (GAMG:82-145, :287-305). FP64 form only.
+ * PCG with the GAMG preconditioner refuses a coupled matrix, as the reference's pcgGamgSolve does
+ * (GAMG:1045). */
+B2G_API b2g_status b2g_gamg_solve_coupled(b2g_mesh* mesh, const double* diag, const double* upper,
+                                          const double* pairCoeffs, const double* source, double* psi,
+                                          const b2g_controls* controls, int memspace, void* stream,
+                                          b2g_perf* out, b2g_solve_log* log);
+/* b2g_matrix_create with the pair's coefficients: every level's pair coefficient is restricted from
+ * the finer level's (the sum from zero over the merged faces in ascending face order, GAMG:520-522)
+ * and the level entries below (Amul, smoothing, scale, normFactor, the coarsest PCG-DIC) carry it. */
+B2G_API b2g_status b2g_matrix_create_coupled(b2g_mesh* mesh, const double* diag, const double* upper,
+                                             const double* pairCoeffs, int memspace, void* stream,
+                                             b2g_matrix** out);
+/* Level `level`'s pair coefficients (HOST array of b2g_mesh_level_pair's size). */
+B2G_API b2g_status b2g_matrix_level_pair_coeffs(const b2g_matrix* m, int level, double* coeffs);
+/* The standalone GAMG solve on an existing matrix (coupled or not), source and psi in `memspace`. */
+B2G_API b2g_status b2g_matrix_gamg_solve(b2g_matrix* m, const double* source, double* psi,
+                                         const b2g_controls* controls, int memspace, b2g_perf* out,
+                                         b2g_solve_log* log);
 
 /* ---- one matrix on the hierarchy: the pieces, for callers that drive them (and for tests) ---- */
 
