@@ -360,6 +360,12 @@ def run_ours(args, world, rank, local):
     served = None
     if not args.no_serve and world == 1:
         served = serve_stream(args, b2g, local)
+    coupled = None
+    if not args.no_coupled:
+        try:
+            coupled = coupled_leg(args, b2g, local, world, rank)
+        except Exception as e:  # an extra leg: its failure is reported, the headline line still prints
+            coupled = {"error": f"{type(e).__name__}: {e}"}
 
     line = {
         "metric": METRIC, "value": per_solve, "unit": "s", "n_gpus": world, "steps": args.steps,
@@ -405,6 +411,7 @@ def run_ours(args, world, rank, local):
         "cpu_baseline": cpu,
         "batched": batched,
         "served": served,
+        "coupled": coupled,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -518,6 +525,64 @@ def batched_leg(args, b2g, local, world=1, rank=0):
                                            "mean": float(np.mean(its_mc))},
                             "max_final_residual": float(max(p.finalResidual for p in perfs_mc)),
                             "colouring_build_s": prep_s}}
+
+
+def coupled_leg(args, b2g, local, world=1, rank=0):
+    """The coupled (cyclic) pair on the standalone GAMG solve: a periodic n^3 box (graded 20:1 in y, a
+    cyclic pair joining z = 0 and z = Lz), GaussSeidel, tol 1e-6 relTol 0.05, from psi = 0, fields
+    resident; beside it the reference's own gamgSolve with the coupled patch (oracle/_ref) on one host
+    core, with the iteration counts and the field difference."""
+    import torch
+
+    from brae_b200 import cases
+    n = args.coupled_n
+    c, own, nbr, pc = cases.periodic_box(n, n, n, lengths=(2.0, 1.0, 1.0), grading_y=20.0)
+    dev = torch.device("cuda", local)
+    td = lambda a, dt=torch.float64: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)
+    mesh = b2g.Mesh(td(c.lower, torch.int32), td(c.upper, torch.int32), td(c.Sf.reshape(-1)), td(c.magSf),
+                    c.n_cells, 10, True)
+    t0 = time.perf_counter()
+    mesh.set_pair(own, nbr)
+    pair_build = time.perf_counter() - t0
+    A = b2g.Matrix(mesh, td(c.diag), td(c.coef), pair_coeffs=td(pc))
+    ctl = b2g.controls_default(solver="GAMG", tolerance=TOL, relTol=REL_TOL, maxIter=MAX_ITER)
+    src = td(c.source)
+    psi = torch.zeros(c.n_cells, dtype=torch.float64, device=dev)
+    for _ in range(max(args.warmup, 1)):
+        psi.zero_()
+        A.gamg_solve(src, psi, ctl, history_cap=0)
+    stream = torch.cuda.current_stream()
+    times = []
+    perf = None
+    for _ in range(max(1, min(args.steps, 3))):
+        psi.zero_()
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        perf, _ = A.gamg_solve(src, psi, ctl, history_cap=0)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        times.append(a0.elapsed_time(a1) / 1e3)
+    out = {"workload": f"periodic_box_{n}^3 (graded 20:1 in y, cyclic pair z=0 <-> z=Lz): standalone GAMG "
+                       f"(GaussSeidel) with the coupled pair, FP64, tol 1e-6 relTol 0.05",
+           "cells": c.n_cells, "pair_faces": int(len(own)), "levels": mesh.n_levels,
+           "pair_build_s": pair_build, "s": barrier_max(float(np.mean(times)), world), "perf": list(perf)}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle.bindings import REF_SO, Oracle, Reference
+        from oracle.bindings import controls as oc_controls
+        impl, kind = (Reference(), "reference") if os.path.exists(REF_SO) else (Oracle(), "port")
+        agg = impl.agglomerate(c.lower, c.upper, c.Sf, c.magSf, c.n_cells, 10, True)
+        t0 = time.perf_counter()
+        ref = impl.gamg_solve_pair(agg, c.diag, c.coef, own, nbr, pc, c.source, np.zeros(c.n_cells),
+                                   oc_controls(tolerance=TOL, relTol=REL_TOL, maxIter=MAX_ITER))
+        ts = time.perf_counter() - t0
+        x = psi.cpu().numpy()
+        out["cpu_baseline"] = {"value": ts, "unit": "s", "cores": 1, "kind": kind,
+                               "sample": "one full solve from psi = 0 (hierarchy built once, untimed)",
+                               "perf": list(ref["perf"]),
+                               "field_rel_diff_vs_gpu": float(np.abs(ref["psi"] - x).max() / np.abs(ref["psi"]).max())}
+        out["speedup_vs_cpu"] = ts / out["s"]
+    return out
 
 
 def serve_stream(args, b2g, local):
@@ -663,6 +728,9 @@ def main():
     ap.add_argument("--serve-rate-low", type=float, default=150.0,
                     help="a second stream below the server's capacity (0: none)")
     ap.add_argument("--serve", action="store_true", help="run the served stream alone")
+    ap.add_argument("--no-coupled", action="store_true", help="skip the coupled-pair leg")
+    ap.add_argument("--coupled", action="store_true", help="run the coupled-pair leg alone")
+    ap.add_argument("--coupled-n", type=int, default=160, help="cells per side of the periodic box")
     ap.add_argument("--sweep", action="store_true",
                     help="time the finest-level Gauss-Seidel sweep of the --n box alone (for profiling)")
     args = ap.parse_args()
@@ -675,6 +743,13 @@ def main():
         import brae_b200.native as b2g
         torch.cuda.set_device(0)
         print(json.dumps({"batched": batched_leg(args, b2g, 0)}), flush=True)
+        return
+    if args.coupled:
+        import torch
+
+        import brae_b200.native as b2g
+        torch.cuda.set_device(0)
+        print(json.dumps({"coupled": coupled_leg(args, b2g, 0)}), flush=True)
         return
     if args.serve:
         import torch

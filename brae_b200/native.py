@@ -339,7 +339,7 @@ class Matrix:
             upper = _as_host(upper, np.float64)
             if pair_coeffs is not None:
                 pair_coeffs = _as_host(pair_coeffs, np.float64)
-        ms = _memspace(diag, upper)
+        ms = _memspace(diag, upper, pair_coeffs)
         h = C.c_void_p()
         if pair_coeffs is None:
             _check(lib.b2g_matrix_create(mesh.handle, _ptr(diag), _ptr(upper), ms, _stream(), C.byref(h)))
