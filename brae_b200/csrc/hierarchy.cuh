@@ -121,6 +121,16 @@ struct LevelAddr
     std::unique_ptr<LevelAddr> revDesc;
     DBuf<int> revDescPos;
     PairLevel pair;         // the coupled pair, if the mesh carries one (nFaces 0 otherwise)
+    // The one-block resident Gauss-Seidel sweep of a small one-part level (solver.cu gsResident),
+    // built on first use: the part's positions run by depth, depth d's are [start[d], start[d+1]).
+    struct Resident
+    {
+        bool built = false;
+        bool ok = false;     // the level qualifies (one part, small enough, positions by depth)
+        int nDepth = 0;
+        int block = 0;       // threads: the widest depth rounded up to a warp, 64..256
+        DBuf<int> start;     // [nDepth+1]
+    } resident;
 };
 
 // Level step i -> i+1 (GamgAgglomeration's restrictAddressing / faceRestrictAddressing /

@@ -18,6 +18,8 @@ bool g_profiling = false;
 namespace {
 
 constexpr int NT = 256;          // threads of the row and reduction kernels
+constexpr int kResidentMaxCells = 24576;         // the largest level the resident sweep takes
+constexpr size_t kResidentSmem = 200 * 1024;     // its shared memory: psi of the level and the depth ranges
 constexpr int kMaxPartials = 1024;
 
 int rowsGrid(int n)
@@ -260,6 +262,115 @@ __global__ void __launch_bounds__(1024) mcSmoothCluster(int nColours, const int*
         }
 }
 
+// One smoothing call of the exact Gauss-Seidel on a small one-part level in ONE block: psi of the
+// whole level in shared memory, the positions walked depth by depth (the part's positions run by
+// depth) with a block barrier between depths. A cell's lower-index neighbours have smaller depths (new
+// values by then) and its higher-index neighbours larger ones (still old), so each row reads what the
+// sequential sweep reads and computes it with the same rounding in the same order: the source minus
+// the row's terms in row order, then the division. Row data do not depend on psi, so each thread
+// loads its next depth's row into registers, and the row bounds one depth further ahead, before it
+// computes the current one: the chain per depth is the shared-memory gathers, the row's arithmetic
+// and the barrier. Cells beyond the block's width at a depth are computed straight from memory.
+constexpr int kResidentK = 16;         // row entries a thread holds in registers
+constexpr int kResidentMaxBlock = 256;
+
+template <class T>
+struct ResidentRow
+{
+    int p;  // position, -1: none at this depth
+    int w;  // entries
+    int e0;
+    T b, d;
+    T v[kResidentK];
+    int c[kResidentK];
+};
+
+template <class T>
+__device__ __forceinline__ void residentLoad(const Rows<T>& A, const T* __restrict__ b, int p, int e0, int e1,
+                                             ResidentRow<T>& r)
+{
+    r.p = p;
+    r.w = 0;
+    if (p < 0) return;
+    r.e0 = e0;
+    r.w = e1 - e0;
+    r.b = b[p];
+    r.d = A.diag[p];
+#pragma unroll
+    for (int q = 0; q < kResidentK; ++q)
+        if (q < r.w)
+        {
+            r.v[q] = A.val[e0 + q];
+            r.c[q] = A.col[e0 + q];
+        }
+}
+
+template <class T>
+__device__ __forceinline__ void residentRow(const Rows<T>& A, const ResidentRow<T>& r, T* x)
+{
+    T acc = r.b;
+#pragma unroll
+    for (int q = 0; q < kResidentK; ++q)
+        if (q < r.w) acc = subRn(acc, mulRn(r.v[q], x[r.c[q]]));
+    for (int q = kResidentK; q < r.w; ++q) acc = subRn(acc, mulRn(A.val[r.e0 + q], x[A.col[r.e0 + q]]));
+    x[r.p] = divRn(acc, r.d);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kResidentMaxBlock) gsResident(Rows<T> A, int nDepth, const int* __restrict__ depthStart,
+                                                                const T* __restrict__ b, T* __restrict__ psi, int nSweeps)
+{
+    extern __shared__ __align__(16) unsigned char residentSm[];
+    T* x = reinterpret_cast<T*>(residentSm);
+    int* ds = reinterpret_cast<int*>(residentSm + sizeof(T) * static_cast<size_t>(A.n));
+    const int t = threadIdx.x;
+    const int B = blockDim.x;
+    for (int i = t; i < A.n; i += B) x[i] = psi[i];
+    for (int i = t; i <= nDepth; i += B) ds[i] = depthStart[i];
+    __syncthreads();
+    for (int sw = 0; sw < nSweeps; ++sw)
+    {
+        ResidentRow<T> cur, nxt;
+        {
+            const int p = nDepth > 0 && ds[0] + t < ds[1] ? ds[0] + t : -1;
+            residentLoad(A, b, p, p >= 0 ? A.rowStart[p] : 0, p >= 0 ? A.rowStart[p + 1] : 0, cur);
+        }
+        int pn = -1, en0 = 0, en1 = 0;
+        if (nDepth > 1 && ds[1] + t < ds[2])
+        {
+            pn = ds[1] + t;
+            en0 = A.rowStart[pn];
+            en1 = A.rowStart[pn + 1];
+        }
+        for (int d = 0; d < nDepth; ++d)
+        {
+            // the next depth's row (its bounds were loaded a depth ago) and the bounds after it
+            residentLoad(A, b, pn, en0, en1, nxt);
+            int pf = -1, ef0 = 0, ef1 = 0;
+            if (d + 2 < nDepth && ds[d + 2] + t < ds[d + 3])
+            {
+                pf = ds[d + 2] + t;
+                ef0 = A.rowStart[pf];
+                ef1 = A.rowStart[pf + 1];
+            }
+            if (cur.p >= 0) residentRow(A, cur, x);
+            for (int p = ds[d] + t + B; p < ds[d + 1]; p += B)
+            {
+                T acc = b[p];
+                for (int e = A.rowStart[p]; e < A.rowStart[p + 1]; ++e) acc = subRn(acc, mulRn(A.val[e], x[A.col[e]]));
+                x[p] = divRn(acc, A.diag[p]);
+            }
+            __syncthreads();
+            cur = nxt;
+            pn = pf;
+            en0 = ef0;
+            en1 = ef1;
+        }
+    }
+    __syncthreads();
+    for (int i = t; i < A.n; i += B) psi[i] = x[i];
+}
+
 // symGaussSeidel: bPrime = source minus the row's first (neighbour-of) terms, in the reversed
 // positions with psi beside it
 template <class T>
@@ -387,6 +498,8 @@ void allowSweepSmem(int device)
     std::atomic<unsigned long long>& d = done[sizeof(T) == 8 ? 0 : 1];
     if (d.load() & bit) return;
     B2G_CUDA(cudaFuncSetAttribute(k::gsSweep<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024));
+    B2G_CUDA(cudaFuncSetAttribute(k::gsResident<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(kResidentSmem)));
     d.fetch_or(bit);
 }
 
@@ -694,6 +807,7 @@ void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps,
         symSmooth<T>(level, psiL, src, nSweeps);
         return;
     }
+    if (!trace && level > 0 && residentSweeps<T>(level, psiL, src, nSweeps)) return;
     for (int sw = 0; sw < nSweeps; ++sw) gsLaunch<T>(mesh->lev[level], data<T>().coef[level], psiL, src, trace, level == 0);
 }
 
@@ -761,10 +875,67 @@ void Matrix::ensureSym(int level)
 }
 
 // What the smoother needs built before an iteration is captured (builds synchronise the stream).
+// The resident sweep's depth ranges of `level` (mesh data, built once): only for a one-part level of
+// at most kResidentMaxCells cells whose positions run by depth.
+void Matrix::ensureResident(int level)
+{
+    LevelAddr& L = mesh->lev[level];
+    LevelAddr::Resident& R = L.resident;
+    if (R.built) return;
+    R.built = true;
+    R.ok = false;
+    const int n = L.nCells;
+    if (L.gs.nParts != 1 || n == 0 || n > kResidentMaxCells) return;
+    const std::vector<int> depth = L.gs.depth.download(stream);
+    const std::vector<int> posCell = L.gs.posCell.download(stream);
+    std::vector<int> start(1, 0);
+    int prev = 0;
+    for (int p = 0; p < n; ++p)
+    {
+        const int dp = depth[posCell[p]];
+        if (dp < prev) return;  // not by depth: keep the pipelined sweep
+        while (static_cast<int>(start.size()) <= dp) start.push_back(p);
+        prev = dp;
+    }
+    start.push_back(n);
+    const int nDepth = static_cast<int>(start.size()) - 1;
+    int width = 0;
+    for (int d = 0; d < nDepth; ++d) width = std::max(width, start[d + 1] - start[d]);
+    R.nDepth = nDepth;
+    R.block = std::min(k::kResidentMaxBlock, std::max(64, (width + 31) / 32 * 32));
+    R.start.upload(start.data(), start.size(), stream);
+    B2G_CUDA(cudaStreamSynchronize(stream));
+    R.ok = true;
+}
+
+// nSweeps exact Gauss-Seidel sweeps of a small one-part level in one resident block (gsResident);
+// false if the level does not qualify (the caller then launches the pipelined sweep per sweep)
+template <class T>
+bool Matrix::residentSweeps(int level, T* psiL, const T* src, int nSweeps)
+{
+    LevelAddr& L = mesh->lev[level];
+    if (!L.resident.built)
+    {
+        if (capturing) return false;
+        ensureResident(level);
+    }
+    if (!L.resident.ok) return false;
+    const size_t smem = sizeof(T) * static_cast<size_t>(L.nCells) + sizeof(int) * (L.resident.nDepth + 1);
+    if (smem > kResidentSmem) return false;
+    k::gsResident<T><<<1, L.resident.block, smem, stream>>>(rowsOf(L, data<T>().coef[level]), L.resident.nDepth,
+                                                            L.resident.start.p, src, psiL, nSweeps);
+    B2G_LAUNCH_CHECK();
+    ++launches;
+    return true;
+}
+
 void Matrix::prepareSmoother(const b2g_controls& c)
 {
     const bool sym = c.smoother == B2G_SMOOTHER_SYM_GAUSS_SEIDEL;
     const bool dic = c.smoother == B2G_SMOOTHER_DIC || c.smoother == B2G_SMOOTHER_DIC_GAUSS_SEIDEL;
+    // the resident sweep's depth ranges of the small one-part levels, before any iteration is captured
+    if (c.smoother != B2G_SMOOTHER_DIC)
+        for (int i = 1; i < nLevels(); ++i) ensureResident(i);
     if (coupled && c.smoother != B2G_SMOOTHER_DIC)
     {
         // the Gauss-Seidel smoothers' bPrime per level, allocated before any iteration is captured

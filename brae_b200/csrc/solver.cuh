@@ -119,6 +119,8 @@ struct Matrix
     template <class T> void ensureDic(int level);
     template <class T> void dicSmooth(int level, T* psi, const T* source, int nSweeps);
     template <class T> void symSmooth(int level, T* psi, const T* source, int nSweeps);
+    void ensureResident(int level);            // the resident sweep's depth ranges (on the mesh, once)
+    template <class T> bool residentSweeps(int level, T* psi, const T* source, int nSweeps);
     void mcLaunch(int level, bool fused, int cluster, int block, float* psi, const float* source, int nSweeps,
                   bool timed, bool symmetric = false);
     void tuneMulticolour(int level);
