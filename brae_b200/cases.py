@@ -166,30 +166,47 @@ def box_case(nx: int, ny: int, nz: int, lengths=(1.0, 1.0, 1.0), grading_y: floa
 
 
 def periodic_box(nx: int, ny: int, nz: int, lengths=(2.0, 1.0, 1.0), grading_y: float = 1.0,
-                 two_phase: bool = False, seed: int = 0):
-    """box_case with a cyclic pair joining the z = 0 and z = Lz faces: two coupled patches, the
-    bottom one first, each listing its cells in face order (x fastest) and its neighbours across the
-    pair face for face. Returns (case, own, nbr, coeff): the pair in the form a coupled patch's
-    faceCells / neighbour faceCells / boundaryCoeffs give it, with the matrix's sign convention that
-    Amul subtracts coeff * psi[nbr]. The pair's diagonal share is folded into case.diag (the coupled
-    patch's internalCoeffs), so the pair coefficient is the off-diagonal's negative."""
+                 two_phase: bool = False, seed: int = 0, axes=("z",)):
+    """box_case with cyclic pairs: along z (the default) joining the z = 0 and z = Lz faces, and
+    along x (axes containing "x") joining x = 0 and x = Lx. Each axis gives two coupled patches, the
+    low one first, each listing its cells in face order and its neighbours across the pair face for
+    face; the patches follow in the order of `axes`. Returns (case, own, nbr, coeff): the pair in the
+    form the coupled patches' faceCells / neighbour faceCells / boundaryCoeffs give it, with the
+    matrix's sign convention that Amul subtracts coeff * psi[nbr]. The pair's diagonal share is
+    folded into case.diag (the coupled patches' internalCoeffs), so the pair coefficient is the
+    off-diagonal's negative. With both axes the box's edge cells own two pair faces."""
     c = box_case(nx, ny, nz, lengths, grading_y, two_phase, seed, name=f"periodic_{nx}x{ny}x{nz}")
     lx, ly, lz = lengths
-    dx = np.full(nx, lx / nx)
+    dx = lx / nx
     dy = graded_spacing(ny, ly, grading_y)
     dz = lz / nz
-    j, i = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
-    i = i.ravel(); j = j.ravel()
-    bottom = (j * nx + i).astype(np.int64)
-    top = bottom + (nz - 1) * nx * ny
-    area = dx[i] * dy[j]
-    coeff = area / dz  # the two half-cells across the pair face
-    if two_phase:
-        zc0 = 0.5 * dz
-        coeff = coeff / _rho(np.full(coeff.shape, zc0), dz)
-    own = np.concatenate([bottom, top]).astype(np.int32)
-    nbr = np.concatenate([top, bottom]).astype(np.int32)
-    pc = np.concatenate([coeff, coeff])
+    zc = (np.arange(nz) + 0.5) * dz
+    owns, nbrs, coefs = [], [], []
+    for ax in axes:
+        if ax == "z":
+            j, i = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+            i = i.ravel(); j = j.ravel()
+            low = (j * nx + i).astype(np.int64)
+            high = low + (nz - 1) * nx * ny
+            coeff = dx * dy[j] / dz  # the two half-cells across the pair face
+            if two_phase:
+                coeff = coeff / _rho(np.full(coeff.shape, zc[0]), dz)
+        elif ax == "x":
+            k, j = np.meshgrid(np.arange(nz), np.arange(ny), indexing="ij")
+            j = j.ravel(); k = k.ravel()
+            low = (k * nx * ny + j * nx).astype(np.int64)
+            high = low + (nx - 1)
+            coeff = dy[j] * dz / dx
+            if two_phase:
+                coeff = coeff / _rho(zc[k], dz)
+        else:
+            raise ValueError(f"periodic axis {ax!r}: x or z")
+        owns += [low, high]
+        nbrs += [high, low]
+        coefs += [coeff, coeff]
+    own = np.concatenate(owns).astype(np.int32)
+    nbr = np.concatenate(nbrs).astype(np.int32)
+    pc = np.concatenate(coefs)
     diag = c.diag.copy()
     np.add.at(diag, own, pc)
     c.diag = diag

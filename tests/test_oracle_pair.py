@@ -18,6 +18,9 @@ CASES = [
     ("tiny", dict(nx=8, ny=7, nz=6)),
     ("graded", dict(nx=12, ny=10, nz=9, grading_y=5.0)),
     ("two_phase", dict(nx=16, ny=14, nz=18, grading_y=20.0, two_phase=True)),
+    # pairs along x and z: the edge cells own two pair faces, added in face order
+    ("two_axes", dict(nx=10, ny=9, nz=8, grading_y=5.0, axes=("x", "z"))),
+    ("two_axes_two_phase", dict(nx=12, ny=10, nz=14, grading_y=20.0, two_phase=True, axes=("z", "x"))),
 ]
 
 
@@ -34,6 +37,21 @@ def test_pair_gamg_oracle_equals_reference_bitwise(oracle, reference, name, kw):
         assert so["perf"] == sr["perf"], smoother
         assert np.array_equal(so["psi"], sr["psi"]), smoother
         assert 1 <= so["perf"][2] < 1000
+
+
+def test_pair_controls_oracle_equals_reference(oracle, reference):
+    # pre-sweeps, no correction scaling, other sweep counts: every branch of the V-cycle with the pair
+    c, own, nbr, pc = cases.periodic_box(12, 10, 9, grading_y=5.0, axes=("x", "z"))
+    ao = oracle.agglomerate(c.lower, c.upper, c.Sf, c.magSf, c.n_cells, 10, True)
+    ar = reference.agglomerate(c.lower, c.upper, c.Sf, c.magSf, c.n_cells, 10, True)
+    psi0 = np.zeros(c.n_cells)
+    for kw in (dict(nPreSweeps=2), dict(scaleCorrection=False), dict(nPostSweeps=1, maxPostSweeps=2, nFinestSweeps=3),
+               dict(nPreSweeps=1, preSweepsLevelMultiplier=2, smoother="DICGaussSeidel")):
+        ctl = controls(tolerance=1e-8, relTol=0.0, **kw)
+        so = oracle.gamg_solve_pair(ao, c.diag, c.coef, own, nbr, pc, c.source, psi0, ctl)
+        sr = reference.gamg_solve_pair(ar, c.diag, c.coef, own, nbr, pc, c.source, psi0, ctl)
+        assert so["perf"] == sr["perf"], kw
+        assert np.array_equal(so["psi"], sr["psi"]), kw
 
 
 def test_pair_changes_the_solution(oracle):
