@@ -21,6 +21,8 @@ BOXES = [
     ("tiny", dict(nx=8, ny=7, nz=6)),
     ("graded", dict(nx=12, ny=10, nz=9, grading_y=5.0)),
     ("two_phase", dict(nx=20, ny=18, nz=24, grading_y=20.0, two_phase=True)),
+    # pairs along x and z: the edge cells own two pair faces on the finest level too
+    ("two_axes", dict(nx=14, ny=12, nz=10, grading_y=5.0, axes=("x", "z"))),
 ]
 
 
