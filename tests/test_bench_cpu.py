@@ -1,0 +1,32 @@
+"""bench.py's reference arm on the CPU: `--impl reference` times the reference's own host solve
+(oracle/_ref, else the oracle port) and prints one JSON line with the keys the measurement contract
+names. A small box keeps it to seconds."""
+import json
+import os
+import subprocess
+import sys
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_reference_arm_json_line():
+    env = dict(os.environ)
+    env.pop("WORLD_SIZE", None)
+    r = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference", "--n", "20",
+                        "--steps", "1", "--warmup", "0"], capture_output=True, text=True, cwd=REPO, env=env,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [x for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    assert d["unit"] == "s" and d["higher_is_better"] is False
+    assert d["value"] > 0 and d["n_gpus"] == 1 and d["steps"] == 1
+    cb = d["cpu_baseline"]
+    assert cb["kind"] in ("reference", "port") and cb["cores"] == 1 and cb["value"] == d["value"]
+    assert cb["sample"]
+    e2e = d["e2e"]
+    assert e2e["value"] == d["value"] and e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+    assert d["config"]["cells"] == 20 ** 3
+    init, final, iters = d["config"]["solver_perf"]
+    assert init == 1.0 and 0 < final < 0.05 and iters >= 1
