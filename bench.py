@@ -174,22 +174,29 @@ def traffic_per_launch(kernel: str, workload: str):
     return None if v is None else float(v)
 
 
-def cpu_reference_solve(case, tag):
-    """The reference's own host path (oracle/_ref) if built, else the oracle port: (seconds per
-    solve, kind, perf, psi, build seconds). Single-threaded."""
+def workload_name(n: int) -> str:
+    """The headline workload, worded once for both arms."""
+    return f"graded_channel_{n}^3: FP64 PCG+GAMG(GaussSeidel) tol 1e-6 relTol 0.05"
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def reference_impl():
+    """The reference's own host path (oracle/_ref) if built, else the oracle port."""
     from oracle.bindings import REF_SO, Oracle, Reference
     if os.path.exists(REF_SO):
-        impl, kind = Reference(), "reference"
-    else:
-        impl, kind = Oracle(), "port"
-    t0 = time.perf_counter()
-    agg = impl.agglomerate(case.lower, case.upper, case.Sf, case.magSf, case.n_cells, 10, True)
-    tb = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    out = impl.pcg_gamg_solve(agg, case.diag, case.coef, case.source, np.zeros(case.n_cells), TOL,
-                              REL_TOL, MAX_ITER)
-    ts = time.perf_counter() - t0
-    return ts, kind, out["perf"], out["psi"], tb
+        return Reference(), "reference"
+    return Oracle(), "port"
 
 
 def run_reference(args, world, rank):
@@ -197,8 +204,7 @@ def run_reference(args, world, rank):
     if rank != 0:
         return
     case = cases.graded_channel(args.n)
-    from oracle.bindings import REF_SO, Oracle, Reference
-    impl, kind = (Reference(), "reference") if os.path.exists(REF_SO) else (Oracle(), "port")
+    impl, kind = reference_impl()
     agg = impl.agglomerate(case.lower, case.upper, case.Sf, case.magSf, case.n_cells, 10, True)
     steps = max(1, min(args.steps, 3))
     warm = 0
@@ -217,13 +223,42 @@ def run_reference(args, world, rank):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": world,
         "steps": steps, "warmup": warm, "ms_per_step": v * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"graded_channel_{args.n}^3 FP64 PCG+GAMG tol 1e-6 relTol 0.05",
-                   "cells": case.n_cells, "faces": case.n_faces, "solver_perf": list(perf)},
-        "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": kind,
-                         "sample": f"full {args.n}^3 solve from psi = 0 (hierarchy built once, untimed)"},
+        "config": {"workload": workload_name(args.n), "cells": case.n_cells, "faces": case.n_faces,
+                   "solver_perf": list(perf)},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "cpu_model": cpu_model(), "kind": kind,
+                         "sample": f"full {args.n}^3 pcgGamgSolve from psi = 0 on one host core, including the "
+                                   f"Galerkin hierarchy build it does in every call (agglomeration built once, "
+                                   f"untimed)"},
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def level_table(mesh, amul_lv, smooth_lv, fp_bytes=8):
+    """Per level: cells, faces, and from a profiled solve the Amul and smoothing times with their
+    algorithmic bytes (Amul 24 nC + 16 nF, one exact sweep 32 nC + 16 nF in FP64) and GB/s; plus the
+    all-level sums."""
+    rows = []
+    tot = {"smooth_ms": 0.0, "smooth_bytes": 0.0, "amul_ms": 0.0, "amul_bytes": 0.0}
+    for lv in range(mesh.n_levels + 1):
+        nc, nf = mesh.level_size(lv)
+        row = {"level": lv, "cells": nc, "faces": nf}
+        if lv < len(smooth_lv) and smooth_lv[lv][2] > 0:
+            ms_, calls, sweeps = smooth_lv[lv]
+            byt = (32 * nc + 16 * nf) * sweeps
+            row.update(smooth_ms=ms_, smooth_calls=int(calls), sweeps=int(sweeps),
+                       us_per_sweep=ms_ * 1e3 / sweeps, smooth_gbs=byt / max(ms_ * 1e-3, 1e-12) / 1e9)
+            tot["smooth_ms"] += ms_
+            tot["smooth_bytes"] += byt
+        if lv < len(amul_lv) and amul_lv[lv][2] > 0:
+            ms_, calls, n_amul = amul_lv[lv]
+            byt = (24 * nc + 16 * nf) * n_amul
+            row.update(amul_ms=ms_, amuls=int(n_amul), us_per_amul=ms_ * 1e3 / n_amul,
+                       amul_gbs=byt / max(ms_ * 1e-3, 1e-12) / 1e9)
+            tot["amul_ms"] += ms_
+            tot["amul_bytes"] += byt
+        rows.append(row)
+    return rows, tot
 
 
 def run_ours(args, world, rank, local):
@@ -239,47 +274,52 @@ def run_ours(args, world, rank, local):
     mesh = b2g.Mesh(td(case.lower, torch.int32), td(case.upper, torch.int32), td(case.Sf.reshape(-1)),
                     td(case.magSf), case.n_cells, 10, True)
     build_wall = time.perf_counter() - t0
-    A = b2g.Matrix(mesh, td(case.diag), td(case.coef))
+    d_diag, d_coef = td(case.diag), td(case.coef)
+    A = b2g.Matrix(mesh, d_diag, d_coef)
     src = td(case.source)
     psi = torch.zeros(case.n_cells, dtype=torch.float64, device=dev)
     ctl = b2g.controls_default(tolerance=TOL, relTol=REL_TOL, maxIter=MAX_ITER)
-    for _ in range(args.warmup):
-        psi.zero_()
-        A.solve(src, psi, ctl, history_cap=0)
-    # finest-level Amul and Gauss-Seidel launches are bracketed by CUDA events (event-record nodes
-    # inside each iteration's graph), read after every iteration: live per-kernel times of the
-    # timed solves themselves
-    b2g.set_profiling(True)
-    psi.zero_()
-    A.solve(src, psi, ctl, history_cap=0)  # captures the profiled graphs (untimed)
-    ms_acc = np.zeros(4)
-    cnt_acc = np.zeros(4)
     stream = torch.cuda.current_stream()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def step(c=ctl, hist=0, coarse=0):
+        # one pcgGamgSolve as the reference times it: the Galerkin hierarchy of this call's matrix
+        # (GamgHierarchy::build in every call), then the solve from psi = 0
+        A.set_coeffs(d_diag, d_coef)
+        psi.zero_()
+        return A.solve(src, psi, c, history_cap=hist, coarsest_cap=coarse)
+
+    for _ in range(args.warmup):
+        step()
     barrier(world)
     torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
         e0.record(stream)
         perf = None
         for _ in range(args.steps):
-            psi.zero_()
-            perf, _, _ = A.solve(src, psi, ctl, history_cap=0)
-            ms, cnt = A.timings()
-            ms_acc += ms
-            cnt_acc += cnt
+            perf = step()[0]
         e1.record(stream)
         torch.cuda.synchronize()
-    b2g.set_profiling(False)
     elapsed = barrier_max(e0.elapsed_time(e1) / 1e3, world)
     per_solve = elapsed / args.steps
     psi64 = psi.cpu().numpy()
+    launches_per_step = A.timings()[1][3]
+
+    # a separate profiled pass (events around every level's Amuls and smoothing calls, inside the
+    # iteration graphs): the per-kernel and per-level times the roofline uses
+    b2g.set_profiling(True)
+    step()  # captures the profiled graph
+    step()
+    ms4, cnt4 = A.timings()
+    levels, tot = level_table(mesh, A.level_timings(0), A.level_timings(1))
+    b2g.set_profiling(False)
 
     # end to end: the reference-facing call with pinned host buffers, copies inside the timed region
     pin = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).pin_memory()
     h_diag, h_up, h_src = pin(case.diag), pin(case.coef), pin(case.source)
     h_psi = torch.zeros(case.n_cells, dtype=torch.float64).pin_memory()
     ctl2 = b2g.controls_default(tolerance=TOL, relTol=REL_TOL, maxIter=MAX_ITER)
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = max(1, min(args.steps, 5))
     b2g.pcg_gamg_solve(mesh, h_diag.numpy(), h_up.numpy(), h_src.numpy(), h_psi.numpy(), ctl2)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -292,67 +332,91 @@ def run_ours(args, world, rank, local):
     d2h = 8 * case.n_cells
     del h_diag, h_up, h_src
 
-    # the precision form on the two-phase (1000:1) coefficient, same mesh and hierarchy
-    tp = cases.graded_channel(args.n, two_phase=True)
-    A2 = b2g.Matrix(mesh, td(tp.diag), td(tp.coef))
-    src2 = td(tp.source)
-    forms = {}
-    for name, prec in (("fp64", 0), ("fp32_precond", 1), ("fp32_precond_multicolour", 2)):
-        c2 = b2g.controls_default(tolerance=TOL, relTol=REL_TOL, maxIter=MAX_ITER, precision=prec)
-        x = torch.zeros(case.n_cells, dtype=torch.float64, device=dev)
-        A2.solve(src2, x, c2, history_cap=0)
-        ts = []
-        for _ in range(max(1, min(args.steps, 3))):
-            x.zero_()
-            torch.cuda.synchronize()
-            a0 = torch.cuda.Event(enable_timing=True)
-            a1 = torch.cuda.Event(enable_timing=True)
-            a0.record(stream)
-            p2, _, _ = A2.solve(src2, x, c2, history_cap=0)
-            a1.record(stream)
-            torch.cuda.synchronize()
-            ts.append(a0.elapsed_time(a1) / 1e3)
-        forms[name] = dict(s=barrier_max(float(np.mean(ts)), world), perf=list(p2), psi=x.cpu().numpy())
-    # the multicolour sweep's bandwidth on the finest level (events inside the solve's graph)
-    c_mc = b2g.controls_default(tolerance=TOL, relTol=REL_TOL, maxIter=MAX_ITER, precision=2)
-    x = torch.zeros(case.n_cells, dtype=torch.float64, device=dev)
-    b2g.set_profiling(True)
-    A2.solve(src2, x, c_mc, history_cap=0)  # captures the profiled graph
-    x.zero_()
-    A2.solve(src2, x, c_mc, history_cap=0)
-    mc_ms, mc_cnt = A2.timings()
-    b2g.set_profiling(False)
-    n_colours = len(mesh.colouring(0)) - 1
-    tuned = [dict(level=l, cells=mesh.level_size(l)[0], colours=len(mesh.colouring(l)) - 1, **mesh.sweep_shape(l))
-             for l in range(mesh.n_levels + 1)]
-    mc_sweeps = mc_cnt[1] / max(n_colours, 1)
-    mc_sweep_ms = mc_ms[1] / max(mc_sweeps, 1)
-    mc_bytes = 20 * case.n_cells + 16 * case.n_faces  # FP32: diag, b, psi read + write, row position; two (column, coefficient) entries per face
-    mc_gbs = mc_bytes / (mc_sweep_ms * 1e-3) / 1e9
-    ref_x = forms["fp64"]["psi"]
-    field_err = float(np.abs(forms["fp32_precond"]["psi"] - ref_x).max() / np.abs(ref_x).max())
-    field_err_mc = float(np.abs(forms["fp32_precond_multicolour"]["psi"] - ref_x).max() / np.abs(ref_x).max())
+    # the FP64 solve to tolerance 1e-6 with relTol 0 (many iterations): iteration count, residual
+    # history and field, against the reference's own solve below
+    ctl0 = b2g.controls_default(tolerance=1e-6, relTol=0.0, maxIter=MAX_ITER)
+    step(ctl0)
+    torch.cuda.synchronize()
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    perf0, hist0, coarse0 = step(ctl0, hist=MAX_ITER, coarse=8192)
+    a1.record(stream)
+    torch.cuda.synchronize()
+    t_rel0 = a0.elapsed_time(a1) / 1e3
+    x_rel0 = psi.cpu().numpy()
 
-    # roofline of the dominant kernel: the finest level's Gauss-Seidel sweep (its share is below)
+    precision = precision_leg(args, b2g, mesh, dev, stream, world)
+
+    # roofline of the dominant kernel: the exact Gauss-Seidel sweep (finest level; all levels beside it)
     peak, peak_kind = measured_peaks()
     n, nf = case.n_cells, case.n_faces
-    gs_launches = max(cnt_acc[1], 1)
-    gs_ms = ms_acc[1] / gs_launches
-    amul_ms = ms_acc[0] / max(cnt_acc[0], 1)
-    gs_bytes = 32 * n + 16 * nf       # diag, b, psi read + write; upper; two labels
+    fin = levels[0]
+    gs_bytes = 32 * n + 16 * nf       # one sweep: diag, b, psi read + write; upper; two labels
     amul_bytes = 24 * n + 16 * nf     # diag, x, y; upper; two labels
-    gs_gbs = gs_bytes / (gs_ms * 1e-3) / 1e9
-    amul_gbs = amul_bytes / (amul_ms * 1e-3) / 1e9
+    gs_gbs = fin["smooth_gbs"]
     traffic = traffic_per_launch("gsSweep", f"graded_channel_{args.n}")
+    all_sweep_gbs = tot["smooth_bytes"] / max(tot["smooth_ms"] * 1e-3, 1e-12) / 1e9
+    all_amul_gbs = tot["amul_bytes"] / max(tot["amul_ms"] * 1e-3, 1e-12) / 1e9
 
     cpu = None
+    reference_checks = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        ts, kind, cperf, cpsi, tb = cpu_reference_solve(case, "fp64")
-        cpu = {"value": ts, "unit": "s", "cores": 1, "kind": kind,
-               "sample": f"one full {args.n}^3 FP64 solve from psi = 0 on one host core "
-                         f"(hierarchy built once, {tb:.1f} s, untimed)",
+        impl, kind = reference_impl()
+        t0 = time.perf_counter()
+        agg = impl.agglomerate(case.lower, case.upper, case.Sf, case.magSf, case.n_cells, 10, True)
+        tb = time.perf_counter() - t0
+        H = agg.hierarchy
+        bad = []
+        for s_ in range(min(H.n_levels, mesh.n_levels)):
+            st = mesh.step(s_)
+            same = (np.array_equal(st["restrict"], H.restrict[s_]) and
+                    np.array_equal(st["face_restrict"], H.face_restrict[s_]) and
+                    np.array_equal(st["flip"].astype(np.int32), np.asarray(H.flip[s_]).astype(np.int32)) and
+                    np.array_equal(st["lower"], H.lower[s_ + 1]) and np.array_equal(st["upper"], H.upper[s_ + 1]))
+            if not same:
+                bad.append(s_)
+        hier_same = H.n_levels == mesh.n_levels and bool(H.forward) == bool(mesh.forward) and not bad
+        t0 = time.perf_counter()
+        out = impl.pcg_gamg_solve(agg, case.diag, case.coef, case.source, np.zeros(case.n_cells), TOL, REL_TOL,
+                                  MAX_ITER)
+        ts = time.perf_counter() - t0
+        cperf, cpsi = out["perf"], out["psi"]
+        cpu = {"value": ts, "unit": "s", "cores": 1, "cpu_model": cpu_model(), "kind": kind,
+               "sample": f"one full {args.n}^3 pcgGamgSolve from psi = 0 on one host core, including the Galerkin "
+                         f"hierarchy build it does in every call (agglomeration {tb:.1f} s, once, untimed)",
                "iterations": cperf[2], "final_residual": cperf[1],
-               "field_rel_diff_vs_gpu": float(np.abs(cpsi - psi64).max() / np.abs(cpsi).max())}
+               "field_rel_diff_vs_gpu": float(np.abs(cpsi - psi64).max() / np.abs(cpsi).max()),
+               "agglomeration_s": tb}
+        t0 = time.perf_counter()
+        ref0 = impl.pcg_gamg_solve(agg, case.diag, case.coef, case.source, np.zeros(case.n_cells), 1e-6, 0.0,
+                                   MAX_ITER)
+        t_ref0 = time.perf_counter() - t0
+        rp = ref0["perf"]
+        rc = np.asarray(ref0["coarsest"], dtype=np.float64).reshape(-1, 3)
+        gc = np.asarray(coarse0, dtype=np.float64).reshape(-1, 3)
+        same_len = rc.shape == gc.shape
+        reference_checks = {
+            "hierarchy_bitexact": bool(hier_same), "levels": [int(mesh.n_levels), int(H.n_levels)],
+            "forward": [bool(mesh.forward), bool(H.forward)], "mismatched_steps": bad,
+            "compared": "every step's restrict, faceRestrict and flip maps and the coarse lower/upper addressing, "
+                        "device against the reference's faceAreaPairGamgAgglomeration",
+            "fp64_tol1e-6_relTol0": {
+                "gpu_s": t_rel0, "reference_cpu_s": t_ref0,
+                "iterations": [int(perf0.nIterations), int(rp[2])],
+                "iterations_equal": int(perf0.nIterations) == int(rp[2]),
+                "initial_residual": [perf0.initialResidual, rp[0]],
+                "final_residual": [perf0.finalResidual, rp[1]],
+                "final_residual_diff_rel_to_initial": abs(perf0.finalResidual - rp[1]) / max(rp[0], 1e-300),
+                "gpu_history": list(hist0),
+                "coarsest_solves": [int(gc.shape[0]), int(rc.shape[0])],
+                "coarsest_iterations_equal": bool(same_len and np.array_equal(gc[:, 2], rc[:, 2])),
+                "coarsest_residual_max_rel_diff": float(np.max(np.abs(gc[:, :2] - rc[:, :2]) /
+                                                               np.maximum(np.abs(rc[:, :2]), 1e-300)))
+                if same_len and rc.size else None,
+                "field_rel_diff": float(np.abs(ref0["psi"] - x_rel0).max() / np.abs(ref0["psi"]).max()),
+                "tolerances": "iterations equal; final residual within 1e-12 of the initial; field within 1e-10",
+            },
+        }
 
     batched = None
     if not args.no_batched:
@@ -372,41 +436,34 @@ def run_ours(args, world, rank, local):
         "warmup": args.warmup, "ms_per_step": per_solve * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {
-            "workload": f"graded_channel_{args.n}^3: FP64 PCG+GAMG(GaussSeidel) tol 1e-6 relTol 0.05",
+            "workload": workload_name(args.n),
+            "step": "b2g_matrix_set_coeffs (fine level in, every coarse level rebuilt by Galerkin summation, as "
+                    "pcgGamgSolve does in every call) + the PCG solve from psi = 0",
             "cells": n, "faces": nf, "levels": mesh.n_levels, "solver_perf": list(perf),
             "mesh_build_s": mesh.build_ms / 1e3, "mesh_build_wall_s": build_wall,
             "l2": "inputs larger than L2 (the 20M-cell system is ~2.5 GB)",
             "parallelism": f"replicas x{world} (one independent solve per GPU)",
         },
-        "precision_form": {
-            "workload": f"graded_channel_{args.n}^3 two-phase 1000:1, tol 1e-6 relTol 0.05",
-            "fp64_s": forms["fp64"]["s"], "fp32_precond_s": forms["fp32_precond"]["s"],
-            "speedup": forms["fp64"]["s"] / forms["fp32_precond"]["s"],
-            "fp64_perf": forms["fp64"]["perf"], "fp32_precond_perf": forms["fp32_precond"]["perf"],
-            "field_rel_err_vs_fp64": field_err,
-            "multicolour": {
-                "s": forms["fp32_precond_multicolour"]["s"],
-                "speedup": forms["fp64"]["s"] / forms["fp32_precond_multicolour"]["s"],
-                "perf": forms["fp32_precond_multicolour"]["perf"],
-                "field_rel_err_vs_fp64": field_err_mc,
-                "note": "FP32 V-cycle with Gauss-Seidel sweeps colour by colour (B2G_PRECISION_FP32_PRECOND_MULTICOLOUR)",
-                "autotuned_sweep_shapes": tuned,
-                "finest_sweep": {"colours": n_colours, "ms": mc_sweep_ms, "algorithmic_bytes": mc_bytes,
-                                 "achieved_gbs": mc_gbs, "frac_of_measured_hbm": mc_gbs / measured_peaks()[0]},
-            },
-        },
+        "reference_checks": reference_checks,
+        "precision_form": precision,
         "kernels": {
-            "gs_finest_us_per_launch": gs_ms * 1e3, "gs_finest_launches": int(cnt_acc[1]),
-            "gs_finest_share": float(ms_acc[1] / ms_acc[3]),
-            "amul_finest_us_per_launch": amul_ms * 1e3, "amul_finest_gbs": amul_gbs,
-            "amul_finest_share": float(ms_acc[0] / ms_acc[3]),
+            "profiled_solve_ms": ms4[3],
+            "gs_finest_us_per_sweep": fin.get("us_per_sweep"), "gs_finest_sweeps": fin.get("sweeps"),
+            "gs_finest_share": fin.get("smooth_ms", 0.0) / ms4[3],
+            "smoothing_all_levels_share": tot["smooth_ms"] / ms4[3],
+            "amul_finest_us": fin.get("us_per_amul"), "amul_finest_gbs": fin.get("amul_gbs"),
+            "amul_all_levels_share": tot["amul_ms"] / ms4[3],
+            "levels": levels,
         },
-        "roofline": {"kernel": "gsSweep (finest level, one sweep)", "bound": "hbm",
+        "roofline": {"kernel": "gsSweep, finest level (exact Gauss-Seidel; per sweep)", "bound": "hbm",
                      "achieved": gs_gbs, "peak": peak, "unit": "GB/s", "frac": gs_gbs / peak,
-                     "traffic": traffic, "peak_source": peak_kind,
-                     "algorithmic_bytes_per_launch": gs_bytes},
+                     "traffic": traffic, "peak_source": peak_kind, "algorithmic_bytes_per_sweep": gs_bytes,
+                     "all_levels": {"sweep_gbs": all_sweep_gbs, "sweep_frac": all_sweep_gbs / peak,
+                                    "amul_gbs": all_amul_gbs, "amul_frac": all_amul_gbs / peak},
+                     "amul_finest": {"gbs": fin.get("amul_gbs"), "frac": (fin.get("amul_gbs") or 0.0) / peak,
+                                     "algorithmic_bytes": amul_bytes}},
         "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": int(cnt_acc[3]),
+        "gpu_launches": int(launches_per_step * args.steps),
         "clocks": clocks.summary(),
         "cpu_baseline": cpu,
         "batched": batched,
@@ -415,6 +472,73 @@ def run_ours(args, world, rank, local):
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def precision_leg(args, b2g, mesh, dev, stream, world):
+    """The precision form on the two-phase (1000:1) coefficient, same mesh and hierarchy: plain FP64,
+    the FP32-preconditioned form in exact order and in multicolour order, each solved to the same
+    tolerance (relTol 0) from psi = 0, with time, iterations, final residual and the relative field
+    error against the FP64 solve at that tolerance; first at the configuration's tolerance 1e-6, then
+    tighter, to find where the field error reaches 1e-8. Also the configuration's relTol 0.05 case."""
+    import torch
+
+    from brae_b200 import cases
+    tp = cases.graded_channel(args.n, two_phase=True)
+    td = lambda a: torch.as_tensor(np.ascontiguousarray(a)).to(dev, torch.float64)
+    A2 = b2g.Matrix(mesh, td(tp.diag), td(tp.coef))
+    src2 = td(tp.source)
+    x = torch.zeros(tp.n_cells, dtype=torch.float64, device=dev)
+    names = {0: "fp64", 1: "fp32_precond", 2: "fp32_precond_multicolour"}
+
+    def run(prec, tol, rel, reps):
+        c2 = b2g.controls_default(tolerance=tol, relTol=rel, maxIter=MAX_ITER, precision=prec)
+        x.zero_()
+        A2.solve(src2, x, c2, history_cap=0)  # builds and captures (untimed)
+        ts = []
+        p2 = None
+        for _ in range(reps):
+            x.zero_()
+            torch.cuda.synchronize()
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            p2 = A2.solve(src2, x, c2, history_cap=0)[0]
+            a1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(a0.elapsed_time(a1) / 1e3)
+        return barrier_max(float(np.median(ts)), world), p2, x.cpu().numpy()
+
+    def at(tol, rel, forms, reps):
+        res = {}
+        for prec in forms:
+            s_, p2, xx = run(prec, tol, rel, reps)
+            res[names[prec]] = {"s": s_, "iterations": int(p2.nIterations), "final_residual": p2.finalResidual,
+                                "initial_residual": p2.initialResidual, "x": xx}
+        ref = res["fp64"]["x"]
+        scale = np.abs(ref).max()
+        for k, r in res.items():
+            r["field_rel_err_vs_fp64"] = float(np.abs(r.pop("x") - ref).max() / scale) if k != "fp64" else 0.0
+            r["speedup_vs_fp64"] = res["fp64"]["s"] / r["s"]
+        del ref
+        return res
+
+    reps = max(1, min(args.steps, 3))
+    out = {"workload": f"graded_channel_{args.n}^3 two-phase 1000:1 (rho = 1000 below z = 0.5, 1 above, tanh "
+                       f"interface 3 cells wide)",
+           "headline_form": "fp32_precond_multicolour (FP64 outer PCG, FP32 V-cycle, Gauss-Seidel colour by colour)"}
+    out["tol1e-6_relTol0"] = at(1e-6, 0.0, (0, 1, 2), reps)
+    out["tol1e-6_relTol0"]["equal_residual"] = (
+        "every form solved until its final residual is below 1e-6 of the normalisation (relTol 0)")
+    out["relTol0.05"] = at(TOL, REL_TOL, (0, 1, 2), reps)
+    sweep = []
+    for tol in args.precision_tols:
+        r = at(tol, 0.0, (0, 2), max(1, min(reps, 2)))
+        r["tolerance"] = tol
+        sweep.append(r)
+    out["tolerance_sweep"] = sweep
+    ok = [r["tolerance"] for r in sweep if r["fp32_precond_multicolour"]["field_rel_err_vs_fp64"] <= 1e-8]
+    out["loosest_tolerance_with_field_err_le_1e-8"] = max(ok) if ok else None
+    del A2
+    return out
 
 
 def batched_leg(args, b2g, local, world=1, rank=0):
@@ -612,14 +736,16 @@ def serve_stream(args, b2g, local):
     out = {"population": {"cases_per_class": [len(r) for r in resident],
                           "cells": [[n for _, n, _ in r] for r in resident], "setup_s": setup_s,
                           "slots": args.serve_slots, "hbm_cap_gb": 150},
-           "offered_rate_per_s": args.serve_rate, "stream_s": args.serve_seconds}
+           "offered_rate_per_s": args.serve_rate, "stream_s": args.serve_seconds,
+           "tolerance": args.serve_tol, "relTol": args.serve_reltol}
     runs = [(form, prec, args.serve_rate) for form, prec in (("fp64", 0), ("fp32_precond", 1),
                                                                ("fp32_precond_multicolour", 2))]
     if args.serve_rate_low > 0:
         runs += [(form + "_at_low_rate", prec, args.serve_rate_low)
                  for form, prec in (("fp64", 0), ("fp32_precond", 1), ("fp32_precond_multicolour", 2))]
     for form, prec, rate in runs:
-        ctl = b2g.controls_default(tolerance=TOL, relTol=REL_TOL, maxIter=MAX_ITER, precision=prec)
+        ctl = b2g.controls_default(tolerance=args.serve_tol, relTol=args.serve_reltol, maxIter=MAX_ITER,
+                                   precision=prec)
         # warm every case once in this form (captures its iteration graph)
         for row in resident:
             for cid, n, src in row:
@@ -704,9 +830,12 @@ def run_sweep(args):
     b2g.set_profiling(False)
     n, nf = case.n_cells, case.n_faces
     gs_us = ms[1] / max(cnt[1], 1) * 1e3
+    am_us = ms[0] / max(cnt[0], 1) * 1e3
     print(json.dumps({"sweep": f"graded_channel_{args.n}^3 finest level", "cells": n, "faces": nf,
-                      "gs_us_per_launch": gs_us, "gs_launches": int(cnt[1]),
-                      "gs_algorithmic_gbs": (32 * n + 16 * nf) / (gs_us * 1e-6) / 1e9}), flush=True)
+                      "gs_us_per_sweep": gs_us, "gs_sweeps": int(cnt[1]),
+                      "gs_algorithmic_gbs": (32 * n + 16 * nf) / (gs_us * 1e-6) / 1e9,
+                      "amul_us": am_us, "amuls": int(cnt[0]),
+                      "amul_algorithmic_gbs": (24 * n + 16 * nf) / (am_us * 1e-6) / 1e9}), flush=True)
 
 
 def main():
@@ -725,12 +854,16 @@ def main():
                     help="length of the served stream's arrival window (the full stream is 60 s)")
     ap.add_argument("--serve-rate", type=float, default=500.0, help="offered requests per second")
     ap.add_argument("--serve-slots", type=int, default=6, help="server worker slots")
+    ap.add_argument("--serve-tol", type=float, default=1e-6, help="tolerance of the served solves")
+    ap.add_argument("--serve-reltol", type=float, default=0.0, help="relTol of the served solves")
     ap.add_argument("--serve-rate-low", type=float, default=150.0,
                     help="a second stream below the server's capacity (0: none)")
     ap.add_argument("--serve", action="store_true", help="run the served stream alone")
     ap.add_argument("--no-coupled", action="store_true", help="skip the coupled-pair leg")
     ap.add_argument("--coupled", action="store_true", help="run the coupled-pair leg alone")
     ap.add_argument("--coupled-n", type=int, default=160, help="cells per side of the periodic box")
+    ap.add_argument("--precision-tols", type=float, nargs="*", default=[1e-8, 1e-10, 1e-11, 1e-12],
+                    help="tighter tolerances of the precision form's field-error sweep")
     ap.add_argument("--sweep", action="store_true",
                     help="time the finest-level Gauss-Seidel sweep of the --n box alone (for profiling)")
     args = ap.parse_args()

@@ -75,6 +75,13 @@ struct DBuf
             B2G_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), count * sizeof(T), libraryPool(), stream));
         }
     }
+    // alloc unless the array already holds exactly `count` elements: a rebuild with new values keeps
+    // the address, so launches captured in a CUDA graph stay valid
+    void ensure(size_t count, cudaStream_t stream)
+    {
+        if (p && n == count) return;
+        alloc(count, stream);
+    }
     void zero(cudaStream_t stream)
     {
         if (n) B2G_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), stream));

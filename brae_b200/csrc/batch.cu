@@ -728,6 +728,9 @@ k::GsArgs<T> gsArgsOf(const LevelAddr& L, const LevelCoef<T>& C, const T* b, T* 
     a.b = b;
     a.psi = psi;
     a.progress = progress;
+    a.ticket = nullptr;  // the batched launch draws its tickets from the level's own counter
+    a.spinLimit = k::kSpinLimit;
+    a.publish = 1;
     a.err = err;
     a.trace = nullptr;
     a.traceDepths = 0;
@@ -879,8 +882,10 @@ Batch::Batch(std::vector<Matrix*> cs, cudaStream_t s) : stream(s), cases(std::mo
             partBase.push_back(totalParts);
             totalParts += L.gs.nParts;
         }
-        B.progress.alloc(std::max<size_t>(1, static_cast<size_t>(totalParts) * k::kProgressStride), stream);
+        // the parts' progress lines, then one line for the launch's ticket counter
+        B.progress.alloc((static_cast<size_t>(totalParts) + 1) * k::kProgressStride, stream);
         B.progress.zero(stream);
+        B.ticketAt = static_cast<size_t>(totalParts) * k::kProgressStride;
         int pb = 0;
         for (int c = 0; c < K; ++c)
         {
@@ -1106,7 +1111,8 @@ void Batch::smooth(int lv, int nSweeps)
     for (int sw = 0; sw < nSweeps; ++sw)
     {
         B2G_CUDA(cudaMemsetAsync(B.progress.p, 0, B.progress.bytes(), stream));
-        k::gsSweepBatch<T><<<B.nParts, B.block, smem, stream>>>(args, B.parts.p, active.p);
+        k::gsSweepBatch<T><<<B.nParts, B.block, smem, stream>>>(
+            args, B.parts.p, active.p, reinterpret_cast<int*>(B.progress.p + B.ticketAt));
         B2G_LAUNCH_CHECK();
         ++launches;
     }

@@ -97,6 +97,7 @@ struct BatchLevel
     int block = 0;
     size_t smem64 = 0, smem32 = 0;
     DBuf<unsigned> progress;
+    size_t ticketAt = 0;  // the sweep launch's ticket counter: the word after the parts' progress lines
     std::vector<TileList> mc;  // per colour: the swept large cases' rows of that colour (multicolour form)
     DBuf<int> mcSmall;         // the swept small cases (descriptors): one block each sweeps them whole
     int nMcSmall = 0;

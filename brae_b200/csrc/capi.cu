@@ -681,6 +681,21 @@ b2g_status b2g_matrix_create(b2g_mesh* mesh, const double* diag, const double* u
     });
 }
 
+b2g_status b2g_matrix_set_coeffs(b2g_matrix* m, const double* diag, const double* upper, int memspace)
+{
+    return guarded([&] {
+        need(m && diag, "b2g_matrix_set_coeffs: null argument");
+        need(memspace == B2G_MEM_HOST || memspace == B2G_MEM_DEVICE, "b2g_matrix_set_coeffs: bad memspace");
+        need(m->mesh->m.lev[0].nFaces == 0 || upper, "b2g_matrix_set_coeffs: null upper");
+        if (m->mat->coupled)
+            b2g::fail(B2G_ERR_REFUSED, "b2g_matrix_set_coeffs: a matrix with a coupled pair takes new coefficients "
+                                       "through b2g_matrix_create_coupled");
+        m->mat->setFine(diag, upper, memspace);
+        m->mat->buildCoarse();
+        B2G_CUDA(cudaStreamSynchronize(m->mesh->m.stream));
+    });
+}
+
 b2g_status b2g_matrix_destroy(b2g_matrix* m)
 {
     return guarded([&] {
@@ -756,6 +771,37 @@ b2g_status b2g_level_smooth_trace(b2g_matrix* m, int level, double* psi, const d
         A.toPos(level, static_cast<const double*>(psi), A.ioBuf(0));
         A.toPos(level, source, A.ioBuf(1));
         A.smooth<double>(level, B2G_SMOOTHER_GAUSS_SEIDEL, A.ioBuf(0), A.ioBuf(1), 1, trace);
+        A.fromPos(level, static_cast<const double*>(A.ioBuf(0)), psi);
+        A.checkDeviceError();
+    });
+}
+
+b2g_status b2g_level_smooth_stall(b2g_matrix* m, int level, double* psi, const double* source, long long spinLimit,
+                                  int* nParts)
+{
+    return guarded([&] {
+        need(m && psi && source, "b2g_level_smooth_stall: null argument");
+        need(level >= 0 && level <= m->mat->nLevels(), "b2g_level_smooth_stall: level out of range");
+        need(spinLimit >= 1 && spinLimit <= b2g::k::kSpinLimit, "b2g_level_smooth_stall: spinLimit out of range");
+        b2g::Matrix& A = *m->mat;
+        const b2g::LevelAddr& L = A.mesh->lev[level];
+        if (nParts) *nParts = L.gs.nParts;
+        A.toPos(level, static_cast<const double*>(psi), A.ioBuf(0));
+        A.toPos(level, source, A.ioBuf(1));
+        A.spinLimit = spinLimit;
+        A.publish = 0;
+        try
+        {
+            A.gsLaunch<double>(L, A.v64.coef[level], A.ioBuf(0), A.ioBuf(1), nullptr, false);
+        }
+        catch (...)
+        {
+            A.spinLimit = b2g::k::kSpinLimit;
+            A.publish = 1;
+            throw;
+        }
+        A.spinLimit = b2g::k::kSpinLimit;
+        A.publish = 1;
         A.fromPos(level, static_cast<const double*>(A.ioBuf(0)), psi);
         A.checkDeviceError();
     });
@@ -964,8 +1010,11 @@ b2g_status b2g_pcg_gamg_solve(b2g_mesh* mesh, const double* diag, const double* 
 {
     return guarded([&] {
         need(mesh && diag && controls, "b2g_pcg_gamg_solve: null argument");
+        need(memspace == B2G_MEM_HOST || memspace == B2G_MEM_DEVICE, "b2g_pcg_gamg_solve: bad memspace");
+        need(mesh->m.lev[0].nFaces == 0 || upper, "b2g_pcg_gamg_solve: null upper");
         (void)stream;
-        b2g::Matrix A(&mesh->m, mesh->m.stream);
+        if (!mesh->solveMatrix) mesh->solveMatrix.reset(new b2g::Matrix(&mesh->m, mesh->m.stream));
+        b2g::Matrix& A = *mesh->solveMatrix;
         A.setFine(diag, upper, memspace);
         b2g::capi::solveOn(A, source, psi, controls, memspace, out, log, false);
     });
@@ -977,8 +1026,11 @@ b2g_status b2g_gamg_solve(b2g_mesh* mesh, const double* diag, const double* uppe
 {
     return guarded([&] {
         need(mesh && diag && controls, "b2g_gamg_solve: null argument");
+        need(memspace == B2G_MEM_HOST || memspace == B2G_MEM_DEVICE, "b2g_gamg_solve: bad memspace");
+        need(mesh->m.lev[0].nFaces == 0 || upper, "b2g_gamg_solve: null upper");
         (void)stream;
-        b2g::Matrix A(&mesh->m, mesh->m.stream);
+        if (!mesh->solveMatrix) mesh->solveMatrix.reset(new b2g::Matrix(&mesh->m, mesh->m.stream));
+        b2g::Matrix& A = *mesh->solveMatrix;
         A.setFine(diag, upper, memspace);
         b2g::capi::solveOn(A, source, psi, controls, memspace, out, log, true);
     });
@@ -1082,6 +1134,24 @@ b2g_status b2g_matrix_timings(const b2g_matrix* m, double* ms4, long long* count
     });
 }
 
+b2g_status b2g_matrix_level_timings(const b2g_matrix* m, int kind, int capacity, double* ms, long long* regions,
+                                    long long* units, int* nLevels)
+{
+    return guarded([&] {
+        need(m != nullptr, "b2g_matrix_level_timings: null matrix");
+        need(kind == 0 || kind == 1, "b2g_matrix_level_timings: kind is 0 (Amul) or 1 (smoothing)");
+        const b2g::Matrix& A = *m->mat;
+        const int have = static_cast<int>(A.lvMs[kind].size());
+        if (nLevels) *nLevels = have;
+        for (int l = 0; l < std::min(have, capacity); ++l)
+        {
+            if (ms) ms[l] = A.lvMs[kind][l];
+            if (regions) regions[l] = A.lvCalls[kind][l];
+            if (units) units[l] = A.lvUnits[kind][l];
+        }
+    });
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------------------------
@@ -1105,27 +1175,54 @@ static __device__ __align__(256) double g_staticScratch[kStaticDoubles];
 // reads it (the copies of psi and source, the residual, the DIC reciprocals, the PCG vectors and
 // the performance record), whatever an earlier call left there.
 //
+// The context current on this thread (the driver's cuCtxGetCurrent, reached through the runtime so
+// that the library does not link the driver library itself), or null if it cannot be asked.
+void* currentContext()
+{
+    using CtxGetCurrent = int (*)(void**);
+    static const CtxGetCurrent fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<CtxGetCurrent>(f);
+    }();
+    void* ctx = nullptr;
+    if (fn && fn(&ctx) != 0) ctx = nullptr;
+    return ctx;
+}
+
 // The device address of g_staticScratch on the current device. In host code the symbol is only a
 // host-side stand-in, so the address is looked up once per device (with that device current) and
-// cached; the first call on a device does this.
+// cached; the first call on a device does this. The cache remembers the context it was looked up
+// in: after a device reset the primary context is a new one, its module a new image, and the
+// address is looked up again instead of reusing the old one.
 double* staticScratchAddress()
 {
+    struct Slot
+    {
+        void* ctx = nullptr;
+        double* addr = nullptr;
+    };
     static std::mutex mu;
-    static double* addr[64] = {};
+    static Slot slot[64];
     int dev = 0;
     B2G_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) b2g::fail(B2G_ERR_STATE, "b2g_level_pcg_dic_static: device ordinal out of range");
+    void* ctx = currentContext();
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev])
+    if (!slot[dev].addr || slot[dev].ctx != ctx || !ctx)
     {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_staticScratch);
         if (e != cudaSuccess)
             b2g::fail(B2G_ERR_CUDA, std::string("b2g_level_pcg_dic_static: cudaGetSymbolAddress failed: ") +
                                         cudaGetErrorString(e));
-        addr[dev] = static_cast<double*>(p);
+        slot[dev].addr = static_cast<double*>(p);
+        slot[dev].ctx = ctx;
     }
-    return addr[dev];
+    return slot[dev].addr;
 }
 
 }  // namespace

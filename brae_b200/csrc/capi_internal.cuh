@@ -10,6 +10,10 @@
 struct b2g_mesh
 {
     b2g::Mesh m;
+    // The matrix b2g_pcg_gamg_solve / b2g_gamg_solve solve on: kept between calls (the mesh-lifetime
+    // cache of the reference's device path), its coefficients replaced by each call, so that its
+    // buffers and captured iteration graphs are reused. Declared after `m`: destroyed before it.
+    std::unique_ptr<b2g::Matrix> solveMatrix;
 };
 
 struct b2g_matrix

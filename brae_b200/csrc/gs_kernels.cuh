@@ -64,7 +64,7 @@ constexpr int kFill = 256;                     // B: window fill block (position
 constexpr int kStages = 4;                     // S: pipeline slots
 constexpr int kMaxTable = 65535;               // value-table entries a 16-bit code can name
 constexpr int kMaxCompute = 384;               // compute threads per CTA, at most (+ 4 warps)
-constexpr long long kSpinLimit = 1LL << 24;    // polls before a wait gives up
+constexpr long long kSpinLimit = 1LL << 24;    // polls before a wait gives up (the default)
 constexpr int kProgressStride = 32;            // progress words 128 bytes apart: one L2 line per part,
                                                // so that a part's publishes meet only its own pollers
 
@@ -158,6 +158,12 @@ struct GsArgs
     const T* __restrict__ b;                 // [n (+pad)] by position
     T* psi;                                  // [n] by position, updated in place (padded)
     unsigned* progress;                      // [P][kProgressStride] (word 0 of each line used)
+    int* ticket;                             // the launch's part ticket (zeroed before it), or null:
+                                             // part = blockIdx.x
+    long long spinLimit;                     // polls before a wait gives up (kSpinLimit)
+    int publish;                             // 1; 0 only to test the bounded waits: no part releases
+                                             // its progress, so a part that needs another's values
+                                             // waits for a word nothing sets and gives up
     int* err;
     unsigned long long* trace;               // diagnostic, or null (SM clock64 stamps): [nChunks][4]
                                              // compute thread 0 (chunk start, past the depth
@@ -328,13 +334,13 @@ __device__ __forceinline__ void computeSync(int nThreads)
 constexpr long long kErrPollMask = 4095;
 __device__ __forceinline__ bool errSet(const int* err) { return *reinterpret_cast<const volatile int*>(err) != 0; }
 
-__device__ __forceinline__ void waitMbar(unsigned long long* b, unsigned parity, int* err)
+__device__ __forceinline__ void waitMbar(unsigned long long* b, unsigned parity, int* err, long long limit)
 {
     long long it = 0;
     while (!mbarTryWait(b, parity))
     {
         if ((++it & kErrPollMask) == 0 && errSet(err)) return;
-        if (it > kSpinLimit)
+        if (it > limit)
         {
             atomicExch(err, 1);
             return;
@@ -343,13 +349,13 @@ __device__ __forceinline__ void waitMbar(unsigned long long* b, unsigned parity,
 }
 
 // wait until the shared word *w >= target
-__device__ __forceinline__ void waitShared(const unsigned* w, unsigned target, int* err)
+__device__ __forceinline__ void waitShared(const unsigned* w, unsigned target, int* err, long long limit)
 {
     long long it = 0;
     while (ldAcquireCta(w) < target)
     {
         if ((++it & kErrPollMask) == 0 && errSet(err)) return;
-        if (it > kSpinLimit)
+        if (it > limit)
         {
             atomicExch(err, 1);
             return;
@@ -461,7 +467,7 @@ __device__ __forceinline__ void gsSweepPart(const GsArgs<T>& a, const int p)
             if ((++it & kErrPollMask) == 0)
             {
                 if (__shfl_sync(0xffffffffu, errSet(a.err) ? 1 : 0, 0)) break;
-                if (it > 16 * kSpinLimit)
+                if (it > 16 * a.spinLimit)
                 {
                     if (lane == 0) atomicExch(a.err, 1);
                     break;
@@ -477,7 +483,7 @@ __device__ __forceinline__ void gsSweepPart(const GsArgs<T>& a, const int p)
         // One lane spins on the shared pubDepth and releases each new value at GPU scope at once:
         // the release is cumulative over the psi stores the compute warps made before their barrier
         // and their release of pubDepth, which this lane acquired.
-        if (t != M + 64 || a.hasDown[p] == 0) return;
+        if (t != M + 64 || a.hasDown[p] == 0 || !a.publish) return;
         unsigned published = 0xffffffffu;
         long long it = 0;
         while (true)
@@ -493,7 +499,7 @@ __device__ __forceinline__ void gsSweepPart(const GsArgs<T>& a, const int p)
             if ((++it & kErrPollMask) == 0)
             {
                 if (errSet(a.err)) break;
-                if (it > 256 * kSpinLimit)
+                if (it > 16 * a.spinLimit)
                 {
                     atomicExch(a.err, 1);
                     break;
@@ -526,7 +532,7 @@ __device__ __forceinline__ void gsSweepPart(const GsArgs<T>& a, const int p)
                 r1 = r2;
                 if (j + 2 < nCh) r2 = loadChunkRec(a.chunkRec, c0 + j + 2);
                 if (ptr) ptr[4 * (size_t)(c0 + j)] = clockStamp();
-                if (j >= kStages) waitMbar(&empty[s], static_cast<unsigned>((j / kStages - 1) & 1), a.err);
+                if (j >= kStages) waitMbar(&empty[s], static_cast<unsigned>((j / kStages - 1) & 1), a.err, a.spinLimit);
                 const unsigned slotA = slotsA + static_cast<unsigned>(s) * sb;
                 // the record and the gather sources first: the gather warp starts from them
                 const int4* rg = a.chunkRec + 3 * (size_t)(c0 + j);
@@ -549,6 +555,18 @@ __device__ __forceinline__ void gsSweepPart(const GsArgs<T>& a, const int p)
                 if (ptr) ptr[4 * (size_t)(c0 + j) + 1] = clockStamp();
                 if (++s == kStages) s = 0;
             }
+            // before the CTA can exit, the last stages' copies have landed: on an error path the
+            // compute warps may give up waiting for them, and no bulk copy may still be writing into
+            // the shared memory of a CTA that has exited (a bulk copy always completes, so this
+            // wait ends; it is bounded all the same, and not cut short by the error word)
+            for (int j = max(0, nCh - kStages); j < nCh; ++j)
+            {
+                long long it = 0;
+                while (!mbarTryWait(&full[j % kStages], static_cast<unsigned>((j / kStages) & 1)) &&
+                       ++it <= a.spinLimit)
+                {
+                }
+            }
             return;
         }
         const int lane = t - M - 32;
@@ -557,7 +575,7 @@ __device__ __forceinline__ void gsSweepPart(const GsArgs<T>& a, const int p)
         for (int j = 0; j < nCh; ++j)
         {
             // the TMA warp published this stage's record and sources once the slot was free
-            waitMbar(&lists[s], phase, a.err);
+            waitMbar(&lists[s], phase, a.err, a.spinLimit);
             const int4 rb1 = srec[s][1];
             const int4 rb2 = srec[s][2];
             const int gat0 = rb1.x, nGat = rb1.y, needUp = rb1.w, sameWait = rb2.x, nOld = rb2.y >> 1;
@@ -574,10 +592,10 @@ __device__ __forceinline__ void gsSweepPart(const GsArgs<T>& a, const int p)
                 // when empty[sw % S] completes phase sw / S; the slot wait for chunk j already
                 // covers every chunk up to j - S, and phase sw / S + 1 needs chunk sw + S > j, so
                 // the parity is unambiguous)
-                if (needUp >= 0) waitShared(&upMin, static_cast<unsigned>(needUp) + 1u, a.err);
+                if (needUp >= 0) waitShared(&upMin, static_cast<unsigned>(needUp) + 1u, a.err, a.spinLimit);
                 const int sw = sameWait - c0;
                 if (sameWait >= 0 && sw > j - kStages)
-                    waitMbar(&empty[sw % kStages], static_cast<unsigned>((sw / kStages) & 1), a.err);
+                    waitMbar(&empty[sw % kStages], static_cast<unsigned>((sw / kStages) & 1), a.err, a.spinLimit);
                 if (ptr) ptr[4 * (size_t)(c0 + j) + 2] = clockStamp();
             }
             __syncwarp();
@@ -609,7 +627,7 @@ __device__ __forceinline__ void gsSweepPart(const GsArgs<T>& a, const int p)
         if (a.trace && t == 0) a.trace[4 * (size_t)(c0 + j)] = clockStamp();
         // the record is published with the stage's gather sources, well before the data: the
         // progress this part publishes at a depth change must not wait for this chunk's data
-        waitMbar(&lists[s], phase, a.err);
+        waitMbar(&lists[s], phase, a.err, a.spinLimit);
         const ChunkRec cr = loadChunkRec(srec[s], 0);
         if (cr.newDepth && j > 0)
         {
@@ -619,7 +637,7 @@ __device__ __forceinline__ void gsSweepPart(const GsArgs<T>& a, const int p)
             if (t == 0) stReleaseCta(&pubDepth, static_cast<unsigned>(cr.depth));
         }
         if (a.trace && t == 0) a.trace[4 * (size_t)(c0 + j) + 1] = clockStamp();
-        waitMbar(&full[s], phase, a.err);
+        waitMbar(&full[s], phase, a.err, a.spinLimit);
         if (a.trace && t == 0) a.trace[4 * (size_t)(c0 + j) + 2] = clockStamp();
         if (t < cr.m)
         {
@@ -673,24 +691,38 @@ __device__ __forceinline__ void gsSweepPart(const GsArgs<T>& a, const int p)
     }
 }
 
+// FORWARD PROGRESS. A part waits only for lower-numbered parts (of its own case in a batch). A CTA
+// takes its part from a ticket counter when it starts, not from blockIdx: the ticket it draws is
+// held only by a CTA that is already running, so every lower-numbered part is running or done
+// whatever order the hardware dispatches the blocks in, and however many other kernels share the
+// SMs (several server slots, say) -- every wait is for a part that is running.
+__device__ __forceinline__ int drawTicket(int* ticket)
+{
+    __shared__ int part;
+    if (threadIdx.x == 0) part = ticket ? atomicAdd(ticket, 1) : static_cast<int>(blockIdx.x);
+    __syncthreads();
+    return part;
+}
+
 // One sweep of one level: grid = the level's P parts.
 template <class T>
 __global__ void __launch_bounds__(kMaxCompute + 128, 1) gsSweep(GsArgs<T> a)
 {
-    gsSweepPart<T>(a, blockIdx.x);
+    gsSweepPart<T>(a, drawTicket(a.ticket));
 }
 
-// One sweep of one level of many independent cases in ONE launch: block i runs part parts[i].y of
-// the case whose arguments are cases[parts[i].x]; parts[i].z indexes `active` (may be null), and a
-// case whose flag is 0 is skipped. A case's parts follow each other in block order, and a part waits
-// only for lower-numbered parts of its own case, which are dispatched first.
+// One sweep of one level of many independent cases in ONE launch: the CTA with ticket i runs part
+// parts[i].y of the case whose arguments are cases[parts[i].x]; parts[i].z indexes `active` (may be
+// null), and a case whose flag is 0 is skipped. A case's parts follow each other in ticket order, and
+// a part waits only for lower-numbered parts of its own case, which hold lower tickets.
 template <class T>
 __global__ void __launch_bounds__(kMaxCompute + 128, 1) gsSweepBatch(const GsArgs<T>* __restrict__ cases,
                                                                      const int4* __restrict__ parts,
-                                                                     const int* __restrict__ active)
+                                                                     const int* __restrict__ active,
+                                                                     int* __restrict__ ticket)
 {
     __shared__ __align__(16) GsArgs<T> sa;
-    const int4 cp = parts[blockIdx.x];
+    const int4 cp = parts[drawTicket(ticket)];
     if (active && active[cp.z] == 0) return;
     static_assert(sizeof(GsArgs<T>) % 4 == 0, "GsArgs copied word by word");
     constexpr int kWords = static_cast<int>(sizeof(GsArgs<T>) / 4);

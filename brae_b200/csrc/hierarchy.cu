@@ -1317,7 +1317,8 @@ void buildGsSchedule(LevelAddr& L, cudaStream_t s)
         break;
     }
     G.partPosStart = std::move(dPartStart);
-    G.progress.alloc(static_cast<size_t>(P) * k::kProgressStride, s);
+    // the parts' progress lines, then one line for a launch's ticket counter
+    G.progress.alloc(static_cast<size_t>(P + 1) * k::kProgressStride, s);
     G.progress.zero(s);
     B2G_CUDA(cudaStreamSynchronize(s));
 }

@@ -166,11 +166,11 @@ __global__ void kGsLayout(int n, long long nnz, const int* __restrict__ posCell,
 template <class T>
 void allocGsLayout(const LevelAddr& L, LevelCoef<T>& C, cudaStream_t s)
 {
-    C.gsDiag.alloc(L.nCells + 8, s);
+    C.gsDiag.ensure(L.nCells + 8, s);
     C.gsDiag.zero(s);
-    C.rowVal.alloc(std::max<size_t>(2 * (size_t)L.nFaces, 1), s);
+    C.rowVal.ensure(std::max<size_t>(2 * (size_t)L.nFaces, 1), s);
     const long long bytes = sizeof(T) == 8 ? L.gs.blobBytes64 : L.gs.blobBytes32;
-    C.blob.alloc(static_cast<size_t>(std::max<long long>(bytes, 16)), s);
+    C.blob.ensure(static_cast<size_t>(std::max<long long>(bytes, 16)), s);
     C.blob.zero(s);
 }
 
@@ -503,7 +503,7 @@ void allowSweepSmem(int device)
     d.fetch_or(bit);
 }
 
-cudaEvent_t Matrix::timedBegin(int cls)
+cudaEvent_t Matrix::timedBegin(int kind, int level, int units)
 {
     if (!g_profiling) return nullptr;
     std::pair<cudaEvent_t, cudaEvent_t> e;
@@ -517,51 +517,65 @@ cudaEvent_t Matrix::timedBegin(int cls)
         B2G_CUDA(cudaEventCreate(&e.first));
         B2G_CUDA(cudaEventCreate(&e.second));
     }
+    TimedRegion r;
+    r.start = e.first;
+    r.end = e.second;
+    r.kind = kind;
+    r.level = level;
+    r.units = units;
     if (capturing)
     {
         // an event-record node in the graph, re-recorded by every replay
-        B2G_CUDA(cudaEventRecordWithFlags(e.first, stream, cudaEventRecordExternal));
-        capturing->ev[cls].push_back(e);
+        B2G_CUDA(cudaEventRecordWithFlags(r.start, stream, cudaEventRecordExternal));
+        capturing->regions.push_back(r);
     }
     else
     {
-        B2G_CUDA(cudaEventRecord(e.first, stream));
-        (cls == 0 ? evAmul : evGs).push_back(e);
+        B2G_CUDA(cudaEventRecord(r.start, stream));
+        evOpen.push_back(r);
     }
-    return e.first;
+    return r.start;
 }
 
-void Matrix::timedEnd(int cls, cudaEvent_t start)
+// regions never nest: the one being closed is the last one opened
+void Matrix::timedEnd(cudaEvent_t start)
 {
     if (!start) return;
     if (capturing)
-        B2G_CUDA(cudaEventRecordWithFlags(capturing->ev[cls].back().second, stream, cudaEventRecordExternal));
+        B2G_CUDA(cudaEventRecordWithFlags(capturing->regions.back().end, stream, cudaEventRecordExternal));
     else
-        B2G_CUDA(cudaEventRecord((cls == 0 ? evAmul : evGs).back().second, stream));
+        B2G_CUDA(cudaEventRecord(evOpen.back().end, stream));
+}
+
+void Matrix::addRegion(const TimedRegion& r)
+{
+    float x = 0.f;
+    B2G_CUDA(cudaEventElapsedTime(&x, r.start, r.end));
+    const size_t need = static_cast<size_t>(r.level) + 1;
+    for (int k = 0; k < 2; ++k)
+        if (lvMs[k].size() < need)
+        {
+            lvMs[k].resize(need, 0.0);
+            lvCalls[k].resize(need, 0);
+            lvUnits[k].resize(need, 0);
+        }
+    lvMs[r.kind][r.level] += x;
+    lvCalls[r.kind][r.level] += 1;
+    lvUnits[r.kind][r.level] += r.units;
 }
 
 void Matrix::collectGraphTimings(IterationGraph& G)
 {
     if (!g_profiling) return;
-    for (int cls = 0; cls < 2; ++cls)
-        for (auto& e : G.ev[cls])
-        {
-            float x = 0.f;
-            B2G_CUDA(cudaEventElapsedTime(&x, e.first, e.second));
-            graphMs[cls] += x;
-            graphCounts[cls] += 1;
-        }
+    for (const TimedRegion& r : G.regions) addRegion(r);
 }
 
 void Matrix::releaseGraph(IterationGraph& G)
 {
     if (G.exec) cudaGraphExecDestroy(G.exec);
     G.exec = nullptr;
-    for (auto& v : G.ev)
-    {
-        for (auto& e : v) evFree.push_back(e);
-        v.clear();
-    }
+    for (const TimedRegion& r : G.regions) evFree.emplace_back(r.start, r.end);
+    G.regions.clear();
 }
 
 void Matrix::timingsBegin()
@@ -572,8 +586,12 @@ void Matrix::timingsBegin()
         counts[i] = 0;
     }
     launches = 0;
-    graphMs[0] = graphMs[1] = 0.0;
-    graphCounts[0] = graphCounts[1] = 0;
+    for (int k = 0; k < 2; ++k)
+    {
+        lvMs[k].clear();
+        lvCalls[k].clear();
+        lvUnits[k].clear();
+    }
     if (!g_profiling) return;
     if (!evSolve[0])
     {
@@ -592,33 +610,34 @@ void Matrix::timingsEnd()
     float t = 0.f;
     B2G_CUDA(cudaEventElapsedTime(&t, evSolve[0], evSolve[1]));
     ms[3] = t;
-    for (int cls = 0; cls < 2; ++cls)
+    for (const TimedRegion& r : evOpen)
     {
-        auto& v = cls == 0 ? evAmul : evGs;
-        for (auto& e : v)
-        {
-            float x = 0.f;
-            B2G_CUDA(cudaEventElapsedTime(&x, e.first, e.second));
-            ms[cls] += x;
-            evFree.push_back(e);
-        }
-        counts[cls] = static_cast<long long>(v.size()) + graphCounts[cls];
-        ms[cls] += graphMs[cls];
-        v.clear();
+        addRegion(r);
+        evFree.emplace_back(r.start, r.end);
     }
+    evOpen.clear();
+    for (int k = 0; k < 2; ++k)
+        if (!lvMs[k].empty())
+        {
+            ms[k] = lvMs[k][0];
+            counts[k] = lvUnits[k][0];
+        }
     ms[2] = ms[3] - ms[0] - ms[1];
-    counts[2] = counts[3] - counts[0] - counts[1];
+    long long regions = 0;
+    for (int k = 0; k < 2; ++k)
+        if (!lvCalls[k].empty()) regions += lvCalls[k][0];
+    counts[2] = counts[3] - regions;
 }
 
 Matrix::~Matrix()
 {
     for (IterationGraph* g : {&pcgGraph, &gamgGraph}) releaseGraph(*g);
-    for (auto* v : {&evAmul, &evGs, &evFree})
-        for (auto& e : *v)
-        {
-            cudaEventDestroy(e.first);
-            cudaEventDestroy(e.second);
-        }
+    for (const TimedRegion& r : evOpen) evFree.emplace_back(r.start, r.end);
+    for (auto& e : evFree)
+    {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
     if (evSolve[0])
     {
         cudaEventDestroy(evSolve[0]);
@@ -654,13 +673,14 @@ void Matrix::setFine(const double* diag, const double* upper, int memspace)
     const LevelAddr& L = mesh->lev[0];
     LevelCoef<double>& C = v64.coef[0];
     const cudaMemcpyKind kind = memspace == B2G_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
-    C.diag.alloc(L.nCells, stream);
-    C.upper.alloc(L.nFaces, stream);
+    C.diag.ensure(L.nCells, stream);
+    C.upper.ensure(L.nFaces, stream);
     B2G_CUDA(cudaMemcpyAsync(C.diag.p, diag, sizeof(double) * L.nCells, kind, stream));
     if (L.nFaces) B2G_CUDA(cudaMemcpyAsync(C.upper.p, upper, sizeof(double) * L.nFaces, kind, stream));
     fillGsLayout(L, C, stream);
     coarseBuilt = false;
     v32.built = false;
+    ++coefGen;
 }
 
 // GamgHierarchy::build (GAMG:565-623): Galerkin coarse matrices level by level
@@ -674,8 +694,8 @@ void Matrix::buildCoarse()
         const LevelAddr& Cl = mesh->lev[i + 1];
         const LevelCoef<double>& F = v64.coef[i];
         LevelCoef<double>& C = v64.coef[i + 1];
-        C.diag.alloc(Cl.nCells, stream);
-        C.upper.alloc(Cl.nFaces, stream);
+        C.diag.ensure(Cl.nCells, stream);
+        C.upper.ensure(Cl.nFaces, stream);
         k::galerkinDiag<<<rowsGrid(Cl.nCells), NT, 0, stream>>>(Cl.nCells, S.cellStart.p, S.cellList.p, S.intStart.p,
                                                                 S.intList.p, F.diag.p, F.upper.p, C.diag.p);
         if (Cl.nFaces)
@@ -689,13 +709,13 @@ void Matrix::buildCoarse()
     v64.src.resize(nL);
     for (int i = 0; i < nL; ++i)
     {
-        v64.corr[i].alloc(nAlloc(i + 1), stream);
-        v64.src[i].alloc(nAlloc(i + 1), stream);
+        v64.corr[i].ensure(nAlloc(i + 1), stream);
+        v64.src[i].ensure(nAlloc(i + 1), stream);
     }
-    v64.ACf.alloc(nAlloc(0), stream);
-    v64.preSmoothed.alloc(nAlloc(0), stream);
+    v64.ACf.ensure(nAlloc(0), stream);
+    v64.preSmoothed.ensure(nAlloc(0), stream);
     const int nc = nL > 0 ? mesh->lev[nL].nCells : mesh->lev[0].nCells;
-    for (DBuf<double>* b : {&v64.cpA, &v64.cwA, &v64.crA, &v64.crD}) b->alloc(std::max(nc, 1), stream);
+    for (DBuf<double>* b : {&v64.cpA, &v64.cwA, &v64.crA, &v64.crD}) b->ensure(std::max(nc, 1), stream);
     v64.built = true;
     coarseBuilt = true;
 }
@@ -719,16 +739,16 @@ void Matrix::ensureFp32()
     v32.src.resize(nL);
     for (int i = 0; i < nL; ++i)
     {
-        v32.corr[i].alloc(nAlloc(i + 1), stream);
-        v32.src[i].alloc(nAlloc(i + 1), stream);
+        v32.corr[i].ensure(nAlloc(i + 1), stream);
+        v32.src[i].ensure(nAlloc(i + 1), stream);
     }
     const size_t n0 = nAlloc(0);
-    v32.ACf.alloc(n0, stream);
-    v32.preSmoothed.alloc(n0, stream);
-    v32.partial.alloc(2 * kMaxPartials, stream);
-    v32.sf.alloc(1, stream);
-    for (DBuf<float>* b : {&r32, &w32, &AwA32, &fc32, &fr32}) b->alloc(n0, stream);
-    rOld.alloc(n0, stream);
+    v32.ACf.ensure(n0, stream);
+    v32.preSmoothed.ensure(n0, stream);
+    v32.partial.ensure(2 * kMaxPartials, stream);
+    v32.sf.ensure(1, stream);
+    for (DBuf<float>* b : {&r32, &w32, &AwA32, &fc32, &fr32}) b->ensure(n0, stream);
+    rOld.ensure(n0, stream);
     v32.built = true;
 }
 
@@ -760,9 +780,9 @@ template <class T>
 void Matrix::amul(int level, const T* x, T* y)
 {
     const LevelAddr& L = mesh->lev[level];
-    cudaEvent_t e = level == 0 ? timedBegin(0) : nullptr;
+    cudaEvent_t e = timedBegin(0, level, 1);
     k::amul<T><<<rowsGrid(L.nCells), NT, 0, stream>>>(rowsOf(L, data<T>().coef[level]), x, y);
-    timedEnd(0, e);
+    timedEnd(e);
     B2G_LAUNCH_CHECK();
     ++launches;
 }
@@ -771,6 +791,14 @@ template <class T>
 void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps, unsigned long long* trace)
 {
     if (nSweeps <= 0) return;
+    cudaEvent_t e = timedBegin(1, level, nSweeps);
+    smoothCall<T>(level, smoother, psiL, src, nSweeps, trace);
+    timedEnd(e);
+}
+
+template <class T>
+void Matrix::smoothCall(int level, int smoother, T* psiL, const T* src, int nSweeps, unsigned long long* trace)
+{
     if (smoother < B2G_SMOOTHER_GAUSS_SEIDEL || smoother > B2G_SMOOTHER_DIC_GAUSS_SEIDEL)
         fail(B2G_ERR_ARGUMENT, "b2g: unknown smoother");
     if (smoother == B2G_SMOOTHER_DIC || smoother == B2G_SMOOTHER_DIC_GAUSS_SEIDEL)
@@ -835,14 +863,16 @@ void Matrix::gsLaunch(const LevelAddr& L, const LevelCoef<T>& C, T* psiL, const 
     a.b = src;
     a.psi = psiL;
     a.progress = G.progress.p;
+    a.ticket = reinterpret_cast<int*>(G.progress.p + static_cast<size_t>(G.nParts) * k::kProgressStride);
+    a.spinLimit = spinLimit;
+    a.publish = publish;
     a.err = err.p;
     a.trace = trace;
     a.traceDepths = G.maxDepth + 2;
     const size_t smem = k::gsSmemBytes<T>(G.maxCells, G.maxEnt, G.maxGat);
     B2G_CUDA(cudaMemsetAsync(G.progress.p, 0, G.progress.bytes(), stream));
-    cudaEvent_t e = timed ? timedBegin(1) : nullptr;
+    (void)timed;
     k::gsSweep<T><<<G.nParts, G.maxCells + 128, smem, stream>>>(a);
-    timedEnd(1, e);
     B2G_LAUNCH_CHECK();
     launches += 1;
 }
@@ -859,7 +889,8 @@ void Matrix::ensureSym(int level)
         D.revB.resize(mesh->lev.size());
         D.revX.resize(mesh->lev.size());
     }
-    if (D.rev[level].blob.p) return;
+    if (D.revGen.size() < mesh->lev.size()) D.revGen.resize(mesh->lev.size(), -1);
+    if (D.rev[level].blob.p && D.revGen[level] == coefGen) return;
     LevelAddr& L = mesh->lev[level];
     buildReversedLevel(L, stream);
     const LevelAddr& R = *L.rev;
@@ -868,10 +899,11 @@ void Matrix::ensureSym(int level)
     k::revDiag<T><<<rowsGrid(R.nCells), NT, 0, stream>>>(R.nCells, R.gs.posCell.p, v64.coef[level].diag.p, C.gsDiag.p);
     B2G_LAUNCH_CHECK();
     fillBlobs<T>(R, C, v64.coef[level].upper.p, stream);
-    D.revB[level].alloc(std::max(R.gs.nAlloc, 1), stream);
-    D.revX[level].alloc(std::max(R.gs.nAlloc, 1), stream);
+    D.revB[level].ensure(std::max(R.gs.nAlloc, 1), stream);
+    D.revX[level].ensure(std::max(R.gs.nAlloc, 1), stream);
     D.revB[level].zero(stream);
     D.revX[level].zero(stream);
+    D.revGen[level] = coefGen;
 }
 
 // What the smoother needs built before an iteration is captured (builds synchronise the stream).
@@ -969,11 +1001,13 @@ void Matrix::ensureDic(int level)
         if (v->size() < nl) v->resize(nl);
     for (auto* v : {&D.rdPos, &D.dicR, &D.dicLoB, &D.dicLoX, &D.dicUpB, &D.dicUpX})
         if (v->size() < nl) v->resize(nl);
-    if (D.dicLo[level].blob.p) return;
+    if (D.dicGen.size() < nl) D.dicGen.resize(nl, -1);
+    if (D.dicLo[level].blob.p && D.dicGen[level] == coefGen) return;
     LevelAddr& L = mesh->lev[level];
     const int n = L.nCells, nF = L.nFaces;
     if (rdCell.size() < nl) rdCell.resize(nl);
-    if (!rdCell[level].p)
+    if (rdGen.size() < nl) rdGen.resize(nl, -1);
+    if (!rdCell[level].p || rdGen[level] != coefGen)
     {
         const std::vector<double> diag = v64.coef[level].diag.download(stream);
         const std::vector<double> coef = v64.coef[level].upper.download(stream);
@@ -982,7 +1016,11 @@ void Matrix::ensureDic(int level)
         std::vector<double> rD(diag);
         for (int f = 0; f < nF; ++f) rD[up[f]] -= coef[f] * coef[f] / rD[lo[f]];
         for (int c = 0; c < n; ++c) rD[c] = 1.0 / rD[c];
-        rdCell[level].upload(rD.data(), rD.size(), stream);
+        rdCell[level].ensure(rD.size(), stream);
+        B2G_CUDA(cudaMemcpyAsync(rdCell[level].p, rD.data(), sizeof(double) * rD.size(), cudaMemcpyHostToDevice,
+                                 stream));
+        B2G_CUDA(cudaStreamSynchronize(stream));  // rD is a host temporary
+        rdGen[level] = coefGen;
     }
     buildLowerLevel(L, stream);
     buildReversedLevel(L, stream, true);
@@ -1003,22 +1041,23 @@ void Matrix::ensureDic(int level)
         B2G_LAUNCH_CHECK();
         fillBlobs<T>(R, C, which == 0 ? loVal.p : upVal.p, stream);
     }
-    D.rdPos[level].alloc(nAlloc(level), stream);
+    D.rdPos[level].ensure(nAlloc(level), stream);
     D.rdPos[level].zero(stream);
     k::byPosition<T><<<rowsGrid(n), NT, 0, stream>>>(n, L.gs.posCell.p, rdCell[level].p, D.rdPos[level].p);
     B2G_LAUNCH_CHECK();
-    D.dicR[level].alloc(nAlloc(level), stream);
+    D.dicR[level].ensure(nAlloc(level), stream);
     for (auto* v : {&D.dicLoB, &D.dicLoX})
     {
-        (*v)[level].alloc(std::max(L.lowerOnly->gs.nAlloc, 1), stream);
+        (*v)[level].ensure(std::max(L.lowerOnly->gs.nAlloc, 1), stream);
         (*v)[level].zero(stream);
     }
     for (auto* v : {&D.dicUpB, &D.dicUpX})
     {
-        (*v)[level].alloc(std::max(L.revDesc->gs.nAlloc, 1), stream);
+        (*v)[level].ensure(std::max(L.revDesc->gs.nAlloc, 1), stream);
         (*v)[level].zero(stream);
     }
     B2G_CUDA(cudaStreamSynchronize(stream));  // loVal / upVal are read by the blob builds
+    D.dicGen[level] = coefGen;
 }
 
 // DICSmoother::smooth (gamg_solver_cpp.cu:234-317): per sweep r = source - A psi, w = rD r, the two
@@ -1135,23 +1174,19 @@ void Matrix::mcLaunch(int level, bool fused, int cluster, int block, float* psiL
     const LevelCoef<float>& F = v32.coef[level];
     if (cluster > 0)
     {
-        cudaEvent_t ev = timed && level == 0 ? timedBegin(1) : nullptr;
-        ClusterLaunch L(cluster, stream);
+                ClusterLaunch L(cluster, stream);
         B2G_CUDA(cudaLaunchKernelEx(&L.cfg, k::mcSmoothCluster, C.nColours, static_cast<const int*>(C.colourStartD.p),
                                     nSweeps, symmetric ? 1 : 0, static_cast<const int*>(C.pos.p),
                                     static_cast<const int*>(C.sliceBase.p), static_cast<const int*>(C.col.p),
                                     static_cast<const float*>(F.mcVal.p), static_cast<const float*>(F.mcDiag.p), src,
                                     psiL));
-        timedEnd(1, ev);
         ++launches;
         return;
     }
     if (fused)
     {
-        cudaEvent_t ev = timed && level == 0 ? timedBegin(1) : nullptr;
-        k::mcSmoothSmall<<<1, 1024, 0, stream>>>(C.nColours, C.colourStartD.p, nSweeps, symmetric ? 1 : 0, C.pos.p,
+                k::mcSmoothSmall<<<1, 1024, 0, stream>>>(C.nColours, C.colourStartD.p, nSweeps, symmetric ? 1 : 0, C.pos.p,
                                                   C.sliceBase.p, C.col.p, F.mcVal.p, F.mcDiag.p, src, psiL);
-        timedEnd(1, ev);
         B2G_LAUNCH_CHECK();
         ++launches;
         return;
@@ -1163,10 +1198,8 @@ void Matrix::mcLaunch(int level, bool fused, int cluster, int block, float* psiL
             const int k = i < C.nColours ? i : 2 * C.nColours - 1 - i;
             const int b = C.colourStart[k], e = C.colourStart[k + 1];
             if (e <= b) continue;
-            cudaEvent_t ev = timed && level == 0 ? timedBegin(1) : nullptr;
-            k::mcSweep<<<std::min(ceilDiv(e - b, block), 16 * DeviceInfo::get().numSMs), block, 0, stream>>>(
+                        k::mcSweep<<<std::min(ceilDiv(e - b, block), 16 * DeviceInfo::get().numSMs), block, 0, stream>>>(
                 b, e, C.pos.p, C.sliceBase.p, C.col.p, F.mcVal.p, F.mcDiag.p, src, psiL);
-            timedEnd(1, ev);
             B2G_LAUNCH_CHECK();
             ++launches;
         }
@@ -1233,24 +1266,25 @@ void Matrix::tuneMulticolour(int level)
 void Matrix::ensureMulticolour()
 {
     ensureFp32();
-    if (mcBuilt) return;
+    if (mcBuilt && mcGen == coefGen) return;
     for (int i = 0; i <= nLevels(); ++i)
     {
         LevelAddr& L = mesh->lev[i];
         buildColouring(L, stream);
         LevelCoef<float>& F = v32.coef[i];
         const Colouring& C = L.mc;
-        F.mcVal.alloc(std::max<long long>(C.nEnt, 1), stream);
-        F.mcDiag.alloc(std::max(C.nRows, 1), stream);
+        F.mcVal.ensure(std::max<long long>(C.nEnt, 1), stream);
+        F.mcDiag.ensure(std::max(C.nRows, 1), stream);
         const long long m = std::max<long long>(C.nEnt, C.nRows);
         if (m)
             k::mcValues<<<std::min(ceilDiv(m, NT), 8192), NT, 0, stream>>>(C.nEnt, C.nRows, C.face.p, C.pos.p,
                                                                            v64.coef[i].upper.p, F.gsDiag.p,
                                                                            F.mcVal.p, F.mcDiag.p);
         B2G_LAUNCH_CHECK();
-        tuneMulticolour(i);
+        if (!C.tuned) tuneMulticolour(i);
     }
     mcBuilt = true;
+    mcGen = coefGen;
 }
 
 template <class T>
@@ -1269,7 +1303,9 @@ void Matrix::scale(int level, T* field, T* Acf, const T* src)
     else
     {
         const int g = redGrid(L.nCells);
+        cudaEvent_t e = timedBegin(0, level, 1);
         k::amulScaleDots<T, NT><<<g, NT, 0, stream>>>(rowsOf(L, D.coef[level]), field, src, Acf, D.partial.p);
+        timedEnd(e);
         k::scaleFactor<T, NT><<<1, NT, 0, stream>>>(D.partial.p, g, D.sf.p);
     }
     k::scaleUpdate<T><<<rowsGrid(L.nCells), NT, 0, stream>>>(L.nCells, D.sf.p, field, src, Acf,
@@ -1459,9 +1495,9 @@ void Matrix::vcycle(const b2g_controls& c, T* x, const T* src, T* Apsi, T* fcor,
         else
         {
             const int g = redGrid(F.nCells);
-            cudaEvent_t e = timedBegin(0);
+            cudaEvent_t e = timedBegin(0, 0, 1);
             k::amulScaleDots<T, NT><<<g, NT, 0, stream>>>(rowsOf(F, D.coef[0]), fcor, fres, Apsi, D.partial.p);
-            timedEnd(0, e);
+            timedEnd(e);
             k::scaleFactor<T, NT><<<1, NT, 0, stream>>>(D.partial.p, g, D.sf.p);
         }
         k::scaleUpdateAdd<T><<<rowsGrid(F.nCells), NT, 0, stream>>>(F.nCells, D.sf.p, fcor, fres, Apsi,
@@ -1562,10 +1598,39 @@ void Matrix::checkDeviceError()
     }
 }
 
+// The addresses of the per-level buffers an iteration's launches read and write, hashed: a graph
+// captured before a buffer moved is never replayed (a rebuild with new coefficients keeps them in
+// place, so the graph of the previous coefficients stays valid).
+unsigned long long Matrix::layoutFingerprint() const
+{
+    unsigned long long h = 1469598103934665603ull;
+    auto mix = [&h](const void* p) {
+        h ^= reinterpret_cast<unsigned long long>(p);
+        h *= 1099511628211ull;
+    };
+    for (const auto* b : {&psi, &source, &rA, &wA, &pA, &AwA, &fc, &fr, &rOld}) mix(b->p);
+    for (const auto* b : {&r32, &w32, &AwA32, &fc32, &fr32}) mix(b->p);
+    for (const auto& C : v64.coef)
+        for (const void* q : {(const void*)C.gsDiag.p, (const void*)C.rowVal.p, (const void*)C.blob.p}) mix(q);
+    for (const auto& C : v32.coef)
+        for (const void* q : {(const void*)C.gsDiag.p, (const void*)C.rowVal.p, (const void*)C.blob.p,
+                              (const void*)C.mcVal.p, (const void*)C.mcDiag.p})
+            mix(q);
+    for (const auto& b : v64.corr) mix(b.p);
+    for (const auto& b : v64.src) mix(b.p);
+    for (const auto& b : v32.corr) mix(b.p);
+    for (const auto& b : v32.src) mix(b.p);
+    for (const auto* b : {&v64.ACf, &v64.preSmoothed, &v64.partial, &v64.sf, &v64.cpA, &v64.cwA, &v64.crA, &v64.crD})
+        mix(b->p);
+    for (const auto* b : {&v32.ACf, &v32.preSmoothed, &v32.partial, &v32.sf}) mix(b->p);
+    return h;
+}
+
 template <class F>
 void Matrix::runIteration(IterationGraph& G, const b2g_controls& c, F&& body)
 {
-    std::vector<unsigned char> key(sizeof(b2g_controls) + sizeof(void*) + 3 * sizeof(int));
+    std::vector<unsigned char> key(sizeof(b2g_controls) + sizeof(void*) + 3 * sizeof(int) +
+                                   sizeof(unsigned long long));
     unsigned char* k = key.data();
     std::memcpy(k, &c, sizeof(b2g_controls));
     k += sizeof(b2g_controls);
@@ -1574,6 +1639,9 @@ void Matrix::runIteration(IterationGraph& G, const b2g_controls& c, F&& body)
     k += sizeof(void*);
     const int flags[3] = {coarseLogCapacity, serial ? 1 : 0, g_profiling ? 1 : 0};
     std::memcpy(k, flags, sizeof(flags));
+    k += sizeof(flags);
+    const unsigned long long fp = layoutFingerprint();
+    std::memcpy(k, &fp, sizeof(fp));
     if (!G.exec || G.key != key)
     {
         releaseGraph(G);
@@ -1755,5 +1823,7 @@ template void Matrix::smooth<float>(int, int, float*, const float*, int, unsigne
 template void Matrix::scale<double>(int, double*, double*, const double*);
 template void Matrix::restrictTo<double>(int, const double*, double*);
 template void Matrix::prolongFrom<double>(int, const double*, double*);
+template void Matrix::gsLaunch<double>(const LevelAddr&, const LevelCoef<double>&, double*, const double*,
+                                        unsigned long long*, bool);
 
 }  // namespace b2g

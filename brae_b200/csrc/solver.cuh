@@ -51,6 +51,8 @@ struct VCycleData
     std::vector<DBuf<T>> rdPos, dicR, dicLoB, dicLoX, dicUpB, dicUpX;
     // a coupled matrix: per level the Gauss-Seidel smoothers' bPrime with the pair folded in
     std::vector<DBuf<T>> pairB;
+    // the coefficient generation (Matrix::coefGen) each level's reversed and DIC layouts were filled for
+    std::vector<long long> revGen, dicGen;
     // FP32 form only: dense Cholesky of the coarsest level
     bool built = false;
 };
@@ -58,14 +60,21 @@ struct VCycleData
 // One PCG (or GAMG) iteration captured as a CUDA graph, replayed while the launches it captured stay
 // valid: the key holds what they depend on beyond the matrix's fixed buffers (the controls, the
 // coarsest-level log, the reduction order).
+// A profiled region (b2g_set_profiling): the events around one Amul (kind 0) or one smoothing call
+// (kind 1) of one level, and its units (Amuls, or the sweeps of the smoothing call).
+struct TimedRegion
+{
+    cudaEvent_t start = nullptr, end = nullptr;
+    int kind = 0, level = 0, units = 0;
+};
+
 struct IterationGraph
 {
     cudaGraphExec_t exec = nullptr;
     std::vector<unsigned char> key;
     long long launchesPerReplay = 0;
-    // profiling: event pairs captured as event-record nodes around the finest level's Amul (0) and
-    // Gauss-Seidel (1) launches; re-recorded by every replay, read after it
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[2];
+    // profiling: the regions captured as event-record nodes; re-recorded by every replay, read after it
+    std::vector<TimedRegion> regions;
 };
 
 struct Matrix
@@ -86,20 +95,31 @@ struct Matrix
     int coarseLogCapacity = 0;
     IterationGraph pcgGraph, gamgGraph;
     bool serial = false;                      // B2G_REDUCTION_SERIAL for the current solve
+    // the sweep's bounded waits: polls before giving up, and whether parts publish their progress
+    // (changed only by b2g_level_smooth_stall, which tests that the waits end)
+    long long spinLimit = k::kSpinLimit;
+    int publish = 1;
     bool coupled = false;                     // the matrix carries the mesh's coupled pair (FP64 only)
     bool multicolour = false;                 // the FP32 V-cycle sweeps colour by colour
     bool mcBuilt = false;
-    // timing (b2g_set_profiling): events around the finest level's Amul and Gauss-Seidel launches
-    double ms[4] = {0, 0, 0, 0};              // finest Amul, finest Gauss-Seidel, other, whole solve
-    long long counts[4] = {0, 0, 0, 0};       // launches of the same classes (whole solve: all)
+    // bumped by every setFine: layouts filled from the coefficients (the multicolour values, the
+    // reversed and DIC layouts) are refilled, into the same buffers, when their generation is older
+    long long coefGen = 0, mcGen = -1;
+    std::vector<long long> rdGen;
+    // timing (b2g_set_profiling): events around every level's Amuls and smoothing calls
+    double ms[4] = {0, 0, 0, 0};              // finest Amul, finest smoothing, other, whole solve
+    long long counts[4] = {0, 0, 0, 0};       // finest Amuls, finest sweeps, other launches, all launches
     long long launches = 0;
-    double graphMs[2] = {0, 0};               // finest Amul / Gauss-Seidel time inside graph replays
-    long long graphCounts[2] = {0, 0};
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evAmul, evGs, evFree;
+    std::vector<double> lvMs[2];              // per kind (0 Amul, 1 smoothing) and level: milliseconds,
+    std::vector<long long> lvCalls[2], lvUnits[2];  // timed regions, units (Amuls / sweeps)
+    std::vector<TimedRegion> evOpen;          // regions recorded outside a capture, read at the end
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evFree;
     cudaEvent_t evSolve[2] = {nullptr, nullptr};
     IterationGraph* capturing = nullptr;      // the graph being captured, if any
-    cudaEvent_t timedBegin(int cls);          // records a start event if profiling (cls 0 Amul, 1 GS)
-    void timedEnd(int cls, cudaEvent_t start);
+    // records a start event if profiling; the region is closed by timedEnd
+    cudaEvent_t timedBegin(int kind, int level, int units);
+    void timedEnd(cudaEvent_t start);
+    void addRegion(const TimedRegion& r);     // a finished region into the per-level sums
     void timingsBegin();
     void timingsEnd();
     ~Matrix();
@@ -136,6 +156,8 @@ struct Matrix
     template <class T> void amul(int level, const T* x, T* y);
     template <class T> void smooth(int level, int smoother, T* psi, const T* source, int nSweeps,
                                    unsigned long long* trace = nullptr);
+    template <class T> void smoothCall(int level, int smoother, T* psi, const T* source, int nSweeps,
+                                       unsigned long long* trace);
     template <class T> void scale(int level, T* field, T* Acf, const T* source);
     template <class T> void restrictTo(int step, const T* fine, T* coarse);
     template <class T> void prolongFrom(int step, const T* coarse, T* fine);
@@ -159,6 +181,7 @@ struct Matrix
     void checkDeviceError();
     // runs `body` (the launches of one iteration) through G: captured on first use, replayed after
     template <class F> void runIteration(IterationGraph& G, const b2g_controls& c, F&& body);
+    unsigned long long layoutFingerprint() const;
     void collectGraphTimings(IterationGraph& G);  // after a replay has finished
     void releaseGraph(IterationGraph& G);
     template <class T> VCycleData<T>& data();

@@ -87,6 +87,7 @@ def _load():
                                 C.POINTER(_Log)]),
         "b2g_matrix_create": (ip, [vp, vp, vp, ip, vp, C.POINTER(vp)]),
         "b2g_matrix_destroy": (ip, [vp]),
+        "b2g_matrix_set_coeffs": (ip, [vp, vp, vp, ip]),
         "b2g_matrix_get_level": (ip, [vp, ip, vp, vp]),
         "b2g_level_amul": (ip, [vp, ip, vp, vp]),
         "b2g_level_smooth": (ip, [vp, ip, ip, vp, vp, ip]),
@@ -104,7 +105,9 @@ def _load():
         "b2g_matrix_pcg_solve": (ip, [vp, vp, vp, C.POINTER(Controls), ip, C.POINTER(_Perf),
                                       C.POINTER(_Log)]),
         "b2g_matrix_timings": (ip, [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
+        "b2g_matrix_level_timings": (ip, [vp, ip, ip, vp, vp, vp, C.POINTER(C.c_int)]),
         "b2g_level_smooth_trace": (ip, [vp, ip, vp, vp, vp, ip, C.POINTER(C.c_int)]),
+        "b2g_level_smooth_stall": (ip, [vp, ip, vp, vp, C.c_longlong, C.POINTER(C.c_int)]),
         "b2g_batch_create": (ip, [C.POINTER(vp), ip, C.POINTER(vp)]),
         "b2g_batch_solve": (ip, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(Controls), ip, C.POINTER(_Perf)]),
         "b2g_batch_launches": (ip, [vp, C.POINTER(C.c_longlong)]),
@@ -143,6 +146,7 @@ EXPORTED = [
     "b2g_server_submit", "b2g_server_wait", "b2g_server_case_bytes", "b2g_batch_create", "b2g_batch_solve",
     "b2g_batch_launches", "b2g_batch_destroy", "b2g_mesh_set_pair", "b2g_mesh_level_pair",
     "b2g_gamg_solve_coupled", "b2g_matrix_create_coupled", "b2g_matrix_level_pair_coeffs", "b2g_matrix_gamg_solve",
+    "b2g_matrix_set_coeffs", "b2g_matrix_level_timings", "b2g_level_smooth_stall",
 ]
 
 
@@ -349,6 +353,13 @@ class Matrix:
         self.handle = h
         self.mesh = mesh
 
+    def set_coeffs(self, diag, upper):
+        """New fine-level coefficients on the same mesh; every coarse level is rebuilt in place."""
+        if not _is_torch(diag):
+            diag = _as_host(diag, np.float64)
+            upper = _as_host(upper, np.float64)
+        _check(lib.b2g_matrix_set_coeffs(self.handle, _ptr(diag), _ptr(upper), _memspace(diag, upper)))
+
     def pair_coeffs(self, level: int):
         m = len(self.mesh.level_pair(level)[0])
         c = np.empty(m)
@@ -395,6 +406,14 @@ class Matrix:
                                               int(trace.numel()), sched))
         return info
 
+    def smooth_stall(self, level, psi, source, spin_limit):
+        """One sweep in which no part publishes its progress, waits limited to `spin_limit` polls
+        (b2g_level_smooth_stall): returns (status name, the level's part count)."""
+        parts = C.c_int()
+        rc = lib.b2g_level_smooth_stall(self.handle, level, _ptr(psi), _ptr(source), int(spin_limit),
+                                        C.byref(parts))
+        return STATUS.get(rc, str(rc)), parts.value
+
     def scale(self, level, field, Acf, source):
         _check(lib.b2g_level_scale(self.handle, level, _ptr(field), _ptr(Acf), _ptr(source)))
 
@@ -432,11 +451,23 @@ class Matrix:
                 lb.history(), lb.coarsest())
 
     def timings(self):
-        """(ms, counts) of the last solve: [finest Amul, finest Gauss-Seidel, other, whole solve]."""
+        """(ms, counts) of the last solve: [finest Amuls, finest smoothing (count: sweeps), other
+        (count: launches), whole solve (count: all launches)]."""
         ms = (C.c_double * 4)()
         n = (C.c_longlong * 4)()
         _check(lib.b2g_matrix_timings(self.handle, ms, n))
         return list(ms), list(n)
+
+    def level_timings(self, kind: int):
+        """Per level of the last profiled solve, kind 0 (Amul) or 1 (smoothing): a list of
+        (ms, timed regions, units) -- units are Amuls, or the sweeps of the smoothing calls."""
+        cap = self.mesh.n_levels + 1
+        ms = (C.c_double * cap)()
+        reg = (C.c_longlong * cap)()
+        un = (C.c_longlong * cap)()
+        have = C.c_int()
+        _check(lib.b2g_matrix_level_timings(self.handle, kind, cap, ms, reg, un, C.byref(have)))
+        return [(ms[i], reg[i], un[i]) for i in range(min(have.value, cap))]
 
 
 def set_profiling(on: bool) -> None:

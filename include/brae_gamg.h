@@ -215,7 +215,10 @@ B2G_API b2g_status b2g_mesh_build_ms(const b2g_mesh* mesh, float* ms);
  * is overwritten with the solution; `out` receives the SolverPerformance. The preconditioner is
  * built only when the initial residual has not already converged (PCG.C:111-118).
  * Replaces pcgGamgSolve (GAMGH:217-229) and devicePcgGamgSolve (DGAMG:143-154).
- * `diag`, `source`, `psi` are [nCells], `upper` is [nFaces] (lower == upper). `log` may be NULL. */
+ * `diag`, `source`, `psi` are [nCells], `upper` is [nFaces] (lower == upper). `log` may be NULL.
+ * The mesh keeps the matrix it solves on between calls (its buffers and captured iteration graphs):
+ * each call replaces its coefficients and rebuilds the coarse levels. Calls on one mesh must not
+ * overlap (the reference's solve is not re-entrant either). */
 B2G_API b2g_status b2g_pcg_gamg_solve(b2g_mesh* mesh, const double* diag, const double* upper,
                                       const double* source, double* psi,
                                       const b2g_controls* controls, int memspace, void* stream,
@@ -276,6 +279,12 @@ B2G_API b2g_status b2g_matrix_gamg_solve(b2g_matrix* m, const double* source, do
  * gamg_solver_cpp.cu:474-526), plus the per-level coefficient layouts the kernels read. */
 B2G_API b2g_status b2g_matrix_create(b2g_mesh* mesh, const double* diag, const double* upper,
                                      int memspace, void* stream, b2g_matrix** out);
+/* New coefficients for an existing matrix on the same mesh (the next time step's pressure matrix):
+ * the fine level is replaced and every coarse level rebuilt, as GamgHierarchy::build does in each
+ * pcgGamgSolve call (gamg_solver_cpp.cu:1081-1083), into the buffers the matrix already holds, so
+ * its captured iteration graphs are replayed, not captured again. Refused for a coupled matrix. */
+B2G_API b2g_status b2g_matrix_set_coeffs(b2g_matrix* m, const double* diag, const double* upper,
+                                         int memspace);
 B2G_API b2g_status b2g_matrix_destroy(b2g_matrix* m);
 /* Copies level `level`'s diag [nCells] and upper [nFaces] to HOST arrays. */
 B2G_API b2g_status b2g_matrix_get_level(const b2g_matrix* m, int level, double* diag,
@@ -324,11 +333,18 @@ B2G_API b2g_status b2g_matrix_pcg_solve(b2g_matrix* m, const double* source, dou
 
 /* ---- introspection ---------------------------------------------------------------------------- */
 
-/* Device time of the last solve on `m` by kernel class (milliseconds, `ms4`) and launches of each
- * class (`counts4`): [0] Amul on the finest level, [1] Gauss-Seidel sweeps on the finest level,
- * [2] everything else, [3] the whole solve. Times are taken with events on the solve's stream only
- * while b2g_set_profiling(1) is on (counts always). Either pointer may be NULL. */
+/* Device time of the last solve on `m` by kernel class (milliseconds, `ms4`) and counts of each
+ * class (`counts4`): [0] Amuls on the finest level, [1] smoothing on the finest level (the count is
+ * sweeps), [2] everything else (the count is launches), [3] the whole solve (all launches). Times
+ * are taken with events on the solve's stream only while b2g_set_profiling(1) is on (the launch
+ * count always). Either pointer may be NULL. */
 B2G_API b2g_status b2g_matrix_timings(const b2g_matrix* m, double* ms4, long long* counts4);
+/* The same per level, for `kind` 0 (Amul, including the one of the correction scaling) or 1
+ * (smoothing calls): for levels 0..capacity-1, milliseconds, timed regions and units (Amuls, or
+ * the sweeps of the smoothing calls) of the last solve. *nLevels receives the number of levels
+ * with a record. Any array may be NULL. */
+B2G_API b2g_status b2g_matrix_level_timings(const b2g_matrix* m, int kind, int capacity, double* ms,
+                                            long long* regions, long long* units, int* nLevels);
 B2G_API b2g_status b2g_set_profiling(int on);
 
 /* Diagnostic: one Gauss-Seidel sweep of `level` (device pointers) recording into the device array
@@ -339,6 +355,14 @@ B2G_API b2g_status b2g_set_profiling(int on);
  * and depth d two (d published to the downstream parts, upstream parts first seen at d).
  * `schedule` (host, may be NULL) receives {nParts, nChunks, chunk cell capacity, chunk entry
  * capacity, max depth}. */
+/* Diagnostic, for testing that the sweep's device-side waits end: one Gauss-Seidel sweep of `level`
+ * (device pointers) in which no part publishes its progress, every wait limited to `spinLimit` polls
+ * (1 .. 2^24). A part that needs values of another part waits for a progress word nothing sets,
+ * gives up, and the call returns B2G_ERR_DEVICE_TIMEOUT with psi invalid; the context stays usable.
+ * A level swept by one part has no such wait and returns B2G_OK. *nParts (may be NULL) receives the
+ * level's part count. No counterpart in the reference. */
+B2G_API b2g_status b2g_level_smooth_stall(b2g_matrix* m, int level, double* psi, const double* source,
+                                          long long spinLimit, int* nParts);
 B2G_API b2g_status b2g_level_smooth_trace(b2g_matrix* m, int level, double* psi, const double* source,
                                           unsigned long long* trace, int traceCapacity, int* schedule);
 /* Diagnostic: the Gauss-Seidel schedule of `level` to HOST arrays (either may be NULL):

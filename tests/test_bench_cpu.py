@@ -30,3 +30,8 @@ def test_reference_arm_json_line():
     assert d["config"]["cells"] == 20 ** 3
     init, final, iters = d["config"]["solver_perf"]
     assert init == 1.0 and 0 < final < 0.05 and iters >= 1
+    # both arms word the workload from one function, so the driver sees the same configuration
+    sys.path.insert(0, REPO)
+    import bench
+    assert d["config"]["workload"] == bench.workload_name(20)
+    assert d["cpu_baseline"]["cpu_model"]
