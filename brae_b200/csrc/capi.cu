@@ -493,6 +493,12 @@ b2g_status b2g_set_profiling(int on)
     return B2G_OK;
 }
 
+b2g_status b2g_set_sweep_pipeline(int on)
+{
+    b2g::g_pipeline = on != 0;
+    return B2G_OK;
+}
+
 b2g_status b2g_controls_default(b2g_controls* out)
 {
     return guarded([&] {
@@ -804,6 +810,44 @@ b2g_status b2g_level_smooth_stall(b2g_matrix* m, int level, double* psi, const d
         A.publish = 1;
         A.fromPos(level, static_cast<const double*>(A.ioBuf(0)), psi);
         A.checkDeviceError();
+    });
+}
+
+b2g_status b2g_level_smooth_pipelined(b2g_matrix* m, int level, double* psi, const double* source, int nSweeps,
+                                      int ranks)
+{
+    return guarded([&] {
+        need(m && psi && source, "b2g_level_smooth_pipelined: null argument");
+        need(level >= 0 && level <= m->mat->nLevels(), "b2g_level_smooth_pipelined: level out of range");
+        need(nSweeps >= 1, "b2g_level_smooth_pipelined: nSweeps must be positive");
+        need(ranks == 1 || ranks == 2 || ranks == 4 || ranks == 8 || ranks == 16,
+             "b2g_level_smooth_pipelined: ranks is 1, 2, 4, 8 or 16");
+        b2g::Matrix& A = *m->mat;
+        need(!A.coupled, "b2g_level_smooth_pipelined: not for a coupled matrix");
+        A.toPos(level, static_cast<const double*>(psi), A.ioBuf(0));
+        A.toPos(level, source, A.ioBuf(1));
+        if (!A.pipeForced<double>(level, A.ioBuf(0), A.ioBuf(1), nSweeps, ranks))
+            b2g::fail(B2G_ERR_ARGUMENT, "b2g_level_smooth_pipelined: the level does not fit that many CTAs");
+        A.fromPos(level, static_cast<const double*>(A.ioBuf(0)), psi);
+        B2G_CUDA(cudaStreamSynchronize(A.stream));
+    });
+}
+
+b2g_status b2g_level_pipe_shape(const b2g_mesh* mesh, int level, int nSweeps, int valueBytes, int* ranks,
+                                int* nSteps, float* msPipe, float* msSweeps)
+{
+    return guarded([&] {
+        need(mesh != nullptr, "b2g_level_pipe_shape: null mesh");
+        need(level >= 0 && level <= mesh->m.nLevels(), "b2g_level_pipe_shape: level out of range");
+        need(valueBytes == 4 || valueBytes == 8, "b2g_level_pipe_shape: valueBytes is 4 or 8");
+        const auto& pipe = mesh->m.lev[level].pipe;
+        const auto it = pipe.find(nSweeps * 16 + valueBytes);
+        const bool have = it != pipe.end();
+        const bool use = have && it->second.use;
+        if (ranks) *ranks = use ? it->second.sched->ranks : 0;
+        if (nSteps) *nSteps = use ? it->second.sched->nSteps : 0;
+        if (msPipe) *msPipe = have ? it->second.msPipe : 0.f;
+        if (msSweeps) *msSweeps = have ? it->second.msSweeps : 0.f;
     });
 }
 

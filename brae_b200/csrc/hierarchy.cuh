@@ -4,9 +4,36 @@
 
 #include "b2g_common.cuh"
 
+#include <map>
 #include <memory>
 
 namespace b2g {
+
+// One smoothing call's sweeps of a level in one pipelined launch (pipe_kernels.cuh), for a given
+// sweep count: the combined steps of every (sweep, cell) item, the cells split into `ranks`
+// contiguous ranges held in the shared memory of one CTA each (one cluster when ranks > 1).
+struct PipeSchedule
+{
+    int sweeps = 0;
+    int ranks = 0;
+    int nSteps = 0;
+    int maxLocal = 0;           // shared-memory slots per rank
+    DBuf<int> stepStart;        // [ranks][nSteps + 1] item ranges
+    DBuf<int4> item;            // [sweeps * nCells] {position, local slot, first entry, end entry}
+    DBuf<unsigned> entAddr;     // [2 * nFaces] per position-order row entry: rank << 24 | slot
+    DBuf<int> localPos;         // [ranks][maxLocal] position of each slot
+    DBuf<int> localCount;       // [ranks]
+};
+
+// The choice for one (level, sweep count, value type), by measurement (Matrix::ensurePipe): the
+// pipelined launch with the fastest rank count, or the sweep-by-sweep launches when those are faster.
+struct PipeChoice
+{
+    bool use = false;
+    std::unique_ptr<PipeSchedule> sched;
+    float msPipe = 0.f;   // per smoothing call, the chosen pipelined shape
+    float msSweeps = 0.f; // per smoothing call, sweep by sweep
+};
 
 // The sweep order of one level and its Gauss-Seidel schedule (gs_kernels.cuh). Cells are split into
 // `nParts` contiguous index ranges; each part lists its cells by (depth, cell), depth being the cell's
@@ -121,6 +148,8 @@ struct LevelAddr
     std::unique_ptr<LevelAddr> revDesc;
     DBuf<int> revDescPos;
     PairLevel pair;         // the coupled pair, if the mesh carries one (nFaces 0 otherwise)
+    // pipelined smoothing calls, keyed by sweeps * 16 + the value size (built on first use)
+    std::map<int, PipeChoice> pipe;
     // The one-block resident Gauss-Seidel sweep of a small one-part level (solver.cu gsResident),
     // built on first use: the part's positions run by depth, depth d's are [start[d], start[d+1]).
     struct Resident

@@ -1,0 +1,329 @@
+// pipe.cu -- the pipelined multi-sweep Gauss-Seidel launch (pipe_kernels.cuh): its schedule, built
+// once per (level, sweep count) on the host from the level's addressing, and the choice, by
+// measurement on the device, between its shapes (one CTA, or a cluster of 2..16 CTAs) and the
+// sweep-by-sweep launches.
+//
+// Reference: the sweeps it reproduces are gaussSeidelSweeps, src/OpenFOAM/matrices/
+// smooth_solver_cpp.cu:87-166 (forward only for GaussSeidel, :144), called nSweeps times per
+// smoothing call by GaussSeidelSmoother::smooth (gamg_solver_cpp.cu:234-317).
+
+#include "pipe_kernels.cuh"
+#include "solver.cuh"
+
+#include <algorithm>
+#include <atomic>
+#include <vector>
+
+namespace b2g {
+namespace {
+
+constexpr size_t kPipeSmemCap = 220 * 1024;  // dynamic shared memory of one rank: its psi slots
+
+// The level's addressing on the host, as the schedule builder reads it.
+struct LevelHost
+{
+    int n = 0, nF = 0;
+    std::vector<int> lower, upper, depth, posCell, posRow, entColPos;
+};
+
+LevelHost download(const LevelAddr& L, cudaStream_t s)
+{
+    LevelHost H;
+    H.n = L.nCells;
+    H.nF = L.nFaces;
+    H.lower = L.lower.download(s);
+    H.upper = L.upper.download(s);
+    H.depth = L.gs.depth.download(s);
+    H.posCell = L.gs.posCell.download(s);
+    H.posRow = L.gs.posRow.download(s);
+    H.entColPos = L.gs.entColPos.download(s);
+    H.lower.resize(H.nF);
+    H.upper.resize(H.nF);
+    H.posRow.resize(static_cast<size_t>(H.n) + 1);
+    H.entColPos.resize(2 * static_cast<size_t>(H.nF));
+    return H;
+}
+
+// T_s(c) of every item (s, c), s < S (pipe_kernels.cuh): T_0 is the depth; then per sweep the upper
+// neighbours' and the cell's own previous step, then the lower neighbours' in face order (faces are
+// sorted by owner, so a face's owner has its final value when the face is reached).
+std::vector<int> combinedSteps(const LevelHost& H, int S, int& nSteps)
+{
+    const size_t n = static_cast<size_t>(H.n);
+    std::vector<int> T(static_cast<size_t>(S) * n);
+    std::copy(H.depth.begin(), H.depth.begin() + n, T.begin());
+    for (int s = 1; s < S; ++s)
+    {
+        const int* prev = T.data() + (s - 1) * n;
+        int* cur = T.data() + s * n;
+        for (size_t c = 0; c < n; ++c) cur[c] = prev[c] + 1;
+        for (int f = 0; f < H.nF; ++f) cur[H.lower[f]] = std::max(cur[H.lower[f]], prev[H.upper[f]] + 1);
+        for (int f = 0; f < H.nF; ++f) cur[H.upper[f]] = std::max(cur[H.upper[f]], cur[H.lower[f]] + 1);
+    }
+    nSteps = T.empty() ? 0 : *std::max_element(T.begin(), T.end()) + 1;
+    return T;
+}
+
+// The schedule for R ranks, or null when a rank's slots do not fit the shared memory.
+std::unique_ptr<PipeSchedule> assemble(const LevelHost& H, const std::vector<int>& T, int S, int nSteps, int R,
+                                       size_t valueBytes, cudaStream_t s)
+{
+    const int n = H.n;
+    if (n == 0 || R < 1 || R > k::kPipeMaxRanks) return nullptr;
+    // ranks: contiguous cell ranges; slots: a rank's cells in position order
+    std::vector<int> rankOf(n), slotOf(n), count(R, 0);
+    for (int c = 0; c < n; ++c) rankOf[c] = static_cast<int>(static_cast<long long>(c) * R / n);
+    for (int p = 0; p < n; ++p)
+    {
+        const int c = H.posCell[p];
+        slotOf[c] = count[rankOf[c]]++;
+    }
+    const int maxLocal = *std::max_element(count.begin(), count.end());
+    if (static_cast<size_t>(maxLocal) * valueBytes > kPipeSmemCap || maxLocal >= (1 << 24)) return nullptr;
+    std::vector<int> localPos(static_cast<size_t>(R) * maxLocal, 0);
+    for (int p = 0; p < n; ++p)
+    {
+        const int c = H.posCell[p];
+        localPos[static_cast<size_t>(rankOf[c]) * maxLocal + slotOf[c]] = p;
+    }
+    // items, rank-major then by step, in position order within a (rank, step)
+    const size_t stride = static_cast<size_t>(nSteps) + 1;
+    std::vector<int> start(static_cast<size_t>(R) * stride + 1, 0);
+    for (int c = 0; c < n; ++c)
+        for (int q = 0; q < S; ++q) ++start[static_cast<size_t>(rankOf[c]) * stride + T[static_cast<size_t>(q) * n + c] + 1];
+    for (size_t i = 1; i < start.size(); ++i) start[i] += start[i - 1];
+    std::vector<int> cursor(start.begin(), start.end() - 1);
+    std::vector<int4> item(static_cast<size_t>(S) * n);
+    for (int p = 0; p < n; ++p)
+    {
+        const int c = H.posCell[p];
+        for (int q = 0; q < S; ++q)
+        {
+            const int at = cursor[static_cast<size_t>(rankOf[c]) * stride + T[static_cast<size_t>(q) * n + c]]++;
+            item[at] = make_int4(p, slotOf[c], H.posRow[p], H.posRow[p + 1]);
+        }
+    }
+    // per rank and step its item range [stepStart[r][t], stepStart[r][t + 1]): the last entry of a
+    // rank's row is the first of the next rank's, so the table is start[] read per rank
+    std::vector<int> stepStart(static_cast<size_t>(R) * stride);
+    for (int r = 0; r < R; ++r)
+        for (size_t t = 0; t < stride; ++t) stepStart[r * stride + t] = start[r * stride + t];
+    std::vector<unsigned> entAddr(H.entColPos.size());
+    for (size_t e = 0; e < entAddr.size(); ++e)
+    {
+        const int c = H.posCell[H.entColPos[e]];
+        entAddr[e] = static_cast<unsigned>(rankOf[c]) << 24 | static_cast<unsigned>(slotOf[c]);
+    }
+    auto P = std::make_unique<PipeSchedule>();
+    P->sweeps = S;
+    P->ranks = R;
+    P->nSteps = nSteps;
+    P->maxLocal = maxLocal;
+    P->stepStart.upload(stepStart.data(), stepStart.size(), s);
+    P->item.upload(item.data(), item.size(), s);
+    P->entAddr.upload(entAddr.data(), std::max<size_t>(entAddr.size(), 1), s);
+    P->localPos.upload(localPos.data(), localPos.size(), s);
+    P->localCount.upload(count.data(), count.size(), s);
+    B2G_CUDA(cudaStreamSynchronize(s));  // the host vectors go out of scope
+    return P;
+}
+
+template <class T>
+void allowPipeSmem()
+{
+    static std::atomic<unsigned long long> done{0};  // one bit per device
+    int dev = 0;
+    B2G_CUDA(cudaGetDevice(&dev));
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (done.load() & bit) return;
+    B2G_CUDA(cudaFuncSetAttribute(k::gsPipe<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(kPipeSmemCap)));
+    B2G_CUDA(cudaFuncSetAttribute(k::gsPipe<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(kPipeSmemCap)));
+    // clusters above 8 CTAs are non-portable: opt in (refused on devices without them; the tuner
+    // then finds no such shape resident)
+    if (cudaFuncSetAttribute(k::gsPipe<T, true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+        cudaGetLastError();
+    done.fetch_or(bit);
+}
+
+// The launch configuration of a pipelined call.
+struct PipeLaunch
+{
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg;
+    PipeLaunch(int ranks, size_t smem, cudaStream_t s)
+    {
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = static_cast<unsigned>(ranks);
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg = cudaLaunchConfig_t{};
+        cfg.gridDim = dim3(static_cast<unsigned>(ranks));
+        cfg.blockDim = dim3(k::kPipeBlock);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+    }
+};
+
+template <class T>
+bool pipeClusterFits(int ranks, size_t smem, cudaStream_t s)
+{
+    PipeLaunch L(ranks, smem, s);
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k::gsPipe<T, true>, &L.cfg) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return false;
+    }
+    return n >= 1;
+}
+
+int pipeKey(int sweeps, size_t valueBytes) { return sweeps * 16 + static_cast<int>(valueBytes); }
+
+}  // namespace
+
+template <class T>
+void Matrix::pipeLaunch(int level, const PipeSchedule& P, T* psiL, const T* src)
+{
+    const LevelAddr& L = mesh->lev[level];
+    k::PipeArgs<T> a;
+    a.A = rowsOf(L, data<T>().coef[level]);
+    a.nSteps = P.nSteps;
+    a.maxLocal = P.maxLocal;
+    a.stepStart = P.stepStart.p;
+    a.item = P.item.p;
+    a.entAddr = P.entAddr.p;
+    a.localPos = P.localPos.p;
+    a.localCount = P.localCount.p;
+    a.b = src;
+    a.psi = psiL;
+    const size_t smem = sizeof(T) * static_cast<size_t>(P.maxLocal);
+    if (P.ranks == 1)
+    {
+        k::gsPipe<T, false><<<1, k::kPipeBlock, smem, stream>>>(a);
+        B2G_LAUNCH_CHECK();
+    }
+    else
+    {
+        PipeLaunch C(P.ranks, smem, stream);
+        B2G_CUDA(cudaLaunchKernelEx(&C.cfg, k::gsPipe<T, true>, a));
+    }
+    ++launches;
+}
+
+// The pipelined smoothing call of `level` for nSweeps sweeps, tried once per (level, sweep count,
+// value type) on this matrix's values: every shape whose slots fit (one CTA; clusters of 2, 4, 8, 16
+// CTAs that can be resident) against the sweep-by-sweep launches, the fastest kept. Every shape
+// computes every row from the same operands in the same order, so the choice changes the time only.
+// Outside any capture (it synchronises); the work vectors it sweeps are scratch.
+template <class T>
+void Matrix::ensurePipe(int level, int nSweeps)
+{
+    LevelAddr& L = mesh->lev[level];
+    const int key = pipeKey(nSweeps, sizeof(T));
+    if (L.pipe.count(key)) return;
+    PipeChoice& C = L.pipe[key];
+    if (nSweeps < 1 || L.nCells == 0 || L.nCells > k::kPipeMaxRanks * static_cast<int>(kPipeSmemCap / sizeof(T)))
+        return;
+    allowPipeSmem<T>();
+    const LevelHost H = download(L, stream);
+    int nSteps = 0;
+    const std::vector<int> Tsteps = combinedSteps(H, nSweeps, nSteps);
+    DBuf<T> x, b;
+    x.alloc(nAlloc(level), stream);
+    b.alloc(nAlloc(level), stream);
+    x.zero(stream);
+    b.zero(stream);
+    cudaEvent_t e0, e1;
+    B2G_CUDA(cudaEventCreate(&e0));
+    B2G_CUDA(cudaEventCreate(&e1));
+    const long long l0 = launches;
+    auto timeIt = [&](auto&& launch) {
+        launch();  // warm
+        B2G_CUDA(cudaEventRecord(e0, stream));
+        for (int i = 0; i < 3; ++i) launch();
+        B2G_CUDA(cudaEventRecord(e1, stream));
+        B2G_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        B2G_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        return ms / 3.f;
+    };
+    // sweep by sweep: the resident block where the level takes it, else one launch per sweep
+    C.msSweeps = timeIt([&] {
+        if (!residentSweeps<T>(level, x.p, b.p, nSweeps))
+            for (int sw = 0; sw < nSweeps; ++sw) gsLaunch<T>(L, data<T>().coef[level], x.p, b.p, nullptr, false);
+    });
+    checkDeviceError();
+    float best = C.msSweeps;
+    for (int R : {1, 2, 4, 8, 16})
+    {
+        std::unique_ptr<PipeSchedule> P = assemble(H, Tsteps, nSweeps, nSteps, R, sizeof(T), stream);
+        if (!P) continue;
+        if (R > 1 && !pipeClusterFits<T>(R, sizeof(T) * static_cast<size_t>(P->maxLocal), stream)) continue;
+        const float ms = timeIt([&] { pipeLaunch<T>(level, *P, x.p, b.p); });
+        if (!C.sched || ms < C.msPipe)
+        {
+            C.msPipe = ms;
+            if (ms < best)
+            {
+                best = ms;
+                C.sched = std::move(P);
+            }
+        }
+    }
+    C.use = C.sched != nullptr;
+    launches = l0;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    B2G_CUDA(cudaStreamSynchronize(stream));
+}
+
+// nSweeps sweeps of `level` in one pipelined launch when the level's tuned choice says so; false
+// when the sweeps run sweep by sweep (or the choice is not made yet and a capture is on).
+template <class T>
+bool Matrix::pipeSweeps(int level, T* psiL, const T* src, int nSweeps)
+{
+    LevelAddr& L = mesh->lev[level];
+    auto it = L.pipe.find(pipeKey(nSweeps, sizeof(T)));
+    if (it == L.pipe.end())
+    {
+        if (capturing || !g_pipeline) return false;
+        ensurePipe<T>(level, nSweeps);
+        it = L.pipe.find(pipeKey(nSweeps, sizeof(T)));
+    }
+    if (!g_pipeline || !it->second.use) return false;
+    pipeLaunch<T>(level, *it->second.sched, psiL, src);
+    return true;
+}
+
+// A pipelined smoothing call on a given number of ranks, whatever the tuned choice (for tests):
+// false when the level's cells do not fit that many CTAs or such a cluster cannot be resident.
+template <class T>
+bool Matrix::pipeForced(int level, T* psiL, const T* src, int nSweeps, int ranks)
+{
+    const LevelAddr& L = mesh->lev[level];
+    if (nSweeps < 1 || L.nCells == 0) return false;
+    allowPipeSmem<T>();
+    const LevelHost H = download(L, stream);
+    int nSteps = 0;
+    const std::vector<int> Tsteps = combinedSteps(H, nSweeps, nSteps);
+    std::unique_ptr<PipeSchedule> P = assemble(H, Tsteps, nSweeps, nSteps, ranks, sizeof(T), stream);
+    if (!P) return false;
+    if (ranks > 1 && !pipeClusterFits<T>(ranks, sizeof(T) * static_cast<size_t>(P->maxLocal), stream)) return false;
+    pipeLaunch<T>(level, *P, psiL, src);
+    B2G_CUDA(cudaStreamSynchronize(stream));  // P is released on return
+    return true;
+}
+
+template void Matrix::ensurePipe<double>(int, int);
+template bool Matrix::pipeForced<double>(int, double*, const double*, int, int);
+template void Matrix::ensurePipe<float>(int, int);
+template bool Matrix::pipeSweeps<double>(int, double*, const double*, int);
+template bool Matrix::pipeSweeps<float>(int, float*, const float*, int);
+template void Matrix::pipeLaunch<double>(int, const PipeSchedule&, double*, const double*);
+template void Matrix::pipeLaunch<float>(int, const PipeSchedule&, float*, const float*);
+
+}  // namespace b2g

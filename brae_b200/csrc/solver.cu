@@ -14,6 +14,7 @@
 namespace b2g {
 
 bool g_profiling = false;
+bool g_pipeline = true;
 
 namespace {
 
@@ -134,19 +135,6 @@ bool convergedH(double fin, double init, double tol, double relTol)
     return fin < tol || (relTol > kSmall && fin < relTol * init);
 }
 
-// the level's rows, with the coupled pair's entries when the matrix carries one
-template <class T>
-k::Rows<T> rowsOf(const LevelAddr& L, const LevelCoef<T>& C)
-{
-    k::Rows<T> r{L.nCells, L.gs.posRow.p, L.gs.entColPos.p, C.rowVal.p, C.gsDiag.p};
-    if (C.pairVal.p && L.pair.nFaces > 0)
-    {
-        r.pairStart = L.pair.start.p;
-        r.pairCol = L.pair.col.p;
-        r.pairVal = C.pairVal.p;
-    }
-    return r;
-}
 
 // the position-ordered coefficients of one level: diagonal and CSR rows
 __global__ void kGsLayout(int n, long long nnz, const int* __restrict__ posCell, const int* __restrict__ entFacePos,
@@ -835,6 +823,7 @@ void Matrix::smoothCall(int level, int smoother, T* psiL, const T* src, int nSwe
         symSmooth<T>(level, psiL, src, nSweeps);
         return;
     }
+    if (!trace && pipeSweeps<T>(level, psiL, src, nSweeps)) return;
     if (!trace && level > 0 && residentSweeps<T>(level, psiL, src, nSweeps)) return;
     for (int sw = 0; sw < nSweeps; ++sw) gsLaunch<T>(mesh->lev[level], data<T>().coef[level], psiL, src, trace, level == 0);
 }
@@ -965,6 +954,25 @@ void Matrix::prepareSmoother(const b2g_controls& c)
 {
     const bool sym = c.smoother == B2G_SMOOTHER_SYM_GAUSS_SEIDEL;
     const bool dic = c.smoother == B2G_SMOOTHER_DIC || c.smoother == B2G_SMOOTHER_DIC_GAUSS_SEIDEL;
+    // the pipelined launches of the Gauss-Seidel smoothing calls the V-cycle makes (finest sweeps on
+    // level 0; pre- and post-sweeps of every smoothed coarse level), chosen before any capture
+    const bool gsSweeps = c.smoother == B2G_SMOOTHER_GAUSS_SEIDEL || c.smoother == B2G_SMOOTHER_DIC_GAUSS_SEIDEL;
+    const bool exact32 = c.precision == B2G_PRECISION_FP32_PRECOND && c.solver != B2G_SOLVER_GAMG;
+    const bool exact64 = c.precision == B2G_PRECISION_FP64 || c.solver == B2G_SOLVER_GAMG;
+    if (g_pipeline && gsSweeps && (exact32 || exact64))
+    {
+        auto want = [&](int level, int nSweeps) {
+            if (nSweeps <= 0 || level > nLevels()) return;
+            if (exact64) ensurePipe<double>(level, nSweeps);
+            else ensurePipe<float>(level, nSweeps);
+        };
+        want(0, c.nFinestSweeps);
+        for (int li = 0; li + 1 < nLevels(); ++li)
+        {
+            want(li + 1, std::min(c.nPostSweeps + c.postSweepsLevelMultiplier * li, c.maxPostSweeps));
+            if (c.nPreSweeps) want(li + 1, std::min(c.nPreSweeps + c.preSweepsLevelMultiplier * li, c.maxPreSweeps));
+        }
+    }
     // the resident sweep's depth ranges of the small one-part levels, before any iteration is captured
     if (c.smoother != B2G_SMOOTHER_DIC)
         for (int i = 1; i < nLevels(); ++i) ensureResident(i);
@@ -1637,7 +1645,7 @@ void Matrix::runIteration(IterationGraph& G, const b2g_controls& c, F&& body)
     const void* logp = coarseLog.p;
     std::memcpy(k, &logp, sizeof(void*));
     k += sizeof(void*);
-    const int flags[3] = {coarseLogCapacity, serial ? 1 : 0, g_profiling ? 1 : 0};
+    const int flags[3] = {coarseLogCapacity, serial ? 1 : 0, (g_profiling ? 1 : 0) | (g_pipeline ? 2 : 0)};
     std::memcpy(k, flags, sizeof(flags));
     k += sizeof(flags);
     const unsigned long long fp = layoutFingerprint();
@@ -1825,5 +1833,9 @@ template void Matrix::restrictTo<double>(int, const double*, double*);
 template void Matrix::prolongFrom<double>(int, const double*, double*);
 template void Matrix::gsLaunch<double>(const LevelAddr&, const LevelCoef<double>&, double*, const double*,
                                         unsigned long long*, bool);
+template void Matrix::gsLaunch<float>(const LevelAddr&, const LevelCoef<float>&, float*, const float*,
+                                       unsigned long long*, bool);
+template bool Matrix::residentSweeps<double>(int, double*, const double*, int);
+template bool Matrix::residentSweeps<float>(int, float*, const float*, int);
 
 }  // namespace b2g

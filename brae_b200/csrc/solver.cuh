@@ -77,6 +77,23 @@ struct IterationGraph
     std::vector<TimedRegion> regions;
 };
 
+// the level's rows, with the coupled pair's entries when the matrix carries one
+template <class T>
+k::Rows<T> rowsOf(const LevelAddr& L, const LevelCoef<T>& C)
+{
+    k::Rows<T> r{L.nCells, L.gs.posRow.p, L.gs.entColPos.p, C.rowVal.p, C.gsDiag.p};
+    if (C.pairVal.p && L.pair.nFaces > 0)
+    {
+        r.pairStart = L.pair.start.p;
+        r.pairCol = L.pair.col.p;
+        r.pairVal = C.pairVal.p;
+    }
+    return r;
+}
+
+// Whether smoothing calls may take the pipelined multi-sweep launch (pipe.cu; b2g_set_sweep_pipeline).
+extern bool g_pipeline;
+
 struct Matrix
 {
     Mesh* mesh = nullptr;
@@ -141,6 +158,11 @@ struct Matrix
     template <class T> void symSmooth(int level, T* psi, const T* source, int nSweeps);
     void ensureResident(int level);            // the resident sweep's depth ranges (on the mesh, once)
     template <class T> bool residentSweeps(int level, T* psi, const T* source, int nSweeps);
+    // the pipelined multi-sweep launch (pipe.cu): the level's tuned choice, built on first use
+    template <class T> void ensurePipe(int level, int nSweeps);
+    template <class T> bool pipeSweeps(int level, T* psi, const T* source, int nSweeps);
+    template <class T> void pipeLaunch(int level, const PipeSchedule& P, T* psi, const T* source);
+    template <class T> bool pipeForced(int level, T* psi, const T* source, int nSweeps, int ranks);
     void mcLaunch(int level, bool fused, int cluster, int block, float* psi, const float* source, int nSweeps,
                   bool timed, bool symmetric = false);
     void tuneMulticolour(int level);

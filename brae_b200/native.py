@@ -70,6 +70,10 @@ def _load():
         "b2g_last_error": (C.c_char_p, []),
         "b2g_version": (C.c_char_p, []),
         "b2g_set_profiling": (ip, [ip]),
+        "b2g_set_sweep_pipeline": (ip, [ip]),
+        "b2g_level_smooth_pipelined": (ip, [vp, ip, vp, vp, ip, ip]),
+        "b2g_level_pipe_shape": (ip, [vp, ip, ip, ip, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float),
+                                      C.POINTER(C.c_float)]),
         "b2g_controls_default": (ip, [C.POINTER(Controls)]),
         "b2g_controls_read": (ip, [C.c_char_p, C.POINTER(Controls)]),
         "b2g_mesh_create": (ip, [ip, ip, vp, vp, vp, vp, ip, C.POINTER(C.c_int), ip, vp,
@@ -146,7 +150,8 @@ EXPORTED = [
     "b2g_server_submit", "b2g_server_wait", "b2g_server_case_bytes", "b2g_batch_create", "b2g_batch_solve",
     "b2g_batch_launches", "b2g_batch_destroy", "b2g_mesh_set_pair", "b2g_mesh_level_pair",
     "b2g_gamg_solve_coupled", "b2g_matrix_create_coupled", "b2g_matrix_level_pair_coeffs", "b2g_matrix_gamg_solve",
-    "b2g_matrix_set_coeffs", "b2g_matrix_level_timings", "b2g_level_smooth_stall",
+    "b2g_matrix_set_coeffs", "b2g_matrix_level_timings", "b2g_level_smooth_stall", "b2g_set_sweep_pipeline",
+    "b2g_level_smooth_pipelined", "b2g_level_pipe_shape",
 ]
 
 
@@ -289,6 +294,13 @@ class Mesh:
         return {"one_block": whole.value == 1, "cluster_ctas": whole.value if whole.value > 1 else 0,
                 "threads": thr.value, "ms_per_sweep": ms.value}
 
+    def pipe_shape(self, level: int, n_sweeps: int, value_bytes: int = 8) -> dict:
+        """The tuned choice for `level`'s smoothing calls of n_sweeps sweeps (b2g_level_pipe_shape)."""
+        r, st, mp, ms = C.c_int(), C.c_int(), C.c_float(), C.c_float()
+        _check(lib.b2g_level_pipe_shape(self.handle, level, n_sweeps, value_bytes, C.byref(r), C.byref(st),
+                                        C.byref(mp), C.byref(ms)))
+        return {"ranks": r.value, "steps": st.value, "ms_pipelined": mp.value, "ms_sweep_by_sweep": ms.value}
+
     def set_pair(self, own, nbr) -> None:
         """The coupled (cyclic) pair: faceCells and neighbour cells of the coupled patches' faces, each
         face once from its own side (b2g_mesh_set_pair); every coarse level's is built from it."""
@@ -406,6 +418,10 @@ class Matrix:
                                               int(trace.numel()), sched))
         return info
 
+    def smooth_pipelined(self, level, psi, source, n_sweeps, ranks):
+        """n_sweeps sweeps in one pipelined launch on `ranks` CTAs (b2g_level_smooth_pipelined)."""
+        _check(lib.b2g_level_smooth_pipelined(self.handle, level, _ptr(psi), _ptr(source), n_sweeps, ranks))
+
     def smooth_stall(self, level, psi, source, spin_limit):
         """One sweep in which no part publishes its progress, waits limited to `spin_limit` polls
         (b2g_level_smooth_stall): returns (status name, the level's part count)."""
@@ -472,6 +488,11 @@ class Matrix:
 
 def set_profiling(on: bool) -> None:
     _check(lib.b2g_set_profiling(1 if on else 0))
+
+
+def set_sweep_pipeline(on: bool) -> None:
+    """Whether smoothing calls may run their sweeps in one pipelined launch (the default)."""
+    _check(lib.b2g_set_sweep_pipeline(1 if on else 0))
 
 
 def pcg_gamg_solve(mesh: Mesh, diag, upper, source, psi, controls: Controls | None = None,

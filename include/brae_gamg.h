@@ -346,6 +346,11 @@ B2G_API b2g_status b2g_matrix_timings(const b2g_matrix* m, double* ms4, long lon
 B2G_API b2g_status b2g_matrix_level_timings(const b2g_matrix* m, int kind, int capacity, double* ms,
                                             long long* regions, long long* units, int* nLevels);
 B2G_API b2g_status b2g_set_profiling(int on);
+/* Whether the exact Gauss-Seidel smoothing calls may run all their sweeps in one pipelined launch
+ * (on by default; the choice per level is made by measurement on a matrix's first solve). The
+ * results are the same bit for bit either way; off runs every sweep as its own launch. Process-wide,
+ * like b2g_set_profiling. No counterpart in the reference. */
+B2G_API b2g_status b2g_set_sweep_pipeline(int on);
 
 /* Diagnostic: one Gauss-Seidel sweep of `level` (device pointers) recording into the device array
  * `trace` [8 * nChunks + 4 * nParts + 2 * nParts * (maxDepth + 2)] (SM-cycle stamps): per schedule
@@ -363,6 +368,20 @@ B2G_API b2g_status b2g_set_profiling(int on);
  * level's part count. No counterpart in the reference. */
 B2G_API b2g_status b2g_level_smooth_stall(b2g_matrix* m, int level, double* psi, const double* source,
                                           long long spinLimit, int* nParts);
+/* nSweeps exact Gauss-Seidel sweeps of `level` (device pointers, natural cell order) in ONE
+ * pipelined launch on `ranks` CTAs (1, 2, 4, 8 or 16; a thread-block cluster when above 1), whatever
+ * shape the level's tuned choice would take: sweep s+1 runs on a cell once every value its row reads
+ * is final, which gives bit for bit the result of nSweeps sequential sweeps (gaussSeidelSweeps,
+ * smooth_solver_cpp.cu:87-166, called nSweeps times). B2G_ERR_ARGUMENT when the level's cells do not
+ * fit that many CTAs' shared memory or such a cluster cannot be resident. For tests and tuning. */
+B2G_API b2g_status b2g_level_smooth_pipelined(b2g_matrix* m, int level, double* psi, const double* source,
+                                              int nSweeps, int ranks);
+/* The tuned choice for smoothing calls of nSweeps sweeps on `level` in values of `valueBytes` (8 FP64,
+ * 4 FP32): *ranks the pipelined launch's CTAs (0: sweep by sweep, or not tuned yet), *nSteps its
+ * combined steps, and the measured milliseconds per call of the best pipelined shape and of the
+ * sweep-by-sweep launches. Any output may be NULL. */
+B2G_API b2g_status b2g_level_pipe_shape(const b2g_mesh* mesh, int level, int nSweeps, int valueBytes, int* ranks,
+                                        int* nSteps, float* msPipe, float* msSweeps);
 B2G_API b2g_status b2g_level_smooth_trace(b2g_matrix* m, int level, double* psi, const double* source,
                                           unsigned long long* trace, int traceCapacity, int* schedule);
 /* Diagnostic: the Gauss-Seidel schedule of `level` to HOST arrays (either may be NULL):
