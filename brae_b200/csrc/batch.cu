@@ -729,6 +729,7 @@ k::GsArgs<T> gsArgsOf(const LevelAddr& L, const LevelCoef<T>& C, const T* b, T* 
     a.psi = psi;
     a.progress = progress;
     a.ticket = nullptr;  // the batched launch draws its tickets from the level's own counter
+    a.items = 0;
     a.spinLimit = k::kSpinLimit;
     a.publish = 1;
     a.err = err;

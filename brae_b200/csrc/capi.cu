@@ -820,14 +820,16 @@ b2g_status b2g_level_smooth_pipelined(b2g_matrix* m, int level, double* psi, con
         need(m && psi && source, "b2g_level_smooth_pipelined: null argument");
         need(level >= 0 && level <= m->mat->nLevels(), "b2g_level_smooth_pipelined: level out of range");
         need(nSweeps >= 1, "b2g_level_smooth_pipelined: nSweeps must be positive");
-        need(ranks == 1 || ranks == 2 || ranks == 4 || ranks == 8 || ranks == 16,
-             "b2g_level_smooth_pipelined: ranks is 1, 2, 4, 8 or 16");
+        need(ranks == 1 || ranks == 2 || ranks == 4 || ranks == 8 || ranks == 16 || ranks == -1,
+             "b2g_level_smooth_pipelined: ranks is 1, 2, 4, 8, 16 or -1 (the item schedule)");
         b2g::Matrix& A = *m->mat;
         need(!A.coupled, "b2g_level_smooth_pipelined: not for a coupled matrix");
         A.toPos(level, static_cast<const double*>(psi), A.ioBuf(0));
         A.toPos(level, source, A.ioBuf(1));
         if (!A.pipeForced<double>(level, A.ioBuf(0), A.ioBuf(1), nSweeps, ranks))
-            b2g::fail(B2G_ERR_ARGUMENT, "b2g_level_smooth_pipelined: the level does not fit that many CTAs");
+            b2g::fail(B2G_ERR_ARGUMENT, ranks < 0 ? "b2g_level_smooth_pipelined: the level has no item schedule "
+                                                    "(one part, or one sweep)"
+                                                  : "b2g_level_smooth_pipelined: the level does not fit that many CTAs");
         A.fromPos(level, static_cast<const double*>(A.ioBuf(0)), psi);
         B2G_CUDA(cudaStreamSynchronize(A.stream));
     });
@@ -843,10 +845,11 @@ b2g_status b2g_level_pipe_shape(const b2g_mesh* mesh, int level, int nSweeps, in
         const auto& pipe = mesh->m.lev[level].pipe;
         const auto it = pipe.find(nSweeps * 16 + valueBytes);
         const bool have = it != pipe.end();
-        const bool use = have && it->second.use;
-        if (ranks) *ranks = use ? it->second.sched->ranks : 0;
-        if (nSteps) *nSteps = use ? it->second.sched->nSteps : 0;
-        if (msPipe) *msPipe = have ? it->second.msPipe : 0.f;
+        const int mode = have ? it->second.mode : 0;
+        if (ranks) *ranks = mode == 1 ? it->second.sched->ranks : mode == 2 ? -it->second.items->nParts : 0;
+        if (nSteps)
+            *nSteps = mode == 1 ? it->second.sched->nSteps : mode == 2 ? it->second.items->maxDepth + 1 : 0;
+        if (msPipe) *msPipe = !have ? 0.f : mode == 2 ? it->second.msItems : it->second.msPipe;
         if (msSweeps) *msSweeps = have ? it->second.msSweeps : 0.f;
     });
 }

@@ -82,18 +82,21 @@ inline void gsWindowExtents(int M, int& ahead, int& behind)
 
 __host__ __device__ inline unsigned r16(unsigned b) { return (b + 15u) & ~15u; }
 
-// A chunk's blob: [diagonal: m T][row descriptors: m u32][coefficients: nEnt T][codes: nEnt u16],
-// each part starting 16-byte aligned (nEnt is a multiple of 32).
+// A chunk's blob: [diagonal: m T][row descriptors: m u32]([storage positions: m u32])[coefficients:
+// nEnt T][codes: nEnt u16], each part starting 16-byte aligned (nEnt is a multiple of 32). The
+// storage positions are there only in an item schedule (several sweeps pipelined, below), whose
+// window slots index items, not the psi positions they write.
 struct BlobLayout
 {
-    unsigned desc, val, code, bytes;
+    unsigned desc, store, val, code, bytes;
 };
 template <class T>
-__host__ __device__ inline BlobLayout blobLayout(int m, int nEnt)
+__host__ __device__ inline BlobLayout blobLayout(int m, int nEnt, int items = 0)
 {
     BlobLayout L;
     L.desc = r16(static_cast<unsigned>(sizeof(T)) * m);
-    L.val = L.desc + r16(4u * m);
+    L.store = L.desc + r16(4u * m);
+    L.val = items ? L.store + r16(4u * m) : L.store;
     L.code = L.val + static_cast<unsigned>(sizeof(T)) * nEnt;
     L.bytes = L.code + r16(2u * nEnt);
     return L;
@@ -118,24 +121,24 @@ __host__ __device__ inline unsigned tableBytes(int G)
     return r16(static_cast<unsigned>(sizeof(T)) * (kWin + kStages * G + 1));
 }
 template <class T>
-__host__ __device__ inline unsigned slotBOffset(int M, int E)
+__host__ __device__ inline unsigned slotBOffset(int M, int E, int items = 0)
 {
-    return blobLayout<T>(M, E).bytes;
+    return blobLayout<T>(M, E, items).bytes;
 }
 template <class T>
-__host__ __device__ inline unsigned slotListOffset(int M, int E)
+__host__ __device__ inline unsigned slotListOffset(int M, int E, int items = 0)
 {
-    return slotBOffset<T>(M, E) + r16(static_cast<unsigned>(sizeof(T)) * (M + 8));
+    return slotBOffset<T>(M, E, items) + r16(static_cast<unsigned>(sizeof(T)) * (M + 8));
 }
 template <class T>
-__host__ __device__ inline unsigned slotBytes(int M, int E, int G)
+__host__ __device__ inline unsigned slotBytes(int M, int E, int G, int items = 0)
 {
-    return slotListOffset<T>(M, E) + r16(4u * (G + 8));
+    return slotListOffset<T>(M, E, items) + r16(4u * (G + 8));
 }
 template <class T>
-__host__ __device__ inline size_t gsSmemBytes(int M, int E, int G)
+__host__ __device__ inline size_t gsSmemBytes(int M, int E, int G, int items = 0)
 {
-    return static_cast<size_t>(tableBytes<T>(G)) + kStages * static_cast<size_t>(slotBytes<T>(M, E, G));
+    return static_cast<size_t>(tableBytes<T>(G)) + kStages * static_cast<size_t>(slotBytes<T>(M, E, G, items));
 }
 
 template <class T>
@@ -160,6 +163,10 @@ struct GsArgs
     unsigned* progress;                      // [P][kProgressStride] (word 0 of each line used)
     int* ticket;                             // the launch's part ticket (zeroed before it), or null:
                                              // part = blockIdx.x
+    int items;                               // 0: one sweep, positions; 1: an item schedule (several
+                                             // sweeps pipelined: "positions" index (sweep, cell)
+                                             // items, b is by item, the window is not filled ahead,
+                                             // and each item writes psi at its blob's storage position)
     long long spinLimit;                     // polls before a wait gives up (kSpinLimit)
     int publish;                             // 1; 0 only to test the bounded waits: no part releases
                                              // its progress, so a part that needs another's values
@@ -403,9 +410,9 @@ __device__ __forceinline__ void gsSweepPart(const GsArgs<T>& a, const int p)
     const int G = a.maxGat;
     const unsigned tableA = smemAddr(smem);
     const unsigned slotsA = tableA + tableBytes<T>(G);
-    const unsigned sb = slotBytes<T>(M, a.maxEnt, G);
-    const unsigned bOff = slotBOffset<T>(M, a.maxEnt);     // b follows the blob in a slot
-    const unsigned lOff = slotListOffset<T>(M, a.maxEnt);  // then the gather sources
+    const unsigned sb = slotBytes<T>(M, a.maxEnt, G, a.items);
+    const unsigned bOff = slotBOffset<T>(M, a.maxEnt, a.items);     // b follows the blob in a slot
+    const unsigned lOff = slotListOffset<T>(M, a.maxEnt, a.items);  // then the gather sources
     const int t = threadIdx.x;
     const int c0 = a.partChunkStart[p];
     const int nCh = a.partChunkStart[p + 1] - c0;
@@ -542,9 +549,11 @@ __device__ __forceinline__ void gsSweepPart(const GsArgs<T>& a, const int p)
                 const Cover cl = coverOf(a.gatSrc, cr.gat0, cr.nGat);
                 mbarExpectTx(&lists[s], cr.nGat ? cl.bytes : 0u);
                 if (cr.nGat) tmaLoad(slotA + lOff, cl.src, cl.bytes, &lists[s]);
-                const BlobLayout bl = blobLayout<T>(cr.m, cr.nEnt);
+                const BlobLayout bl = blobLayout<T>(cr.m, cr.nEnt, a.items);
                 const Cover cbv = coverOf(a.b, cr.pos0, cr.m);
-                const int target = min(fillEnd, ((cr.pos0 + a.ahead + kFill - 1) / kFill) * kFill);
+                // the window ahead of the front holds old psi values; an item schedule's window holds
+                // item results only (its old values are gathered)
+                const int target = a.items ? filled : min(fillEnd, ((cr.pos0 + a.ahead + kFill - 1) / kFill) * kFill);
                 const int nFill = target > filled ? (target - filled) / kFill : 0;
                 mbarExpectTx(&full[s], bl.bytes + cbv.bytes + static_cast<unsigned>(nFill) * kFill * kT);
                 tmaLoad(slotA, a.blob + 16 * static_cast<size_t>(blobOf<T>(cr)), bl.bytes, &full[s]);
@@ -642,7 +651,7 @@ __device__ __forceinline__ void gsSweepPart(const GsArgs<T>& a, const int p)
         if (t < cr.m)
         {
             const unsigned slotA = slotsA + static_cast<unsigned>(s) * sb;
-            const BlobLayout bl = blobLayout<T>(cr.m, cr.nEnt);
+            const BlobLayout bl = blobLayout<T>(cr.m, cr.nEnt, a.items);
             const unsigned lb = (static_cast<unsigned>(cr.pos0) * kT & 15u) / kT;  // lead of b's cover
             const unsigned pe = ldsU32(slotA + bl.desc + 4u * t);
             T acc = ldsT(slotA + bOff + kT * (lb + t), T());
@@ -671,7 +680,7 @@ __device__ __forceinline__ void gsSweepPart(const GsArgs<T>& a, const int p)
             // this window slot is refilled by TMA (the async proxy) one window later; the fence comes
             // before the global store so that it does not wait for that store
             fenceProxyAsyncShared();
-            a.psi[pos] = res;
+            a.psi[a.items ? static_cast<int>(ldsU32(slotA + bl.store + 4u * t)) : pos] = res;
         }
         if (a.trace && t == 0) a.trace[4 * (size_t)(c0 + j) + 3] = clockStamp();
         __syncwarp();
@@ -738,21 +747,24 @@ template <class T>
 __global__ void buildChunkBlobs(int nCh, const int4* __restrict__ recs, const T* __restrict__ posDiag,
                                 const unsigned* __restrict__ posEnt, const unsigned short* __restrict__ code,
                                 const int* __restrict__ entFace, const double* __restrict__ upper,
-                                unsigned char* __restrict__ blob)
+                                unsigned char* __restrict__ blob, const int* __restrict__ itemStore)
 {
     for (int c = blockIdx.x; c < nCh; c += gridDim.x)
     {
         const ChunkRec r = loadChunkRec(recs, c);
-        const BlobLayout L = blobLayout<T>(r.m, r.nEnt);
+        const BlobLayout L = blobLayout<T>(r.m, r.nEnt, itemStore ? 1 : 0);
         unsigned char* b = blob + 16 * static_cast<size_t>(blobOf<T>(r));
         T* dg = reinterpret_cast<T*>(b);
         unsigned* ds = reinterpret_cast<unsigned*>(b + L.desc);
+        unsigned* st = reinterpret_cast<unsigned*>(b + L.store);
         T* vl = reinterpret_cast<T*>(b + L.val);
         unsigned short* cd = reinterpret_cast<unsigned short*>(b + L.code);
         for (int i = threadIdx.x; i < r.m; i += blockDim.x)
         {
-            dg[i] = posDiag[r.pos0 + i];
+            const int p = itemStore ? itemStore[r.pos0 + i] : r.pos0 + i;
+            dg[i] = posDiag[p];
             ds[i] = posEnt[r.pos0 + i];
+            if (itemStore) st[i] = static_cast<unsigned>(p);
         }
         for (int e = threadIdx.x; e < r.nEnt; e += blockDim.x)
         {

@@ -9,32 +9,6 @@
 
 namespace b2g {
 
-// One smoothing call's sweeps of a level in one pipelined launch (pipe_kernels.cuh), for a given
-// sweep count: the combined steps of every (sweep, cell) item, the cells split into `ranks`
-// contiguous ranges held in the shared memory of one CTA each (one cluster when ranks > 1).
-struct PipeSchedule
-{
-    int sweeps = 0;
-    int ranks = 0;
-    int nSteps = 0;
-    int maxLocal = 0;           // shared-memory slots per rank
-    DBuf<int> stepStart;        // [ranks][nSteps + 1] item ranges
-    DBuf<int4> item;            // [sweeps * nCells] {position, local slot, first entry, end entry}
-    DBuf<unsigned> entAddr;     // [2 * nFaces] per position-order row entry: rank << 24 | slot
-    DBuf<int> localPos;         // [ranks][maxLocal] position of each slot
-    DBuf<int> localCount;       // [ranks]
-};
-
-// The choice for one (level, sweep count, value type), by measurement (Matrix::ensurePipe): the
-// pipelined launch with the fastest rank count, or the sweep-by-sweep launches when those are faster.
-struct PipeChoice
-{
-    bool use = false;
-    std::unique_ptr<PipeSchedule> sched;
-    float msPipe = 0.f;   // per smoothing call, the chosen pipelined shape
-    float msSweeps = 0.f; // per smoothing call, sweep by sweep
-};
-
 // The sweep order of one level and its Gauss-Seidel schedule (gs_kernels.cuh). Cells are split into
 // `nParts` contiguous index ranges; each part lists its cells by (depth, cell), depth being the cell's
 // level in the forward DAG (a cell depends on the owners of the faces it is the neighbour of).
@@ -74,7 +48,44 @@ struct GsSchedule
     DBuf<int> gatSrc;          // [nGather] position of each gathered value
     DBuf<unsigned> progress;   // [nParts][kProgressStride] per-part progress words, one L2 line each
                                // (reset before each launch)
+    // an item schedule (items.cu) of `items` sweeps pipelined: "positions" index (sweep, cell) items,
+    // and itemStore[i] is the psi position item i writes
+    int items = 0;
+    DBuf<int> itemStore;
 };
+
+// One smoothing call's sweeps of a level in one pipelined launch (pipe_kernels.cuh), for a given
+// sweep count: the combined steps of every (sweep, cell) item, the cells split into `ranks`
+// contiguous ranges held in the shared memory of one CTA each (one cluster when ranks > 1).
+struct PipeSchedule
+{
+    int sweeps = 0;
+    int ranks = 0;
+    int nSteps = 0;
+    int maxLocal = 0;           // shared-memory slots per rank
+    DBuf<int> stepStart;        // [ranks][nSteps + 1] item ranges
+    DBuf<int4> item;            // [sweeps * nCells] {position, local slot, first entry, end entry}
+    DBuf<unsigned> entAddr;     // [2 * nFaces] per position-order row entry: rank << 24 | slot
+    DBuf<int> localPos;         // [ranks][maxLocal] position of each slot
+    DBuf<int> localCount;       // [ranks]
+};
+
+// The choice for one (level, sweep count, value type), by measurement (Matrix::ensurePipe): the
+// pipelined launch with the fastest rank count, or the sweep-by-sweep launches when those are faster.
+struct PipeChoice
+{
+    int mode = 0;                        // 0 sweep by sweep, 1 the shared-memory launch, 2 items
+    std::unique_ptr<PipeSchedule> sched; // mode 1
+    std::unique_ptr<GsSchedule> items;   // mode 2: the multi-part sweep over (sweep, cell) items
+    float msPipe = 0.f;   // per smoothing call, the best shared-memory shape (0: none fits)
+    float msItems = 0.f;  // per smoothing call, the item schedule (0: not built)
+    float msSweeps = 0.f; // per smoothing call, sweep by sweep
+};
+
+struct LevelAddr;
+// The item schedule of L for S sweeps pipelined in one launch (items.cu), or null when the level has
+// one part or exceeds the schedule's limits.
+std::unique_ptr<GsSchedule> buildGsItems(const LevelAddr& L, int S, cudaStream_t s);
 
 // A colouring of one level for the multicolour sweep of the FP32 V-cycle: no two cells of one colour
 // share a face, so a colour's cells are updated in parallel. Rows are the level's cells colour by

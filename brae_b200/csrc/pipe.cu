@@ -214,11 +214,95 @@ void Matrix::pipeLaunch(int level, const PipeSchedule& P, T* psiL, const T* src)
     ++launches;
 }
 
+// An item schedule's buffers on this matrix, the chunk blobs refilled when the coefficients changed
+// since they were filled (outside any capture).
+template <class T>
+typename VCycleData<T>::ItemBuffers& Matrix::itemBuffers(int level, const GsSchedule& G)
+{
+    VCycleData<T>& D = data<T>();
+    auto& B = D.items[std::make_pair(level, G.items)];
+    if (B.gen != coefGen)
+    {
+        if (capturing) fail(B2G_ERR_STATE, "b2g: an item schedule's blobs were not filled before the capture");
+        const long long bytes = sizeof(T) == 8 ? G.blobBytes64 : G.blobBytes32;
+        B.blob.ensure(static_cast<size_t>(std::max<long long>(bytes, 16)), stream);
+        B.blob.zero(stream);
+        B.b.ensure(static_cast<size_t>(std::max(G.nAlloc, 1)), stream);
+        B.b.zero(stream);
+        if (G.nChunks)
+            k::buildChunkBlobs<T><<<std::min(G.nChunks, 65535), 128, 0, stream>>>(
+                G.nChunks, reinterpret_cast<const int4*>(G.chunkRec.p), D.coef[level].gsDiag.p, G.posEnt.p,
+                G.gsCode.p, G.gsEntFace.p, v64.coef[level].upper.p, B.blob.p, G.itemStore.p);
+        B2G_LAUNCH_CHECK();
+        B.gen = coefGen;
+    }
+    return B;
+}
+
+namespace {
+template <class T>
+__global__ void kByItem(int nItems, const int* __restrict__ itemStore, const T* __restrict__ src, T* __restrict__ out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nItems; i += gridDim.x * blockDim.x)
+        out[i] = src[itemStore[i]];
+}
+}  // namespace
+
+// The item schedule's sweeps in one launch: the source by item, then the multi-part sweep over the
+// items, launched cooperatively (every part resident at once: parts wait for later parts too).
+template <class T>
+void Matrix::itemsLaunch(int level, const GsSchedule& G, T* psiL, const T* src)
+{
+    auto& B = itemBuffers<T>(level, G);
+    const int nItems = G.items * mesh->lev[level].nCells;
+    kByItem<T><<<std::min(ceilDiv(nItems, 256), 4096), 256, 0, stream>>>(nItems, G.itemStore.p, src, B.b.p);
+    B2G_LAUNCH_CHECK();
+    k::GsArgs<T> a;
+    a.nParts = G.nParts;
+    a.maxCells = G.maxCells;
+    a.maxEnt = G.maxEnt;
+    a.maxGat = G.maxGat;
+    a.ahead = 0;
+    a.nPadded = G.nPadded;
+    a.partChunkStart = G.partChunkStart.p;
+    a.partPosStart = G.partPosStart.p;
+    a.chunkRec = reinterpret_cast<const int4*>(G.chunkRec.p);
+    a.upStart = G.upStart.p;
+    a.upList = G.upList.p;
+    a.hasDown = G.hasDown.p;
+    a.blob = B.blob.p;
+    a.gatSrc = G.gatSrc.p;
+    a.b = B.b.p;
+    a.psi = psiL;
+    a.progress = G.progress.p;
+    a.ticket = reinterpret_cast<int*>(G.progress.p + static_cast<size_t>(G.nParts) * k::kProgressStride);
+    a.items = 1;
+    a.spinLimit = spinLimit;
+    a.publish = publish;
+    a.err = err.p;
+    a.trace = nullptr;
+    a.traceDepths = 0;
+    B2G_CUDA(cudaMemsetAsync(G.progress.p, 0, G.progress.bytes(), stream));
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(static_cast<unsigned>(G.nParts));
+    cfg.blockDim = dim3(static_cast<unsigned>(G.maxCells + 128));
+    cfg.dynamicSmemBytes = k::gsSmemBytes<T>(G.maxCells, G.maxEnt, G.maxGat, 1);
+    cfg.stream = stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    B2G_CUDA(cudaLaunchKernelEx(&cfg, k::gsSweep<T>, a));
+    launches += 2;
+}
+
 // The pipelined smoothing call of `level` for nSweeps sweeps, tried once per (level, sweep count,
-// value type) on this matrix's values: every shape whose slots fit (one CTA; clusters of 2, 4, 8, 16
-// CTAs that can be resident) against the sweep-by-sweep launches, the fastest kept. Every shape
-// computes every row from the same operands in the same order, so the choice changes the time only.
-// Outside any capture (it synchronises); the work vectors it sweeps are scratch.
+// value type) on this matrix's values: every shared-memory shape whose slots fit (one CTA; clusters
+// of 2, 4, 8, 16 CTAs that can be resident) and, on a multi-part level, the item schedule, against
+// the sweep-by-sweep launches; the fastest is kept. Every shape computes every row from the same
+// operands in the same order, so the choice changes the time only. Outside any capture (it
+// synchronises); the work vectors it sweeps are scratch.
 template <class T>
 void Matrix::ensurePipe(int level, int nSweeps)
 {
@@ -226,12 +310,8 @@ void Matrix::ensurePipe(int level, int nSweeps)
     const int key = pipeKey(nSweeps, sizeof(T));
     if (L.pipe.count(key)) return;
     PipeChoice& C = L.pipe[key];
-    if (nSweeps < 1 || L.nCells == 0 || L.nCells > k::kPipeMaxRanks * static_cast<int>(kPipeSmemCap / sizeof(T)))
-        return;
+    if (nSweeps < 2 || L.nCells == 0) return;
     allowPipeSmem<T>();
-    const LevelHost H = download(L, stream);
-    int nSteps = 0;
-    const std::vector<int> Tsteps = combinedSteps(H, nSweeps, nSteps);
     DBuf<T> x, b;
     x.alloc(nAlloc(level), stream);
     b.alloc(nAlloc(level), stream);
@@ -258,27 +338,76 @@ void Matrix::ensurePipe(int level, int nSweeps)
     });
     checkDeviceError();
     float best = C.msSweeps;
-    for (int R : {1, 2, 4, 8, 16})
+    if (L.nCells <= k::kPipeMaxRanks * static_cast<int>(kPipeSmemCap / sizeof(T)))
     {
-        std::unique_ptr<PipeSchedule> P = assemble(H, Tsteps, nSweeps, nSteps, R, sizeof(T), stream);
-        if (!P) continue;
-        if (R > 1 && !pipeClusterFits<T>(R, sizeof(T) * static_cast<size_t>(P->maxLocal), stream)) continue;
-        const float ms = timeIt([&] { pipeLaunch<T>(level, *P, x.p, b.p); });
-        if (!C.sched || ms < C.msPipe)
+        const LevelHost H = download(L, stream);
+        int nSteps = 0;
+        const std::vector<int> Tsteps = combinedSteps(H, nSweeps, nSteps);
+        for (int R : {1, 2, 4, 8, 16})
         {
-            C.msPipe = ms;
+            std::unique_ptr<PipeSchedule> P = assemble(H, Tsteps, nSweeps, nSteps, R, sizeof(T), stream);
+            if (!P) continue;
+            if (R > 1 && !pipeClusterFits<T>(R, sizeof(T) * static_cast<size_t>(P->maxLocal), stream)) continue;
+            const float ms = timeIt([&] { pipeLaunch<T>(level, *P, x.p, b.p); });
+            if (C.msPipe == 0.f || ms < C.msPipe) C.msPipe = ms;
             if (ms < best)
             {
                 best = ms;
                 C.sched = std::move(P);
+                C.mode = 1;
             }
         }
     }
-    C.use = C.sched != nullptr;
+    if (L.gs.nParts > 1)
+    {
+        std::unique_ptr<GsSchedule> G = buildGsItems(L, nSweeps, stream);
+        float ms = 0.f;
+        if (G)
+        {
+            try
+            {
+                ms = timeIt([&] { itemsLaunch<T>(level, *G, x.p, b.p); });
+                checkDeviceError();
+            }
+            catch (const Error&)
+            {
+                // a cooperative launch of that many parts refused here: no item schedule for the level
+                cudaGetLastError();
+                G.reset();
+                data<T>().items.erase(std::make_pair(level, nSweeps));
+            }
+        }
+        if (G)
+        {
+            C.msItems = ms;
+            if (ms < best)
+            {
+                best = ms;
+                C.items = std::move(G);
+                C.sched.reset();
+                C.mode = 2;
+            }
+            else
+            {
+                // not kept: this matrix's buffers for it go too
+                data<T>().items.erase(std::make_pair(level, nSweeps));
+            }
+        }
+    }
     launches = l0;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     B2G_CUDA(cudaStreamSynchronize(stream));
+}
+
+// Before a capture: the item blobs of every item-schedule choice, filled for the current
+// coefficients.
+template <class T>
+void Matrix::refreshItems()
+{
+    for (int lv = 0; lv <= nLevels(); ++lv)
+        for (auto& kv : mesh->lev[lv].pipe)
+            if (kv.second.mode == 2 && kv.first % 16 == static_cast<int>(sizeof(T))) itemBuffers<T>(lv, *kv.second.items);
 }
 
 // nSweeps sweeps of `level` in one pipelined launch when the level's tuned choice says so; false
@@ -294,9 +423,19 @@ bool Matrix::pipeSweeps(int level, T* psiL, const T* src, int nSweeps)
         ensurePipe<T>(level, nSweeps);
         it = L.pipe.find(pipeKey(nSweeps, sizeof(T)));
     }
-    if (!g_pipeline || !it->second.use) return false;
-    pipeLaunch<T>(level, *it->second.sched, psiL, src);
-    return true;
+    if (!g_pipeline) return false;
+    const PipeChoice& C = it->second;
+    if (C.mode == 1)
+    {
+        pipeLaunch<T>(level, *C.sched, psiL, src);
+        return true;
+    }
+    if (C.mode == 2)
+    {
+        itemsLaunch<T>(level, *C.items, psiL, src);
+        return true;
+    }
+    return false;
 }
 
 // A pipelined smoothing call on a given number of ranks, whatever the tuned choice (for tests):
@@ -306,6 +445,18 @@ bool Matrix::pipeForced(int level, T* psiL, const T* src, int nSweeps, int ranks
 {
     const LevelAddr& L = mesh->lev[level];
     if (nSweeps < 1 || L.nCells == 0) return false;
+    if (ranks < 0)
+    {
+        // the item schedule, built for this call; its buffers on this matrix are dropped after it
+        std::unique_ptr<GsSchedule> G = buildGsItems(L, nSweeps, stream);
+        if (!G) return false;
+        data<T>().items.erase(std::make_pair(level, nSweeps));
+        itemsLaunch<T>(level, *G, psiL, src);
+        B2G_CUDA(cudaStreamSynchronize(stream));
+        data<T>().items.erase(std::make_pair(level, nSweeps));
+        checkDeviceError();
+        return true;
+    }
     allowPipeSmem<T>();
     const LevelHost H = download(L, stream);
     int nSteps = 0;
@@ -325,5 +476,8 @@ template bool Matrix::pipeSweeps<double>(int, double*, const double*, int);
 template bool Matrix::pipeSweeps<float>(int, float*, const float*, int);
 template void Matrix::pipeLaunch<double>(int, const PipeSchedule&, double*, const double*);
 template void Matrix::pipeLaunch<float>(int, const PipeSchedule&, float*, const float*);
+template void Matrix::refreshItems<double>();
+template void Matrix::refreshItems<float>();
+template void Matrix::itemsLaunch<double>(int, const GsSchedule&, double*, const double*);
 
 }  // namespace b2g

@@ -170,7 +170,7 @@ void fillBlobs(const LevelAddr& L, LevelCoef<T>& C, const double* upper, cudaStr
     if (G.nChunks)
         k::buildChunkBlobs<T><<<std::min(G.nChunks, 65535), 128, 0, s>>>(
             G.nChunks, reinterpret_cast<const int4*>(G.chunkRec.p), C.gsDiag.p, G.posEnt.p, G.gsCode.p,
-            G.gsEntFace.p, upper, C.blob.p);
+            G.gsEntFace.p, upper, C.blob.p, nullptr);
     B2G_LAUNCH_CHECK();
 }
 
@@ -853,6 +853,7 @@ void Matrix::gsLaunch(const LevelAddr& L, const LevelCoef<T>& C, T* psiL, const 
     a.psi = psiL;
     a.progress = G.progress.p;
     a.ticket = reinterpret_cast<int*>(G.progress.p + static_cast<size_t>(G.nParts) * k::kProgressStride);
+    a.items = 0;
     a.spinLimit = spinLimit;
     a.publish = publish;
     a.err = err.p;
@@ -972,6 +973,8 @@ void Matrix::prepareSmoother(const b2g_controls& c)
             want(li + 1, std::min(c.nPostSweeps + c.postSweepsLevelMultiplier * li, c.maxPostSweeps));
             if (c.nPreSweeps) want(li + 1, std::min(c.nPreSweeps + c.preSweepsLevelMultiplier * li, c.maxPreSweeps));
         }
+        if (exact64) refreshItems<double>();
+        else refreshItems<float>();
     }
     // the resident sweep's depth ranges of the small one-part levels, before any iteration is captured
     if (c.smoother != B2G_SMOOTHER_DIC)

@@ -6,6 +6,8 @@
 #include "hierarchy.cuh"
 #include "ldu_kernels.cuh"
 
+#include <map>
+
 namespace b2g {
 
 // Device-resident PCG scalars (one slot each, so a captured iteration needs no host round trip).
@@ -53,6 +55,15 @@ struct VCycleData
     std::vector<DBuf<T>> pairB;
     // the coefficient generation (Matrix::coefGen) each level's reversed and DIC layouts were filled for
     std::vector<long long> revGen, dicGen;
+    // item schedules (items.cu), per (level, sweeps): this matrix's chunk blobs in T, the source by
+    // item, and the coefficient generation the blobs were filled for
+    struct ItemBuffers
+    {
+        DBuf<unsigned char> blob;
+        DBuf<T> b;
+        long long gen = -1;
+    };
+    std::map<std::pair<int, int>, ItemBuffers> items;
     // FP32 form only: dense Cholesky of the coarsest level
     bool built = false;
 };
@@ -163,6 +174,10 @@ struct Matrix
     template <class T> bool pipeSweeps(int level, T* psi, const T* source, int nSweeps);
     template <class T> void pipeLaunch(int level, const PipeSchedule& P, T* psi, const T* source);
     template <class T> bool pipeForced(int level, T* psi, const T* source, int nSweeps, int ranks);
+    // an item schedule's launch (items.cu): its blobs filled for the current coefficients first
+    template <class T> typename VCycleData<T>::ItemBuffers& itemBuffers(int level, const GsSchedule& G);
+    template <class T> void itemsLaunch(int level, const GsSchedule& G, T* psi, const T* source);
+    template <class T> void refreshItems();
     void mcLaunch(int level, bool fused, int cluster, int block, float* psi, const float* source, int nSweeps,
                   bool timed, bool symmetric = false);
     void tuneMulticolour(int level);

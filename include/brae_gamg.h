@@ -369,17 +369,20 @@ B2G_API b2g_status b2g_set_sweep_pipeline(int on);
 B2G_API b2g_status b2g_level_smooth_stall(b2g_matrix* m, int level, double* psi, const double* source,
                                           long long spinLimit, int* nParts);
 /* nSweeps exact Gauss-Seidel sweeps of `level` (device pointers, natural cell order) in ONE
- * pipelined launch on `ranks` CTAs (1, 2, 4, 8 or 16; a thread-block cluster when above 1), whatever
- * shape the level's tuned choice would take: sweep s+1 runs on a cell once every value its row reads
- * is final, which gives bit for bit the result of nSweeps sequential sweeps (gaussSeidelSweeps,
+ * pipelined launch on `ranks` CTAs holding psi in shared memory (1, 2, 4, 8 or 16; a thread-block
+ * cluster when above 1), or with ranks = -1 as the level's multi-part sweep over (sweep, cell) items,
+ * whatever form the level's tuned choice would take: sweep s+1 runs on a cell once every value its row
+ * reads is final, which gives bit for bit the result of nSweeps sequential sweeps (gaussSeidelSweeps,
  * smooth_solver_cpp.cu:87-166, called nSweeps times). B2G_ERR_ARGUMENT when the level's cells do not
- * fit that many CTAs' shared memory or such a cluster cannot be resident. For tests and tuning. */
+ * fit that many CTAs' shared memory, such a cluster cannot be resident, or (ranks -1) the level has
+ * one part or nSweeps is 1. For tests and tuning. */
 B2G_API b2g_status b2g_level_smooth_pipelined(b2g_matrix* m, int level, double* psi, const double* source,
                                               int nSweeps, int ranks);
 /* The tuned choice for smoothing calls of nSweeps sweeps on `level` in values of `valueBytes` (8 FP64,
- * 4 FP32): *ranks the pipelined launch's CTAs (0: sweep by sweep, or not tuned yet), *nSteps its
- * combined steps, and the measured milliseconds per call of the best pipelined shape and of the
- * sweep-by-sweep launches. Any output may be NULL. */
+ * 4 FP32): *ranks the pipelined launch's CTAs holding psi in shared memory, or minus the part count of
+ * the pipelined multi-part sweep over (sweep, cell) items (0: sweep by sweep, or not tuned yet),
+ * *nSteps its combined steps, and the measured milliseconds per call of the chosen pipelined form
+ * (else the best shared-memory shape) and of the sweep-by-sweep launches. Any output may be NULL. */
 B2G_API b2g_status b2g_level_pipe_shape(const b2g_mesh* mesh, int level, int nSweeps, int valueBytes, int* ranks,
                                         int* nSteps, float* msPipe, float* msSweeps);
 B2G_API b2g_status b2g_level_smooth_trace(b2g_matrix* m, int level, double* psi, const double* source,

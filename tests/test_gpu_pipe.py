@@ -59,7 +59,7 @@ def test_forced_shapes_bitexact(b2g, oracle, name, kw):
         b = rng.uniform(-1.0, 1.0, n)
         for sweeps in (1, 2, 4):
             want = oracle.smooth(lo, up, d, u, x0, b, sweeps)
-            for ranks in (1, 2, 4, 8, 16):
+            for ranks in (1, 2, 4, 8, 16, -1):
                 x = dev(x0)
                 try:
                     A.smooth_pipelined(lv, x, dev(b), sweeps, ranks)
@@ -120,3 +120,27 @@ def test_solve_same_with_and_without_pipeline(b2g, oracle, smoother, precision):
     timed = [mesh.pipe_shape(lv, s, 8 if precision == "fp64" else 4)["ms_pipelined"]
              for lv in range(mesh.n_levels) for s in (2, 3, 4)]
     assert any(t > 0 for t in timed)
+
+
+def test_item_schedule_many_parts(b2g, oracle):
+    # the multi-part sweep over (sweep, cell) items on levels cut into many parts, which wait for
+    # parts after them as well as before: bit for bit the oracle's sequential sweeps
+    c = cases.box_case(64, 64, 64, (2.0, 1.0, 1.0), 20.0)
+    mesh = b2g.Mesh(c.lower, c.upper, c.Sf, c.magSf, c.n_cells, 10, True)
+    A = b2g.Matrix(mesh, dev(c.diag), dev(c.coef))
+    rng = np.random.default_rng(11)
+    ran = 0
+    for lv in (0, 1, 2):
+        lo, up, d, u = _level_system(mesh, A, c, lv)
+        x0 = rng.uniform(-1.0, 1.0, d.shape[0])
+        b = rng.uniform(-1.0, 1.0, d.shape[0])
+        for sweeps in (2, 4):
+            x = dev(x0)
+            try:
+                A.smooth_pipelined(lv, x, dev(b), sweeps, -1)
+            except b2g.GamgError as e:
+                assert e.status == "ARGUMENT"
+                continue
+            assert np.array_equal(x.cpu().numpy(), oracle.smooth(lo, up, d, u, x0, b, sweeps)), (lv, sweeps)
+            ran += 1
+    assert ran >= 4
