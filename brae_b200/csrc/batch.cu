@@ -957,6 +957,8 @@ Batch::Batch(std::vector<Matrix*> cs, cudaStream_t s) : stream(s), cases(std::mo
     // the batched sweep's shared-memory ceiling (this translation unit's instances)
     B2G_CUDA(cudaFuncSetAttribute(k::gsSweepBatch<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024));
     B2G_CUDA(cudaFuncSetAttribute(k::gsSweepBatch<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024));
+    B2G_CUDA(cudaFuncSetAttribute(k::coarseDenseSolveBatch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(sizeof(double)) * k::kDenseMax * k::kDenseMax));
     partial.alloc(2 * static_cast<size_t>(maxTiles), stream);
     partial32.alloc(2 * static_cast<size_t>(maxTiles), stream);
     sf64.alloc(K, stream);
@@ -965,6 +967,30 @@ Batch::Batch(std::vector<Matrix*> cs, cudaStream_t s) : stream(s), cases(std::mo
     active.zero(stream);
     nActive.alloc(1, stream);
     perf.alloc(K, stream);
+    B2G_CUDA(cudaStreamSynchronize(stream));
+}
+
+// Each case's dense coarsest factor for its current coefficients, and the batched solve's table (the
+// FP32 coarsest vectors of every case); denseAll only when every case has its factor.
+void Batch::prepareDense()
+{
+    const int K = static_cast<int>(cases.size());
+    std::vector<k::DenseCase> h(K);
+    bool all = true;
+    for (int c = 0; c < K; ++c)
+    {
+        Matrix& A = *cases[c];
+        A.ensureDense();
+        const int lv = A.nLevels();
+        all = all && A.denseUse && lv > 0;
+        if (!all) break;
+        h[c].n = A.n(lv);
+        h[c].L = A.denseL.p;
+        h[c].b = A.v32.src[lv - 1].p;
+        h[c].x = A.v32.corr[lv - 1].p;
+    }
+    denseAll = all;
+    if (all) denseCases.upload(h.data(), h.size(), stream);
     B2G_CUDA(cudaStreamSynchronize(stream));
 }
 
@@ -1180,6 +1206,12 @@ void Batch::vcycle(const b2g_controls& c, int fresRole)
         k::coarsestPcgDicBatch<<<K, 32, 0, stream>>>(coarsestArgs.p, c.precTolerance, c.precRelTol, act);
         launches += 2;
     }
+    else if (denseNow)
+    {
+        // the FP32 forms' direct coarsest solve: every case's dense Cholesky factor, one warp each
+        k::coarseDenseSolveBatch<<<K, 32, sizeof(double) * k::kDenseMax * k::kDenseMax, stream>>>(denseCases.p, act);
+        ++launches;
+    }
     else
     {
         bCast<double, float><<<B2G_TILES(coarsestTiles)>>>(coarsestTiles.tiles.p, segD.p, segF.p, V_SRC, V_SRC, act);
@@ -1335,6 +1367,12 @@ void Batch::solve(const b2g_controls& c, const double* const* source, double* co
         fail(B2G_ERR_ARGUMENT, "b2g batch: unknown precision form");
     multicolour = c.precision == B2G_PRECISION_FP32_PRECOND_MULTICOLOUR;
     if (multicolour) prepareMulticolour();
+    denseNow = false;
+    if (c.precision != B2G_PRECISION_FP64 && c.coarsestDirect)
+    {
+        prepareDense();
+        denseNow = denseAll;
+    }
     const int K = static_cast<int>(cases.size());
     serial = c.reduction == B2G_REDUCTION_SERIAL;
     launches = 0;
@@ -1386,7 +1424,7 @@ void Batch::solve(const b2g_controls& c, const double* const* source, double* co
         // one captured graph per controls and reduction order
         std::vector<unsigned char> key(sizeof(b2g_controls) + 1);
         std::memcpy(key.data(), &c, sizeof(b2g_controls));
-        key[sizeof(b2g_controls)] = serial ? 1 : 0;
+        key[sizeof(b2g_controls)] = static_cast<unsigned char>((serial ? 1 : 0) | (denseNow ? 2 : 0));
         if (eagerIterations == 0 && (!graph.exec || graph.key != key))
         {
             // a batch's first iteration runs as plain launches: capturing pays off only from the

@@ -116,6 +116,9 @@ struct Batch
     std::vector<BatchLevel> lev;
     TileList coarsestTiles;                 // each case's cells on its coarsest level
     DBuf<k::CoarsestArgs<double>> coarsestArgs;  // [K] FP64 coarsest solve on (V_CORR, V_SRC)
+    DBuf<k::DenseCase> denseCases;          // [K] the FP32 forms' direct coarsest solves (coarsestDirect)
+    bool denseAll = false;                  // every case has its dense factor for the current values
+    void prepareDense();
     DBuf<int> active;                       // [K]
     DBuf<int> nActive;                      // [1]
     DBuf<int> err;
@@ -127,6 +130,7 @@ struct Batch
     std::vector<SegLevel<float>> hostF;    // host copy of segF
     bool mcReady = false;                   // the multicolour layouts are prepared
     bool multicolour = false;               // the current solve sweeps the FP32 V-cycle colour by colour
+    bool denseNow = false;                  // the current solve takes the dense coarsest factors
     int eagerIterations = 0;                // iterations run without a graph (the first one)
     bool serial = false;
     long long launches = 0;

@@ -503,7 +503,7 @@ b2g_status b2g_controls_default(b2g_controls* out)
 {
     return guarded([&] {
         need(out != nullptr, "b2g_controls_default: null output");
-        b2g_controls c;
+        b2g_controls c{};
         c.solver = B2G_SOLVER_PCG_GAMG;
         c.tolerance = 1e-6;
         c.relTol = 0.0;
@@ -524,6 +524,7 @@ b2g_status b2g_controls_default(b2g_controls* out)
         c.nVcycles = 2;
         c.precision = B2G_PRECISION_FP64;
         c.reduction = B2G_REDUCTION_TREE;
+        c.coarsestDirect = 1;
         *out = c;
     });
 }
@@ -532,7 +533,7 @@ b2g_status b2g_controls_read(const char* text, b2g_controls* out)
 {
     return guarded([&] {
         need(text != nullptr && out != nullptr, "b2g_controls_read: null argument");
-        b2g_controls c;
+        b2g_controls c{};
         b2g_controls_default(&c);
         Dict d;
         const std::vector<std::string> tok = tokenize(text);
@@ -831,6 +832,27 @@ b2g_status b2g_level_smooth_pipelined(b2g_matrix* m, int level, double* psi, con
                                                     "(one part, or one sweep)"
                                                   : "b2g_level_smooth_pipelined: the level does not fit that many CTAs");
         A.fromPos(level, static_cast<const double*>(A.ioBuf(0)), psi);
+        B2G_CUDA(cudaStreamSynchronize(A.stream));
+    });
+}
+
+b2g_status b2g_coarsest_dense_solve(b2g_matrix* m, double* psi, const double* source)
+{
+    return guarded([&] {
+        need(m && psi && source, "b2g_coarsest_dense_solve: null argument");
+        b2g::Matrix& A = *m->mat;
+        const int lv = A.nLevels();
+        need(lv > 0, "b2g_coarsest_dense_solve: the mesh has no coarse levels");
+        A.ensureDense();
+        if (!A.denseUse)
+            b2g::fail(B2G_ERR_ARGUMENT, "b2g_coarsest_dense_solve: the coarsest level has no dense factor (more than "
+                                        "96 cells, or not positive definite)");
+        const int n = A.n(lv);
+        A.toPos(lv, source, A.ioBuf(1));
+        b2g::k::coarseDenseSolve<double><<<1, 32, sizeof(double) * n * n, A.stream>>>(n, A.denseL.p, A.ioBuf(1),
+                                                                                       A.ioBuf(0));
+        B2G_LAUNCH_CHECK();
+        A.fromPos(lv, static_cast<const double*>(A.ioBuf(0)), psi);
         B2G_CUDA(cudaStreamSynchronize(A.stream));
     });
 }

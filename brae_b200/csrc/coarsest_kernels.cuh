@@ -248,5 +248,170 @@ static __global__ void __launch_bounds__(32) coarsestPcgDicBatch(const CoarsestA
     coarsestPcgDicWarp<double>(a);
 }
 
+// ---------------------------------------------------------------------------------------------
+// The coarsest level solved directly, for the FP32-preconditioned forms: a dense FP64 Cholesky
+// factor A = L L^T, made once per coarse matrix and applied by two triangular substitutions in
+// every V-cycle (the reference's precision/serving form solves its coarsest level directly too,
+// device_amg_coarse.cu:545-700; the FP64 parity form keeps the reference's PCG-DIC). The level is
+// numbered by position, as its vectors are. The factor is taken only when every pivot is above
+// kDensePivotMin * max|diag| (a singular, all-Neumann level is left to PCG-DIC).
+// ---------------------------------------------------------------------------------------------
+
+constexpr int kDenseMax = 96;              // the largest coarsest level factored densely
+constexpr int kDenseRows = kDenseMax / 32; // rows a lane holds in the substitutions
+constexpr double kDensePivotMin = 1e-10;
+
+struct DenseArgs
+{
+    int n, nF;
+    const int* __restrict__ lower;   // by face, cell ids
+    const int* __restrict__ upper;
+    const int* __restrict__ posOf;   // cell -> position
+    const double* __restrict__ diag; // by position
+    const double* __restrict__ coef; // by face
+    double* L;                       // [n * n] column-major: L(i, k) at k * n + i (lower triangle)
+    int* ok;                         // 1: L holds the factor; 0: a pivot was too small
+};
+
+// One warp: A into shared memory (column-major, both triangles), then right-looking Cholesky one
+// column at a time -- the pivot's square root, the column divided by it, the trailing lower
+// triangle updated by the column's outer product. Each entry is updated in increasing k, so the
+// factor does not depend on how lanes share the work. Shared memory: n * n doubles.
+static __global__ void __launch_bounds__(32) coarseDenseFactor(DenseArgs a)
+{
+    extern __shared__ double denseSh[];
+    const int n = a.n;
+    const int lane = threadIdx.x;
+    for (int i = lane; i < n * n; i += 32) denseSh[i] = 0.0;
+    __syncwarp();
+    double dmax = 0.0;
+    for (int c = lane; c < n; c += 32)
+    {
+        const double d = a.diag[c];
+        denseSh[c * n + c] = d;
+        dmax = fmax(dmax, fabs(d));
+    }
+    for (int f = lane; f < a.nF; f += 32)
+    {
+        const int pl = a.posOf[a.lower[f]], pu = a.posOf[a.upper[f]];
+        denseSh[pl * n + pu] = a.coef[f];
+        denseSh[pu * n + pl] = a.coef[f];
+    }
+    for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+    __syncwarp();
+    int ok = 1;
+    for (int k = 0; k < n && ok; ++k)
+    {
+        const double d = denseSh[k * n + k];
+        if (!(d > kDensePivotMin * dmax))
+        {
+            ok = 0;
+            break;
+        }
+        const double lkk = sqrt(d);
+        __syncwarp();
+        for (int i = k + 1 + lane; i < n; i += 32) denseSh[k * n + i] = divRn(denseSh[k * n + i], lkk);
+        if (lane == 0) denseSh[k * n + k] = lkk;
+        __syncwarp();
+        const int m = n - k - 1;
+        for (int idx = lane; idx < m * m; idx += 32)
+        {
+            const int jj = idx / m, ii = idx % m;
+            if (ii < jj) continue;
+            const int i = k + 1 + ii, j = k + 1 + jj;
+            denseSh[j * n + i] = subRn(denseSh[j * n + i], mulRn(denseSh[k * n + i], denseSh[k * n + j]));
+        }
+        __syncwarp();
+    }
+    for (int i = lane; i < n * n; i += 32) a.L[i] = denseSh[i];
+    if (lane == 0) *a.ok = ok;
+}
+
+// x = L^-T L^-1 b by one warp: row i in lane i % 32, slot i / 32 (registers); the factor in shared
+// memory. Forward: y_k /= L(k,k), then y_i -= L(i,k) y_k below it; backward with L^T the same
+// upwards. b and x by position, in T (widened to FP64 and narrowed back).
+template <class T>
+__device__ __forceinline__ void denseSolveWarp(int n, const double* __restrict__ L, const T* __restrict__ b,
+                                               T* __restrict__ x, double* sh)
+{
+    const int lane = threadIdx.x;
+    for (int i = lane; i < n * n; i += 32) sh[i] = L[i];
+    double y[kDenseRows];
+#pragma unroll
+    for (int s = 0; s < kDenseRows; ++s)
+    {
+        const int i = lane + 32 * s;
+        y[s] = i < n ? static_cast<double>(b[i]) : 0.0;
+    }
+    __syncwarp();
+    for (int k = 0; k < n; ++k)
+    {
+        const int ks = k >> 5;
+#pragma unroll
+        for (int s = 0; s < kDenseRows; ++s)
+            if (s == ks && (k & 31) == lane) y[s] = divRn(y[s], sh[k * n + k]);
+        double v = 0.0;
+#pragma unroll
+        for (int s = 0; s < kDenseRows; ++s)
+            if (s == ks) v = y[s];
+        const double yk = __shfl_sync(0xffffffffu, v, k & 31);
+#pragma unroll
+        for (int s = 0; s < kDenseRows; ++s)
+        {
+            const int i = lane + 32 * s;
+            if (i > k && i < n) y[s] = subRn(y[s], mulRn(sh[k * n + i], yk));
+        }
+    }
+    for (int k = n - 1; k >= 0; --k)
+    {
+        const int ks = k >> 5;
+#pragma unroll
+        for (int s = 0; s < kDenseRows; ++s)
+            if (s == ks && (k & 31) == lane) y[s] = divRn(y[s], sh[k * n + k]);
+        double v = 0.0;
+#pragma unroll
+        for (int s = 0; s < kDenseRows; ++s)
+            if (s == ks) v = y[s];
+        const double yk = __shfl_sync(0xffffffffu, v, k & 31);
+#pragma unroll
+        for (int s = 0; s < kDenseRows; ++s)
+        {
+            const int i = lane + 32 * s;
+            if (i < k) y[s] = subRn(y[s], mulRn(sh[i * n + k], yk));
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < kDenseRows; ++s)
+    {
+        const int i = lane + 32 * s;
+        if (i < n) x[i] = static_cast<T>(y[s]);
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(32) coarseDenseSolve(int n, const double* __restrict__ L, const T* __restrict__ b,
+                                                       T* __restrict__ x)
+{
+    extern __shared__ double denseSh[];
+    denseSolveWarp<T>(n, L, b, x, denseSh);
+}
+
+// Many cases' coarsest levels, one warp each (block i: case i), skipped where `active` is 0.
+struct DenseCase
+{
+    int n;
+    const double* L;
+    const float* b;
+    float* x;
+};
+static __global__ void __launch_bounds__(32) coarseDenseSolveBatch(const DenseCase* __restrict__ cases,
+                                                                  const int* __restrict__ active)
+{
+    extern __shared__ double denseSh[];
+    if (active && active[blockIdx.x] == 0) return;
+    const DenseCase c = cases[blockIdx.x];
+    denseSolveWarp<float>(c.n, c.L, c.b, c.x, denseSh);
+}
+
 }  // namespace k
 }  // namespace b2g

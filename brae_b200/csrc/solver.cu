@@ -488,6 +488,9 @@ void allowSweepSmem(int device)
     B2G_CUDA(cudaFuncSetAttribute(k::gsSweep<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024));
     B2G_CUDA(cudaFuncSetAttribute(k::gsResident<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(kResidentSmem)));
+    constexpr int denseSmem = static_cast<int>(sizeof(double)) * k::kDenseMax * k::kDenseMax;
+    B2G_CUDA(cudaFuncSetAttribute(k::coarseDenseSolve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, denseSmem));
+    B2G_CUDA(cudaFuncSetAttribute(k::coarseDenseFactor, cudaFuncAttributeMaxDynamicSharedMemorySize, denseSmem));
     d.fetch_or(bit);
 }
 
@@ -1409,11 +1412,50 @@ void Matrix::coarsestSolve<double>(int level, double* x, const double* src, doub
 
 // The FP32 V-cycle solves its coarsest level in FP64 (the level has 10-20 cells; its precision is
 // free): the FP32 source is widened, solved by the same PCG-DIC, and narrowed back.
+// The coarsest level's dense Cholesky factor for the current coefficients (one warp on the device);
+// the factor is used when every pivot was large enough.
+void Matrix::ensureDense()
+{
+    if (denseGen == coefGen) return;
+    buildCoarse();
+    denseUse = false;
+    denseGen = coefGen;
+    const int lv = nLevels();
+    const LevelAddr& L = mesh->lev[lv];
+    const int n = L.nCells;
+    if (n == 0 || n > k::kDenseMax) return;
+    denseL.ensure(static_cast<size_t>(n) * n, stream);
+    denseOk.ensure(1, stream);
+    k::DenseArgs a;
+    a.n = n;
+    a.nF = L.nFaces;
+    a.lower = L.lower.p;
+    a.upper = L.upper.p;
+    a.posOf = L.gs.posOf.p;
+    a.diag = v64.coef[lv].gsDiag.p;
+    a.coef = v64.coef[lv].upper.p;
+    a.L = denseL.p;
+    a.ok = denseOk.p;
+    k::coarseDenseFactor<<<1, 32, sizeof(double) * n * n, stream>>>(a);
+    B2G_LAUNCH_CHECK();
+    int ok = 0;
+    B2G_CUDA(cudaMemcpyAsync(&ok, denseOk.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    B2G_CUDA(cudaStreamSynchronize(stream));
+    denseUse = ok != 0;
+}
+
 template <>
 void Matrix::coarsestSolve<float>(int level, float* x, const float* src, float tol, float relTol,
                                   k::DevPerf* out, bool logIt)
 {
     const int n = mesh->lev[level].nCells;
+    if (denseNow && denseUse && denseGen == coefGen)
+    {
+        k::coarseDenseSolve<float><<<1, 32, sizeof(double) * n * n, stream>>>(n, denseL.p, src, x);
+        B2G_LAUNCH_CHECK();
+        ++launches;
+        return;
+    }
     double* x64 = v64.corr[level - 1].p;
     double* s64 = v64.src[level - 1].p;
     castInto<double, float>(n, src, s64, stream);
@@ -1535,6 +1577,8 @@ void Matrix::precondition(const b2g_controls& c, double* w, const double* r)
     {
         if (multicolour) ensureMulticolour();
         ensureFp32();
+        denseNow = c.coarsestDirect != 0;
+        if (denseNow && !capturing) ensureDense();
         castInto<float, double>(n0, r, r32.p, stream);
         zeroArray<float>(n0, w32.p, stream);
         const float* frp = r32.p;
@@ -1722,6 +1766,7 @@ b2g_perf Matrix::pcg(const b2g_controls& c, b2g_solve_log* log)
     buildCoarse();
     const bool flexible = c.precision != B2G_PRECISION_FP64;
     if (flexible) ensureFp32();
+    if (flexible && c.coarsestDirect) ensureDense();
     if (c.precision == B2G_PRECISION_FP32_PRECOND_MULTICOLOUR) ensureMulticolour();
     prepareSmoother(c);
     kPcgStart<<<1, 1, 0, stream>>>(scal.p);

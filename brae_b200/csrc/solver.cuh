@@ -178,6 +178,14 @@ struct Matrix
     template <class T> typename VCycleData<T>::ItemBuffers& itemBuffers(int level, const GsSchedule& G);
     template <class T> void itemsLaunch(int level, const GsSchedule& G, T* psi, const T* source);
     template <class T> void refreshItems();
+    // the coarsest level's dense Cholesky factor (FP32-preconditioned forms, coarsestDirect), made for
+    // the current coefficients by ensureDense outside any capture
+    DBuf<double> denseL;
+    DBuf<int> denseOk;
+    long long denseGen = -1;
+    bool denseUse = false;   // the factor exists (positive definite, at most kDenseMax cells)
+    bool denseNow = false;   // the current solve takes it
+    void ensureDense();
     void mcLaunch(int level, bool fused, int cluster, int block, float* psi, const float* source, int nSweeps,
                   bool timed, bool symmetric = false);
     void tuneMulticolour(int level);

@@ -40,7 +40,7 @@ class Controls(C.Structure):
                 ("postSweepsLevelMultiplier", C.c_int), ("maxPostSweeps", C.c_int),
                 ("nFinestSweeps", C.c_int), ("scaleCorrection", C.c_int),
                 ("nCellsInCoarsestLevel", C.c_int), ("nVcycles", C.c_int), ("precision", C.c_int),
-                ("reduction", C.c_int)]
+                ("reduction", C.c_int), ("coarsestDirect", C.c_int)]
 
 
 class _Perf(C.Structure):
@@ -71,6 +71,7 @@ def _load():
         "b2g_version": (C.c_char_p, []),
         "b2g_set_profiling": (ip, [ip]),
         "b2g_set_sweep_pipeline": (ip, [ip]),
+        "b2g_coarsest_dense_solve": (ip, [vp, vp, vp]),
         "b2g_level_smooth_pipelined": (ip, [vp, ip, vp, vp, ip, ip]),
         "b2g_level_pipe_shape": (ip, [vp, ip, ip, ip, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float),
                                       C.POINTER(C.c_float)]),
@@ -151,7 +152,7 @@ EXPORTED = [
     "b2g_batch_launches", "b2g_batch_destroy", "b2g_mesh_set_pair", "b2g_mesh_level_pair",
     "b2g_gamg_solve_coupled", "b2g_matrix_create_coupled", "b2g_matrix_level_pair_coeffs", "b2g_matrix_gamg_solve",
     "b2g_matrix_set_coeffs", "b2g_matrix_level_timings", "b2g_level_smooth_stall", "b2g_set_sweep_pipeline",
-    "b2g_level_smooth_pipelined", "b2g_level_pipe_shape",
+    "b2g_level_smooth_pipelined", "b2g_level_pipe_shape", "b2g_coarsest_dense_solve",
 ]
 
 
@@ -421,6 +422,10 @@ class Matrix:
     def smooth_pipelined(self, level, psi, source, n_sweeps, ranks):
         """n_sweeps sweeps in one pipelined launch on `ranks` CTAs (b2g_level_smooth_pipelined)."""
         _check(lib.b2g_level_smooth_pipelined(self.handle, level, _ptr(psi), _ptr(source), n_sweeps, ranks))
+
+    def coarsest_dense_solve(self, psi, source):
+        """psi = A^-1 source on the coarsest level by its dense Cholesky factor."""
+        _check(lib.b2g_coarsest_dense_solve(self.handle, _ptr(psi), _ptr(source)))
 
     def smooth_stall(self, level, psi, source, spin_limit):
         """One sweep in which no part publishes its progress, waits limited to `spin_limit` polls

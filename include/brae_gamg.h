@@ -123,6 +123,11 @@ typedef struct
     int nVcycles;                /* 2 (GAMGPreconditioner.C:60) */
     int precision;               /* B2G_PRECISION_FP64 */
     int reduction;               /* B2G_REDUCTION_TREE */
+    /* 1: the FP32-preconditioned forms solve the coarsest level directly, by a dense FP64 Cholesky
+     * factor made once per coarse matrix (up to 96 cells; a level that is not positive definite
+     * keeps PCG-DIC), as the reference's precision form does; 0: PCG-DIC to precTolerance /
+     * precRelTol. The FP64 form always runs the reference's PCG-DIC. No fvSolution key. */
+    int coarsestDirect;          /* 1 */
 } b2g_controls;
 
 /* SolverPerformance (PCGH:16-21) */
@@ -378,6 +383,11 @@ B2G_API b2g_status b2g_level_smooth_stall(b2g_matrix* m, int level, double* psi,
  * one part or nSweeps is 1. For tests and tuning. */
 B2G_API b2g_status b2g_level_smooth_pipelined(b2g_matrix* m, int level, double* psi, const double* source,
                                               int nSweeps, int ranks);
+/* psi = A^-1 source on the coarsest level by its dense Cholesky factor (device pointers, natural
+ * cell order): the direct coarsest solve the FP32-preconditioned forms take (coarsestDirect).
+ * B2G_ERR_ARGUMENT when the level has more than 96 cells or is not positive definite. The factor of
+ * the matrix's current coefficients is made on first use. For tests. */
+B2G_API b2g_status b2g_coarsest_dense_solve(b2g_matrix* m, double* psi, const double* source);
 /* The tuned choice for smoothing calls of nSweeps sweeps on `level` in values of `valueBytes` (8 FP64,
  * 4 FP32): *ranks the pipelined launch's CTAs holding psi in shared memory, or minus the part count of
  * the pipelined multi-part sweep over (sweep, cell) items (0: sweep by sweep, or not tuned yet),
