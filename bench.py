@@ -313,6 +313,12 @@ def run_ours(args, world, rank, local):
     ms4, cnt4 = A.timings()
     levels, tot = level_table(mesh, A.level_timings(0), A.level_timings(1))
     b2g.set_profiling(False)
+    for row in levels:
+        # the sweep tuner's choice for the level's smoothing calls: ranks > 0 the shared-memory pipelined
+        # launch on that many CTAs, < 0 the pipelined multi-part sweep over items (minus its parts),
+        # 0 sweep by sweep
+        if row.get("smooth_calls"):
+            row["sweep_shape"] = mesh.pipe_shape(row["level"], row["sweeps"] // row["smooth_calls"], 8)
 
     # end to end: the reference-facing call with pinned host buffers, copies inside the timed region
     pin = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).pin_memory()

@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libbrae_gamg.so")
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
-SOURCES = ["hierarchy.cu", "solver.cu", "capi.cu", "server.cu", "batch.cu", "pair.cu", "pipe.cu", "items.cu"]
+SOURCES = ["hierarchy.cu", "solver.cu", "capi.cu", "server.cu", "batch.cu", "pair.cu", "pipe.cu", "items.cu", "assemble.cu"]
 FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
          "--fmad=false", "-Xcompiler", "-fPIC,-fvisibility=hidden,-ffp-contract=off", "-Xptxas", "-O3"]
 

@@ -60,7 +60,8 @@ struct PipeRow
     int e0;
     T b, d;
     T v[kPipeK];
-    unsigned a[kPipeK];  // shared (R = 1) or shared::cluster address of each entry's value
+    unsigned ea[kPipeK];  // each entry's value: owner rank << 24 | slot (turned into an address at use,
+                          // so that loading the next step's row never waits for its loads)
 };
 
 __device__ __forceinline__ unsigned pipeSmemAddr(const void* p)
@@ -112,14 +113,17 @@ __device__ __forceinline__ void pipeBarrier()
     }
 }
 
-// the value address of an entry: its owner rank's slot
-__device__ __forceinline__ unsigned pipeAddr(unsigned ea, const unsigned* rbase, unsigned tsize)
+// the value address of an entry: its owner rank's slot, in the rank's shared memory (the same
+// offset in every CTA of the launch)
+template <class T, bool kCluster>
+__device__ __forceinline__ unsigned pipeAddr(unsigned ea, unsigned xa)
 {
-    return rbase[ea >> 24] + tsize * (ea & 0xffffffu);
+    const unsigned local = xa + static_cast<unsigned>(sizeof(T)) * (ea & 0xffffffu);
+    return kCluster ? mapaCluster(local, ea >> 24) : local;
 }
 
 template <class T>
-__device__ __forceinline__ void pipeLoad(const PipeArgs<T>& a, int k, const unsigned* rbase, PipeRow<T>& r)
+__device__ __forceinline__ void pipeLoad(const PipeArgs<T>& a, int k, PipeRow<T>& r)
 {
     r.slot = -1;
     r.w = 0;
@@ -135,22 +139,25 @@ __device__ __forceinline__ void pipeLoad(const PipeArgs<T>& a, int k, const unsi
         if (q < r.w)
         {
             r.v[q] = a.A.val[it.z + q];
-            r.a[q] = pipeAddr(a.entAddr[it.z + q], rbase, sizeof(T));
+            r.ea[q] = a.entAddr[it.z + q];
         }
 }
 
 // the row in the reference's order: the source minus each entry's coefficient times its value, then
 // the division by the diagonal
 template <class T, bool kCluster>
-__device__ __forceinline__ void pipeRow(const PipeArgs<T>& a, const PipeRow<T>& r, const unsigned* rbase, unsigned xa)
+__device__ __forceinline__ void pipeRow(const PipeArgs<T>& a, const PipeRow<T>& r, unsigned xa)
 {
+    T x[kPipeK];
+#pragma unroll
+    for (int q = 0; q < kPipeK; ++q)
+        if (q < r.w) x[q] = pipeLd<kCluster>(pipeAddr<T, kCluster>(r.ea[q], xa), T());
     T acc = r.b;
 #pragma unroll
     for (int q = 0; q < kPipeK; ++q)
-        if (q < r.w) acc = subRn(acc, mulRn(r.v[q], pipeLd<kCluster>(r.a[q], T())));
+        if (q < r.w) acc = subRn(acc, mulRn(r.v[q], x[q]));
     for (int q = kPipeK; q < r.w; ++q)
-        acc = subRn(acc, mulRn(a.A.val[r.e0 + q],
-                               pipeLd<kCluster>(pipeAddr(a.entAddr[r.e0 + q], rbase, sizeof(T)), T())));
+        acc = subRn(acc, mulRn(a.A.val[r.e0 + q], pipeLd<kCluster>(pipeAddr<T, kCluster>(a.entAddr[r.e0 + q], xa), T())));
     pipeSt(xa + static_cast<unsigned>(sizeof(T)) * static_cast<unsigned>(r.slot), divRn(acc, r.d));
 }
 
@@ -160,7 +167,6 @@ template <class T, bool kCluster>
 __global__ void __launch_bounds__(kPipeBlock, 1) gsPipe(PipeArgs<T> a)
 {
     extern __shared__ __align__(16) unsigned char pipeSm[];
-    __shared__ unsigned rbase[kPipeMaxRanks];
     T* x = reinterpret_cast<T*>(pipeSm);
     const int rank = kCluster ? static_cast<int>(clusterRank()) : 0;
     const int t = threadIdx.x;
@@ -169,26 +175,24 @@ __global__ void __launch_bounds__(kPipeBlock, 1) gsPipe(PipeArgs<T> a)
     const int cnt = a.localCount[rank];
     const int* lp = a.localPos + static_cast<size_t>(rank) * a.maxLocal;
     for (int i = t; i < cnt; i += B) x[i] = a.psi[lp[i]];
-    if (t < kPipeMaxRanks)
-        rbase[t] = kCluster && t < static_cast<int>(gridDim.x) ? mapaCluster(xa, static_cast<unsigned>(t)) : xa;
-    // every rank's psi is in place (and rbase written) before any row reads it
+    // every rank's psi is in place before any row reads it
     pipeBarrier<kCluster>();
     const int* ss = a.stepStart + static_cast<size_t>(rank) * (a.nSteps + 1);
     PipeRow<T> cur, nxt;
-    pipeLoad(a, a.nSteps > 0 && ss[0] + t < ss[1] ? ss[0] + t : -1, rbase, cur);
+    pipeLoad(a, a.nSteps > 0 && ss[0] + t < ss[1] ? ss[0] + t : -1, cur);
     int kn = a.nSteps > 1 && ss[1] + t < ss[2] ? ss[1] + t : -1;
     for (int T_ = 0; T_ < a.nSteps; ++T_)
     {
         // the next step's row (its item index was found a step ago) and the item index after it
-        pipeLoad(a, kn, rbase, nxt);
+        pipeLoad(a, kn, nxt);
         kn = T_ + 2 < a.nSteps && ss[T_ + 2] + t < ss[T_ + 3] ? ss[T_ + 2] + t : -1;
-        if (cur.slot >= 0) pipeRow<T, kCluster>(a, cur, rbase, xa);
+        if (cur.slot >= 0) pipeRow<T, kCluster>(a, cur, xa);
         // items beyond the block's width at this step, straight from memory
         for (int k = ss[T_] + t + B; k < ss[T_ + 1]; k += B)
         {
             PipeRow<T> r;
-            pipeLoad(a, k, rbase, r);
-            pipeRow<T, kCluster>(a, r, rbase, xa);
+            pipeLoad(a, k, r);
+            pipeRow<T, kCluster>(a, r, xa);
         }
         pipeBarrier<kCluster>();
         cur = nxt;

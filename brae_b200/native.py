@@ -72,6 +72,7 @@ def _load():
         "b2g_set_profiling": (ip, [ip]),
         "b2g_set_sweep_pipeline": (ip, [ip]),
         "b2g_coarsest_dense_solve": (ip, [vp, vp, vp]),
+        "b2g_assemble_pressure": (ip, [vp] + [vp] * 6 + [ip] + [vp] * 6 + [ip, dp] + [vp] * 5 + [ip, vp]),
         "b2g_level_smooth_pipelined": (ip, [vp, ip, vp, vp, ip, ip]),
         "b2g_level_pipe_shape": (ip, [vp, ip, ip, ip, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float),
                                       C.POINTER(C.c_float)]),
@@ -152,7 +153,7 @@ EXPORTED = [
     "b2g_batch_launches", "b2g_batch_destroy", "b2g_mesh_set_pair", "b2g_mesh_level_pair",
     "b2g_gamg_solve_coupled", "b2g_matrix_create_coupled", "b2g_matrix_level_pair_coeffs", "b2g_matrix_gamg_solve",
     "b2g_matrix_set_coeffs", "b2g_matrix_level_timings", "b2g_level_smooth_stall", "b2g_set_sweep_pipeline",
-    "b2g_level_smooth_pipelined", "b2g_level_pipe_shape", "b2g_coarsest_dense_solve",
+    "b2g_level_smooth_pipelined", "b2g_level_pipe_shape", "b2g_coarsest_dense_solve", "b2g_assemble_pressure",
 ]
 
 
@@ -517,6 +518,36 @@ def pcg_gamg_solve(mesh: Mesh, diag, upper, source, psi, controls: Controls | No
                                   C.byref(controls), ms, _stream(), C.byref(p), C.byref(lb.log)))
     return (SolverPerformance(p.initialResidual, p.finalResidual, p.nIterations), lb.history(),
             lb.coarsest())
+
+
+def assemble_pressure(mesh: Mesh, system: dict, p_ref_cell: int = -1, p_ref_value: float = 0.0) -> dict:
+    """simpleFoam's pressure equation ahead of the solve on the device (b2g_assemble_pressure). `system`
+    holds numpy arrays (host) or CUDA tensors: weights, deltaCoeffs, magSf, phi per internal face; V, rAU
+    per cell; bFaceCells, bMagSf, bDeltaCoeffs, bType, bValue, bPhi per boundary face. Returns diag,
+    coef, source, internalCoeffs, boundaryCoeffs in the same memory."""
+    keys = ("weights", "deltaCoeffs", "magSf", "V", "rAU", "phi", "bFaceCells", "bMagSf", "bDeltaCoeffs", "bType",
+            "bValue", "bPhi")
+    arr = {}
+    for k in keys:
+        a = system[k]
+        if not _is_torch(a):
+            a = np.ascontiguousarray(a, np.int32 if k in ("bFaceCells", "bType") else np.float64)
+        arr[k] = a
+    ms = _memspace(*arr.values())
+    nC, nF, nB = mesh.n_cells, mesh.n_faces, int(arr["bFaceCells"].shape[0])
+    if ms == B2G_MEM_HOST:
+        out = {k: np.zeros(n) for k, n in (("diag", nC), ("coef", nF), ("source", nC), ("internalCoeffs", nB),
+                                            ("boundaryCoeffs", nB))}
+    else:
+        import torch
+        dev = arr["V"].device
+        out = {k: torch.zeros(n, dtype=torch.float64, device=dev) for k, n in (
+            ("diag", nC), ("coef", nF), ("source", nC), ("internalCoeffs", nB), ("boundaryCoeffs", nB))}
+    _check(lib.b2g_assemble_pressure(mesh.handle, *[_ptr(arr[k]) for k in keys[:6]], nB,
+                                     *[_ptr(arr[k]) for k in keys[6:]], int(p_ref_cell), float(p_ref_value),
+                                     _ptr(out["diag"]), _ptr(out["coef"]), _ptr(out["source"]),
+                                     _ptr(out["internalCoeffs"]), _ptr(out["boundaryCoeffs"]), ms, _stream()))
+    return out
 
 
 def gamg_solve(mesh: Mesh, diag, upper, source, psi, controls: Controls,

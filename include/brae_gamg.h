@@ -415,6 +415,25 @@ B2G_API b2g_status b2g_fold_boundary(int nCells, int nBFaces, const int32_t* fac
                                      const double* boundaryCoeffs, const unsigned char* coupled, double* diag,
                                      double* source, int memspace, void* stream);
 
+/* The pressure equation ahead of the solve, on the device: simpleFoam's pEqn.H stages 4-5 as the
+ * reference's cpu::assemblePEqn computes them (src/applications/solvers/simpleFoam/pEqn_cpp.cu:209-260)
+ * on an orthogonal mesh with uncoupled patches -- fvm::laplacian(fvc::interpolate(rAU), p) ==
+ * fvc::div(phiHbyA), then setReference -- bit for bit. The mesh gives the internal faces' addressing;
+ * per internal face the linear-interpolation weights, deltaCoeffs, |Sf| and phiHbyA, per cell V and
+ * rAU; the boundary faces patch by patch with their cell, |Sf|, deltaCoeffs, pressure condition
+ * (bType 1 fixedValue bValue, 0 zeroGradient, 2 empty: left out of the divergence) and phiHbyA;
+ * pRefCell -1 for no reference. Out: diag, upper (== lower) and source, and per boundary face the
+ * internalCoeffs and boundaryCoeffs that b2g_fold_boundary folds in before the solve. All arrays in
+ * `memspace`. A non-orthogonal correction and coupled patches are not assembled here. */
+B2G_API b2g_status b2g_assemble_pressure(b2g_mesh* mesh, const double* weights, const double* deltaCoeffs,
+                                         const double* magSf, const double* V, const double* rAU,
+                                         const double* phiHbyA, int nBFaces, const int32_t* bFaceCells,
+                                         const double* bMagSf, const double* bDeltaCoeffs, const int32_t* bType,
+                                         const double* bValue, const double* bPhiHbyA, int pRefCell,
+                                         double pRefValue, double* diag, double* upper, double* source,
+                                         double* internalCoeffs, double* boundaryCoeffs, int memspace,
+                                         void* stream);
+
 /* ---- the batched form: many independent cases in one solve ------------------------------------ */
 
 /* A batch of matrices (each on its own mesh), solved together: every step of every level is one

@@ -180,6 +180,9 @@ class Oracle:
             _f64p, _f64p, C.POINTER(Controls), C.c_void_p, C.c_int]
         L.oc_amul_pair.argtypes = lvl + pair + [_f64p, _f64p]
         L.oc_smooth_pair.argtypes = lvl + pair + [_f64p, _f64p, C.c_int, C.c_int]
+        L.oc_assemble_pressure.argtypes = [C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, _f64p, _f64p,
+                                           _f64p, C.c_int, _i32p, _f64p, _f64p, _i32p, _f64p, _f64p, C.c_int,
+                                           C.c_double, _f64p, _f64p, _f64p, _f64p, _f64p]
 
     # -- agglomeration --------------------------------------------------------------------------
     def agglomerate(self, lower, upper, Sf, magSf, n_cells, n_coarsest=10, forward=True):
@@ -282,6 +285,21 @@ class Oracle:
                                    hist.ctypes.data, cap)
         return dict(psi=x, perf=p.as_tuple(), history=hist[:min(p.nIterations, cap)])
 
+    # -- the pressure equation's assembly ---------------------------------------------------------
+    def assemble_pressure(self, sys_: dict, p_ref_cell=-1, p_ref_value=0.0):
+        """cpu::assemblePEqn restated (oc_assemble_pressure) on a PressureSystem dict (see
+        Reference.box_pressure_system): returns diag, coef, source, internalCoeffs, boundaryCoeffs."""
+        nC, nF, nB = len(sys_["V"]), len(sys_["lower"]), len(sys_["bFaceCells"])
+        out = {k: np.zeros(n) for k, n in (("diag", nC), ("coef", nF), ("source", nC),
+                                            ("internalCoeffs", nB), ("boundaryCoeffs", nB))}
+        self.lib.oc_assemble_pressure(nC, nF, *[np.ascontiguousarray(sys_[k]) for k in (
+            "lower", "upper", "weights", "deltaCoeffs", "magSf", "V", "rAU", "phi")], nB,
+            *[np.ascontiguousarray(sys_[k]) for k in ("bFaceCells", "bMagSf", "bDeltaCoeffs", "bType", "bValue",
+                                                        "bPhi")],
+            int(p_ref_cell), float(p_ref_value), out["diag"], out["coef"], out["source"], out["internalCoeffs"],
+            out["boundaryCoeffs"])
+        return out
+
     # -- the coupled pair -----------------------------------------------------------------------
     @staticmethod
     def _pair(own, nbr, coeff):
@@ -359,6 +377,47 @@ class Reference:
     def _check(self, rc):
         if rc != 0:
             raise RuntimeError(self.lib.ref_last_error().decode())
+
+    # -- the pressure equation's assembly (ref_peqn.cpp over cpu::assemblePEqn) -----------------
+    BOX_PATCHES = ("inlet", "outlet", "wallYmin", "wallYmax", "wallZmin", "wallZmax")
+
+    def box_pressure_system(self, n, spacing, fixed, values, rAU, phi, phi_b, p_ref_cell=-1, p_ref_value=0.0):
+        """The reference's own assembly of the pressure equation on its own Nx x Ny x Nz box (cell sizes
+        `spacing`), the pressure fixedValue values[i] on patch i where fixed[i], zeroGradient elsewhere
+        (patches in BOX_PATCHES order). Returns the inputs and the geometry the assembly read (a
+        PressureSystem dict the oracle and the device take) and the reference's matrix."""
+        L = self.lib
+        if not getattr(self, "_peqn", False):
+            L.ref_peqn_last_error.restype = C.c_char_p
+            L.ref_box_assemble_peqn.argtypes = [C.c_int] * 3 + [C.c_double] * 3 + [_i32p, _f64p, _f64p, _f64p,
+                                                                                  _f64p, C.c_int, C.c_double] + \
+                [_i32p, _i32p, _f64p, _f64p, _f64p, _f64p, _i32p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p]
+            self._peqn = True
+        nx, ny, nz = n
+        nC = nx * ny * nz
+        nF = 3 * nC - (ny * nz + nx * nz + nx * ny)
+        sizes = [ny * nz, ny * nz, nx * nz, nx * nz, nx * ny, nx * ny]
+        nB = sum(sizes)
+        g = {"lower": np.zeros(nF, np.int32), "upper": np.zeros(nF, np.int32), "weights": np.zeros(nF),
+             "deltaCoeffs": np.zeros(nF), "magSf": np.zeros(nF), "V": np.zeros(nC),
+             "bFaceCells": np.zeros(nB, np.int32), "bMagSf": np.zeros(nB), "bDeltaCoeffs": np.zeros(nB)}
+        m = {"diag": np.zeros(nC), "coef": np.zeros(nF), "source": np.zeros(nC), "internalCoeffs": np.zeros(nB),
+             "boundaryCoeffs": np.zeros(nB)}
+        rc = L.ref_box_assemble_peqn(nx, ny, nz, *[float(x) for x in spacing],
+                                     np.ascontiguousarray(fixed, np.int32), np.ascontiguousarray(values, np.float64),
+                                     np.ascontiguousarray(rAU, np.float64), np.ascontiguousarray(phi, np.float64),
+                                     np.ascontiguousarray(phi_b, np.float64), int(p_ref_cell), float(p_ref_value),
+                                     g["lower"], g["upper"], g["weights"], g["deltaCoeffs"], g["magSf"], g["V"],
+                                     g["bFaceCells"], g["bMagSf"], g["bDeltaCoeffs"], m["diag"], m["coef"],
+                                     m["source"], m["internalCoeffs"], m["boundaryCoeffs"])
+        if rc != 0:
+            raise RuntimeError(L.ref_peqn_last_error().decode())
+        btype = np.concatenate([np.full(sz, 1 if f else 0, np.int32) for sz, f in zip(sizes, fixed)])
+        bval = np.concatenate([np.full(sz, float(v) if f else 0.0) for sz, f, v in zip(sizes, fixed, values)])
+        g.update(rAU=np.ascontiguousarray(rAU, np.float64), phi=np.ascontiguousarray(phi, np.float64),
+                 bPhi=np.ascontiguousarray(phi_b, np.float64), bType=btype, bValue=bval,
+                 patchSizes=np.asarray(sizes, np.int32))
+        return g, m
 
     def agglomerate(self, lower, upper, Sf, magSf, n_cells, n_coarsest=10, forward=True):
         lower = np.ascontiguousarray(lower, np.int32)

@@ -1171,3 +1171,58 @@ void oc_smooth_pair(int nCells, int nFaces, const int* lower, const int* upper, 
     smoother_smooth(&sm, psi, source, nSweeps);
     smoother_free(&sm);
 }
+
+/* ------------------------------------------------------------------------------------------------
+ * The pressure equation's assembly (cpu::assemblePEqn, pEqn_cpp.cu:209-260), orthogonal, uncoupled
+ * ------------------------------------------------------------------------------------------------ */
+void oc_assemble_pressure(int nCells, int nFaces, const int* lower, const int* upper, const double* weights,
+                          const double* deltaCoeffs, const double* magSf, const double* V, const double* rAU,
+                          const double* phi, int nBFaces, const int* bFaceCells, const double* bMagSf,
+                          const double* bDeltaCoeffs, const int* bType, const double* bValue,
+                          const double* bPhi, int pRefCell, double pRefValue, double* diag, double* coef,
+                          double* source, double* internalCoeffs, double* boundaryCoeffs)
+{
+    int c, f, b;
+    double* d = (double*)malloc(sizeof(double) * (size_t)(nCells > 0 ? nCells : 1));
+    /* fvm::laplacian(interpolate(rAU), p) (fvm.cuh:130-150, fvc.cu:639-640) */
+    for (c = 0; c < nCells; ++c) diag[c] = 0.0;
+    for (f = 0; f < nFaces; ++f)
+    {
+        const double w = weights[f];
+        const double rf = w * rAU[lower[f]] + (1.0 - w) * rAU[upper[f]];
+        const double k = deltaCoeffs[f] * rf * magSf[f];
+        coef[f] = k;
+        diag[lower[f]] -= k;
+        diag[upper[f]] -= k;
+    }
+    /* laplacianBoundaryCoeffs (fvm.cuh:40-95): pGamma = rAUf_b*|Sf|, the boundary rAUf being the
+     * cell's; fixedValue's gradient coefficients -deltaCoeffs and value*deltaCoeffs, zeroGradient's 0 */
+    for (b = 0; b < nBFaces; ++b)
+    {
+        const double pGamma = rAU[bFaceCells[b]] * bMagSf[b];
+        const int fixed = bType[b] == 1;
+        const double gIC = fixed ? -bDeltaCoeffs[b] : 0.0;
+        const double gBC = fixed ? bValue[b] * bDeltaCoeffs[b] : 0.0;
+        internalCoeffs[b] = pGamma * gIC;
+        boundaryCoeffs[b] = (-pGamma) * gBC;
+    }
+    /* the laplacian's own source is zero on an orthogonal mesh; source += div(phiHbyA)*V with
+     * div = surfaceIntegrate (fvc.cu:706-730) */
+    for (c = 0; c < nCells; ++c) d[c] = 0.0;
+    for (f = 0; f < nFaces; ++f)
+    {
+        d[lower[f]] += phi[f];
+        d[upper[f]] -= phi[f];
+    }
+    for (b = 0; b < nBFaces; ++b)
+        if (bType[b] != 2) d[bFaceCells[b]] += bPhi[b];
+    for (c = 0; c < nCells; ++c) d[c] /= V[c];
+    for (c = 0; c < nCells; ++c) source[c] = 0.0 + d[c] * V[c];
+    /* setReference (fvMatrix.C:1011-1023 as pEqn_cpp.cu:248-255 applies it) */
+    if (pRefCell >= 0 && pRefCell < nCells)
+    {
+        source[pRefCell] += diag[pRefCell] * pRefValue;
+        diag[pRefCell] += diag[pRefCell];
+    }
+    free(d);
+}

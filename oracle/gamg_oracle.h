@@ -134,6 +134,22 @@ void oc_smooth_pair(int nCells, int nFaces, const int* lower, const int* upper, 
                     const double* coef, int nIf, const int* ifOwn, const int* ifNbr, const double* ifCoeff,
                     double* psi, const double* source, int nSweeps, int smoother);
 
+/* The pressure equation's assembly before the solve (simpleFoam pEqn.H stages 4-5, the reference's
+ * cpu::assemblePEqn, src/applications/solvers/simpleFoam/pEqn_cpp.cu:209-260) on an orthogonal mesh
+ * with uncoupled patches: fvc::interpolate(rAU) (fvc.cu:626-650; a boundary face takes its cell's
+ * value), fvm::laplacian (fvm.cuh:130-150: upper = lower = deltaCoeffs*rAUf*|Sf| per internal face,
+ * diag = minus their sum in face order; laplacianBoundaryCoeffs fvm.cuh:40-95 with the fixedValue
+ * gradient coefficients fv_patch_field.cuh:590-602, zeroGradient's zero), source = div(phiHbyA)*V
+ * (fvc.cu:706-730: the face sum in face order, the boundary faces patch by patch, divided by V, then
+ * multiplied by V back), and setReference (pEqn_cpp.cu:248-255). Boundary faces are given patch by
+ * patch: bType 1 fixedValue bValue, 0 zeroGradient, 2 empty (left out of the divergence). */
+void oc_assemble_pressure(int nCells, int nFaces, const int* lower, const int* upper, const double* weights,
+                          const double* deltaCoeffs, const double* magSf, const double* V, const double* rAU,
+                          const double* phi, int nBFaces, const int* bFaceCells, const double* bMagSf,
+                          const double* bDeltaCoeffs, const int* bType, const double* bValue,
+                          const double* bPhi, int pRefCell, double pRefValue, double* diag, double* coef,
+                          double* source, double* internalCoeffs, double* boundaryCoeffs);
+
 #ifdef __cplusplus
 }
 #endif
