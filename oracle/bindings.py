@@ -54,10 +54,11 @@ class Perf(C.Structure):
 
 
 def build(reference_root: str | None = None) -> None:
-    """Compiles the restatement, and the reference library too when its source tree is present."""
+    """Compiles the restatement, and the reference library too when a reference source tree is named
+    (reference_root, else the REF environment variable) and present."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    ref = reference_root or os.environ.get("REF", "/root/reference")
-    if os.path.isdir(os.path.join(ref, "src")):
+    ref = reference_root or os.environ.get("REF")
+    if ref and os.path.isdir(os.path.join(ref, "src")):
         subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REF={ref}"], check=True)
 
 

@@ -97,7 +97,7 @@ def read_solution(path):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="the reference's source tree")
     args = ap.parse_args()
     ref = args.ref
     tmp = os.path.join(REPO, "oracle", "_ref")
