@@ -7,6 +7,7 @@
 //
 // Reference: GAMG = src/matrices/lduMatrix/solvers/GAMG/gamg_solver_cpp.cu
 #include "batch.cuh"
+#include "pipe_kernels.cuh"
 #include "capi_internal.cuh"
 
 #include <algorithm>
@@ -910,6 +911,7 @@ Batch::Batch(std::vector<Matrix*> cs, cudaStream_t s) : stream(s), cases(std::mo
         }
         B.nParts = static_cast<int>(parts.size());
         B.block = maxM + 128;
+        B.hostParts = parts;
         if (!parts.empty())
         {
             B.gs64.upload(g64.data(), g64.size(), stream);
@@ -1135,13 +1137,110 @@ void Batch::smooth(int lv, int nSweeps)
     const k::GsArgs<T>* args = sizeof(T) == 8 ? reinterpret_cast<const k::GsArgs<T>*>(B.gs64.p)
                                               : reinterpret_cast<const k::GsArgs<T>*>(B.gs32.p);
     const size_t smem = sizeof(T) == 8 ? B.smem64 : B.smem32;
+    const int4* parts = B.parts.p;
+    int nParts = B.nParts;
+    auto pit = B.pipe.find(nSweeps * 16 + static_cast<int>(sizeof(T)));
+    if (pipeOn && pit != B.pipe.end())
+    {
+        // the cases whose level fits one CTA: every sweep in one pipelined launch; the rest below
+        const BatchLevel::Pipe& P = pit->second;
+        if (P.nSmall)
+        {
+            launchPipeBatch<T>(P.table.p, P.caseOf.p, P.nSmall, P.smem, active.p, stream);
+            ++launches;
+        }
+        parts = P.partsBig.p;
+        nParts = P.nPartsBig;
+    }
+    if (nParts == 0) return;
     for (int sw = 0; sw < nSweeps; ++sw)
     {
         B2G_CUDA(cudaMemsetAsync(B.progress.p, 0, B.progress.bytes(), stream));
-        k::gsSweepBatch<T><<<B.nParts, B.block, smem, stream>>>(
-            args, B.parts.p, active.p, reinterpret_cast<int*>(B.progress.p + B.ticketAt));
+        k::gsSweepBatch<T><<<nParts, B.block, smem, stream>>>(
+            args, parts, active.p, reinterpret_cast<int*>(B.progress.p + B.ticketAt));
         B2G_LAUNCH_CHECK();
         ++launches;
+    }
+}
+
+// The batched pipelined sweeps of level lv for nSweeps sweeps in T: per case whose level fits one
+// CTA's shared memory, the one-CTA schedule (on its mesh, built once) with that case's vectors; the
+// other cases' parts for the sweep-by-sweep launch. Outside any capture.
+template <class T>
+void Batch::preparePipe(int lv, int nSweeps)
+{
+    BatchLevel& B = lev[lv];
+    const int key = nSweeps * 16 + static_cast<int>(sizeof(T));
+    if (B.pipe.count(key) || B.nParts == 0) return;
+    BatchLevel::Pipe& P = B.pipe[key];
+    const int K = static_cast<int>(cases.size());
+    std::vector<k::PipeArgs<T>> table;
+    std::vector<int> caseOf;
+    std::vector<char> small(K, 0);
+    for (int c = 0; c < K; ++c)
+    {
+        if (nLevelsOf[c] < lv + 1 || lv > nLevelsOf[c]) continue;
+        Matrix& A = *cases[c];
+        LevelAddr& L = A.mesh->lev[lv];
+        if (L.nCells == 0) continue;
+        const PipeSchedule* S = pipeOneCta(L, nSweeps, sizeof(T), stream);
+        if (!S) continue;
+        k::PipeArgs<T> a;
+        a.A = rowsOf(L, A.data<T>().coef[lv]);
+        a.nSteps = S->nSteps;
+        a.maxLocal = S->maxLocal;
+        a.stepStart = S->stepStart.p;
+        a.item = S->item.p;
+        a.entAddr = S->entAddr.p;
+        a.localPos = S->localPos.p;
+        a.localCount = S->localCount.p;
+        if (sizeof(T) == 8)
+        {
+            a.b = reinterpret_cast<const T*>(lv == 0 ? A.rA.p : A.v64.src[lv - 1].p);
+            a.psi = reinterpret_cast<T*>(lv == 0 ? A.wA.p : A.v64.corr[lv - 1].p);
+        }
+        else
+        {
+            a.b = reinterpret_cast<const T*>(lv == 0 ? A.r32.p : A.v32.src[lv - 1].p);
+            a.psi = reinterpret_cast<T*>(lv == 0 ? A.w32.p : A.v32.corr[lv - 1].p);
+        }
+        table.push_back(a);
+        caseOf.push_back(c);
+        small[c] = 1;
+        P.smem = std::max(P.smem, sizeof(T) * static_cast<size_t>(S->maxLocal));
+    }
+    std::vector<int4> big;
+    for (const int4& q : B.hostParts)
+        if (!small[q.z]) big.push_back(q);
+    P.nSmall = static_cast<int>(table.size());
+    P.nPartsBig = static_cast<int>(big.size());
+    if (P.nSmall)
+    {
+        P.table.upload(reinterpret_cast<const unsigned char*>(table.data()), sizeof(k::PipeArgs<T>) * table.size(),
+                       stream);
+        P.caseOf.upload(caseOf.data(), caseOf.size(), stream);
+    }
+    if (P.nPartsBig) P.partsBig.upload(big.data(), big.size(), stream);
+    B2G_CUDA(cudaStreamSynchronize(stream));
+}
+
+// Every batched pipelined sweep the controls' V-cycle makes, before the iterations run.
+void Batch::preparePipes(const b2g_controls& c)
+{
+    pipeOn = g_pipeline && !multicolour && c.smoother == B2G_SMOOTHER_GAUSS_SEIDEL;
+    if (!pipeOn) return;
+    const bool fp64 = c.precision == B2G_PRECISION_FP64;
+    auto want = [&](int lv, int s) {
+        if (s <= 0 || lv >= static_cast<int>(lev.size())) return;
+        if (fp64) preparePipe<double>(lv, s);
+        else preparePipe<float>(lv, s);
+    };
+    want(0, c.nFinestSweeps);
+    for (int lv = 1; lv < static_cast<int>(lev.size()); ++lv)
+    {
+        const int li = lv - 1;
+        want(lv, std::min(c.nPostSweeps + c.postSweepsLevelMultiplier * li, c.maxPostSweeps));
+        if (c.nPreSweeps) want(lv, std::min(c.nPreSweeps + c.preSweepsLevelMultiplier * li, c.maxPreSweeps));
     }
 }
 
@@ -1373,6 +1472,7 @@ void Batch::solve(const b2g_controls& c, const double* const* source, double* co
         prepareDense();
         denseNow = denseAll;
     }
+    preparePipes(c);
     const int K = static_cast<int>(cases.size());
     serial = c.reduction == B2G_REDUCTION_SERIAL;
     launches = 0;
@@ -1424,7 +1524,7 @@ void Batch::solve(const b2g_controls& c, const double* const* source, double* co
         // one captured graph per controls and reduction order
         std::vector<unsigned char> key(sizeof(b2g_controls) + 1);
         std::memcpy(key.data(), &c, sizeof(b2g_controls));
-        key[sizeof(b2g_controls)] = static_cast<unsigned char>((serial ? 1 : 0) | (denseNow ? 2 : 0));
+        key[sizeof(b2g_controls)] = static_cast<unsigned char>((serial ? 1 : 0) | (denseNow ? 2 : 0) | (pipeOn ? 4 : 0));
         if (eagerIterations == 0 && (!graph.exec || graph.key != key))
         {
             // a batch's first iteration runs as plain launches: capturing pays off only from the

@@ -15,6 +15,8 @@
 // kernels skip inactive cases, whose fields stay as they were.
 #pragma once
 
+#include <map>
+
 #include "solver.cuh"
 
 namespace b2g {
@@ -98,6 +100,19 @@ struct BatchLevel
     size_t smem64 = 0, smem32 = 0;
     DBuf<unsigned> progress;
     size_t ticketAt = 0;  // the sweep launch's ticket counter: the word after the parts' progress lines
+    std::vector<int4> hostParts;  // the parts table on the host
+    // the exact form's smoothing calls by sweeps * 16 + value size: the cases whose level fits one CTA
+    // run all their sweeps in one pipelined launch (pipe_kernels.cuh), the others the sweep above
+    struct Pipe
+    {
+        int nSmall = 0;
+        size_t smem = 0;
+        DBuf<unsigned char> table;   // k::PipeArgs<T>[nSmall]
+        DBuf<int> caseOf;            // [nSmall]
+        DBuf<int4> partsBig;         // the parts of the cases that do not fit
+        int nPartsBig = 0;
+    };
+    std::map<int, Pipe> pipe;
     std::vector<TileList> mc;  // per colour: the swept large cases' rows of that colour (multicolour form)
     DBuf<int> mcSmall;         // the swept small cases (descriptors): one block each sweeps them whole
     int nMcSmall = 0;
@@ -119,6 +134,9 @@ struct Batch
     DBuf<k::DenseCase> denseCases;          // [K] the FP32 forms' direct coarsest solves (coarsestDirect)
     bool denseAll = false;                  // every case has its dense factor for the current values
     void prepareDense();
+    template <class T> void preparePipe(int lv, int nSweeps);
+    void preparePipes(const b2g_controls& c);
+    bool pipeOn = false;                    // the current solve takes the batched pipelined sweeps
     DBuf<int> active;                       // [K]
     DBuf<int> nActive;                      // [1]
     DBuf<int> err;

@@ -86,6 +86,9 @@ struct LevelAddr;
 // The item schedule of L for S sweeps pipelined in one launch (items.cu), or null when the level has
 // one part or exceeds the schedule's limits.
 std::unique_ptr<GsSchedule> buildGsItems(const LevelAddr& L, int S, cudaStream_t s);
+// L's one-CTA pipelined schedule for S sweeps in values of valueBytes (pipe.cu), built once and kept on
+// the level; null when the level's psi does not fit one CTA's shared memory.
+const PipeSchedule* pipeOneCta(LevelAddr& L, int S, size_t valueBytes, cudaStream_t s);
 
 // A colouring of one level for the multicolour sweep of the FP32 V-cycle: no two cells of one colour
 // share a face, so a colour's cells are updated in parallel. Rows are the level's cells colour by
@@ -161,6 +164,8 @@ struct LevelAddr
     PairLevel pair;         // the coupled pair, if the mesh carries one (nFaces 0 otherwise)
     // pipelined smoothing calls, keyed by sweeps * 16 + the value size (built on first use)
     std::map<int, PipeChoice> pipe;
+    // the one-CTA pipelined schedule by the same key (the batched form's; null: the level does not fit)
+    std::map<int, std::unique_ptr<PipeSchedule>> pipeOne;
     // The one-block resident Gauss-Seidel sweep of a small one-part level (solver.cu gsResident),
     // built on first use: the part's positions run by depth, depth d's are [start[d], start[d+1]).
     struct Resident

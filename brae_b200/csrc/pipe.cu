@@ -469,6 +469,43 @@ bool Matrix::pipeForced(int level, T* psiL, const T* src, int nSweeps, int ranks
     return true;
 }
 
+const PipeSchedule* pipeOneCta(LevelAddr& L, int S, size_t valueBytes, cudaStream_t s)
+{
+    const int key = pipeKey(S, valueBytes);
+    auto it = L.pipeOne.find(key);
+    if (it != L.pipeOne.end()) return it->second.get();
+    std::unique_ptr<PipeSchedule>& P = L.pipeOne[key];
+    if (S < 1 || L.nCells == 0 || static_cast<size_t>(L.nCells) * valueBytes > kPipeSmemCap) return nullptr;
+    const LevelHost H = download(L, s);
+    int nSteps = 0;
+    const std::vector<int> Tsteps = combinedSteps(H, S, nSteps);
+    P = assemble(H, Tsteps, S, nSteps, 1, valueBytes, s);
+    return P.get();
+}
+
+// The batched one-CTA launch's shared-memory ceiling, once per device and value type.
+template <class T>
+static void allowPipeBatchSmem()
+{
+    static std::atomic<unsigned long long> done{0};
+    int dev = 0;
+    B2G_CUDA(cudaGetDevice(&dev));
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (done.load() & bit) return;
+    B2G_CUDA(cudaFuncSetAttribute(k::gsPipeBatch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(kPipeSmemCap)));
+    done.fetch_or(bit);
+}
+template <class T>
+void launchPipeBatch(const void* table, const int* caseOf, int n, size_t smem, const int* active, cudaStream_t s)
+{
+    allowPipeBatchSmem<T>();
+    k::gsPipeBatch<T><<<n, k::kPipeBlock, smem, s>>>(static_cast<const k::PipeArgs<T>*>(table), caseOf, active);
+    B2G_LAUNCH_CHECK();
+}
+template void launchPipeBatch<double>(const void*, const int*, int, size_t, const int*, cudaStream_t);
+template void launchPipeBatch<float>(const void*, const int*, int, size_t, const int*, cudaStream_t);
+
 template void Matrix::ensurePipe<double>(int, int);
 template bool Matrix::pipeForced<double>(int, double*, const double*, int, int);
 template void Matrix::ensurePipe<float>(int, int);

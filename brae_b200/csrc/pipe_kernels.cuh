@@ -164,7 +164,7 @@ __device__ __forceinline__ void pipeRow(const PipeArgs<T>& a, const PipeRow<T>& 
 // One smoothing call (all its sweeps) of one level. Grid = one cluster of R CTAs (kCluster) or one
 // CTA; dynamic shared memory = maxLocal values of T.
 template <class T, bool kCluster>
-__global__ void __launch_bounds__(kPipeBlock, 1) gsPipe(PipeArgs<T> a)
+__device__ __forceinline__ void gsPipeBody(const PipeArgs<T>& a)
 {
     extern __shared__ __align__(16) unsigned char pipeSm[];
     T* x = reinterpret_cast<T*>(pipeSm);
@@ -200,6 +200,24 @@ __global__ void __launch_bounds__(kPipeBlock, 1) gsPipe(PipeArgs<T> a)
     // the last barrier above ordered every read of this CTA's values before the write-back; no rank
     // reads another's shared memory after it, so the CTAs may leave in any order
     for (int i = t; i < cnt; i += B) a.psi[lp[i]] = x[i];
+}
+
+template <class T, bool kCluster>
+__global__ void __launch_bounds__(kPipeBlock, 1) gsPipe(PipeArgs<T> a)
+{
+    gsPipeBody<T, kCluster>(a);
+}
+
+// One smoothing call of many independent cases' levels in ONE launch, each on one CTA: block i runs
+// the pipelined sweeps of table[i], skipped when its case's `active` flag (may be null) is 0.
+template <class T>
+__global__ void __launch_bounds__(kPipeBlock, 1) gsPipeBatch(const PipeArgs<T>* __restrict__ table,
+                                                             const int* __restrict__ caseOf,
+                                                             const int* __restrict__ active)
+{
+    if (active && active[caseOf[blockIdx.x]] == 0) return;
+    const PipeArgs<T> a = table[blockIdx.x];
+    gsPipeBody<T, false>(a);
 }
 
 }  // namespace k

@@ -104,6 +104,10 @@ k::Rows<T> rowsOf(const LevelAddr& L, const LevelCoef<T>& C)
 
 // Whether smoothing calls may take the pipelined multi-sweep launch (pipe.cu; b2g_set_sweep_pipeline).
 extern bool g_pipeline;
+// The batched one-CTA pipelined launch (pipe.cu): n cases' levels, table = k::PipeArgs<T>[n] on the
+// device, caseOf[n] each entry's case (its `active` flag; active may be null).
+template <class T>
+void launchPipeBatch(const void* table, const int* caseOf, int n, size_t smem, const int* active, cudaStream_t s);
 
 struct Matrix
 {
