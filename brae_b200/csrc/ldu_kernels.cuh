@@ -165,6 +165,66 @@ __global__ void scaleUpdateAdd(int n, const T* __restrict__ sfp, const T* __rest
     }
 }
 
+// THE FINEST LEVEL'S CORRECTION, FUSED: prolongField (GAMG:422-432) injects the coarse correction
+// into a fine vector that only the scaling and the update then read. Here that vector is never
+// stored: every read of it takes coarse[prolongP[c]] instead -- the same values, the same operations in
+// the same order, so the results are those of the three separate steps bit for bit. (Not for a level
+// with a coupled pair, whose Amul reads the pair's neighbours too.)
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) amulScaleDotsProlong(Rows<T> A, const int* __restrict__ prolongP,
+                                                           const T* __restrict__ coarse,
+                                                           const T* __restrict__ source, T* __restrict__ Acf,
+                                                           T* __restrict__ partial)
+{
+    __shared__ T sh[NT / 32];
+    T num = T(0), den = T(0);
+    for (int c = blockIdx.x * NT + threadIdx.x; c < A.n; c += gridDim.x * NT)
+    {
+        const T fc = coarse[prolongP[c]];
+        T acc = mulRn(A.diag[c], fc);
+        const int e1 = A.rowStart[c + 1];
+        for (int e = A.rowStart[c]; e < e1; ++e) acc = addRn(acc, mulRn(A.val[e], coarse[prolongP[A.col[e]]]));
+        Acf[c] = acc;
+        num = addRn(num, mulRn(fc, source[c]));
+        den = addRn(den, mulRn(fc, acc));
+    }
+    num = blockSum<T, NT>(num, sh);
+    den = blockSum<T, NT>(den, sh);
+    if (threadIdx.x == 0)
+    {
+        partial[2 * blockIdx.x] = num;
+        partial[2 * blockIdx.x + 1] = den;
+    }
+}
+
+// psi += sf*P + (source - sf*Acf)/diag with P = coarse[prolongP[c]] (scaleUpdateAdd on the injection)
+template <class T>
+__global__ void scaleUpdateAddProlong(int n, const T* __restrict__ sfp, const int* __restrict__ prolongP,
+                                      const T* __restrict__ coarse, const T* __restrict__ source,
+                                      const T* __restrict__ Acf, const T* __restrict__ diag, T* __restrict__ psi)
+{
+    const T sf = *sfp;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+    {
+        const T corr = addRn(mulRn(sf, coarse[prolongP[c]]), divRn(subRn(source[c], mulRn(sf, Acf[c])), diag[c]));
+        psi[c] = addRn(psi[c], corr);
+    }
+}
+
+// The residual between V-cycles, FUSED: Apsi = A*psi (Amul's order) and r = source - Apsi in one pass,
+// the product never stored (Amul then subtract, bit for bit)
+template <class T>
+__global__ void amulSubtract(Rows<T> A, const T* __restrict__ source, const T* __restrict__ x, T* __restrict__ r)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.n; c += gridDim.x * blockDim.x)
+    {
+        T acc = mulRn(A.diag[c], x[c]);
+        const int e1 = A.rowStart[c + 1];
+        for (int e = A.rowStart[c]; e < e1; ++e) acc = addRn(acc, mulRn(A.val[e], x[A.col[e]]));
+        r[c] = subRn(source[c], pairSub(A, c, acc, x));
+    }
+}
+
 // psi += correction, unscaled (scaleCorrection off)
 template <class T>
 __global__ void addInPlace(int n, T* __restrict__ psi, const T* __restrict__ corr)

@@ -778,6 +778,18 @@ void Matrix::amul(int level, const T* x, T* y)
     ++launches;
 }
 
+// r = source - A*psi on the finest level, Amul's rounding (fused Amul and subtract; GAMG:1098-1106)
+template <class T>
+void Matrix::residualBetween(const T* source, const T* x, T* r)
+{
+    const LevelAddr& F = mesh->lev[0];
+    cudaEvent_t e = timedBegin(0, 0, 1);
+    k::amulSubtract<T><<<rowsGrid(F.nCells), NT, 0, stream>>>(rowsOf(F, data<T>().coef[0]), source, x, r);
+    timedEnd(e);
+    B2G_LAUNCH_CHECK();
+    ++launches;
+}
+
 template <class T>
 void Matrix::smooth(int level, int smoother, T* psiL, const T* src, int nSweeps, unsigned long long* trace)
 {
@@ -1533,8 +1545,26 @@ void Matrix::vcycle(const b2g_controls& c, T* x, const T* src, T* Apsi, T* fcor,
         smooth<T>(lv, c.smoother, D.corr[li].p, D.src[li].p,
                   std::min(c.nPostSweeps + c.postSweepsLevelMultiplier * li, c.maxPostSweeps));
     }
-    prolongFrom<T>(0, D.corr[0].p, fcor);
     const LevelAddr& F = mesh->lev[0];
+    if (c.scaleCorrection && !(serial && sizeof(T) == 8) && !(D.coef[0].pairVal.p && F.pair.nFaces > 0))
+    {
+        // prolong, scale and correct without storing the prolonged correction (bit for bit the same)
+        const Step& S0 = mesh->step[0];
+        const int g = redGrid(F.nCells);
+        cudaEvent_t e = timedBegin(0, 0, 1);
+        k::amulScaleDotsProlong<T, NT><<<g, NT, 0, stream>>>(rowsOf(F, D.coef[0]), S0.prolongP.p, D.corr[0].p, fres,
+                                                             Apsi, D.partial.p);
+        timedEnd(e);
+        k::scaleFactor<T, NT><<<1, NT, 0, stream>>>(D.partial.p, g, D.sf.p);
+        k::scaleUpdateAddProlong<T><<<rowsGrid(F.nCells), NT, 0, stream>>>(F.nCells, D.sf.p, S0.prolongP.p,
+                                                                          D.corr[0].p, fres, Apsi,
+                                                                          D.coef[0].gsDiag.p, x);
+        B2G_LAUNCH_CHECK();
+        launches += 3;
+        smooth<T>(0, c.smoother, x, src, c.nFinestSweeps);
+        return;
+    }
+    prolongFrom<T>(0, D.corr[0].p, fcor);
     if (c.scaleCorrection)
     {
         if (serial && sizeof(T) == 8)
@@ -1587,9 +1617,7 @@ void Matrix::precondition(const b2g_controls& c, double* w, const double* r)
             vcycle<float>(c, w32.p, r32.p, AwA32.p, fc32.p, frp);
             if (cycle < c.nVcycles - 1)
             {
-                amul<float>(0, w32.p, AwA32.p);
-                k::subtract<float><<<rowsGrid(n0), NT, 0, stream>>>(n0, r32.p, AwA32.p, fr32.p);
-                B2G_LAUNCH_CHECK();
+                residualBetween<float>(r32.p, w32.p, fr32.p);
                 frp = fr32.p;
             }
         }
@@ -1603,9 +1631,7 @@ void Matrix::precondition(const b2g_controls& c, double* w, const double* r)
         vcycle<double>(c, w, r, AwA.p, fc.p, frp);
         if (cycle < c.nVcycles - 1)
         {
-            amul<double>(0, w, AwA.p);
-            k::subtract<double><<<rowsGrid(n0), NT, 0, stream>>>(n0, r, AwA.p, fr.p);
-            B2G_LAUNCH_CHECK();
+            residualBetween<double>(r, w, fr.p);
             frp = fr.p;
         }
     }

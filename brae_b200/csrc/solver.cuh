@@ -203,6 +203,7 @@ struct Matrix
 
     // pieces (device pointers)
     template <class T> void amul(int level, const T* x, T* y);
+    template <class T> void residualBetween(const T* source, const T* x, T* r);
     template <class T> void smooth(int level, int smoother, T* psi, const T* source, int nSweeps,
                                    unsigned long long* trace = nullptr);
     template <class T> void smoothCall(int level, int smoother, T* psi, const T* source, int nSweeps,
