@@ -5,18 +5,22 @@
 Workload (one step = one pressure solve, psi from zero): a 272^3 hex box, 2 x 1 x 1 m, graded 20:1
 toward y = 0 and y = 1, fixedValue outlet at x = 2, seeded face-flux source (brae_b200.cases), plain
 FP64 PCG + GAMG(GaussSeidel, 0/2, nCellsInCoarsestLevel 10), tolerance 1e-6, relTol 0.05,
-maxIter 1000. The hierarchy is built once per mesh and timed apart ("mesh_build_s"). The same
-mesh with the 1000:1 two-phase coefficient is then solved in plain FP64 and in the FP32-
-preconditioned form; their times, final residuals and field error are reported beside it.
+maxIter 1000. A step is what the reference's pcgGamgSolve does per call: the matrix's coefficients in
+(b2g_matrix_set_coeffs), every coarse level rebuilt by Galerkin summation, then the solve. The
+agglomeration is built once per mesh and timed apart ("mesh_build_s").
 
-`value` is seconds per solve with every input resident in HBM (max over ranks); `e2e` is the same
+`value` is seconds per step with every input resident in HBM (max over ranks); `e2e` is the same
 solve through the C ABI with host (pinned) buffers, copies in the timed region. N > 1 runs N
 independent replicas, one per GPU (the solve does not shard). `--impl reference` times the
 reference's own CPU implementation (oracle/_ref, else the oracle port) on the same workload.
 
-The "served" object is the serving form (b2g_server): Poisson arrivals at --serve-rate per second
-(500) for --serve-seconds (4; the full stream is 60 s) over a resident population of graded boxes
-(70 % 16k-128k cells, 25 % 0.5M-2M, 5 % 8M), both forms, with p50/p99 latency and solves/s.
+Beside the headline: a profiled pass (per-level Amul and smoothing times and GB/s), the same solve to
+tolerance 1e-6 with relTol 0 against the reference's own solve (iterations, residuals, field) with the
+hierarchy compared map for map, the precision form on the two-phase (1000:1) coefficient (FP64, FP32
+exact order, FP32 multicolour, at equal residual and tighter), the batched form and the served stream
+(b2g_server: Poisson arrivals at --serve-rate per second for --serve-seconds over a resident population
+of graded boxes, 70 % 16k-128k cells, 25 % 0.5M-2M, 5 % 8M, tolerance 1e-6 relTol 0; then repeated
+streams at a rate the server keeps up with).
 """
 from __future__ import annotations
 
@@ -755,24 +759,29 @@ def serve_stream(args, b2g, local):
                           "slots": args.serve_slots, "hbm_cap_gb": 150},
            "offered_rate_per_s": args.serve_rate, "stream_s": args.serve_seconds,
            "tolerance": args.serve_tol, "relTol": args.serve_reltol}
-    runs = [(form, prec, args.serve_rate) for form, prec in (("fp64", 0), ("fp32_precond", 1),
-                                                               ("fp32_precond_multicolour", 2))]
-    if args.serve_rate_low > 0:
-        runs += [(form + "_at_low_rate", prec, args.serve_rate_low)
-                 for form, prec in (("fp64", 0), ("fp32_precond", 1), ("fp32_precond_multicolour", 2))]
-    for form, prec, rate in runs:
+    forms = [f for f in (("fp64", 0), ("fp32_precond", 1), ("fp32_precond_multicolour", 2))
+             if f[0] in args.serve_forms]
+    out["window_note"] = (f"the configured stream is 60 s at 500/s; this run offers {args.serve_rate:g}/s for "
+                          f"{args.serve_seconds:g} s" + ("" if args.serve_seconds >= 60 else
+                                                         " (shorter than configured, to keep the run to minutes)"))
+
+    warmed = set()
+
+    def one_stream(form, prec, rate, seconds, seed):
         ctl = b2g.controls_default(tolerance=args.serve_tol, relTol=args.serve_reltol, maxIter=MAX_ITER,
                                    precision=prec)
-        # warm every case once in this form (captures its iteration graph)
-        for row in resident:
-            for cid, n, src in row:
-                buf = free[cid][0]
-                srv.wait(srv.submit(cid, src, ctl, out=buf))
-                buf[:] = 0.0
-        rng = np.random.default_rng(2)
-        gaps = rng.exponential(1.0 / rate, size=int(rate * args.serve_seconds * 1.5) + 16)
+        if form not in warmed:
+            # warm every case once in this form (captures its iteration graph)
+            for row in resident:
+                for cid, n, src in row:
+                    buf = free[cid][0]
+                    srv.wait(srv.submit(cid, src, ctl, out=buf))
+                    buf[:] = 0.0
+            warmed.add(form)
+        rng = np.random.default_rng(seed)
+        gaps = rng.exponential(1.0 / rate, size=int(rate * seconds * 1.5) + 16)
         arrivals = np.cumsum(gaps)
-        arrivals = arrivals[arrivals < args.serve_seconds]
+        arrivals = arrivals[arrivals < seconds]
         cls = np.searchsorted(probs, rng.random(arrivals.size), side="right").clip(0, 2)
         pick = rng.random(arrivals.size)
         lock = threading.Lock()
@@ -815,12 +824,31 @@ def serve_stream(args, b2g, local):
         th.join()
         wall = time.perf_counter() - start
         lat_a = np.asarray(lat)
-        out[form] = {"offered_rate_per_s": rate, "requests": int(arrivals.size), "p50_ms": float(np.percentile(lat_a, 50)),
+        return {"offered_rate_per_s": rate, "requests": int(arrivals.size), "p50_ms": float(np.percentile(lat_a, 50)),
                      "p99_ms": float(np.percentile(lat_a, 99)), "mean_ms": float(lat_a.mean()),
-                     "solves_per_s": arrivals.size / wall, "drain_s": wall - args.serve_seconds,
+                     "solves_per_s": arrivals.size / wall, "drain_s": wall - seconds,
                      "max_outstanding": outstanding[1], "mean_iterations": float(np.mean(iters)),
                      "by_class": [{"requests": len(l), "p50_ms": float(np.percentile(l, 50)) if l else None,
                                    "p99_ms": float(np.percentile(l, 99)) if l else None} for l in lat_cls]}
+
+    for form, prec in forms:
+        out[form] = one_stream(form, prec, args.serve_rate, args.serve_seconds, 2)
+    # a rate the server keeps up with (a fraction of the capacity the offered stream showed), repeated
+    # with different arrival seeds: the spread of the latencies
+    for form, prec in forms:
+        cap = out[form]["solves_per_s"]
+        rate = max(1.0, args.serve_capacity_fraction * cap)
+        reps = [one_stream(form, prec, rate, args.serve_stable_seconds, 2 + r) for r in range(args.serve_repeats)]
+        p50 = [r["p50_ms"] for r in reps]
+        p99 = [r["p99_ms"] for r in reps]
+        out[form + "_at_stable_rate"] = {
+            "offered_rate_per_s": rate, "stream_s": args.serve_stable_seconds, "repeats": len(reps),
+            "p50_ms": {"min": min(p50), "median": float(np.median(p50)), "max": max(p50)},
+            "p99_ms": {"min": min(p99), "median": float(np.median(p99)), "max": max(p99)},
+            "solves_per_s": [r["solves_per_s"] for r in reps],
+            "max_outstanding": [r["max_outstanding"] for r in reps],
+            "mean_iterations": float(np.mean([r["mean_iterations"] for r in reps])),
+            "by_class": [r["by_class"] for r in reps]}
     srv.close()
     return out
 
@@ -873,8 +901,12 @@ def main():
     ap.add_argument("--serve-slots", type=int, default=6, help="server worker slots")
     ap.add_argument("--serve-tol", type=float, default=1e-6, help="tolerance of the served solves")
     ap.add_argument("--serve-reltol", type=float, default=0.0, help="relTol of the served solves")
-    ap.add_argument("--serve-rate-low", type=float, default=150.0,
-                    help="a second stream below the server's capacity (0: none)")
+    ap.add_argument("--serve-forms", nargs="*", default=["fp64", "fp32_precond_multicolour"],
+                    help="forms of the served stream (fp64, fp32_precond, fp32_precond_multicolour)")
+    ap.add_argument("--serve-capacity-fraction", type=float, default=0.8,
+                    help="the stable stream's rate as a fraction of the capacity the offered stream showed")
+    ap.add_argument("--serve-stable-seconds", type=float, default=8.0, help="length of each stable stream")
+    ap.add_argument("--serve-repeats", type=int, default=3, help="repeats of the stable stream")
     ap.add_argument("--serve", action="store_true", help="run the served stream alone")
     ap.add_argument("--no-coupled", action="store_true", help="skip the coupled-pair leg")
     ap.add_argument("--coupled", action="store_true", help="run the coupled-pair leg alone")
