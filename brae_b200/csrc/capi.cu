@@ -858,7 +858,7 @@ b2g_status b2g_coarsest_dense_solve(b2g_matrix* m, double* psi, const double* so
 }
 
 b2g_status b2g_level_pipe_shape(const b2g_mesh* mesh, int level, int nSweeps, int valueBytes, int* ranks,
-                                int* nSteps, float* msPipe, float* msSweeps)
+                                int* nSteps, float* msPipe, float* msSweeps, float* msShared, float* msItems)
 {
     return guarded([&] {
         need(mesh != nullptr, "b2g_level_pipe_shape: null mesh");
@@ -873,6 +873,8 @@ b2g_status b2g_level_pipe_shape(const b2g_mesh* mesh, int level, int nSweeps, in
             *nSteps = mode == 1 ? it->second.sched->nSteps : mode == 2 ? it->second.items->maxDepth + 1 : 0;
         if (msPipe) *msPipe = !have ? 0.f : mode == 2 ? it->second.msItems : it->second.msPipe;
         if (msSweeps) *msSweeps = have ? it->second.msSweeps : 0.f;
+        if (msShared) *msShared = have ? it->second.msPipe : 0.f;
+        if (msItems) *msItems = have ? it->second.msItems : 0.f;
     });
 }
 

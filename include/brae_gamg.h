@@ -392,9 +392,11 @@ B2G_API b2g_status b2g_coarsest_dense_solve(b2g_matrix* m, double* psi, const do
  * 4 FP32): *ranks the pipelined launch's CTAs holding psi in shared memory, or minus the part count of
  * the pipelined multi-part sweep over (sweep, cell) items (0: sweep by sweep, or not tuned yet),
  * *nSteps its combined steps, and the measured milliseconds per call of the chosen pipelined form
- * (else the best shared-memory shape) and of the sweep-by-sweep launches. Any output may be NULL. */
+ * (else the best shared-memory shape), of the sweep-by-sweep launches, of the best shared-memory
+ * shape and of the item schedule (0: not tried). Any output may be NULL. */
 B2G_API b2g_status b2g_level_pipe_shape(const b2g_mesh* mesh, int level, int nSweeps, int valueBytes, int* ranks,
-                                        int* nSteps, float* msPipe, float* msSweeps);
+                                        int* nSteps, float* msPipe, float* msSweeps, float* msShared,
+                                        float* msItems);
 B2G_API b2g_status b2g_level_smooth_trace(b2g_matrix* m, int level, double* psi, const double* source,
                                           unsigned long long* trace, int traceCapacity, int* schedule);
 /* Diagnostic: the Gauss-Seidel schedule of `level` to HOST arrays (either may be NULL):
