@@ -528,6 +528,36 @@ __global__ void kCsrPositions(int n, const int* __restrict__ order, const int* _
     }
 }
 
+// a 32-position slice's width, times 32: its longest row
+__global__ void kEllWidth(int n, int nSlices, const int* __restrict__ posRow, int* __restrict__ width32)
+{
+    const int sl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sl >= nSlices) return;
+    int w = 0;
+    for (int i = 32 * sl; i < min(n, 32 * sl + 32); ++i) w = max(w, posRow[i + 1] - posRow[i]);
+    width32[sl] = 32 * w;
+}
+
+// entry q of the row in lane l of slice s at base[s] + 32*q + l; -1 past the row's end
+__global__ void kEllFill(int n, const int* __restrict__ posRow, const int* __restrict__ colPos,
+                         const int* __restrict__ base, int* __restrict__ ellCol, int* __restrict__ ellEnt)
+{
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int sl = static_cast<int>(t >> 5), lane = static_cast<int>(t & 31);
+    if (sl * 32LL >= n) return;
+    const int i = 32 * sl + lane;
+    const int b0 = base[sl];
+    const int w = (base[sl + 1] - b0) >> 5;
+    const int r0 = i < n ? posRow[i] : 0;
+    const int len = i < n ? posRow[i + 1] - r0 : 0;
+    for (int q = 0; q < w; ++q)
+    {
+        const int e = b0 + 32 * q + lane;
+        ellCol[e] = q < len ? colPos[r0 + q] : -1;
+        ellEnt[e] = q < len ? r0 + q : -1;
+    }
+}
+
 __global__ void kChunkOfPos(int n, int nChunks, const int* __restrict__ chunkStart, int* __restrict__ chunkOf)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1037,6 +1067,8 @@ void buildHierarchyFromMaps(Mesh& M, const double* dSf, const double* dMagSf,
 // Gauss-Seidel schedule
 // ---------------------------------------------------------------------------------------------
 
+void buildEll(GsSchedule& G, int n, cudaStream_t s);
+
 void buildGsSchedule(LevelAddr& L, cudaStream_t s)
 {
     GsSchedule& G = L.gs;
@@ -1320,7 +1352,26 @@ void buildGsSchedule(LevelAddr& L, cudaStream_t s)
     // the parts' progress lines, then one line for a launch's ticket counter
     G.progress.alloc(static_cast<size_t>(P + 1) * k::kProgressStride, s);
     G.progress.zero(s);
+    if (n >= kEllMinCells) buildEll(G, n, s);
     B2G_CUDA(cudaStreamSynchronize(s));
+}
+
+// the sliced ELL copy of a level's position-order rows (ldu_kernels.cuh Rows)
+void buildEll(GsSchedule& G, int n, cudaStream_t s)
+{
+    const int nSlices = (n + 31) / 32;
+    DBuf<int> width32;
+    width32.alloc(nSlices, s);
+    kEllWidth<<<grid(nSlices), TPB, 0, s>>>(n, nSlices, G.posRow.p, width32.p);
+    B2G_LAUNCH_CHECK();
+    G.ellBase.alloc(static_cast<size_t>(nSlices) + 1, s);
+    const long long nEnt = exclusiveScan(width32.p, G.ellBase.p, nSlices, s);
+    if (nEnt >= (1LL << 31)) fail(B2G_ERR_ARGUMENT, "b2g: a level's sliced rows exceed 2^31 entries.");
+    G.nEllEnt = nEnt;
+    G.ellCol.alloc(std::max<long long>(nEnt, 1), s);
+    G.ellEnt.alloc(std::max<long long>(nEnt, 1), s);
+    kEllFill<<<grid(nSlices * 32LL), TPB, 0, s>>>(n, G.posRow.p, G.entColPos.p, G.ellBase.p, G.ellCol.p, G.ellEnt.p);
+    B2G_LAUNCH_CHECK();
 }
 
 namespace {

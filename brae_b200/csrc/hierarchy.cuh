@@ -52,7 +52,15 @@ struct GsSchedule
     // and itemStore[i] is the psi position item i writes
     int items = 0;
     DBuf<int> itemStore;
+    // the position-order rows in sliced ELL (ldu_kernels.cuh Rows), on levels of at least
+    // kEllMinCells cells: per 32-position slice its entry base [nCells/32 + 1], per entry the column
+    // position (-1 past the row's end) and the CSR entry it copies (-1 there)
+    long long nEllEnt = 0;
+    DBuf<int> ellBase, ellCol, ellEnt;
 };
+
+// the smallest level that gets the sliced ELL copy of its rows
+constexpr int kEllMinCells = 65536;
 
 // One smoothing call's sweeps of a level in one pipelined launch (pipe_kernels.cuh), for a given
 // sweep count: the combined steps of every (sweep, cell) item, the cells split into `ranks`

@@ -43,7 +43,38 @@ struct Rows
     const int* __restrict__ pairStart = nullptr;
     const int* __restrict__ pairCol = nullptr;
     const T* __restrict__ pairVal = nullptr;
+    // the same rows in sliced ELL, where the level has it: the row of position c is lane c % 32 of
+    // slice c / 32, its entry q at ellBase[slice] + 32*q + lane (column -1 past the row's end), so a
+    // warp's 32 rows load each entry in one coalesced access
+    const int* __restrict__ ellBase = nullptr;
+    const int* __restrict__ ellCol = nullptr;
+    const T* __restrict__ ellVal = nullptr;
 };
+
+// The row of position c folded into acc in the row's entry order: acc = term(acc, coefficient, column
+// position) per entry, from the sliced ELL copy when the level has one, else from the CSR rows -- the
+// same entries in the same order either way.
+template <class T, class F>
+__device__ __forceinline__ T rowFold(const Rows<T>& A, int c, T acc, F term)
+{
+    if (A.ellBase)
+    {
+        const int sl = c >> 5, lane = c & 31;
+        const int b0 = A.ellBase[sl];
+        const int w = (A.ellBase[sl + 1] - b0) >> 5;
+        for (int q = 0; q < w; ++q)
+        {
+            const int e = b0 + 32 * q + lane;
+            const int cp = A.ellCol[e];
+            if (cp < 0) break;
+            acc = term(acc, A.ellVal[e], cp);
+        }
+        return acc;
+    }
+    const int e1 = A.rowStart[c + 1];
+    for (int e = A.rowStart[c]; e < e1; ++e) acc = term(acc, A.val[e], A.col[e]);
+    return acc;
+}
 
 // The pair's terms of row c after the face terms, in face order: acc - coef*x[nbr] each (Amul's sign)
 template <class T>
@@ -64,8 +95,7 @@ __global__ void amul(Rows<T> A, const T* __restrict__ x, T* __restrict__ y)
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.n; c += gridDim.x * blockDim.x)
     {
         T acc = mulRn(A.diag[c], x[c]);
-        const int e1 = A.rowStart[c + 1];
-        for (int e = A.rowStart[c]; e < e1; ++e) acc = addRn(acc, mulRn(A.val[e], x[A.col[e]]));
+        acc = rowFold(A, c, acc, [x](T a, T v, int cp) { return addRn(a, mulRn(v, x[cp])); });
         y[c] = pairSub(A, c, acc, x);
     }
 }
@@ -102,8 +132,7 @@ __global__ void __launch_bounds__(NT) amulScaleDots(Rows<T> A, const T* __restri
     {
         const T fc = field[c];
         T acc = mulRn(A.diag[c], fc);
-        const int e1 = A.rowStart[c + 1];
-        for (int e = A.rowStart[c]; e < e1; ++e) acc = addRn(acc, mulRn(A.val[e], field[A.col[e]]));
+        acc = rowFold(A, c, acc, [field](T a, T v, int cp) { return addRn(a, mulRn(v, field[cp])); });
         acc = pairSub(A, c, acc, field);
         Acf[c] = acc;
         num = addRn(num, mulRn(fc, source[c]));
@@ -182,8 +211,8 @@ __global__ void __launch_bounds__(NT) amulScaleDotsProlong(Rows<T> A, const int*
     {
         const T fc = coarse[prolongP[c]];
         T acc = mulRn(A.diag[c], fc);
-        const int e1 = A.rowStart[c + 1];
-        for (int e = A.rowStart[c]; e < e1; ++e) acc = addRn(acc, mulRn(A.val[e], coarse[prolongP[A.col[e]]]));
+        acc = rowFold(A, c, acc,
+                      [coarse, prolongP](T a, T v, int cp) { return addRn(a, mulRn(v, coarse[prolongP[cp]])); });
         Acf[c] = acc;
         num = addRn(num, mulRn(fc, source[c]));
         den = addRn(den, mulRn(fc, acc));
@@ -219,8 +248,7 @@ __global__ void amulSubtract(Rows<T> A, const T* __restrict__ source, const T* _
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.n; c += gridDim.x * blockDim.x)
     {
         T acc = mulRn(A.diag[c], x[c]);
-        const int e1 = A.rowStart[c + 1];
-        for (int e = A.rowStart[c]; e < e1; ++e) acc = addRn(acc, mulRn(A.val[e], x[A.col[e]]));
+        acc = rowFold(A, c, acc, [x](T a, T v, int cp) { return addRn(a, mulRn(v, x[cp])); });
         r[c] = subRn(source[c], pairSub(A, c, acc, x));
     }
 }
@@ -322,8 +350,7 @@ __global__ void residual(Rows<T> A, const T* __restrict__ source, const T* __res
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.n; c += gridDim.x * blockDim.x)
     {
         T acc = subRn(source[c], mulRn(A.diag[c], psi[c]));
-        const int e1 = A.rowStart[c + 1];
-        for (int e = A.rowStart[c]; e < e1; ++e) acc = subRn(acc, mulRn(A.val[e], psi[A.col[e]]));
+        acc = rowFold(A, c, acc, [psi](T a, T v, int cp) { return subRn(a, mulRn(v, psi[cp])); });
         // the pair with the sign Amul's term does not have (GAMG:110-115)
         if (A.pairStart)
             for (int k = A.pairStart[c]; k < A.pairStart[c + 1]; ++k)

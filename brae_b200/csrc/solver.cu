@@ -174,6 +174,28 @@ void fillBlobs(const LevelAddr& L, LevelCoef<T>& C, const double* upper, cudaStr
     B2G_LAUNCH_CHECK();
 }
 
+// the level's sliced ELL coefficients from its CSR ones (GsSchedule::ellEnt), where it has the layout
+template <class T>
+__global__ void kEllValues(long long nEnt, const int* __restrict__ ellEnt, const T* __restrict__ rowVal,
+                           T* __restrict__ ellVal)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nEnt; e += (long long)gridDim.x * blockDim.x)
+    {
+        const int q = ellEnt[e];
+        ellVal[e] = q >= 0 ? rowVal[q] : T(0);
+    }
+}
+
+template <class T>
+void fillEll(const LevelAddr& L, LevelCoef<T>& C, cudaStream_t s)
+{
+    if (!L.gs.nEllEnt) return;
+    C.ellVal.ensure(static_cast<size_t>(L.gs.nEllEnt), s);
+    kEllValues<T><<<std::min(ceilDiv(L.gs.nEllEnt, NT), 8192), NT, 0, s>>>(L.gs.nEllEnt, L.gs.ellEnt.p, C.rowVal.p,
+                                                                         C.ellVal.p);
+    B2G_LAUNCH_CHECK();
+}
+
 void fillGsLayout(const LevelAddr& L, LevelCoef<double>& C, cudaStream_t s)
 {
     allocGsLayout(L, C, s);
@@ -183,6 +205,7 @@ void fillGsLayout(const LevelAddr& L, LevelCoef<double>& C, cudaStream_t s)
         kGsLayout<<<std::min(ceilDiv(m, NT), 8192), NT, 0, s>>>(L.nCells, nnz, L.gs.posCell.p, L.gs.entFacePos.p,
                                                                 C.diag.p, C.upper.p, C.gsDiag.p, C.rowVal.p);
     B2G_LAUNCH_CHECK();
+    fillEll<double>(L, C, s);
     fillBlobs<double>(L, C, C.upper.p, s);
 }
 
@@ -724,6 +747,7 @@ void Matrix::ensureFp32()
         allocGsLayout(L, C, stream);
         castInto<float, double>(L.nCells, v64.coef[i].gsDiag.p, C.gsDiag.p, stream);
         castInto<float, double>(2LL * L.nFaces, v64.coef[i].rowVal.p, C.rowVal.p, stream);
+        fillEll<float>(L, C, stream);
         fillBlobs<float>(L, C, v64.coef[i].upper.p, stream);
     }
     v32.corr.resize(nL);
@@ -1692,10 +1716,12 @@ unsigned long long Matrix::layoutFingerprint() const
     for (const auto* b : {&psi, &source, &rA, &wA, &pA, &AwA, &fc, &fr, &rOld}) mix(b->p);
     for (const auto* b : {&r32, &w32, &AwA32, &fc32, &fr32}) mix(b->p);
     for (const auto& C : v64.coef)
-        for (const void* q : {(const void*)C.gsDiag.p, (const void*)C.rowVal.p, (const void*)C.blob.p}) mix(q);
+        for (const void* q : {(const void*)C.gsDiag.p, (const void*)C.rowVal.p, (const void*)C.blob.p,
+                              (const void*)C.ellVal.p})
+            mix(q);
     for (const auto& C : v32.coef)
         for (const void* q : {(const void*)C.gsDiag.p, (const void*)C.rowVal.p, (const void*)C.blob.p,
-                              (const void*)C.mcVal.p, (const void*)C.mcDiag.p})
+                              (const void*)C.mcVal.p, (const void*)C.mcDiag.p, (const void*)C.ellVal.p})
             mix(q);
     for (const auto& b : v64.corr) mix(b.p);
     for (const auto& b : v64.src) mix(b.p);

@@ -26,6 +26,7 @@ struct LevelCoef
     DBuf<T> upper;  // [nFaces] LDU coefficient, upper == lower (FP64 only)
     DBuf<T> gsDiag; // [nCells (+pad)] diagonal by position
     DBuf<T> rowVal; // [2*nFaces] coefficient per CSR entry, rows by position
+    DBuf<T> ellVal; // the same in the level's sliced ELL layout (GsSchedule::ellEnt), where it has one
     DBuf<unsigned char> blob;  // the sweep's chunk blobs (gs_kernels.cuh) in T
     DBuf<float> mcVal, mcDiag;  // FP32 only: the multicolour layout's coefficients (hierarchy.cuh Colouring)
     // FP64 only, a coupled matrix: the pair's coefficient per pair face and per row entry (pair.cu)
@@ -98,6 +99,12 @@ k::Rows<T> rowsOf(const LevelAddr& L, const LevelCoef<T>& C)
         r.pairStart = L.pair.start.p;
         r.pairCol = L.pair.col.p;
         r.pairVal = C.pairVal.p;
+    }
+    if (L.gs.nEllEnt && C.ellVal.p)
+    {
+        r.ellBase = L.gs.ellBase.p;
+        r.ellCol = L.gs.ellCol.p;
+        r.ellVal = C.ellVal.p;
     }
     return r;
 }
