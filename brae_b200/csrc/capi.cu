@@ -437,8 +437,28 @@ std::unique_ptr<b2g_mesh> createMesh(int nCells, int nFaces, const int32_t* lowe
     return h;
 }
 
+// The host source and psi copied into A.fc / A.fr on the matrix's side stream, after the copies already
+// queued on its stream (the matrix's coefficients) have crossed; joinSideCopies makes the stream wait.
+void stageSideCopies(b2g::Matrix& A, const double* source, const double* psi)
+{
+    if (!A.sideStream)
+    {
+        B2G_CUDA(cudaStreamCreateWithFlags(&A.sideStream, cudaStreamNonBlocking));
+        B2G_CUDA(cudaEventCreateWithFlags(&A.sideEv[0], cudaEventDisableTiming));
+        B2G_CUDA(cudaEventCreateWithFlags(&A.sideEv[1], cudaEventDisableTiming));
+    }
+    const size_t bytes = sizeof(double) * static_cast<size_t>(A.n(0));
+    B2G_CUDA(cudaEventRecord(A.sideEv[0], A.stream));
+    B2G_CUDA(cudaStreamWaitEvent(A.sideStream, A.sideEv[0], 0));
+    B2G_CUDA(cudaMemcpyAsync(A.fc.p, source, bytes, cudaMemcpyHostToDevice, A.sideStream));
+    B2G_CUDA(cudaMemcpyAsync(A.fr.p, psi, bytes, cudaMemcpyHostToDevice, A.sideStream));
+    B2G_CUDA(cudaEventRecord(A.sideEv[1], A.sideStream));
+}
+
+void joinSideCopies(b2g::Matrix& A) { B2G_CUDA(cudaStreamWaitEvent(A.stream, A.sideEv[1], 0)); }
+
 void solveOn(b2g::Matrix& A, const double* source, double* psi, const b2g_controls* c, int memspace,
-             b2g_perf* out, b2g_solve_log* log, bool standalone)
+             b2g_perf* out, b2g_solve_log* log, bool standalone, bool staged)
 {
     need(c && source && psi && out, "b2g solve: null argument");
     need(memspace == B2G_MEM_HOST || memspace == B2G_MEM_DEVICE, "b2g solve: bad memspace");
@@ -455,8 +475,11 @@ void solveOn(b2g::Matrix& A, const double* source, double* psi, const b2g_contro
     // outside a solve) and permuted on the device; device fields are permuted in place of a copy
     if (memspace == B2G_MEM_HOST)
     {
-        B2G_CUDA(cudaMemcpyAsync(A.fc.p, source, sizeof(double) * n0, cudaMemcpyHostToDevice, A.stream));
-        B2G_CUDA(cudaMemcpyAsync(A.fr.p, psi, sizeof(double) * n0, cudaMemcpyHostToDevice, A.stream));
+        if (!staged)
+        {
+            B2G_CUDA(cudaMemcpyAsync(A.fc.p, source, sizeof(double) * n0, cudaMemcpyHostToDevice, A.stream));
+            B2G_CUDA(cudaMemcpyAsync(A.fr.p, psi, sizeof(double) * n0, cudaMemcpyHostToDevice, A.stream));
+        }
         A.toPos(0, static_cast<const double*>(A.fc.p), A.source.p);
         A.toPos(0, static_cast<const double*>(A.fr.p), A.psi.p);
     }
@@ -1071,7 +1094,7 @@ b2g_status b2g_matrix_pcg_solve(b2g_matrix* m, const double* source, double* psi
 {
     return guarded([&] {
         need(m != nullptr, "b2g_matrix_pcg_solve: null matrix");
-        b2g::capi::solveOn(*m->mat, source, psi, controls, memspace, out, log, false);
+        b2g::capi::solveOn(*m->mat, source, psi, controls, memspace, out, log, false, false);
     });
 }
 
@@ -1087,7 +1110,18 @@ b2g_status b2g_pcg_gamg_solve(b2g_mesh* mesh, const double* diag, const double* 
         if (!mesh->solveMatrix) mesh->solveMatrix.reset(new b2g::Matrix(&mesh->m, mesh->m.stream));
         b2g::Matrix& A = *mesh->solveMatrix;
         A.setFine(diag, upper, memspace);
-        b2g::capi::solveOn(A, source, psi, controls, memspace, out, log, false);
+        bool staged = false;
+        if (memspace == B2G_MEM_HOST && source && psi && mesh->m.nLevels() > 0)
+        {
+            // the source and the initial guess cross on a second stream once the matrix has, while the
+            // first builds the coarse levels (built here rather than after the first residual: the same
+            // matrices, only earlier)
+            b2g::capi::stageSideCopies(A, source, psi);
+            A.buildCoarse();
+            b2g::capi::joinSideCopies(A);
+            staged = true;
+        }
+        b2g::capi::solveOn(A, source, psi, controls, memspace, out, log, false, staged);
     });
 }
 
@@ -1103,7 +1137,7 @@ b2g_status b2g_gamg_solve(b2g_mesh* mesh, const double* diag, const double* uppe
         if (!mesh->solveMatrix) mesh->solveMatrix.reset(new b2g::Matrix(&mesh->m, mesh->m.stream));
         b2g::Matrix& A = *mesh->solveMatrix;
         A.setFine(diag, upper, memspace);
-        b2g::capi::solveOn(A, source, psi, controls, memspace, out, log, true);
+        b2g::capi::solveOn(A, source, psi, controls, memspace, out, log, true, false);
     });
 }
 
@@ -1189,7 +1223,7 @@ b2g_status b2g_matrix_gamg_solve(b2g_matrix* m, const double* source, double* ps
 {
     return guarded([&] {
         need(m != nullptr, "b2g_matrix_gamg_solve: null matrix");
-        b2g::capi::solveOn(*m->mat, source, psi, controls, memspace, out, log, true);
+        b2g::capi::solveOn(*m->mat, source, psi, controls, memspace, out, log, true, false);
     });
 }
 

@@ -66,8 +66,13 @@ std::unique_ptr<b2g_mesh> createMesh(int nCells, int nFaces, const int32_t* lowe
 
 // A whole solve on the finest level of A (on A.stream): source and psi from `memspace`, psi
 // overwritten with the solution; the PCG + GAMG solver, or GAMG alone when `standalone`.
+// `staged`: host fields already copied into A.fc / A.fr (stageSideCopies, joined).
 void solveOn(b2g::Matrix& A, const double* source, double* psi, const b2g_controls* c, int memspace,
-             b2g_perf* out, b2g_solve_log* log, bool standalone);
+             b2g_perf* out, b2g_solve_log* log, bool standalone, bool staged = false);
+// Host source and psi into A.fc / A.fr on the matrix's side stream, behind the copies queued on its
+// stream; joinSideCopies makes its stream wait for them.
+void stageSideCopies(b2g::Matrix& A, const double* source, const double* psi);
+void joinSideCopies(b2g::Matrix& A);
 
 }  // namespace capi
 }  // namespace b2g

@@ -657,6 +657,13 @@ Matrix::~Matrix()
         cudaEventDestroy(evSolve[0]);
         cudaEventDestroy(evSolve[1]);
     }
+    if (sideStream)
+    {
+        cudaStreamSynchronize(sideStream);
+        cudaEventDestroy(sideEv[0]);
+        cudaEventDestroy(sideEv[1]);
+        cudaStreamDestroy(sideStream);
+    }
 }
 
 template <> VCycleData<double>& Matrix::data<double>() { return v64; }

@@ -154,6 +154,8 @@ struct Matrix
     std::vector<TimedRegion> evOpen;          // regions recorded outside a capture, read at the end
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evFree;
     cudaEvent_t evSolve[2] = {nullptr, nullptr};
+    cudaStream_t sideStream = nullptr;        // host-field uploads beside the coarse build (capi.cu)
+    cudaEvent_t sideEv[2] = {nullptr, nullptr};
     IterationGraph* capturing = nullptr;      // the graph being captured, if any
     // records a start event if profiling; the region is closed by timedEnd
     cudaEvent_t timedBegin(int kind, int level, int units);
