@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cstddef>
 #include <cstring>
+#include <mutex>
 
 namespace b2g {
 
@@ -1596,14 +1597,50 @@ void Batch::solve(const b2g_controls& c, const double* const* source, double* co
 // C ABI
 // ---------------------------------------------------------------------------------------------
 
+namespace {
+
+// Batch streams are never destroyed. A batch builds layouts that its meshes keep (the one-CTA
+// pipelined schedules of pipeOneCta) on its own stream, and a mesh frees them on that stream when it
+// goes, which may be long after the batch: a destroyed batch hands its stream back here, idle, for
+// the next batch on the same device.
+std::mutex g_batchStreamMu;
+std::vector<std::pair<int, cudaStream_t>> g_idleBatchStreams;  // (device, stream)
+
+cudaStream_t takeBatchStream(int device)
+{
+    {
+        std::lock_guard<std::mutex> lk(g_batchStreamMu);
+        for (size_t i = 0; i < g_idleBatchStreams.size(); ++i)
+            if (g_idleBatchStreams[i].first == device)
+            {
+                const cudaStream_t s = g_idleBatchStreams[i].second;
+                g_idleBatchStreams.erase(g_idleBatchStreams.begin() + static_cast<std::ptrdiff_t>(i));
+                return s;
+            }
+    }
+    cudaStream_t s = nullptr;
+    B2G_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    return s;
+}
+
+void giveBackBatchStream(int device, cudaStream_t s)
+{
+    cudaStreamSynchronize(s);
+    std::lock_guard<std::mutex> lk(g_batchStreamMu);
+    g_idleBatchStreams.emplace_back(device, s);
+}
+
+}  // namespace
+
 struct b2g_batch
 {
+    int device = 0;
     cudaStream_t stream = nullptr;
     std::unique_ptr<b2g::Batch> batch;
     ~b2g_batch()
     {
         batch.reset();
-        if (stream) cudaStreamDestroy(stream);
+        if (stream) giveBackBatchStream(device, stream);
     }
 };
 
@@ -1625,7 +1662,8 @@ B2G_API b2g_status b2g_batch_create(b2g_matrix* const* matrices, int count, b2g_
             cs.push_back(matrices[i]->mat.get());
         }
         std::unique_ptr<b2g_batch> h(new b2g_batch);
-        B2G_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        B2G_CUDA(cudaGetDevice(&h->device));
+        h->stream = takeBatchStream(h->device);
         h->batch.reset(new b2g::Batch(std::move(cs), h->stream));
         *out = h.release();
     });

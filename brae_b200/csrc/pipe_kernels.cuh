@@ -122,13 +122,13 @@ __device__ __forceinline__ unsigned pipeAddr(unsigned ea, unsigned xa)
     return kCluster ? mapaCluster(local, ea >> 24) : local;
 }
 
+// a row's loads once its item is known (they wait for no load of their own)
 template <class T>
-__device__ __forceinline__ void pipeLoad(const PipeArgs<T>& a, int k, PipeRow<T>& r)
+__device__ __forceinline__ void pipeLoadRow(const PipeArgs<T>& a, const int4& it, bool has, PipeRow<T>& r)
 {
     r.slot = -1;
     r.w = 0;
-    if (k < 0) return;
-    const int4 it = a.item[k];
+    if (!has) return;
     r.slot = it.y;
     r.e0 = it.z;
     r.w = it.w - it.z;
@@ -141,6 +141,13 @@ __device__ __forceinline__ void pipeLoad(const PipeArgs<T>& a, int k, PipeRow<T>
             r.v[q] = a.A.val[it.z + q];
             r.ea[q] = a.entAddr[it.z + q];
         }
+}
+
+template <class T>
+__device__ __forceinline__ void pipeLoad(const PipeArgs<T>& a, int k, PipeRow<T>& r)
+{
+    const int4 it = k >= 0 ? a.item[k] : make_int4(0, -1, 0, 0);
+    pipeLoadRow(a, it, k >= 0, r);
 }
 
 // the row in the reference's order: the source minus each entry's coefficient times its value, then
@@ -178,14 +185,20 @@ __device__ __forceinline__ void gsPipeBody(const PipeArgs<T>& a)
     // every rank's psi is in place before any row reads it
     pipeBarrier<kCluster>();
     const int* ss = a.stepStart + static_cast<size_t>(rank) * (a.nSteps + 1);
+    // a thread's item at step T is ss[T] + t when that is below ss[T + 1]. Its item record is loaded
+    // two steps ahead and its row one step ahead, so that no step waits on a load chain: at step T
+    // the row of step T+1 is loaded from a record that arrived a step ago, while the record of step
+    // T+2 is on its way.
+    auto itemAt = [&](int T_) { return T_ < a.nSteps && ss[T_] + t < ss[T_ + 1] ? ss[T_] + t : -1; };
     PipeRow<T> cur, nxt;
-    pipeLoad(a, a.nSteps > 0 && ss[0] + t < ss[1] ? ss[0] + t : -1, cur);
-    int kn = a.nSteps > 1 && ss[1] + t < ss[2] ? ss[1] + t : -1;
+    pipeLoad(a, a.nSteps > 0 ? itemAt(0) : -1, cur);
+    int kn = itemAt(1);
+    int4 itn = kn >= 0 ? a.item[kn] : make_int4(0, -1, 0, 0);
     for (int T_ = 0; T_ < a.nSteps; ++T_)
     {
-        // the next step's row (its item index was found a step ago) and the item index after it
-        pipeLoad(a, kn, nxt);
-        kn = T_ + 2 < a.nSteps && ss[T_ + 2] + t < ss[T_ + 3] ? ss[T_ + 2] + t : -1;
+        pipeLoadRow(a, itn, kn >= 0, nxt);
+        kn = itemAt(T_ + 2);
+        if (kn >= 0) itn = a.item[kn];
         if (cur.slot >= 0) pipeRow<T, kCluster>(a, cur, xa);
         // items beyond the block's width at this step, straight from memory
         for (int k = ss[T_] + t + B; k < ss[T_ + 1]; k += B)

@@ -72,6 +72,28 @@ def test_batch_serial_bitexact(b2g, oracle, ctl_kw):
     assert batch.launches() > 0
 
 
+def test_batch_destroyed_before_its_meshes(b2g, oracle):
+    # a batch builds level-held layouts of its meshes on its stream; the meshes outlive the batch and
+    # free them later, and a second batch on the same meshes reuses what the first built
+    import gc
+    built, meshes, mats = _build(b2g, BOXES[:3])
+    ctl = b2g.controls_default(tolerance=1e-8, relTol=0.0, reduction="serial")
+    for _ in range(2):
+        batch = b2g.Batch(mats)
+        psis = [np.zeros(c.n_cells) for c in built]
+        perfs = batch.solve([c.source for c in built], psis, ctl)
+        del batch
+        gc.collect()
+        for c, psi, perf in zip(built, psis, perfs):
+            want = _oracle(oracle, c, 1e-8, 0.0, {})
+            assert tuple(perf) == want["perf"] and np.array_equal(psi, want["psi"])
+    del mats
+    gc.collect()
+    del meshes
+    gc.collect()
+    torch.cuda.synchronize()
+
+
 def test_batch_tree_parity_and_alone(b2g, oracle):
     built, meshes, mats = _build(b2g, BOXES)
     tol, rel = 1e-8, 0.0
