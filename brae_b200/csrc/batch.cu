@@ -974,26 +974,30 @@ Batch::Batch(std::vector<Matrix*> cs, cudaStream_t s) : stream(s), cases(std::mo
 }
 
 // Each case's dense coarsest factor for its current coefficients, and the batched solve's table (the
-// FP32 coarsest vectors of every case); denseAll only when every case has its factor.
+// FP32 coarsest vectors of every case that has its factor, n = 0 for the others): a case is solved
+// as it is alone, by its factor where it has one and by PCG-DIC where it has none.
 void Batch::prepareDense()
 {
     const int K = static_cast<int>(cases.size());
-    std::vector<k::DenseCase> h(K);
-    bool all = true;
+    std::vector<k::DenseCase> h(K, k::DenseCase{0, nullptr, nullptr, nullptr});
+    int with = 0;
     for (int c = 0; c < K; ++c)
     {
         Matrix& A = *cases[c];
         A.ensureDense();
         const int lv = A.nLevels();
-        all = all && A.denseUse && lv > 0;
-        if (!all) break;
+        if (!A.denseUse || lv == 0) continue;
         h[c].n = A.n(lv);
         h[c].L = A.denseL.p;
         h[c].b = A.v32.src[lv - 1].p;
         h[c].x = A.v32.corr[lv - 1].p;
+        ++with;
     }
-    denseAll = all;
-    if (all) denseCases.upload(h.data(), h.size(), stream);
+    // the factors were made on the cases' own streams
+    for (Matrix* A : cases) B2G_CUDA(cudaStreamSynchronize(A->stream));
+    denseAny = with > 0;
+    denseAll = with == K;
+    if (denseAny) denseCases.upload(h.data(), h.size(), stream);
     B2G_CUDA(cudaStreamSynchronize(stream));
 }
 
@@ -1306,21 +1310,27 @@ void Batch::vcycle(const b2g_controls& c, int fresRole)
         k::coarsestPcgDicBatch<<<K, 32, 0, stream>>>(coarsestArgs.p, c.precTolerance, c.precRelTol, act);
         launches += 2;
     }
-    else if (denseNow)
-    {
-        // the FP32 forms' direct coarsest solve: every case's dense Cholesky factor, one warp each
-        k::coarseDenseSolveBatch<<<K, 32, sizeof(double) * k::kDenseMax * k::kDenseMax, stream>>>(denseCases.p, act);
-        ++launches;
-    }
     else
     {
-        bCast<double, float><<<B2G_TILES(coarsestTiles)>>>(coarsestTiles.tiles.p, segD.p, segF.p, V_SRC, V_SRC, act);
-        bCast<double, float><<<B2G_TILES(coarsestTiles)>>>(coarsestTiles.tiles.p, segD.p, segF.p, V_CORR, V_CORR, act);
-        // the single-case FP32 form hands the FP64 solve tolerances rounded to float
-        k::coarsestPcgDicBatch<<<K, 32, 0, stream>>>(coarsestArgs.p, static_cast<double>(static_cast<float>(c.precTolerance)),
-                                                     static_cast<double>(static_cast<float>(c.precRelTol)), act);
-        bCast<float, double><<<B2G_TILES(coarsestTiles)>>>(coarsestTiles.tiles.p, segF.p, segD.p, V_CORR, V_CORR, act);
-        launches += 5;
+        // the FP32 forms: PCG-DIC in FP64 for the cases without a dense factor (for every active case,
+        // unless all have one), then the cases' dense Cholesky factors, one warp each, whose solves
+        // overwrite the corrections of the cases that have one
+        if (!(denseNow && denseAll))
+        {
+            bCast<double, float><<<B2G_TILES(coarsestTiles)>>>(coarsestTiles.tiles.p, segD.p, segF.p, V_SRC, V_SRC, act);
+            bCast<double, float><<<B2G_TILES(coarsestTiles)>>>(coarsestTiles.tiles.p, segD.p, segF.p, V_CORR, V_CORR, act);
+            // the single-case FP32 form hands the FP64 solve tolerances rounded to float
+            k::coarsestPcgDicBatch<<<K, 32, 0, stream>>>(coarsestArgs.p, static_cast<double>(static_cast<float>(c.precTolerance)),
+                                                         static_cast<double>(static_cast<float>(c.precRelTol)), act);
+            bCast<float, double><<<B2G_TILES(coarsestTiles)>>>(coarsestTiles.tiles.p, segF.p, segD.p, V_CORR, V_CORR, act);
+            launches += 5;
+        }
+        if (denseNow)
+        {
+            k::coarseDenseSolveBatch<<<K, 32, sizeof(double) * k::kDenseMax * k::kDenseMax, stream>>>(denseCases.p,
+                                                                                                    act);
+            ++launches;
+        }
     }
     B2G_LAUNCH_CHECK();
     // up
@@ -1471,7 +1481,7 @@ void Batch::solve(const b2g_controls& c, const double* const* source, double* co
     if (c.precision != B2G_PRECISION_FP64 && c.coarsestDirect)
     {
         prepareDense();
-        denseNow = denseAll;
+        denseNow = denseAny;
     }
     preparePipes(c);
     const int K = static_cast<int>(cases.size());
@@ -1525,7 +1535,7 @@ void Batch::solve(const b2g_controls& c, const double* const* source, double* co
         // one captured graph per controls and reduction order
         std::vector<unsigned char> key(sizeof(b2g_controls) + 1);
         std::memcpy(key.data(), &c, sizeof(b2g_controls));
-        key[sizeof(b2g_controls)] = static_cast<unsigned char>((serial ? 1 : 0) | (denseNow ? 2 : 0) | (pipeOn ? 4 : 0));
+        key[sizeof(b2g_controls)] = static_cast<unsigned char>((serial ? 1 : 0) | (denseNow ? 2 : 0) | (pipeOn ? 4 : 0) | (denseAll ? 8 : 0));
         if (eagerIterations == 0 && (!graph.exec || graph.key != key))
         {
             // a batch's first iteration runs as plain launches: capturing pays off only from the

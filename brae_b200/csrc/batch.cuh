@@ -133,6 +133,7 @@ struct Batch
     DBuf<k::CoarsestArgs<double>> coarsestArgs;  // [K] FP64 coarsest solve on (V_CORR, V_SRC)
     DBuf<k::DenseCase> denseCases;          // [K] the FP32 forms' direct coarsest solves (coarsestDirect)
     bool denseAll = false;                  // every case has its dense factor for the current values
+    bool denseAny = false;                  // some case has its dense factor
     void prepareDense();
     template <class T> void preparePipe(int lv, int nSweeps);
     void preparePipes(const b2g_controls& c);

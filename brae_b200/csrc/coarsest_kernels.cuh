@@ -396,7 +396,8 @@ __global__ void __launch_bounds__(32) coarseDenseSolve(int n, const double* __re
     denseSolveWarp<T>(n, L, b, x, denseSh);
 }
 
-// Many cases' coarsest levels, one warp each (block i: case i), skipped where `active` is 0.
+// Many cases' coarsest levels, one warp each (block i: case i), skipped where `active` is 0 or the
+// case has no factor (n = 0).
 struct DenseCase
 {
     int n;
@@ -410,6 +411,7 @@ static __global__ void __launch_bounds__(32) coarseDenseSolveBatch(const DenseCa
     extern __shared__ double denseSh[];
     if (active && active[blockIdx.x] == 0) return;
     const DenseCase c = cases[blockIdx.x];
+    if (c.n == 0) return;
     denseSolveWarp<float>(c.n, c.L, c.b, c.x, denseSh);
 }
 
