@@ -238,12 +238,13 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def level_table(mesh, amul_lv, smooth_lv, fp_bytes=8):
+def level_table(mesh, amul_lv, smooth_lv, fused_lv=(), fp_bytes=8):
     """Per level: cells, faces, and from a profiled solve the Amul and smoothing times with their
-    algorithmic bytes (Amul 24 nC + 16 nF, one exact sweep 32 nC + 16 nF in FP64) and GB/s; plus the
-    all-level sums."""
+    algorithmic bytes (Amul 24 nC + 16 nF, one exact sweep 32 nC + 16 nF in FP64) and GB/s, and the
+    time of the Amuls fused with another step (the residual, the scaling dots, the prolongation);
+    plus the all-level sums."""
     rows = []
-    tot = {"smooth_ms": 0.0, "smooth_bytes": 0.0, "amul_ms": 0.0, "amul_bytes": 0.0}
+    tot = {"smooth_ms": 0.0, "smooth_bytes": 0.0, "amul_ms": 0.0, "amul_bytes": 0.0, "fused_ms": 0.0}
     for lv in range(mesh.n_levels + 1):
         nc, nf = mesh.level_size(lv)
         row = {"level": lv, "cells": nc, "faces": nf}
@@ -261,6 +262,10 @@ def level_table(mesh, amul_lv, smooth_lv, fp_bytes=8):
                        amul_gbs=byt / max(ms_ * 1e-3, 1e-12) / 1e9)
             tot["amul_ms"] += ms_
             tot["amul_bytes"] += byt
+        if lv < len(fused_lv) and fused_lv[lv][2] > 0:
+            ms_, calls, n_amul = fused_lv[lv]
+            row.update(fused_amul_ms=ms_, fused_amuls=int(n_amul), us_per_fused_amul=ms_ * 1e3 / n_amul)
+            tot["fused_ms"] += ms_
         rows.append(row)
     return rows, tot
 
@@ -315,7 +320,7 @@ def run_ours(args, world, rank, local):
     step()  # captures the profiled graph
     step()
     ms4, cnt4 = A.timings()
-    levels, tot = level_table(mesh, A.level_timings(0), A.level_timings(1))
+    levels, tot = level_table(mesh, A.level_timings(0), A.level_timings(1), A.level_timings(2))
     b2g.set_profiling(False)
     for row in levels:
         # the sweep tuner's choice for the level's smoothing calls: ranks > 0 the shared-memory pipelined
@@ -466,6 +471,8 @@ def run_ours(args, world, rank, local):
             "smoothing_all_levels_share": tot["smooth_ms"] / ms4[3],
             "amul_finest_us": fin.get("us_per_amul"), "amul_finest_gbs": fin.get("amul_gbs"),
             "amul_all_levels_share": tot["amul_ms"] / ms4[3],
+            "fused_amul_finest_us": fin.get("us_per_fused_amul"),
+            "fused_amul_all_levels_share": tot["fused_ms"] / ms4[3],
             "levels": levels,
         },
         "roofline": {"kernel": "gsSweep, finest level (exact Gauss-Seidel; per sweep)", "bound": "hbm",

@@ -997,8 +997,51 @@ void Batch::prepareDense()
     for (Matrix* A : cases) B2G_CUDA(cudaStreamSynchronize(A->stream));
     denseAny = with > 0;
     denseAll = with == K;
-    if (denseAny) denseCases.upload(h.data(), h.size(), stream);
+    if (denseAny)
+    {
+        // refilled in place: a captured iteration graph names the table's address
+        denseCases.ensure(h.size(), stream);
+        B2G_CUDA(cudaMemcpyAsync(denseCases.p, h.data(), sizeof(k::DenseCase) * h.size(), cudaMemcpyHostToDevice,
+                                 stream));
+    }
     B2G_CUDA(cudaStreamSynchronize(stream));
+}
+
+// A hash of every device address the batch's iteration hands its kernels (its tables, the cases'
+// buffers): a captured graph is replayed only while it is unchanged.
+unsigned long long Batch::layoutFingerprint() const
+{
+    unsigned long long h = 1469598103934665603ull;
+    auto mix = [&](const void* p) {
+        h ^= reinterpret_cast<unsigned long long>(p);
+        h *= 1099511628211ull;
+    };
+    for (const void* p : {(const void*)segD.p, (const void*)segF.p, (const void*)coarsestArgs.p,
+                          (const void*)denseCases.p, (const void*)active.p, (const void*)nActive.p, (const void*)err.p,
+                          (const void*)partial.p, (const void*)sf64.p, (const void*)partial32.p, (const void*)sf32.p,
+                          (const void*)perf.p, (const void*)coarsestTiles.tiles.p})
+        mix(p);
+    for (const BatchLevel& B : lev)
+    {
+        for (const TileList* L : {&B.all, &B.up, &B.scale, &B.down})
+        {
+            mix(L->tiles.p);
+            mix(L->segOf.p);
+            mix(L->tileStart.p);
+        }
+        for (const void* p : {(const void*)B.gs64.p, (const void*)B.gs32.p, (const void*)B.parts.p,
+                              (const void*)B.progress.p, (const void*)B.mcSmall.p})
+            mix(p);
+        for (const auto& kv : B.pipe)
+        {
+            mix(kv.second.table.p);
+            mix(kv.second.caseOf.p);
+            mix(kv.second.partsBig.p);
+        }
+        for (const TileList& L : B.mc) mix(L.tiles.p);
+    }
+    for (const Matrix* A : cases) h ^= A->layoutFingerprint() + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2);
+    return h;
 }
 
 // The multicolour layout of every case's levels (built on each mesh once) in the FP32 descriptors,
@@ -1176,7 +1219,8 @@ void Batch::preparePipe(int lv, int nSweeps)
 {
     BatchLevel& B = lev[lv];
     const int key = nSweeps * 16 + static_cast<int>(sizeof(T));
-    if (B.pipe.count(key) || B.nParts == 0) return;
+    if (B.nParts == 0) return;
+    if (B.pipe.count(key)) return;
     BatchLevel::Pipe& P = B.pipe[key];
     const int K = static_cast<int>(cases.size());
     std::vector<k::PipeArgs<T>> table;
@@ -1190,29 +1234,22 @@ void Batch::preparePipe(int lv, int nSweeps)
         if (L.nCells == 0) continue;
         const PipeSchedule* S = pipeOneCta(L, nSweeps, sizeof(T), stream);
         if (!S) continue;
-        k::PipeArgs<T> a;
-        a.A = rowsOf(L, A.data<T>().coef[lv]);
-        a.nSteps = S->nSteps;
-        a.maxLocal = S->maxLocal;
-        a.stepStart = S->stepStart.p;
-        a.item = S->item.p;
-        a.entAddr = S->entAddr.p;
-        a.localPos = S->localPos.p;
-        a.localCount = S->localCount.p;
+        const T* b;
+        T* psi;
         if (sizeof(T) == 8)
         {
-            a.b = reinterpret_cast<const T*>(lv == 0 ? A.rA.p : A.v64.src[lv - 1].p);
-            a.psi = reinterpret_cast<T*>(lv == 0 ? A.wA.p : A.v64.corr[lv - 1].p);
+            b = reinterpret_cast<const T*>(lv == 0 ? A.rA.p : A.v64.src[lv - 1].p);
+            psi = reinterpret_cast<T*>(lv == 0 ? A.wA.p : A.v64.corr[lv - 1].p);
         }
         else
         {
-            a.b = reinterpret_cast<const T*>(lv == 0 ? A.r32.p : A.v32.src[lv - 1].p);
-            a.psi = reinterpret_cast<T*>(lv == 0 ? A.w32.p : A.v32.corr[lv - 1].p);
+            b = reinterpret_cast<const T*>(lv == 0 ? A.r32.p : A.v32.src[lv - 1].p);
+            psi = reinterpret_cast<T*>(lv == 0 ? A.w32.p : A.v32.corr[lv - 1].p);
         }
-        table.push_back(a);
+        table.push_back(A.pipeArgs<T>(lv, *S, psi, b));
         caseOf.push_back(c);
         small[c] = 1;
-        P.smem = std::max(P.smem, sizeof(T) * static_cast<size_t>(S->maxLocal));
+        P.smem = std::max(P.smem, pipeSmemBytes(*S, sizeof(T)));
     }
     std::vector<int4> big;
     for (const int4& q : B.hostParts)
@@ -1533,9 +1570,12 @@ void Batch::solve(const b2g_controls& c, const double* const* source, double* co
     while (going > 0)
     {
         // one captured graph per controls and reduction order
-        std::vector<unsigned char> key(sizeof(b2g_controls) + 1);
+        std::vector<unsigned char> key(sizeof(b2g_controls) + 1 + sizeof(unsigned long long));
         std::memcpy(key.data(), &c, sizeof(b2g_controls));
-        key[sizeof(b2g_controls)] = static_cast<unsigned char>((serial ? 1 : 0) | (denseNow ? 2 : 0) | (pipeOn ? 4 : 0) | (denseAll ? 8 : 0));
+        key[sizeof(b2g_controls)] = static_cast<unsigned char>((serial ? 1 : 0) | (denseNow ? 2 : 0) | (pipeOn ? 4 : 0) |
+                                                               (denseAll ? 8 : 0) | (multicolour ? 16 : 0));
+        const unsigned long long fp = layoutFingerprint();
+        std::memcpy(key.data() + sizeof(b2g_controls) + 1, &fp, sizeof(fp));
         if (eagerIterations == 0 && (!graph.exec || graph.key != key))
         {
             // a batch's first iteration runs as plain launches: capturing pays off only from the

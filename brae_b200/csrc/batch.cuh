@@ -135,6 +135,7 @@ struct Batch
     bool denseAll = false;                  // every case has its dense factor for the current values
     bool denseAny = false;                  // some case has its dense factor
     void prepareDense();
+    unsigned long long layoutFingerprint() const;
     template <class T> void preparePipe(int lv, int nSweeps);
     void preparePipes(const b2g_controls& c);
     bool pipeOn = false;                    // the current solve takes the batched pipelined sweeps

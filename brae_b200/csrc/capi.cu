@@ -844,8 +844,9 @@ b2g_status b2g_level_smooth_pipelined(b2g_matrix* m, int level, double* psi, con
         need(m && psi && source, "b2g_level_smooth_pipelined: null argument");
         need(level >= 0 && level <= m->mat->nLevels(), "b2g_level_smooth_pipelined: level out of range");
         need(nSweeps >= 1, "b2g_level_smooth_pipelined: nSweeps must be positive");
-        need(ranks == 1 || ranks == 2 || ranks == 4 || ranks == 8 || ranks == 16 || ranks == -1,
-             "b2g_level_smooth_pipelined: ranks is 1, 2, 4, 8, 16 or -1 (the item schedule)");
+        need(ranks == 1 || ranks == 2 || ranks == 4 || ranks == 8 || ranks == 16 || ranks == -1 || ranks > 16,
+             "b2g_level_smooth_pipelined: ranks is 1, 2, 4, 8, 16, above 16 (the grid form) or -1 (the item "
+             "schedule)");
         b2g::Matrix& A = *m->mat;
         need(!A.coupled, "b2g_level_smooth_pipelined: not for a coupled matrix");
         A.toPos(level, static_cast<const double*>(psi), A.ioBuf(0));
@@ -881,7 +882,8 @@ b2g_status b2g_coarsest_dense_solve(b2g_matrix* m, double* psi, const double* so
 }
 
 b2g_status b2g_level_pipe_shape(const b2g_mesh* mesh, int level, int nSweeps, int valueBytes, int* ranks,
-                                int* nSteps, float* msPipe, float* msSweeps, float* msShared, float* msItems)
+                                int* nSteps, float* msPipe, float* msSweeps, float* msShared, float* msItems,
+                                float* msGrid, int* gridForm)
 {
     return guarded([&] {
         need(mesh != nullptr, "b2g_level_pipe_shape: null mesh");
@@ -894,7 +896,11 @@ b2g_status b2g_level_pipe_shape(const b2g_mesh* mesh, int level, int nSweeps, in
         if (ranks) *ranks = mode == 1 ? it->second.sched->ranks : mode == 2 ? -it->second.items->nParts : 0;
         if (nSteps)
             *nSteps = mode == 1 ? it->second.sched->nSteps : mode == 2 ? it->second.items->maxDepth + 1 : 0;
-        if (msPipe) *msPipe = !have ? 0.f : mode == 2 ? it->second.msItems : it->second.msPipe;
+        const bool grid = mode == 1 && it->second.sched->grid;
+        if (msPipe)
+            *msPipe = !have ? 0.f : mode == 2 ? it->second.msItems : grid ? it->second.msGrid : it->second.msPipe;
+        if (msGrid) *msGrid = have ? it->second.msGrid : 0.f;
+        if (gridForm) *gridForm = grid ? 1 : 0;
         if (msSweeps) *msSweeps = have ? it->second.msSweeps : 0.f;
         if (msShared) *msShared = have ? it->second.msPipe : 0.f;
         if (msItems) *msItems = have ? it->second.msItems : 0.f;
@@ -1244,7 +1250,8 @@ b2g_status b2g_matrix_level_timings(const b2g_matrix* m, int kind, int capacity,
 {
     return guarded([&] {
         need(m != nullptr, "b2g_matrix_level_timings: null matrix");
-        need(kind == 0 || kind == 1, "b2g_matrix_level_timings: kind is 0 (Amul) or 1 (smoothing)");
+        need(kind >= 0 && kind <= 2,
+             "b2g_matrix_level_timings: kind is 0 (Amul), 1 (smoothing) or 2 (Amul fused with another step)");
         const b2g::Matrix& A = *m->mat;
         const int have = static_cast<int>(A.lvMs[kind].size());
         if (nLevels) *nLevels = have;

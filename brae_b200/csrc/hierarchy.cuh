@@ -64,30 +64,47 @@ constexpr int kEllMinCells = 65536;
 
 // One smoothing call's sweeps of a level in one pipelined launch (pipe_kernels.cuh), for a given
 // sweep count: the combined steps of every (sweep, cell) item, the cells split into `ranks`
-// contiguous ranges held in the shared memory of one CTA each (one cluster when ranks > 1).
+// contiguous ranges held in the shared memory of one CTA each (one cluster when ranks > 1), or, in
+// the grid form, owned by one of `ranks` resident CTAs with psi in global memory.
 struct PipeSchedule
 {
     int sweeps = 0;
     int ranks = 0;
     int nSteps = 0;
-    int maxLocal = 0;           // shared-memory slots per rank
+    int maxLocal = 0;           // shared-memory slots per rank (0 in the grid form)
     DBuf<int> stepStart;        // [ranks][nSteps + 1] item ranges
-    DBuf<int4> item;            // [sweeps * nCells] {position, local slot, first entry, end entry}
+    DBuf<int4> item;            // [sweeps * nCells] {position, value slot, first entry, end entry}
     DBuf<unsigned> entAddr;     // [2 * nFaces] per position-order row entry: rank << 24 | slot
     DBuf<int> localPos;         // [ranks][maxLocal] position of each slot
     DBuf<int> localCount;       // [ranks]
+    // the grid form: a row's value slot is its position and it reads psi at the level's columns; each
+    // rank waits for its neighbour ranks only
+    bool grid = false;
+    DBuf<int> nbrStart;         // [ranks + 1]
+    DBuf<int> nbrList;
+    DBuf<unsigned> progress;    // [ranks][kProgressStride]
 };
 
+// The dynamic shared memory of a pipelined launch in values of valueBytes: the rank's slots, then its
+// step table.
+inline size_t pipeSmemBytes(const PipeSchedule& P, size_t valueBytes)
+{
+    if (P.grid) return sizeof(int) * (P.nSteps + 1);
+    return ((valueBytes * static_cast<size_t>(P.maxLocal) + 15) / 16) * 16 + sizeof(int) * (P.nSteps + 1);
+}
+
 // The choice for one (level, sweep count, value type), by measurement (Matrix::ensurePipe): the
-// pipelined launch with the fastest rank count, or the sweep-by-sweep launches when those are faster.
+// pipelined launch with the fastest shape (shared memory on 1-16 CTAs, or the grid form), the item
+// schedule, or the sweep-by-sweep launches when those are faster.
 struct PipeChoice
 {
-    int mode = 0;                        // 0 sweep by sweep, 1 the shared-memory launch, 2 items
-    std::unique_ptr<PipeSchedule> sched; // mode 1
+    int mode = 0;                        // 0 sweep by sweep, 1 the pipelined launch, 2 items
+    std::unique_ptr<PipeSchedule> sched; // mode 1 (shared memory, or the grid form)
     std::unique_ptr<GsSchedule> items;   // mode 2: the multi-part sweep over (sweep, cell) items
     float msPipe = 0.f;   // per smoothing call, the best shared-memory shape (0: none fits)
     float msItems = 0.f;  // per smoothing call, the item schedule (0: not built)
     float msSweeps = 0.f; // per smoothing call, sweep by sweep
+    float msGrid = 0.f;   // per smoothing call, the best grid form (0: not tried)
 };
 
 struct LevelAddr;

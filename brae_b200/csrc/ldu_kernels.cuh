@@ -62,12 +62,15 @@ __device__ __forceinline__ T rowFold(const Rows<T>& A, int c, T acc, F term)
         const int sl = c >> 5, lane = c & 31;
         const int b0 = A.ellBase[sl];
         const int w = (A.ellBase[sl + 1] - b0) >> 5;
+        // no early exit: the padding entries (column -1) are all past the row's end and skipped,
+        // and without a data-dependent branch the loads of several entries are in flight at once
+#pragma unroll 4
         for (int q = 0; q < w; ++q)
         {
             const int e = b0 + 32 * q + lane;
             const int cp = A.ellCol[e];
-            if (cp < 0) break;
-            acc = term(acc, A.ellVal[e], cp);
+            const T v = A.ellVal[e];
+            if (cp >= 0) acc = term(acc, v, cp);
         }
         return acc;
     }

@@ -66,10 +66,10 @@ std::vector<int> combinedSteps(const LevelHost& H, int S, int& nSteps)
 
 // The schedule for R ranks, or null when a rank's slots do not fit the shared memory.
 std::unique_ptr<PipeSchedule> assemble(const LevelHost& H, const std::vector<int>& T, int S, int nSteps, int R,
-                                       size_t valueBytes, cudaStream_t s)
+                                       size_t valueBytes, cudaStream_t s, bool grid = false)
 {
     const int n = H.n;
-    if (n == 0 || R < 1 || R > k::kPipeMaxRanks) return nullptr;
+    if (n == 0 || R < 1 || (!grid && R > k::kPipeMaxRanks)) return nullptr;
     // ranks: contiguous cell ranges; slots: a rank's cells in position order
     std::vector<int> rankOf(n), slotOf(n), count(R, 0);
     for (int c = 0; c < n; ++c) rankOf[c] = static_cast<int>(static_cast<long long>(c) * R / n);
@@ -78,14 +78,20 @@ std::unique_ptr<PipeSchedule> assemble(const LevelHost& H, const std::vector<int
         const int c = H.posCell[p];
         slotOf[c] = count[rankOf[c]]++;
     }
-    const int maxLocal = *std::max_element(count.begin(), count.end());
+    const int maxLocal = grid ? 0 : *std::max_element(count.begin(), count.end());
     if (static_cast<size_t>(maxLocal) * valueBytes > kPipeSmemCap || maxLocal >= (1 << 24)) return nullptr;
-    std::vector<int> localPos(static_cast<size_t>(R) * maxLocal, 0);
-    for (int p = 0; p < n; ++p)
-    {
-        const int c = H.posCell[p];
-        localPos[static_cast<size_t>(rankOf[c]) * maxLocal + slotOf[c]] = p;
-    }
+    std::vector<int> localPos(std::max<size_t>(static_cast<size_t>(R) * maxLocal, 1), 0);
+    if (!grid)
+        for (int p = 0; p < n; ++p)
+        {
+            const int c = H.posCell[p];
+            localPos[static_cast<size_t>(rankOf[c]) * maxLocal + slotOf[c]] = p;
+        }
+    if (((valueBytes * static_cast<size_t>(maxLocal) + 15) / 16) * 16 + sizeof(int) * (nSteps + 1) > kPipeSmemCap)
+        return nullptr;
+    // the grid form: a value is named by its position, and a row's value slot is its position
+    if (grid)
+        for (int p = 0; p < n; ++p) slotOf[H.posCell[p]] = p;
     // items, rank-major then by step, in position order within a (rank, step)
     const size_t stride = static_cast<size_t>(nSteps) + 1;
     std::vector<int> start(static_cast<size_t>(R) * stride + 1, 0);
@@ -108,11 +114,15 @@ std::unique_ptr<PipeSchedule> assemble(const LevelHost& H, const std::vector<int
     std::vector<int> stepStart(static_cast<size_t>(R) * stride);
     for (int r = 0; r < R; ++r)
         for (size_t t = 0; t < stride; ++t) stepStart[r * stride + t] = start[r * stride + t];
-    std::vector<unsigned> entAddr(H.entColPos.size());
-    for (size_t e = 0; e < entAddr.size(); ++e)
+    std::vector<unsigned> entAddr;
+    if (!grid)
     {
-        const int c = H.posCell[H.entColPos[e]];
-        entAddr[e] = static_cast<unsigned>(rankOf[c]) << 24 | static_cast<unsigned>(slotOf[c]);
+        entAddr.resize(H.entColPos.size());
+        for (size_t e = 0; e < entAddr.size(); ++e)
+        {
+            const int c = H.posCell[H.entColPos[e]];
+            entAddr[e] = static_cast<unsigned>(rankOf[c]) << 24 | static_cast<unsigned>(slotOf[c]);
+        }
     }
     auto P = std::make_unique<PipeSchedule>();
     P->sweeps = S;
@@ -121,9 +131,33 @@ std::unique_ptr<PipeSchedule> assemble(const LevelHost& H, const std::vector<int
     P->maxLocal = maxLocal;
     P->stepStart.upload(stepStart.data(), stepStart.size(), s);
     P->item.upload(item.data(), item.size(), s);
-    P->entAddr.upload(entAddr.data(), std::max<size_t>(entAddr.size(), 1), s);
+    if (!grid) P->entAddr.upload(entAddr.data(), std::max<size_t>(entAddr.size(), 1), s);
     P->localPos.upload(localPos.data(), localPos.size(), s);
     P->localCount.upload(count.data(), count.size(), s);
+    if (grid)
+    {
+        // each rank's neighbour ranks: the other ends of its cells' faces
+        std::vector<std::vector<int>> nb(R);
+        for (int f = 0; f < H.nF; ++f)
+        {
+            const int a = rankOf[H.lower[f]], b = rankOf[H.upper[f]];
+            if (a == b) continue;
+            nb[a].push_back(b);
+            nb[b].push_back(a);
+        }
+        std::vector<int> nbrStart(static_cast<size_t>(R) + 1, 0), nbrList;
+        for (int r = 0; r < R; ++r)
+        {
+            std::sort(nb[r].begin(), nb[r].end());
+            nb[r].erase(std::unique(nb[r].begin(), nb[r].end()), nb[r].end());
+            nbrList.insert(nbrList.end(), nb[r].begin(), nb[r].end());
+            nbrStart[r + 1] = static_cast<int>(nbrList.size());
+        }
+        P->grid = true;
+        P->nbrStart.upload(nbrStart.data(), nbrStart.size(), s);
+        P->nbrList.upload(nbrList.data(), std::max<size_t>(nbrList.size(), 1), s);
+        P->progress.alloc(static_cast<size_t>(R) * k::kProgressStride, s);
+    }
     B2G_CUDA(cudaStreamSynchronize(s));  // the host vectors go out of scope
     return P;
 }
@@ -181,16 +215,39 @@ bool pipeClusterFits(int ranks, size_t smem, cudaStream_t s)
     return n >= 1;
 }
 
+// Whether `ranks` CTAs of the grid form can all be resident (its launch is cooperative).
+template <class T>
+bool pipeGridFits(int ranks, size_t smem)
+{
+    if (smem > 48 * 1024) return false;
+    int dev = 0, sms = 0, perSm = 0;
+    B2G_CUDA(cudaGetDevice(&dev));
+    B2G_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k::gsPipeGrid<T>, k::kPipeGridBlock, smem) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return false;
+    }
+    return ranks <= perSm * sms;
+}
+
+int smCount()
+{
+    int dev = 0, sms = 0;
+    B2G_CUDA(cudaGetDevice(&dev));
+    B2G_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    return sms;
+}
+
 int pipeKey(int sweeps, size_t valueBytes) { return sweeps * 16 + static_cast<int>(valueBytes); }
 
 }  // namespace
 
 template <class T>
-void Matrix::pipeLaunch(int level, const PipeSchedule& P, T* psiL, const T* src)
+k::PipeArgs<T> Matrix::pipeArgs(int level, const PipeSchedule& P, T* psiL, const T* src)
 {
-    const LevelAddr& L = mesh->lev[level];
     k::PipeArgs<T> a;
-    a.A = rowsOf(L, data<T>().coef[level]);
+    a.A = rowsOf(mesh->lev[level], data<T>().coef[level]);
     a.nSteps = P.nSteps;
     a.maxLocal = P.maxLocal;
     a.stepStart = P.stepStart.p;
@@ -200,7 +257,37 @@ void Matrix::pipeLaunch(int level, const PipeSchedule& P, T* psiL, const T* src)
     a.localCount = P.localCount.p;
     a.b = src;
     a.psi = psiL;
-    const size_t smem = sizeof(T) * static_cast<size_t>(P.maxLocal);
+    return a;
+}
+
+template <class T>
+void Matrix::pipeLaunch(int level, const PipeSchedule& P, T* psiL, const T* src)
+{
+    const k::PipeArgs<T> a = pipeArgs<T>(level, P, psiL, src);
+    const size_t smem = pipeSmemBytes(P, sizeof(T));
+    if (P.grid)
+    {
+        k::PipeGridSync g;
+        g.progress = P.progress.p;
+        g.nbrStart = P.nbrStart.p;
+        g.nbrList = P.nbrList.p;
+        g.spinLimit = spinLimit;
+        g.err = err.p;
+        B2G_CUDA(cudaMemsetAsync(P.progress.p, 0, P.progress.bytes(), stream));
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(static_cast<unsigned>(P.ranks));
+        cfg.blockDim = dim3(k::kPipeGridBlock);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = stream;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        B2G_CUDA(cudaLaunchKernelEx(&cfg, k::gsPipeGrid<T>, a, g));
+        launches += 2;
+        return;
+    }
     if (P.ranks == 1)
     {
         k::gsPipe<T, false><<<1, k::kPipeBlock, smem, stream>>>(a);
@@ -347,7 +434,7 @@ void Matrix::ensurePipe(int level, int nSweeps)
         {
             std::unique_ptr<PipeSchedule> P = assemble(H, Tsteps, nSweeps, nSteps, R, sizeof(T), stream);
             if (!P) continue;
-            if (R > 1 && !pipeClusterFits<T>(R, sizeof(T) * static_cast<size_t>(P->maxLocal), stream)) continue;
+            if (R > 1 && !pipeClusterFits<T>(R, pipeSmemBytes(*P, sizeof(T)), stream)) continue;
             const float ms = timeIt([&] { pipeLaunch<T>(level, *P, x.p, b.p); });
             if (C.msPipe == 0.f || ms < C.msPipe) C.msPipe = ms;
             if (ms < best)
@@ -360,6 +447,36 @@ void Matrix::ensurePipe(int level, int nSweeps)
     }
     if (L.gs.nParts > 1)
     {
+        // the grid form: one CTA per SM, or per two
+        const LevelHost H = download(L, stream);
+        int nSteps = 0;
+        const std::vector<int> Tsteps = combinedSteps(H, nSweeps, nSteps);
+        const int sms = smCount();
+        for (int R : {sms, sms / 2})
+        {
+            if (R < 2 || R > L.nCells) continue;
+            std::unique_ptr<PipeSchedule> P = assemble(H, Tsteps, nSweeps, nSteps, R, sizeof(T), stream, true);
+            if (!P || !pipeGridFits<T>(R, pipeSmemBytes(*P, sizeof(T)))) continue;
+            float ms = 0.f;
+            try
+            {
+                ms = timeIt([&] { pipeLaunch<T>(level, *P, x.p, b.p); });
+                checkDeviceError();
+            }
+            catch (const Error&)
+            {
+                // a cooperative launch of that many CTAs refused here
+                cudaGetLastError();
+                continue;
+            }
+            if (C.msGrid == 0.f || ms < C.msGrid) C.msGrid = ms;
+            if (ms < best)
+            {
+                best = ms;
+                C.sched = std::move(P);
+                C.mode = 1;
+            }
+        }
         std::unique_ptr<GsSchedule> G = buildGsItems(L, nSweeps, stream);
         float ms = 0.f;
         if (G)
@@ -407,7 +524,10 @@ void Matrix::refreshItems()
 {
     for (int lv = 0; lv <= nLevels(); ++lv)
         for (auto& kv : mesh->lev[lv].pipe)
-            if (kv.second.mode == 2 && kv.first % 16 == static_cast<int>(sizeof(T))) itemBuffers<T>(lv, *kv.second.items);
+        {
+            if (kv.first % 16 != static_cast<int>(sizeof(T))) continue;
+            if (kv.second.mode == 2) itemBuffers<T>(lv, *kv.second.items);
+        }
 }
 
 // nSweeps sweeps of `level` in one pipelined launch when the level's tuned choice says so; false
@@ -461,11 +581,15 @@ bool Matrix::pipeForced(int level, T* psiL, const T* src, int nSweeps, int ranks
     const LevelHost H = download(L, stream);
     int nSteps = 0;
     const std::vector<int> Tsteps = combinedSteps(H, nSweeps, nSteps);
-    std::unique_ptr<PipeSchedule> P = assemble(H, Tsteps, nSweeps, nSteps, ranks, sizeof(T), stream);
+    const bool grid = ranks > k::kPipeMaxRanks;
+    if (grid && ranks > L.nCells) return false;
+    std::unique_ptr<PipeSchedule> P = assemble(H, Tsteps, nSweeps, nSteps, ranks, sizeof(T), stream, grid);
     if (!P) return false;
-    if (ranks > 1 && !pipeClusterFits<T>(ranks, sizeof(T) * static_cast<size_t>(P->maxLocal), stream)) return false;
+    if (grid && !pipeGridFits<T>(ranks, pipeSmemBytes(*P, sizeof(T)))) return false;
+    if (!grid && ranks > 1 && !pipeClusterFits<T>(ranks, pipeSmemBytes(*P, sizeof(T)), stream)) return false;
     pipeLaunch<T>(level, *P, psiL, src);
     B2G_CUDA(cudaStreamSynchronize(stream));  // P is released on return
+    checkDeviceError();
     return true;
 }
 
@@ -514,6 +638,8 @@ template bool Matrix::pipeSweeps<float>(int, float*, const float*, int);
 template void Matrix::pipeLaunch<double>(int, const PipeSchedule&, double*, const double*);
 template void Matrix::pipeLaunch<float>(int, const PipeSchedule&, float*, const float*);
 template void Matrix::refreshItems<double>();
+template k::PipeArgs<double> Matrix::pipeArgs<double>(int, const PipeSchedule&, double*, const double*);
+template k::PipeArgs<float> Matrix::pipeArgs<float>(int, const PipeSchedule&, float*, const float*);
 template void Matrix::refreshItems<float>();
 template void Matrix::itemsLaunch<double>(int, const GsSchedule&, double*, const double*);
 

@@ -20,48 +20,81 @@
 // on the R CTAs of a thread-block cluster (R <= 16), each holding the cells of one contiguous cell
 // range ("rank"). A row reads its values from the CTA that owns each one (distributed shared memory
 // for another rank's), each thread computes its items of the step, and a barrier over the CTA (R = 1)
-// or the cluster (release / acquire at cluster scope) separates the steps. Row data do not depend on
-// psi: each thread loads its next step's row into registers, and the item after it, before it
-// computes the current one, so the chain per step is the shared-memory reads, the arithmetic and the
-// barrier. Every CTA runs the same number of barriers and no data-dependent wait: the launch cannot
-// stall (the CTAs of a cluster are resident together).
+// or the cluster (release / acquire at cluster scope) separates the steps. Every CTA runs the same
+// number of barriers and no data-dependent wait: the launch cannot stall (the CTAs of a cluster are
+// resident together).
+//
+// THE GRID FORM (gsPipeGrid, levels too large for one cluster's shared memory): psi stays in global
+// memory (L2), R CTAs -- all resident, the launch is cooperative -- own one contiguous cell range
+// each, and after its items of step T a CTA publishes T + 1 (a release at GPU scope). Before step T
+// a CTA waits until every NEIGHBOUR rank -- one owning a cell that shares a face with one of its
+// cells -- has published T. That suffices both ways: every value a row of step T reads was written
+// at an earlier step by its own rank or a neighbour (read after write), and every later overwrite of
+// a value read at step T happens at a later step of a neighbour, which waits for this rank's step T
+// first (write after read). Each wait has an iteration limit; when one runs out the error word is
+// set, every CTA leaves, and the call reports a timeout.
+//
+// THE ROWS. An item is {position, value slot, first and end row entry}: the row is read in place
+// from the level's position-order rows (no copy per sweep, so a level's rows stay in L2). Row data do
+// not depend on psi, so they are loaded ahead: a thread loads its item record two steps ahead and its
+// row one step ahead, and no step waits on a load chain -- the chain per step is the value reads,
+// the arithmetic and the barrier. A warp's loops run to the widest row among its lanes (a warp-wide
+// maximum), each lane adding only its own row's entries.
 #pragma once
 
 #include "b2g_common.cuh"
+#include "gs_kernels.cuh"
 #include "ldu_kernels.cuh"
 
 namespace b2g {
 namespace k {
 
-constexpr int kPipeK = 16;        // row entries a thread holds in registers
-constexpr int kPipeBlock = 256;   // threads per CTA
+constexpr int kPipeK = 16;        // row entries a thread holds in registers (shared-memory forms)
+constexpr int kPipeGridK = 8;     // the same in the grid form (its 384 threads have fewer registers)
+constexpr int kPipeBlock = 256;   // threads per CTA (shared-memory forms)
+constexpr int kPipeWarps = kPipeBlock / 32;
+constexpr int kPipeGridBlock = 384;
 constexpr int kPipeMaxRanks = 16;
 
 template <class T>
 struct PipeArgs
 {
-    Rows<T> A;                          // the level's position-order rows (diag, rowStart, val)
+    Rows<T> A;                          // the level's position-order rows (diag, val; col = the other
+                                        // cell's position, which the grid form reads psi at)
     int nSteps;
-    int maxLocal;                       // shared-memory slots per rank
+    int maxLocal;                       // shared-memory slots per rank (0 in the grid form)
     const int* __restrict__ stepStart;  // [ranks][nSteps + 1] item ranges of each rank per step
-    const int4* __restrict__ item;      // {position, local slot, first entry, end entry}
+    const int4* __restrict__ item;      // {position, value slot, first entry, end entry}
     const unsigned* __restrict__ entAddr;   // per row entry: owner rank << 24 | local slot of its value
+                                            // (the shared-memory forms)
     const int* __restrict__ localPos;   // [ranks][maxLocal] position of each local slot
     const int* __restrict__ localCount; // [ranks]
     const T* __restrict__ b;            // by position
     T* psi;                             // by position
 };
 
-template <class T>
+// The grid form's synchronisation.
+struct PipeGridSync
+{
+    unsigned* progress;                 // [ranks][kProgressStride]: word 0 = the steps the rank has done
+    const int* __restrict__ nbrStart;   // [ranks + 1] each rank's neighbour ranks in nbrList
+    const int* __restrict__ nbrList;
+    long long spinLimit;                // polls before a wait gives up
+    int* err;                           // set to 1 when a wait gives up
+};
+
+template <class T, int K>
 struct PipeRow
 {
-    int slot;   // -1: no item for this thread at this step
-    int w;      // entries
+    int slot;   // -1: no item for this thread
+    int w;      // the row's entries
+    int wq;     // the widest row of the warp (warp-uniform)
     int e0;
     T b, d;
-    T v[kPipeK];
-    unsigned ea[kPipeK];  // each entry's value: owner rank << 24 | slot (turned into an address at use,
-                          // so that loading the next step's row never waits for its loads)
+    T v[K];
+    unsigned ea[K];  // each entry's value: owner rank << 24 | slot, or its position in the grid form
+                     // (turned into an address at use, so that loading the next step's row never
+                     // waits for its loads)
 };
 
 __device__ __forceinline__ unsigned pipeSmemAddr(const void* p)
@@ -98,6 +131,19 @@ __device__ __forceinline__ float pipeLd(unsigned a, float)
 }
 __device__ __forceinline__ void pipeSt(unsigned a, double v) { asm volatile("st.shared.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory"); }
 __device__ __forceinline__ void pipeSt(unsigned a, float v) { asm volatile("st.shared.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory"); }
+// psi in the grid form: coherent at GPU scope (another SM wrote it; not from a stale L1 line)
+__device__ __forceinline__ double gridLd(const double* p)
+{
+    double v;
+    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ float gridLd(const float* p)
+{
+    float v;
+    asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
+    return v;
+}
 
 template <bool kCluster>
 __device__ __forceinline__ void pipeBarrier()
@@ -122,59 +168,101 @@ __device__ __forceinline__ unsigned pipeAddr(unsigned ea, unsigned xa)
     return kCluster ? mapaCluster(local, ea >> 24) : local;
 }
 
-// a row's loads once its item is known (they wait for no load of their own)
-template <class T>
-__device__ __forceinline__ void pipeLoadRow(const PipeArgs<T>& a, const int4& it, bool has, PipeRow<T>& r)
+// a row's loads once its item record is known (they wait for no load of their own); every lane of
+// the warp calls it (the warp-wide width)
+template <class T, int K, bool kGrid>
+__device__ __forceinline__ void pipeLoadRow(const PipeArgs<T>& a, int4 it, bool has, PipeRow<T, K>& r)
 {
-    r.slot = -1;
-    r.w = 0;
-    if (!has) return;
-    r.slot = it.y;
+    r.slot = has ? it.y : -1;
+    r.w = has ? it.w - it.z : 0;
     r.e0 = it.z;
-    r.w = it.w - it.z;
+    r.wq = __reduce_max_sync(0xffffffffu, r.w);
+    if (!has) return;
     r.b = a.b[it.x];
     r.d = a.A.diag[it.x];
 #pragma unroll
-    for (int q = 0; q < kPipeK; ++q)
-        if (q < r.w)
+    for (int k = 0; k < K; ++k)
+    {
+        if (k >= r.wq) break;
+        if (k < r.w)
         {
-            r.v[q] = a.A.val[it.z + q];
-            r.ea[q] = a.entAddr[it.z + q];
+            r.v[k] = a.A.val[it.z + k];
+            r.ea[k] = kGrid ? static_cast<unsigned>(a.A.col[it.z + k]) : a.entAddr[it.z + k];
         }
-}
-
-template <class T>
-__device__ __forceinline__ void pipeLoad(const PipeArgs<T>& a, int k, PipeRow<T>& r)
-{
-    const int4 it = k >= 0 ? a.item[k] : make_int4(0, -1, 0, 0);
-    pipeLoadRow(a, it, k >= 0, r);
+    }
 }
 
 // the row in the reference's order: the source minus each entry's coefficient times its value, then
-// the division by the diagonal
+// the division by the diagonal (the shared-memory forms)
 template <class T, bool kCluster>
-__device__ __forceinline__ void pipeRow(const PipeArgs<T>& a, const PipeRow<T>& r, unsigned xa)
+__device__ __forceinline__ void pipeRow(const PipeArgs<T>& a, const PipeRow<T, kPipeK>& r, unsigned xa)
 {
     T x[kPipeK];
 #pragma unroll
-    for (int q = 0; q < kPipeK; ++q)
-        if (q < r.w) x[q] = pipeLd<kCluster>(pipeAddr<T, kCluster>(r.ea[q], xa), T());
+    for (int k = 0; k < kPipeK; ++k)
+    {
+        if (k >= r.wq) break;
+        if (k < r.w) x[k] = pipeLd<kCluster>(pipeAddr<T, kCluster>(r.ea[k], xa), T());
+    }
     T acc = r.b;
 #pragma unroll
-    for (int q = 0; q < kPipeK; ++q)
-        if (q < r.w) acc = subRn(acc, mulRn(r.v[q], x[q]));
-    for (int q = kPipeK; q < r.w; ++q)
-        acc = subRn(acc, mulRn(a.A.val[r.e0 + q], pipeLd<kCluster>(pipeAddr<T, kCluster>(a.entAddr[r.e0 + q], xa), T())));
+    for (int k = 0; k < kPipeK; ++k)
+    {
+        if (k >= r.wq) break;
+        if (k < r.w) acc = subRn(acc, mulRn(r.v[k], x[k]));
+    }
+    for (int k = kPipeK; k < r.w; ++k)
+        acc = subRn(acc, mulRn(a.A.val[r.e0 + k], pipeLd<kCluster>(pipeAddr<T, kCluster>(a.entAddr[r.e0 + k], xa), T())));
     pipeSt(xa + static_cast<unsigned>(sizeof(T)) * static_cast<unsigned>(r.slot), divRn(acc, r.d));
 }
 
+// the same row in the grid form: values from psi in global memory, the result stored there
+template <class T>
+__device__ __forceinline__ void pipeRowGrid(const PipeArgs<T>& a, const PipeRow<T, kPipeGridK>& r)
+{
+    T x[kPipeGridK];
+#pragma unroll
+    for (int k = 0; k < kPipeGridK; ++k)
+    {
+        if (k >= r.wq) break;
+        if (k < r.w) x[k] = gridLd(a.psi + r.ea[k]);
+    }
+    T acc = r.b;
+#pragma unroll
+    for (int k = 0; k < kPipeGridK; ++k)
+    {
+        if (k >= r.wq) break;
+        if (k < r.w) acc = subRn(acc, mulRn(r.v[k], x[k]));
+    }
+    for (int k = kPipeGridK; k < r.w; ++k) acc = subRn(acc, mulRn(a.A.val[r.e0 + k], gridLd(a.psi + a.A.col[r.e0 + k])));
+    a.psi[r.slot] = divRn(acc, r.d);
+}
+
+// A row straight from memory (the items beyond the block's width at a step: rare, so not staged)
+template <class T, bool kCluster>
+__device__ __forceinline__ void pipeRowDirect(const PipeArgs<T>& a, int4 it, unsigned xa)
+{
+    T acc = a.b[it.x];
+    for (int e = it.z; e < it.w; ++e)
+        acc = subRn(acc, mulRn(a.A.val[e], pipeLd<kCluster>(pipeAddr<T, kCluster>(a.entAddr[e], xa), T())));
+    pipeSt(xa + static_cast<unsigned>(sizeof(T)) * static_cast<unsigned>(it.y), divRn(acc, a.A.diag[it.x]));
+}
+template <class T>
+__device__ __forceinline__ void pipeRowGridDirect(const PipeArgs<T>& a, int4 it)
+{
+    T acc = a.b[it.x];
+    for (int e = it.z; e < it.w; ++e) acc = subRn(acc, mulRn(a.A.val[e], gridLd(a.psi + a.A.col[e])));
+    a.psi[it.y] = divRn(acc, a.A.diag[it.x]);
+}
+
 // One smoothing call (all its sweeps) of one level. Grid = one cluster of R CTAs (kCluster) or one
-// CTA; dynamic shared memory = maxLocal values of T.
+// CTA; dynamic shared memory = pipeSmemBytes (the rank's slots, then its step table).
 template <class T, bool kCluster>
 __device__ __forceinline__ void gsPipeBody(const PipeArgs<T>& a)
 {
     extern __shared__ __align__(16) unsigned char pipeSm[];
     T* x = reinterpret_cast<T*>(pipeSm);
+    int* ss = reinterpret_cast<int*>(pipeSm + ((sizeof(T) * static_cast<size_t>(a.maxLocal) + 15) / 16) * 16);
     const int rank = kCluster ? static_cast<int>(clusterRank()) : 0;
     const int t = threadIdx.x;
     const int B = blockDim.x;
@@ -182,34 +270,37 @@ __device__ __forceinline__ void gsPipeBody(const PipeArgs<T>& a)
     const int cnt = a.localCount[rank];
     const int* lp = a.localPos + static_cast<size_t>(rank) * a.maxLocal;
     for (int i = t; i < cnt; i += B) x[i] = a.psi[lp[i]];
+    const int* gss = a.stepStart + static_cast<size_t>(rank) * (a.nSteps + 1);
+    for (int i = t; i <= a.nSteps; i += B) ss[i] = gss[i];
     // every rank's psi is in place before any row reads it
     pipeBarrier<kCluster>();
-    const int* ss = a.stepStart + static_cast<size_t>(rank) * (a.nSteps + 1);
-    // a thread's item at step T is ss[T] + t when that is below ss[T + 1]. Its item record is loaded
-    // two steps ahead and its row one step ahead, so that no step waits on a load chain: at step T
-    // the row of step T+1 is loaded from a record that arrived a step ago, while the record of step
-    // T+2 is on its way.
+    // this thread's item at step T_, or -1
     auto itemAt = [&](int T_) { return T_ < a.nSteps && ss[T_] + t < ss[T_ + 1] ? ss[T_] + t : -1; };
-    PipeRow<T> cur, nxt;
-    pipeLoad(a, a.nSteps > 0 ? itemAt(0) : -1, cur);
-    int kn = itemAt(1);
-    int4 itn = kn >= 0 ? a.item[kn] : make_int4(0, -1, 0, 0);
-    for (int T_ = 0; T_ < a.nSteps; ++T_)
-    {
-        pipeLoadRow(a, itn, kn >= 0, nxt);
-        kn = itemAt(T_ + 2);
-        if (kn >= 0) itn = a.item[kn];
+    const int4 none = make_int4(0, -1, 0, 0);
+    PipeRow<T, kPipeK> r0, r1;
+    int k1 = itemAt(0);
+    pipeLoadRow<T, kPipeK, false>(a, k1 >= 0 ? a.item[k1] : none, k1 >= 0, r0);
+    k1 = itemAt(1);
+    int4 it1 = k1 >= 0 ? a.item[k1] : none;
+    // one step: the next row's loads from its record (loaded a step ago), the record after it, this
+    // step's rows, the barrier
+    auto step = [&](int T_, const PipeRow<T, kPipeK>& cur, PipeRow<T, kPipeK>& nxt) {
+        pipeLoadRow<T, kPipeK, false>(a, it1, k1 >= 0, nxt);
+        k1 = itemAt(T_ + 2);
+        if (k1 >= 0) it1 = a.item[k1];
         if (cur.slot >= 0) pipeRow<T, kCluster>(a, cur, xa);
         // items beyond the block's width at this step, straight from memory
-        for (int k = ss[T_] + t + B; k < ss[T_ + 1]; k += B)
-        {
-            PipeRow<T> r;
-            pipeLoad(a, k, r);
-            pipeRow<T, kCluster>(a, r, xa);
-        }
+        for (int k = ss[T_] + t + B; k < ss[T_ + 1]; k += B) pipeRowDirect<T, kCluster>(a, a.item[k], xa);
         pipeBarrier<kCluster>();
-        cur = nxt;
+    };
+    // two steps per iteration, the rows alternating between r0 and r1 (no copies)
+    int T_ = 0;
+    for (; T_ + 1 < a.nSteps; T_ += 2)
+    {
+        step(T_, r0, r1);
+        step(T_ + 1, r1, r0);
     }
+    if (T_ < a.nSteps) step(T_, r0, r1);
     // the last barrier above ordered every read of this CTA's values before the write-back; no rank
     // reads another's shared memory after it, so the CTAs may leave in any order
     for (int i = t; i < cnt; i += B) a.psi[lp[i]] = x[i];
@@ -231,6 +322,70 @@ __global__ void __launch_bounds__(kPipeBlock, 1) gsPipeBatch(const PipeArgs<T>* 
     if (active && active[caseOf[blockIdx.x]] == 0) return;
     const PipeArgs<T> a = table[blockIdx.x];
     gsPipeBody<T, false>(a);
+}
+
+// One smoothing call of one level in the grid form: block r is rank r (all resident: a cooperative
+// launch); dynamic shared memory = the rank's step table. The caller zeroes the progress words.
+template <class T>
+__global__ void __launch_bounds__(kPipeGridBlock, 1) gsPipeGrid(PipeArgs<T> a, PipeGridSync g)
+{
+    extern __shared__ __align__(16) int gridSs[];
+    __shared__ int stop;
+    const int rank = blockIdx.x;
+    const int t = threadIdx.x;
+    const int B = blockDim.x;
+    const int* gss = a.stepStart + static_cast<size_t>(rank) * (a.nSteps + 1);
+    for (int i = t; i <= a.nSteps; i += B) gridSs[i] = gss[i];
+    if (t == 0) stop = 0;
+    __syncthreads();
+    const int n0 = g.nbrStart[rank], n1 = g.nbrStart[rank + 1];
+    unsigned* mine = g.progress + static_cast<size_t>(rank) * kProgressStride;
+    auto itemAt = [&](int T_) { return T_ < a.nSteps && gridSs[T_] + t < gridSs[T_ + 1] ? gridSs[T_] + t : -1; };
+    const int4 none = make_int4(0, -1, 0, 0);
+    PipeRow<T, kPipeGridK> r0, r1;
+    int k1 = itemAt(0);
+    pipeLoadRow<T, kPipeGridK, true>(a, k1 >= 0 ? a.item[k1] : none, k1 >= 0, r0);
+    k1 = itemAt(1);
+    int4 it1 = k1 >= 0 ? a.item[k1] : none;
+    // one step; false when a wait gave up (every thread of the CTA sees the same)
+    auto step = [&](int T_, const PipeRow<T, kPipeGridK>& cur, PipeRow<T, kPipeGridK>& nxt) -> bool {
+        pipeLoadRow<T, kPipeGridK, true>(a, it1, k1 >= 0, nxt);
+        k1 = itemAt(T_ + 2);
+        if (k1 >= 0) it1 = a.item[k1];
+        if (T_ > 0)
+        {
+            // every neighbour rank has done step T_ - 1
+            for (int i = n0 + t; i < n1; i += B)
+            {
+                const unsigned* w = g.progress + static_cast<size_t>(g.nbrList[i]) * kProgressStride;
+                long long spins = 0;
+                while (ldAcquire(w) < static_cast<unsigned>(T_))
+                {
+                    if (++spins > g.spinLimit || *reinterpret_cast<volatile int*>(g.err) != 0)
+                    {
+                        atomicExch(g.err, 1);
+                        stop = 1;
+                        break;
+                    }
+                }
+            }
+            __syncthreads();
+            if (stop) return false;
+        }
+        if (cur.slot >= 0) pipeRowGrid<T>(a, cur);
+        for (int k = gridSs[T_] + t + B; k < gridSs[T_ + 1]; k += B) pipeRowGridDirect<T>(a, a.item[k]);
+        // the barrier orders the CTA's psi stores before thread 0's release (release is cumulative)
+        __syncthreads();
+        if (t == 0) stRelease(mine, static_cast<unsigned>(T_ + 1));
+        return true;
+    };
+    int T_ = 0;
+    for (; T_ + 1 < a.nSteps; T_ += 2)
+    {
+        if (!step(T_, r0, r1)) return;
+        if (!step(T_ + 1, r1, r0)) return;
+    }
+    if (T_ < a.nSteps) step(T_, r0, r1);
 }
 
 }  // namespace k

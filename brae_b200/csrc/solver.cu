@@ -566,7 +566,7 @@ void Matrix::addRegion(const TimedRegion& r)
     float x = 0.f;
     B2G_CUDA(cudaEventElapsedTime(&x, r.start, r.end));
     const size_t need = static_cast<size_t>(r.level) + 1;
-    for (int k = 0; k < 2; ++k)
+    for (int k = 0; k < 3; ++k)
         if (lvMs[k].size() < need)
         {
             lvMs[k].resize(need, 0.0);
@@ -600,7 +600,7 @@ void Matrix::timingsBegin()
         counts[i] = 0;
     }
     launches = 0;
-    for (int k = 0; k < 2; ++k)
+    for (int k = 0; k < 3; ++k)
     {
         lvMs[k].clear();
         lvCalls[k].clear();
@@ -638,7 +638,7 @@ void Matrix::timingsEnd()
         }
     ms[2] = ms[3] - ms[0] - ms[1];
     long long regions = 0;
-    for (int k = 0; k < 2; ++k)
+    for (int k = 0; k < 3; ++k)
         if (!lvCalls[k].empty()) regions += lvCalls[k][0];
     counts[2] = counts[3] - regions;
 }
@@ -814,7 +814,7 @@ template <class T>
 void Matrix::residualBetween(const T* source, const T* x, T* r)
 {
     const LevelAddr& F = mesh->lev[0];
-    cudaEvent_t e = timedBegin(0, 0, 1);
+    cudaEvent_t e = timedBegin(2, 0, 1);
     k::amulSubtract<T><<<rowsGrid(F.nCells), NT, 0, stream>>>(rowsOf(F, data<T>().coef[0]), source, x, r);
     timedEnd(e);
     B2G_LAUNCH_CHECK();
@@ -1360,7 +1360,7 @@ void Matrix::scale(int level, T* field, T* Acf, const T* src)
     else
     {
         const int g = redGrid(L.nCells);
-        cudaEvent_t e = timedBegin(0, level, 1);
+        cudaEvent_t e = timedBegin(2, level, 1);
         k::amulScaleDots<T, NT><<<g, NT, 0, stream>>>(rowsOf(L, D.coef[level]), field, src, Acf, D.partial.p);
         timedEnd(e);
         k::scaleFactor<T, NT><<<1, NT, 0, stream>>>(D.partial.p, g, D.sf.p);
@@ -1582,7 +1582,7 @@ void Matrix::vcycle(const b2g_controls& c, T* x, const T* src, T* Apsi, T* fcor,
         // prolong, scale and correct without storing the prolonged correction (bit for bit the same)
         const Step& S0 = mesh->step[0];
         const int g = redGrid(F.nCells);
-        cudaEvent_t e = timedBegin(0, 0, 1);
+        cudaEvent_t e = timedBegin(2, 0, 1);
         k::amulScaleDotsProlong<T, NT><<<g, NT, 0, stream>>>(rowsOf(F, D.coef[0]), S0.prolongP.p, D.corr[0].p, fres,
                                                              Apsi, D.partial.p);
         timedEnd(e);
@@ -1609,7 +1609,7 @@ void Matrix::vcycle(const b2g_controls& c, T* x, const T* src, T* Apsi, T* fcor,
         else
         {
             const int g = redGrid(F.nCells);
-            cudaEvent_t e = timedBegin(0, 0, 1);
+            cudaEvent_t e = timedBegin(2, 0, 1);
             k::amulScaleDots<T, NT><<<g, NT, 0, stream>>>(rowsOf(F, D.coef[0]), fcor, fres, Apsi, D.partial.p);
             timedEnd(e);
             k::scaleFactor<T, NT><<<1, NT, 0, stream>>>(D.partial.p, g, D.sf.p);
@@ -1737,6 +1737,9 @@ unsigned long long Matrix::layoutFingerprint() const
     for (const auto* b : {&v64.ACf, &v64.preSmoothed, &v64.partial, &v64.sf, &v64.cpA, &v64.cwA, &v64.crA, &v64.crD})
         mix(b->p);
     for (const auto* b : {&v32.ACf, &v32.preSmoothed, &v32.partial, &v32.sf}) mix(b->p);
+    for (const auto& kv : v64.items) mix(kv.second.blob.p);
+    for (const auto& kv : v32.items) mix(kv.second.blob.p);
+    for (const void* q : {(const void*)denseL.p}) mix(q);
     return h;
 }
 

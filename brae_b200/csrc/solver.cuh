@@ -5,6 +5,7 @@
 #include "gs_kernels.cuh"
 #include "hierarchy.cuh"
 #include "ldu_kernels.cuh"
+#include "pipe_kernels.cuh"
 
 #include <map>
 
@@ -149,8 +150,9 @@ struct Matrix
     double ms[4] = {0, 0, 0, 0};              // finest Amul, finest smoothing, other, whole solve
     long long counts[4] = {0, 0, 0, 0};       // finest Amuls, finest sweeps, other launches, all launches
     long long launches = 0;
-    std::vector<double> lvMs[2];              // per kind (0 Amul, 1 smoothing) and level: milliseconds,
-    std::vector<long long> lvCalls[2], lvUnits[2];  // timed regions, units (Amuls / sweeps)
+    std::vector<double> lvMs[3];              // per kind (0 Amul, 1 smoothing, 2 Amul fused with the residual,
+                                              // the scaling or the prolongation) and level: milliseconds,
+    std::vector<long long> lvCalls[3], lvUnits[3];  // timed regions, units (Amuls / sweeps)
     std::vector<TimedRegion> evOpen;          // regions recorded outside a capture, read at the end
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evFree;
     cudaEvent_t evSolve[2] = {nullptr, nullptr};
@@ -186,6 +188,7 @@ struct Matrix
     template <class T> void ensurePipe(int level, int nSweeps);
     template <class T> bool pipeSweeps(int level, T* psi, const T* source, int nSweeps);
     template <class T> void pipeLaunch(int level, const PipeSchedule& P, T* psi, const T* source);
+    template <class T> k::PipeArgs<T> pipeArgs(int level, const PipeSchedule& P, T* psi, const T* source);
     template <class T> bool pipeForced(int level, T* psi, const T* source, int nSweeps, int ranks);
     // an item schedule's launch (items.cu): its blobs filled for the current coefficients first
     template <class T> typename VCycleData<T>::ItemBuffers& itemBuffers(int level, const GsSchedule& G);

@@ -75,7 +75,8 @@ def _load():
         "b2g_assemble_pressure": (ip, [vp] + [vp] * 6 + [ip] + [vp] * 6 + [ip, dp] + [vp] * 5 + [ip, vp]),
         "b2g_level_smooth_pipelined": (ip, [vp, ip, vp, vp, ip, ip]),
         "b2g_level_pipe_shape": (ip, [vp, ip, ip, ip, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float),
-                                      C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+                                      C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                      C.POINTER(C.c_float), C.POINTER(C.c_int)]),
         "b2g_controls_default": (ip, [C.POINTER(Controls)]),
         "b2g_controls_read": (ip, [C.c_char_p, C.POINTER(Controls)]),
         "b2g_mesh_create": (ip, [ip, ip, vp, vp, vp, vp, ip, C.POINTER(C.c_int), ip, vp,
@@ -299,10 +300,12 @@ class Mesh:
     def pipe_shape(self, level: int, n_sweeps: int, value_bytes: int = 8) -> dict:
         """The tuned choice for `level`'s smoothing calls of n_sweeps sweeps (b2g_level_pipe_shape)."""
         r, st, mp, ms, msh, mit = C.c_int(), C.c_int(), C.c_float(), C.c_float(), C.c_float(), C.c_float()
+        mg, gf = C.c_float(), C.c_int()
         _check(lib.b2g_level_pipe_shape(self.handle, level, n_sweeps, value_bytes, C.byref(r), C.byref(st),
-                                        C.byref(mp), C.byref(ms), C.byref(msh), C.byref(mit)))
+                                        C.byref(mp), C.byref(ms), C.byref(msh), C.byref(mit), C.byref(mg),
+                                        C.byref(gf)))
         return {"ranks": r.value, "steps": st.value, "ms_pipelined": mp.value, "ms_sweep_by_sweep": ms.value,
-                "ms_shared_memory": msh.value, "ms_items": mit.value}
+                "ms_shared_memory": msh.value, "ms_items": mit.value, "ms_grid": mg.value, "grid": bool(gf.value)}
 
     def set_pair(self, own, nbr) -> None:
         """The coupled (cyclic) pair: faceCells and neighbour cells of the coupled patches' faces, each
@@ -482,8 +485,9 @@ class Matrix:
         return list(ms), list(n)
 
     def level_timings(self, kind: int):
-        """Per level of the last profiled solve, kind 0 (Amul) or 1 (smoothing): a list of
-        (ms, timed regions, units) -- units are Amuls, or the sweeps of the smoothing calls."""
+        """Per level of the last profiled solve, kind 0 (Amul), 1 (smoothing) or 2 (Amul fused with the
+        residual, the scaling or the prolongation): a list of (ms, timed regions, units) -- units are
+        Amuls, or the sweeps of the smoothing calls."""
         cap = self.mesh.n_levels + 1
         ms = (C.c_double * cap)()
         reg = (C.c_longlong * cap)()

@@ -339,15 +339,16 @@ B2G_API b2g_status b2g_matrix_pcg_solve(b2g_matrix* m, const double* source, dou
 /* ---- introspection ---------------------------------------------------------------------------- */
 
 /* Device time of the last solve on `m` by kernel class (milliseconds, `ms4`) and counts of each
- * class (`counts4`): [0] Amuls on the finest level, [1] smoothing on the finest level (the count is
- * sweeps), [2] everything else (the count is launches), [3] the whole solve (all launches). Times
+ * class (`counts4`): [0] plain Amuls on the finest level (those fused with another step count as
+ * everything else), [1] smoothing on the finest level (the count is sweeps), [2] everything else
+ * (the count is launches), [3] the whole solve (all launches). Times
  * are taken with events on the solve's stream only while b2g_set_profiling(1) is on (the launch
  * count always). Either pointer may be NULL. */
 B2G_API b2g_status b2g_matrix_timings(const b2g_matrix* m, double* ms4, long long* counts4);
-/* The same per level, for `kind` 0 (Amul, including the one of the correction scaling) or 1
- * (smoothing calls): for levels 0..capacity-1, milliseconds, timed regions and units (Amuls, or
- * the sweeps of the smoothing calls) of the last solve. *nLevels receives the number of levels
- * with a record. Any array may be NULL. */
+/* The same per level, for `kind` 0 (Amul), 1 (smoothing calls) or 2 (Amul fused with another step:
+ * the residual between V-cycles, the correction scaling's dots, the finest prolongation): for levels
+ * 0..capacity-1, milliseconds, timed regions and units (Amuls, or the sweeps of the smoothing calls)
+ * of the last solve. *nLevels receives the number of levels with a record. Any array may be NULL. */
 B2G_API b2g_status b2g_matrix_level_timings(const b2g_matrix* m, int kind, int capacity, double* ms,
                                             long long* regions, long long* units, int* nLevels);
 B2G_API b2g_status b2g_set_profiling(int on);
@@ -375,12 +376,14 @@ B2G_API b2g_status b2g_level_smooth_stall(b2g_matrix* m, int level, double* psi,
                                           long long spinLimit, int* nParts);
 /* nSweeps exact Gauss-Seidel sweeps of `level` (device pointers, natural cell order) in ONE
  * pipelined launch on `ranks` CTAs holding psi in shared memory (1, 2, 4, 8 or 16; a thread-block
- * cluster when above 1), or with ranks = -1 as the level's multi-part sweep over (sweep, cell) items,
- * whatever form the level's tuned choice would take: sweep s+1 runs on a cell once every value its row
- * reads is final, which gives bit for bit the result of nSweeps sequential sweeps (gaussSeidelSweeps,
- * smooth_solver_cpp.cu:87-166, called nSweeps times). B2G_ERR_ARGUMENT when the level's cells do not
- * fit that many CTAs' shared memory, such a cluster cannot be resident, or (ranks -1) the level has
- * one part or nSweeps is 1. For tests and tuning. */
+ * cluster when above 1), on `ranks` CTAs of the grid form when above 16 (psi in global memory, every
+ * CTA resident, each waiting for its neighbour ranks only), or with ranks = -1 as the level's
+ * multi-part sweep over (sweep, cell) items, whatever form the level's tuned choice would take: sweep
+ * s+1 runs on a cell once every value its row reads is final, which gives bit for bit the result of
+ * nSweeps sequential sweeps (gaussSeidelSweeps, smooth_solver_cpp.cu:87-166, called nSweeps times).
+ * B2G_ERR_ARGUMENT when the level's cells do not fit that many CTAs' shared memory, such a cluster or
+ * grid cannot be resident, or (ranks -1) the level has one part or nSweeps is 1; B2G_ERR_DEVICE_TIMEOUT
+ * when a grid-form wait gave up. For tests and tuning. */
 B2G_API b2g_status b2g_level_smooth_pipelined(b2g_matrix* m, int level, double* psi, const double* source,
                                               int nSweeps, int ranks);
 /* psi = A^-1 source on the coarsest level by its dense Cholesky factor (device pointers, natural
@@ -389,14 +392,15 @@ B2G_API b2g_status b2g_level_smooth_pipelined(b2g_matrix* m, int level, double* 
  * the matrix's current coefficients is made on first use. For tests. */
 B2G_API b2g_status b2g_coarsest_dense_solve(b2g_matrix* m, double* psi, const double* source);
 /* The tuned choice for smoothing calls of nSweeps sweeps on `level` in values of `valueBytes` (8 FP64,
- * 4 FP32): *ranks the pipelined launch's CTAs holding psi in shared memory, or minus the part count of
- * the pipelined multi-part sweep over (sweep, cell) items (0: sweep by sweep, or not tuned yet),
- * *nSteps its combined steps, and the measured milliseconds per call of the chosen pipelined form
- * (else the best shared-memory shape), of the sweep-by-sweep launches, of the best shared-memory
- * shape and of the item schedule (0: not tried). Any output may be NULL. */
+ * 4 FP32): *ranks the pipelined launch's CTAs (holding psi in shared memory, or of the grid form when
+ * *gridForm is 1), or minus the part count of the pipelined multi-part sweep over (sweep, cell) items
+ * (0: sweep by sweep, or not tuned yet), *nSteps its combined steps, and the measured milliseconds
+ * per call of the chosen pipelined form (else the best shared-memory shape), of the sweep-by-sweep
+ * launches, of the best shared-memory shape, of the item schedule and of the best grid form (0: not
+ * tried). Any output may be NULL. */
 B2G_API b2g_status b2g_level_pipe_shape(const b2g_mesh* mesh, int level, int nSweeps, int valueBytes, int* ranks,
                                         int* nSteps, float* msPipe, float* msSweeps, float* msShared,
-                                        float* msItems);
+                                        float* msItems, float* msGrid, int* gridForm);
 B2G_API b2g_status b2g_level_smooth_trace(b2g_matrix* m, int level, double* psi, const double* source,
                                           unsigned long long* trace, int traceCapacity, int* schedule);
 /* Diagnostic: the Gauss-Seidel schedule of `level` to HOST arrays (either may be NULL):

@@ -2,9 +2,10 @@
 
 nSweeps sequential sweeps (gaussSeidelSweeps, src/OpenFOAM/matrices/smooth_solver_cpp.cu:87-166, once
 per sweep) run as ONE launch in which sweep s+1 starts on a cell as soon as every value its row reads
-is final. Every shape (one CTA; clusters of 2, 4, 8, 16 CTAs holding psi in distributed shared memory)
-must give the oracle's sweeps exactly, on every level, and whole solves must not change when the
-launch is switched on or off.
+is final. Every shape (one CTA; clusters of 2, 4, 8, 16 CTAs holding psi in distributed shared memory;
+the grid form, psi in global memory and each CTA waiting for its neighbour ranks) must give the
+oracle's sweeps exactly, on every level, and whole solves must not change when the launch is switched
+on or off.
 """
 import numpy as np
 import pytest
@@ -59,7 +60,7 @@ def test_forced_shapes_bitexact(b2g, oracle, name, kw):
         b = rng.uniform(-1.0, 1.0, n)
         for sweeps in (1, 2, 4):
             want = oracle.smooth(lo, up, d, u, x0, b, sweeps)
-            for ranks in (1, 2, 4, 8, 16, -1):
+            for ranks in (1, 2, 4, 8, 16, -1, 24, 64):
                 x = dev(x0)
                 try:
                     A.smooth_pipelined(lv, x, dev(b), sweeps, ranks)
@@ -144,3 +145,25 @@ def test_item_schedule_many_parts(b2g, oracle):
             assert np.array_equal(x.cpu().numpy(), oracle.smooth(lo, up, d, u, x0, b, sweeps)), (lv, sweeps)
             ran += 1
     assert ran >= 4
+
+
+def test_grid_form_many_ranks(b2g, oracle):
+    # the grid form on the levels of a box cut into many ranks: one per SM and fewer, every sweep count
+    c = cases.box_case(64, 64, 64, (2.0, 1.0, 1.0), 20.0)
+    mesh = b2g.Mesh(c.lower, c.upper, c.Sf, c.magSf, c.n_cells, 10, True)
+    A = b2g.Matrix(mesh, dev(c.diag), dev(c.coef))
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    rng = np.random.default_rng(13)
+    ran = 0
+    for lv in (0, 1, 2, 4):
+        lo, up, d, u = _level_system(mesh, A, c, lv)
+        x0 = rng.uniform(-1.0, 1.0, d.shape[0])
+        b = rng.uniform(-1.0, 1.0, d.shape[0])
+        for sweeps in (1, 2, 4):
+            want = oracle.smooth(lo, up, d, u, x0, b, sweeps)
+            for ranks in (sms, sms // 2, 17):
+                x = dev(x0)
+                A.smooth_pipelined(lv, x, dev(b), sweeps, ranks)
+                assert np.array_equal(x.cpu().numpy(), want), (lv, sweeps, ranks)
+                ran += 1
+    assert ran == 4 * 3 * 3
