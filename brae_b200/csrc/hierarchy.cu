@@ -1684,6 +1684,18 @@ void buildLowerLevel(LevelAddr& L, cudaStream_t s)
     L.lowerOnly = std::move(R);
 }
 
+namespace {
+__global__ void kEllColCoarse(long long nEnt, const int* __restrict__ ellCol, const int* __restrict__ prolongP,
+                              int* __restrict__ out)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nEnt; e += (long long)gridDim.x * blockDim.x)
+    {
+        const int c = ellCol[e];
+        out[e] = c >= 0 ? prolongP[c] : -1;
+    }
+}
+}  // namespace
+
 void buildStepMaps(Mesh& M, int i)
 {
     cudaStream_t s = M.stream;
@@ -1701,6 +1713,14 @@ void buildStepMaps(Mesh& M, int i)
     S.prolongP.alloc(S.nFine, s);
     kProlongMap<<<grid(S.nFine), TPB, 0, s>>>(S.nFine, F.posCell.p, S.restrictAddr.p, C.posOf.p, S.prolongP.p);
     B2G_LAUNCH_CHECK();
+    if (i == 0 && F.nEllEnt > 0)
+    {
+        GsSchedule& G = M.lev[0].gs;
+        G.ellColCoarse.alloc(static_cast<size_t>(G.nEllEnt), s);
+        kEllColCoarse<<<static_cast<unsigned>(std::min<long long>((G.nEllEnt + TPB - 1) / TPB, 65535LL)), TPB, 0, s>>>(
+            G.nEllEnt, G.ellCol.p, S.prolongP.p, G.ellColCoarse.p);
+        B2G_LAUNCH_CHECK();
+    }
 }
 
 cudaMemPool_t libraryPool()

@@ -57,6 +57,9 @@ struct GsSchedule
     // position (-1 past the row's end) and the CSR entry it copies (-1 there)
     long long nEllEnt = 0;
     DBuf<int> ellBase, ellCol, ellEnt;
+    // the finest level's: per ELL entry the coarse position its column is prolonged from (-1 past the
+    // row's end), so that the correction scaling reads the coarse correction with one gather
+    DBuf<int> ellColCoarse;
 };
 
 // the smallest level that gets the sliced ELL copy of its rows
@@ -85,13 +88,10 @@ struct PipeSchedule
     DBuf<unsigned> progress;    // [ranks][kProgressStride]
 };
 
-// The dynamic shared memory of a pipelined launch in values of valueBytes: the rank's slots, then its
-// step table.
-inline size_t pipeSmemBytes(const PipeSchedule& P, size_t valueBytes)
-{
-    if (P.grid) return sizeof(int) * (P.nSteps + 1);
-    return ((valueBytes * static_cast<size_t>(P.maxLocal) + 15) / 16) * 16 + sizeof(int) * (P.nSteps + 1);
-}
+// The dynamic shared memory of a pipelined launch in values of valueBytes (pipe.cu): the rank's
+// slots in the shared-memory forms, the rank's step table in the grid form.
+size_t pipeSmemBytes(const PipeSchedule& P, size_t valueBytes);
+
 
 // The choice for one (level, sweep count, value type), by measurement (Matrix::ensurePipe): the
 // pipelined launch with the fastest shape (shared memory on 1-16 CTAs, or the grid form), the item

@@ -204,6 +204,7 @@ __global__ void scaleUpdateAdd(int n, const T* __restrict__ sfp, const T* __rest
 // with a coupled pair, whose Amul reads the pair's neighbours too.)
 template <class T, int NT>
 __global__ void __launch_bounds__(NT) amulScaleDotsProlong(Rows<T> A, const int* __restrict__ prolongP,
+                                                           const int* __restrict__ ellColCoarse,
                                                            const T* __restrict__ coarse,
                                                            const T* __restrict__ source, T* __restrict__ Acf,
                                                            T* __restrict__ partial)
@@ -214,8 +215,26 @@ __global__ void __launch_bounds__(NT) amulScaleDotsProlong(Rows<T> A, const int*
     {
         const T fc = coarse[prolongP[c]];
         T acc = mulRn(A.diag[c], fc);
-        acc = rowFold(A, c, acc,
-                      [coarse, prolongP](T a, T v, int cp) { return addRn(a, mulRn(v, coarse[prolongP[cp]])); });
+        if (A.ellBase && ellColCoarse)
+        {
+            // the sliced rows with each column's coarse position at hand: one gather per entry
+            const int sl = c >> 5, lane = c & 31;
+            const int b0 = A.ellBase[sl];
+            const int w = (A.ellBase[sl + 1] - b0) >> 5;
+#pragma unroll 4
+            for (int q = 0; q < w; ++q)
+            {
+                const int e = b0 + 32 * q + lane;
+                const int cc = ellColCoarse[e];
+                const T v = A.ellVal[e];
+                if (cc >= 0) acc = addRn(acc, mulRn(v, coarse[cc]));
+            }
+        }
+        else
+        {
+            acc = rowFold(A, c, acc,
+                          [coarse, prolongP](T a, T v, int cp) { return addRn(a, mulRn(v, coarse[prolongP[cp]])); });
+        }
         Acf[c] = acc;
         num = addRn(num, mulRn(fc, source[c]));
         den = addRn(den, mulRn(fc, acc));

@@ -87,8 +87,7 @@ std::unique_ptr<PipeSchedule> assemble(const LevelHost& H, const std::vector<int
             const int c = H.posCell[p];
             localPos[static_cast<size_t>(rankOf[c]) * maxLocal + slotOf[c]] = p;
         }
-    if (((valueBytes * static_cast<size_t>(maxLocal) + 15) / 16) * 16 + sizeof(int) * (nSteps + 1) > kPipeSmemCap)
-        return nullptr;
+    if (grid && sizeof(int) * (nSteps + 1) > 48 * 1024) return nullptr;
     // the grid form: a value is named by its position, and a row's value slot is its position
     if (grid)
         for (int p = 0; p < n; ++p) slotOf[H.posCell[p]] = p;
@@ -242,6 +241,12 @@ int smCount()
 int pipeKey(int sweeps, size_t valueBytes) { return sweeps * 16 + static_cast<int>(valueBytes); }
 
 }  // namespace
+
+size_t pipeSmemBytes(const PipeSchedule& P, size_t valueBytes)
+{
+    if (P.grid) return sizeof(int) * (P.nSteps + 1);
+    return valueBytes * static_cast<size_t>(P.maxLocal);
+}
 
 template <class T>
 k::PipeArgs<T> Matrix::pipeArgs(int level, const PipeSchedule& P, T* psiL, const T* src)

@@ -36,10 +36,10 @@
 //
 // THE ROWS. An item is {position, value slot, first and end row entry}: the row is read in place
 // from the level's position-order rows (no copy per sweep, so a level's rows stay in L2). Row data do
-// not depend on psi, so they are loaded ahead: a thread loads its item record two steps ahead and its
-// row one step ahead, and no step waits on a load chain -- the chain per step is the value reads,
-// the arithmetic and the barrier. A warp's loops run to the widest row among its lanes (a warp-wide
-// maximum), each lane adding only its own row's entries.
+// not depend on psi, so they are loaded ahead into registers: in the shared-memory forms a thread
+// loads its next step's row before it computes the current one; in the grid form it loads its item
+// record two steps ahead and its row one step ahead, and its loops run to the widest row of its warp
+// (a warp-wide maximum), each lane adding only its own row's entries.
 #pragma once
 
 #include "b2g_common.cuh"
@@ -192,27 +192,43 @@ __device__ __forceinline__ void pipeLoadRow(const PipeArgs<T>& a, int4 it, bool 
     }
 }
 
+// the shared-memory forms: item k's row into registers (no load waits for another)
+template <class T>
+__device__ __forceinline__ void pipeLoad(const PipeArgs<T>& a, int k, PipeRow<T, kPipeK>& r)
+{
+    r.slot = -1;
+    r.w = 0;
+    if (k < 0) return;
+    const int4 it = a.item[k];
+    r.slot = it.y;
+    r.e0 = it.z;
+    r.w = it.w - it.z;
+    r.b = a.b[it.x];
+    r.d = a.A.diag[it.x];
+#pragma unroll
+    for (int q = 0; q < kPipeK; ++q)
+        if (q < r.w)
+        {
+            r.v[q] = a.A.val[it.z + q];
+            r.ea[q] = a.entAddr[it.z + q];
+        }
+}
+
 // the row in the reference's order: the source minus each entry's coefficient times its value, then
-// the division by the diagonal (the shared-memory forms)
+// the division by the diagonal
 template <class T, bool kCluster>
 __device__ __forceinline__ void pipeRow(const PipeArgs<T>& a, const PipeRow<T, kPipeK>& r, unsigned xa)
 {
     T x[kPipeK];
 #pragma unroll
-    for (int k = 0; k < kPipeK; ++k)
-    {
-        if (k >= r.wq) break;
-        if (k < r.w) x[k] = pipeLd<kCluster>(pipeAddr<T, kCluster>(r.ea[k], xa), T());
-    }
+    for (int q = 0; q < kPipeK; ++q)
+        if (q < r.w) x[q] = pipeLd<kCluster>(pipeAddr<T, kCluster>(r.ea[q], xa), T());
     T acc = r.b;
 #pragma unroll
-    for (int k = 0; k < kPipeK; ++k)
-    {
-        if (k >= r.wq) break;
-        if (k < r.w) acc = subRn(acc, mulRn(r.v[k], x[k]));
-    }
-    for (int k = kPipeK; k < r.w; ++k)
-        acc = subRn(acc, mulRn(a.A.val[r.e0 + k], pipeLd<kCluster>(pipeAddr<T, kCluster>(a.entAddr[r.e0 + k], xa), T())));
+    for (int q = 0; q < kPipeK; ++q)
+        if (q < r.w) acc = subRn(acc, mulRn(r.v[q], x[q]));
+    for (int q = kPipeK; q < r.w; ++q)
+        acc = subRn(acc, mulRn(a.A.val[r.e0 + q], pipeLd<kCluster>(pipeAddr<T, kCluster>(a.entAddr[r.e0 + q], xa), T())));
     pipeSt(xa + static_cast<unsigned>(sizeof(T)) * static_cast<unsigned>(r.slot), divRn(acc, r.d));
 }
 
@@ -238,15 +254,7 @@ __device__ __forceinline__ void pipeRowGrid(const PipeArgs<T>& a, const PipeRow<
     a.psi[r.slot] = divRn(acc, r.d);
 }
 
-// A row straight from memory (the items beyond the block's width at a step: rare, so not staged)
-template <class T, bool kCluster>
-__device__ __forceinline__ void pipeRowDirect(const PipeArgs<T>& a, int4 it, unsigned xa)
-{
-    T acc = a.b[it.x];
-    for (int e = it.z; e < it.w; ++e)
-        acc = subRn(acc, mulRn(a.A.val[e], pipeLd<kCluster>(pipeAddr<T, kCluster>(a.entAddr[e], xa), T())));
-    pipeSt(xa + static_cast<unsigned>(sizeof(T)) * static_cast<unsigned>(it.y), divRn(acc, a.A.diag[it.x]));
-}
+// A row straight from memory (the grid form's items beyond the block's width at a step: rare)
 template <class T>
 __device__ __forceinline__ void pipeRowGridDirect(const PipeArgs<T>& a, int4 it)
 {
@@ -256,13 +264,12 @@ __device__ __forceinline__ void pipeRowGridDirect(const PipeArgs<T>& a, int4 it)
 }
 
 // One smoothing call (all its sweeps) of one level. Grid = one cluster of R CTAs (kCluster) or one
-// CTA; dynamic shared memory = pipeSmemBytes (the rank's slots, then its step table).
+// CTA; dynamic shared memory = maxLocal values of T.
 template <class T, bool kCluster>
 __device__ __forceinline__ void gsPipeBody(const PipeArgs<T>& a)
 {
     extern __shared__ __align__(16) unsigned char pipeSm[];
     T* x = reinterpret_cast<T*>(pipeSm);
-    int* ss = reinterpret_cast<int*>(pipeSm + ((sizeof(T) * static_cast<size_t>(a.maxLocal) + 15) / 16) * 16);
     const int rank = kCluster ? static_cast<int>(clusterRank()) : 0;
     const int t = threadIdx.x;
     const int B = blockDim.x;
@@ -270,37 +277,28 @@ __device__ __forceinline__ void gsPipeBody(const PipeArgs<T>& a)
     const int cnt = a.localCount[rank];
     const int* lp = a.localPos + static_cast<size_t>(rank) * a.maxLocal;
     for (int i = t; i < cnt; i += B) x[i] = a.psi[lp[i]];
-    const int* gss = a.stepStart + static_cast<size_t>(rank) * (a.nSteps + 1);
-    for (int i = t; i <= a.nSteps; i += B) ss[i] = gss[i];
     // every rank's psi is in place before any row reads it
     pipeBarrier<kCluster>();
-    // this thread's item at step T_, or -1
-    auto itemAt = [&](int T_) { return T_ < a.nSteps && ss[T_] + t < ss[T_ + 1] ? ss[T_] + t : -1; };
-    const int4 none = make_int4(0, -1, 0, 0);
-    PipeRow<T, kPipeK> r0, r1;
-    int k1 = itemAt(0);
-    pipeLoadRow<T, kPipeK, false>(a, k1 >= 0 ? a.item[k1] : none, k1 >= 0, r0);
-    k1 = itemAt(1);
-    int4 it1 = k1 >= 0 ? a.item[k1] : none;
-    // one step: the next row's loads from its record (loaded a step ago), the record after it, this
-    // step's rows, the barrier
-    auto step = [&](int T_, const PipeRow<T, kPipeK>& cur, PipeRow<T, kPipeK>& nxt) {
-        pipeLoadRow<T, kPipeK, false>(a, it1, k1 >= 0, nxt);
-        k1 = itemAt(T_ + 2);
-        if (k1 >= 0) it1 = a.item[k1];
+    const int* ss = a.stepStart + static_cast<size_t>(rank) * (a.nSteps + 1);
+    PipeRow<T, kPipeK> cur, nxt;
+    pipeLoad(a, a.nSteps > 0 && ss[0] + t < ss[1] ? ss[0] + t : -1, cur);
+    int kn = a.nSteps > 1 && ss[1] + t < ss[2] ? ss[1] + t : -1;
+    for (int T_ = 0; T_ < a.nSteps; ++T_)
+    {
+        // the next step's row (its item index was found a step ago) and the item index after it
+        pipeLoad(a, kn, nxt);
+        kn = T_ + 2 < a.nSteps && ss[T_ + 2] + t < ss[T_ + 3] ? ss[T_ + 2] + t : -1;
         if (cur.slot >= 0) pipeRow<T, kCluster>(a, cur, xa);
         // items beyond the block's width at this step, straight from memory
-        for (int k = ss[T_] + t + B; k < ss[T_ + 1]; k += B) pipeRowDirect<T, kCluster>(a, a.item[k], xa);
+        for (int k = ss[T_] + t + B; k < ss[T_ + 1]; k += B)
+        {
+            PipeRow<T, kPipeK> r;
+            pipeLoad(a, k, r);
+            pipeRow<T, kCluster>(a, r, xa);
+        }
         pipeBarrier<kCluster>();
-    };
-    // two steps per iteration, the rows alternating between r0 and r1 (no copies)
-    int T_ = 0;
-    for (; T_ + 1 < a.nSteps; T_ += 2)
-    {
-        step(T_, r0, r1);
-        step(T_ + 1, r1, r0);
+        cur = nxt;
     }
-    if (T_ < a.nSteps) step(T_, r0, r1);
     // the last barrier above ordered every read of this CTA's values before the write-back; no rank
     // reads another's shared memory after it, so the CTAs may leave in any order
     for (int i = t; i < cnt; i += B) a.psi[lp[i]] = x[i];

@@ -1583,7 +1583,8 @@ void Matrix::vcycle(const b2g_controls& c, T* x, const T* src, T* Apsi, T* fcor,
         const Step& S0 = mesh->step[0];
         const int g = redGrid(F.nCells);
         cudaEvent_t e = timedBegin(2, 0, 1);
-        k::amulScaleDotsProlong<T, NT><<<g, NT, 0, stream>>>(rowsOf(F, D.coef[0]), S0.prolongP.p, D.corr[0].p, fres,
+        k::amulScaleDotsProlong<T, NT><<<g, NT, 0, stream>>>(rowsOf(F, D.coef[0]), S0.prolongP.p,
+                                                             F.gs.ellColCoarse.p, D.corr[0].p, fres,
                                                              Apsi, D.partial.p);
         timedEnd(e);
         k::scaleFactor<T, NT><<<1, NT, 0, stream>>>(D.partial.p, g, D.sf.p);
