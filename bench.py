@@ -840,16 +840,27 @@ def serve_stream(args, b2g, local):
 
     for form, prec in forms:
         out[form] = one_stream(form, prec, args.serve_rate, args.serve_seconds, 2)
-    # a rate the server keeps up with (a fraction of the capacity the offered stream showed), repeated
-    # with different arrival seeds: the spread of the latencies
+    # a rate the server keeps up with, repeated with different arrival seeds: the spread of the
+    # latencies. It starts at a fraction of the throughput the offered stream showed and is lowered
+    # until a probe stream drains within a second of its window (a queue that does not grow).
     for form, prec in forms:
         cap = out[form]["solves_per_s"]
         rate = max(1.0, args.serve_capacity_fraction * cap)
+        probes = []
+        for attempt in range(5):
+            pr = one_stream(form, prec, rate, args.serve_stable_seconds, 100 + attempt)
+            probes.append({"offered_rate_per_s": rate, "drain_s": pr["drain_s"], "p50_ms": pr["p50_ms"],
+                           "p99_ms": pr["p99_ms"], "max_outstanding": pr["max_outstanding"]})
+            if pr["drain_s"] <= 1.0:
+                break
+            rate = max(1.0, 0.65 * rate)
         reps = [one_stream(form, prec, rate, args.serve_stable_seconds, 2 + r) for r in range(args.serve_repeats)]
         p50 = [r["p50_ms"] for r in reps]
         p99 = [r["p99_ms"] for r in reps]
         out[form + "_at_stable_rate"] = {
             "offered_rate_per_s": rate, "stream_s": args.serve_stable_seconds, "repeats": len(reps),
+            "rate_search": probes,
+            "drain_s": [r["drain_s"] for r in reps],
             "p50_ms": {"min": min(p50), "median": float(np.median(p50)), "max": max(p50)},
             "p99_ms": {"min": min(p99), "median": float(np.median(p99)), "max": max(p99)},
             "solves_per_s": [r["solves_per_s"] for r in reps],
@@ -915,9 +926,10 @@ def main():
     ap.add_argument("--serve-reltol", type=float, default=0.0, help="relTol of the served solves")
     ap.add_argument("--serve-forms", nargs="*", default=["fp64", "fp32_precond_multicolour"],
                     help="forms of the served stream (fp64, fp32_precond, fp32_precond_multicolour)")
-    ap.add_argument("--serve-capacity-fraction", type=float, default=0.8,
-                    help="the stable stream's rate as a fraction of the capacity the offered stream showed")
-    ap.add_argument("--serve-stable-seconds", type=float, default=8.0, help="length of each stable stream")
+    ap.add_argument("--serve-capacity-fraction", type=float, default=0.6,
+                    help="the first probe's rate for the stable stream, as a fraction of the throughput the "
+                         "offered stream showed")
+    ap.add_argument("--serve-stable-seconds", type=float, default=6.0, help="length of each stable stream")
     ap.add_argument("--serve-repeats", type=int, default=3, help="repeats of the stable stream")
     ap.add_argument("--serve", action="store_true", help="run the served stream alone")
     ap.add_argument("--no-coupled", action="store_true", help="skip the coupled-pair leg")
