@@ -842,7 +842,7 @@ def serve_stream(args, b2g, local):
         out[form] = one_stream(form, prec, args.serve_rate, args.serve_seconds, 2)
     # a rate the server keeps up with, repeated with different arrival seeds: the spread of the
     # latencies. It starts at a fraction of the throughput the offered stream showed and is lowered
-    # until a probe stream drains within a second of its window (a queue that does not grow).
+    # until a probe stream drains within half a second of its window (a queue that does not grow).
     for form, prec in forms:
         cap = out[form]["solves_per_s"]
         rate = max(1.0, args.serve_capacity_fraction * cap)
@@ -851,7 +851,7 @@ def serve_stream(args, b2g, local):
             pr = one_stream(form, prec, rate, args.serve_stable_seconds, 100 + attempt)
             probes.append({"offered_rate_per_s": rate, "drain_s": pr["drain_s"], "p50_ms": pr["p50_ms"],
                            "p99_ms": pr["p99_ms"], "max_outstanding": pr["max_outstanding"]})
-            if pr["drain_s"] <= 1.0:
+            if pr["drain_s"] <= 0.5:
                 break
             rate = max(1.0, 0.65 * rate)
         reps = [one_stream(form, prec, rate, args.serve_stable_seconds, 2 + r) for r in range(args.serve_repeats)]

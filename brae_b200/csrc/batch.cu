@@ -1188,7 +1188,7 @@ void Batch::smooth(int lv, int nSweeps)
     const int4* parts = B.parts.p;
     int nParts = B.nParts;
     auto pit = B.pipe.find(nSweeps * 16 + static_cast<int>(sizeof(T)));
-    if (pipeOn && pit != B.pipe.end())
+    if (pipeOn && pit != B.pipe.end() && pit->second.use)
     {
         // the cases whose level fits one CTA: every sweep in one pipelined launch; the rest below
         const BatchLevel::Pipe& P = pit->second;
@@ -1264,6 +1264,31 @@ void Batch::preparePipe(int lv, int nSweeps)
     }
     if (P.nPartsBig) P.partsBig.upload(big.data(), big.size(), stream);
     B2G_CUDA(cudaStreamSynchronize(stream));
+    if (!P.nSmall) return;
+    // the batch's own choice, by measurement: the pipelined launch for the small cases' levels, or the
+    // sweep-by-sweep launches for every case (the same bits either way); every case swept while timing
+    B2G_CUDA(cudaMemsetAsync(active.p, 0xff, sizeof(int) * K, stream));
+    cudaEvent_t e0, e1;
+    B2G_CUDA(cudaEventCreate(&e0));
+    B2G_CUDA(cudaEventCreate(&e1));
+    const long long l0 = launches;
+    auto timeIt = [&](bool use) {
+        P.use = use;
+        smooth<T>(lv, nSweeps);  // warm
+        B2G_CUDA(cudaEventRecord(e0, stream));
+        for (int i = 0; i < 2; ++i) smooth<T>(lv, nSweeps);
+        B2G_CUDA(cudaEventRecord(e1, stream));
+        B2G_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        B2G_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        return ms / 2.f;
+    };
+    P.msPipe = timeIt(true);
+    P.msSweeps = timeIt(false);
+    P.use = P.msPipe < P.msSweeps;
+    launches = l0;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
 }
 
 // Every batched pipelined sweep the controls' V-cycle makes, before the iterations run.

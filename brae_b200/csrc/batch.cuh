@@ -111,6 +111,8 @@ struct BatchLevel
         DBuf<int> caseOf;            // [nSmall]
         DBuf<int4> partsBig;         // the parts of the cases that do not fit
         int nPartsBig = 0;
+        bool use = false;            // measured faster than the sweep-by-sweep launches
+        float msPipe = 0.f, msSweeps = 0.f;  // per smoothing call of every case, as measured
     };
     std::map<int, Pipe> pipe;
     std::vector<TileList> mc;  // per colour: the swept large cases' rows of that colour (multicolour form)
