@@ -481,7 +481,8 @@ def run_ours(args, world, rank, local):
                      "all_levels": {"sweep_gbs": all_sweep_gbs, "sweep_frac": all_sweep_gbs / peak,
                                     "amul_gbs": all_amul_gbs, "amul_frac": all_amul_gbs / peak},
                      "amul_finest": {"gbs": fin.get("amul_gbs"), "frac": (fin.get("amul_gbs") or 0.0) / peak,
-                                     "algorithmic_bytes": amul_bytes}},
+                                     "algorithmic_bytes": amul_bytes,
+                                     "traffic": traffic_per_launch("amul", f"graded_channel_{args.n}")}},
         "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches_per_step * args.steps),
         "clocks": clocks.summary(),

@@ -316,11 +316,16 @@ typename VCycleData<T>::ItemBuffers& Matrix::itemBuffers(int level, const GsSche
     if (B.gen != coefGen)
     {
         if (capturing) fail(B2G_ERR_STATE, "b2g: an item schedule's blobs were not filled before the capture");
+        // the blobs' padding is zeroed when the buffers are new; a refill writes the same bytes
         const long long bytes = sizeof(T) == 8 ? G.blobBytes64 : G.blobBytes32;
+        const void* blobWas = B.blob.p;
+        const size_t blobN = B.blob.n;
         B.blob.ensure(static_cast<size_t>(std::max<long long>(bytes, 16)), stream);
-        B.blob.zero(stream);
+        if (B.blob.p != blobWas || B.blob.n != blobN) B.blob.zero(stream);
+        const void* bWas = B.b.p;
+        const size_t bN = B.b.n;
         B.b.ensure(static_cast<size_t>(std::max(G.nAlloc, 1)), stream);
-        B.b.zero(stream);
+        if (B.b.p != bWas || B.b.n != bN) B.b.zero(stream);
         if (G.nChunks)
             k::buildChunkBlobs<T><<<std::min(G.nChunks, 65535), 128, 0, stream>>>(
                 G.nChunks, reinterpret_cast<const int4*>(G.chunkRec.p), D.coef[level].gsDiag.p, G.posEnt.p,

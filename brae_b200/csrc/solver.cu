@@ -151,15 +151,21 @@ __global__ void kGsLayout(int n, long long nnz, const int* __restrict__ posCell,
 }
 
 // (+8 elements of zeroed padding past the diagonal: bulk copies round position ranges out to 16 bytes)
+// The padding of the diagonal and of the chunk blobs is zeroed when the buffers are new; a refill with
+// new coefficients writes the same bytes as the first fill, so the padding stays zero.
 template <class T>
 void allocGsLayout(const LevelAddr& L, LevelCoef<T>& C, cudaStream_t s)
 {
+    const void* diagWas = C.gsDiag.p;
+    const size_t diagN = C.gsDiag.n;
     C.gsDiag.ensure(L.nCells + 8, s);
-    C.gsDiag.zero(s);
+    if (C.gsDiag.p != diagWas || C.gsDiag.n != diagN) C.gsDiag.zero(s);
     C.rowVal.ensure(std::max<size_t>(2 * (size_t)L.nFaces, 1), s);
     const long long bytes = sizeof(T) == 8 ? L.gs.blobBytes64 : L.gs.blobBytes32;
+    const void* blobWas = C.blob.p;
+    const size_t blobN = C.blob.n;
     C.blob.ensure(static_cast<size_t>(std::max<long long>(bytes, 16)), s);
-    C.blob.zero(s);
+    if (C.blob.p != blobWas || C.blob.n != blobN) C.blob.zero(s);
 }
 
 // the sweep's chunk blobs in T, from the FP64 LDU coefficients
