@@ -837,6 +837,40 @@ b2g_status b2g_level_smooth_stall(b2g_matrix* m, int level, double* psi, const d
     });
 }
 
+b2g_status b2g_level_grid_stall(b2g_matrix* m, int level, double* psi, const double* source, int nSweeps, int ranks,
+                                long long spinLimit)
+{
+    return guarded([&] {
+        need(m && psi && source, "b2g_level_grid_stall: null argument");
+        need(level >= 0 && level <= m->mat->nLevels(), "b2g_level_grid_stall: level out of range");
+        need(nSweeps >= 2, "b2g_level_grid_stall: nSweeps must be at least 2 (one step waits for another)");
+        need(ranks > b2g::k::kPipeMaxRanks, "b2g_level_grid_stall: ranks must be above 16 (the grid form)");
+        need(spinLimit >= 1 && spinLimit <= b2g::k::kSpinLimit, "b2g_level_grid_stall: spinLimit out of range");
+        b2g::Matrix& A = *m->mat;
+        need(!A.coupled, "b2g_level_grid_stall: not for a coupled matrix");
+        A.toPos(level, static_cast<const double*>(psi), A.ioBuf(0));
+        A.toPos(level, source, A.ioBuf(1));
+        A.spinLimit = spinLimit;
+        A.publish = 0;
+        bool ran = false;
+        try
+        {
+            ran = A.pipeForced<double>(level, A.ioBuf(0), A.ioBuf(1), nSweeps, ranks);
+        }
+        catch (...)
+        {
+            A.spinLimit = b2g::k::kSpinLimit;
+            A.publish = 1;
+            throw;
+        }
+        A.spinLimit = b2g::k::kSpinLimit;
+        A.publish = 1;
+        if (!ran) b2g::fail(B2G_ERR_ARGUMENT, "b2g_level_grid_stall: the level does not fit that many CTAs");
+        A.fromPos(level, static_cast<const double*>(A.ioBuf(0)), psi);
+        B2G_CUDA(cudaStreamSynchronize(A.stream));
+    });
+}
+
 b2g_status b2g_level_smooth_pipelined(b2g_matrix* m, int level, double* psi, const double* source, int nSweeps,
                                       int ranks)
 {

@@ -278,6 +278,7 @@ void Matrix::pipeLaunch(int level, const PipeSchedule& P, T* psiL, const T* src)
         g.nbrList = P.nbrList.p;
         g.spinLimit = spinLimit;
         g.err = err.p;
+        g.publish = publish;
         B2G_CUDA(cudaMemsetAsync(P.progress.p, 0, P.progress.bytes(), stream));
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeCooperative;

@@ -81,6 +81,7 @@ struct PipeGridSync
     const int* __restrict__ nbrList;
     long long spinLimit;                // polls before a wait gives up
     int* err;                           // set to 1 when a wait gives up
+    int publish;                        // 0: no rank publishes its progress (a test of the waits' limit)
 };
 
 template <class T, int K>
@@ -374,7 +375,7 @@ __global__ void __launch_bounds__(kPipeGridBlock, 1) gsPipeGrid(PipeArgs<T> a, P
         for (int k = gridSs[T_] + t + B; k < gridSs[T_ + 1]; k += B) pipeRowGridDirect<T>(a, a.item[k]);
         // the barrier orders the CTA's psi stores before thread 0's release (release is cumulative)
         __syncthreads();
-        if (t == 0) stRelease(mine, static_cast<unsigned>(T_ + 1));
+        if (t == 0 && g.publish) stRelease(mine, static_cast<unsigned>(T_ + 1));
         return true;
     };
     int T_ = 0;

@@ -73,6 +73,7 @@ def _load():
         "b2g_set_sweep_pipeline": (ip, [ip]),
         "b2g_coarsest_dense_solve": (ip, [vp, vp, vp]),
         "b2g_assemble_pressure": (ip, [vp] + [vp] * 6 + [ip] + [vp] * 6 + [ip, dp] + [vp] * 5 + [ip, vp]),
+        "b2g_level_grid_stall": (ip, [vp, ip, vp, vp, ip, ip, C.c_longlong]),
         "b2g_level_smooth_pipelined": (ip, [vp, ip, vp, vp, ip, ip]),
         "b2g_level_pipe_shape": (ip, [vp, ip, ip, ip, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float),
                                       C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
@@ -154,7 +155,7 @@ EXPORTED = [
     "b2g_batch_launches", "b2g_batch_destroy", "b2g_mesh_set_pair", "b2g_mesh_level_pair",
     "b2g_gamg_solve_coupled", "b2g_matrix_create_coupled", "b2g_matrix_level_pair_coeffs", "b2g_matrix_gamg_solve",
     "b2g_matrix_set_coeffs", "b2g_matrix_level_timings", "b2g_level_smooth_stall", "b2g_set_sweep_pipeline",
-    "b2g_level_smooth_pipelined", "b2g_level_pipe_shape", "b2g_coarsest_dense_solve", "b2g_assemble_pressure",
+    "b2g_level_smooth_pipelined", "b2g_level_grid_stall", "b2g_level_pipe_shape", "b2g_coarsest_dense_solve", "b2g_assemble_pressure",
 ]
 
 
@@ -427,6 +428,11 @@ class Matrix:
     def smooth_pipelined(self, level, psi, source, n_sweeps, ranks):
         """n_sweeps sweeps in one pipelined launch on `ranks` CTAs (b2g_level_smooth_pipelined)."""
         _check(lib.b2g_level_smooth_pipelined(self.handle, level, _ptr(psi), _ptr(source), n_sweeps, ranks))
+
+    def grid_stall(self, level, psi, source, n_sweeps, ranks, spin_limit):
+        """The grid form with no rank publishing its progress (b2g_level_grid_stall): the status name."""
+        rc = lib.b2g_level_grid_stall(self.handle, level, _ptr(psi), _ptr(source), n_sweeps, ranks, int(spin_limit))
+        return STATUS.get(rc, str(rc))
 
     def coarsest_dense_solve(self, psi, source):
         """psi = A^-1 source on the coarsest level by its dense Cholesky factor."""

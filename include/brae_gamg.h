@@ -374,6 +374,12 @@ B2G_API b2g_status b2g_set_sweep_pipeline(int on);
  * level's part count. No counterpart in the reference. */
 B2G_API b2g_status b2g_level_smooth_stall(b2g_matrix* m, int level, double* psi, const double* source,
                                           long long spinLimit, int* nParts);
+/* The grid form of the pipelined sweeps (ranks above 16 CTAs, nSweeps at least 2) with no rank
+ * publishing its progress: every wait for a neighbour rank runs out after spinLimit polls, the kernel
+ * ends, and the call returns B2G_ERR_DEVICE_TIMEOUT with the context still usable. psi is left in an
+ * unspecified state. For tests of the waits' limit. */
+B2G_API b2g_status b2g_level_grid_stall(b2g_matrix* m, int level, double* psi, const double* source, int nSweeps,
+                                        int ranks, long long spinLimit);
 /* nSweeps exact Gauss-Seidel sweeps of `level` (device pointers, natural cell order) in ONE
  * pipelined launch on `ranks` CTAs holding psi in shared memory (1, 2, 4, 8 or 16; a thread-block
  * cluster when above 1), on `ranks` CTAs of the grid form when above 16 (psi in global memory, every

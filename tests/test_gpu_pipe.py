@@ -167,3 +167,21 @@ def test_grid_form_many_ranks(b2g, oracle):
                 assert np.array_equal(x.cpu().numpy(), want), (lv, sweeps, ranks)
                 ran += 1
     assert ran == 4 * 3 * 3
+
+
+def test_grid_form_wait_gives_up(b2g, oracle):
+    # the grid form with no rank publishing its progress: every rank's wait for its neighbours runs
+    # out after a short limit, the kernel ends and the call reports a device time-out; the context
+    # stays usable and the next call on the same matrix is bit for bit the oracle's
+    c = cases.box_case(64, 64, 64, (2.0, 1.0, 1.0), 20.0)
+    mesh = b2g.Mesh(c.lower, c.upper, c.Sf, c.magSf, c.n_cells, 10, True)
+    A = b2g.Matrix(mesh, dev(c.diag), dev(c.coef))
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    rng = np.random.default_rng(17)
+    lo, up, d, u = _level_system(mesh, A, c, 1)
+    x0 = rng.uniform(-1.0, 1.0, d.shape[0])
+    b = rng.uniform(-1.0, 1.0, d.shape[0])
+    assert A.grid_stall(1, dev(x0), dev(b), 2, sms, 1 << 14) == "DEVICE_TIMEOUT"
+    x = dev(x0)
+    A.smooth_pipelined(1, x, dev(b), 2, sms)
+    assert np.array_equal(x.cpu().numpy(), oracle.smooth(lo, up, d, u, x0, b, 2))
