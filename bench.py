@@ -39,6 +39,9 @@ sys.path.insert(0, HERE)
 
 METRIC = "20M-cell p-solve s, FP32-precond vs FP64 at equal residual; served p50/p99 latency"
 TOL, REL_TOL, MAX_ITER = 1e-6, 0.05, 1000
+# the batched form's part rule (b2g_set_part_cells): one part per 128 cells of a level's average depth,
+# against 48 for one solve (on B200 the batch was faster with 128: its cases fill the GPU together)
+BATCH_PART_CELLS = 128
 
 
 BACKEND = "nccl"
@@ -604,14 +607,19 @@ def batched_leg(args, b2g, local, world=1, rank=0):
     dims = [all_dims[i] for i in mine]
     built, meshes, mats = [], [], []
     td = lambda a, dt=torch.float64: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)
-    for d in dims:
-        c = cases.box_case(*d["n"], d["lengths"], d["grading"], False, 0)
-        m = b2g.Mesh(td(c.lower, torch.int32), td(c.upper, torch.int32), td(c.Sf.reshape(-1)), td(c.magSf),
-                     c.n_cells, 10, True)
-        meshes.append(m)
-        mats.append(b2g.Matrix(m, td(c.diag), td(c.coef)))
-        built.append((c.n_cells, c.n_faces, c.source))
-        del c
+    # the batch's own part rule (its cases fill the GPU together): fewer parts per level than one solve
+    b2g.set_part_cells(BATCH_PART_CELLS)
+    try:
+        for d in dims:
+            c = cases.box_case(*d["n"], d["lengths"], d["grading"], False, 0)
+            m = b2g.Mesh(td(c.lower, torch.int32), td(c.upper, torch.int32), td(c.Sf.reshape(-1)), td(c.magSf),
+                         c.n_cells, 10, True)
+            meshes.append(m)
+            mats.append(b2g.Matrix(m, td(c.diag), td(c.coef)))
+            built.append((c.n_cells, c.n_faces, c.source))
+            del c
+    finally:
+        b2g.set_part_cells(48)
     sizes = [n for n, _, _ in built]
     off = np.concatenate([[0], np.cumsum(sizes)])
     src_all = torch.cat([td(s) for _, _, s in built])
@@ -681,6 +689,7 @@ def batched_leg(args, b2g, local, world=1, rank=0):
     return {"workload": f"{n_cases} cases, cells log-uniform 4096..1048576 (seed 1), FP32-precond PCG+GAMG "
                         f"tol 1e-6 relTol 0", "cases": n_cases, "cells": int(n_cells),
             "sharding": f"by case over {world} rank(s), no collective on the data path",
+            "part_cells": BATCH_PART_CELLS,
             "setup_s": setup_s, "batch_s": batch_s, "cases_per_s": n_cases / batch_s,
             "cells_per_s": n_cells / batch_s, "gpu_launches": int(launches),
             "iterations": {"min": int(min(its)), "max": int(max(its)), "mean": float(np.mean(its))},

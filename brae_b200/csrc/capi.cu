@@ -522,6 +522,14 @@ b2g_status b2g_set_sweep_pipeline(int on)
     return B2G_OK;
 }
 
+b2g_status b2g_set_part_cells(int cells)
+{
+    return guarded([&] {
+        need(cells >= 1 && cells <= 65536, "b2g_set_part_cells: cells must be in [1, 65536]");
+        b2g::g_partCells.store(cells);
+    });
+}
+
 b2g_status b2g_controls_default(b2g_controls* out)
 {
     return guarded([&] {

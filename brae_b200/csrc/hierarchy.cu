@@ -1109,12 +1109,13 @@ void buildGsSchedule(LevelAddr& L, cudaStream_t s)
     }
     // parts: contiguous cell ranges balanced by row length; enough of them to fill the GPU when a
     // depth holds many cells, one when the level is narrow (a single CTA then walks it). One part per
-    // 48 cells of the average depth: measured on B200 against 16, 24, 32, 128, 384 and 1024 (graded
-    // 128^3 and 272^3 solves), more parts shorten each part's chain more than the hand-offs cost.
+    // g_partCells cells of the average depth, 48 by default: measured on B200 against 16, 24, 32,
+    // 128, 384 and 1024 (graded 128^3 and 272^3 solves), more parts shorten each part's chain more
+    // than the hand-offs cost. A batch, whose cases fill the GPU together, is faster with 128.
     const int depthCount = G.maxDepth + 1;
     const long long avgPerDepth = (static_cast<long long>(n) + depthCount - 1) / depthCount;
     const int nSM = DeviceInfo::get().numSMs;
-    int P = static_cast<int>(std::min<long long>(nSM, std::max<long long>(1, avgPerDepth / 48)));
+    int P = static_cast<int>(std::min<long long>(nSM, std::max<long long>(1, avgPerDepth / g_partCells.load())));
     if (n < 4096) P = 1;
     G.nParts = P;
     if (n >= (1 << 30)) fail(B2G_ERR_ARGUMENT, "b2g: a level of 2^30 cells or more does not fit the sweep's codes.");

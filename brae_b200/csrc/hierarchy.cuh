@@ -2,6 +2,8 @@
 // with the derived layouts every kernel reads, and each level step's restriction maps.
 #pragma once
 
+#include <atomic>
+
 #include "b2g_common.cuh"
 
 #include <map>
@@ -64,6 +66,10 @@ struct GsSchedule
 
 // the smallest level that gets the sliced ELL copy of its rows
 constexpr int kEllMinCells = 65536;
+
+// the multi-part sweep's part rule for meshes built from now on: one part per this many cells of a
+// level's average depth (b2g_set_part_cells)
+extern std::atomic<int> g_partCells;
 
 // One smoothing call's sweeps of a level in one pipelined launch (pipe_kernels.cuh), for a given
 // sweep count: the combined steps of every (sweep, cell) item, the cells split into `ranks`

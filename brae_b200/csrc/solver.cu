@@ -15,6 +15,7 @@ namespace b2g {
 
 bool g_profiling = false;
 bool g_pipeline = true;
+std::atomic<int> g_partCells{48};
 
 namespace {
 

@@ -73,6 +73,7 @@ def _load():
         "b2g_set_sweep_pipeline": (ip, [ip]),
         "b2g_coarsest_dense_solve": (ip, [vp, vp, vp]),
         "b2g_assemble_pressure": (ip, [vp] + [vp] * 6 + [ip] + [vp] * 6 + [ip, dp] + [vp] * 5 + [ip, vp]),
+        "b2g_set_part_cells": (ip, [ip]),
         "b2g_level_grid_stall": (ip, [vp, ip, vp, vp, ip, ip, C.c_longlong]),
         "b2g_level_smooth_pipelined": (ip, [vp, ip, vp, vp, ip, ip]),
         "b2g_level_pipe_shape": (ip, [vp, ip, ip, ip, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float),
@@ -155,7 +156,7 @@ EXPORTED = [
     "b2g_batch_launches", "b2g_batch_destroy", "b2g_mesh_set_pair", "b2g_mesh_level_pair",
     "b2g_gamg_solve_coupled", "b2g_matrix_create_coupled", "b2g_matrix_level_pair_coeffs", "b2g_matrix_gamg_solve",
     "b2g_matrix_set_coeffs", "b2g_matrix_level_timings", "b2g_level_smooth_stall", "b2g_set_sweep_pipeline",
-    "b2g_level_smooth_pipelined", "b2g_level_grid_stall", "b2g_level_pipe_shape", "b2g_coarsest_dense_solve", "b2g_assemble_pressure",
+    "b2g_level_smooth_pipelined", "b2g_level_grid_stall", "b2g_set_part_cells", "b2g_level_pipe_shape", "b2g_coarsest_dense_solve", "b2g_assemble_pressure",
 ]
 
 
@@ -501,6 +502,11 @@ class Matrix:
         have = C.c_int()
         _check(lib.b2g_matrix_level_timings(self.handle, kind, cap, ms, reg, un, C.byref(have)))
         return [(ms[i], reg[i], un[i]) for i in range(min(have.value, cap))]
+
+
+def set_part_cells(cells: int) -> None:
+    """The multi-part sweep's part rule for meshes created from now on (b2g_set_part_cells)."""
+    _check(lib.b2g_set_part_cells(int(cells)))
 
 
 def set_profiling(on: bool) -> None:

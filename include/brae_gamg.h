@@ -357,6 +357,12 @@ B2G_API b2g_status b2g_set_profiling(int on);
  * results are the same bit for bit either way; off runs every sweep as its own launch. Process-wide,
  * like b2g_set_profiling. No counterpart in the reference. */
 B2G_API b2g_status b2g_set_sweep_pipeline(int on);
+/* The part rule of the multi-part Gauss-Seidel sweep for meshes created after the call: one part (a
+ * persistent CTA walking a contiguous cell range) per `cells` cells of a level's average depth, at
+ * most one per SM (48 by default, measured best for one solve on the GPU; a batch, whose cases fill
+ * the GPU together, wants fewer parts). Results are the same bit for bit for every rule. 1 <= cells
+ * <= 65536; process-wide. No counterpart in the reference. */
+B2G_API b2g_status b2g_set_part_cells(int cells);
 
 /* Diagnostic: one Gauss-Seidel sweep of `level` (device pointers) recording into the device array
  * `trace` [8 * nChunks + 4 * nParts + 2 * nParts * (maxDepth + 2)] (SM-cycle stamps): per schedule

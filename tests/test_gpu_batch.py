@@ -180,3 +180,21 @@ def test_batch_device_fields_and_refusals(b2g, oracle):
                     b2g.controls_default(solver="GAMG"))
     with pytest.raises(b2g.GamgError, match="appears twice"):
         b2g.Batch([mats[0], mats[1], mats[0]])
+
+
+def test_batch_part_rule(b2g, oracle):
+    # meshes built with the batch's part rule (fewer parts per level): the same bits as the oracle
+    b2g.set_part_cells(128)
+    try:
+        built, meshes, mats = _build(b2g, BOXES[2:5])
+    finally:
+        b2g.set_part_cells(48)
+    batch = b2g.Batch(mats)
+    ctl = b2g.controls_default(tolerance=1e-8, relTol=0.0, reduction="serial")
+    psis = [np.zeros(c.n_cells) for c in built]
+    perfs = batch.solve([c.source for c in built], psis, ctl)
+    for c, psi, perf in zip(built, psis, perfs):
+        want = _oracle(oracle, c, 1e-8, 0.0, {})
+        assert tuple(perf) == want["perf"] and np.array_equal(psi, want["psi"])
+    with pytest.raises(b2g.GamgError):
+        b2g.set_part_cells(0)
