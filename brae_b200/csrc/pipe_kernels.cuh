@@ -52,8 +52,7 @@ namespace k {
 constexpr int kPipeK = 16;        // row entries a thread holds in registers (shared-memory forms)
 constexpr int kPipeGridK = 8;     // the same in the grid form (its 384 threads have fewer registers)
 constexpr int kPipeBlock = 256;   // threads per CTA (shared-memory forms)
-constexpr int kPipeWarps = kPipeBlock / 32;
-constexpr int kPipeGridBlock = 384;
+constexpr int kPipeGridBlock = 384;  // threads per CTA (the grid form: 168 registers, one CTA per SM)
 constexpr int kPipeMaxRanks = 16;
 
 template <class T>
