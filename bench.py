@@ -363,10 +363,14 @@ def run_ours(args, world, rank, local):
     t_rel0 = a0.elapsed_time(a1) / 1e3
     x_rel0 = psi.cpu().numpy()
 
-    try:
-        precision = precision_leg(args, b2g, mesh, dev, stream, world)
-    except Exception as e:  # an extra leg: its failure is reported, the headline line still prints
-        precision = {"error": f"{type(e).__name__}: {e}"}
+    # the extra legs of one GPU (precision form, served stream, coupled pair) run at N = 1 only: with N
+    # replicas they would repeat the same work on every rank and add nothing to the scaling line
+    precision = None
+    if world == 1:
+        try:
+            precision = precision_leg(args, b2g, mesh, dev, stream, world)
+        except Exception as e:  # an extra leg: its failure is reported, the headline line still prints
+            precision = {"error": f"{type(e).__name__}: {e}"}
 
     # roofline of the dominant kernel: the exact Gauss-Seidel sweep (finest level; all levels beside it)
     peak, peak_kind = measured_peaks()
@@ -446,7 +450,7 @@ def run_ours(args, world, rank, local):
     if not args.no_serve and world == 1:
         served = serve_stream(args, b2g, local)
     coupled = None
-    if not args.no_coupled:
+    if not args.no_coupled and world == 1:
         try:
             coupled = coupled_leg(args, b2g, local, world, rank)
         except Exception as e:  # an extra leg: its failure is reported, the headline line still prints
