@@ -372,9 +372,11 @@ __global__ void __launch_bounds__(kPipeGridBlock, 1) gsPipeGrid(PipeArgs<T> a, P
         }
         if (cur.slot >= 0) pipeRowGrid<T>(a, cur);
         for (int k = gridSs[T_] + t + B; k < gridSs[T_ + 1]; k += B) pipeRowGridDirect<T>(a, a.item[k]);
-        // the barrier orders the CTA's psi stores before thread 0's release (release is cumulative)
+        // the barrier orders the CTA's psi stores before the release (release is cumulative). The last
+        // thread releases: it polls no neighbour, so the release's wait for the stores to land does not
+        // hold up this CTA's next polls.
         __syncthreads();
-        if (t == 0 && g.publish) stRelease(mine, static_cast<unsigned>(T_ + 1));
+        if (t == B - 1 && g.publish) stRelease(mine, static_cast<unsigned>(T_ + 1));
         return true;
     };
     int T_ = 0;
