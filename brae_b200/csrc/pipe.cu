@@ -1,7 +1,7 @@
 // pipe.cu -- the pipelined multi-sweep Gauss-Seidel launch (pipe_kernels.cuh): its schedule, built
-// once per (level, sweep count) on the host from the level's addressing, and the choice, by
-// measurement on the device, between its shapes (one CTA, or a cluster of 2..16 CTAs) and the
-// sweep-by-sweep launches.
+// once per (level, sweep count, shape) on the host from the level's addressing, and the choice, by
+// measurement on the device, between its shapes (one CTA; a cluster of 2..16 CTAs; the grid form on
+// 148 or 74 resident CTAs), the item schedule (items.cu) and the sweep-by-sweep launches.
 //
 // Reference: the sweeps it reproduces are gaussSeidelSweeps, src/OpenFOAM/matrices/
 // smooth_solver_cpp.cu:87-166 (forward only for GaussSeidel, :144), called nSweeps times per
@@ -64,7 +64,8 @@ std::vector<int> combinedSteps(const LevelHost& H, int S, int& nSteps)
     return T;
 }
 
-// The schedule for R ranks, or null when a rank's slots do not fit the shared memory.
+// The schedule for R ranks, or null when a rank's slots do not fit the shared memory (the grid form:
+// R resident CTAs, psi in global memory, each rank's neighbour ranks listed).
 std::unique_ptr<PipeSchedule> assemble(const LevelHost& H, const std::vector<int>& T, int S, int nSteps, int R,
                                        size_t valueBytes, cudaStream_t s, bool grid = false)
 {
