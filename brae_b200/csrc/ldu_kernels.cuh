@@ -211,66 +211,33 @@ __global__ void __launch_bounds__(NT) amulScaleDotsProlong(Rows<T> A, const int*
 {
     __shared__ T sh[NT / 32];
     T num = T(0), den = T(0);
-    const int stride = gridDim.x * NT;
-    if (A.ellBase && ellColCoarse)
+    for (int c = blockIdx.x * NT + threadIdx.x; c < A.n; c += gridDim.x * NT)
     {
-        // two rows a pass (c and c + stride, the order the sums take them in either way), their entries
-        // interleaved so that both rows' loads are in flight together
-        for (int c = blockIdx.x * NT + threadIdx.x; c < A.n; c += 2 * stride)
+        const T fc = coarse[prolongP[c]];
+        T acc = mulRn(A.diag[c], fc);
+        if (A.ellBase && ellColCoarse)
         {
-            const int c2 = c + stride;
-            const bool two = c2 < A.n;
-            const int lane = c & 31;
-            const T fc1 = coarse[prolongP[c]];
-            const T fc2 = two ? coarse[prolongP[c2]] : T(0);
-            T acc1 = mulRn(A.diag[c], fc1);
-            T acc2 = two ? mulRn(A.diag[c2], fc2) : T(0);
-            const int b1 = A.ellBase[c >> 5];
-            const int w1 = (A.ellBase[(c >> 5) + 1] - b1) >> 5;
-            const int b2 = two ? A.ellBase[c2 >> 5] : 0;
-            const int w2 = two ? (A.ellBase[(c2 >> 5) + 1] - b2) >> 5 : 0;
-            const int wm = max(w1, w2);
-#pragma unroll 2
-            for (int q = 0; q < wm; ++q)
+            // the sliced rows with each column's coarse position at hand: one gather per entry
+            const int sl = c >> 5, lane = c & 31;
+            const int b0 = A.ellBase[sl];
+            const int w = (A.ellBase[sl + 1] - b0) >> 5;
+#pragma unroll 4
+            for (int q = 0; q < w; ++q)
             {
-                if (q < w1)
-                {
-                    const int e = b1 + 32 * q + lane;
-                    const int cc = ellColCoarse[e];
-                    const T v = A.ellVal[e];
-                    if (cc >= 0) acc1 = addRn(acc1, mulRn(v, coarse[cc]));
-                }
-                if (q < w2)
-                {
-                    const int e = b2 + 32 * q + lane;
-                    const int cc = ellColCoarse[e];
-                    const T v = A.ellVal[e];
-                    if (cc >= 0) acc2 = addRn(acc2, mulRn(v, coarse[cc]));
-                }
-            }
-            Acf[c] = acc1;
-            num = addRn(num, mulRn(fc1, source[c]));
-            den = addRn(den, mulRn(fc1, acc1));
-            if (two)
-            {
-                Acf[c2] = acc2;
-                num = addRn(num, mulRn(fc2, source[c2]));
-                den = addRn(den, mulRn(fc2, acc2));
+                const int e = b0 + 32 * q + lane;
+                const int cc = ellColCoarse[e];
+                const T v = A.ellVal[e];
+                if (cc >= 0) acc = addRn(acc, mulRn(v, coarse[cc]));
             }
         }
-    }
-    else
-    {
-        for (int c = blockIdx.x * NT + threadIdx.x; c < A.n; c += stride)
+        else
         {
-            const T fc = coarse[prolongP[c]];
-            T acc = mulRn(A.diag[c], fc);
             acc = rowFold(A, c, acc,
                           [coarse, prolongP](T a, T v, int cp) { return addRn(a, mulRn(v, coarse[prolongP[cp]])); });
-            Acf[c] = acc;
-            num = addRn(num, mulRn(fc, source[c]));
-            den = addRn(den, mulRn(fc, acc));
         }
+        Acf[c] = acc;
+        num = addRn(num, mulRn(fc, source[c]));
+        den = addRn(den, mulRn(fc, acc));
     }
     num = blockSum<T, NT>(num, sh);
     den = blockSum<T, NT>(den, sh);
