@@ -17,7 +17,7 @@
 namespace b2g {
 namespace {
 
-constexpr size_t kPipeSmemCap = 220 * 1024;  // dynamic shared memory of one rank: its psi slots
+constexpr size_t kPipeSmemCap = 220 * 1024;  // dynamic shared memory of one rank: its psi slots and step table
 
 // The level's addressing on the host, as the schedule builder reads it.
 struct LevelHost
@@ -80,7 +80,9 @@ std::unique_ptr<PipeSchedule> assemble(const LevelHost& H, const std::vector<int
         slotOf[c] = count[rankOf[c]]++;
     }
     const int maxLocal = grid ? 0 : *std::max_element(count.begin(), count.end());
-    if (static_cast<size_t>(maxLocal) * valueBytes > kPipeSmemCap || maxLocal >= (1 << 24)) return nullptr;
+    if (maxLocal >= (1 << 24)) return nullptr;
+    if (!grid && k::pipeStepTableAt(maxLocal, valueBytes) + sizeof(int) * (static_cast<size_t>(nSteps) + 1) > kPipeSmemCap)
+        return nullptr;
     std::vector<int> localPos(std::max<size_t>(static_cast<size_t>(R) * maxLocal, 1), 0);
     if (!grid)
         for (int p = 0; p < n; ++p)
@@ -245,8 +247,8 @@ int pipeKey(int sweeps, size_t valueBytes) { return sweeps * 16 + static_cast<in
 
 size_t pipeSmemBytes(const PipeSchedule& P, size_t valueBytes)
 {
-    if (P.grid) return sizeof(int) * (P.nSteps + 1);
-    return valueBytes * static_cast<size_t>(P.maxLocal);
+    const size_t table = sizeof(int) * (static_cast<size_t>(P.nSteps) + 1);
+    return P.grid ? table : k::pipeStepTableAt(P.maxLocal, valueBytes) + table;
 }
 
 template <class T>

@@ -54,6 +54,9 @@ constexpr int kPipeGridK = 8;     // the same in the grid form (its 384 threads 
 constexpr int kPipeBlock = 256;   // threads per CTA (shared-memory forms)
 constexpr int kPipeGridBlock = 384;  // threads per CTA (the grid form: 168 registers, one CTA per SM)
 constexpr int kPipeMaxRanks = 16;
+// entries past those a thread holds in registers are loaded this many at a time in the shared-memory
+// forms (as many as fit the registers left beside the rows held)
+template <class T> constexpr int kPipeTail = sizeof(T) == 8 ? 4 : 8;
 
 template <class T>
 struct PipeArgs
@@ -192,17 +195,15 @@ __device__ __forceinline__ void pipeLoadRow(const PipeArgs<T>& a, int4 it, bool 
     }
 }
 
-// the shared-memory forms: item k's row into registers (no load waits for another)
+// the shared-memory forms: a row into registers once its item record is known (no load waits for
+// another)
 template <class T>
-__device__ __forceinline__ void pipeLoad(const PipeArgs<T>& a, int k, PipeRow<T, kPipeK>& r)
+__device__ __forceinline__ void pipeLoadRec(const PipeArgs<T>& a, int4 it, bool has, PipeRow<T, kPipeK>& r)
 {
-    r.slot = -1;
-    r.w = 0;
-    if (k < 0) return;
-    const int4 it = a.item[k];
-    r.slot = it.y;
+    r.slot = has ? it.y : -1;
+    r.w = has ? it.w - it.z : 0;
     r.e0 = it.z;
-    r.w = it.w - it.z;
+    if (!has) return;
     r.b = a.b[it.x];
     r.d = a.A.diag[it.x];
 #pragma unroll
@@ -212,6 +213,33 @@ __device__ __forceinline__ void pipeLoad(const PipeArgs<T>& a, int k, PipeRow<T,
             r.v[q] = a.A.val[it.z + q];
             r.ea[q] = a.entAddr[it.z + q];
         }
+}
+
+// Entries [e, end) of a row, folded into acc in order, kPipeTail<T> at a time: the loads of a group are
+// in flight together (one entry at a time, each would wait out its own load), the subtractions keep
+// the row's order.
+template <class T, bool kCluster>
+__device__ __forceinline__ T pipeTail(const PipeArgs<T>& a, int e, int end, T acc, unsigned xa)
+{
+    for (; e < end; e += kPipeTail<T>)
+    {
+        T v[kPipeTail<T>], y[kPipeTail<T>];
+        unsigned ea[kPipeTail<T>];
+#pragma unroll
+        for (int j = 0; j < kPipeTail<T>; ++j)
+            if (e + j < end)
+            {
+                v[j] = a.A.val[e + j];
+                ea[j] = a.entAddr[e + j];
+            }
+#pragma unroll
+        for (int j = 0; j < kPipeTail<T>; ++j)
+            if (e + j < end) y[j] = pipeLd<kCluster>(pipeAddr<T, kCluster>(ea[j], xa), T());
+#pragma unroll
+        for (int j = 0; j < kPipeTail<T>; ++j)
+            if (e + j < end) acc = subRn(acc, mulRn(v[j], y[j]));
+    }
+    return acc;
 }
 
 // the row in the reference's order: the source minus each entry's coefficient times its value, then
@@ -227,9 +255,16 @@ __device__ __forceinline__ void pipeRow(const PipeArgs<T>& a, const PipeRow<T, k
 #pragma unroll
     for (int q = 0; q < kPipeK; ++q)
         if (q < r.w) acc = subRn(acc, mulRn(r.v[q], x[q]));
-    for (int q = kPipeK; q < r.w; ++q)
-        acc = subRn(acc, mulRn(a.A.val[r.e0 + q], pipeLd<kCluster>(pipeAddr<T, kCluster>(a.entAddr[r.e0 + q], xa), T())));
+    acc = pipeTail<T, kCluster>(a, r.e0 + kPipeK, r.e0 + r.w, acc, xa);
     pipeSt(xa + static_cast<unsigned>(sizeof(T)) * static_cast<unsigned>(r.slot), divRn(acc, r.d));
+}
+
+// A row straight from memory (the items beyond the block's width at a step)
+template <class T, bool kCluster>
+__device__ __forceinline__ void pipeRowDirect(const PipeArgs<T>& a, int4 it, unsigned xa)
+{
+    const T acc = pipeTail<T, kCluster>(a, it.z, it.w, a.b[it.x], xa);
+    pipeSt(xa + static_cast<unsigned>(sizeof(T)) * static_cast<unsigned>(it.y), divRn(acc, a.A.diag[it.x]));
 }
 
 // the same row in the grid form: values from psi in global memory, the result stored there
@@ -263,41 +298,56 @@ __device__ __forceinline__ void pipeRowGridDirect(const PipeArgs<T>& a, int4 it)
     a.psi[it.y] = divRn(acc, a.A.diag[it.x]);
 }
 
+// Where a rank's step table starts in the dynamic shared memory of the shared-memory forms: after its
+// maxLocal values, 16-byte aligned.
+__host__ __device__ constexpr size_t pipeStepTableAt(int maxLocal, size_t valueBytes)
+{
+    return (valueBytes * static_cast<size_t>(maxLocal) + 15) / 16 * 16;
+}
+
 // One smoothing call (all its sweeps) of one level. Grid = one cluster of R CTAs (kCluster) or one
-// CTA; dynamic shared memory = maxLocal values of T.
+// CTA; dynamic shared memory = maxLocal values of T, then the rank's step table. Each thread holds two
+// rows (the current step's and the next's) and the item record of the step after them, so no load of
+// a step waits for another load of the same step. (Unrolling the step loop by two, to swap the rows
+// without a copy, needs more registers than a thread has: it spilled and was slower.)
 template <class T, bool kCluster>
 __device__ __forceinline__ void gsPipeBody(const PipeArgs<T>& a)
 {
     extern __shared__ __align__(16) unsigned char pipeSm[];
     T* x = reinterpret_cast<T*>(pipeSm);
+    int* ss = reinterpret_cast<int*>(pipeSm + pipeStepTableAt(a.maxLocal, sizeof(T)));
     const int rank = kCluster ? static_cast<int>(clusterRank()) : 0;
     const int t = threadIdx.x;
     const int B = blockDim.x;
     const unsigned xa = pipeSmemAddr(x);
     const int cnt = a.localCount[rank];
     const int* lp = a.localPos + static_cast<size_t>(rank) * a.maxLocal;
+    const int* gss = a.stepStart + static_cast<size_t>(rank) * (a.nSteps + 1);
+    for (int i = t; i <= a.nSteps; i += B) ss[i] = gss[i];
     for (int i = t; i < cnt; i += B) x[i] = a.psi[lp[i]];
     // every rank's psi is in place before any row reads it
     pipeBarrier<kCluster>();
-    const int* ss = a.stepStart + static_cast<size_t>(rank) * (a.nSteps + 1);
-    PipeRow<T, kPipeK> cur, nxt;
-    pipeLoad(a, a.nSteps > 0 && ss[0] + t < ss[1] ? ss[0] + t : -1, cur);
-    int kn = a.nSteps > 1 && ss[1] + t < ss[2] ? ss[1] + t : -1;
-    for (int T_ = 0; T_ < a.nSteps; ++T_)
-    {
-        // the next step's row (its item index was found a step ago) and the item index after it
-        pipeLoad(a, kn, nxt);
-        kn = T_ + 2 < a.nSteps && ss[T_ + 2] + t < ss[T_ + 3] ? ss[T_ + 2] + t : -1;
+    auto itemAt = [&](int T_) { return T_ < a.nSteps && ss[T_] + t < ss[T_ + 1] ? ss[T_] + t : -1; };
+    const int4 none = make_int4(0, -1, 0, 0);
+    PipeRow<T, kPipeK> r0, r1;
+    int k1 = itemAt(0);
+    pipeLoadRec(a, k1 >= 0 ? a.item[k1] : none, k1 >= 0, r0);
+    k1 = itemAt(1);
+    int4 it1 = k1 >= 0 ? a.item[k1] : none;
+    auto step = [&](int T_, const PipeRow<T, kPipeK>& cur, PipeRow<T, kPipeK>& nxt) {
+        // the next step's row (its item record was loaded a step ago) and the record after it
+        pipeLoadRec(a, it1, k1 >= 0, nxt);
+        k1 = itemAt(T_ + 2);
+        if (k1 >= 0) it1 = a.item[k1];
         if (cur.slot >= 0) pipeRow<T, kCluster>(a, cur, xa);
         // items beyond the block's width at this step, straight from memory
-        for (int k = ss[T_] + t + B; k < ss[T_ + 1]; k += B)
-        {
-            PipeRow<T, kPipeK> r;
-            pipeLoad(a, k, r);
-            pipeRow<T, kCluster>(a, r, xa);
-        }
+        for (int k = ss[T_] + t + B; k < ss[T_ + 1]; k += B) pipeRowDirect<T, kCluster>(a, a.item[k], xa);
         pipeBarrier<kCluster>();
-        cur = nxt;
+    };
+    for (int T_ = 0; T_ < a.nSteps; ++T_)
+    {
+        step(T_, r0, r1);
+        r0 = r1;
     }
     // the last barrier above ordered every read of this CTA's values before the write-back; no rank
     // reads another's shared memory after it, so the CTAs may leave in any order
