@@ -49,7 +49,10 @@
 namespace b2g {
 namespace k {
 
-constexpr int kPipeK = 16;        // row entries a thread holds in registers (shared-memory forms)
+// row entries a thread holds in registers in the shared-memory forms: as many as fit beside two rows
+// (20 FP64, 24 FP32); measured against 12 and 16, the longer rows of the coarse levels (a quarter of
+// them past 16 entries) cost more in tail loads than the registers
+template <class T> constexpr int kPipeK = sizeof(T) == 8 ? 20 : 24;
 constexpr int kPipeGridK = 8;     // the same in the grid form (its 384 threads have fewer registers)
 constexpr int kPipeBlock = 256;   // threads per CTA (shared-memory forms)
 constexpr int kPipeGridBlock = 384;  // threads per CTA (the grid form: 168 registers, one CTA per SM)
@@ -198,7 +201,7 @@ __device__ __forceinline__ void pipeLoadRow(const PipeArgs<T>& a, int4 it, bool 
 // the shared-memory forms: a row into registers once its item record is known (no load waits for
 // another)
 template <class T>
-__device__ __forceinline__ void pipeLoadRec(const PipeArgs<T>& a, int4 it, bool has, PipeRow<T, kPipeK>& r)
+__device__ __forceinline__ void pipeLoadRec(const PipeArgs<T>& a, int4 it, bool has, PipeRow<T, kPipeK<T>>& r)
 {
     r.slot = has ? it.y : -1;
     r.w = has ? it.w - it.z : 0;
@@ -207,7 +210,7 @@ __device__ __forceinline__ void pipeLoadRec(const PipeArgs<T>& a, int4 it, bool 
     r.b = a.b[it.x];
     r.d = a.A.diag[it.x];
 #pragma unroll
-    for (int q = 0; q < kPipeK; ++q)
+    for (int q = 0; q < kPipeK<T>; ++q)
         if (q < r.w)
         {
             r.v[q] = a.A.val[it.z + q];
@@ -245,17 +248,17 @@ __device__ __forceinline__ T pipeTail(const PipeArgs<T>& a, int e, int end, T ac
 // the row in the reference's order: the source minus each entry's coefficient times its value, then
 // the division by the diagonal
 template <class T, bool kCluster>
-__device__ __forceinline__ void pipeRow(const PipeArgs<T>& a, const PipeRow<T, kPipeK>& r, unsigned xa)
+__device__ __forceinline__ void pipeRow(const PipeArgs<T>& a, const PipeRow<T, kPipeK<T>>& r, unsigned xa)
 {
-    T x[kPipeK];
+    T x[kPipeK<T>];
 #pragma unroll
-    for (int q = 0; q < kPipeK; ++q)
+    for (int q = 0; q < kPipeK<T>; ++q)
         if (q < r.w) x[q] = pipeLd<kCluster>(pipeAddr<T, kCluster>(r.ea[q], xa), T());
     T acc = r.b;
 #pragma unroll
-    for (int q = 0; q < kPipeK; ++q)
+    for (int q = 0; q < kPipeK<T>; ++q)
         if (q < r.w) acc = subRn(acc, mulRn(r.v[q], x[q]));
-    acc = pipeTail<T, kCluster>(a, r.e0 + kPipeK, r.e0 + r.w, acc, xa);
+    acc = pipeTail<T, kCluster>(a, r.e0 + kPipeK<T>, r.e0 + r.w, acc, xa);
     pipeSt(xa + static_cast<unsigned>(sizeof(T)) * static_cast<unsigned>(r.slot), divRn(acc, r.d));
 }
 
@@ -329,12 +332,12 @@ __device__ __forceinline__ void gsPipeBody(const PipeArgs<T>& a)
     pipeBarrier<kCluster>();
     auto itemAt = [&](int T_) { return T_ < a.nSteps && ss[T_] + t < ss[T_ + 1] ? ss[T_] + t : -1; };
     const int4 none = make_int4(0, -1, 0, 0);
-    PipeRow<T, kPipeK> r0, r1;
+    PipeRow<T, kPipeK<T>> r0, r1;
     int k1 = itemAt(0);
     pipeLoadRec(a, k1 >= 0 ? a.item[k1] : none, k1 >= 0, r0);
     k1 = itemAt(1);
     int4 it1 = k1 >= 0 ? a.item[k1] : none;
-    auto step = [&](int T_, const PipeRow<T, kPipeK>& cur, PipeRow<T, kPipeK>& nxt) {
+    auto step = [&](int T_, const PipeRow<T, kPipeK<T>>& cur, PipeRow<T, kPipeK<T>>& nxt) {
         // the next step's row (its item record was loaded a step ago) and the record after it
         pipeLoadRec(a, it1, k1 >= 0, nxt);
         k1 = itemAt(T_ + 2);
