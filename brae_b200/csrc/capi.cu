@@ -991,6 +991,21 @@ b2g_status b2g_level_sweep_shape(const b2g_mesh* mesh, int level, int* wholeLeve
     });
 }
 
+b2g_status b2g_level_mc_pipe(const b2g_mesh* mesh, int level, int nSweeps, int symmetric, int* ranks,
+                             float* msPipe, float* msColours)
+{
+    return guarded([&] {
+        need(mesh != nullptr, "b2g_level_mc_pipe: null mesh");
+        need(level >= 0 && level <= mesh->m.nLevels(), "b2g_level_mc_pipe: no such level");
+        const b2g::Colouring& C = mesh->m.lev[level].mc;
+        const auto it = C.pipe.find(nSweeps * 2 + (symmetric ? 1 : 0));
+        const bool have = it != C.pipe.end();
+        if (ranks) *ranks = have && it->second.use ? it->second.sched->ranks : 0;
+        if (msPipe) *msPipe = have ? it->second.msPipe : 0.f;
+        if (msColours) *msColours = have ? it->second.msColours : 0.f;
+    });
+}
+
 b2g_status b2g_fold_boundary(int nCells, int nBFaces, const int32_t* faceCells, const double* internalCoeffs,
                              const double* boundaryCoeffs, const unsigned char* coupled, double* diag, double* source,
                              int memspace, void* stream)

@@ -145,6 +145,15 @@ struct Colouring
     int cluster = 0;
     int block = 256;
     float msPerSweep = 0.f;
+    // per smoothing call of nSweeps sweeps (key nSweeps * 2 + symmetric): the pipelined shared-memory
+    // launch (pipe.cu) whose steps are the colours, kept where it measured faster than the shape above
+    struct Pipe
+    {
+        std::unique_ptr<PipeSchedule> sched;
+        bool use = false;
+        float msPipe = 0.f, msColours = 0.f;  // per smoothing call, as measured
+    };
+    std::map<int, Pipe> pipe;
 };
 
 // The coupled (cyclic) pair of one level (pair.cu, b2g_mesh_set_pair): its faces, each once from

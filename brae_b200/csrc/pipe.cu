@@ -164,6 +164,34 @@ std::unique_ptr<PipeSchedule> assemble(const LevelHost& H, const std::vector<int
     return P;
 }
 
+// The multicolour smoother's sweeps as a pipelined schedule: item (sweep s, cell c) runs at step
+// s * stepsPerSweep + k for a cell of colour k; symmetric sweeps visit the colours forward then back,
+// each cell twice a sweep. No two cells of a colour share a face, so a step's items are independent,
+// and each row reads the values the colour-by-colour sweep gives it. Null when a cell has no colour.
+std::unique_ptr<PipeSchedule> colourSchedule(const LevelHost& H, const Colouring& C, const std::vector<int>& rowPos,
+                                             int nSweeps, bool symmetric, int R, cudaStream_t s)
+{
+    const int n = H.n;
+    std::vector<int> colourOf(n, -1);
+    for (int k = 0; k < C.nColours; ++k)
+        for (int r = C.colourStart[k]; r < C.colourStart[k + 1]; ++r)
+            if (rowPos[r] >= 0) colourOf[H.posCell[rowPos[r]]] = k;
+    for (int c = 0; c < n; ++c)
+        if (colourOf[c] < 0) return nullptr;
+    const int per = symmetric ? 2 : 1;
+    const int stepsPerSweep = per * C.nColours;
+    const int S = nSweeps * per;
+    std::vector<int> T(static_cast<size_t>(S) * n);
+    for (int sw = 0; sw < nSweeps; ++sw)
+        for (int c = 0; c < n; ++c)
+        {
+            const int k = colourOf[c];
+            T[static_cast<size_t>(sw * per) * n + c] = sw * stepsPerSweep + k;
+            if (symmetric) T[static_cast<size_t>(sw * per + 1) * n + c] = sw * stepsPerSweep + 2 * C.nColours - 1 - k;
+        }
+    return assemble(H, T, S, nSweeps * stepsPerSweep, R, sizeof(float), s);
+}
+
 template <class T>
 void allowPipeSmem()
 {
@@ -180,6 +208,17 @@ void allowPipeSmem()
     // then finds no such shape resident)
     if (cudaFuncSetAttribute(k::gsPipe<T, true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
         cudaGetLastError();
+    if constexpr (sizeof(T) == 4)
+    {
+        // the multicolour smoother's launches (the colours as steps)
+        B2G_CUDA(cudaFuncSetAttribute(k::gsPipe<T, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(kPipeSmemCap)));
+        B2G_CUDA(cudaFuncSetAttribute(k::gsPipe<T, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(kPipeSmemCap)));
+        if (cudaFuncSetAttribute(k::gsPipe<T, true, true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+            cudaSuccess)
+            cudaGetLastError();
+    }
     done.fetch_or(bit);
 }
 
@@ -205,11 +244,17 @@ struct PipeLaunch
 };
 
 template <class T>
-bool pipeClusterFits(int ranks, size_t smem, cudaStream_t s)
+bool pipeClusterFits(int ranks, size_t smem, cudaStream_t s, bool fma = false)
 {
     PipeLaunch L(ranks, smem, s);
     int n = 0;
-    if (cudaOccupancyMaxActiveClusters(&n, k::gsPipe<T, true>, &L.cfg) != cudaSuccess)
+    cudaError_t e;
+    if constexpr (sizeof(T) == 4)
+        e = fma ? cudaOccupancyMaxActiveClusters(&n, k::gsPipe<T, true, true>, &L.cfg)
+                : cudaOccupancyMaxActiveClusters(&n, k::gsPipe<T, true>, &L.cfg);
+    else
+        e = cudaOccupancyMaxActiveClusters(&n, k::gsPipe<T, true>, &L.cfg);
+    if (e != cudaSuccess)
     {
         cudaGetLastError();
         return false;
@@ -269,7 +314,7 @@ k::PipeArgs<T> Matrix::pipeArgs(int level, const PipeSchedule& P, T* psiL, const
 }
 
 template <class T>
-void Matrix::pipeLaunch(int level, const PipeSchedule& P, T* psiL, const T* src)
+void Matrix::pipeLaunch(int level, const PipeSchedule& P, T* psiL, const T* src, bool fma)
 {
     const k::PipeArgs<T> a = pipeArgs<T>(level, P, psiL, src);
     const size_t smem = pipeSmemBytes(P, sizeof(T));
@@ -297,6 +342,24 @@ void Matrix::pipeLaunch(int level, const PipeSchedule& P, T* psiL, const T* src)
         launches += 2;
         return;
     }
+    if constexpr (sizeof(T) == 4)
+        if (fma)
+        {
+            // the multicolour smoother's arithmetic
+            if (P.ranks == 1)
+            {
+                k::gsPipe<T, false, true><<<1, k::kPipeBlock, smem, stream>>>(a);
+                B2G_LAUNCH_CHECK();
+            }
+            else
+            {
+                PipeLaunch C(P.ranks, smem, stream);
+                B2G_CUDA(cudaLaunchKernelEx(&C.cfg, k::gsPipe<T, true, true>, a));
+            }
+            ++launches;
+            return;
+        }
+    if (fma) fail(B2G_ERR_STATE, "b2g: the multicolour pipelined launch is FP32 only");
     if (P.ranks == 1)
     {
         k::gsPipe<T, false><<<1, k::kPipeBlock, smem, stream>>>(a);
@@ -531,6 +594,65 @@ void Matrix::ensurePipe(int level, int nSweeps)
     B2G_CUDA(cudaStreamSynchronize(stream));
 }
 
+// The multicolour smoothing call of nSweeps sweeps on `level` as one pipelined launch over the colours
+// (colourSchedule), on one CTA or a cluster of 2-16, against the tuned colour-by-colour shape
+// (Matrix::tuneMulticolour): the faster is kept. Both compute every row with the same fused
+// multiply-adds in the same order on the same values, so the choice changes the time only.
+void Matrix::ensureMcPipe(int level, int nSweeps, bool symmetric)
+{
+    LevelAddr& L = mesh->lev[level];
+    Colouring& C = L.mc;
+    const int key = nSweeps * 2 + (symmetric ? 1 : 0);
+    if (C.pipe.count(key)) return;
+    Colouring::Pipe& M = C.pipe[key];
+    if (nSweeps < 1 || L.nCells == 0 || C.nColours == 0 || !C.tuned) return;
+    if (L.nCells > k::kPipeMaxRanks * static_cast<int>(kPipeSmemCap / sizeof(float))) return;
+    allowPipeSmem<float>();
+    float* x = level == 0 ? w32.p : v32.corr[level - 1].p;
+    float* b = level == 0 ? r32.p : v32.src[level - 1].p;
+    // scratch vectors of the level (the times do not depend on the values)
+    B2G_CUDA(cudaMemsetAsync(x, 0, sizeof(float) * static_cast<size_t>(nAlloc(level)), stream));
+    B2G_CUDA(cudaMemsetAsync(b, 0, sizeof(float) * static_cast<size_t>(nAlloc(level)), stream));
+    cudaEvent_t e0, e1;
+    B2G_CUDA(cudaEventCreate(&e0));
+    B2G_CUDA(cudaEventCreate(&e1));
+    const long long l0 = launches;
+    auto timeIt = [&](auto&& launch) {
+        launch();  // warm
+        B2G_CUDA(cudaEventRecord(e0, stream));
+        for (int i = 0; i < 3; ++i) launch();
+        B2G_CUDA(cudaEventRecord(e1, stream));
+        B2G_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        B2G_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        return ms / 3.f;
+    };
+    M.msColours = timeIt([&] { mcLaunch(level, C.fused, C.cluster, C.block, x, b, nSweeps, false, symmetric); });
+    checkDeviceError();
+    const LevelHost H = download(L, stream);
+    const std::vector<int> rowPos = C.pos.download(stream);
+    float best = M.msColours;
+    for (int R : {1, 2, 4, 8, 16})
+    {
+        std::unique_ptr<PipeSchedule> P = colourSchedule(H, C, rowPos, nSweeps, symmetric, R, stream);
+        if (!P) continue;
+        if (R > 1 && !pipeClusterFits<float>(R, pipeSmemBytes(*P, sizeof(float)), stream, true)) continue;
+        const float ms = timeIt([&] { pipeLaunch<float>(level, *P, x, b, true); });
+        if (M.msPipe == 0.f || ms < M.msPipe) M.msPipe = ms;
+        if (ms < best)
+        {
+            best = ms;
+            M.sched = std::move(P);
+            M.use = true;
+        }
+    }
+    launches = l0;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    B2G_CUDA(cudaStreamSynchronize(stream));
+    checkDeviceError();
+}
+
 // Before a capture: the item blobs of every item-schedule choice, filled for the current
 // coefficients.
 template <class T>
@@ -649,8 +771,8 @@ template bool Matrix::pipeForced<double>(int, double*, const double*, int, int);
 template void Matrix::ensurePipe<float>(int, int);
 template bool Matrix::pipeSweeps<double>(int, double*, const double*, int);
 template bool Matrix::pipeSweeps<float>(int, float*, const float*, int);
-template void Matrix::pipeLaunch<double>(int, const PipeSchedule&, double*, const double*);
-template void Matrix::pipeLaunch<float>(int, const PipeSchedule&, float*, const float*);
+template void Matrix::pipeLaunch<double>(int, const PipeSchedule&, double*, const double*, bool);
+template void Matrix::pipeLaunch<float>(int, const PipeSchedule&, float*, const float*, bool);
 template void Matrix::refreshItems<double>();
 template k::PipeArgs<double> Matrix::pipeArgs<double>(int, const PipeSchedule&, double*, const double*);
 template k::PipeArgs<float> Matrix::pipeArgs<float>(int, const PipeSchedule&, float*, const float*);

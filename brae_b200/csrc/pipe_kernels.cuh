@@ -218,10 +218,23 @@ __device__ __forceinline__ void pipeLoadRec(const PipeArgs<T>& a, int4 it, bool 
         }
 }
 
+// One term of a row: the exact sweeps subtract the rounded product (the reference's arithmetic); the
+// multicolour smoother (kFma) folds it in one fused multiply-add, as its colour-by-colour kernels do.
+template <bool kFma>
+__device__ __forceinline__ double pipeTerm(double acc, double v, double x)
+{
+    return kFma ? __fma_rn(-v, x, acc) : subRn(acc, mulRn(v, x));
+}
+template <bool kFma>
+__device__ __forceinline__ float pipeTerm(float acc, float v, float x)
+{
+    return kFma ? __fmaf_rn(-v, x, acc) : subRn(acc, mulRn(v, x));
+}
+
 // Entries [e, end) of a row, folded into acc in order, kPipeTail<T> at a time: the loads of a group are
 // in flight together (one entry at a time, each would wait out its own load), the subtractions keep
 // the row's order.
-template <class T, bool kCluster>
+template <class T, bool kCluster, bool kFma>
 __device__ __forceinline__ T pipeTail(const PipeArgs<T>& a, int e, int end, T acc, unsigned xa)
 {
     for (; e < end; e += kPipeTail<T>)
@@ -240,14 +253,14 @@ __device__ __forceinline__ T pipeTail(const PipeArgs<T>& a, int e, int end, T ac
             if (e + j < end) y[j] = pipeLd<kCluster>(pipeAddr<T, kCluster>(ea[j], xa), T());
 #pragma unroll
         for (int j = 0; j < kPipeTail<T>; ++j)
-            if (e + j < end) acc = subRn(acc, mulRn(v[j], y[j]));
+            if (e + j < end) acc = pipeTerm<kFma>(acc, v[j], y[j]);
     }
     return acc;
 }
 
 // the row in the reference's order: the source minus each entry's coefficient times its value, then
 // the division by the diagonal
-template <class T, bool kCluster>
+template <class T, bool kCluster, bool kFma>
 __device__ __forceinline__ void pipeRow(const PipeArgs<T>& a, const PipeRow<T, kPipeK<T>>& r, unsigned xa)
 {
     T x[kPipeK<T>];
@@ -257,16 +270,16 @@ __device__ __forceinline__ void pipeRow(const PipeArgs<T>& a, const PipeRow<T, k
     T acc = r.b;
 #pragma unroll
     for (int q = 0; q < kPipeK<T>; ++q)
-        if (q < r.w) acc = subRn(acc, mulRn(r.v[q], x[q]));
-    acc = pipeTail<T, kCluster>(a, r.e0 + kPipeK<T>, r.e0 + r.w, acc, xa);
+        if (q < r.w) acc = pipeTerm<kFma>(acc, r.v[q], x[q]);
+    acc = pipeTail<T, kCluster, kFma>(a, r.e0 + kPipeK<T>, r.e0 + r.w, acc, xa);
     pipeSt(xa + static_cast<unsigned>(sizeof(T)) * static_cast<unsigned>(r.slot), divRn(acc, r.d));
 }
 
 // A row straight from memory (the items beyond the block's width at a step)
-template <class T, bool kCluster>
+template <class T, bool kCluster, bool kFma>
 __device__ __forceinline__ void pipeRowDirect(const PipeArgs<T>& a, int4 it, unsigned xa)
 {
-    const T acc = pipeTail<T, kCluster>(a, it.z, it.w, a.b[it.x], xa);
+    const T acc = pipeTail<T, kCluster, kFma>(a, it.z, it.w, a.b[it.x], xa);
     pipeSt(xa + static_cast<unsigned>(sizeof(T)) * static_cast<unsigned>(it.y), divRn(acc, a.A.diag[it.x]));
 }
 
@@ -313,7 +326,7 @@ __host__ __device__ constexpr size_t pipeStepTableAt(int maxLocal, size_t valueB
 // rows (the current step's and the next's) and the item record of the step after them, so no load of
 // a step waits for another load of the same step. (Unrolling the step loop by two, to swap the rows
 // without a copy, needs more registers than a thread has: it spilled and was slower.)
-template <class T, bool kCluster>
+template <class T, bool kCluster, bool kFma = false>
 __device__ __forceinline__ void gsPipeBody(const PipeArgs<T>& a)
 {
     extern __shared__ __align__(16) unsigned char pipeSm[];
@@ -342,9 +355,9 @@ __device__ __forceinline__ void gsPipeBody(const PipeArgs<T>& a)
         pipeLoadRec(a, it1, k1 >= 0, nxt);
         k1 = itemAt(T_ + 2);
         if (k1 >= 0) it1 = a.item[k1];
-        if (cur.slot >= 0) pipeRow<T, kCluster>(a, cur, xa);
+        if (cur.slot >= 0) pipeRow<T, kCluster, kFma>(a, cur, xa);
         // items beyond the block's width at this step, straight from memory
-        for (int k = ss[T_] + t + B; k < ss[T_ + 1]; k += B) pipeRowDirect<T, kCluster>(a, a.item[k], xa);
+        for (int k = ss[T_] + t + B; k < ss[T_ + 1]; k += B) pipeRowDirect<T, kCluster, kFma>(a, a.item[k], xa);
         pipeBarrier<kCluster>();
     };
     for (int T_ = 0; T_ < a.nSteps; ++T_)
@@ -357,10 +370,11 @@ __device__ __forceinline__ void gsPipeBody(const PipeArgs<T>& a)
     for (int i = t; i < cnt; i += B) a.psi[lp[i]] = x[i];
 }
 
-template <class T, bool kCluster>
+// kFma: the multicolour smoother's arithmetic (its steps are the colours of a colouring schedule)
+template <class T, bool kCluster, bool kFma = false>
 __global__ void __launch_bounds__(kPipeBlock, 1) gsPipe(PipeArgs<T> a)
 {
-    gsPipeBody<T, kCluster>(a);
+    gsPipeBody<T, kCluster, kFma>(a);
 }
 
 // One smoothing call of many independent cases' levels in ONE launch, each on one CTA: block i runs

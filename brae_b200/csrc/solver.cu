@@ -1029,6 +1029,22 @@ void Matrix::prepareSmoother(const b2g_controls& c)
         if (exact64) refreshItems<double>();
         else refreshItems<float>();
     }
+    // the multicolour form: each smoothing call the V-cycle makes as one pipelined launch over the
+    // colours where that measured faster, chosen before any capture
+    const bool mcSweeps = c.smoother != B2G_SMOOTHER_DIC && c.solver != B2G_SOLVER_GAMG &&
+                          c.precision == B2G_PRECISION_FP32_PRECOND_MULTICOLOUR;
+    if (g_pipeline && mcSweeps)
+    {
+        auto want = [&](int level, int nSweeps) {
+            if (nSweeps > 0 && level <= nLevels()) ensureMcPipe(level, nSweeps, sym);
+        };
+        want(0, c.nFinestSweeps);
+        for (int li = 0; li + 1 < nLevels(); ++li)
+        {
+            want(li + 1, std::min(c.nPostSweeps + c.postSweepsLevelMultiplier * li, c.maxPostSweeps));
+            if (c.nPreSweeps) want(li + 1, std::min(c.nPreSweeps + c.preSweepsLevelMultiplier * li, c.maxPreSweeps));
+        }
+    }
     // the resident sweep's depth ranges of the small one-part levels, before any iteration is captured
     if (c.smoother != B2G_SMOOTHER_DIC)
         for (int i = 1; i < nLevels(); ++i) ensureResident(i);
@@ -1181,6 +1197,13 @@ void Matrix::symSmooth(int level, T* psiL, const T* src, int nSweeps)
 void Matrix::mcSmooth(int level, float* psiL, const float* src, int nSweeps, bool symmetric)
 {
     const Colouring& C = mesh->lev[level].mc;
+    // the call as one pipelined launch over the colours, where that measured faster (ensureMcPipe)
+    const auto it = C.pipe.find(nSweeps * 2 + (symmetric ? 1 : 0));
+    if (g_pipeline && it != C.pipe.end() && it->second.use)
+    {
+        pipeLaunch<float>(level, *it->second.sched, psiL, src, true);
+        return;
+    }
     mcLaunch(level, C.fused, C.cluster, C.block, psiL, src, nSweeps, true, symmetric);
 }
 

@@ -187,7 +187,7 @@ struct Matrix
     // the pipelined multi-sweep launch (pipe.cu): the level's tuned choice, built on first use
     template <class T> void ensurePipe(int level, int nSweeps);
     template <class T> bool pipeSweeps(int level, T* psi, const T* source, int nSweeps);
-    template <class T> void pipeLaunch(int level, const PipeSchedule& P, T* psi, const T* source);
+    template <class T> void pipeLaunch(int level, const PipeSchedule& P, T* psi, const T* source, bool fma = false);
     template <class T> k::PipeArgs<T> pipeArgs(int level, const PipeSchedule& P, T* psi, const T* source);
     template <class T> bool pipeForced(int level, T* psi, const T* source, int nSweeps, int ranks);
     // an item schedule's launch (items.cu): its blobs filled for the current coefficients first
@@ -205,6 +205,10 @@ struct Matrix
     void mcLaunch(int level, bool fused, int cluster, int block, float* psi, const float* source, int nSweeps,
                   bool timed, bool symmetric = false);
     void tuneMulticolour(int level);
+    // the multicolour smoothing call of nSweeps sweeps on `level` as one pipelined launch whose steps
+    // are the colours (pipe.cu), chosen by timing against the tuned colour-by-colour shape; outside any
+    // capture
+    void ensureMcPipe(int level, int nSweeps, bool symmetric);
     int nLevels() const { return mesh->nLevels(); }
     int n(int level) const { return mesh->lev[level].nCells; }
     size_t nAlloc(int level) const { return static_cast<size_t>(std::max(mesh->lev[level].gs.nAlloc, 1)); }

@@ -110,6 +110,7 @@ def _load():
         "b2g_level_colouring": (ip, [vp, ip, C.POINTER(C.c_int), vp]),
         "b2g_fold_boundary": (ip, [ip, ip, vp, vp, vp, vp, vp, vp, ip, vp]),
         "b2g_level_sweep_shape": (ip, [vp, ip, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float)]),
+        "b2g_level_mc_pipe": (ip, [vp, ip, ip, ip, C.POINTER(C.c_int), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
         "b2g_precondition": (ip, [vp, C.POINTER(Controls), vp, vp, C.POINTER(_Log)]),
         "b2g_matrix_pcg_solve": (ip, [vp, vp, vp, C.POINTER(Controls), ip, C.POINTER(_Perf),
                                       C.POINTER(_Log)]),
@@ -151,7 +152,7 @@ EXPORTED = [
     "b2g_level_amul", "b2g_level_smooth", "b2g_level_scale", "b2g_step_restrict",
     "b2g_step_prolong", "b2g_level_norm_factor", "b2g_level_pcg_dic", "b2g_precondition",
     "b2g_matrix_pcg_solve", "b2g_matrix_timings", "b2g_level_smooth_trace", "b2g_level_pcg_dic_static",
-    "b2g_level_schedule", "b2g_level_colouring", "b2g_fold_boundary", "b2g_level_sweep_shape", "b2g_server_create", "b2g_server_destroy", "b2g_server_add_case",
+    "b2g_level_schedule", "b2g_level_colouring", "b2g_fold_boundary", "b2g_level_sweep_shape", "b2g_level_mc_pipe", "b2g_server_create", "b2g_server_destroy", "b2g_server_add_case",
     "b2g_server_submit", "b2g_server_wait", "b2g_server_case_bytes", "b2g_batch_create", "b2g_batch_solve",
     "b2g_batch_launches", "b2g_batch_destroy", "b2g_mesh_set_pair", "b2g_mesh_level_pair",
     "b2g_gamg_solve_coupled", "b2g_matrix_create_coupled", "b2g_matrix_level_pair_coeffs", "b2g_matrix_gamg_solve",
@@ -290,6 +291,14 @@ class Mesh:
         starts = np.zeros(n.value + 1, np.int32)
         _check(lib.b2g_level_colouring(self.handle, level, C.byref(n), _ptr(starts)))
         return starts
+
+    def mc_pipe(self, level: int, n_sweeps: int, symmetric: bool = False) -> dict:
+        """Whether `level`'s multicolour smoothing calls of n_sweeps sweeps run as one pipelined launch
+        over the colours (b2g_level_mc_pipe): its CTAs (0: colour by colour) and both measured times."""
+        r, mp, mc = C.c_int(), C.c_float(), C.c_float()
+        _check(lib.b2g_level_mc_pipe(self.handle, level, n_sweeps, 1 if symmetric else 0, C.byref(r), C.byref(mp),
+                                     C.byref(mc)))
+        return {"ranks": r.value, "ms_pipelined": mp.value, "ms_colours": mc.value}
 
     def sweep_shape(self, level: int) -> dict:
         """The autotuner's multicolour sweep shape for `level` (zeros before the form's first solve):

@@ -521,6 +521,14 @@ B2G_API b2g_status b2g_level_colouring(const b2g_mesh* mesh, int level, int* nCo
  * size; *msPerSweep the measured time of one sweep. All 0 before. */
 B2G_API b2g_status b2g_level_sweep_shape(const b2g_mesh* mesh, int level, int* wholeLevelCtas,
                                          int* threadsPerBlock, float* msPerSweep);
+/* Diagnostic: for `level`'s multicolour smoothing calls of nSweeps sweeps (symmetric 1 for
+ * symGaussSeidel), whether they run as one pipelined launch whose steps are the colours: *ranks its
+ * CTAs (one, or a thread-block cluster), 0 if the colour-by-colour shape above was faster or the
+ * level is not pipelined; *msPipe the best pipelined shape's measured time per call (0: not tried);
+ * *msColours the colour-by-colour shape's. All 0 before the form's first solve. Any output may be
+ * NULL. */
+B2G_API b2g_status b2g_level_mc_pipe(const b2g_mesh* mesh, int level, int nSweeps, int symmetric, int* ranks,
+                                     float* msPipe, float* msColours);
 
 /* Library version string. */
 B2G_API const char* b2g_version(void);

@@ -330,6 +330,36 @@ def test_fp32_multicolour_form(b2g, oracle, kw):
         assert len(mesh.colouring(level)) >= 2
 
 
+@pytest.mark.parametrize("smoother", ["GaussSeidel", "symGaussSeidel"])
+@pytest.mark.parametrize("kw", [dict(nx=32, ny=30, nz=28, lengths=(2.0, 1.0, 1.0), grading_y=20.0),
+                                dict(nx=24, ny=20, nz=22, lengths=(2.0, 1.0, 1.0), grading_y=20.0, two_phase=True)],
+                         ids=["graded", "two_phase"])
+def test_fp32_multicolour_pipelined_same_bits(b2g, kw, smoother):
+    # the multicolour smoothing calls as one pipelined launch over the colours (psi in shared memory)
+    # where the tuner measured that faster: every row the same fused multiply-adds in the same order
+    # on the same values as the colour-by-colour launches, so the solve's bits do not change
+    c = cases.box_case(**kw)
+    mesh = b2g.Mesh(c.lower, c.upper, c.Sf, c.magSf, c.n_cells, 10, True)
+    ctl = b2g.controls_default(tolerance=1e-9, relTol=0.0, precision="fp32_precond_multicolour", smoother=smoother)
+    out = {}
+    try:
+        for on in (True, False):
+            b2g.set_sweep_pipeline(on)
+            psi = np.zeros(c.n_cells)
+            perf = b2g.pcg_gamg_solve(mesh, c.diag, c.coef, c.source, psi, ctl)[0]
+            out[on] = (psi, tuple(perf))
+    finally:
+        b2g.set_sweep_pipeline(True)
+    assert out[True][1] == out[False][1]
+    assert np.array_equal(out[True][0], out[False][0])
+    assert out[True][1][1] < 1e-9
+    sym = smoother == "symGaussSeidel"
+    shapes = [mesh.mc_pipe(lv, 2 if lv == 0 else min(2 + lv - 1, 4), sym) for lv in range(mesh.n_levels + 1)]
+    # each smoothed coarse level's calls were timed both ways, and some took the pipelined launch
+    assert all(s["ms_colours"] > 0.0 for s in shapes[1:mesh.n_levels])
+    assert any(s["ranks"] > 0 for s in shapes)
+
+
 def test_refusals(b2g):
     # three cells and no faces: no pass reduces the count, so no coarse level exists and the solve
     # refuses by name, as GAMGSolver.C:333 does
