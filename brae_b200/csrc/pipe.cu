@@ -1,7 +1,9 @@
 // pipe.cu -- the pipelined multi-sweep Gauss-Seidel launch (pipe_kernels.cuh): its schedule, built
 // once per (level, sweep count, shape) on the host from the level's addressing, and the choice, by
 // measurement on the device, between its shapes (one CTA; a cluster of 2..16 CTAs; the grid form on
-// 148 or 74 resident CTAs), the item schedule (items.cu) and the sweep-by-sweep launches.
+// 148 or 74 resident CTAs), the item schedule (items.cu) and the sweep-by-sweep launches. The same
+// launch also runs the multicolour FP32 smoother's calls, with the colours as its steps
+// (colourSchedule, Matrix::ensureMcPipe).
 //
 // Reference: the sweeps it reproduces are gaussSeidelSweeps, src/OpenFOAM/matrices/
 // smooth_solver_cpp.cu:87-166 (forward only for GaussSeidel, :144), called nSweeps times per
